@@ -1,0 +1,190 @@
+/*
+ * snapmrf.h -- C ABI of the B200-native snapMRF hot path.
+ *
+ * The path: MRF dictionary generation (extended-phase-graph recursion for
+ * the FISP / SSFP / SR / SE / TSE echo types, ROA Bloch isochromats) and
+ * maximum-inner-product template matching of voxel signal evolutions into
+ * T1 / T2 / B0 / B1 / PD maps.
+ *
+ * Conventions (all entry points):
+ *   - plain C types only; complex arrays are interleaved float pairs
+ *     (re, im), i.e. the reference's float2 layout;
+ *   - device pointers are caller-owned; scratch is allocated stream-ordered
+ *     inside the call and released before it returns;
+ *   - `stream` is a cudaStream_t passed as void* (NULL = legacy stream);
+ *     device work is enqueued on it and the call returns without waiting,
+ *     except where a function says it synchronises;
+ *   - every entry point returns a snapmrf_status; snapmrf_last_error()
+ *     returns the message of the last failure on the calling thread.
+ *     Nothing in the library prints, waits on stdin or exits.
+ *
+ * Layouts follow the reference (src/functions.h, src/mrf.cu):
+ *   params [NATOMS][nparams] = {T1 ms, T2 ms, B0 Hz, B1}
+ *   schedule h_mrf [4][NREPS] = CSV columns (flip, phase, TR, TE)
+ *   atoms  [NATOMS][nreps] complex
+ *   image  [nvoxels][img_stride] complex
+ *   maps   [nvoxels][nmaps] = {T1, T2, B0, B1, PD}
+ */
+#ifndef SNAPMRF_H
+#define SNAPMRF_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum snapmrf_status {
+    SNAPMRF_OK = 0,
+    SNAPMRF_ERR_INVALID = 1,     /* bad argument or size */
+    SNAPMRF_ERR_ECHO_TYPE = 2,   /* unknown echo type (reference: err(EX_USAGE)) */
+    SNAPMRF_ERR_CUDA = 3,        /* a CUDA runtime call or launch failed */
+    SNAPMRF_ERR_ALLOC = 4,       /* device or host allocation failed */
+    SNAPMRF_ERR_IO = 5,          /* file open / read / write failed */
+    SNAPMRF_ERR_FORMAT = 6,      /* malformed RA / CSV / grid string */
+    SNAPMRF_ERR_UNSUPPORTED = 7, /* valid request this build does not handle */
+    SNAPMRF_ERR_DEVICE = 8       /* device-side check failed (bounded wait, bad index) */
+} snapmrf_status;
+
+/* Message of the last failing call on this thread ("" if none). */
+const char *snapmrf_last_error(void);
+/* Library version string. */
+const char *snapmrf_version(void);
+
+/* ------------------------------------------------------------------------
+ * Host: schedules, grids and the parameter table.
+ * Each keeps the float arithmetic of the reference function it replaces.
+ * ---------------------------------------------------------------------- */
+
+/* Number of '\n' in the file (replaces csv_dim, src/functions.cu:100-120).
+ * Returns (size_t)-1 when the file cannot be opened. */
+size_t snapmrf_csv_dim(const char *path);
+
+/* Reads up to nreps schedule rows into h_mrf[4][nreps], skipping the first
+ * two 100-byte fgets chunks exactly like csv_read (src/functions.cu:122-158). */
+int snapmrf_csv_read(float *h_mrf, size_t nreps, const char *path);
+
+/* "min", "min:max" or "min:step:max" (parse_range, src/functions.cu:197-237). */
+int snapmrf_parse_range(const char *str, float *min, float *step, float *max, size_t *len);
+
+/* Length of a '+'-joined grid string (parse_length, src/functions.cu:239-269).
+ * Returns 0 on a malformed string. */
+size_t snapmrf_parse_length(const char *str);
+
+/* Fills h_p[LEN] from a grid string (parse_params, src/functions.cu:315-353). */
+int snapmrf_parse_params(float *h_p, const char *str, size_t LEN);
+
+/* linspace / logspace (src/functions.cu:271-313), including logspace's
+ * symmetric negative branch used by the -N grids. */
+void snapmrf_linspace(float *h_p, float min, float step, size_t len);
+void snapmrf_logspace(float *h_p, float min, float max, size_t len);
+
+/* Atoms with T1 > T2, times l_b0 * l_b1 (compute_natoms, src/functions.cu:393-414). */
+size_t snapmrf_compute_natoms(const float *h_t1, const float *h_t2, size_t l_t1,
+                              size_t l_t2, size_t l_b0, size_t l_b1);
+
+/* params[NATOMS][nparams] in B1 > B0 > T2 > T1 order, T1 > T2 only
+ * (trans_params, src/functions.cu:355-391). */
+int snapmrf_trans_params(float *h_params, const float *h_t1, const float *h_t2,
+                         const float *h_b0, const float *h_b1, size_t l_t1, size_t l_t2,
+                         size_t l_b0, size_t l_b1, size_t NATOMS, int nparams);
+
+/* ------------------------------------------------------------------------
+ * RA files (replaces ra_read / ra_write / ra_free, src/ra.h:60-74,
+ * src/ra.cu:23-104).  Same 48-byte header + dims + data layout.
+ * ---------------------------------------------------------------------- */
+typedef struct snapmrf_ra {
+    uint64_t flags;
+    uint64_t eltype; /* 0 user, 1 int, 2 uint, 3 float, 4 complex */
+    uint64_t elbyte;
+    uint64_t size;   /* data bytes */
+    uint64_t ndims;
+    uint64_t *dims;
+    uint8_t *data;
+} snapmrf_ra;
+
+/* Reads an RA file; data in page-locked host memory when pinned != 0
+ * (the reference builds with -DCUDA_HOST_MALLOC, src/ra.cu:39-44).
+ * Checks the magic number and that the file holds `size` data bytes. */
+int snapmrf_ra_read(snapmrf_ra *a, const char *path, int pinned);
+int snapmrf_ra_write(const snapmrf_ra *a, const char *path);
+void snapmrf_ra_free(snapmrf_ra *a);
+
+/* ------------------------------------------------------------------------
+ * Dictionary generation (replaces MRF_dict, src/functions.cu:1224-1315, and
+ * the echo-type engines epg_sr/epg_se/epg_tse/epg_fisp/epg_ssfp/roa_ssfp,
+ * src/functions.cu:687-1222).
+ * ---------------------------------------------------------------------- */
+
+/* Generate every B1 block for the non-SSFP echo types, flip angle scaled by
+ * the block's B1 (the reference's epg_fisp/sr/se/tse/roa fill block 0 only,
+ * unscaled, src/functions.cu:1293-1309). */
+#define SNAPMRF_DICT_ALL_B1_BLOCKS 0x1u
+/* Normalise every generated atom to unit l2 norm (the reference normalises
+ * only epg_ssfp and roa_ssfp, src/functions.cu:1268, 1297). */
+#define SNAPMRF_DICT_NORMALIZE 0x2u
+/* Use the reference's operation order (complex state, separate relaxation
+ * and RF steps) even where the real-valued fast recursion applies. */
+#define SNAPMRF_DICT_REFERENCE_ORDER 0x4u
+
+typedef struct snapmrf_dict_opts {
+    unsigned flags;  /* SNAPMRF_DICT_* */
+    int n_iso;       /* ROA isochromats per atom, dephased across 2*pi per TR (1 = reference) */
+    float *d_norms;  /* optional out [NATOMS]: l2 norm of each generated atom before normalisation */
+} snapmrf_dict_opts;
+
+/* d_atoms: out, device [NATOMS][nreps] complex (blocks the echo type does
+ *          not generate are left untouched, as in the reference)
+ * d_params: device [NATOMS][nparams]; h_mrf: host [4][NREPS];
+ * nreps <= NREPS time points; natoms atoms per B1 block (NATOMS % natoms == 0);
+ * nstates EPG states w; echo_type in {epg_ssfp, roa_ssfp, epg_sr, epg_se,
+ * epg_tse1, epg_tse2, epg_fisp}; opts may be NULL (reference behaviour). */
+int snapmrf_mrf_dict(float *d_atoms, const float *d_params, const float *h_mrf,
+                     size_t nreps, size_t NREPS, size_t NATOMS, size_t natoms,
+                     int nparams, int nstates, const char *echo_type,
+                     const snapmrf_dict_opts *opts, void *stream);
+
+/* In-place unit-l2 normalisation of NATOMS atoms of nreps samples
+ * (replaces the normalize kernel, src/functions.cu:670-685). */
+int snapmrf_normalize(float *d_atoms, size_t nreps, size_t NATOMS, float *d_norms,
+                      void *stream);
+
+/* ------------------------------------------------------------------------
+ * Matching (replaces MRF_match / MRF_minimatch / generate_maps /
+ * merge_maps / compute_nsplits, src/functions.cu:1317-1584).
+ * ---------------------------------------------------------------------- */
+#define SNAPMRF_PREC_FP32 0  /* FP32 scores (the reference's cublasCgemm form) */
+
+/* Skip the device check that every B1 block holds one B1 value (true for
+ * any params table built by trans_params); without the flag the call
+ * synchronises `stream` once to read the check's result. */
+#define SNAPMRF_MATCH_ASSUME_UNIFORM_B1 0x1u
+
+typedef struct snapmrf_match_opts {
+    int precision;          /* SNAPMRF_PREC_* */
+    unsigned flags;         /* SNAPMRF_MATCH_* */
+    size_t img_stride;      /* complex samples between voxels (0 = nreps) */
+    size_t atom_stride;     /* complex samples between atoms (0 = nreps) */
+    const float *b1map;     /* optional [nvoxels] B1 map: match within the nearest B1 block */
+    int b1map_on_host;      /* b1map is host memory */
+    int64_t *d_index;       /* optional out [nvoxels]: chosen global atom index */
+} snapmrf_match_opts;
+
+/* d_maps: out, device [nvoxels][nmaps] (nmaps == 5, nparams == 4)
+ * img: [nvoxels][img_stride] complex, host memory when img_on_host != 0
+ * (page-locked host memory makes the upload asynchronous);
+ * nreps time points are matched.  Per B1 block the first atom with the
+ * largest |<atom, voxel>| wins; blocks are merged by nearest B1 when a B1
+ * map is given (ties to the lower block, differences >= 10 to block 0),
+ * otherwise by the largest PD (ties to the lower block). */
+int snapmrf_mrf_match(float *d_maps, const float *img, int img_on_host,
+                      const float *d_atoms, const float *d_params, size_t nreps,
+                      size_t NATOMS, size_t natoms, size_t nvoxels, int nparams, int nmaps,
+                      const snapmrf_match_opts *opts, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SNAPMRF_H */

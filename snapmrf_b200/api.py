@@ -1,0 +1,296 @@
+"""Python mirror of the reference's host interface (src/functions.h,
+src/ra.h) over the C ABI of libsnapmrf.so (include/snapmrf.h).
+
+Function names and argument meaning follow the reference: MRF_dict,
+MRF_match, csv_dim, csv_read, parse_length, parse_params, logspace,
+compute_natoms, trans_params, ra_read, ra_write.  Device buffers are passed
+as torch CUDA tensors (or raw device addresses); torch is used only for
+device memory and streams.  Where the reference prints and exits, these
+raise SnapMRFError with the library's message.  There is no CPU fallback:
+every compute entry point runs the CUDA kernels of libsnapmrf.so and fails
+loudly if the library is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+_PKG = Path(__file__).resolve().parent
+LIB_PATH = _PKG / "libsnapmrf.so"
+
+NPARAMS = 4  # src/mrf.cu:58
+NMAPS = 5    # src/mrf.cu:59
+
+# dictionary flags (include/snapmrf.h)
+DICT_ALL_B1_BLOCKS = 0x1
+DICT_NORMALIZE = 0x2
+DICT_REFERENCE_ORDER = 0x4
+# matching
+PREC_FP32 = 0
+MATCH_ASSUME_UNIFORM_B1 = 0x1
+
+ECHO_TYPES = ("epg_ssfp", "roa_ssfp", "epg_sr", "epg_se", "epg_tse1", "epg_tse2", "epg_fisp")
+
+RA_MAGIC = 0x7961727261776172
+RA_TYPES = {(1, 4): np.int32, (1, 8): np.int64, (2, 4): np.uint32, (2, 8): np.uint64,
+            (3, 4): np.float32, (3, 8): np.float64, (4, 8): np.complex64, (4, 16): np.complex128}
+
+
+class SnapMRFError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"snapmrf status {status}: {msg}")
+        self.status = status
+
+
+class DictOpts(C.Structure):
+    _fields_ = [("flags", C.c_uint), ("n_iso", C.c_int), ("d_norms", C.c_void_p)]
+
+
+class MatchOpts(C.Structure):
+    _fields_ = [("precision", C.c_int), ("flags", C.c_uint), ("img_stride", C.c_size_t),
+                ("atom_stride", C.c_size_t), ("b1map", C.c_void_p), ("b1map_on_host", C.c_int),
+                ("d_index", C.c_void_p)]
+
+
+class RA(C.Structure):
+    _fields_ = [("flags", C.c_uint64), ("eltype", C.c_uint64), ("elbyte", C.c_uint64),
+                ("size", C.c_uint64), ("ndims", C.c_uint64), ("dims", C.POINTER(C.c_uint64)),
+                ("data", C.c_void_p)]
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Loads libsnapmrf.so (built in-tree by __graft_entry__.build())."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise SnapMRFError(-1, f"{LIB_PATH} is not built; run __graft_entry__.build() first")
+        L = C.CDLL(str(LIB_PATH))
+        sz, vp, fp = C.c_size_t, C.c_void_p, C.POINTER(C.c_float)
+        L.snapmrf_last_error.restype = C.c_char_p
+        L.snapmrf_version.restype = C.c_char_p
+        L.snapmrf_csv_dim.restype = sz
+        L.snapmrf_csv_dim.argtypes = [C.c_char_p]
+        L.snapmrf_csv_read.argtypes = [vp, sz, C.c_char_p]
+        L.snapmrf_parse_range.argtypes = [C.c_char_p, fp, fp, fp, C.POINTER(sz)]
+        L.snapmrf_parse_length.restype = sz
+        L.snapmrf_parse_length.argtypes = [C.c_char_p]
+        L.snapmrf_parse_params.argtypes = [vp, C.c_char_p, sz]
+        L.snapmrf_linspace.argtypes = [vp, C.c_float, C.c_float, sz]
+        L.snapmrf_logspace.argtypes = [vp, C.c_float, C.c_float, sz]
+        L.snapmrf_compute_natoms.restype = sz
+        L.snapmrf_compute_natoms.argtypes = [vp, vp, sz, sz, sz, sz]
+        L.snapmrf_trans_params.argtypes = [vp, vp, vp, vp, vp, sz, sz, sz, sz, sz, C.c_int]
+        L.snapmrf_ra_read.argtypes = [C.POINTER(RA), C.c_char_p, C.c_int]
+        L.snapmrf_ra_write.argtypes = [C.POINTER(RA), C.c_char_p]
+        L.snapmrf_ra_free.argtypes = [C.POINTER(RA)]
+        L.snapmrf_ra_free.restype = None
+        L.snapmrf_mrf_dict.argtypes = [vp, vp, vp, sz, sz, sz, sz, C.c_int, C.c_int, C.c_char_p,
+                                       C.POINTER(DictOpts), vp]
+        L.snapmrf_normalize.argtypes = [vp, sz, sz, vp, vp]
+        L.snapmrf_mrf_match.argtypes = [vp, vp, C.c_int, vp, vp, sz, sz, sz, sz, C.c_int, C.c_int,
+                                        C.POINTER(MatchOpts), vp]
+        _lib = L
+    return _lib
+
+
+def _check(rc: int) -> None:
+    if rc != 0:
+        raise SnapMRFError(rc, lib().snapmrf_last_error().decode(errors="replace"))
+
+
+def _ptr(x) -> int | None:
+    """Device/host address of a torch tensor, numpy array or raw int."""
+    if x is None:
+        return None
+    if isinstance(x, int):
+        return x
+    if isinstance(x, np.ndarray):
+        return x.ctypes.data
+    return x.data_ptr()
+
+
+def _stream_ptr(stream) -> int | None:
+    if stream is None:
+        try:
+            import torch
+            if torch.cuda.is_available():
+                return torch.cuda.current_stream().cuda_stream
+        except Exception:
+            pass
+        return None
+    if isinstance(stream, int):
+        return stream
+    return stream.cuda_stream
+
+
+# ---------------------------------------------------------------------------
+# host: CSV, grids, params (src/functions.cu:100-414)
+# ---------------------------------------------------------------------------
+
+def csv_dim(path: str) -> int:
+    n = lib().snapmrf_csv_dim(str(path).encode())
+    if n == C.c_size_t(-1).value:
+        raise SnapMRFError(5, lib().snapmrf_last_error().decode())
+    return n
+
+
+def csv_read(path: str, nreps: int) -> np.ndarray:
+    """Schedule h_mrf[4][nreps] (flip, phase, TR, TE columns)."""
+    out = np.zeros((4, nreps), np.float32)
+    _check(lib().snapmrf_csv_read(out.ctypes.data, nreps, str(path).encode()))
+    return out
+
+
+def parse_range(s: str):
+    mn, st, mx = C.c_float(), C.c_float(), C.c_float()
+    n = C.c_size_t()
+    _check(lib().snapmrf_parse_range(s.encode(), C.byref(mn), C.byref(st), C.byref(mx), C.byref(n)))
+    return mn.value, st.value, mx.value, n.value
+
+
+def parse_length(s: str) -> int:
+    n = lib().snapmrf_parse_length(s.encode())
+    if n == 0:
+        raise SnapMRFError(6, lib().snapmrf_last_error().decode())
+    return n
+
+
+def parse_params(s: str) -> np.ndarray:
+    n = parse_length(s)
+    out = np.zeros(n, np.float32)
+    _check(lib().snapmrf_parse_params(out.ctypes.data, s.encode(), n))
+    return out
+
+
+def linspace(mn: float, step: float, n: int) -> np.ndarray:
+    out = np.zeros(n, np.float32)
+    lib().snapmrf_linspace(out.ctypes.data, mn, step, n)
+    return out
+
+
+def logspace(mn: float, mx: float, n: int) -> np.ndarray:
+    out = np.zeros(n, np.float32)
+    lib().snapmrf_logspace(out.ctypes.data, mn, mx, n)
+    return out
+
+
+def compute_natoms(t1, t2, l_b0: int, l_b1: int) -> int:
+    t1 = np.ascontiguousarray(t1, np.float32)
+    t2 = np.ascontiguousarray(t2, np.float32)
+    return lib().snapmrf_compute_natoms(t1.ctypes.data, t2.ctypes.data, len(t1), len(t2), l_b0, l_b1)
+
+
+def trans_params(t1, t2, b0, b1) -> np.ndarray:
+    """params[NATOMS][4] = {T1, T2, B0, B1}, B1 > B0 > T2 > T1 order, T1 > T2."""
+    t1, t2, b0, b1 = (np.ascontiguousarray(v, np.float32) for v in (t1, t2, b0, b1))
+    n = compute_natoms(t1, t2, len(b0), len(b1))
+    out = np.zeros((n, NPARAMS), np.float32)
+    if n:
+        _check(lib().snapmrf_trans_params(out.ctypes.data, t1.ctypes.data, t2.ctypes.data,
+                                          b0.ctypes.data, b1.ctypes.data, len(t1), len(t2),
+                                          len(b0), len(b1), n, NPARAMS))
+    return out
+
+
+def grid_params(T1: str, T2: str, B0: str = "0", B1: str = "1"):
+    """The mrf CLI's grid pipeline (src/mrf.cu:205-253): returns
+    (params [NATOMS][4], NATOMS, natoms)."""
+    t1, t2, b0, b1 = (parse_params(s) for s in (T1, T2, B0, B1))
+    p = trans_params(t1, t2, b0, b1)
+    return p, p.shape[0], p.shape[0] // len(b1)
+
+
+# ---------------------------------------------------------------------------
+# RA files (src/ra.cu)
+# ---------------------------------------------------------------------------
+
+def ra_read(path: str) -> np.ndarray:
+    """Reads an RA file into an array of shape dims[::-1] (dims[0] fastest)."""
+    a = RA()
+    _check(lib().snapmrf_ra_read(C.byref(a), str(path).encode(), 0))
+    try:
+        dims = [a.dims[i] for i in range(a.ndims)]
+        dt = RA_TYPES.get((a.eltype, a.elbyte))
+        if dt is None:
+            raise SnapMRFError(7, f"{path}: RA eltype {a.eltype}/{a.elbyte} not supported")
+        buf = (C.c_uint8 * a.size).from_address(a.data) if a.size else b""
+        arr = np.frombuffer(bytes(buf), dtype=dt).reshape(tuple(reversed(dims)))
+        return arr.copy()
+    finally:
+        lib().snapmrf_ra_free(C.byref(a))
+
+
+def ra_write(path: str, arr: np.ndarray) -> None:
+    """Writes arr (shape dims[::-1]) as RA: complex64 -> complex, float32 -> float."""
+    arr = np.ascontiguousarray(arr)
+    code = {np.dtype(np.complex64): (4, 8), np.dtype(np.complex128): (4, 16),
+            np.dtype(np.float32): (3, 4), np.dtype(np.float64): (3, 8),
+            np.dtype(np.int32): (1, 4), np.dtype(np.int64): (1, 8)}.get(arr.dtype)
+    if code is None:
+        raise SnapMRFError(7, f"dtype {arr.dtype} not supported")
+    dims = (C.c_uint64 * arr.ndim)(*reversed(arr.shape))
+    a = RA(0, code[0], code[1], arr.nbytes, arr.ndim, C.cast(dims, C.POINTER(C.c_uint64)),
+           arr.ctypes.data)
+    _check(lib().snapmrf_ra_write(C.byref(a), str(path).encode()))
+
+
+# ---------------------------------------------------------------------------
+# device entry points
+# ---------------------------------------------------------------------------
+
+def MRF_dict(d_atoms, d_params, h_mrf, nreps: int, NREPS: int, NATOMS: int, natoms: int,
+             nparams: int = NPARAMS, nstates: int = 101, echo_type: str = "epg_ssfp", *,
+             flags: int = 0, n_iso: int = 1, d_norms=None, stream=None) -> None:
+    """Dictionary generation (src/functions.cu:1224-1315).
+
+    d_atoms: device complex64 [NATOMS][nreps] (out); d_params: device float32
+    [NATOMS][nparams]; h_mrf: host float32 [4][NREPS] schedule."""
+    h_mrf = np.ascontiguousarray(h_mrf, np.float32)
+    if h_mrf.size < 4 * NREPS:
+        raise SnapMRFError(1, "h_mrf must hold 4*NREPS values")
+    opts = DictOpts(flags, n_iso, _ptr(d_norms))
+    _check(lib().snapmrf_mrf_dict(_ptr(d_atoms), _ptr(d_params), h_mrf.ctypes.data, nreps, NREPS,
+                                  NATOMS, natoms, nparams, nstates, echo_type.encode(),
+                                  C.byref(opts), _stream_ptr(stream)))
+
+
+def normalize(d_atoms, nreps: int, NATOMS: int, d_norms=None, stream=None) -> None:
+    """Unit-l2 normalisation of atoms in place (src/functions.cu:670-685)."""
+    _check(lib().snapmrf_normalize(_ptr(d_atoms), nreps, NATOMS, _ptr(d_norms), _stream_ptr(stream)))
+
+
+def MRF_match(d_maps, img, d_atoms, d_params, NREPS: int, nreps: int, NATOMS: int, natoms: int,
+              nvoxels: int, nparams: int = NPARAMS, nmaps: int = NMAPS, in_b1map=None, *,
+              precision: int = PREC_FP32, flags: int = 0, img_stride: int = 0,
+              d_index=None, stream=None) -> None:
+    """Template matching (src/functions.cu:1493-1584).
+
+    img: host numpy complex64 [nvoxels][stride] or a device tensor; NREPS is
+    the dictionary's time points (atom stride), nreps the matched time points.
+    in_b1map: None, a path to an RA B1 map, a host array or a device tensor."""
+    on_host = isinstance(img, np.ndarray)
+    if on_host:
+        img = np.ascontiguousarray(img, np.complex64)
+        if not img_stride:
+            img_stride = img.shape[-1] if img.ndim > 1 else nreps
+    b1 = None
+    b1_host = 0
+    if in_b1map is not None:
+        if isinstance(in_b1map, (str, os.PathLike)):
+            in_b1map = ra_read(in_b1map).astype(np.float32).reshape(-1)
+        if isinstance(in_b1map, np.ndarray):
+            in_b1map = np.ascontiguousarray(in_b1map, np.float32).reshape(-1)
+            if in_b1map.size < nvoxels:
+                raise SnapMRFError(1, "B1 map has fewer values than voxels")
+            b1_host = 1
+        b1 = in_b1map
+    opts = MatchOpts(precision, flags, img_stride, NREPS, _ptr(b1), b1_host, _ptr(d_index))
+    _check(lib().snapmrf_mrf_match(_ptr(d_maps), _ptr(img), 1 if on_host else 0, _ptr(d_atoms),
+                                   _ptr(d_params), nreps, NATOMS, natoms, nvoxels, nparams, nmaps,
+                                   C.byref(opts), _stream_ptr(stream)))

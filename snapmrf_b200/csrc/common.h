@@ -1,0 +1,71 @@
+// Internal helpers shared by the snapMRF B200 library sources.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cstdio>
+#include <cstdarg>
+#include <string>
+
+#include "snapmrf.h"
+
+namespace snapmrf {
+
+// Records `msg` as this thread's last error and returns `code`.
+int set_error(int code, const char *fmt, ...);
+void clear_error();
+
+}  // namespace snapmrf
+
+#define SNAPMRF_FAIL(code, ...) return ::snapmrf::set_error((code), __VA_ARGS__)
+
+#ifdef __CUDACC__
+#include <cuda_runtime.h>
+
+// Propagates a CUDA runtime failure as SNAPMRF_ERR_CUDA with its location.
+#define SNAPMRF_CUDA(expr)                                                              \
+    do {                                                                                \
+        cudaError_t _e = (expr);                                                        \
+        if (_e != cudaSuccess)                                                          \
+            return ::snapmrf::set_error(_e == cudaErrorMemoryAllocation ? SNAPMRF_ERR_ALLOC \
+                                                                        : SNAPMRF_ERR_CUDA, \
+                                        "%s failed: %s (%s:%d)", #expr,                 \
+                                        cudaGetErrorString(_e), __FILE__, __LINE__);    \
+    } while (0)
+
+#define SNAPMRF_LAUNCH_CHECK() SNAPMRF_CUDA(cudaGetLastError())
+
+namespace snapmrf {
+
+// Stream-ordered scratch allocation that is released on scope exit.
+struct DeviceScratch {
+    void *ptr = nullptr;
+    cudaStream_t stream = nullptr;
+    DeviceScratch() = default;
+    DeviceScratch(const DeviceScratch &) = delete;
+    DeviceScratch &operator=(const DeviceScratch &) = delete;
+    cudaError_t alloc(size_t bytes, cudaStream_t s) {
+        stream = s;
+        return cudaMallocAsync(&ptr, bytes ? bytes : 16, s);
+    }
+    ~DeviceScratch() {
+        if (ptr) cudaFreeAsync(ptr, stream);
+    }
+    template <class T> T *as() const { return static_cast<T *>(ptr); }
+};
+
+// Complex helpers with the reference's float2 operator arithmetic
+// (src/float2math.h:23-45): nvcc contracts them the same way.
+__host__ __device__ __forceinline__ float2 c_mul(float2 a, float2 b) {
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__host__ __device__ __forceinline__ float2 c_scale(float2 a, float s) {
+    return make_float2(a.x * s, a.y * s);
+}
+__host__ __device__ __forceinline__ float2 c_conj(float2 a) { return make_float2(a.x, -a.y); }
+__host__ __device__ __forceinline__ float2 c_add(float2 a, float2 b) {
+    return make_float2(a.x + b.x, a.y + b.y);
+}
+
+}  // namespace snapmrf
+#endif  // __CUDACC__

@@ -1,0 +1,242 @@
+// Dictionary generation on sm_100a: extended-phase-graph recursion for the
+// SSFP / SR / SE / TSE / FISP echo types and single- or multi-isochromat ROA
+// Bloch simulation.  Replaces MRF_dict and the per-operator kernels of the
+// reference (src/functions.cu:416-1315).
+//
+// Design: the reference launches ~14 kernels and a cuBLAS handle per time
+// step over a global [atom][state][3] state array.  Here one launch runs the
+// whole recursion: an atom's EPG state lives in the registers of a group of
+// L lanes (S states per lane), the F-state shift is a shuffle between
+// neighbouring lanes, per-step constants (RF transition matrix, relaxation
+// and precession factors) are staged in shared memory per chunk of time
+// steps, and the readout is staged in shared memory and written coalesced.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "common.h"
+#include "epg_kernels.cuh"
+
+namespace snapmrf {
+
+// ---------------------------------------------------------------------------
+// Schedule preparation
+// ---------------------------------------------------------------------------
+
+// Per-block flip angles.  epg_ssfp scales the flip-angle row in place by the
+// block's B1 and back by 1/B1 after the block (src/functions.cu:969-973,
+// 1011-1013); that float round trip is reproduced so block j sees exactly the
+// reference's angles.  Other echo types use the converted angle, times b1
+// when every block is generated (the B1 extension).
+__global__ void prepare_alpha_kernel(float *alpha, const float *fa, const float *params,
+                                     int nparams, long long nreps, long long natoms,
+                                     long long nblocks, int mode) {
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= nreps) return;
+    float v = fa[t];
+    for (long long j = 0; j < nblocks; j++) {
+        float b1 = params[j * natoms * nparams + 3];
+        if (mode == 0) {            // SSFP drift
+            v *= b1;
+            alpha[j * nreps + t] = v;
+            float inv = 1.f / b1;
+            v *= inv;
+        } else if (mode == 1) {     // alpha * b1
+            alpha[j * nreps + t] = fa[t] * b1;
+        } else {                    // unscaled
+            alpha[j * nreps + t] = fa[t];
+        }
+    }
+}
+
+static int parse_echo(const char *s) {
+    if (!s) return -1;
+    if (!strcmp(s, "epg_ssfp")) return ECHO_SSFP;
+    if (!strcmp(s, "roa_ssfp")) return ECHO_ROA;
+    if (!strcmp(s, "epg_sr")) return ECHO_SR;
+    if (!strcmp(s, "epg_se")) return ECHO_SE;
+    if (!strcmp(s, "epg_tse1") || !strcmp(s, "epg_tse2")) return ECHO_TSE;
+    if (!strcmp(s, "epg_fisp")) return ECHO_FISP;
+    return -1;
+}
+
+// Lanes per atom (power of two) and states per lane for w states:
+// least padding first, then more states per lane.
+static void choose_layout(int w, int *L, int *S) {
+    int bestL = 32, bestS = 8, bestPad = 1 << 30;
+    for (int s = kMaxStatesPerLane; s >= 1; s--)
+        for (int l = 1; l <= 32; l *= 2)
+            if (l * s >= w) {
+                int pad = l * s - w;
+                if (pad < bestPad) { bestPad = pad; bestL = l; bestS = s; }
+                break;
+            }
+    *L = bestL;
+    *S = bestS;
+}
+
+template <int ECHO, int S>
+static cudaError_t launch_epg_ref(const EpgArgs &a, dim3 grid, cudaStream_t st) {
+    size_t smem = epg_ref_smem_bytes(ECHO, a.L);
+    auto k = epg_ref_kernel<ECHO, S>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    k<<<grid, kEpgThreads, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+template <int ECHO>
+static cudaError_t dispatch_states(const EpgArgs &a, int S, dim3 grid, cudaStream_t st) {
+    switch (S) {
+    case 1: return launch_epg_ref<ECHO, 1>(a, grid, st);
+    case 2: return launch_epg_ref<ECHO, 2>(a, grid, st);
+    case 3: return launch_epg_ref<ECHO, 3>(a, grid, st);
+    case 4: return launch_epg_ref<ECHO, 4>(a, grid, st);
+    case 5: return launch_epg_ref<ECHO, 5>(a, grid, st);
+    case 6: return launch_epg_ref<ECHO, 6>(a, grid, st);
+    case 7: return launch_epg_ref<ECHO, 7>(a, grid, st);
+    default: return launch_epg_ref<ECHO, 8>(a, grid, st);
+    }
+}
+
+static cudaError_t launch_epg(int echo, const EpgArgs &a, int S, dim3 grid, cudaStream_t st) {
+    switch (echo) {
+    case ECHO_SSFP: return dispatch_states<ECHO_SSFP>(a, S, grid, st);
+    case ECHO_SR: return dispatch_states<ECHO_SR>(a, S, grid, st);
+    case ECHO_SE: return dispatch_states<ECHO_SE>(a, S, grid, st);
+    case ECHO_TSE: return dispatch_states<ECHO_TSE>(a, S, grid, st);
+    default: return dispatch_states<ECHO_FISP>(a, S, grid, st);
+    }
+}
+
+}  // namespace snapmrf
+
+using namespace snapmrf;
+
+extern "C" int snapmrf_mrf_dict(float *d_atoms, const float *d_params, const float *h_mrf,
+                                size_t nreps, size_t NREPS, size_t NATOMS, size_t natoms,
+                                int nparams, int nstates, const char *echo_type,
+                                const snapmrf_dict_opts *opts, void *stream) {
+    cudaStream_t st = (cudaStream_t)stream;
+    int echo = parse_echo(echo_type);
+    if (echo < 0)
+        SNAPMRF_FAIL(SNAPMRF_ERR_ECHO_TYPE, "Please put in correct echo types (got '%s')",
+                     echo_type ? echo_type : "(null)");
+    if (!d_atoms || !d_params || !h_mrf) SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "MRF_dict: null pointer");
+    if (nparams < 4) SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "MRF_dict: nparams must be >= 4");
+    if (nreps == 0 || nreps > NREPS)
+        SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "MRF_dict: need 0 < nreps <= NREPS (%zu, %zu)", nreps, NREPS);
+    if (natoms == 0 || NATOMS % natoms != 0)
+        SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "MRF_dict: NATOMS (%zu) must be a multiple of natoms (%zu)",
+                     NATOMS, natoms);
+    if (nstates < 1 || nstates > 32 * kMaxStatesPerLane)
+        SNAPMRF_FAIL(SNAPMRF_ERR_UNSUPPORTED, "MRF_dict: nstates must be in [1, %d]", 32 * kMaxStatesPerLane);
+    unsigned flags = opts ? opts->flags : 0u;
+    int n_iso = opts ? opts->n_iso : 1;
+    if (n_iso < 1) n_iso = 1;
+    if (n_iso > 1 && echo != ECHO_ROA)
+        SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "MRF_dict: n_iso > 1 applies to roa_ssfp only");
+    float *d_norms = opts ? opts->d_norms : nullptr;
+    if (natoms > (size_t)(65535ull * 1024ull * 1024ull))
+        SNAPMRF_FAIL(SNAPMRF_ERR_UNSUPPORTED, "MRF_dict: too many atoms per block");
+
+    const size_t nblocks = NATOMS / natoms;
+    if (nblocks > 65535) SNAPMRF_FAIL(SNAPMRF_ERR_UNSUPPORTED, "MRF_dict: more than 65535 B1 blocks");
+    const bool all_blocks = (echo == ECHO_SSFP) || (flags & SNAPMRF_DICT_ALL_B1_BLOCKS);
+    const size_t gen_blocks = all_blocks ? nblocks : 1;
+    const bool normalize = echo == ECHO_SSFP || echo == ECHO_ROA || (flags & SNAPMRF_DICT_NORMALIZE);
+
+    // Converted schedule (MRF_dict, src/functions.cu:1229-1291): SSFP and ROA
+    // take the CSV's flip fraction of 60 deg, phase in degrees and TR/TE
+    // extensions of 16 / 3.5 ms; the other echo types use the values raw.
+    std::vector<float> sched(4 * nreps);
+    for (int r = 0; r < 4; r++)
+        for (size_t t = 0; t < nreps; t++) sched[r * nreps + t] = h_mrf[r * NREPS + t];
+    if (echo == ECHO_SSFP || echo == ECHO_ROA) {
+        const float nominal_flip = 60.f, TR_base = 16.f, TE_base = 3.5f;
+        const float fa_scale = (float)(nominal_flip * M_PI / 180.f);
+        const float ph_scale = (float)(M_PI / 180.f);
+        for (size_t t = 0; t < nreps; t++) {
+            sched[t] *= fa_scale;
+            sched[nreps + t] *= ph_scale;
+            sched[2 * nreps + t] += TR_base;
+            sched[3 * nreps + t] += TE_base;
+        }
+    }
+
+    DeviceScratch scratch;
+    SNAPMRF_CUDA(scratch.alloc((4 * nreps + gen_blocks * nreps) * sizeof(float), st));
+    float *d_sched = scratch.as<float>();
+    float *d_alpha = d_sched + 4 * nreps;
+    SNAPMRF_CUDA(cudaMemcpyAsync(d_sched, sched.data(), 4 * nreps * sizeof(float),
+                                 cudaMemcpyHostToDevice, st));
+    int mode = (echo == ECHO_SSFP) ? 0 : (all_blocks ? 1 : 2);
+    prepare_alpha_kernel<<<(unsigned)((nreps + 255) / 256), 256, 0, st>>>(
+        d_alpha, d_sched, d_params, nparams, (long long)nreps, (long long)natoms,
+        (long long)gen_blocks, mode);
+    SNAPMRF_LAUNCH_CHECK();
+
+    EpgArgs a;
+    a.atoms = reinterpret_cast<float2 *>(d_atoms);
+    a.norms = d_norms;
+    a.alpha = d_alpha;
+    a.sched = d_sched;
+    a.params = d_params;
+    a.nparams = nparams;
+    a.nreps = (long long)nreps;
+    a.natoms = (long long)natoms;
+    a.nstates = nstates;
+    a.own_params = (echo == ECHO_SSFP) ? 0 : 1;
+    a.normalize = normalize ? 1 : 0;
+    a.n_iso = n_iso;
+
+    if (echo == ECHO_ROA) {
+        if (n_iso > 32 * 8) SNAPMRF_FAIL(SNAPMRF_ERR_UNSUPPORTED, "MRF_dict: n_iso must be <= 256");
+        a.L = 1;
+        SNAPMRF_CUDA(launch_roa(a, (long long)natoms, (unsigned)gen_blocks, st));
+        return SNAPMRF_OK;
+    }
+    int L, S;
+    choose_layout(nstates, &L, &S);
+    a.L = L;
+    const int apc = kEpgThreads / L;
+    dim3 grid((unsigned)((natoms + apc - 1) / apc), (unsigned)gen_blocks);
+    if (grid.x > 0x7fffffffu) SNAPMRF_FAIL(SNAPMRF_ERR_UNSUPPORTED, "MRF_dict: grid too large");
+    SNAPMRF_CUDA(launch_epg(echo, a, S, grid, st));
+    return SNAPMRF_OK;
+}
+
+namespace snapmrf {
+
+// normalize (src/functions.cu:670-685): a / ||a||_2 when ||a|| > 0, one warp
+// per atom (the sum is a lane-strided tree instead of the reference's serial
+// loop, so it differs from it by rounding only).
+__global__ void normalize_kernel(float2 *atoms, float *norms, long long nreps, long long natoms) {
+    long long a = (blockIdx.x * (long long)blockDim.x + threadIdx.x) / 32;
+    int lane = threadIdx.x % 32;
+    if (a >= natoms) return;
+    float2 *p = atoms + a * nreps;
+    float s = 0.f;
+    for (long long t = lane; t < nreps; t += 32) s += p[t].x * p[t].x + p[t].y * p[t].y;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (norms && lane == 0) norms[a] = sqrtf(s);
+    float inv = s;
+    if (inv > 0.f) inv = 1.f / sqrtf(inv);
+    for (long long t = lane; t < nreps; t += 32) p[t] = c_scale(p[t], inv);
+}
+
+}  // namespace snapmrf
+
+extern "C" int snapmrf_normalize(float *d_atoms, size_t nreps, size_t NATOMS, float *d_norms,
+                                 void *stream) {
+    if (!d_atoms) SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "normalize: null pointer");
+    if (nreps == 0 || NATOMS == 0) return SNAPMRF_OK;
+    long long threads = (long long)NATOMS * 32;
+    snapmrf::normalize_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, (cudaStream_t)stream>>>(
+        reinterpret_cast<float2 *>(d_atoms), d_norms, (long long)nreps, (long long)NATOMS);
+    SNAPMRF_LAUNCH_CHECK();
+    return SNAPMRF_OK;
+}

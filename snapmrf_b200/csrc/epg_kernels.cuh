@@ -1,0 +1,545 @@
+// EPG / ROA device kernels (reference operation order).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "common.h"
+
+namespace snapmrf {
+
+enum Echo { ECHO_SSFP = 0, ECHO_ROA = 1, ECHO_SR = 2, ECHO_SE = 3, ECHO_TSE = 4, ECHO_FISP = 5 };
+
+constexpr int kEpgThreads = 128;      // threads per CTA
+constexpr int kChunk = 16;            // time steps staged per shared-memory chunk
+constexpr int kMaxStatesPerLane = 8;  // register-resident EPG states per lane
+
+struct EpgArgs {
+    float2 *atoms;        // out [blocks][natoms][nreps]
+    float *norms;         // optional out [blocks][natoms]
+    const float *alpha;   // [gen_blocks][nreps] flip angle per block (rad)
+    const float *sched;   // [4][nreps] converted schedule (alpha, phi rad; TR, TE ms)
+    const float *params;  // [NATOMS][nparams]
+    int nparams;
+    long long nreps;
+    long long natoms;     // atoms per B1 block
+    int nstates;          // EPG states w
+    int L;                // lanes per atom (power of two)
+    int own_params;       // 1: each atom's own row; 0: block-0 row (epg_ssfp)
+    int normalize;        // unit-norm each atom (src/functions.cu:670-685)
+    int n_iso;            // ROA isochromats
+};
+
+// Number of per-(atom, step) factors staged: E1/E2 at TE and at TR-TE, plus
+// the B0 precession phasors at TE and TR-TE for SSFP.
+__host__ __device__ constexpr int epg_nf(int echo) { return echo == ECHO_SSFP ? 8 : 4; }
+
+inline size_t epg_ref_smem_bytes(int echo, int L) {
+    int apc = kEpgThreads / L;
+    return (size_t)kChunk * 9 * sizeof(float2) + (size_t)apc * kChunk * epg_nf(echo) * sizeof(float) +
+           (size_t)apc * kChunk * sizeof(float2) + (size_t)apc * 3 * sizeof(float);
+}
+
+// RF transition matrix of fill_transition_matrix (src/functions.cu:483-508),
+// same float2 expressions; T[3r + l] multiplies state channel l into row r.
+__device__ __forceinline__ void rf_matrix(float alpha, float phi, float2 *T) {
+    float sa, ca;
+    __sincosf(alpha, &sa, &ca);
+    float sa2 = (1 - ca) / 2;
+    float ca2 = (1 + ca) / 2;
+    float sp, cp;
+    __sincosf(phi, &sp, &cp);
+    float2 z = make_float2(cp, sp);
+    float2 zinv = c_conj(z);
+    const float2 im = make_float2(0.f, 1.f);
+    const float2 mim = make_float2(-im.x, -im.y);
+    T[0] = make_float2(ca2, 0.f);
+    T[3] = c_mul(c_scale(zinv, sa2), zinv);
+    T[6] = c_mul(c_scale(c_scale(mim, 0.5f), sa), zinv);
+    T[1] = c_scale(c_mul(z, z), sa2);
+    T[4] = make_float2(ca2, 0.f);
+    T[7] = c_scale(c_mul(c_scale(im, 0.5f), z), sa);
+    T[2] = c_scale(c_mul(mim, z), sa);
+    T[5] = c_mul(c_scale(im, sa), zinv);
+    T[8] = make_float2(ca, 0.f);
+}
+
+// One output row of the 3x3 complex RF product, accumulated with FMAs over
+// the three state channels (the in-place cublasCgemm of
+// src/functions.cu:510-528).
+__device__ __forceinline__ float2 rf_row(float2 a0, float2 a1, float2 a2, float2 o0, float2 o1,
+                                         float2 o2) {
+    float rx = a0.x * o0.x;
+    rx = fmaf(-a0.y, o0.y, rx);
+    rx = fmaf(a1.x, o1.x, rx);
+    rx = fmaf(-a1.y, o1.y, rx);
+    rx = fmaf(a2.x, o2.x, rx);
+    rx = fmaf(-a2.y, o2.y, rx);
+    float ry = a0.x * o0.y;
+    ry = fmaf(a0.y, o0.x, ry);
+    ry = fmaf(a1.x, o1.y, ry);
+    ry = fmaf(a1.y, o1.x, ry);
+    ry = fmaf(a2.x, o2.y, ry);
+    ry = fmaf(a2.y, o2.x, ry);
+    return make_float2(rx, ry);
+}
+
+// Register-resident EPG state of one lane: states k = gl*S + j.
+template <int S>
+struct LaneState {
+    float2 fp[S], fm[S], zz[S];
+};
+
+template <int S>
+__device__ __forceinline__ void st_rf(LaneState<S> &s, const float2 *T) {
+    float2 t0 = T[0], t1 = T[1], t2 = T[2], t3 = T[3], t4 = T[4], t5 = T[5], t6 = T[6], t7 = T[7],
+           t8 = T[8];
+#pragma unroll
+    for (int j = 0; j < S; j++) {
+        float2 o0 = s.fp[j], o1 = s.fm[j], o2 = s.zz[j];
+        s.fp[j] = rf_row(t0, t1, t2, o0, o1, o2);
+        s.fm[j] = rf_row(t3, t4, t5, o0, o1, o2);
+        s.zz[j] = rf_row(t6, t7, t8, o0, o1, o2);
+    }
+}
+
+// decay_signal_stage1/2 (src/functions.cu:544-569): F+- *= E2, Z *= E1, then
+// Z0 += 1 - E1 as a separate rounding.
+template <int S>
+__device__ __forceinline__ void st_relax(LaneState<S> &s, float E1, float E2, bool lane0) {
+#pragma unroll
+    for (int j = 0; j < S; j++) {
+        s.fp[j] = c_scale(s.fp[j], E2);
+        s.fm[j] = c_scale(s.fm[j], E2);
+        s.zz[j] = c_scale(s.zz[j], E1);
+    }
+    if (lane0) s.zz[0].x = __fadd_rn(s.zz[0].x, 1 - E1);
+}
+
+// shift_phase (EPG, src/functions.cu:585-607): F+ *= e, F- *= conj(e).
+template <int S>
+__device__ __forceinline__ void st_b0(LaneState<S> &s, float2 e) {
+    float2 ec = c_conj(e);
+#pragma unroll
+    for (int j = 0; j < S; j++) {
+        s.fp[j] = c_mul(e, s.fp[j]);
+        s.fm[j] = c_mul(ec, s.fm[j]);
+    }
+}
+
+// dephase_gradients (src/functions.cu:619-668): F+[k] <- F+[k-1],
+// F-[k] <- F-[k+1], F+[0] = conj(F-[0]), F-[w-1] = 0.  Slots k >= w are kept
+// zero so that F-[w-1] picks up a zero.
+template <int S>
+__device__ __forceinline__ void st_shift(LaneState<S> &s, int gl, int L, int w) {
+    const unsigned full = 0xffffffffu;
+    float2 top = s.fp[S - 1];
+    float2 up;
+    up.x = __shfl_up_sync(full, top.x, 1, L);
+    up.y = __shfl_up_sync(full, top.y, 1, L);
+    float2 bot = s.fm[0];
+    float2 dn;
+    dn.x = __shfl_down_sync(full, bot.x, 1, L);
+    dn.y = __shfl_down_sync(full, bot.y, 1, L);
+#pragma unroll
+    for (int j = S - 1; j >= 1; j--) s.fp[j] = s.fp[j - 1];
+    s.fp[0] = up;
+#pragma unroll
+    for (int j = 0; j < S - 1; j++) s.fm[j] = s.fm[j + 1];
+    s.fm[S - 1] = (gl == L - 1) ? make_float2(0.f, 0.f) : dn;
+    if (gl == 0) s.fp[0] = c_conj(s.fm[0]);
+#pragma unroll
+    for (int j = 0; j < S; j++)
+        if (gl * S + j >= w) s.fp[j] = make_float2(0.f, 0.f);
+}
+
+// init_rf_pulse (EPG, src/functions.cu:456-481) into state 0.
+template <int S>
+__device__ __forceinline__ void st_init(LaneState<S> &s, bool lane0, float t1, float t2,
+                                        float alpha_deg, float phi_deg, float TI) {
+#pragma unroll
+    for (int j = 0; j < S; j++) {
+        s.fp[j] = make_float2(0.f, 0.f);
+        s.fm[j] = make_float2(0.f, 0.f);
+        s.zz[j] = make_float2(0.f, 0.f);
+    }
+    float alpha = (float)(alpha_deg * M_PI / 180.f);
+    float phi = (float)(phi_deg * M_PI / 180.f);
+    float e1 = expf(-TI / t1);
+    float e2 = expf(-TI / t2);
+    float sa, ca, sph, cph;
+    __sincosf(alpha, &sa, &ca);
+    __sincosf(phi, &sph, &cph);
+    float2 tmp2 = c_scale(make_float2(sph, cph), e2 * sa);
+    if (lane0) {
+        s.fp[0] = c_conj(tmp2);
+        s.fm[0] = tmp2;
+        s.zz[0] = make_float2(e1 * ca + 1 - e1, 0.f);
+    }
+}
+
+// B0 phase of shift_phase: cexpf(2*pi*B0*t/1000) with the argument
+// evaluated in double like the reference expression.
+__device__ __forceinline__ float2 b0_phasor(float B0, float t) {
+    float th = (float)(2 * M_PI * B0 * t / 1000.f);
+    float s, c;
+    __sincosf(th, &s, &c);
+    return make_float2(c, s);
+}
+
+// The fused EPG recursion, reference operation order.  One CTA handles
+// kEpgThreads / L atoms of one B1 block (blockIdx.y).
+template <int ECHO, int S>
+__global__ void __launch_bounds__(kEpgThreads) epg_ref_kernel(EpgArgs a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    constexpr int NF = epg_nf(ECHO);
+    const int L = a.L;
+    const int apc = kEpgThreads / L;
+    const int tid = threadIdx.x;
+    const int g = tid / L;
+    const int gl = tid % L;
+    const bool lane0 = (gl == 0);
+    const long long blk = blockIdx.y;
+    const long long nreps = a.nreps;
+    const long long atom0 = (long long)blockIdx.x * apc;
+    const long long ab = atom0 + g;
+    const bool active = ab < a.natoms;
+    const long long gatom = blk * a.natoms + ab;
+
+    float2 *sT = reinterpret_cast<float2 *>(smem_raw);
+    float *sF = reinterpret_cast<float *>(sT + kChunk * 9);
+    float2 *sR = reinterpret_cast<float2 *>(sF + apc * kChunk * NF);
+    float *sP = reinterpret_cast<float *>(sR + apc * kChunk);
+
+    for (int i = tid; i < apc; i += kEpgThreads) {
+        long long at = atom0 + i;
+        float t1 = 1.f, t2 = 1.f, b0 = 0.f;
+        if (at < a.natoms) {
+            long long row = a.own_params ? blk * a.natoms + at : at;
+            const float *p = a.params + row * a.nparams;
+            t1 = p[0];
+            t2 = p[1];
+            b0 = p[2];
+        }
+        sP[3 * i] = t1;
+        sP[3 * i + 1] = t2;
+        sP[3 * i + 2] = b0;
+    }
+    __syncthreads();
+    const float T1 = sP[3 * g], T2 = sP[3 * g + 1];
+
+    const float *alpha = a.alpha + blk * nreps;
+    const float *phi = a.sched + nreps;
+    const float *TR = a.sched + 2 * nreps;
+    const float *TE = a.sched + 3 * nreps;
+    const int w = a.nstates;
+
+    LaneState<S> s;
+    if (ECHO == ECHO_SSFP) {
+        st_init<S>(s, lane0, T1, T2, 180.f, 0.f, 40.f);
+    } else if (ECHO == ECHO_SE || ECHO == ECHO_TSE) {
+        st_init<S>(s, lane0, T1, T2, 90.f, 90.f, 0.f);
+        st_shift<S>(s, gl, L, w);
+        float te0 = TE[0];
+        st_relax<S>(s, expf(-te0 / T1), expf(-te0 / T2), lane0);
+    } else {
+        st_init<S>(s, lane0, T1, T2, 0.f, 0.f, 0.f);
+    }
+
+    float nrm = 0.f;
+    float2 *out = a.atoms + gatom * nreps;
+    for (long long t0 = 0; t0 < nreps; t0 += kChunk) {
+        const int nch = (int)min((long long)kChunk, nreps - t0);
+        __syncthreads();
+        for (int i = tid; i < nch; i += kEpgThreads) rf_matrix(alpha[t0 + i], phi[t0 + i], sT + 9 * i);
+        for (int idx = tid; idx < apc * nch; idx += kEpgThreads) {
+            int ga = idx / nch, i = idx - ga * nch;
+            float t1 = sP[3 * ga], t2 = sP[3 * ga + 1];
+            float tr = TR[t0 + i], te = TE[t0 + i];
+            float ta = te, tb = tr - te;
+            float *f = sF + (ga * kChunk + i) * NF;
+            f[0] = expf(-ta / t1);
+            f[1] = expf(-ta / t2);
+            f[2] = expf(-tb / t1);
+            f[3] = expf(-tb / t2);
+            if (ECHO == ECHO_SSFP) {
+                float b0 = sP[3 * ga + 2];
+                float2 ea = b0_phasor(b0, ta), eb = b0_phasor(b0, tb);
+                f[4] = ea.x;
+                f[5] = ea.y;
+                f[6] = eb.x;
+                f[7] = eb.y;
+            }
+        }
+        __syncthreads();
+        for (int i = 0; i < nch; i++) {
+            const float *f = sF + (g * kChunk + i) * NF;
+            st_rf<S>(s, sT + 9 * i);
+            if (ECHO == ECHO_SR) {
+                st_relax<S>(s, f[0], f[1], lane0);
+            } else if (ECHO == ECHO_SE || ECHO == ECHO_TSE) {
+                st_shift<S>(s, gl, L, w);
+                st_relax<S>(s, f[0], f[1], lane0);
+            } else if (ECHO == ECHO_FISP) {
+                st_relax<S>(s, f[0], f[1], lane0);
+            } else {
+                st_relax<S>(s, f[0], f[1], lane0);
+                st_b0<S>(s, make_float2(f[4], f[5]));
+            }
+            if (lane0) {
+                float2 v = s.fp[0];
+                sR[g * kChunk + i] = v;
+                nrm += v.x * v.x + v.y * v.y;
+            }
+            if (ECHO == ECHO_SR) {
+                st_relax<S>(s, f[2], f[3], lane0);
+            } else if (ECHO == ECHO_SE || ECHO == ECHO_TSE || ECHO == ECHO_FISP) {
+                st_shift<S>(s, gl, L, w);
+                st_relax<S>(s, f[2], f[3], lane0);
+            } else {
+                st_b0<S>(s, make_float2(f[6], f[7]));
+                st_shift<S>(s, gl, L, w);
+                st_relax<S>(s, f[2], f[3], lane0);
+            }
+        }
+        __syncwarp();
+        if (active)
+            for (int q = gl; q < nch; q += L) out[t0 + q] = sR[g * kChunk + q];
+    }
+    if (a.normalize || a.norms) {
+        nrm = __shfl_sync(0xffffffffu, nrm, 0, L);
+        if (a.norms && lane0 && active) a.norms[gatom] = sqrtf(nrm);
+        if (a.normalize) {
+            __syncwarp();
+            float inv = nrm;
+            if (inv > 0.f) inv = 1.f / sqrtf(inv);
+            if (active)
+                for (long long q = gl; q < nreps; q += L) out[q] = c_scale(out[q], inv);
+        }
+    }
+}
+
+// ROA (src/functions.cu:1021-1222).  State m = (Mx, My, Mz).  Per step:
+// rotation R(alpha, phi), relaxation over the full TR, z-rotation by
+// beta = pi*B0*TR/1000, readout Mx + iMy, z-rotation by beta.
+struct RoaStep {
+    float T[9];
+};
+
+// fill_transition_matrix (ROA, src/functions.cu:1049-1075); the Sgemm with
+// OP_N reads it column-major: new[i] = sum_l T[i + 3l] * m[l].
+__device__ __forceinline__ void roa_matrix(float alpha, float phi, float *T) {
+    float s_a, c_a, s_p, c_p;
+    __sincosf(alpha, &s_a, &c_a);
+    __sincosf(phi, &s_p, &c_p);
+    float s2 = 2 * c_p * s_p, c2 = c_p * c_p - s_p * s_p;
+    T[0] = c2;
+    T[1] = -s2;
+    T[2] = 0.f;
+    T[3] = s2 * c_a;
+    T[4] = c2 * c_a;
+    T[5] = -s_a;
+    T[6] = s2 * s_a;
+    T[7] = c2 * s_a;
+    T[8] = c_a;
+}
+
+// init_rf_pulse (ROA, src/functions.cu:1022-1047) with alpha 180, phi 0, TI 0.
+__device__ __forceinline__ void roa_init(float t1, float t2, float &m0, float &m1, float &m2) {
+    float ia = (float)(180.f * M_PI / 180.f), ip = (float)(0.f * M_PI / 180.f);
+    float e1 = expf(-0.f / t1), e2 = expf(-0.f / t2);
+    float sa, ca, sph, cph;
+    __sincosf(ia, &sa, &ca);
+    __sincosf(ip, &sph, &cph);
+    float sph2 = 2 * cph * sph, cph2 = cph * cph - sph * sph;
+    m0 = e2 * sph2 * sa;
+    m1 = e2 * cph2 * sa;
+    m2 = e1 * ca + 1 - e1;
+}
+
+// Single isochromat (the reference's roa_ssfp): one thread per atom.
+__global__ void __launch_bounds__(kEpgThreads) roa_kernel(EpgArgs a) {
+    __shared__ RoaStep sT[kChunk];
+    __shared__ float2 sR[kEpgThreads][kChunk + 1];
+    const int tid = threadIdx.x;
+    const long long blk = blockIdx.y;
+    const long long nreps = a.nreps;
+    const long long atom0 = (long long)blockIdx.x * kEpgThreads;
+    const long long ab = atom0 + tid;
+    const bool active = ab < a.natoms;
+    const long long gatom = blk * a.natoms + ab;
+    float t1 = 1.f, t2 = 1.f, b0 = 0.f;
+    if (active) {
+        const float *p = a.params + (blk * a.natoms + ab) * a.nparams;
+        t1 = p[0];
+        t2 = p[1];
+        b0 = p[2];
+    }
+    const float *alpha = a.alpha + blk * nreps;
+    const float *phi = a.sched + nreps;
+    const float *TR = a.sched + 2 * nreps;
+    float m0, m1, m2;
+    roa_init(t1, t2, m0, m1, m2);
+    float nrm = 0.f;
+    const int warp = tid / 32, lane = tid % 32;
+    for (long long t0 = 0; t0 < nreps; t0 += kChunk) {
+        const int nch = (int)min((long long)kChunk, nreps - t0);
+        __syncthreads();
+        for (int i = tid; i < nch; i += kEpgThreads) roa_matrix(alpha[t0 + i], phi[t0 + i], sT[i].T);
+        __syncthreads();
+        for (int i = 0; i < nch; i++) {
+            const float *T = sT[i].T;
+            float n0 = T[0] * m0 + T[3] * m1 + T[6] * m2;
+            float n1 = T[1] * m0 + T[4] * m1 + T[7] * m2;
+            float n2 = T[2] * m0 + T[5] * m1 + T[8] * m2;
+            float tr = TR[t0 + i];
+            float E1 = expf(-tr / t1), E2 = expf(-tr / t2);
+            m0 = E2 * n0;
+            m1 = E2 * n1;
+            m2 = E1 * n2 + (1 - E1);
+            float beta = (float)(M_PI * b0 * tr / 1000.f);
+            float sb, cb;
+            __sincosf(beta, &sb, &cb);
+            float w1 = m0, w2 = m1;
+            m0 = cb * w1 + sb * w2;
+            m1 = cb * w2 - sb * w1;
+            sR[tid][i] = make_float2(m0, m1);
+            nrm += m0 * m0 + m1 * m1;
+            w1 = m0;
+            w2 = m1;
+            m0 = cb * w1 + sb * w2;
+            m1 = cb * w2 - sb * w1;
+        }
+        __syncthreads();
+        for (int r = warp; r < kEpgThreads; r += kEpgThreads / 32) {
+            long long at = atom0 + r;
+            if (at >= a.natoms) continue;
+            float2 *o = a.atoms + (blk * a.natoms + at) * nreps + t0;
+            for (int q = lane; q < nch; q += 32) o[q] = sR[r][q];
+        }
+    }
+    __syncthreads();
+    if (a.norms && active) a.norms[gatom] = sqrtf(nrm);
+    if (a.normalize && active) {
+        float inv = nrm;
+        if (inv > 0.f) inv = 1.f / sqrtf(inv);
+        float2 *out = a.atoms + gatom * nreps;
+        for (long long q = 0; q < nreps; q++) out[q] = c_scale(out[q], inv);
+    }
+}
+
+// Multi-isochromat ROA: one warp per atom, lanes hold IPL isochromats each.
+// Isochromat j precesses by an extra pi*j/n_iso per half TR (2*pi*j/n_iso
+// per TR, so the n_iso isochromats dephase uniformly across 2*pi); the
+// readout is the mean of Mx + iMy over isochromats.
+template <int IPL>
+__global__ void __launch_bounds__(kEpgThreads) roa_iso_kernel(EpgArgs a) {
+    constexpr int WPC = kEpgThreads / 32;
+    __shared__ RoaStep sT[kChunk];
+    __shared__ float2 sPart[WPC][kChunk][33];
+    const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
+    const long long blk = blockIdx.y;
+    const long long nreps = a.nreps;
+    const long long ab = (long long)blockIdx.x * WPC + warp;
+    const bool active = ab < a.natoms;
+    const long long gatom = blk * a.natoms + ab;
+    float t1 = 1.f, t2 = 1.f, b0 = 0.f;
+    if (active) {
+        const float *p = a.params + gatom * a.nparams;
+        t1 = p[0];
+        t2 = p[1];
+        b0 = p[2];
+    }
+    const float *alpha = a.alpha + blk * nreps;
+    const float *phi = a.sched + nreps;
+    const float *TR = a.sched + 2 * nreps;
+    const int n_iso = a.n_iso;
+    float m0[IPL], m1[IPL], m2[IPL], cd[IPL], sd[IPL];
+    bool valid[IPL];
+#pragma unroll
+    for (int q = 0; q < IPL; q++) {
+        int j = lane * IPL + q;
+        valid[q] = j < n_iso;
+        roa_init(t1, t2, m0[q], m1[q], m2[q]);
+        double d = M_PI * (double)j / (double)n_iso;
+        cd[q] = (float)cos(d);
+        sd[q] = (float)sin(d);
+    }
+    const float inv_n = 1.f / (float)n_iso;
+    float nrm = 0.f;
+    float2 *out = a.atoms + gatom * nreps;
+    for (long long t0 = 0; t0 < nreps; t0 += kChunk) {
+        const int nch = (int)min((long long)kChunk, nreps - t0);
+        __syncthreads();
+        for (int i = tid; i < nch; i += kEpgThreads) roa_matrix(alpha[t0 + i], phi[t0 + i], sT[i].T);
+        __syncthreads();
+        for (int i = 0; i < nch; i++) {
+            const float *T = sT[i].T;
+            float tr = TR[t0 + i];
+            float E1 = expf(-tr / t1), E2 = expf(-tr / t2);
+            float beta = (float)(M_PI * b0 * tr / 1000.f);
+            float sb, cb;
+            __sincosf(beta, &sb, &cb);
+            float px = 0.f, py = 0.f;
+#pragma unroll
+            for (int q = 0; q < IPL; q++) {
+                float n0 = T[0] * m0[q] + T[3] * m1[q] + T[6] * m2[q];
+                float n1 = T[1] * m0[q] + T[4] * m1[q] + T[7] * m2[q];
+                float n2 = T[2] * m0[q] + T[5] * m1[q] + T[8] * m2[q];
+                float x = E2 * n0, y = E2 * n1;
+                m2[q] = E1 * n2 + (1 - E1);
+                // rotation by beta then by the isochromat's delta
+                float cx = cb * cd[q] - sb * sd[q], sx = sb * cd[q] + cb * sd[q];
+                float w1 = cx * x + sx * y, w2 = cx * y - sx * x;
+                if (valid[q]) {
+                    px += w1;
+                    py += w2;
+                }
+                m0[q] = cx * w1 + sx * w2;
+                m1[q] = cx * w2 - sx * w1;
+            }
+            sPart[warp][i][lane] = make_float2(px, py);
+        }
+        __syncwarp();
+        if (lane < nch) {
+            float sx = 0.f, sy = 0.f;
+            for (int l = 0; l < 32; l++) {
+                float2 v = sPart[warp][lane][l];
+                sx += v.x;
+                sy += v.y;
+            }
+            sPart[warp][lane][32] = make_float2(sx * inv_n, sy * inv_n);
+        }
+        __syncwarp();
+        for (int i = 0; i < nch; i++) {
+            float2 v = sPart[warp][i][32];
+            nrm += v.x * v.x + v.y * v.y;
+        }
+        if (active && lane < nch) out[t0 + lane] = sPart[warp][lane][32];
+    }
+    __syncwarp();
+    if (a.norms && active && lane == 0) a.norms[gatom] = sqrtf(nrm);
+    if (a.normalize && active) {
+        float inv = nrm;
+        if (inv > 0.f) inv = 1.f / sqrtf(inv);
+        for (long long q = lane; q < nreps; q += 32) out[q] = c_scale(out[q], inv);
+    }
+}
+
+inline cudaError_t launch_roa(const EpgArgs &a, long long natoms, unsigned gen_blocks,
+                              cudaStream_t st) {
+    if (a.n_iso <= 1) {
+        dim3 grid((unsigned)((natoms + kEpgThreads - 1) / kEpgThreads), gen_blocks);
+        roa_kernel<<<grid, kEpgThreads, 0, st>>>(a);
+    } else {
+        const long long wpc = kEpgThreads / 32;
+        dim3 grid((unsigned)((natoms + wpc - 1) / wpc), gen_blocks);
+        int ipl = (a.n_iso + 31) / 32;
+        if (ipl <= 1) roa_iso_kernel<1><<<grid, kEpgThreads, 0, st>>>(a);
+        else if (ipl <= 2) roa_iso_kernel<2><<<grid, kEpgThreads, 0, st>>>(a);
+        else if (ipl <= 4) roa_iso_kernel<4><<<grid, kEpgThreads, 0, st>>>(a);
+        else roa_iso_kernel<8><<<grid, kEpgThreads, 0, st>>>(a);
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace snapmrf

@@ -1,0 +1,335 @@
+// Maximum-inner-product matching on sm_100a (replaces MRF_match,
+// MRF_minimatch, generate_maps, merge_maps and compute_nsplits,
+// src/functions.cu:1317-1584).
+//
+// The reference runs a full FP32 CGEMM of every voxel against every B1
+// block, materialises the score matrix, scans it per voxel, then merges the
+// blocks.  Here voxels are first grouped by the B1 block they will be merged
+// into (counting sort), each group is scored only against its block's atoms
+// by a fused complex GEMM whose epilogue keeps the running first-argmax of
+// |s|^2, and CTAs that split a block's atoms merge their winners with one
+// 64-bit atomicMax per voxel on (score bits << 32 | ~index): larger score
+// wins, equal scores go to the lower atom index, like the reference's strict
+// '>' scan.  Without a B1 map the blocks' max-PD merge is the global first
+// argmax, which is computed directly over all atoms.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "common.h"
+#include "match_kernels.cuh"
+
+namespace snapmrf {
+
+// Nearest-B1 block per voxel (merge_maps with a B1 map,
+// src/functions.cu:1351-1384): strict '<' from an initial 10, so ties go to
+// the lower block and a voxel more than 10 away from every block (or NaN)
+// goes to block 0.
+__global__ void assign_bins_kernel(int *vox_bin, int *counts, const float *b1map,
+                                   const float *params, int nparams, long long natoms,
+                                   int nblocks, long long nvox) {
+    long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (v >= nvox) return;
+    float gt = b1map[v];
+    int best = 0;
+    float best_abs = 10.f;
+    for (int k = 0; k < nblocks; k++) {
+        float b1 = params[(long long)k * natoms * nparams + 3];
+        float d = fabsf(gt - b1);
+        if (d < best_abs) {
+            best_abs = d;
+            best = k;
+        }
+    }
+    vox_bin[v] = best;
+    atomicAdd(&counts[best], 1);
+}
+
+// Exclusive scans of the per-bin voxel counts (slots) and voxel tiles.
+__global__ void scan_bins_kernel(const int *counts, long long *slot_start, long long *tile_start,
+                                 long long *cursor, int nbins) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    long long s = 0, t = 0;
+    for (int b = 0; b < nbins; b++) {
+        slot_start[b] = s;
+        tile_start[b] = t;
+        cursor[b] = s;
+        s += counts[b];
+        t += (counts[b] + kMatchVT - 1) / kMatchVT;
+    }
+    slot_start[nbins] = s;
+    tile_start[nbins] = t;
+}
+
+__global__ void scatter_bins_kernel(long long *perm, long long *cursor, const int *vox_bin,
+                                    long long nvox) {
+    long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (v >= nvox) return;
+    long long pos = atomicAdd((unsigned long long *)&cursor[vox_bin[v]], 1ull);
+    perm[pos] = v;
+}
+
+// Bins that all hold every voxel: slot_start[b] = b*nvox, tile_start[b] = b*vt.
+__global__ void uniform_bins_kernel(long long *slot_start, long long *tile_start, int nbins,
+                                    long long nvox, long long vt) {
+    long long b = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (b > nbins) return;
+    slot_start[b] = b * nvox;
+    tile_start[b] = b * vt;
+}
+
+// Every block's B1 equal to its first atom's (true for trans_params tables).
+__global__ void check_uniform_b1_kernel(int *bad, const float *params, int nparams,
+                                        long long natoms, long long NATOMS) {
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= NATOMS) return;
+    long long head = (i / natoms) * natoms;
+    if (params[i * nparams + 3] != params[head * nparams + 3]) atomicExch(bad, 1);
+}
+
+// Per voxel: decode the winning atom, recompute its exact FP32 inner product
+// (PD = hypotf(|s|), generate_maps, src/functions.cu:1318-1349) and write
+// maps[v] = {T1, T2, B0, B1, PD}.  One warp per voxel.
+__global__ void finalize_maps_kernel(float *maps, long long *index_out, const unsigned long long *keys,
+                                     const long long *perm, const int *vox_bin, const float2 *atoms,
+                                     long long atom_stride, const float2 *img, long long img_stride,
+                                     long long nreps, const float *params, int nparams,
+                                     long long natoms_per_bin, long long nslots) {
+    long long s = (blockIdx.x * (long long)blockDim.x + threadIdx.x) / 32;
+    int lane = threadIdx.x % 32;
+    if (s >= nslots) return;
+    long long v = perm ? perm[s] : s;
+    long long bin = vox_bin ? vox_bin[v] : 0;
+    unsigned long long key = keys[s];
+    long long local = key ? (long long)(0xffffffffull - (key & 0xffffffffull)) : 0;
+    long long g = bin * natoms_per_bin + local;
+    const float2 *d = atoms + g * atom_stride;
+    const float2 *x = img + v * img_stride;
+    float re = 0.f, im = 0.f;
+    if (key) {
+        for (long long t = lane; t < nreps; t += 32) {
+            float2 a = d[t], b = x[t];
+            re += a.x * b.x + a.y * b.y;
+            im += a.x * b.y - a.y * b.x;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            re += __shfl_xor_sync(0xffffffffu, re, o);
+            im += __shfl_xor_sync(0xffffffffu, im, o);
+        }
+    }
+    if (lane == 0) {
+        const float *p = params + g * nparams;
+        float *m = maps + v * 5;
+        m[0] = p[0];
+        m[1] = p[1];
+        m[2] = p[2];
+        m[3] = p[3];
+        m[4] = key ? hypotf(re, im) : 0.f;
+        if (index_out) index_out[v] = g;
+    }
+}
+
+// General B1-map merge when a block holds several B1 values: every block was
+// matched against every voxel (keys[k * nvox + v]); pick the block whose
+// matched atom's B1 is nearest the map (src/functions.cu:1351-1384).
+__global__ void merge_nearest_b1_kernel(unsigned long long *keys_out, int *vox_bin,
+                                        const unsigned long long *keys, const float *b1map,
+                                        const float *params, int nparams, long long natoms,
+                                        int nblocks, long long nvox) {
+    long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (v >= nvox) return;
+    float gt = b1map[v];
+    int best = 0;
+    float best_abs = 10.f;
+    for (int k = 0; k < nblocks; k++) {
+        unsigned long long key = keys[(long long)k * nvox + v];
+        long long local = key ? (long long)(0xffffffffull - (key & 0xffffffffull)) : 0;
+        float b1 = params[((long long)k * natoms + local) * nparams + 3];
+        float d = fabsf(gt - b1);
+        if (d < best_abs) {
+            best_abs = d;
+            best = k;
+        }
+    }
+    vox_bin[v] = best;
+    keys_out[v] = keys[(long long)best * nvox + v];
+}
+
+static inline unsigned nblk(long long n, int t) { return (unsigned)((n + t - 1) / t); }
+
+}  // namespace snapmrf
+
+using namespace snapmrf;
+
+extern "C" int snapmrf_mrf_match(float *d_maps, const float *img, int img_on_host,
+                                 const float *d_atoms, const float *d_params, size_t nreps,
+                                 size_t NATOMS, size_t natoms, size_t nvoxels, int nparams,
+                                 int nmaps, const snapmrf_match_opts *opts, void *stream) {
+    cudaStream_t st = (cudaStream_t)stream;
+    if (!d_maps || !img || !d_atoms || !d_params)
+        SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "MRF_match: null pointer");
+    if (nmaps != 5 || nparams < 4)
+        SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "MRF_match: nmaps must be 5 and nparams >= 4");
+    if (nreps == 0 || nvoxels == 0 || natoms == 0 || NATOMS % natoms != 0)
+        SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "MRF_match: bad sizes (nreps %zu, nvoxels %zu, NATOMS %zu, natoms %zu)",
+                     nreps, nvoxels, NATOMS, natoms);
+    int precision = opts ? opts->precision : SNAPMRF_PREC_FP32;
+    if (precision != SNAPMRF_PREC_FP32)
+        SNAPMRF_FAIL(SNAPMRF_ERR_UNSUPPORTED, "MRF_match: unknown precision %d", precision);
+    size_t img_stride = (opts && opts->img_stride) ? opts->img_stride : nreps;
+    size_t atom_stride = (opts && opts->atom_stride) ? opts->atom_stride : nreps;
+    if (img_stride < nreps || atom_stride < nreps)
+        SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "MRF_match: strides must be >= nreps");
+    if (natoms >= 0xffffffffull || NATOMS >= (1ull << 40))
+        SNAPMRF_FAIL(SNAPMRF_ERR_UNSUPPORTED, "MRF_match: too many atoms per block");
+    const float *b1map = opts ? opts->b1map : nullptr;
+    const size_t nblocks = NATOMS / natoms;
+    if (nblocks > 65535) SNAPMRF_FAIL(SNAPMRF_ERR_UNSUPPORTED, "MRF_match: more than 65535 B1 blocks");
+    unsigned flags = opts ? opts->flags : 0u;
+    int64_t *d_index = opts ? opts->d_index : nullptr;
+
+    // Image on the device: one strided 2D copy instead of one copy per voxel
+    // (src/functions.cu:1524-1530).
+    DeviceScratch s_img;
+    const float2 *d_img = reinterpret_cast<const float2 *>(img);
+    long long istride = (long long)img_stride;
+    if (img_on_host) {
+        SNAPMRF_CUDA(s_img.alloc(nvoxels * nreps * sizeof(float2), st));
+        SNAPMRF_CUDA(cudaMemcpy2DAsync(s_img.ptr, nreps * sizeof(float2), img, img_stride * sizeof(float2),
+                                       nreps * sizeof(float2), nvoxels, cudaMemcpyHostToDevice, st));
+        d_img = s_img.as<float2>();
+        istride = (long long)nreps;
+    }
+    DeviceScratch s_b1;
+    const float *d_b1 = b1map;
+    if (b1map && opts->b1map_on_host) {
+        SNAPMRF_CUDA(s_b1.alloc(nvoxels * sizeof(float), st));
+        SNAPMRF_CUDA(cudaMemcpyAsync(s_b1.ptr, b1map, nvoxels * sizeof(float), cudaMemcpyHostToDevice, st));
+        d_b1 = s_b1.as<float>();
+    }
+
+    // Mode: global argmax (no B1 map), nearest-B1 bins (uniform blocks), or
+    // every block against every voxel followed by the nearest-B1 merge.
+    bool general = false;
+    if (d_b1 && nblocks > 1 && !(flags & SNAPMRF_MATCH_ASSUME_UNIFORM_B1)) {
+        DeviceScratch s_bad;
+        SNAPMRF_CUDA(s_bad.alloc(sizeof(int), st));
+        SNAPMRF_CUDA(cudaMemsetAsync(s_bad.ptr, 0, sizeof(int), st));
+        check_uniform_b1_kernel<<<nblk((long long)NATOMS, 256), 256, 0, st>>>(
+            s_bad.as<int>(), d_params, nparams, (long long)natoms, (long long)NATOMS);
+        SNAPMRF_LAUNCH_CHECK();
+        int bad = 0;
+        SNAPMRF_CUDA(cudaMemcpyAsync(&bad, s_bad.ptr, sizeof(int), cudaMemcpyDeviceToHost, st));
+        SNAPMRF_CUDA(cudaStreamSynchronize(st));
+        general = bad != 0;
+    }
+
+    const long long nvox = (long long)nvoxels;
+    int nbins;
+    long long per_bin_atoms, nslots;
+    if (!d_b1) {
+        nbins = 1;
+        per_bin_atoms = (long long)NATOMS;
+        nslots = nvox;
+    } else if (!general) {
+        nbins = (int)nblocks;
+        per_bin_atoms = (long long)natoms;
+        nslots = nvox;
+    } else {
+        nbins = (int)nblocks;
+        per_bin_atoms = (long long)natoms;
+        nslots = nvox * (long long)nblocks;
+    }
+
+    // scratch: keys[nslots] u64 | perm[nvox] i64 | slot_start, tile_start,
+    // cursor [nbins+1] i64 | vox_bin[nvox] i32 | counts[nbins] i32
+    size_t bytes = (size_t)nslots * 8 + (size_t)nvox * 8 + 3 * (size_t)(nbins + 1) * 8 +
+                   (size_t)nvox * 4 + (size_t)nbins * 4 + 64;
+    DeviceScratch s_work;
+    SNAPMRF_CUDA(s_work.alloc(bytes, st));
+    unsigned long long *keys = s_work.as<unsigned long long>();
+    long long *perm = reinterpret_cast<long long *>(keys + nslots);
+    long long *slot_start = perm + nvox;
+    long long *tile_start = slot_start + (nbins + 1);
+    long long *cursor = tile_start + (nbins + 1);
+    int *vox_bin = reinterpret_cast<int *>(cursor + (nbins + 1));
+    int *counts = vox_bin + nvox;
+    SNAPMRF_CUDA(cudaMemsetAsync(keys, 0, (size_t)nslots * 8, st));
+
+    MatchArgs m;
+    m.atoms = reinterpret_cast<const float2 *>(d_atoms);
+    m.atom_stride = (long long)atom_stride;
+    m.img = d_img;
+    m.img_stride = istride;
+    m.nreps = (long long)nreps;
+    m.nbins = nbins;
+    m.bin_natoms = per_bin_atoms;
+    m.nvox = nvox;
+    m.keys = keys;
+
+    if (!d_b1) {
+        // one bin, identity permutation
+        uniform_bins_kernel<<<1, 256, 0, st>>>(slot_start, tile_start, 1, nvox,
+                                               (nvox + kMatchVT - 1) / kMatchVT);
+        SNAPMRF_LAUNCH_CHECK();
+        m.perm = nullptr;
+        m.perm_mod = 0;
+    } else if (!general) {
+        SNAPMRF_CUDA(cudaMemsetAsync(counts, 0, (size_t)nbins * 4, st));
+        assign_bins_kernel<<<nblk(nvox, 256), 256, 0, st>>>(vox_bin, counts, d_b1, d_params, nparams,
+                                                            (long long)natoms, nbins, nvox);
+        SNAPMRF_LAUNCH_CHECK();
+        scan_bins_kernel<<<1, 32, 0, st>>>(counts, slot_start, tile_start, cursor, nbins);
+        SNAPMRF_LAUNCH_CHECK();
+        scatter_bins_kernel<<<nblk(nvox, 256), 256, 0, st>>>(perm, cursor, vox_bin, nvox);
+        SNAPMRF_LAUNCH_CHECK();
+        m.perm = perm;
+        m.perm_mod = 0;
+    } else {
+        uniform_bins_kernel<<<nblk(nbins + 1, 256), 256, 0, st>>>(slot_start, tile_start, nbins, nvox,
+                                                                  (nvox + kMatchVT - 1) / kMatchVT);
+        SNAPMRF_LAUNCH_CHECK();
+        m.perm = nullptr;
+        m.perm_mod = nvox;
+    }
+    m.slot_start = slot_start;
+    m.tile_start = tile_start;
+
+    // Grid: y walks voxel tiles (bin-major, so concurrent CTAs share a bin's
+    // atoms in L2), x splits a bin's atom tiles so that small voxel counts
+    // still fill the 148 SMs.
+    long long max_tiles = general ? (long long)nbins * ((nvox + kMatchVT - 1) / kMatchVT)
+                                  : (nvox + kMatchVT - 1) / kMatchVT + nbins;
+    long long atiles = (per_bin_atoms + kMatchAT - 1) / kMatchAT;
+    long long est_tiles = general ? max_tiles : (nvox + kMatchVT - 1) / kMatchVT;
+    long long target = 148 * 2 * 4;
+    long long splits = std::max(1ll, std::min(atiles, (target + est_tiles - 1) / std::max(1ll, est_tiles)));
+    m.atiles_per_split = (int)((atiles + splits - 1) / splits);
+    splits = (atiles + m.atiles_per_split - 1) / m.atiles_per_split;
+    dim3 grid((unsigned)splits, (unsigned)std::min(max_tiles, 65535ll));
+    SNAPMRF_CUDA(launch_match_fp32(m, grid, st));
+
+    const unsigned long long *fkeys = keys;
+    if (general) {
+        DeviceScratch s_merged;
+        SNAPMRF_CUDA(s_merged.alloc((size_t)nvox * 8, st));
+        merge_nearest_b1_kernel<<<nblk(nvox, 256), 256, 0, st>>>(s_merged.as<unsigned long long>(), vox_bin,
+                                                                 keys, d_b1, d_params, nparams,
+                                                                 (long long)natoms, nbins, nvox);
+        SNAPMRF_LAUNCH_CHECK();
+        finalize_maps_kernel<<<nblk(nvox * 32, 256), 256, 0, st>>>(
+            d_maps, (long long *)d_index, s_merged.as<unsigned long long>(), nullptr, vox_bin,
+            m.atoms, m.atom_stride, d_img, istride, (long long)nreps, d_params, nparams,
+            (long long)natoms, nvox);
+        SNAPMRF_LAUNCH_CHECK();
+        return SNAPMRF_OK;
+    }
+    finalize_maps_kernel<<<nblk(nvox * 32, 256), 256, 0, st>>>(
+        d_maps, (long long *)d_index, fkeys, d_b1 ? perm : nullptr, d_b1 ? vox_bin : nullptr, m.atoms,
+        m.atom_stride, d_img, istride, (long long)nreps, d_params, nparams, per_bin_atoms, nvox);
+    SNAPMRF_LAUNCH_CHECK();
+    return SNAPMRF_OK;
+}
