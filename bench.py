@@ -1,0 +1,454 @@
+"""Benchmark of the snapMRF hot path on B200: dictionary generation + B1-bin
+matching for one 240x240 B1-mapped MR-fingerprinting slice.
+
+Workload "fisp_b1map_240x240" (the full-size plain FP32 EPG-FISP form):
+  schedule  T = 1000, alpha_t = 10 + 50|sin(pi t / 250)| deg with alpha_0 =
+            180 deg (inversion), phase 0, TR_t ~ U[11, 15] ms (seed 1),
+            TE = TR / 2
+  grid      T1 = 100 * 1.05^k <= 5000 ms (81) x T2 = 10 * 1.05^k <= 2000 ms
+            (109), T1 > T2 -> 6938 pairs, x B1 = 0.60:0.02:1.40 (41 blocks)
+            = 284,458 atoms, w = 50 EPG states, atoms normalised
+  voxels    240 x 240; B1 map 1 + 0.3 (x^2 + y^2 - 0.5) clipped to
+            [0.6, 1.4]; 5 seeded elliptical tissue regions, +-5 % per-voxel
+            T1/T2 jitter, M0 ~ U[0.6, 1], random phase, complex Gaussian
+            noise at SNR 40 (sigma = ||s|| / sqrt(T) / 40); each voxel is
+            matched within its nearest B1 block
+One step = MRF_dict (all 41 blocks) + MRF_match of every voxel, the two
+calls the reference's mrf CLI makes.  `value` is voxels/s with inputs
+resident in HBM; `e2e` runs the same step through the public API from pinned
+host buffers with the uploads and the map download inside the timed region.
+Every input and output exceeds L2 (dictionary 2.28 GB, image 461 MB), so no
+flush is needed between steps.
+
+Multi-GPU (torchrun, one process per GPU): rank r processes its own slice
+(seeded by r) end to end, with no data-path collective; timing is the max
+over ranks of each rank's CUDA-event time.
+
+--impl reference times the reference algorithm's CPU implementation (the
+oracle, C, OpenMP over all host cores) on a bounded sample of the same
+workload and reports the same metric.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WORKLOAD = "fisp_b1map_240x240"
+T = 1000
+NSTATES = 50
+NX = NY = 240
+SNR = 40.0
+FLOP_PER_STATE_STEP = 66        # RF 54 + two relaxations 6 + 6
+PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
+
+
+# ---------------------------------------------------------------------------
+# workload
+# ---------------------------------------------------------------------------
+
+def schedule(seed: int = 1) -> np.ndarray:
+    """Raw epg_fisp schedule h_mrf[4][T]: alpha (rad), phase (rad), TR, TE (ms)."""
+    rng = np.random.default_rng(seed)
+    t = np.arange(T)
+    a = 10.0 + 50.0 * np.abs(np.sin(np.pi * t / 250.0))
+    a[0] = 180.0
+    tr = rng.uniform(11.0, 15.0, T)
+    return np.array([np.deg2rad(a), np.zeros(T), tr, tr / 2], np.float32)
+
+
+def grid():
+    t1 = np.array([100.0 * 1.05 ** k for k in range(200) if 100.0 * 1.05 ** k <= 5000.0], np.float32)
+    t2 = np.array([10.0 * 1.05 ** k for k in range(200) if 10.0 * 1.05 ** k <= 2000.0], np.float32)
+    b1 = np.array([0.60 + 0.02 * k for k in range(41)], np.float32)
+    return t1, t2, np.zeros(1, np.float32), b1
+
+
+def phantom(seed: int):
+    """B1 map, true (T1, T2) and M0 per voxel (Fortran voxel order like the
+    reference's RA images: x fastest)."""
+    rng = np.random.default_rng(1000 + seed)
+    y, x = np.meshgrid(np.linspace(-1, 1, NY), np.linspace(-1, 1, NX), indexing="ij")
+    b1 = np.clip(1.0 + 0.3 * (x ** 2 + y ** 2 - 0.5), 0.6, 1.4).astype(np.float32)
+    tissue = np.zeros(x.shape, np.int64)
+    t1v = rng.uniform(300.0, 3000.0, 5)
+    t2v = np.array([rng.uniform(30.0, min(400.0, v / 3)) for v in t1v])
+    for r in range(1, 5):
+        cx, cy = rng.uniform(-0.5, 0.5, 2)
+        ax_, ay_ = rng.uniform(0.15, 0.45, 2)
+        th = rng.uniform(0, np.pi)
+        xr = (x - cx) * np.cos(th) + (y - cy) * np.sin(th)
+        yr = -(x - cx) * np.sin(th) + (y - cy) * np.cos(th)
+        tissue[(xr / ax_) ** 2 + (yr / ay_) ** 2 <= 1.0] = r
+    t1 = t1v[tissue] * rng.uniform(0.95, 1.05, x.shape)
+    t2 = t2v[tissue] * rng.uniform(0.95, 1.05, x.shape)
+    m0 = rng.uniform(0.6, 1.0, x.shape)
+    ph = rng.uniform(0, 2 * np.pi, x.shape)
+    return (b1.reshape(-1), t1.reshape(-1).astype(np.float32), t2.reshape(-1).astype(np.float32),
+            m0.reshape(-1), ph.reshape(-1))
+
+
+def make_inputs(snap, torch, seed: int):
+    """Host inputs of one slice: (h_mrf, params, natoms, img, b1map, truth)."""
+    h_mrf = schedule(1)
+    t1, t2, b0, b1 = grid()
+    params = snap.trans_params(t1, t2, b0, b1)
+    natoms = params.shape[0] // len(b1)
+    b1map, vt1, vt2, m0, ph = phantom(seed)
+    nvox = b1map.size
+    # voxel signals: the same recursion at each voxel's own (T1, T2, B1),
+    # generated on the GPU with one B1 block per voxel
+    vparams = np.stack([vt1, vt2, np.zeros(nvox, np.float32), b1map], 1).astype(np.float32)
+    d_vp = torch.from_numpy(vparams).cuda()
+    d_sig = torch.empty((nvox, T, 2), dtype=torch.float32, device="cuda")
+    snap.MRF_dict(d_sig, d_vp, h_mrf, T, T, nvox, 1, 4, NSTATES, "epg_fisp",
+                  flags=snap.DICT_ALL_B1_BLOCKS)
+    torch.cuda.synchronize()
+    sig = d_sig.cpu().numpy()
+    sig = (sig[..., 0] + 1j * sig[..., 1]) * (m0 * np.exp(1j * ph))[:, None]
+    rng = np.random.default_rng(2000 + seed)
+    sigma = np.linalg.norm(sig, axis=1, keepdims=True) / np.sqrt(T) / SNR
+    noise = sigma / np.sqrt(2) * (rng.standard_normal(sig.shape) + 1j * rng.standard_normal(sig.shape))
+    img = (sig + noise).astype(np.complex64)
+    del d_sig, d_vp
+    return h_mrf, params, natoms, img, b1map, (vt1, vt2, m0)
+
+
+# ---------------------------------------------------------------------------
+# measurement helpers
+# ---------------------------------------------------------------------------
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.idx = device_index
+        self.proc = None
+        self.lines: list[str] = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "50"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, mx, pw, reasons = [], [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+                pw.append(float(f[3]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None,
+                "power_w_max": max(pw) if pw else None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def peaks() -> dict:
+    if PEAKS_FILE.exists():
+        p = json.loads(PEAKS_FILE.read_text())
+        return {"hbm_gbs": p.get("hbm_gbs"), "bf16_tflops": p.get("bf16_tflops"),
+                "sm_max_mhz": p.get("sm_max_mhz", 1965.0), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0, "source": "fallback"}
+
+
+def fp32_peak_tflops(sm_mhz: float) -> float:
+    """FP32 FMA peak of 148 SMs x 128 lanes x 2 flop at the given clock."""
+    return 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
+
+
+# ---------------------------------------------------------------------------
+# arms
+# ---------------------------------------------------------------------------
+
+def run_ours(args) -> None:
+    import torch
+    import torch.distributed as dist
+    import snapmrf_b200 as snap
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", init_method="env://",
+                                timeout=__import__("datetime").timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+
+    h_mrf, params, natoms, img, b1map, truth = make_inputs(snap, torch, seed=rank)
+    NATOMS = params.shape[0]
+    nvox = img.shape[0]
+    flags = snap.DICT_ALL_B1_BLOCKS | snap.DICT_NORMALIZE
+
+    # device-resident buffers
+    d_params = torch.from_numpy(params).to(dev)
+    d_atoms = torch.empty((NATOMS, T, 2), dtype=torch.float32, device=dev)
+    d_img = torch.from_numpy(img.view(np.float32).reshape(nvox, T, 2)).to(dev)
+    d_b1 = torch.from_numpy(b1map).to(dev)
+    d_maps = torch.empty((nvox, 5), dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream()
+
+    def step(ev=None):
+        if ev is not None:
+            ev[0].record(stream)
+        snap.MRF_dict(d_atoms, d_params, h_mrf, T, T, NATOMS, natoms, 4, NSTATES, "epg_fisp", flags=flags)
+        if ev is not None:
+            ev[1].record(stream)
+        snap.MRF_match(d_maps, d_img, d_atoms, d_params, T, T, NATOMS, natoms, nvox, in_b1map=d_b1,
+                       flags=snap.MATCH_ASSUME_UNIFORM_B1)
+        if ev is not None:
+            ev[2].record(stream)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    launches0 = snap.kernel_launches()
+    clk = ClockSampler(local)
+    clk.start()
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    t_start.record(stream)
+    for k in range(args.steps):
+        step(evs[k])
+    t_end.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    launches = snap.kernel_launches() - launches0
+    elapsed_ms = t_start.elapsed_time(t_end)
+    dict_ms = float(np.mean([e[0].elapsed_time(e[1]) for e in evs]))
+    match_ms = float(np.mean([e[1].elapsed_time(e[2]) for e in evs]))
+    maps = d_maps.cpu().numpy()
+
+    # end to end through the public API from pinned host buffers
+    h_params = torch.from_numpy(params).pin_memory()
+    h_img = torch.from_numpy(img.view(np.float32).reshape(nvox, T, 2)).pin_memory()
+    h_b1 = torch.from_numpy(b1map).pin_memory()
+    h_maps = torch.empty((nvox, 5), dtype=torch.float32).pin_memory()
+    e2e_atoms = d_atoms  # output buffers are allocated once, like the reference's caller
+
+    def e2e_step():
+        d_p = h_params.to(dev, non_blocking=True)
+        snap.MRF_dict(e2e_atoms, d_p, h_mrf, T, T, NATOMS, natoms, 4, NSTATES, "epg_fisp", flags=flags)
+        snap.MRF_match(d_maps, h_img, e2e_atoms, d_p, T, T, NATOMS, natoms, nvox, in_b1map=h_b1,
+                       img_stride=T, flags=snap.MATCH_ASSUME_UNIFORM_B1)
+        h_maps.copy_(d_maps, non_blocking=True)
+
+    for _ in range(max(1, args.warmup // 2)):
+        e2e_step()
+    torch.cuda.synchronize()
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    e2e_ms = e0.elapsed_time(e1)
+
+    # max over ranks
+    t = torch.tensor([elapsed_ms, e2e_ms, dict_ms, match_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    elapsed_ms, e2e_ms, dict_ms, match_ms = t.tolist()
+
+    if rank == 0:
+        ms_per_step = elapsed_ms / args.steps
+        value = world * nvox / (ms_per_step / 1e3)
+        e2e_value = world * nvox / (e2e_ms / args.steps / 1e3)
+        pk = peaks()
+        sm_mhz = clocks.get("sm_mhz") or pk["sm_max_mhz"]
+        fp32_peak = fp32_peak_tflops(pk["sm_max_mhz"])
+        dict_flops = NATOMS * T * NSTATES * FLOP_PER_STATE_STEP
+        match_flops = nvox * 8.0 * T * natoms
+        dict_tf = dict_flops / (dict_ms / 1e3) / 1e12
+        match_tf = match_flops / (match_ms / 1e3) / 1e12
+        rl_dict = {"kernel": "epg_fisp dictionary", "bound": "fp32", "achieved": round(dict_tf, 2),
+                   "peak": round(fp32_peak, 2), "unit": "TFLOP/s", "frac": round(dict_tf / fp32_peak, 4),
+                   "traffic": None, "algorithmic_flop_per_launch": dict_flops, "ms": round(dict_ms, 3)}
+        rl_match = {"kernel": "fp32 B1-bin match", "bound": "fp32", "achieved": round(match_tf, 2),
+                    "peak": round(fp32_peak, 2), "unit": "TFLOP/s", "frac": round(match_tf / fp32_peak, 4),
+                    "traffic": None, "algorithmic_flop_per_launch": match_flops, "ms": round(match_ms, 3)}
+        dominant, other = (rl_match, rl_dict) if match_ms >= dict_ms else (rl_dict, rl_match)
+        # accuracy of the produced maps against the voxels' true parameters
+        vt1, vt2, _ = truth
+        e1_ = np.abs(maps[:, 0] - vt1) / vt1
+        e2_ = np.abs(maps[:, 1] - vt2) / vt2
+        line = {
+            "metric": "dict atoms/s + matched voxels/s (voxels/s of the full dict+match step)",
+            "value": round(value, 1), "unit": "voxels/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms_per_step, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "T": T, "nstates": NSTATES, "atoms": NATOMS,
+                       "atoms_per_b1_block": natoms, "b1_blocks": NATOMS // natoms, "voxels": nvox,
+                       "echo_type": "epg_fisp", "match": "fp32, nearest B1 block",
+                       "l2": "inputs and outputs larger than L2 (no flush needed)",
+                       "parallelism": f"{world} independent slices" if world > 1 else "single GPU"},
+            "dict_atoms_per_s": round(world * NATOMS / (dict_ms / 1e3), 1),
+            "match_voxels_per_s": round(world * nvox / (match_ms / 1e3), 1),
+            "stage_ms": {"dict": round(dict_ms, 3), "match": round(match_ms, 3)},
+            "roofline": dominant, "roofline_other": other,
+            "peak_note": "fp32 peak = 148 SMs x 128 lanes x 2 flop x max SM clock (nominal); "
+                         f"HBM/bf16 peaks {pk['source']}",
+            "e2e": {"value": round(e2e_value, 1), "unit": "voxels/s",
+                    "h2d_bytes_per_step": int(params.nbytes + img.nbytes + b1map.nbytes + h_mrf.nbytes),
+                    "d2h_bytes_per_step": int(nvox * 5 * 4)},
+            "gpu_launches": int(launches),
+            "clocks": clocks,
+            "maps_error_vs_truth": {"t1_median_rel": round(float(np.median(e1_)), 5),
+                                    "t2_median_rel": round(float(np.median(e2_)), 5)},
+        }
+        if not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(args.cpu_seconds)
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def cpu_sample(seconds: float):
+    """Times the oracle's FP32 CPU path (all host threads) on a bounded
+    sample of the workload sized to about `seconds` of CPU time; returns
+    (step seconds extrapolated to the full workload, sample text, threads)."""
+    from oracle import oracle as orc
+    import snapmrf_b200 as snap
+    nthr = orc.max_threads()
+    h_mrf = schedule(1)
+    t1, t2, b0, b1 = grid()
+    params = snap.trans_params(t1, t2, b0, b1)
+    natoms = params.shape[0] // len(b1)
+    NATOMS = params.shape[0]
+    nvox = NX * NY
+    rng = np.random.default_rng(7)
+
+    def run(na, nv):
+        t0 = time.perf_counter()
+        atoms = orc.dict_atoms("epg_fisp", params[:na], h_mrf, T, natoms=na, nstates=NSTATES,
+                               precision="f32", flags=orc.NORMALIZE, nthreads=nthr)
+        t_dict = time.perf_counter() - t0
+        # one full B1 block (natoms atoms) built from the generated atoms
+        blk = atoms.astype(np.complex64)[np.arange(natoms) % na]
+        vox = (blk[rng.integers(0, natoms, nv)] + np.complex64(0.01)).astype(np.complex64)
+        t0 = time.perf_counter()
+        orc.match(vox, blk, params[:natoms], T, precision="f32", nthreads=nthr)
+        return t_dict, time.perf_counter() - t0
+
+    na0, nv0 = 4 * nthr, nthr
+    td0, tm0 = run(na0, nv0)
+    na = int(min(natoms, max(na0, na0 * (seconds / 2) / max(td0, 1e-3))))
+    nv = int(min(nvox, max(nv0, nv0 * (seconds / 2) / max(tm0, 1e-3))))
+    t_dict, t_match = run(na, nv)
+    step_s = t_dict / na * NATOMS + t_match / nv * nvox
+    sample = (f"oracle FP32 C (OpenMP {nthr} threads): dictionary {na} of {NATOMS} atoms "
+              f"({t_dict:.2f} s), matching {nv} of {nvox} voxels against one {natoms}-atom B1 block "
+              f"({t_match:.2f} s); step time extrapolated linearly")
+    return step_s, sample, nthr
+
+
+def cpu_baseline(seconds: float) -> dict:
+    step_s, sample, nthr = cpu_sample(seconds)
+    return {"value": round(NX * NY / step_s, 3), "unit": "voxels/s", "cores": nthr, "kind": "port",
+            "sample": sample}
+
+
+def run_reference(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    for _ in range(args.warmup):
+        cpu_sample(args.cpu_seconds / 4)
+    times = []
+    sample = ""
+    nthr = 1
+    for _ in range(args.steps):
+        s, sample, nthr = cpu_sample(args.cpu_seconds)
+        times.append(s)
+    step_s = float(np.mean(times))
+    value = NX * NY / step_s
+    line = {"impl": "reference", "metric": "dict atoms/s + matched voxels/s (voxels/s of the full dict+match step)",
+            "value": round(value, 3), "unit": "voxels/s", "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(step_s * 1e3, 1),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": {"workload": WORKLOAD, "T": T, "nstates": NSTATES,
+                                            "voxels": NX * NY, "echo_type": "epg_fisp"},
+            "cpu_baseline": {"value": round(value, 3), "unit": "voxels/s", "cores": nthr, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": round(value, 3), "unit": "voxels/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--cpu-seconds", type=float, default=6.0,
+                    help="approximate CPU seconds of the bounded CPU sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

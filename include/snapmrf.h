@@ -51,6 +51,9 @@ typedef enum snapmrf_status {
 const char *snapmrf_last_error(void);
 /* Library version string. */
 const char *snapmrf_version(void);
+/* Number of CUDA kernels this library has launched in this process (all
+ * threads, all devices): an exact count for benchmarks and tests. */
+uint64_t snapmrf_kernel_launches(void);
 
 /* ------------------------------------------------------------------------
  * Host: schedules, grids and the parameter table.
@@ -101,7 +104,8 @@ typedef struct snapmrf_ra {
     uint64_t size;   /* data bytes */
     uint64_t ndims;
     uint64_t *dims;
-    uint8_t *data;
+    uint8_t *data;   /* page-locked when read with pinned != 0; snapmrf_ra_read
+                        records that in flags bit 63, which is never written */
 } snapmrf_ra;
 
 /* Reads an RA file; data in page-locked host memory when pinned != 0

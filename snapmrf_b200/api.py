@@ -74,6 +74,7 @@ def lib() -> C.CDLL:
         sz, vp, fp = C.c_size_t, C.c_void_p, C.POINTER(C.c_float)
         L.snapmrf_last_error.restype = C.c_char_p
         L.snapmrf_version.restype = C.c_char_p
+        L.snapmrf_kernel_launches.restype = C.c_uint64
         L.snapmrf_csv_dim.restype = sz
         L.snapmrf_csv_dim.argtypes = [C.c_char_p]
         L.snapmrf_csv_read.argtypes = [vp, sz, C.c_char_p]
@@ -97,6 +98,11 @@ def lib() -> C.CDLL:
                                         C.POINTER(MatchOpts), vp]
         _lib = L
     return _lib
+
+
+def kernel_launches() -> int:
+    """Kernels launched by libsnapmrf.so so far in this process."""
+    return lib().snapmrf_kernel_launches()
 
 
 def _check(rc: int) -> None:
@@ -274,8 +280,8 @@ def MRF_match(d_maps, img, d_atoms, d_params, NREPS: int, nreps: int, NATOMS: in
     img: host numpy complex64 [nvoxels][stride] or a device tensor; NREPS is
     the dictionary's time points (atom stride), nreps the matched time points.
     in_b1map: None, a path to an RA B1 map, a host array or a device tensor."""
-    on_host = isinstance(img, np.ndarray)
-    if on_host:
+    on_host = isinstance(img, np.ndarray) or (hasattr(img, "device") and img.device.type == "cpu")
+    if isinstance(img, np.ndarray):
         img = np.ascontiguousarray(img, np.complex64)
         if not img_stride:
             img_stride = img.shape[-1] if img.ndim > 1 else nreps
@@ -288,6 +294,8 @@ def MRF_match(d_maps, img, d_atoms, d_params, NREPS: int, nreps: int, NATOMS: in
             in_b1map = np.ascontiguousarray(in_b1map, np.float32).reshape(-1)
             if in_b1map.size < nvoxels:
                 raise SnapMRFError(1, "B1 map has fewer values than voxels")
+            b1_host = 1
+        elif hasattr(in_b1map, "device") and in_b1map.device.type == "cpu":
             b1_host = 1
         b1 = in_b1map
     opts = MatchOpts(precision, flags, img_stride, NREPS, _ptr(b1), b1_host, _ptr(d_index))

@@ -14,6 +14,8 @@ namespace snapmrf {
 // Records `msg` as this thread's last error and returns `code`.
 int set_error(int code, const char *fmt, ...);
 void clear_error();
+// Adds n to the process-wide kernel launch counter.
+void note_launches(unsigned n);
 
 }  // namespace snapmrf
 
@@ -33,9 +35,19 @@ void clear_error();
                                         cudaGetErrorString(_e), __FILE__, __LINE__);    \
     } while (0)
 
-#define SNAPMRF_LAUNCH_CHECK() SNAPMRF_CUDA(cudaGetLastError())
+#define SNAPMRF_LAUNCH_CHECK()            \
+    do {                                  \
+        ::snapmrf::note_launches(1);      \
+        SNAPMRF_CUDA(cudaGetLastError()); \
+    } while (0)
 
 namespace snapmrf {
+
+// Page-locked staging buffer of this thread on the current device for small
+// uploads, so that cudaMemcpyAsync stays asynchronous.  stage_acquire waits
+// for the previous upload from the buffer (stage_release records it).
+void *stage_acquire(size_t bytes);
+cudaError_t stage_release(cudaStream_t st);
 
 // Stream-ordered scratch allocation that is released on scope exit.
 struct DeviceScratch {

@@ -84,6 +84,7 @@ static cudaError_t launch_epg_ref(const EpgArgs &a, dim3 grid, cudaStream_t st) 
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     k<<<grid, kEpgThreads, smem, st>>>(a);
+    note_launches(1);
     return cudaGetLastError();
 }
 
@@ -170,8 +171,11 @@ extern "C" int snapmrf_mrf_dict(float *d_atoms, const float *d_params, const flo
     SNAPMRF_CUDA(scratch.alloc((4 * nreps + gen_blocks * nreps) * sizeof(float), st));
     float *d_sched = scratch.as<float>();
     float *d_alpha = d_sched + 4 * nreps;
-    SNAPMRF_CUDA(cudaMemcpyAsync(d_sched, sched.data(), 4 * nreps * sizeof(float),
-                                 cudaMemcpyHostToDevice, st));
+    float *h_stage = static_cast<float *>(stage_acquire(4 * nreps * sizeof(float)));
+    if (!h_stage) SNAPMRF_FAIL(SNAPMRF_ERR_ALLOC, "MRF_dict: cannot allocate a pinned staging buffer");
+    memcpy(h_stage, sched.data(), 4 * nreps * sizeof(float));
+    SNAPMRF_CUDA(cudaMemcpyAsync(d_sched, h_stage, 4 * nreps * sizeof(float), cudaMemcpyHostToDevice, st));
+    SNAPMRF_CUDA(stage_release(st));
     int mode = (echo == ECHO_SSFP) ? 0 : (all_blocks ? 1 : 2);
     prepare_alpha_kernel<<<(unsigned)((nreps + 255) / 256), 256, 0, st>>>(
         d_alpha, d_sched, d_params, nparams, (long long)nreps, (long long)natoms,

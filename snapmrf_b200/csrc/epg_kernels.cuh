@@ -126,9 +126,10 @@ __device__ __forceinline__ void st_b0(LaneState<S> &s, float2 e) {
     }
 }
 
-// dephase_gradients (src/functions.cu:619-668): F+[k] <- F+[k-1],
-// F-[k] <- F-[k+1], F+[0] = conj(F-[0]), F-[w-1] = 0.  Slots k >= w are kept
-// zero so that F-[w-1] picks up a zero.
+// dephase_gradients (src/functions.cu:619-668): F+[k] <- F+[k-1] for
+// k = w-1..1, F-[k] <- F-[k+1] for k = 0..w-2 (F-[w-1] keeps its value), then
+// F+[0] = conj(F-[0]) and F-[w-1] = 0.  With w = 1 nothing shifts and F+[0]
+// takes the conjugate of the unshifted F-[0].  Slots k >= w are kept zero.
 template <int S>
 __device__ __forceinline__ void st_shift(LaneState<S> &s, int gl, int L, int w) {
     const unsigned full = 0xffffffffu;
@@ -144,12 +145,18 @@ __device__ __forceinline__ void st_shift(LaneState<S> &s, int gl, int L, int w) 
     for (int j = S - 1; j >= 1; j--) s.fp[j] = s.fp[j - 1];
     s.fp[0] = up;
 #pragma unroll
-    for (int j = 0; j < S - 1; j++) s.fm[j] = s.fm[j + 1];
-    s.fm[S - 1] = (gl == L - 1) ? make_float2(0.f, 0.f) : dn;
+    for (int j = 0; j < S; j++) {
+        const int k = gl * S + j;
+        float2 nxt = (j < S - 1) ? s.fm[j + 1] : ((gl == L - 1) ? make_float2(0.f, 0.f) : dn);
+        if (k != w - 1) s.fm[j] = nxt;
+    }
     if (gl == 0) s.fp[0] = c_conj(s.fm[0]);
 #pragma unroll
-    for (int j = 0; j < S; j++)
-        if (gl * S + j >= w) s.fp[j] = make_float2(0.f, 0.f);
+    for (int j = 0; j < S; j++) {
+        const int k = gl * S + j;
+        if (k >= w) s.fp[j] = make_float2(0.f, 0.f);
+        if (k == w - 1) s.fm[j] = make_float2(0.f, 0.f);
+    }
 }
 
 // init_rf_pulse (EPG, src/functions.cu:456-481) into state 0.
@@ -539,6 +546,7 @@ inline cudaError_t launch_roa(const EpgArgs &a, long long natoms, unsigned gen_b
         else if (ipl <= 4) roa_iso_kernel<4><<<grid, kEpgThreads, 0, st>>>(a);
         else roa_iso_kernel<8><<<grid, kEpgThreads, 0, st>>>(a);
     }
+    note_launches(1);
     return cudaGetLastError();
 }
 

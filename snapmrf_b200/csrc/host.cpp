@@ -4,14 +4,57 @@
 // values (and therefore atom order and map values) are bit-identical; the
 // differences are that failures return a status instead of asserting or
 // crashing.
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 
+#include <map>
+
+#include <cuda_runtime.h>
+
 #include "common.h"
 
 namespace snapmrf {
+
+struct Stage {
+    void *p = nullptr;
+    size_t cap = 0;
+    cudaEvent_t ev = nullptr;
+};
+
+static thread_local std::map<int, Stage> g_stage;
+
+void *stage_acquire(size_t bytes) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+    Stage &s = g_stage[dev];
+    if (s.ev) cudaEventSynchronize(s.ev);
+    if (s.cap < bytes) {
+        if (s.p) cudaFreeHost(s.p);
+        s.cap = 0;
+        size_t want = bytes < 65536 ? 65536 : bytes;
+        if (cudaMallocHost(&s.p, want) != cudaSuccess) {
+            s.p = nullptr;
+            return nullptr;
+        }
+        s.cap = want;
+    }
+    return s.p;
+}
+
+cudaError_t stage_release(cudaStream_t st) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    Stage &s = g_stage[dev];
+    if (!s.ev) {
+        e = cudaEventCreateWithFlags(&s.ev, cudaEventDisableTiming);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaEventRecord(s.ev, st);
+}
 
 static thread_local std::string g_last_error;
 
@@ -27,6 +70,10 @@ int set_error(int code, const char *fmt, ...) {
 
 void clear_error() { g_last_error.clear(); }
 
+static std::atomic<uint64_t> g_launches{0};
+
+void note_launches(unsigned n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
 }  // namespace snapmrf
 
 using snapmrf::set_error;
@@ -34,6 +81,8 @@ using snapmrf::set_error;
 extern "C" const char *snapmrf_last_error(void) { return snapmrf::g_last_error.c_str(); }
 
 extern "C" const char *snapmrf_version(void) { return "snapmrf-b200 0.1 (sm_100a)"; }
+
+extern "C" uint64_t snapmrf_kernel_launches(void) { return snapmrf::g_launches.load(); }
 
 // csv_dim (src/functions.cu:100-120): counts '\n'.  The reference reads with
 // a signed char compared against EOF, so a 0xFF byte also ends the count.

@@ -172,6 +172,7 @@ __global__ void __launch_bounds__(kMatchThreads, 1) match_fp32_kernel(MatchArgs 
 
 inline cudaError_t launch_match_fp32(const MatchArgs &m, dim3 grid, cudaStream_t st) {
     match_fp32_kernel<<<grid, kMatchThreads, 0, st>>>(m);
+    note_launches(1);
     return cudaGetLastError();
 }
 

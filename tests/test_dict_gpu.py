@@ -1,0 +1,161 @@
+"""Dictionary generation on the GPU vs the reference's golden vectors and the
+oracle.  Tolerances:
+  - reference goldens (the reference's own FP32 GPU output): every element
+    within 1e-6 absolute (the reference's own test sums |diff| < 1e-6 over a
+    whole dictionary; that sum is printed and checked at 2e-6);
+  - FP64 oracle: per atom max_t|a - b| / max_t|b| <= 1e-4 at T = 1000 (the
+    RF matrices use the device __sincosf like the reference, whose absolute
+    error ~4e-7 accumulates over the recursion's memory), <= 2e-5 at T <= 300.
+"""
+import numpy as np
+import pytest
+
+from cases import REFERENCE_DICT_CASES, mrf_schedule, reference_case_inputs, rel_err_per_atom
+from gpu_util import run_dict
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("name", list(REFERENCE_DICT_CASES))
+def test_reference_goldens(snap, golden, name):
+    echo, h_mrf, params, NATOMS, natoms, nreps = reference_case_inputs(name, golden)
+    atoms = run_dict(snap, echo, params, h_mrf, nreps, natoms=natoms, nstates=101)
+    ref = golden["atoms_" + name]
+    d = np.abs(atoms.astype(np.complex128) - ref)
+    print(f"{name}: sum|diff| = {d.sum():.3e}  max = {d.max():.3e}")
+    assert d.max() < 1e-6
+    assert d.sum() < 2e-6
+
+
+def _grid(t1s, t2s, b0s=(0.0,), b1s=(1.0,)):
+    rows = [(a, b, c, d) for d in b1s for c in b0s for b in t2s for a in t1s if a > b]
+    return np.array(rows, np.float32)
+
+
+@pytest.mark.parametrize("nstates", [1, 5, 20, 33, 50, 101, 256])
+def test_fisp_vs_oracle_layouts(snap, oracle, nstates):
+    """Every lane/state layout (w from 1 to 256) against the FP64 oracle."""
+    T = 200
+    h = mrf_schedule(T, seed=0)
+    params = _grid(np.geomspace(100, 3000, 9), np.geomspace(10, 1500, 7))
+    got = run_dict(snap, "epg_fisp", params, h, T, nstates=nstates)
+    ref = oracle.dict_atoms("epg_fisp", params, h, T, nstates=nstates, nthreads=8)
+    rel = rel_err_per_atom(got, ref)
+    print(f"w={nstates}: max rel {rel.max():.3e}")
+    assert rel.max() < 2e-5
+
+
+def test_fisp_long_schedule_vs_oracle(snap, oracle):
+    T = 1000
+    h = mrf_schedule(T, seed=1)
+    params = _grid(np.geomspace(100, 5000, 12), np.geomspace(10, 2000, 12))
+    got = run_dict(snap, "epg_fisp", params, h, T, nstates=50)
+    ref = oracle.dict_atoms("epg_fisp", params, h, T, nstates=50, nthreads=8)
+    ref32 = oracle.dict_atoms("epg_fisp", params, h, T, nstates=50, nthreads=8, precision="f32")
+    rel = rel_err_per_atom(got, ref)
+    rel32 = rel_err_per_atom(got, ref32)
+    print(f"T=1000 w=50: max rel vs f64 {rel.max():.3e}, vs f32 oracle {rel32.max():.3e}")
+    assert rel.max() < 1e-4
+
+
+@pytest.mark.parametrize("echo", ["epg_sr", "epg_se", "epg_tse1"])
+def test_other_echo_types_vs_oracle(snap, oracle, echo):
+    T = 64
+    rng = np.random.default_rng(5)
+    h = np.array([rng.uniform(0.3, 3.0, T), rng.uniform(-1, 1, T), rng.uniform(20, 60, T),
+                  rng.uniform(2, 10, T)], np.float32)
+    params = _grid(np.geomspace(200, 2000, 5), np.geomspace(20, 150, 4))
+    got = run_dict(snap, echo, params, h, T, nstates=40)
+    ref = oracle.dict_atoms(echo, params, h, T, nstates=40)
+    rel = rel_err_per_atom(got, ref)
+    print(f"{echo}: max rel {rel.max():.3e}")
+    assert rel.max() < 2e-5
+
+
+def _ssfp_csv(T, seed):
+    """Schedule in the CSV convention of epg_ssfp / roa_ssfp: flip fraction
+    of 60 deg, phase deg, TR and TE extensions of 16 / 3.5 ms."""
+    rng = np.random.default_rng(seed)
+    fa = 0.1 + 0.8 * np.abs(np.sin(np.pi * np.arange(T) / 80))
+    ph = np.where(np.arange(T) % 2 == 0, 0.0, 180.0)
+    return np.array([fa, ph, rng.uniform(-4, -2, T), rng.uniform(-1, 1, T)], np.float32)
+
+
+def test_ssfp_b0_b1_blocks_vs_oracle(snap, oracle):
+    T = 300
+    h = _ssfp_csv(T, 2)
+    params = _grid(np.geomspace(200, 3000, 5), np.geomspace(20, 300, 4), b0s=(-60.0, -7.0, 0.0, 33.0),
+                   b1s=(0.8, 1.0, 1.2))
+    natoms = params.shape[0] // 3
+    got = run_dict(snap, "epg_ssfp", params, h, T, natoms=natoms, nstates=30)
+    ref = oracle.dict_atoms("epg_ssfp", params, h, T, natoms=natoms, nstates=30, nthreads=8)
+    rel = rel_err_per_atom(got, ref)
+    print(f"ssfp B0/B1: max rel {rel.max():.3e}")
+    assert rel.max() < 1e-4
+    np.testing.assert_allclose(np.linalg.norm(got, axis=1), 1.0, rtol=1e-5)
+
+
+@pytest.mark.parametrize("n_iso", [1, 7, 100])
+def test_roa_vs_oracle(snap, oracle, n_iso):
+    T = 200
+    h = _ssfp_csv(T, 4)
+    params = _grid(np.geomspace(200, 3000, 4), np.geomspace(20, 300, 4), b0s=(-40.0, 0.0, 25.0),
+                   b1s=(0.9, 1.1))
+    natoms = params.shape[0] // 2
+    flags = snap.DICT_ALL_B1_BLOCKS if n_iso > 1 else 0
+    got = run_dict(snap, "roa_ssfp", params, h, T, natoms=natoms, n_iso=n_iso, flags=flags)
+    ref = oracle.dict_atoms("roa_ssfp", params, h, T, natoms=natoms, n_iso=n_iso, flags=flags)
+    gen = ref.shape[0]
+    rel = rel_err_per_atom(got[:gen], ref)
+    print(f"roa n_iso={n_iso}: max rel {rel.max():.3e}")
+    assert rel.max() < 1e-4
+
+
+def test_blocks_left_untouched_without_flag(snap, oracle):
+    """epg_fisp fills block 0 only (src/functions.cu:1307-1309)."""
+    T = 20
+    h = mrf_schedule(T, seed=9)
+    params = _grid([500.0, 900.0], [50.0, 80.0], b1s=(0.9, 1.0, 1.1))
+    natoms = params.shape[0] // 3
+    got = run_dict(snap, "epg_fisp", params, h, T, natoms=natoms, nstates=10, fill=123.0)
+    assert np.all(got[natoms:] == np.complex64(123 + 123j))
+    assert not np.any(got[:natoms] == np.complex64(123 + 123j))
+
+
+def test_b1_extension_and_norms(snap, oracle):
+    T = 150
+    h = mrf_schedule(T, seed=2)
+    params = _grid(np.geomspace(300, 3000, 4), np.geomspace(30, 300, 3), b1s=(0.7, 1.0, 1.3))
+    natoms = params.shape[0] // 3
+    flags = snap.DICT_ALL_B1_BLOCKS | snap.DICT_NORMALIZE
+    got, norms = run_dict(snap, "epg_fisp", params, h, T, natoms=natoms, nstates=20, flags=flags,
+                          want_norms=True)
+    ref, rnorms = oracle.dict_atoms("epg_fisp", params, h, T, natoms=natoms, nstates=20, flags=flags,
+                                    return_norms=True)
+    assert rel_err_per_atom(got, ref).max() < 2e-5
+    np.testing.assert_allclose(norms, rnorms, rtol=2e-5)
+
+
+def test_single_time_point_and_ragged_atoms(snap, oracle):
+    h = mrf_schedule(1, seed=3, inversion=False)
+    params = _grid(np.linspace(150, 4000, 37), [100.0])
+    got = run_dict(snap, "epg_fisp", params, h, 1, nstates=7)
+    ref = oracle.dict_atoms("epg_fisp", params, h, 1, nstates=7)
+    np.testing.assert_allclose(got, ref, rtol=1e-6, atol=1e-7)
+
+
+def test_normalize_entry_point(snap):
+    import torch
+    rng = np.random.default_rng(0)
+    a = (rng.standard_normal((33, 77)) + 1j * rng.standard_normal((33, 77))).astype(np.complex64)
+    a[5] = 0
+    d = torch.from_numpy(a.view(np.float32)).cuda()
+    n = torch.zeros(33, device="cuda")
+    snap.normalize(d, 77, 33, n)
+    torch.cuda.synchronize()
+    out = d.cpu().numpy().view(np.complex64)
+    ref_n = np.linalg.norm(a.astype(np.complex128), axis=1)
+    np.testing.assert_allclose(n.cpu().numpy(), ref_n, rtol=1e-5)
+    ok = ref_n > 0
+    np.testing.assert_allclose(out[ok], (a[ok] / ref_n[ok, None]), rtol=1e-5, atol=1e-6)
+    assert np.all(out[5] == 0)
