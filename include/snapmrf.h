@@ -187,6 +187,45 @@ int snapmrf_mrf_match(float *d_maps, const float *img, int img_on_host,
                       size_t NATOMS, size_t natoms, size_t nvoxels, int nparams, int nmaps,
                       const snapmrf_match_opts *opts, void *stream);
 
+/* Largest request snapmrf_mrf_match_noalloc accepts: its working arrays live
+ * in one fixed array of about 1.3 MiB per GPU (sized for 65,536 voxels and
+ * 1,024 B1 blocks). */
+#define SNAPMRF_NOALLOC_MAX_VOXELS 65536
+#define SNAPMRF_NOALLOC_MAX_B1_BLOCKS 1024
+
+/* Matching that allocates no device memory.  No counterpart in the
+ * reference: its MRF_match allocates on every call, as snapmrf_mrf_match does.
+ *
+ * For callers that cannot allocate while they run: a host framework that
+ * has already reserved the GPU's free memory in its own caching allocator
+ * (a cudaMalloc here would fail, or make that allocator flush and
+ * synchronise), or a scanner reconstruction pipeline that forbids
+ * allocation after start-up because an allocation can stall the device.
+ * Every working array comes from one __device__ array of fixed size that
+ * each GPU holds from the moment the library is loaded until the process
+ * exits; nothing is allocated or freed by the call.
+ *
+ * Same results as snapmrf_mrf_match in its FP32 form, with these limits:
+ *   - d_img, d_b1map (optional) and every output are device memory;
+ *   - nvoxels <= SNAPMRF_NOALLOC_MAX_VOXELS and, with a B1 map,
+ *     NATOMS / natoms <= SNAPMRF_NOALLOC_MAX_B1_BLOCKS; larger requests
+ *     return SNAPMRF_ERR_INVALID (split the image into several calls);
+ *   - with a B1 map every B1 block must hold a single B1 value, as every
+ *     table built by snapmrf_trans_params does (no check is made);
+ *   - the first call on a device looks up the array's device address
+ *     (cudaGetSymbolAddress, with that device current): make that first
+ *     call before any stream capture;
+ *   - all calls on a device share the array and it keeps the previous
+ *     call's contents (each call clears what must start at zero): calls
+ *     whose device work overlaps race and give wrong maps, so issue them in
+ *     order on one stream or otherwise serialise them.
+ * Strides of 0 mean nreps. */
+int snapmrf_mrf_match_noalloc(float *d_maps, const float *d_img, size_t img_stride,
+                              const float *d_atoms, size_t atom_stride, const float *d_params,
+                              size_t nreps, size_t NATOMS, size_t natoms, size_t nvoxels,
+                              int nparams, int nmaps, const float *d_b1map, int64_t *d_index,
+                              void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -96,6 +96,8 @@ def lib() -> C.CDLL:
         L.snapmrf_normalize.argtypes = [vp, sz, sz, vp, vp]
         L.snapmrf_mrf_match.argtypes = [vp, vp, C.c_int, vp, vp, sz, sz, sz, sz, C.c_int, C.c_int,
                                         C.POINTER(MatchOpts), vp]
+        L.snapmrf_mrf_match_noalloc.argtypes = [vp, vp, sz, vp, sz, vp, sz, sz, sz, sz, C.c_int, C.c_int,
+                                                vp, vp, vp]
         _lib = L
     return _lib
 
@@ -302,3 +304,24 @@ def MRF_match(d_maps, img, d_atoms, d_params, NREPS: int, nreps: int, NATOMS: in
     _check(lib().snapmrf_mrf_match(_ptr(d_maps), _ptr(img), 1 if on_host else 0, _ptr(d_atoms),
                                    _ptr(d_params), nreps, NATOMS, natoms, nvoxels, nparams, nmaps,
                                    C.byref(opts), _stream_ptr(stream)))
+
+
+NOALLOC_MAX_VOXELS = 65536
+NOALLOC_MAX_B1_BLOCKS = 1024
+
+
+def MRF_match_noalloc(d_maps, d_img, d_atoms, d_params, NREPS: int, nreps: int, NATOMS: int,
+                      natoms: int, nvoxels: int, nparams: int = NPARAMS, nmaps: int = NMAPS,
+                      d_b1map=None, *, img_stride: int = 0, d_index=None, stream=None) -> None:
+    """MRF_match for callers that cannot allocate device memory while they
+    run (a framework whose caching allocator already holds the GPU's free
+    memory, or a reconstruction pipeline that must not allocate after
+    start-up).  Every input and output is a device buffer; the working
+    arrays come from a fixed ~1.3 MiB array the library reserves per GPU, so
+    at most NOALLOC_MAX_VOXELS voxels (and NOALLOC_MAX_B1_BLOCKS B1 blocks
+    with a B1 map) per call.  Calls share that array: do not let two calls
+    run on the GPU at the same time.  The first call on a device sets up
+    the array's address and should precede any stream capture."""
+    _check(lib().snapmrf_mrf_match_noalloc(_ptr(d_maps), _ptr(d_img), img_stride, _ptr(d_atoms), NREPS,
+                                           _ptr(d_params), nreps, NATOMS, natoms, nvoxels, nparams, nmaps,
+                                           _ptr(d_b1map), _ptr(d_index), _stream_ptr(stream)))

@@ -41,6 +41,10 @@ __device__ __forceinline__ bool beats(float s, int i, float bs, int bi) {
     return s > bs || (s == bs && i >= 0 && (bi < 0 || i < bi));
 }
 
+#ifdef SNAPMRF_MATCH_KERNEL_DECLARATION_ONLY
+// Defined once, in match.cu.
+__global__ void __launch_bounds__(kMatchThreads, 1) match_fp32_kernel(MatchArgs m);
+#else
 // One CTA: a tile of kMatchVT voxel slots of one bin against
 // atiles_per_split tiles of kMatchAT atoms of that bin.  Thread (vy, ax)
 // accumulates 4 voxels (vy + 16j) x 8 atoms (ax + 16i) complex scores
@@ -169,6 +173,8 @@ __global__ void __launch_bounds__(kMatchThreads, 1) match_fp32_kernel(MatchArgs 
         }
     }
 }
+
+#endif  // SNAPMRF_MATCH_KERNEL_DECLARATION_ONLY
 
 inline cudaError_t launch_match_fp32(const MatchArgs &m, dim3 grid, cudaStream_t st) {
     match_fp32_kernel<<<grid, kMatchThreads, 0, st>>>(m);
