@@ -68,18 +68,23 @@ def schedule(seed: int = 1) -> np.ndarray:
     return np.array([np.deg2rad(a), np.zeros(T), tr, tr / 2], np.float32)
 
 
-def grid():
+def grid(b1_blocks: int = 41):
+    """T1 / T2 / B0 / B1 grids; b1_blocks < 41 keeps the blocks nearest 1.0
+    (a reduced case of the same workload, used for profiling)."""
     t1 = np.array([100.0 * 1.05 ** k for k in range(200) if 100.0 * 1.05 ** k <= 5000.0], np.float32)
     t2 = np.array([10.0 * 1.05 ** k for k in range(200) if 10.0 * 1.05 ** k <= 2000.0], np.float32)
     b1 = np.array([0.60 + 0.02 * k for k in range(41)], np.float32)
+    if b1_blocks < 41:
+        c = 20 - b1_blocks // 2
+        b1 = b1[c:c + b1_blocks]
     return t1, t2, np.zeros(1, np.float32), b1
 
 
-def phantom(seed: int):
+def phantom(seed: int, nx: int = NX):
     """B1 map, true (T1, T2) and M0 per voxel (Fortran voxel order like the
     reference's RA images: x fastest)."""
     rng = np.random.default_rng(1000 + seed)
-    y, x = np.meshgrid(np.linspace(-1, 1, NY), np.linspace(-1, 1, NX), indexing="ij")
+    y, x = np.meshgrid(np.linspace(-1, 1, nx), np.linspace(-1, 1, nx), indexing="ij")
     b1 = np.clip(1.0 + 0.3 * (x ** 2 + y ** 2 - 0.5), 0.6, 1.4).astype(np.float32)
     tissue = np.zeros(x.shape, np.int64)
     t1v = rng.uniform(300.0, 3000.0, 5)
@@ -99,13 +104,14 @@ def phantom(seed: int):
             m0.reshape(-1), ph.reshape(-1))
 
 
-def make_inputs(snap, torch, seed: int):
+def make_inputs(snap, torch, seed: int, b1_blocks: int = 41, nx: int = NX):
     """Host inputs of one slice: (h_mrf, params, natoms, img, b1map, truth)."""
     h_mrf = schedule(1)
-    t1, t2, b0, b1 = grid()
+    t1, t2, b0, b1 = grid(b1_blocks)
     params = snap.trans_params(t1, t2, b0, b1)
     natoms = params.shape[0] // len(b1)
-    b1map, vt1, vt2, m0, ph = phantom(seed)
+    b1map, vt1, vt2, m0, ph = phantom(seed, nx)
+    b1map = np.clip(b1map, b1.min(), b1.max()).astype(np.float32)
     nvox = b1map.size
     # voxel signals: the same recursion at each voxel's own (T1, T2, B1),
     # generated on the GPU with one B1 block per voxel
@@ -220,7 +226,8 @@ def run_ours(args) -> None:
                                 device_id=torch.device("cuda", local))
     dev = torch.device("cuda", local)
 
-    h_mrf, params, natoms, img, b1map, truth = make_inputs(snap, torch, seed=rank)
+    h_mrf, params, natoms, img, b1map, truth = make_inputs(snap, torch, seed=rank,
+                                                           b1_blocks=args.b1_blocks, nx=args.nx)
     NATOMS = params.shape[0]
     nvox = img.shape[0]
     flags = snap.DICT_ALL_B1_BLOCKS | snap.DICT_NORMALIZE
@@ -274,6 +281,8 @@ def run_ours(args) -> None:
     maps = d_maps.cpu().numpy()
 
     # end to end through the public API from pinned host buffers
+    if args.no_e2e:
+        e2e_ms = float("nan")
     h_params = torch.from_numpy(params).pin_memory()
     h_img = torch.from_numpy(img.view(np.float32).reshape(nvox, T, 2)).pin_memory()
     h_b1 = torch.from_numpy(b1map).pin_memory()
@@ -287,19 +296,20 @@ def run_ours(args) -> None:
                        img_stride=T, flags=snap.MATCH_ASSUME_UNIFORM_B1)
         h_maps.copy_(d_maps, non_blocking=True)
 
-    for _ in range(max(1, args.warmup // 2)):
-        e2e_step()
-    torch.cuda.synchronize()
-    barrier()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        e2e_step()
-    e1.record(stream)
-    torch.cuda.synchronize()
-    barrier()
-    e2e_ms = e0.elapsed_time(e1)
+    if not args.no_e2e:
+        for _ in range(max(1, args.warmup // 2)):
+            e2e_step()
+        torch.cuda.synchronize()
+        barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            e2e_step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        e2e_ms = e0.elapsed_time(e1)
 
     # max over ranks
     t = torch.tensor([elapsed_ms, e2e_ms, dict_ms, match_ms], dtype=torch.float64, device=dev)
@@ -310,7 +320,7 @@ def run_ours(args) -> None:
     if rank == 0:
         ms_per_step = elapsed_ms / args.steps
         value = world * nvox / (ms_per_step / 1e3)
-        e2e_value = world * nvox / (e2e_ms / args.steps / 1e3)
+        e2e_value = world * nvox / (e2e_ms / args.steps / 1e3) if not args.no_e2e else None
         pk = peaks()
         sm_mhz = clocks.get("sm_mhz") or pk["sm_max_mhz"]
         fp32_peak = fp32_peak_tflops(pk["sm_max_mhz"])
@@ -345,7 +355,7 @@ def run_ours(args) -> None:
             "roofline": dominant, "roofline_other": other,
             "peak_note": "fp32 peak = 148 SMs x 128 lanes x 2 flop x max SM clock (nominal); "
                          f"HBM/bf16 peaks {pk['source']}",
-            "e2e": {"value": round(e2e_value, 1), "unit": "voxels/s",
+            "e2e": {"value": round(e2e_value, 1) if e2e_value else None, "unit": "voxels/s",
                     "h2d_bytes_per_step": int(params.nbytes + img.nbytes + b1map.nbytes + h_mrf.nbytes),
                     "d2h_bytes_per_step": int(nvox * 5 * 4)},
             "gpu_launches": int(launches),
@@ -353,6 +363,8 @@ def run_ours(args) -> None:
             "maps_error_vs_truth": {"t1_median_rel": round(float(np.median(e1_)), 5),
                                     "t2_median_rel": round(float(np.median(e2_)), 5)},
         }
+        if args.b1_blocks != 41 or args.nx != NX:
+            line["config"]["workload"] = f"{WORKLOAD} reduced: {NATOMS // natoms} B1 blocks, {args.nx}x{args.nx} voxels"
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(args.cpu_seconds)
         print(json.dumps(line), flush=True)
@@ -442,6 +454,10 @@ def main() -> None:
     ap.add_argument("--cpu-seconds", type=float, default=6.0,
                     help="approximate CPU seconds of the bounded CPU sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
+    ap.add_argument("--b1-blocks", type=int, default=41,
+                    help="reduced case for profiling: keep this many B1 blocks around 1.0")
+    ap.add_argument("--nx", type=int, default=NX, help="reduced case for profiling: nx x nx voxels")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":

@@ -62,11 +62,11 @@ static int parse_echo(const char *s) {
     return -1;
 }
 
-// Lanes per atom (power of two) and states per lane for w states:
+// Lanes per atom (power of two) and states per lane (<= smax) for w states:
 // least padding first, then more states per lane.
-static void choose_layout(int w, int *L, int *S) {
-    int bestL = 32, bestS = 8, bestPad = 1 << 30;
-    for (int s = kMaxStatesPerLane; s >= 1; s--)
+static void choose_layout(int w, int smax, int *L, int *S) {
+    int bestL = 32, bestS = smax, bestPad = 1 << 30;
+    for (int s = smax; s >= 1; s--)
         for (int l = 1; l <= 32; l *= 2)
             if (l * s >= w) {
                 int pad = l * s - w;
@@ -102,6 +102,39 @@ static cudaError_t dispatch_states(const EpgArgs &a, int S, dim3 grid, cudaStrea
     }
 }
 
+template <int ECHO, int S>
+static cudaError_t launch_epg_real(const EpgArgs &a, dim3 grid, cudaStream_t st) {
+    size_t smem = epg_real_smem_bytes(a.L);
+    auto k = epg_real_kernel<ECHO, S>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    k<<<grid, kEpgThreads, smem, st>>>(a);
+    note_launches(1);
+    return cudaGetLastError();
+}
+
+template <int ECHO>
+static cudaError_t dispatch_real(const EpgArgs &a, int S, dim3 grid, cudaStream_t st) {
+    switch (S) {
+    case 1: return launch_epg_real<ECHO, 1>(a, grid, st);
+    case 2: return launch_epg_real<ECHO, 2>(a, grid, st);
+    case 3: return launch_epg_real<ECHO, 3>(a, grid, st);
+    case 4: return launch_epg_real<ECHO, 4>(a, grid, st);
+    case 5: return launch_epg_real<ECHO, 5>(a, grid, st);
+    case 6: return launch_epg_real<ECHO, 6>(a, grid, st);
+    case 7: return launch_epg_real<ECHO, 7>(a, grid, st);
+    case 8: return launch_epg_real<ECHO, 8>(a, grid, st);
+    case 9: return launch_epg_real<ECHO, 9>(a, grid, st);
+    case 10: return launch_epg_real<ECHO, 10>(a, grid, st);
+    case 11: return launch_epg_real<ECHO, 11>(a, grid, st);
+    case 12: return launch_epg_real<ECHO, 12>(a, grid, st);
+    case 13: return launch_epg_real<ECHO, 13>(a, grid, st);
+    case 14: return launch_epg_real<ECHO, 14>(a, grid, st);
+    case 15: return launch_epg_real<ECHO, 15>(a, grid, st);
+    default: return launch_epg_real<ECHO, 16>(a, grid, st);
+    }
+}
+
 static cudaError_t launch_epg(int echo, const EpgArgs &a, int S, dim3 grid, cudaStream_t st) {
     switch (echo) {
     case ECHO_SSFP: return dispatch_states<ECHO_SSFP>(a, S, grid, st);
@@ -132,8 +165,8 @@ extern "C" int snapmrf_mrf_dict(float *d_atoms, const float *d_params, const flo
     if (natoms == 0 || NATOMS % natoms != 0)
         SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "MRF_dict: NATOMS (%zu) must be a multiple of natoms (%zu)",
                      NATOMS, natoms);
-    if (nstates < 1 || nstates > 32 * kMaxStatesPerLane)
-        SNAPMRF_FAIL(SNAPMRF_ERR_UNSUPPORTED, "MRF_dict: nstates must be in [1, %d]", 32 * kMaxStatesPerLane);
+    if (nstates < 1 || nstates > 32 * kMaxRealStatesPerLane)
+        SNAPMRF_FAIL(SNAPMRF_ERR_UNSUPPORTED, "MRF_dict: nstates must be in [1, %d]", 32 * kMaxRealStatesPerLane);
     unsigned flags = opts ? opts->flags : 0u;
     int n_iso = opts ? opts->n_iso : 1;
     if (n_iso < 1) n_iso = 1;
@@ -202,13 +235,29 @@ extern "C" int snapmrf_mrf_dict(float *d_atoms, const float *d_params, const flo
         SNAPMRF_CUDA(launch_roa(a, (long long)natoms, (unsigned)gen_blocks, st));
         return SNAPMRF_OK;
     }
+    // Real-valued recursion (bit-identical, half the state) when every RF
+    // phase is exactly 0 and the echo type has no off-resonance term.
+    bool real_path = !(flags & SNAPMRF_DICT_REFERENCE_ORDER) && (echo == ECHO_FISP || echo == ECHO_SR) &&
+                     nstates <= 32 * kMaxRealStatesPerLane;
+    for (size_t t = 0; real_path && t < nreps; t++)
+        if (sched[nreps + t] != 0.f) real_path = false;
+    if (!real_path && nstates > 32 * kMaxStatesPerLane)
+        SNAPMRF_FAIL(SNAPMRF_ERR_UNSUPPORTED,
+                     "MRF_dict: nstates must be in [1, %d] for this echo type and schedule "
+                     "(up to %d for epg_fisp / epg_sr with all RF phases 0)",
+                     32 * kMaxStatesPerLane, 32 * kMaxRealStatesPerLane);
     int L, S;
-    choose_layout(nstates, &L, &S);
+    choose_layout(nstates, real_path ? kMaxRealStatesPerLane : kMaxStatesPerLane, &L, &S);
     a.L = L;
     const int apc = kEpgThreads / L;
     dim3 grid((unsigned)((natoms + apc - 1) / apc), (unsigned)gen_blocks);
     if (grid.x > 0x7fffffffu) SNAPMRF_FAIL(SNAPMRF_ERR_UNSUPPORTED, "MRF_dict: grid too large");
-    SNAPMRF_CUDA(launch_epg(echo, a, S, grid, st));
+    if (real_path) {
+        SNAPMRF_CUDA(echo == ECHO_FISP ? dispatch_real<ECHO_FISP>(a, S, grid, st)
+                                       : dispatch_real<ECHO_SR>(a, S, grid, st));
+    } else {
+        SNAPMRF_CUDA(launch_epg(echo, a, S, grid, st));
+    }
     return SNAPMRF_OK;
 }
 

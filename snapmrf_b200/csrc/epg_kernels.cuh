@@ -33,10 +33,15 @@ struct EpgArgs {
 // the B0 precession phasors at TE and TR-TE for SSFP.
 __host__ __device__ constexpr int epg_nf(int echo) { return echo == ECHO_SSFP ? 8 : 4; }
 
+// Per-group strides in shared memory, padded so that the groups of a warp
+// hit different banks.
+__host__ __device__ constexpr int epg_f_stride(int echo) { return kChunk * epg_nf(echo) + 4; }
+constexpr int kReadoutStride = kChunk + 1;  // float2 per group
+
 inline size_t epg_ref_smem_bytes(int echo, int L) {
     int apc = kEpgThreads / L;
-    return (size_t)kChunk * 9 * sizeof(float2) + (size_t)apc * kChunk * epg_nf(echo) * sizeof(float) +
-           (size_t)apc * kChunk * sizeof(float2) + (size_t)apc * 3 * sizeof(float);
+    return (size_t)kChunk * 9 * sizeof(float2) + (size_t)apc * epg_f_stride(echo) * sizeof(float) +
+           (size_t)apc * kReadoutStride * sizeof(float2) + (size_t)apc * 3 * sizeof(float);
 }
 
 // RF transition matrix of fill_transition_matrix (src/functions.cu:483-508),
@@ -212,10 +217,11 @@ __global__ void __launch_bounds__(kEpgThreads) epg_ref_kernel(EpgArgs a) {
     const bool active = ab < a.natoms;
     const long long gatom = blk * a.natoms + ab;
 
+    constexpr int FS = epg_f_stride(ECHO);
     float2 *sT = reinterpret_cast<float2 *>(smem_raw);
     float *sF = reinterpret_cast<float *>(sT + kChunk * 9);
-    float2 *sR = reinterpret_cast<float2 *>(sF + apc * kChunk * NF);
-    float *sP = reinterpret_cast<float *>(sR + apc * kChunk);
+    float2 *sR = reinterpret_cast<float2 *>(sF + apc * FS);
+    float *sP = reinterpret_cast<float *>(sR + apc * kReadoutStride);
 
     for (int i = tid; i < apc; i += kEpgThreads) {
         long long at = atom0 + i;
@@ -263,7 +269,7 @@ __global__ void __launch_bounds__(kEpgThreads) epg_ref_kernel(EpgArgs a) {
             float t1 = sP[3 * ga], t2 = sP[3 * ga + 1];
             float tr = TR[t0 + i], te = TE[t0 + i];
             float ta = te, tb = tr - te;
-            float *f = sF + (ga * kChunk + i) * NF;
+            float *f = sF + ga * FS + i * NF;
             f[0] = expf(-ta / t1);
             f[1] = expf(-ta / t2);
             f[2] = expf(-tb / t1);
@@ -279,7 +285,7 @@ __global__ void __launch_bounds__(kEpgThreads) epg_ref_kernel(EpgArgs a) {
         }
         __syncthreads();
         for (int i = 0; i < nch; i++) {
-            const float *f = sF + (g * kChunk + i) * NF;
+            const float *f = sF + g * FS + i * NF;
             st_rf<S>(s, sT + 9 * i);
             if (ECHO == ECHO_SR) {
                 st_relax<S>(s, f[0], f[1], lane0);
@@ -294,7 +300,7 @@ __global__ void __launch_bounds__(kEpgThreads) epg_ref_kernel(EpgArgs a) {
             }
             if (lane0) {
                 float2 v = s.fp[0];
-                sR[g * kChunk + i] = v;
+                sR[g * kReadoutStride + i] = v;
                 nrm += v.x * v.x + v.y * v.y;
             }
             if (ECHO == ECHO_SR) {
@@ -310,7 +316,209 @@ __global__ void __launch_bounds__(kEpgThreads) epg_ref_kernel(EpgArgs a) {
         }
         __syncwarp();
         if (active)
-            for (int q = gl; q < nch; q += L) out[t0 + q] = sR[g * kChunk + q];
+            for (int q = gl; q < nch; q += L) out[t0 + q] = sR[g * kReadoutStride + q];
+    }
+    if (a.normalize || a.norms) {
+        nrm = __shfl_sync(0xffffffffu, nrm, 0, L);
+        if (a.norms && lane0 && active) a.norms[gatom] = sqrtf(nrm);
+        if (a.normalize) {
+            __syncwarp();
+            float inv = nrm;
+            if (inv > 0.f) inv = 1.f / sqrtf(inv);
+            if (active)
+                for (long long q = gl; q < nreps; q += L) out[q] = c_scale(out[q], inv);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Real-valued EPG recursion (FISP / SR with every RF phase exactly 0).
+//
+// With phi = 0 the transition matrix has real F-rows and imaginary Z-column
+// (and the converse for the Z-row), the initial state is Z = 1, and
+// relaxation, the shift and conj() preserve the form: F+ and F- stay purely
+// imaginary and Z real.  The state is then three floats per EPG state
+// (f+ = Im F+, f- = Im F-, z = Re Z) instead of six.  The nine real
+// coefficients are the entries of the same complex matrix, and the FMA
+// chains below are those of rf_row with the terms whose factors are exact
+// zeros removed, so the results are bit-identical to the complex recursion.
+// ---------------------------------------------------------------------------
+constexpr int kMaxRealStatesPerLane = 16;
+
+// c[0..8] = T0.x, T1.x, T2.y | T3.x, T4.x, T5.y | -T6.y, -T7.y, T8.x
+__device__ __forceinline__ void rf_real_coeffs(float alpha, float phi, float *c) {
+    float2 T[9];
+    rf_matrix(alpha, phi, T);
+    c[0] = T[0].x;
+    c[1] = T[1].x;
+    c[2] = T[2].y;
+    c[3] = T[3].x;
+    c[4] = T[4].x;
+    c[5] = T[5].y;
+    c[6] = -T[6].y;
+    c[7] = -T[7].y;
+    c[8] = T[8].x;
+    c[9] = c[10] = c[11] = 0.f;
+}
+
+template <int S>
+struct RealLane {
+    float fp[S], fm[S], zz[S];
+};
+
+template <int S>
+__device__ __forceinline__ void rl_rf(RealLane<S> &s, const float *c) {
+    const float4 a = reinterpret_cast<const float4 *>(c)[0];
+    const float4 b = reinterpret_cast<const float4 *>(c)[1];
+    const float r2 = c[8];
+#pragma unroll
+    for (int j = 0; j < S; j++) {
+        const float p = s.fp[j], m = s.fm[j], z = s.zz[j];
+        float np = a.x * p;
+        np = fmaf(a.y, m, np);
+        np = fmaf(a.z, z, np);
+        float nm = a.w * p;
+        nm = fmaf(b.x, m, nm);
+        nm = fmaf(b.y, z, nm);
+        float nz = b.z * p;
+        nz = fmaf(b.w, m, nz);
+        nz = fmaf(r2, z, nz);
+        s.fp[j] = np;
+        s.fm[j] = nm;
+        s.zz[j] = nz;
+    }
+}
+
+template <int S>
+__device__ __forceinline__ void rl_relax(RealLane<S> &s, float E1, float E2, bool lane0) {
+#pragma unroll
+    for (int j = 0; j < S; j++) {
+        s.fp[j] *= E2;
+        s.fm[j] *= E2;
+        s.zz[j] *= E1;
+    }
+    if (lane0) s.zz[0] = __fadd_rn(s.zz[0], 1 - E1);
+}
+
+// Shift of the real state: Im conj(F-[0]) = -f-[0].
+template <int S>
+__device__ __forceinline__ void rl_shift(RealLane<S> &s, int gl, int L, int w) {
+    const unsigned full = 0xffffffffu;
+    const float up = __shfl_up_sync(full, s.fp[S - 1], 1, L);
+    const float dn = __shfl_down_sync(full, s.fm[0], 1, L);
+#pragma unroll
+    for (int j = S - 1; j >= 1; j--) s.fp[j] = s.fp[j - 1];
+    s.fp[0] = up;
+#pragma unroll
+    for (int j = 0; j < S; j++) {
+        const int k = gl * S + j;
+        float nxt = (j < S - 1) ? s.fm[j + 1] : ((gl == L - 1) ? 0.f : dn);
+        if (k != w - 1) s.fm[j] = nxt;
+    }
+    if (gl == 0) s.fp[0] = -s.fm[0];
+#pragma unroll
+    for (int j = 0; j < S; j++) {
+        const int k = gl * S + j;
+        if (k >= w) s.fp[j] = 0.f;
+        if (k == w - 1) s.fm[j] = 0.f;
+    }
+}
+
+inline size_t epg_real_smem_bytes(int L) {
+    int apc = kEpgThreads / L;
+    return (size_t)kChunk * 12 * sizeof(float) + (size_t)apc * epg_f_stride(ECHO_FISP) * sizeof(float) +
+           (size_t)apc * kReadoutStride * sizeof(float2) + (size_t)apc * 3 * sizeof(float);
+}
+
+template <int ECHO, int S>
+__global__ void __launch_bounds__(kEpgThreads) epg_real_kernel(EpgArgs a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    constexpr int NF = 4;
+    constexpr int FS = epg_f_stride(ECHO_FISP);
+    const int L = a.L;
+    const int apc = kEpgThreads / L;
+    const int tid = threadIdx.x;
+    const int g = tid / L;
+    const int gl = tid % L;
+    const bool lane0 = (gl == 0);
+    const long long blk = blockIdx.y;
+    const long long nreps = a.nreps;
+    const long long atom0 = (long long)blockIdx.x * apc;
+    const long long ab = atom0 + g;
+    const bool active = ab < a.natoms;
+    const long long gatom = blk * a.natoms + ab;
+
+    float *sC = reinterpret_cast<float *>(smem_raw);          // [kChunk][12]
+    float *sF = sC + kChunk * 12;                              // [apc][FS]
+    float2 *sR = reinterpret_cast<float2 *>(sF + apc * FS);    // [apc][kReadoutStride]
+    float *sP = reinterpret_cast<float *>(sR + apc * kReadoutStride);
+
+    for (int i = tid; i < apc; i += kEpgThreads) {
+        long long at = atom0 + i;
+        float t1 = 1.f, t2 = 1.f;
+        if (at < a.natoms) {
+            const float *p = a.params + (blk * a.natoms + at) * a.nparams;
+            t1 = p[0];
+            t2 = p[1];
+        }
+        sP[3 * i] = t1;
+        sP[3 * i + 1] = t2;
+        sP[3 * i + 2] = 0.f;
+    }
+    __syncthreads();
+
+    const float *alpha = a.alpha + blk * nreps;
+    const float *phi = a.sched + nreps;
+    const float *TR = a.sched + 2 * nreps;
+    const float *TE = a.sched + 3 * nreps;
+    const int w = a.nstates;
+
+    // init_rf_pulse with alpha = phi = 0, TI = 0 (the expression of st_init)
+    RealLane<S> s;
+#pragma unroll
+    for (int j = 0; j < S; j++) {
+        s.fp[j] = 0.f;
+        s.fm[j] = 0.f;
+        s.zz[j] = 0.f;
+    }
+    if (lane0) {
+        const float T1 = sP[3 * g];
+        float e1 = expf(-0.f / T1), sa, ca;
+        __sincosf((float)(0.f * M_PI / 180.f), &sa, &ca);
+        s.zz[0] = e1 * ca + 1 - e1;
+    }
+
+    float nrm = 0.f;
+    float2 *out = a.atoms + gatom * nreps;
+    for (long long t0 = 0; t0 < nreps; t0 += kChunk) {
+        const int nch = (int)min((long long)kChunk, nreps - t0);
+        __syncthreads();
+        for (int i = tid; i < nch; i += kEpgThreads) rf_real_coeffs(alpha[t0 + i], phi[t0 + i], sC + 12 * i);
+        for (int idx = tid; idx < apc * nch; idx += kEpgThreads) {
+            int ga = idx / nch, i = idx - ga * nch;
+            float t1 = sP[3 * ga], t2 = sP[3 * ga + 1];
+            float tr = TR[t0 + i], te = TE[t0 + i];
+            float ta = te, tb = tr - te;
+            float4 f = make_float4(expf(-ta / t1), expf(-ta / t2), expf(-tb / t1), expf(-tb / t2));
+            *reinterpret_cast<float4 *>(sF + ga * FS + i * NF) = f;
+        }
+        __syncthreads();
+        for (int i = 0; i < nch; i++) {
+            const float4 f = *reinterpret_cast<const float4 *>(sF + g * FS + i * NF);
+            rl_rf<S>(s, sC + 12 * i);
+            rl_relax<S>(s, f.x, f.y, lane0);
+            if (lane0) {
+                const float v = s.fp[0];
+                sR[g * kReadoutStride + i] = make_float2(0.f, v);
+                // the complex path adds round(0*0 + v*v) = round(v*v)
+                nrm = __fadd_rn(nrm, __fmul_rn(v, v));
+            }
+            if (ECHO == ECHO_FISP) rl_shift<S>(s, gl, L, w);
+            rl_relax<S>(s, f.z, f.w, lane0);
+        }
+        __syncwarp();
+        if (active)
+            for (int q = gl; q < nch; q += L) out[t0 + q] = sR[g * kReadoutStride + q];
     }
     if (a.normalize || a.norms) {
         nrm = __shfl_sync(0xffffffffu, nrm, 0, L);

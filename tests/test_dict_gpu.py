@@ -162,3 +162,31 @@ def test_normalize_entry_point(snap):
     ok = ref_n > 0
     np.testing.assert_allclose(out[ok], (a[ok] / ref_n[ok, None]), rtol=1e-5, atol=1e-6)
     assert np.all(out[5] == 0)
+
+
+@pytest.mark.parametrize("echo", ["epg_fisp", "epg_sr"])
+@pytest.mark.parametrize("nstates", [1, 7, 20, 50, 101, 256])
+def test_real_path_bit_identical_to_complex_path(snap, echo, nstates):
+    """With every RF phase 0 the real-valued recursion (default) must give
+    exactly the complex recursion's atoms (SNAPMRF_DICT_REFERENCE_ORDER)."""
+    T = 300
+    h = mrf_schedule(T, seed=6)
+    params = _grid(np.geomspace(100, 4000, 10), np.geomspace(10, 1500, 8), b1s=(0.9, 1.1))
+    natoms = params.shape[0] // 2
+    flags = snap.DICT_ALL_B1_BLOCKS | snap.DICT_NORMALIZE
+    fast, n1 = run_dict(snap, echo, params, h, T, natoms=natoms, nstates=nstates, flags=flags,
+                        want_norms=True)
+    ref, n2 = run_dict(snap, echo, params, h, T, natoms=natoms, nstates=nstates,
+                       flags=flags | snap.DICT_REFERENCE_ORDER, want_norms=True)
+    assert np.array_equal(fast, ref)
+    assert np.array_equal(n1, n2)
+
+
+def test_real_path_large_state_count(snap, oracle):
+    """w up to 512 on the real path (16 states per lane x 32 lanes)."""
+    T = 120
+    h = mrf_schedule(T, seed=8)
+    params = _grid(np.geomspace(300, 3000, 4), np.geomspace(30, 300, 3))
+    got = run_dict(snap, "epg_fisp", params, h, T, nstates=400)
+    ref = oracle.dict_atoms("epg_fisp", params, h, T, nstates=400)
+    assert rel_err_per_atom(got, ref).max() < 2e-5
