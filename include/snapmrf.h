@@ -159,6 +159,15 @@ int snapmrf_normalize(float *d_atoms, size_t nreps, size_t NATOMS, float *d_norm
  * merge_maps / compute_nsplits, src/functions.cu:1317-1584).
  * ---------------------------------------------------------------------- */
 #define SNAPMRF_PREC_FP32 0  /* FP32 scores (the reference's cublasCgemm form) */
+/* BF16 scores on the tensor cores (FP32 accumulation, each voxel scaled to
+ * unit norm first), a per-voxel top-k (snapmrf_match_opts.topk, 8 or 16;
+ * 16 by default for BF16, 8 for FP16),
+ * then exact FP32 rescoring of those k atoms: the map is the FP32 first
+ * argmax among them.  Needs B1 blocks holding one B1 value each when a B1
+ * map is given. */
+#define SNAPMRF_PREC_BF16 1
+/* The same with FP16 operands (8x finer mantissa than BF16, same rate). */
+#define SNAPMRF_PREC_FP16 2
 
 /* Skip the device check that every B1 block holds one B1 value (true for
  * any params table built by trans_params); without the flag the call
@@ -173,6 +182,7 @@ typedef struct snapmrf_match_opts {
     const float *b1map;     /* optional [nvoxels] B1 map: match within the nearest B1 block */
     int b1map_on_host;      /* b1map is host memory */
     int64_t *d_index;       /* optional out [nvoxels]: chosen global atom index */
+    int topk;               /* tensor-core forms: candidates rescored in FP32, 8 or 16 (0: default) */
 } snapmrf_match_opts;
 
 /* d_maps: out, device [nvoxels][nmaps] (nmaps == 5, nparams == 4)
@@ -186,6 +196,12 @@ int snapmrf_mrf_match(float *d_maps, const float *img, int img_on_host,
                       const float *d_atoms, const float *d_params, size_t nreps,
                       size_t NATOMS, size_t natoms, size_t nvoxels, int nparams, int nmaps,
                       const snapmrf_match_opts *opts, void *stream);
+
+/* Device-side error word of the tensor-core kernels (a bounded wait that
+ * ran out sets it; the maps of that call are then NaN).  Synchronises the
+ * current device; returns 0 when no error was recorded, and clears the word
+ * when reset != 0. */
+int snapmrf_device_error(int reset);
 
 /* Largest request snapmrf_mrf_match_noalloc accepts: its working arrays live
  * in one fixed array of about 1.3 MiB per GPU (sized for 65,536 voxels and

@@ -30,6 +30,8 @@ DICT_NORMALIZE = 0x2
 DICT_REFERENCE_ORDER = 0x4
 # matching
 PREC_FP32 = 0
+PREC_BF16 = 1
+PREC_FP16 = 2
 MATCH_ASSUME_UNIFORM_B1 = 0x1
 
 ECHO_TYPES = ("epg_ssfp", "roa_ssfp", "epg_sr", "epg_se", "epg_tse1", "epg_tse2", "epg_fisp")
@@ -52,7 +54,7 @@ class DictOpts(C.Structure):
 class MatchOpts(C.Structure):
     _fields_ = [("precision", C.c_int), ("flags", C.c_uint), ("img_stride", C.c_size_t),
                 ("atom_stride", C.c_size_t), ("b1map", C.c_void_p), ("b1map_on_host", C.c_int),
-                ("d_index", C.c_void_p)]
+                ("d_index", C.c_void_p), ("topk", C.c_int)]
 
 
 class RA(C.Structure):
@@ -75,6 +77,7 @@ def lib() -> C.CDLL:
         L.snapmrf_last_error.restype = C.c_char_p
         L.snapmrf_version.restype = C.c_char_p
         L.snapmrf_kernel_launches.restype = C.c_uint64
+        L.snapmrf_device_error.argtypes = [C.c_int]
         L.snapmrf_csv_dim.restype = sz
         L.snapmrf_csv_dim.argtypes = [C.c_char_p]
         L.snapmrf_csv_read.argtypes = [vp, sz, C.c_char_p]
@@ -100,6 +103,11 @@ def lib() -> C.CDLL:
                                                 vp, vp, vp]
         _lib = L
     return _lib
+
+
+def device_error(reset: bool = False) -> int:
+    """Error word of the tensor-core kernels (0 = none); synchronises the device."""
+    return lib().snapmrf_device_error(1 if reset else 0)
 
 
 def kernel_launches() -> int:
@@ -276,7 +284,7 @@ def normalize(d_atoms, nreps: int, NATOMS: int, d_norms=None, stream=None) -> No
 def MRF_match(d_maps, img, d_atoms, d_params, NREPS: int, nreps: int, NATOMS: int, natoms: int,
               nvoxels: int, nparams: int = NPARAMS, nmaps: int = NMAPS, in_b1map=None, *,
               precision: int = PREC_FP32, flags: int = 0, img_stride: int = 0,
-              d_index=None, stream=None) -> None:
+              d_index=None, topk: int = 0, stream=None) -> None:
     """Template matching (src/functions.cu:1493-1584).
 
     img: host numpy complex64 [nvoxels][stride] or a device tensor; NREPS is
@@ -300,7 +308,7 @@ def MRF_match(d_maps, img, d_atoms, d_params, NREPS: int, nreps: int, NATOMS: in
         elif hasattr(in_b1map, "device") and in_b1map.device.type == "cpu":
             b1_host = 1
         b1 = in_b1map
-    opts = MatchOpts(precision, flags, img_stride, NREPS, _ptr(b1), b1_host, _ptr(d_index))
+    opts = MatchOpts(precision, flags, img_stride, NREPS, _ptr(b1), b1_host, _ptr(d_index), topk)
     _check(lib().snapmrf_mrf_match(_ptr(d_maps), _ptr(img), 1 if on_host else 0, _ptr(d_atoms),
                                    _ptr(d_params), nreps, NATOMS, natoms, nvoxels, nparams, nmaps,
                                    C.byref(opts), _stream_ptr(stream)))

@@ -20,6 +20,7 @@
 
 #include "common.h"
 #include "match_kernels.cuh"
+#include "match_tc.h"
 
 namespace snapmrf {
 
@@ -177,7 +178,7 @@ extern "C" int snapmrf_mrf_match(float *d_maps, const float *img, int img_on_hos
         SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "MRF_match: bad sizes (nreps %zu, nvoxels %zu, NATOMS %zu, natoms %zu)",
                      nreps, nvoxels, NATOMS, natoms);
     int precision = opts ? opts->precision : SNAPMRF_PREC_FP32;
-    if (precision != SNAPMRF_PREC_FP32)
+    if (precision != SNAPMRF_PREC_FP32 && precision != SNAPMRF_PREC_BF16 && precision != SNAPMRF_PREC_FP16)
         SNAPMRF_FAIL(SNAPMRF_ERR_UNSUPPORTED, "MRF_match: unknown precision %d", precision);
     size_t img_stride = (opts && opts->img_stride) ? opts->img_stride : nreps;
     size_t atom_stride = (opts && opts->atom_stride) ? opts->atom_stride : nreps;
@@ -228,6 +229,31 @@ extern "C" int snapmrf_mrf_match(float *d_maps, const float *img, int img_on_hos
     }
 
     const long long nvox = (long long)nvoxels;
+    if (precision == SNAPMRF_PREC_BF16 || precision == SNAPMRF_PREC_FP16) {
+        if (general)
+            SNAPMRF_FAIL(SNAPMRF_ERR_UNSUPPORTED,
+                         "MRF_match: tensor-core matching needs every B1 block to hold one B1 value");
+        TcMatchRequest q;
+        q.maps = d_maps;
+        q.index_out = (long long *)d_index;
+        q.img = d_img;
+        q.img_stride = istride;
+        q.atoms = reinterpret_cast<const float2 *>(d_atoms);
+        q.atom_stride = (long long)atom_stride;
+        q.params = d_params;
+        q.nparams = nparams;
+        q.nreps = (long long)nreps;
+        q.NATOMS = (long long)NATOMS;
+        q.natoms = (long long)natoms;
+        q.nvox = nvox;
+        q.nblocks = (int)nblocks;
+        q.b1map = d_b1;
+        q.half = precision == SNAPMRF_PREC_FP16;
+        q.topk = (opts && opts->topk) ? opts->topk : (q.half ? 8 : 16);
+        if (q.topk != 8 && q.topk != 16)
+            SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "MRF_match: topk must be 8 or 16 (got %d)", q.topk);
+        return match_bf16(q, st);
+    }
     int nbins;
     long long per_bin_atoms, nslots;
     if (!d_b1) {

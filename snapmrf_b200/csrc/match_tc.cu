@@ -1,0 +1,567 @@
+// Tensor-core matching on sm_100a: BF16 (or FP16) real-stacked scores on
+// tcgen05 with FP32 accumulation in TMEM, a per-voxel running top-k (8 or
+// 16) in the epilogue, then exact FP32 rescoring of the k candidates (the maps then follow the
+// reference's rules: first argmax of |s| among them, PD = |s|).
+//
+// Operands.  The complex score s = sum_t conj(d_t) x_t is a real GEMM over
+// K = 2T: a voxel row is its samples interleaved (Re x_t, Im x_t), and an
+// atom gives two rows, (Re d_t, Im d_t) -> Re s and (-Im d_t, Re d_t) ->
+// Im s.  D = A B^T with A = voxels (M, TMEM lanes) and B = atom rows (N, TMEM
+// columns), so each epilogue thread owns one voxel and sees the (Re s, Im s)
+// column pairs of 128 atoms per tile: the top-k update needs no cross-thread
+// reduction.
+//
+// Kernel (one persistent CTA per SM, 192 threads):
+//   warp 0     TMA producer: voxel tile (128 x 64 bf16) + atom tile
+//              (256 x 64 bf16) per K-chunk into a 4-stage ring, 128-byte
+//              swizzle;
+//   warp 1     allocates 512 TMEM columns, issues tcgen05.mma (M 128, N 256,
+//              K 16) into one of two accumulators, commits to mbarriers;
+//   warps 2-5  epilogue: tcgen05.ld of the finished accumulator, |s|^2,
+//              top-k insertion, release of the accumulator.
+// Work items are (B1 block, 128-voxel tile); each item loops over all atom
+// tiles of its block.  Every mbarrier wait is bounded (sm100.cuh) and sets a
+// device error word instead of hanging.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include <algorithm>
+#include <mutex>
+
+#include "common.h"
+#include "match_tc.h"
+#include "sm100.cuh"
+
+namespace snapmrf {
+
+// Kernels of the FP32 matching path (match.cu).
+__global__ void assign_bins_kernel(int *vox_bin, int *counts, const float *b1map, const float *params,
+                                   int nparams, long long natoms, int nblocks, long long nvox);
+__global__ void scatter_bins_kernel(long long *perm, long long *cursor, const int *vox_bin,
+                                    long long nvox);
+
+namespace tc {
+
+constexpr int BM = 128;                 // voxels per tile (TMEM lanes)
+constexpr int BA = 128;                 // atoms per tile
+constexpr int BN = 2 * BA;              // B rows per tile
+constexpr int BK = 64;                  // bf16 per 128-byte swizzled row
+constexpr int STAGES = 4;
+constexpr int A_BYTES = BM * BK * 2;    // 16 KB
+constexpr int B_BYTES = BN * BK * 2;    // 32 KB
+constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
+constexpr int TOPK_MAX = 16;
+constexpr int THREADS = 192;
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024;
+constexpr uint32_t TMEM_COLS = 512;
+
+__device__ int g_device_error;
+
+struct Args {
+    const long long *tile_start;  // [nbins + 1]
+    int nbins;
+    long long bin_natoms;
+    int nk;                       // K chunks of BK
+    uint32_t idesc;               // tcgen05 instruction descriptor
+    float *top_s;                 // [slots][TOPK]
+    int *top_i;                   // [slots][TOPK]
+    int *err;
+};
+
+__device__ __forceinline__ int find_bin(const long long *tile_start, int nbins, long long item) {
+    int lo = 0, hi = nbins - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) / 2;
+        if (tile_start[mid] <= item) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Insertion into a descending list; strict '>' keeps earlier (lower-index)
+// entries ahead of equal scores.
+template <int TOPK>
+__device__ __forceinline__ void topk_insert(float *ts, int *ti, float s, int i) {
+#pragma unroll
+    for (int k = 0; k < TOPK; k++) {
+        bool gt = s > ts[k];
+        float t = ts[k];
+        int u = ti[k];
+        ts[k] = gt ? s : t;
+        ti[k] = gt ? i : u;
+        s = gt ? t : s;
+        i = gt ? u : i;
+    }
+}
+
+template <int TOPK>
+__global__ void __launch_bounds__(THREADS, 1)
+match_bf16_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, Args p) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t full[STAGES], empty[STAGES], tfull[2], tempty[2], mma_done;
+    __shared__ uint32_t tmem_base_sh;
+    unsigned char *smem = reinterpret_cast<unsigned char *>(
+        (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    const long long total = p.tile_start[p.nbins];
+    const int natiles = (int)((p.bin_natoms + BA - 1) / BA);
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; s++) {
+            sm100::mbar_init(&full[s], 1);
+            sm100::mbar_init(&empty[s], 1);
+        }
+        for (int a = 0; a < 2; a++) {
+            sm100::mbar_init(&tfull[a], 1);
+            sm100::mbar_init(&tempty[a], 128);
+        }
+        sm100::mbar_init(&mma_done, 1);
+        sm100::fence_mbar_init();
+        sm100::prefetch_tmap(&tmA);
+        sm100::prefetch_tmap(&tmB);
+    }
+    if (warp == 1) {
+        sm100::tmem_alloc(&tmem_base_sh, TMEM_COLS);
+        sm100::tmem_relinquish();
+    }
+    sm100::tc_fence_before();
+    __syncthreads();
+    sm100::tc_fence_after();
+    const uint32_t tmem = tmem_base_sh;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            // ---------------- TMA producer ----------------
+            int stage = 0;
+            uint32_t phase = 0;
+            int issued[STAGES];
+            for (int s = 0; s < STAGES; s++) issued[s] = -1;
+            bool ok = true;
+            for (long long item = blockIdx.x; item < total && ok; item += gridDim.x) {
+                const int bin = find_bin(p.tile_start, p.nbins, item);
+                const int vrow = (int)(item * BM);
+                for (int at = 0; at < natiles && ok; at++) {
+                    const int brow = (int)(2 * ((long long)bin * p.bin_natoms + (long long)at * BA));
+                    for (int kc = 0; kc < p.nk; kc++) {
+                        if (!sm100::mbar_wait(&empty[stage], phase ^ 1, p.err, 1)) {
+                            ok = false;
+                            break;
+                        }
+                        sm100::mbar_arrive_expect_tx(&full[stage], STAGE_BYTES);
+                        unsigned char *sa = smem + stage * STAGE_BYTES;
+                        sm100::tma_load_2d(sa, &tmA, &full[stage], kc * BK, vrow);
+                        sm100::tma_load_2d(sa + A_BYTES, &tmB, &full[stage], kc * BK, brow);
+                        issued[stage] = (int)phase;
+                        if (++stage == STAGES) {
+                            stage = 0;
+                            phase ^= 1;
+                        }
+                    }
+                }
+            }
+            // every load issued must land before the CTA may exit
+            for (int s = 0; s < STAGES; s++)
+                if (issued[s] >= 0) sm100::mbar_wait(&full[s], (uint32_t)issued[s], p.err, 5);
+        }
+        __syncwarp();
+    } else if (warp == 1) {
+        if (lane == 0) {
+            // ---------------- MMA issuer ----------------
+            int stage = 0, acc = 0;
+            uint32_t phase = 0, aphase = 0;
+            bool ok = true;
+            const uint32_t idesc = p.idesc;
+            for (long long item = blockIdx.x; item < total && ok; item += gridDim.x) {
+                for (int at = 0; at < natiles && ok; at++) {
+                    if (!sm100::mbar_wait(&tempty[acc], aphase ^ 1, p.err, 2)) {
+                        ok = false;
+                        break;
+                    }
+                    sm100::tc_fence_after();
+                    const uint32_t d = tmem + (uint32_t)(acc * BN);
+                    for (int kc = 0; kc < p.nk; kc++) {
+                        if (!sm100::mbar_wait(&full[stage], phase, p.err, 3)) {
+                            ok = false;
+                            break;
+                        }
+                        sm100::tc_fence_after();
+                        const uint32_t a_addr = sm100::smem_u32(smem + stage * STAGE_BYTES);
+                        const uint32_t b_addr = a_addr + A_BYTES;
+#pragma unroll
+                        for (int k = 0; k < BK / 16; k++)
+                            sm100::mma_bf16(d, sm100::make_sw128_desc(a_addr + k * 32),
+                                            sm100::make_sw128_desc(b_addr + k * 32), idesc,
+                                            (kc > 0 || k > 0) ? 1u : 0u);
+                        sm100::mma_commit(&empty[stage]);
+                        if (++stage == STAGES) {
+                            stage = 0;
+                            phase ^= 1;
+                        }
+                    }
+                    if (!ok) break;
+                    sm100::mma_commit(&tfull[acc]);
+                    acc ^= 1;
+                    if (acc == 0) aphase ^= 1;
+                }
+            }
+            // all issued MMAs complete before TMEM is released
+            sm100::mma_commit(&mma_done);
+            sm100::mbar_wait(&mma_done, 0, p.err, 6);
+        }
+        __syncwarp();
+    } else {
+        // ---------------- epilogue ----------------
+        const int lg = warp % 4;           // TMEM lane group of this warp
+        const int row = lg * 32 + lane;    // voxel row within the tile
+        int acc = 0;
+        uint32_t aphase = 0;
+        bool ok = true;
+        for (long long item = blockIdx.x; item < total && ok; item += gridDim.x) {
+            float ts[TOPK];
+            int ti[TOPK];
+#pragma unroll
+            for (int k = 0; k < TOPK; k++) {
+                ts[k] = 0.f;
+                ti[k] = -1;
+            }
+            for (int at = 0; at < natiles; at++) {
+                // every lane polls, then the warp reconverges and agrees
+                // before the warp-collective tcgen05.ld
+                const bool got = sm100::mbar_wait(&tfull[acc], aphase, p.err, 4);
+                if (!__all_sync(0xffffffffu, got)) {
+                    ok = false;
+                    break;
+                }
+                sm100::tc_fence_after();
+                const uint32_t taddr = tmem + (uint32_t)(acc * BN) + ((uint32_t)(lg * 32) << 16);
+                const int abase = at * BA;
+                const bool full_tile = (long long)abase + BA <= p.bin_natoms;
+#pragma unroll 1
+                for (int c = 0; c < BN / 32; c++) {
+                    float v[32];
+                    sm100::tmem_ld32(taddr + c * 32, v);
+#pragma unroll
+                    for (int j = 0; j < 16; j++) {
+                        const int atom = abase + c * 16 + j;
+                        const float sc = fmaf(v[2 * j], v[2 * j], v[2 * j + 1] * v[2 * j + 1]);
+                        if (sc > ts[TOPK - 1] && (full_tile || atom < p.bin_natoms)) topk_insert<TOPK>(ts, ti, sc, atom);
+                    }
+                }
+                sm100::tc_fence_before();
+                sm100::mbar_arrive(&tempty[acc]);
+                acc ^= 1;
+                if (acc == 0) aphase ^= 1;
+            }
+            const long long slot = item * BM + row;
+#pragma unroll
+            for (int k = 0; k < TOPK_MAX; k++) {
+                p.top_s[slot * TOPK_MAX + k] = k < TOPK ? ts[k] : 0.f;
+                p.top_i[slot * TOPK_MAX + k] = k < TOPK ? ti[k] : -1;
+            }
+        }
+    }
+    __syncthreads();
+    if (warp == 1) {
+        sm100::tc_fence_after();
+        sm100::tmem_dealloc(tmem, TMEM_COLS);
+    }
+}
+
+// Padded bin layout: every B1 block's voxel slots start on a multiple of BM.
+__global__ void scan_padded_kernel(const int *counts, long long *tile_start, long long *cursor, int nbins) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    long long t = 0;
+    for (int b = 0; b < nbins; b++) {
+        tile_start[b] = t;
+        cursor[b] = t * BM;
+        t += (counts[b] + BM - 1) / BM;
+    }
+    tile_start[nbins] = t;
+}
+
+__global__ void global_bin_kernel(long long *tile_start, long long *perm, long long nvox, long long cap) {
+    long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (s == 0) {
+        tile_start[0] = 0;
+        tile_start[1] = (nvox + BM - 1) / BM;
+    }
+    if (s < cap) perm[s] = s < nvox ? s : -1;
+}
+
+// 16-bit element pairs of the two operand formats.
+template <bool HALF> struct Pair;
+template <> struct Pair<false> {
+    using T = __nv_bfloat162;
+    static __device__ __forceinline__ T make(float a, float b) { return __floats2bfloat162_rn(a, b); }
+};
+template <> struct Pair<true> {
+    using T = __half2;
+    static __device__ __forceinline__ T make(float a, float b) { return __floats2half2_rn(a, b); }
+};
+
+// A rows: voxel perm[slot] scaled to unit norm (the argmax over atoms does
+// not depend on the voxel's scale; it keeps FP16 in range), interleaved
+// (Re, Im), zero padded to Kp.  One warp per slot.
+template <bool HALF>
+__global__ void pack_voxels_kernel(void *A, const float2 *img, long long img_stride, const long long *perm,
+                                   long long nslots, long long nreps, long long Kp) {
+    using P = Pair<HALF>;
+    const long long slot = (blockIdx.x * (long long)blockDim.x + threadIdx.x) / 32;
+    const int lane = threadIdx.x % 32;
+    if (slot >= nslots) return;
+    const long long v = perm[slot];
+    const float2 *x = img + (v >= 0 ? v : 0) * img_stride;
+    float n = 0.f;
+    if (v >= 0)
+        for (long long t = lane; t < nreps; t += 32) n += x[t].x * x[t].x + x[t].y * x[t].y;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) n += __shfl_xor_sync(0xffffffffu, n, o);
+    const float inv = n > 0.f ? rsqrtf(n) : 0.f;
+    typename P::T *row = reinterpret_cast<typename P::T *>(A) + slot * (Kp / 2);
+    for (long long t = lane; t < Kp / 2; t += 32) {
+        float2 xv = make_float2(0.f, 0.f);
+        if (v >= 0 && t < nreps) xv = x[t];
+        row[t] = P::make(xv.x * inv, xv.y * inv);
+    }
+}
+
+// B rows: atom a -> row 2a (Re d, Im d) and row 2a+1 (-Im d, Re d).
+template <bool HALF>
+__global__ void pack_atoms_kernel(void *B, const float2 *atoms, long long atom_stride, long long natoms,
+                                  long long nreps, long long Kp) {
+    using P = Pair<HALF>;
+    const long long a = blockIdx.y + (long long)blockIdx.z * gridDim.y;
+    if (a >= natoms) return;
+    typename P::T *r0 = reinterpret_cast<typename P::T *>(B) + (2 * a) * (Kp / 2);
+    typename P::T *r1 = r0 + Kp / 2;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < Kp / 2; t += (long long)gridDim.x * blockDim.x) {
+        float2 d = make_float2(0.f, 0.f);
+        if (t < nreps) d = atoms[a * atom_stride + t];
+        r0[t] = P::make(d.x, d.y);
+        r1[t] = P::make(-d.y, d.x);
+    }
+}
+
+// Exact FP32 rescoring of the top-k (k <= 16) per voxel; one warp per slot.  The map
+// gets the candidate with the largest |s| (lowest atom index on ties,
+// nothing unless |s| > 0, like generate_maps' strict '>' from 0).
+__global__ void rescore_kernel(float *maps, long long *index_out, const float *top_s, const int *top_i,
+                               const long long *perm, const long long *tile_start, int nbins, const int *vox_bin,
+                               const float2 *atoms, long long atom_stride, const float2 *img, long long img_stride,
+                               long long nreps, const float *params, int nparams, long long bin_natoms,
+                               const int *err) {
+    const long long slot = (blockIdx.x * (long long)blockDim.x + threadIdx.x) / 32;
+    const int lane = threadIdx.x % 32;
+    if (slot >= tile_start[nbins] * BM) return;
+    const long long v = perm[slot];
+    if (v < 0) return;
+    const long long bin = vox_bin ? vox_bin[v] : 0;
+    int cand = lane < TOPK_MAX ? top_i[slot * TOPK_MAX + lane] : -1;
+    int ci[TOPK_MAX];
+#pragma unroll
+    for (int k = 0; k < TOPK_MAX; k++) ci[k] = __shfl_sync(0xffffffffu, cand, k);
+    float re[TOPK_MAX], im[TOPK_MAX];
+#pragma unroll
+    for (int k = 0; k < TOPK_MAX; k++) {
+        re[k] = 0.f;
+        im[k] = 0.f;
+    }
+    const float2 *x = img + v * img_stride;
+    for (long long t = lane; t < nreps; t += 32) {
+        const float2 xv = x[t];
+#pragma unroll
+        for (int k = 0; k < TOPK_MAX; k++) {
+            if (ci[k] < 0) continue;
+            const float2 d = atoms[(bin * bin_natoms + ci[k]) * atom_stride + t];
+            re[k] += d.x * xv.x + d.y * xv.y;
+            im[k] += d.x * xv.y - d.y * xv.x;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < TOPK_MAX; k++) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            re[k] += __shfl_xor_sync(0xffffffffu, re[k], o);
+            im[k] += __shfl_xor_sync(0xffffffffu, im[k], o);
+        }
+    }
+    if (lane != 0) return;
+    int best = -1;
+    float bs = 0.f, bre = 0.f, bim = 0.f;
+#pragma unroll
+    for (int k = 0; k < TOPK_MAX; k++) {
+        if (ci[k] < 0) continue;
+        const float sc = re[k] * re[k] + im[k] * im[k];
+        if (sc > bs || (sc == bs && best >= 0 && ci[k] < best)) {
+            if (sc > 0.f) {
+                bs = sc;
+                best = ci[k];
+                bre = re[k];
+                bim = im[k];
+            }
+        }
+    }
+    const long long g = bin * bin_natoms + (best >= 0 ? best : 0);
+    const float *pr = params + g * nparams;
+    float *m = maps + v * 5;
+    const bool bad = err && *err;
+    const float nanv = __int_as_float(0x7fc00000);
+    m[0] = bad ? nanv : pr[0];
+    m[1] = bad ? nanv : pr[1];
+    m[2] = bad ? nanv : pr[2];
+    m[3] = bad ? nanv : pr[3];
+    m[4] = bad ? nanv : (best >= 0 ? hypotf(bre, bim) : 0.f);
+    if (index_out) index_out[v] = bad ? -1 : g;
+}
+
+__global__ void publish_error_kernel(const int *err) {
+    if (*err) atomicCAS(&g_device_error, 0, *err);
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+
+int make_map(CUtensorMap *m, const void *base, long long rows, long long Kp, int box_rows, bool half) {
+    auto enc = encode_fn();
+    if (!enc) SNAPMRF_FAIL(SNAPMRF_ERR_CUDA, "MRF_match: cuTensorMapEncodeTiled is not available");
+    cuuint64_t dims[2] = {(cuuint64_t)Kp, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)(Kp * 2)};
+    cuuint32_t box[2] = {(cuuint32_t)BK, (cuuint32_t)box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = enc(m, half ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(base), dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) SNAPMRF_FAIL(SNAPMRF_ERR_CUDA, "MRF_match: cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return SNAPMRF_OK;
+}
+
+inline unsigned nblk(long long n, int t) { return (unsigned)((n + t - 1) / t); }
+
+}  // namespace tc
+
+int match_bf16(const TcMatchRequest &q, cudaStream_t st) {
+    using namespace tc;
+    const long long nvox = q.nvox;
+    const int nbins = q.b1map ? q.nblocks : 1;
+    const long long bin_natoms = q.b1map ? q.natoms : q.NATOMS;
+    const long long Kp = ((2 * q.nreps + BK - 1) / BK) * BK;
+    const long long cap = ((nvox + BM - 1) / BM + nbins) * BM;  // padded slots, upper bound
+    const long long brows = 2 * q.NATOMS;
+    if (cap > 0x7fffffffll || brows > 0x7fffffffll || Kp > 0x7fffffffll)
+        SNAPMRF_FAIL(SNAPMRF_ERR_UNSUPPORTED, "MRF_match: problem too large for the tensor-core path");
+
+    size_t bytes = 0;
+    auto take = [&](size_t n) {
+        size_t off = bytes;
+        bytes += (n + 255) & ~size_t(255);
+        return off;
+    };
+    const size_t oA = take((size_t)cap * Kp * 2), oB = take((size_t)brows * Kp * 2);
+    const size_t oTs = take((size_t)cap * TOPK_MAX * 4), oTi = take((size_t)cap * TOPK_MAX * 4);
+    const size_t oPerm = take((size_t)cap * 8), oTile = take((size_t)(nbins + 1) * 8);
+    const size_t oCur = take((size_t)(nbins + 1) * 8), oVb = take((size_t)nvox * 4);
+    const size_t oCnt = take((size_t)nbins * 4), oErr = take(4);
+    DeviceScratch s;
+    SNAPMRF_CUDA(s.alloc(bytes, st));
+    unsigned char *b = s.as<unsigned char>();
+    void *A = b + oA;
+    void *B = b + oB;
+    const bool half = q.half;
+    float *top_s = reinterpret_cast<float *>(b + oTs);
+    int *top_i = reinterpret_cast<int *>(b + oTi);
+    long long *perm = reinterpret_cast<long long *>(b + oPerm);
+    long long *tile_start = reinterpret_cast<long long *>(b + oTile);
+    long long *cursor = reinterpret_cast<long long *>(b + oCur);
+    int *vox_bin = reinterpret_cast<int *>(b + oVb);
+    int *counts = reinterpret_cast<int *>(b + oCnt);
+    int *err = reinterpret_cast<int *>(b + oErr);
+    SNAPMRF_CUDA(cudaMemsetAsync(err, 0, 4, st));
+
+    if (q.b1map) {
+        SNAPMRF_CUDA(cudaMemsetAsync(counts, 0, (size_t)nbins * 4, st));
+        SNAPMRF_CUDA(cudaMemsetAsync(perm, 0xff, (size_t)cap * 8, st));
+        assign_bins_kernel<<<nblk(nvox, 256), 256, 0, st>>>(vox_bin, counts, q.b1map, q.params, q.nparams,
+                                                            q.natoms, nbins, nvox);
+        SNAPMRF_LAUNCH_CHECK();
+        scan_padded_kernel<<<1, 32, 0, st>>>(counts, tile_start, cursor, nbins);
+        SNAPMRF_LAUNCH_CHECK();
+        scatter_bins_kernel<<<nblk(nvox, 256), 256, 0, st>>>(perm, cursor, vox_bin, nvox);
+        SNAPMRF_LAUNCH_CHECK();
+    } else {
+        global_bin_kernel<<<nblk(cap, 256), 256, 0, st>>>(tile_start, perm, nvox, cap);
+        SNAPMRF_LAUNCH_CHECK();
+    }
+    {
+        if (half)
+            pack_voxels_kernel<true><<<nblk(cap * 32, 256), 256, 0, st>>>(A, q.img, q.img_stride, perm, cap, q.nreps, Kp);
+        else
+            pack_voxels_kernel<false><<<nblk(cap * 32, 256), 256, 0, st>>>(A, q.img, q.img_stride, perm, cap, q.nreps, Kp);
+        SNAPMRF_LAUNCH_CHECK();
+        const int tpb = 256;
+        const long long pairs = Kp / 2;
+        dim3 g((unsigned)std::min<long long>((pairs + tpb - 1) / tpb, 64), 1, 1);
+        const long long rows = q.NATOMS;
+        g.y = (unsigned)std::min<long long>(rows, 65535);
+        g.z = (unsigned)((rows + g.y - 1) / g.y);
+        if (half)
+            pack_atoms_kernel<true><<<g, tpb, 0, st>>>(B, q.atoms, q.atom_stride, q.NATOMS, q.nreps, Kp);
+        else
+            pack_atoms_kernel<false><<<g, tpb, 0, st>>>(B, q.atoms, q.atom_stride, q.NATOMS, q.nreps, Kp);
+        SNAPMRF_LAUNCH_CHECK();
+    }
+    CUtensorMap mA, mB;
+    int rc = make_map(&mA, A, cap, Kp, BM, half);
+    if (rc) return rc;
+    rc = make_map(&mB, B, brows, Kp, BN, half);
+    if (rc) return rc;
+
+    int num_sms = 0, dev = 0;
+    SNAPMRF_CUDA(cudaGetDevice(&dev));
+    SNAPMRF_CUDA(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev));
+    auto kern = q.topk > 8 ? match_bf16_kernel<16> : match_bf16_kernel<8>;
+    SNAPMRF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
+    Args a;
+    a.tile_start = tile_start;
+    a.nbins = nbins;
+    a.bin_natoms = bin_natoms;
+    a.nk = (int)(Kp / BK);
+    a.idesc = half ? sm100::make_idesc_f16(BM, BN) : sm100::make_idesc_bf16(BM, BN);
+    a.top_s = top_s;
+    a.top_i = top_i;
+    a.err = err;
+    const long long max_items = cap / BM;
+    const unsigned grid = (unsigned)std::max<long long>(1, std::min<long long>(num_sms, max_items));
+    kern<<<grid, THREADS, SMEM_BYTES, st>>>(mA, mB, a);
+    SNAPMRF_LAUNCH_CHECK();
+    rescore_kernel<<<nblk(cap * 32, 256), 256, 0, st>>>(q.maps, q.index_out, top_s, top_i, perm, tile_start, nbins,
+                                                        q.b1map ? vox_bin : nullptr, q.atoms, q.atom_stride, q.img,
+                                                        q.img_stride, q.nreps, q.params, q.nparams, bin_natoms, err);
+    SNAPMRF_LAUNCH_CHECK();
+    publish_error_kernel<<<1, 1, 0, st>>>(err);
+    SNAPMRF_LAUNCH_CHECK();
+    return SNAPMRF_OK;
+}
+
+}  // namespace snapmrf
+
+extern "C" int snapmrf_device_error(int reset) {
+    int v = 0;
+    SNAPMRF_CUDA(cudaMemcpyFromSymbol(&v, snapmrf::tc::g_device_error, sizeof(int)));
+    if (reset) {
+        int z = 0;
+        SNAPMRF_CUDA(cudaMemcpyToSymbol(snapmrf::tc::g_device_error, &z, sizeof(int)));
+    }
+    return v;
+}

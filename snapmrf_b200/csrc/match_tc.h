@@ -1,0 +1,27 @@
+// Host interface of the tensor-core matching path (match_tc.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace snapmrf {
+
+struct TcMatchRequest {
+    float *maps;             // out [nvox][5]
+    long long *index_out;    // optional out [nvox]
+    const float2 *img;       // device [nvox][img_stride]
+    long long img_stride;
+    const float2 *atoms;     // device [NATOMS][atom_stride]
+    long long atom_stride;
+    const float *params;     // device [NATOMS][nparams]
+    int nparams;
+    long long nreps, NATOMS, natoms, nvox;
+    int nblocks;
+    const float *b1map;      // device [nvox] or null
+    bool half;               // fp16 operands instead of bf16
+    int topk;                // candidates rescored in FP32: 8 or 16
+};
+
+// BF16 / FP16 tcgen05 scores + top-k + FP32 rescoring; enqueued on st.
+int match_bf16(const TcMatchRequest &q, cudaStream_t st);
+
+}  // namespace snapmrf

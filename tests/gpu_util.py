@@ -35,7 +35,7 @@ def run_dict(snap, echo, params, h_mrf, nreps, natoms=None, nstates=101, flags=0
 
 
 def run_match(snap, img, atoms, params, nreps=None, natoms=None, b1map=None, device_img=False,
-              flags=0, b1_device=False):
+              flags=0, b1_device=False, precision=0):
     """MRF_match on the GPU; returns (maps [nvox][5], index [nvox])."""
     torch = torch_cuda()
     atoms = np.ascontiguousarray(atoms, np.complex64)
@@ -56,6 +56,6 @@ def run_match(snap, img, atoms, params, nreps=None, natoms=None, b1map=None, dev
     if b1map is not None and b1_device:
         b1 = torch.from_numpy(np.ascontiguousarray(b1map, np.float32)).cuda()
     snap.MRF_match(d_maps, src, d_atoms, d_params, T, nreps, NATOMS, natoms, nvox, in_b1map=b1,
-                   flags=flags, d_index=d_index, img_stride=img.shape[1])
+                   flags=flags, d_index=d_index, img_stride=img.shape[1], precision=precision)
     torch.cuda.synchronize()
     return d_maps.cpu().numpy(), d_index.cpu().numpy()

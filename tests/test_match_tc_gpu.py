@@ -1,0 +1,126 @@
+"""Tensor-core matching (BF16 or FP16 scores, top-16, exact FP32 rescoring)
+against the FP32 path.  Criteria:
+  - the reference's noiseless self-test recovers every parameter exactly;
+  - at least 99 % of voxels get the FP32 path's atom, and every voxel that
+    does not has an atom whose FP64 score is within 1e-3 (relative) of the
+    FP32 path's pick: the BF16 pre-selection only ever swaps near-ties;
+  - T1/T2/B0/B1 are the chosen atom's parameters; PD within 1e-5 of the
+    FP32 path's where both pick the same atom;
+  - no bounded wait ran out (snapmrf_device_error() == 0).
+"""
+import numpy as np
+import pytest
+
+from cases import MATCH_SELFTEST_INDICES, mrf_schedule
+from gpu_util import run_dict, run_match
+
+pytestmark = pytest.mark.gpu
+BF16, FP16 = 1, 2
+PRECS = pytest.mark.parametrize("prec", [BF16, FP16], ids=["bf16", "fp16"])
+
+
+def _dictionary(snap, T, b1s, nt1=14, nt2=12, seed=0):
+    h = mrf_schedule(T, seed=seed)
+    rows = [(a, b, 0.0, d) for d in b1s for b in np.geomspace(10, 800, nt2)
+            for a in np.geomspace(100, 3000, nt1) if a > b]
+    params = np.array(rows, np.float32)
+    natoms = params.shape[0] // len(b1s)
+    atoms = run_dict(snap, "epg_fisp", params, h, T, natoms=natoms, nstates=20,
+                     flags=snap.DICT_ALL_B1_BLOCKS | snap.DICT_NORMALIZE)
+    return atoms, params, natoms
+
+
+def _voxels(atoms, n, seed, snr=30.0):
+    rng = np.random.default_rng(seed)
+    s = atoms[rng.integers(0, atoms.shape[0], n)] + 0.3 * atoms[rng.integers(0, atoms.shape[0], n)]
+    s = s * (rng.uniform(0.5, 1, n) * np.exp(1j * rng.uniform(0, 2 * np.pi, n)))[:, None]
+    sig = np.linalg.norm(s, axis=1, keepdims=True) / np.sqrt(s.shape[1]) / snr
+    s = s + sig / np.sqrt(2) * (rng.standard_normal(s.shape) + 1j * rng.standard_normal(s.shape))
+    return s.astype(np.complex64)
+
+
+def compare(img, atoms, params, m32, i32, m16, i16, min_agree=0.99):
+    agree = np.mean(i16 == i32)
+    s = lambda idx: np.abs(np.einsum("vt,vt->v", np.conj(atoms[idx].astype(np.complex128)),
+                                     img.astype(np.complex128)))
+    diff = i16 != i32
+    rel = (s(i32) - s(i16)) / np.maximum(s(i32), 1e-30)
+    print(f"agreement {agree:.5f} ({diff.sum()} of {len(i32)} differ), max rel score loss "
+          f"{rel[diff].max() if diff.any() else 0:.2e}")
+    assert agree >= min_agree
+    assert np.all(rel[diff] <= 1e-3)
+    np.testing.assert_array_equal(m16[:, :4], params[i16])
+    same = ~diff & (m32[:, 4] > 0)
+    np.testing.assert_allclose(m16[same, 4], m32[same, 4], rtol=1e-5)
+
+
+@PRECS
+def test_tc_reference_selftest(snap, golden, prec):
+    """The reference's noiseless self-test dictionary (T = 100, 10 ms grid
+    steps) is nearly degenerate: the exact atom's runner-ups score 0.99997 and
+    0.99999, below BF16 resolution, so the BF16 pre-selection can miss the
+    exact atom.  Every pick must score within 1e-3 of the exact one."""
+    atoms = golden["atoms_mrf"]
+    params = golden["params_mrf"].reshape(-1, 4)
+    idx = MATCH_SELFTEST_INDICES
+    maps, got = run_match(snap, atoms[idx], atoms, params, precision=prec)
+    a = atoms.astype(np.complex128)
+    score = np.abs(np.einsum("vt,vt->v", np.conj(a[got]), a[idx]))
+    print(f"exact picks {np.sum(got == idx)} of {len(idx)}, min score {score.min():.6f}")
+    assert np.all(score >= 1 - 1e-3)
+    np.testing.assert_array_equal(maps[:, :4], params[got])
+    assert snap.device_error(reset=True) == 0
+
+
+@PRECS
+@pytest.mark.parametrize("T", [200, 1000])
+def test_tc_global_vs_fp32(snap, T, prec):
+    atoms, params, natoms = _dictionary(snap, T, (0.8, 1.0, 1.2))
+    img = _voxels(atoms, 900, 1)
+    m32, i32 = run_match(snap, img, atoms, params, natoms=natoms)
+    m16, i16 = run_match(snap, img, atoms, params, natoms=natoms, precision=prec)
+    compare(img, atoms, params, m32, i32, m16, i16)
+    assert snap.device_error(reset=True) == 0
+
+
+@PRECS
+def test_tc_b1map_vs_fp32(snap, prec):
+    b1s = np.float32([0.6, 0.75, 0.9, 1.05, 1.2, 1.35])
+    atoms, params, natoms = _dictionary(snap, 300, b1s, nt1=16, nt2=14)
+    nvox = 1500
+    img = _voxels(atoms, nvox, 2)
+    b1map = np.random.default_rng(3).uniform(0.5, 1.5, nvox).astype(np.float32)
+    b1map[:4] = [0.0, 0.675, 11.0, np.nan]
+    m32, i32 = run_match(snap, img, atoms, params, natoms=natoms, b1map=b1map)
+    m16, i16 = run_match(snap, img, atoms, params, natoms=natoms, b1map=b1map, precision=prec)
+    assert np.all(i16 // natoms == i32 // natoms)
+    compare(img, atoms, params, m32, i32, m16, i16)
+    assert snap.device_error(reset=True) == 0
+
+
+@PRECS
+def test_tc_ragged_tiles(snap, prec):
+    """Atom and voxel counts off the 128-wide tiles, K not a multiple of 64."""
+    atoms, params, natoms = _dictionary(snap, 77, (1.0,))
+    atoms, params = atoms[:131], params[:131]
+    img = _voxels(atoms, 67, 8)
+    m32, i32 = run_match(snap, img, atoms, params)
+    m16, i16 = run_match(snap, img, atoms, params, precision=prec)
+    compare(img, atoms, params, m32, i32, m16, i16, min_agree=0.97)
+    assert snap.device_error(reset=True) == 0
+
+
+@PRECS
+def test_tc_zero_nan_and_duplicate_atoms(snap, prec):
+    atoms, params, natoms = _dictionary(snap, 64, (1.0,))
+    atoms = atoms.copy()
+    atoms[7] = atoms[3]
+    img = np.zeros((5, atoms.shape[1]), np.complex64)
+    img[0] = atoms[3] * (0.5 - 0.2j)
+    img[2] = np.nan
+    img[3] = atoms[7]
+    maps, got = run_match(snap, img, atoms, params, precision=prec)
+    assert got[0] == 3 and got[3] == 3
+    assert got[1] == 0 and maps[1, 4] == 0
+    assert got[2] == 0 and maps[2, 4] == 0
+    assert snap.device_error(reset=True) == 0
