@@ -54,6 +54,10 @@ const char *snapmrf_version(void);
 /* Number of CUDA kernels this library has launched in this process (all
  * threads, all devices): an exact count for benchmarks and tests. */
 uint64_t snapmrf_kernel_launches(void);
+/* Scratch memory is taken from a per-device pool that keeps freed blocks
+ * for reuse by later calls; this returns the cached memory of the current
+ * device to the driver (it synchronises the device first). */
+int snapmrf_release_scratch(void);
 
 /* ------------------------------------------------------------------------
  * Host: schedules, grids and the parameter table.

@@ -49,6 +49,12 @@ namespace snapmrf {
 void *stage_acquire(size_t bytes);
 cudaError_t stage_release(cudaStream_t st);
 
+// The library's stream-ordered memory pool on the current device.  Its
+// release threshold is unlimited, so scratch freed by one call is reused by
+// the next instead of being returned to the driver at every synchronisation
+// (snapmrf_release_scratch trims it).
+cudaError_t device_pool(cudaMemPool_t *pool);
+
 // Stream-ordered scratch allocation that is released on scope exit.
 struct DeviceScratch {
     void *ptr = nullptr;
@@ -58,7 +64,10 @@ struct DeviceScratch {
     DeviceScratch &operator=(const DeviceScratch &) = delete;
     cudaError_t alloc(size_t bytes, cudaStream_t s) {
         stream = s;
-        return cudaMallocAsync(&ptr, bytes ? bytes : 16, s);
+        cudaMemPool_t pool;
+        cudaError_t e = device_pool(&pool);
+        if (e != cudaSuccess) return e;
+        return cudaMallocFromPoolAsync(&ptr, bytes ? bytes : 16, pool, s);
     }
     ~DeviceScratch() {
         if (ptr) cudaFreeAsync(ptr, stream);

@@ -11,6 +11,7 @@
 #include <cstring>
 
 #include <map>
+#include <mutex>
 
 #include <cuda_runtime.h>
 
@@ -42,6 +43,35 @@ void *stage_acquire(size_t bytes) {
         s.cap = want;
     }
     return s.p;
+}
+
+static std::mutex g_pool_mu;
+static std::map<int, cudaMemPool_t> g_pools;
+
+cudaError_t device_pool(cudaMemPool_t *pool) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lock(g_pool_mu);
+    auto it = g_pools.find(dev);
+    if (it != g_pools.end()) {
+        *pool = it->second;
+        return cudaSuccess;
+    }
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t p;
+    e = cudaMemPoolCreate(&p, &props);
+    if (e != cudaSuccess) return e;
+    uint64_t threshold = ~0ull;
+    e = cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &threshold);
+    if (e != cudaSuccess) return e;
+    g_pools[dev] = p;
+    *pool = p;
+    return cudaSuccess;
 }
 
 cudaError_t stage_release(cudaStream_t st) {
@@ -83,6 +113,18 @@ extern "C" const char *snapmrf_last_error(void) { return snapmrf::g_last_error.c
 extern "C" const char *snapmrf_version(void) { return "snapmrf-b200 0.1 (sm_100a)"; }
 
 extern "C" uint64_t snapmrf_kernel_launches(void) { return snapmrf::g_launches.load(); }
+
+// Returns the scratch memory cached by the library's pool on the current
+// device to the driver (after the device finishes its pending work).
+extern "C" int snapmrf_release_scratch(void) {
+    cudaMemPool_t pool;
+    cudaError_t e = snapmrf::device_pool(&pool);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaMemPoolTrimTo(pool, 0);
+    if (e != cudaSuccess)
+        return set_error(SNAPMRF_ERR_CUDA, "release_scratch: %s", cudaGetErrorString(e));
+    return SNAPMRF_OK;
+}
 
 // csv_dim (src/functions.cu:100-120): counts '\n'.  The reference reads with
 // a signed char compared against EOF, so a 0xFF byte also ends the count.
