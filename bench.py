@@ -302,9 +302,10 @@ def run_ours(args) -> None:
         dist.all_reduce(a, op=dist.ReduceOp.MIN)
         agree = {"bf16": float(a[0]), "fp16": float(a[1])}
         raw = {"bf16": float(a[2]), "fp16": float(a[3])}
-    # headline: the first tensor-core form whose argmax agrees with the FP32
+    # headline: the fastest tensor-core form whose argmax agrees with the FP32
     # form on >= 99.9 % of voxels in this very run, else the FP32 form
-    headline = next((f for f in ("bf16", "fp16") if agree[f] >= 0.999), "fp32")
+    ok = [f for f in ("bf16", "fp16") if agree[f] >= 0.999]
+    headline = min(ok, key=lambda f: forms[f]["elapsed_ms"]) if ok else "fp32"
     prec = PRECS[headline]
     hf = forms[headline]
     clocks, launches, elapsed_ms = hf["clocks"], hf["launches"], hf["elapsed_ms"]

@@ -62,11 +62,11 @@ static int parse_echo(const char *s) {
     return -1;
 }
 
-// Lanes per atom (power of two) and states per lane (<= smax) for w states:
-// least padding first, then more states per lane.
-static void choose_layout(int w, int smax, int *L, int *S) {
+// Lanes per atom (power of two) and states per lane (<= smax, a multiple of
+// `step`) for w states: least padding first, then more states per lane.
+static void choose_layout(int w, int smax, int step, int *L, int *S) {
     int bestL = 32, bestS = smax, bestPad = 1 << 30;
-    for (int s = smax; s >= 1; s--)
+    for (int s = smax; s >= step; s -= step)
         for (int l = 1; l <= 32; l *= 2)
             if (l * s >= w) {
                 int pad = l * s - w;
@@ -113,9 +113,10 @@ static cudaError_t launch_epg_real(const EpgArgs &a, dim3 grid, cudaStream_t st)
     return cudaGetLastError();
 }
 
+// P = pairs of states per lane (S = 2P).
 template <int ECHO>
-static cudaError_t dispatch_real(const EpgArgs &a, int S, dim3 grid, cudaStream_t st) {
-    switch (S) {
+static cudaError_t dispatch_real(const EpgArgs &a, int P, dim3 grid, cudaStream_t st) {
+    switch (P) {
     case 1: return launch_epg_real<ECHO, 1>(a, grid, st);
     case 2: return launch_epg_real<ECHO, 2>(a, grid, st);
     case 3: return launch_epg_real<ECHO, 3>(a, grid, st);
@@ -247,14 +248,17 @@ extern "C" int snapmrf_mrf_dict(float *d_atoms, const float *d_params, const flo
                      "(up to %d for epg_fisp / epg_sr with all RF phases 0)",
                      32 * kMaxStatesPerLane, 32 * kMaxRealStatesPerLane);
     int L, S;
-    choose_layout(nstates, real_path ? kMaxRealStatesPerLane : kMaxStatesPerLane, &L, &S);
+    if (real_path)
+        choose_layout(nstates, kMaxRealStatesPerLane, 2, &L, &S);
+    else
+        choose_layout(nstates, kMaxStatesPerLane, 1, &L, &S);
     a.L = L;
     const int apc = kEpgThreads / L;
     dim3 grid((unsigned)((natoms + apc - 1) / apc), (unsigned)gen_blocks);
     if (grid.x > 0x7fffffffu) SNAPMRF_FAIL(SNAPMRF_ERR_UNSUPPORTED, "MRF_dict: grid too large");
     if (real_path) {
-        SNAPMRF_CUDA(echo == ECHO_FISP ? dispatch_real<ECHO_FISP>(a, S, grid, st)
-                                       : dispatch_real<ECHO_SR>(a, S, grid, st));
+        SNAPMRF_CUDA(echo == ECHO_FISP ? dispatch_real<ECHO_FISP>(a, S / 2, grid, st)
+                                       : dispatch_real<ECHO_SR>(a, S / 2, grid, st));
     } else {
         SNAPMRF_CUDA(launch_epg(echo, a, S, grid, st));
     }

@@ -343,94 +343,96 @@ __global__ void __launch_bounds__(kEpgThreads) epg_ref_kernel(EpgArgs a) {
 // chains below are those of rf_row with the terms whose factors are exact
 // zeros removed, so the results are bit-identical to the complex recursion.
 // ---------------------------------------------------------------------------
-constexpr int kMaxRealStatesPerLane = 16;
+constexpr int kMaxRealStatesPerLane = 32;  // even: states are processed in pairs
 
-// c[0..8] = T0.x, T1.x, T2.y | T3.x, T4.x, T5.y | -T6.y, -T7.y, T8.x
-__device__ __forceinline__ void rf_real_coeffs(float alpha, float phi, float *c) {
+// Coefficient pairs (c, c) of the real recursion for one step, in the order
+// T0.x, T1.x, T2.y | T3.x, T4.x, T5.y | -T6.y, -T7.y, T8.x (float2 each).
+__device__ __forceinline__ void rf_real_coeffs2(float alpha, float phi, float2 *c) {
     float2 T[9];
     rf_matrix(alpha, phi, T);
-    c[0] = T[0].x;
-    c[1] = T[1].x;
-    c[2] = T[2].y;
-    c[3] = T[3].x;
-    c[4] = T[4].x;
-    c[5] = T[5].y;
-    c[6] = -T[6].y;
-    c[7] = -T[7].y;
-    c[8] = T[8].x;
-    c[9] = c[10] = c[11] = 0.f;
+    const float v[9] = {T[0].x, T[1].x, T[2].y, T[3].x, T[4].x, T[5].y, -T[6].y, -T[7].y, T[8].x};
+#pragma unroll
+    for (int i = 0; i < 9; i++) c[i] = make_float2(v[i], v[i]);
+    c[9] = make_float2(0.f, 0.f);
 }
 
-template <int S>
-struct RealLane {
-    float fp[S], fm[S], zz[S];
+// P pairs of EPG states per lane: slot j = 2i + h of pair i is state
+// k = gl * 2P + j.  Packed two-wide FP32 instructions (__ffma2_rn /
+// __fmul2_rn) perform per element exactly the scalar operations of the
+// complex recursion with its zero terms removed.
+template <int P>
+struct RealLane2 {
+    float2 fp[P], fm[P], zz[P];
 };
 
-template <int S>
-__device__ __forceinline__ void rl_rf(RealLane<S> &s, const float *c) {
-    const float4 a = reinterpret_cast<const float4 *>(c)[0];
-    const float4 b = reinterpret_cast<const float4 *>(c)[1];
-    const float r2 = c[8];
+template <int P>
+__device__ __forceinline__ void rl2_rf(RealLane2<P> &s, const float2 *c) {
+    const float2 c0 = c[0], c1 = c[1], c2 = c[2], c3 = c[3], c4 = c[4], c5 = c[5], c6 = c[6], c7 = c[7],
+                 c8 = c[8];
 #pragma unroll
-    for (int j = 0; j < S; j++) {
-        const float p = s.fp[j], m = s.fm[j], z = s.zz[j];
-        float np = a.x * p;
-        np = fmaf(a.y, m, np);
-        np = fmaf(a.z, z, np);
-        float nm = a.w * p;
-        nm = fmaf(b.x, m, nm);
-        nm = fmaf(b.y, z, nm);
-        float nz = b.z * p;
-        nz = fmaf(b.w, m, nz);
-        nz = fmaf(r2, z, nz);
-        s.fp[j] = np;
-        s.fm[j] = nm;
-        s.zz[j] = nz;
+    for (int i = 0; i < P; i++) {
+        const float2 p = s.fp[i], m = s.fm[i], z = s.zz[i];
+        float2 np = __fmul2_rn(c0, p);
+        np = __ffma2_rn(c1, m, np);
+        np = __ffma2_rn(c2, z, np);
+        float2 nm = __fmul2_rn(c3, p);
+        nm = __ffma2_rn(c4, m, nm);
+        nm = __ffma2_rn(c5, z, nm);
+        float2 nz = __fmul2_rn(c6, p);
+        nz = __ffma2_rn(c7, m, nz);
+        nz = __ffma2_rn(c8, z, nz);
+        s.fp[i] = np;
+        s.fm[i] = nm;
+        s.zz[i] = nz;
     }
 }
 
-template <int S>
-__device__ __forceinline__ void rl_relax(RealLane<S> &s, float E1, float E2, bool lane0) {
+// e = (E2, E1) of one interval: F+- *= E2, Z *= E1, then Z0 += 1 - E1.
+template <int P>
+__device__ __forceinline__ void rl2_relax(RealLane2<P> &s, float E1, float E2, bool lane0) {
+    const float2 e2 = make_float2(E2, E2), e1 = make_float2(E1, E1);
 #pragma unroll
-    for (int j = 0; j < S; j++) {
-        s.fp[j] *= E2;
-        s.fm[j] *= E2;
-        s.zz[j] *= E1;
+    for (int i = 0; i < P; i++) {
+        s.fp[i] = __fmul2_rn(s.fp[i], e2);
+        s.fm[i] = __fmul2_rn(s.fm[i], e2);
+        s.zz[i] = __fmul2_rn(s.zz[i], e1);
     }
-    if (lane0) s.zz[0] = __fadd_rn(s.zz[0], 1 - E1);
+    if (lane0) s.zz[0].x = __fadd_rn(s.zz[0].x, 1 - E1);
 }
 
-// Shift of the real state: Im conj(F-[0]) = -f-[0].
-template <int S>
-__device__ __forceinline__ void rl_shift(RealLane<S> &s, int gl, int L, int w) {
+// Gradient shift of the paired real state (see st_shift): F+ up one slot,
+// F- down one slot, f+[0] = -f-[0] (Im of conj), F-[w-1] = 0, slots k >= w
+// zero; with w = 1 the unshifted f-[0] is used.
+template <int P>
+__device__ __forceinline__ void rl2_shift(RealLane2<P> &s, int gl, int L, int w) {
     const unsigned full = 0xffffffffu;
-    const float up = __shfl_up_sync(full, s.fp[S - 1], 1, L);
-    const float dn = __shfl_down_sync(full, s.fm[0], 1, L);
+    const float up = __shfl_up_sync(full, s.fp[P - 1].y, 1, L);
+    const float dn = __shfl_down_sync(full, s.fm[0].x, 1, L);
+    const float old_fm0 = s.fm[0].x;
 #pragma unroll
-    for (int j = S - 1; j >= 1; j--) s.fp[j] = s.fp[j - 1];
-    s.fp[0] = up;
+    for (int i = P - 1; i >= 1; i--) s.fp[i] = make_float2(s.fp[i - 1].y, s.fp[i].x);
+    s.fp[0] = make_float2(up, s.fp[0].x);
 #pragma unroll
-    for (int j = 0; j < S; j++) {
-        const int k = gl * S + j;
-        float nxt = (j < S - 1) ? s.fm[j + 1] : ((gl == L - 1) ? 0.f : dn);
-        if (k != w - 1) s.fm[j] = nxt;
-    }
-    if (gl == 0) s.fp[0] = -s.fm[0];
+    for (int i = 0; i < P - 1; i++) s.fm[i] = make_float2(s.fm[i].y, s.fm[i + 1].x);
+    s.fm[P - 1] = make_float2(s.fm[P - 1].y, (gl == L - 1) ? 0.f : dn);
+    if (gl == 0) s.fp[0].x = -((w == 1) ? old_fm0 : s.fm[0].x);
+    const int k0 = gl * 2 * P;
 #pragma unroll
-    for (int j = 0; j < S; j++) {
-        const int k = gl * S + j;
-        if (k >= w) s.fp[j] = 0.f;
-        if (k == w - 1) s.fm[j] = 0.f;
+    for (int i = 0; i < P; i++) {
+        if (k0 + 2 * i >= w) s.fp[i].x = 0.f;
+        if (k0 + 2 * i + 1 >= w) s.fp[i].y = 0.f;
+        if (k0 + 2 * i == w - 1) s.fm[i].x = 0.f;
+        if (k0 + 2 * i + 1 == w - 1) s.fm[i].y = 0.f;
     }
 }
 
 inline size_t epg_real_smem_bytes(int L) {
     int apc = kEpgThreads / L;
-    return (size_t)kChunk * 12 * sizeof(float) + (size_t)apc * epg_f_stride(ECHO_FISP) * sizeof(float) +
+    return (size_t)kChunk * 10 * sizeof(float2) + (size_t)apc * epg_f_stride(ECHO_FISP) * sizeof(float) +
            (size_t)apc * kReadoutStride * sizeof(float2) + (size_t)apc * 3 * sizeof(float);
 }
 
-template <int ECHO, int S>
+template <int ECHO, int P>
 __global__ void __launch_bounds__(kEpgThreads) epg_real_kernel(EpgArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr int NF = 4;
@@ -448,8 +450,8 @@ __global__ void __launch_bounds__(kEpgThreads) epg_real_kernel(EpgArgs a) {
     const bool active = ab < a.natoms;
     const long long gatom = blk * a.natoms + ab;
 
-    float *sC = reinterpret_cast<float *>(smem_raw);          // [kChunk][12]
-    float *sF = sC + kChunk * 12;                              // [apc][FS]
+    float2 *sC = reinterpret_cast<float2 *>(smem_raw);        // [kChunk][10]
+    float *sF = reinterpret_cast<float *>(sC + kChunk * 10);   // [apc][FS]
     float2 *sR = reinterpret_cast<float2 *>(sF + apc * FS);    // [apc][kReadoutStride]
     float *sP = reinterpret_cast<float *>(sR + apc * kReadoutStride);
 
@@ -474,18 +476,18 @@ __global__ void __launch_bounds__(kEpgThreads) epg_real_kernel(EpgArgs a) {
     const int w = a.nstates;
 
     // init_rf_pulse with alpha = phi = 0, TI = 0 (the expression of st_init)
-    RealLane<S> s;
+    RealLane2<P> s;
 #pragma unroll
-    for (int j = 0; j < S; j++) {
-        s.fp[j] = 0.f;
-        s.fm[j] = 0.f;
-        s.zz[j] = 0.f;
+    for (int i = 0; i < P; i++) {
+        s.fp[i] = make_float2(0.f, 0.f);
+        s.fm[i] = make_float2(0.f, 0.f);
+        s.zz[i] = make_float2(0.f, 0.f);
     }
     if (lane0) {
         const float T1 = sP[3 * g];
         float e1 = expf(-0.f / T1), sa, ca;
         __sincosf((float)(0.f * M_PI / 180.f), &sa, &ca);
-        s.zz[0] = e1 * ca + 1 - e1;
+        s.zz[0].x = e1 * ca + 1 - e1;
     }
 
     float nrm = 0.f;
@@ -493,7 +495,7 @@ __global__ void __launch_bounds__(kEpgThreads) epg_real_kernel(EpgArgs a) {
     for (long long t0 = 0; t0 < nreps; t0 += kChunk) {
         const int nch = (int)min((long long)kChunk, nreps - t0);
         __syncthreads();
-        for (int i = tid; i < nch; i += kEpgThreads) rf_real_coeffs(alpha[t0 + i], phi[t0 + i], sC + 12 * i);
+        for (int i = tid; i < nch; i += kEpgThreads) rf_real_coeffs2(alpha[t0 + i], phi[t0 + i], sC + 10 * i);
         for (int idx = tid; idx < apc * nch; idx += kEpgThreads) {
             int ga = idx / nch, i = idx - ga * nch;
             float t1 = sP[3 * ga], t2 = sP[3 * ga + 1];
@@ -505,16 +507,16 @@ __global__ void __launch_bounds__(kEpgThreads) epg_real_kernel(EpgArgs a) {
         __syncthreads();
         for (int i = 0; i < nch; i++) {
             const float4 f = *reinterpret_cast<const float4 *>(sF + g * FS + i * NF);
-            rl_rf<S>(s, sC + 12 * i);
-            rl_relax<S>(s, f.x, f.y, lane0);
+            rl2_rf<P>(s, sC + 10 * i);
+            rl2_relax<P>(s, f.x, f.y, lane0);
             if (lane0) {
-                const float v = s.fp[0];
+                const float v = s.fp[0].x;
                 sR[g * kReadoutStride + i] = make_float2(0.f, v);
                 // the complex path adds round(0*0 + v*v) = round(v*v)
                 nrm = __fadd_rn(nrm, __fmul_rn(v, v));
             }
-            if (ECHO == ECHO_FISP) rl_shift<S>(s, gl, L, w);
-            rl_relax<S>(s, f.z, f.w, lane0);
+            if (ECHO == ECHO_FISP) rl2_shift<P>(s, gl, L, w);
+            rl2_relax<P>(s, f.z, f.w, lane0);
         }
         __syncwarp();
         if (active)

@@ -327,20 +327,30 @@ __global__ void pack_voxels_kernel(void *A, const float2 *img, long long img_str
     }
 }
 
-// B rows: atom a -> row 2a (Re d, Im d) and row 2a+1 (-Im d, Re d).
+// B rows: atom a -> row 2a (Re d, Im d) and row 2a+1 (-Im d, Re d).  One
+// warp per atom, four samples per lane and step (16-byte stores).
 template <bool HALF>
 __global__ void pack_atoms_kernel(void *B, const float2 *atoms, long long atom_stride, long long natoms,
                                   long long nreps, long long Kp) {
     using P = Pair<HALF>;
-    const long long a = blockIdx.y + (long long)blockIdx.z * gridDim.y;
+    const long long a = (blockIdx.x * (long long)blockDim.x + threadIdx.x) / 32;
+    const int lane = threadIdx.x % 32;
     if (a >= natoms) return;
     typename P::T *r0 = reinterpret_cast<typename P::T *>(B) + (2 * a) * (Kp / 2);
     typename P::T *r1 = r0 + Kp / 2;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < Kp / 2; t += (long long)gridDim.x * blockDim.x) {
-        float2 d = make_float2(0.f, 0.f);
-        if (t < nreps) d = atoms[a * atom_stride + t];
-        r0[t] = P::make(d.x, d.y);
-        r1[t] = P::make(-d.y, d.x);
+    const float2 *src = atoms + a * atom_stride;
+    for (long long t = 4 * lane; t < Kp / 2; t += 128) {
+        uint32_t o0[4], o1[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            float2 d = make_float2(0.f, 0.f);
+            if (t + u < nreps) d = src[t + u];
+            typename P::T x0 = P::make(d.x, d.y), x1 = P::make(-d.y, d.x);
+            o0[u] = *reinterpret_cast<const uint32_t *>(&x0);
+            o1[u] = *reinterpret_cast<const uint32_t *>(&x1);
+        }
+        *reinterpret_cast<uint4 *>(r0 + t) = make_uint4(o0[0], o0[1], o0[2], o0[3]);
+        *reinterpret_cast<uint4 *>(r1 + t) = make_uint4(o1[0], o1[1], o1[2], o1[3]);
     }
 }
 
@@ -509,16 +519,14 @@ int match_bf16(const TcMatchRequest &q, cudaStream_t st) {
         else
             pack_voxels_kernel<false><<<nblk(cap * 32, 256), 256, 0, st>>>(A, q.img, q.img_stride, perm, cap, q.nreps, Kp);
         SNAPMRF_LAUNCH_CHECK();
-        const int tpb = 256;
-        const long long pairs = Kp / 2;
-        dim3 g((unsigned)std::min<long long>((pairs + tpb - 1) / tpb, 64), 1, 1);
-        const long long rows = q.NATOMS;
-        g.y = (unsigned)std::min<long long>(rows, 65535);
-        g.z = (unsigned)((rows + g.y - 1) / g.y);
+        // Kp is a multiple of 64, so every 4-pair group of a row is whole and
+        // 16-byte aligned (row pitch Kp * 2 bytes)
         if (half)
-            pack_atoms_kernel<true><<<g, tpb, 0, st>>>(B, q.atoms, q.atom_stride, q.NATOMS, q.nreps, Kp);
+            pack_atoms_kernel<true><<<nblk(q.NATOMS * 32, 256), 256, 0, st>>>(B, q.atoms, q.atom_stride, q.NATOMS,
+                                                                                q.nreps, Kp);
         else
-            pack_atoms_kernel<false><<<g, tpb, 0, st>>>(B, q.atoms, q.atom_stride, q.NATOMS, q.nreps, Kp);
+            pack_atoms_kernel<false><<<nblk(q.NATOMS * 32, 256), 256, 0, st>>>(B, q.atoms, q.atom_stride, q.NATOMS,
+                                                                                 q.nreps, Kp);
         SNAPMRF_LAUNCH_CHECK();
     }
     CUtensorMap mA, mB;
