@@ -34,7 +34,7 @@ def nvcc() -> str:
 
 
 def _deps(src: Path) -> list[Path]:
-    deps = [src] + sorted(CSRC.glob("*.h")) + sorted(CSRC.glob("*.cuh")) + [ROOT / "include" / "snapmrf.h"]
+    deps = [src] + sorted(CSRC.glob("*.h")) + sorted(CSRC.glob("*.cuh")) + sorted((ROOT / "include").glob("*.h"))
     return [d for d in deps if d.exists()]
 
 
@@ -62,19 +62,37 @@ def _compile(src: str, verbose: bool, extra: list[str]) -> Path:
     return obj
 
 
+COMPAT_LIB = PKG / "libsnapmrf_compat.so"
+CLI = PKG / "mrf"
+RPATH = ["-Xlinker", "-rpath", "-Xlinker", "$ORIGIN"]
+
+
+def _link(target: Path, objs: list[Path], extra: list[str]) -> None:
+    if not _stale(target, objs + ([LIB] if target != LIB else [])):
+        return
+    tmp = target.with_name(target.name + ".tmp")
+    cmd = [nvcc()] + ARCH + extra + ["-o", str(tmp)] + [str(o) for o in objs]
+    if target != LIB:
+        cmd += [f"-L{PKG}", "-lsnapmrf"] + RPATH
+    cmd += ["-lcudart"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"link of {target.name} failed:\n{r.stdout}\n{r.stderr}")
+    os.replace(tmp, target)
+
+
 def build(verbose: bool = False, extra: list[str] | None = None) -> Path:
-    """Compiles every CUDA/C++ source and links libsnapmrf.so; returns its path."""
+    """Compiles every CUDA/C++ source, links libsnapmrf.so, the functions.h
+    compatibility library libsnapmrf_compat.so and the mrf CLI; returns the
+    path of libsnapmrf.so."""
     BUILD.mkdir(exist_ok=True)
     extra = list(extra or [])
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 2)) as ex:
-        objs = list(ex.map(lambda s: _compile(s, verbose, extra), SOURCES))
-    if _stale(LIB, objs):
-        tmp = LIB.with_suffix(".so.tmp")
-        cmd = [nvcc()] + ARCH + ["-shared", "-o", str(tmp)] + [str(o) for o in objs] + ["-lcudart"]
-        r = subprocess.run(cmd, capture_output=True, text=True)
-        if r.returncode != 0:
-            raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
-        os.replace(tmp, LIB)
+        objs = list(ex.map(lambda s: _compile(s, verbose, extra), SOURCES + ["compat.cpp", "mrf_cli.cpp"]))
+    core, compat_o, cli_o = objs[:len(SOURCES)], objs[-2], objs[-1]
+    _link(LIB, core, ["-shared"])
+    _link(COMPAT_LIB, [compat_o], ["-shared"])
+    _link(CLI, [cli_o], [])
     return LIB
 
 

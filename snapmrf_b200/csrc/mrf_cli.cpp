@@ -1,0 +1,257 @@
+// mrf: the command-line driver of the reference (src/mrf.cu:34-386) on the
+// C ABI.  Same flags, positional arguments, defaults and outputs:
+//
+//   mrf [OPTION] <rfpulse.csv> <imgstack.ra>
+//     -M/--b1map RA   -N n (logspace grids)   -a/--atoms RA   -m/--map RA
+//     -p/--params RA  -t/--T1 -s/--T2 -b/--B0 -r/--B1 grids
+//     -w/--nstates n  -e/--echo_type name     -T/--nreps n
+//     -G/--gridsize, -B/--blocksize (accepted, unused)  -h/--help
+// The usage text's spellings --maps, --states and --timepoints are accepted
+// too.  Additive options: --precision fp32|bf16|fp16, --topk 8|16,
+// --all-b1-blocks (non-SSFP echo types over every B1 block), --normalize.
+// Times are wall-clock (CUDA events), not the reference's CPU clock().
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <err.h>
+#include <getopt.h>
+#include <sysexits.h>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "snapmrf.h"
+
+static void check(int rc, const char *what) {
+    if (rc) errx(rc == SNAPMRF_ERR_ECHO_TYPE ? EX_USAGE : EX_SOFTWARE, "%s: %s", what, snapmrf_last_error());
+}
+
+static void cuda_check(cudaError_t e, const char *what) {
+    if (e != cudaSuccess) errx(EX_SOFTWARE, "%s: %s", what, cudaGetErrorString(e));
+}
+
+static void usage() {
+    fprintf(stderr,
+            "MR fingerprinting dictionary generator and image reconstructor\n"
+            "Usage: mrf [OPTION] <rfpulse.csv> <imgstack.ra>\n"
+            "\t-M, --b1map <rafile>\t\t B1 map input RA file\n"
+            "\t-N n\t\t\t\t number of atoms (hard-coded logspace grids)\n"
+            "\t-a, --atoms <rafile>\t\t dictionary atoms output RA file\n"
+            "\t-m, --map, --maps <rafile>\t parameter map output RA file\n"
+            "\t-p, --params <rafile>\t\t dictionary parameters output RA file\n"
+            "\t-t, --T1 start:step:end\t\t T1 grid\n"
+            "\t-s, --T2 start:step:end\t\t T2 grid\n"
+            "\t-b, --B0 start:step:end\t\t B0 grid\n"
+            "\t-r, --B1 start:step:end\t\t B1 grid\n"
+            "\t-w, --nstates, --states n\t number of EPG states\n"
+            "\t-e, --echo_type name\t\t echo type (epg_ssfp, roa_ssfp, epg_sr, epg_se,\n"
+            "\t\t\t\t\t epg_tse1, epg_tse2, epg_fisp)\n"
+            "\t-T, --nreps, --timepoints n\t number of time points\n"
+            "\t-G, --gridsize n, -B, --blocksize n  accepted, unused\n"
+            "\t    --precision fp32|bf16|fp16\t matching form (default fp32)\n"
+            "\t    --topk 8|16\t\t\t candidates rescored in FP32 (tensor-core forms)\n"
+            "\t    --all-b1-blocks\t\t generate every B1 block for non-SSFP echo types\n"
+            "\t    --normalize\t\t\t unit-norm every atom\n"
+            "\t-h, --help\t\t\t show this help\n");
+}
+
+static std::vector<float> grid_values(const char *s) {
+    size_t n = snapmrf_parse_length(s);
+    if (n == 0) errx(EX_USAGE, "bad grid '%s': %s", s, snapmrf_last_error());
+    std::vector<float> v(n);
+    check(snapmrf_parse_params(v.data(), s, n), "parse_params");
+    return v;
+}
+
+static void save_ra(const void *data, uint64_t eltype, uint64_t elbyte, const char *path, uint64_t d0, uint64_t d1) {
+    uint64_t dims[2] = {d0, d1};
+    snapmrf_ra a;
+    a.flags = 0;
+    a.eltype = eltype;
+    a.elbyte = elbyte;
+    a.size = d0 * d1 * elbyte;
+    a.ndims = 2;
+    a.dims = dims;
+    a.data = (uint8_t *)data;
+    check(snapmrf_ra_write(&a, path), "ra_write");
+}
+
+int main(int argc, char **argv) {
+    const char *in_mrf = "../data/MRF001.csv", *in_img = NULL, *in_b1map = NULL;
+    const char *out_maps = NULL, *out_atoms = NULL, *out_params = NULL;
+    const char *T1 = "20:20:3000", *T2 = "20:10:1000", *B0 = "0", *B1 = "1", *echo_type = "epg_ssfp";
+    int nparams = 4, nmaps = 5, nstates = 101;
+    size_t nreps = 1500, NATOMS_req = 0;
+    int precision = SNAPMRF_PREC_FP32, topk = 0;
+    unsigned dict_flags = 0;
+    enum { OPT_PREC = 1000, OPT_TOPK, OPT_ALLB1, OPT_NORM };
+    static struct option longopts[] = {
+        {"b1map", 1, NULL, 'M'},      {"atoms", 1, NULL, 'a'},       {"map", 1, NULL, 'm'},
+        {"maps", 1, NULL, 'm'},       {"params", 1, NULL, 'p'},      {"T1", 1, NULL, 't'},
+        {"T2", 1, NULL, 's'},         {"B0", 1, NULL, 'b'},          {"B1", 1, NULL, 'r'},
+        {"nstates", 1, NULL, 'w'},    {"states", 1, NULL, 'w'},      {"echo_type", 1, NULL, 'e'},
+        {"nreps", 1, NULL, 'T'},      {"timepoints", 1, NULL, 'T'},  {"gridsize", 1, NULL, 'G'},
+        {"blocksize", 1, NULL, 'B'},  {"NATOMS", 1, NULL, 'N'},      {"help", 0, NULL, 'h'},
+        {"precision", 1, NULL, OPT_PREC}, {"topk", 1, NULL, OPT_TOPK},
+        {"all-b1-blocks", 0, NULL, OPT_ALLB1}, {"normalize", 0, NULL, OPT_NORM}, {NULL, 0, NULL, 0}};
+    opterr = 0;
+    int c;
+    while ((c = getopt_long(argc, argv, "M:N:a:m:p:t:s:b:r:w:e:T:G:B:h", longopts, NULL)) != -1) {
+        switch (c) {
+        case 'M': in_b1map = optarg; break;
+        case 'N': NATOMS_req = (size_t)atoi(optarg); break;
+        case 'a': out_atoms = optarg; break;
+        case 'm': out_maps = optarg; break;
+        case 'p': out_params = optarg; break;
+        case 't': T1 = optarg; break;
+        case 's': T2 = optarg; break;
+        case 'b': B0 = optarg; break;
+        case 'r': B1 = optarg; break;
+        case 'w': nstates = atoi(optarg); break;
+        case 'e': echo_type = optarg; break;
+        case 'T': nreps = (size_t)atoi(optarg); break;
+        case 'G': case 'B': break;
+        case OPT_PREC:
+            if (!strcmp(optarg, "fp32")) precision = SNAPMRF_PREC_FP32;
+            else if (!strcmp(optarg, "bf16")) precision = SNAPMRF_PREC_BF16;
+            else if (!strcmp(optarg, "fp16")) precision = SNAPMRF_PREC_FP16;
+            else errx(EX_USAGE, "--precision must be fp32, bf16 or fp16");
+            break;
+        case OPT_TOPK: topk = atoi(optarg); break;
+        case OPT_ALLB1: dict_flags |= SNAPMRF_DICT_ALL_B1_BLOCKS; break;
+        case OPT_NORM: dict_flags |= SNAPMRF_DICT_NORMALIZE; break;
+        case 'h':
+        default: usage(); return 1;
+        }
+    }
+    // positional: the first *.ra is the image stack, the first *.csv the schedule
+    bool have_ra = false, have_csv = false;
+    for (int i = optind; i < argc && !(have_ra && have_csv); i++) {
+        if (!have_ra && strstr(argv[i], ".ra")) { in_img = argv[i]; have_ra = true; }
+        if (!have_csv && strstr(argv[i], ".csv")) { in_mrf = argv[i]; have_csv = true; }
+    }
+    printf("\nnstates : %d\nEcho : %s\n\n", nstates, echo_type);
+
+    // parameter grids (src/mrf.cu:168-232)
+    std::vector<float> t1, t2, b0, b1;
+    if (NATOMS_req != 0) {
+        printf("Hard coding for parameters...\n");
+        size_t l_b1 = 11, l_b0 = 21;
+        size_t l_t = (size_t)roundf(sqrtf((float)(NATOMS_req / l_b0 / l_b1)));
+        if (l_t == 0) l_t = 1;
+        t1.resize(l_t); t2.resize(l_t); b0.resize(l_b0); b1.resize(l_b1);
+        snapmrf_logspace(t1.data(), 100.f, 3000.f, l_t);
+        snapmrf_logspace(t2.data(), 20.f, 1000.f, l_t);
+        snapmrf_logspace(b0.data(), -150.f, 150.f, l_b0);
+        snapmrf_logspace(b1.data(), 0.5f, 1.5f, l_b1);
+    } else {
+        printf("Parsing parameters...\nT1 : %s\nT2 : %s\nB0 : %s\nB1 : %s\n", T1, T2, B0, B1);
+        t1 = grid_values(T1); t2 = grid_values(T2); b0 = grid_values(B0); b1 = grid_values(B1);
+    }
+    size_t NATOMS = snapmrf_compute_natoms(t1.data(), t2.data(), t1.size(), t2.size(), b0.size(), b1.size());
+    size_t natoms = NATOMS / b1.size();
+    printf("l_t1: %zu, l_t2: %zu, l_b0: %zu, l_b1: %zu\nNATOMS: %zu, natoms: %zu\n", t1.size(), t2.size(),
+           b0.size(), b1.size(), NATOMS, natoms);
+    if (NATOMS == 0) errx(EX_SOFTWARE, "Number of atoms is 0!");
+    std::vector<float> h_params(NATOMS * nparams);
+    check(snapmrf_trans_params(h_params.data(), t1.data(), t2.data(), b0.data(), b1.data(), t1.size(), t2.size(),
+                               b0.size(), b1.size(), NATOMS, nparams), "trans_params");
+
+    // schedule (src/mrf.cu:260-276)
+    printf("Input mrf: %s\n", in_mrf);
+    size_t lines = snapmrf_csv_dim(in_mrf);
+    if (lines == (size_t)-1 || lines < 2) errx(EX_NOINPUT, "cannot read schedule %s", in_mrf);
+    size_t NREPS = lines - 1;
+    if (nreps > NREPS) nreps = NREPS;
+    printf("NREPS: %zu, nreps: %zu\n\n", NREPS, nreps);
+    std::vector<float> h_mrf(NREPS * 4);
+    check(snapmrf_csv_read(h_mrf.data(), NREPS, in_mrf), "csv_read");
+
+    cuda_check(cudaSetDevice(0), "cudaSetDevice");
+    cudaStream_t st;
+    cuda_check(cudaStreamCreate(&st), "cudaStreamCreate");
+    float *d_params;
+    float *d_atoms;
+    cuda_check(cudaMalloc((void **)&d_params, h_params.size() * sizeof(float)), "cudaMalloc");
+    cuda_check(cudaMemcpyAsync(d_params, h_params.data(), h_params.size() * sizeof(float), cudaMemcpyHostToDevice, st),
+               "cudaMemcpy");
+    cuda_check(cudaMalloc((void **)&d_atoms, nreps * NATOMS * 2 * sizeof(float)), "cudaMalloc");
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+
+    snapmrf_dict_opts dopt = {dict_flags, 1, NULL};
+    printf("Constructing dictionary...\n");
+    cudaEventRecord(e0, st);
+    check(snapmrf_mrf_dict(d_atoms, d_params, h_mrf.data(), nreps, NREPS, NATOMS, natoms, nparams, nstates,
+                           echo_type, &dopt, st), "MRF_dict");
+    cudaEventRecord(e1, st);
+    cuda_check(cudaStreamSynchronize(st), "dictionary");
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    printf("Elapsed dictionary time: %.4f s\n\n", ms / 1e3);
+
+    if (!in_img && out_maps) printf("NO data specified! Abort matching!\n");
+    if (in_img) {
+        printf("Input img: %s\n", in_img);
+        snapmrf_ra img;
+        check(snapmrf_ra_read(&img, in_img, 1), "ra_read");
+        if (img.eltype != 4 || img.elbyte != 8 || img.ndims < 2)
+            errx(EX_DATAERR, "%s: expected a complex (nt, nx[, ny]) RA image", in_img);
+        size_t nt = img.dims[0];
+        size_t nvoxels = img.dims[1] * (img.ndims > 2 ? img.dims[2] : 1);
+        printf("nt: %zu, voxels: %zu\n\n", nt, nvoxels);
+        std::vector<float> h_b1;
+        snapmrf_match_opts mopt;
+        memset(&mopt, 0, sizeof mopt);
+        mopt.precision = precision;
+        mopt.img_stride = nt;
+        mopt.atom_stride = nreps;
+        mopt.topk = topk;
+        snapmrf_ra b1ra;
+        memset(&b1ra, 0, sizeof b1ra);
+        if (in_b1map) {
+            printf("Input B1 map: %s\n", in_b1map);
+            check(snapmrf_ra_read(&b1ra, in_b1map, 1), "ra_read");
+            if (b1ra.eltype != 3 || b1ra.elbyte != 4 || b1ra.size < nvoxels * sizeof(float))
+                errx(EX_DATAERR, "%s: B1 map must hold %zu float values", in_b1map, nvoxels);
+            mopt.b1map = reinterpret_cast<const float *>(b1ra.data);
+            mopt.b1map_on_host = 1;
+        }
+        float *d_maps;
+        cuda_check(cudaMalloc((void **)&d_maps, nmaps * nvoxels * sizeof(float)), "cudaMalloc");
+        printf("Matching...\n");
+        cudaEventRecord(e0, st);
+        check(snapmrf_mrf_match(d_maps, reinterpret_cast<const float *>(img.data), 1, d_atoms, d_params,
+                                nreps < nt ? nreps : nt, NATOMS, natoms, nvoxels, nparams, nmaps, &mopt, st),
+              "MRF_match");
+        cudaEventRecord(e1, st);
+        cuda_check(cudaStreamSynchronize(st), "matching");
+        cudaEventElapsedTime(&ms, e0, e1);
+        printf("Elapsed matching time: %.4f s\n\n", ms / 1e3);
+        if (!out_maps) out_maps = "../result/maps.ra";
+        printf("Output maps: %s\n", out_maps);
+        std::vector<float> h_maps(nmaps * nvoxels);
+        cuda_check(cudaMemcpy(h_maps.data(), d_maps, h_maps.size() * sizeof(float), cudaMemcpyDeviceToHost),
+                   "cudaMemcpy");
+        save_ra(h_maps.data(), 3, 4, out_maps, nmaps, nvoxels);
+        cudaFree(d_maps);
+        snapmrf_ra_free(&img);
+        if (in_b1map) snapmrf_ra_free(&b1ra);
+    }
+    if (out_atoms) {
+        printf("Output atoms: %s\n", out_atoms);
+        std::vector<float> h(nreps * NATOMS * 2);
+        cuda_check(cudaMemcpy(h.data(), d_atoms, h.size() * sizeof(float), cudaMemcpyDeviceToHost), "cudaMemcpy");
+        save_ra(h.data(), 4, 8, out_atoms, nreps, NATOMS);
+    }
+    if (out_params) {
+        printf("Output params: %s\n", out_params);
+        save_ra(h_params.data(), 3, 4, out_params, nparams, NATOMS);
+    }
+    cudaFree(d_atoms);
+    cudaFree(d_params);
+    cudaStreamDestroy(st);
+    return 0;
+}
