@@ -15,10 +15,15 @@
  *   csv    path out.f32               csv_dim + csv_read; prints NREPS
  *   dict   echo params.f32 mrf.f32 nreps NREPS NATOMS natoms nstates out.c64
  *   match  img.c64 atoms.c64 params.f32 NREPS nreps NATOMS natoms nvox
- *          b1map.ra|- out.f32          (GPU subcommands need a device)
+ *          b1map.ra|- out.f32
+ *   normalize in.c64 nreps natoms out.c64   the reference's normalize kernel
+ *                                     (GPU subcommands need a device)
  * Run with stdin from /dev/null: the reference's gpuAssert waits on getchar().
  */
 #include "functions.h"
+
+extern int gridsize;
+extern int blocksize;
 
 static void *read_file(const char *path, size_t *n)
 {
@@ -156,6 +161,19 @@ int main(int argc, char **argv)
         write_file(argv[11], h, 5 * nvox * sizeof(float));
         fprintf(stderr, "REF_MATCH_MS %.3f\n", ms);
         (void)ni;
+        return 0;
+    }
+    if (!strcmp(cmd, "normalize") && argc == 6) {
+        size_t n;
+        float2 *h = (float2 *)read_file(argv[2], &n);
+        size_t nreps = strtoull(argv[3], 0, 10), natoms = strtoull(argv[4], 0, 10);
+        float2 *d;
+        cuTry(cudaMalloc((void **)&d, n));
+        cuTry(cudaMemcpy(d, h, n, cudaMemcpyHostToDevice));
+        normalize<<<gridsize, blocksize>>>(d, nreps, natoms);
+        cuTry(cudaDeviceSynchronize());
+        cuTry(cudaMemcpy(h, d, n, cudaMemcpyDeviceToHost));
+        write_file(argv[5], h, n);
         return 0;
     }
     fprintf(stderr, "bad arguments\n");

@@ -229,6 +229,13 @@ extern "C" int snapmrf_mrf_dict(float *d_atoms, const float *d_params, const flo
     a.own_params = (echo == ECHO_SSFP) ? 0 : 1;
     a.normalize = normalize ? 1 : 0;
     a.n_iso = n_iso;
+    // init_rf_pulse arguments per engine (src/functions.cu:697, 753, 821, 890,
+    // 965-966, 1175): SSFP 180 deg with TI 40 ms, SE/TSE 90/90, ROA 180,
+    // FISP/SR no pulse
+    a.init_alpha_deg = (echo == ECHO_SSFP || echo == ECHO_ROA) ? 180.f
+                       : (echo == ECHO_SE || echo == ECHO_TSE) ? 90.f : 0.f;
+    a.init_phi_deg = (echo == ECHO_SE || echo == ECHO_TSE) ? 90.f : 0.f;
+    a.init_ti = (echo == ECHO_SSFP) ? 40.f : 0.f;
 
     if (echo == ECHO_ROA) {
         if (n_iso > 32 * 8) SNAPMRF_FAIL(SNAPMRF_ERR_UNSUPPORTED, "MRF_dict: n_iso must be <= 256");

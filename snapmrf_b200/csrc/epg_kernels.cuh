@@ -27,6 +27,10 @@ struct EpgArgs {
     int own_params;       // 1: each atom's own row; 0: block-0 row (epg_ssfp)
     int normalize;        // unit-norm each atom (src/functions.cu:670-685)
     int n_iso;            // ROA isochromats
+    // initial pulse (init_rf_pulse): angles in degrees, TI in ms.  Passed at
+    // run time like the reference's kernel arguments, so that __sincosf is
+    // evaluated on the device rather than folded at compile time.
+    float init_alpha_deg, init_phi_deg, init_ti;
 };
 
 // Number of per-(atom, step) factors staged: E1/E2 at TE and at TR-TE, plus
@@ -247,15 +251,11 @@ __global__ void __launch_bounds__(kEpgThreads) epg_ref_kernel(EpgArgs a) {
     const int w = a.nstates;
 
     LaneState<S> s;
-    if (ECHO == ECHO_SSFP) {
-        st_init<S>(s, lane0, T1, T2, 180.f, 0.f, 40.f);
-    } else if (ECHO == ECHO_SE || ECHO == ECHO_TSE) {
-        st_init<S>(s, lane0, T1, T2, 90.f, 90.f, 0.f);
+    st_init<S>(s, lane0, T1, T2, a.init_alpha_deg, a.init_phi_deg, a.init_ti);
+    if (ECHO == ECHO_SE || ECHO == ECHO_TSE) {
         st_shift<S>(s, gl, L, w);
         float te0 = TE[0];
         st_relax<S>(s, expf(-te0 / T1), expf(-te0 / T2), lane0);
-    } else {
-        st_init<S>(s, lane0, T1, T2, 0.f, 0.f, 0.f);
     }
 
     float nrm = 0.f;
@@ -560,10 +560,12 @@ __device__ __forceinline__ void roa_matrix(float alpha, float phi, float *T) {
     T[8] = c_a;
 }
 
-// init_rf_pulse (ROA, src/functions.cu:1022-1047) with alpha 180, phi 0, TI 0.
-__device__ __forceinline__ void roa_init(float t1, float t2, float &m0, float &m1, float &m2) {
-    float ia = (float)(180.f * M_PI / 180.f), ip = (float)(0.f * M_PI / 180.f);
-    float e1 = expf(-0.f / t1), e2 = expf(-0.f / t2);
+// init_rf_pulse (ROA, src/functions.cu:1022-1047); roa_ssfp calls it with
+// alpha 180, phi 0, TI 0 (run-time values, see EpgArgs).
+__device__ __forceinline__ void roa_init(float t1, float t2, float &m0, float &m1, float &m2, float alpha_deg,
+                                         float phi_deg, float TI) {
+    float ia = (float)(alpha_deg * M_PI / 180.f), ip = (float)(phi_deg * M_PI / 180.f);
+    float e1 = expf(-TI / t1), e2 = expf(-TI / t2);
     float sa, ca, sph, cph;
     __sincosf(ia, &sa, &ca);
     __sincosf(ip, &sph, &cph);
@@ -595,7 +597,7 @@ __global__ void __launch_bounds__(kEpgThreads) roa_kernel(EpgArgs a) {
     const float *phi = a.sched + nreps;
     const float *TR = a.sched + 2 * nreps;
     float m0, m1, m2;
-    roa_init(t1, t2, m0, m1, m2);
+    roa_init(t1, t2, m0, m1, m2, a.init_alpha_deg, a.init_phi_deg, a.init_ti);
     float nrm = 0.f;
     const int warp = tid / 32, lane = tid % 32;
     for (long long t0 = 0; t0 < nreps; t0 += kChunk) {
@@ -605,9 +607,11 @@ __global__ void __launch_bounds__(kEpgThreads) roa_kernel(EpgArgs a) {
         __syncthreads();
         for (int i = 0; i < nch; i++) {
             const float *T = sT[i].T;
-            float n0 = T[0] * m0 + T[3] * m1 + T[6] * m2;
-            float n1 = T[1] * m0 + T[4] * m1 + T[7] * m2;
-            float n2 = T[2] * m0 + T[5] * m1 + T[8] * m2;
+            // the in-place cublasSgemm of apply_rf_pulse (ROA), accumulated
+            // over the three components in order
+            float n0 = fmaf(T[6], m2, fmaf(T[3], m1, T[0] * m0));
+            float n1 = fmaf(T[7], m2, fmaf(T[4], m1, T[1] * m0));
+            float n2 = fmaf(T[8], m2, fmaf(T[5], m1, T[2] * m0));
             float tr = TR[t0 + i];
             float E1 = expf(-tr / t1), E2 = expf(-tr / t2);
             m0 = E2 * n0;
@@ -676,7 +680,7 @@ __global__ void __launch_bounds__(kEpgThreads) roa_iso_kernel(EpgArgs a) {
     for (int q = 0; q < IPL; q++) {
         int j = lane * IPL + q;
         valid[q] = j < n_iso;
-        roa_init(t1, t2, m0[q], m1[q], m2[q]);
+        roa_init(t1, t2, m0[q], m1[q], m2[q], a.init_alpha_deg, a.init_phi_deg, a.init_ti);
         double d = M_PI * (double)j / (double)n_iso;
         cd[q] = (float)cos(d);
         sd[q] = (float)sin(d);
@@ -699,9 +703,9 @@ __global__ void __launch_bounds__(kEpgThreads) roa_iso_kernel(EpgArgs a) {
             float px = 0.f, py = 0.f;
 #pragma unroll
             for (int q = 0; q < IPL; q++) {
-                float n0 = T[0] * m0[q] + T[3] * m1[q] + T[6] * m2[q];
-                float n1 = T[1] * m0[q] + T[4] * m1[q] + T[7] * m2[q];
-                float n2 = T[2] * m0[q] + T[5] * m1[q] + T[8] * m2[q];
+                float n0 = fmaf(T[6], m2[q], fmaf(T[3], m1[q], T[0] * m0[q]));
+                float n1 = fmaf(T[7], m2[q], fmaf(T[4], m1[q], T[1] * m0[q]));
+                float n2 = fmaf(T[8], m2[q], fmaf(T[5], m1[q], T[2] * m0[q]));
                 float x = E2 * n0, y = E2 * n1;
                 m2[q] = E1 * n2 + (1 - E1);
                 // rotation by beta then by the isochromat's delta
