@@ -246,6 +246,49 @@ int snapmrf_mrf_match_noalloc(float *d_maps, const float *d_img, size_t img_stri
                               int nparams, int nmaps, const float *d_b1map, int64_t *d_index,
                               void *stream);
 
+/* ------------------------------------------------------------------------
+ * Derivatives of the EPG signal.  No counterpart in the reference, which
+ * only evaluates the forward recursion; both entry points differentiate its
+ * real-valued FISP / SR recursion (epg_fisp, epg_sr: src/functions.cu:687-739,
+ * 878-933, every RF phase 0) with the B1 extension of snapmrf_mrf_dict
+ * (flip angle alpha_t * B1, no initial pulse).
+ * ------------------------------------------------------------------------ */
+
+/* Reverse mode (adjoint) with checkpointing.
+ *
+ * d_params: device [natoms][nparams] (T1, T2, B0, B1; nparams >= 4);
+ * h_mrf: host [4][NREPS] schedule as for snapmrf_mrf_dict (row 1 must be 0);
+ * d_grad_signal: device complex [natoms][nreps], dL/d(Re s_t, Im s_t) of a
+ * real loss L of the (unnormalised) atoms s;
+ * d_signal: optional out, the atoms (complex [natoms][nreps]);
+ * d_grad_params: out [natoms][3]: dL/dT1, dL/dT2, dL/dB1;
+ * d_grad_alpha: optional out [nreps]: dL/dalpha_t summed over atoms;
+ * d_grad_alpha_atoms: optional out [natoms][nreps]: the per-atom terms;
+ * checkpoint_every: states kept every C steps (0: C = ceil(sqrt(nreps))),
+ * so device scratch is natoms * (nreps/C + C) * 3 * nstates floats (rounded
+ * up to the kernel's state layout). */
+int snapmrf_epg_adjoint(const float *d_params, int nparams, const float *h_mrf, size_t nreps,
+                        size_t NREPS, size_t natoms, int nstates, const char *echo_type,
+                        const float *d_grad_signal, float *d_signal, float *d_grad_params,
+                        float *d_grad_alpha, float *d_grad_alpha_atoms, int checkpoint_every,
+                        void *stream);
+
+/* Per-voxel Gauss-Newton refinement of (T1, T2) after matching.
+ *
+ * Model: voxel x = rho * s(T1, T2, B1) with rho complex, eliminated by
+ * variable projection (rho = <s, x> / <s, s>); each iteration runs the
+ * forward recursion with the tangents ds/dT1 and ds/dT2, then solves the
+ * 2x2 normal equations of the projected residual.  Steps are clipped to
+ * max_rel_step (0: 0.2) times the current value, and T1 > T2 > 0 is kept.
+ * d_theta: device in/out [nvoxels][3] = T1, T2, B1 (B1 is not changed);
+ * img: device complex [nvoxels][img_stride] (0 = nreps);
+ * d_pd (optional out [nvoxels]): |<s, x>| / ||s||, the matching PD of a
+ * normalised atom; d_m0 (optional out [nvoxels]): |rho|.  These two cost
+ * one more forward pass at the final parameters. */
+int snapmrf_refine_gn(float *d_theta, const float *img, size_t img_stride, const float *h_mrf,
+                      size_t nreps, size_t NREPS, size_t nvoxels, int nstates, const char *echo_type,
+                      int iterations, float max_rel_step, float *d_pd, float *d_m0, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -87,3 +87,84 @@ int oracle_max_threads(void)
     return 1;
 #endif
 }
+
+/* ------------------------------------------------------------------------
+ * FP64 forward mode (one tangent) for the FISP / SR recursion with every RF
+ * phase 0 (epg_fisp src/functions.cu:878-933, epg_sr :687-739; RF matrix
+ * :483-508 at phi = 0), the form the derivative kernels differentiate:
+ * state (f+, f-, z) = (Im F+, Im F-, Re Z) per EPG state, flip angle
+ * alpha_t * b1 (the B1 extension of epg_fisp), readout s_t = i f+[0] after
+ * relax(TE) (no normalisation).  Each state carries a value and a
+ * derivative along one direction (dT1, dT2, dB1, dalpha[t]).
+ * mrf is a compact [4][nreps] schedule.
+ *
+ * Outputs: sig[T] (value of Im s_t) and dsig[T] (its tangent);
+ * loss = sum_t |s_t - y_t|^2 and dloss, its derivative along the direction,
+ * with y[2T] interleaved complex targets (NULL: no loss).
+ * ---------------------------------------------------------------------- */
+typedef struct { double v, d; } dual;
+
+static inline dual dmk(double v, double d) { dual r; r.v = v; r.d = d; return r; }
+static inline dual dadd(dual a, dual b) { return dmk(a.v + b.v, a.d + b.d); }
+static inline dual dmul(dual a, dual b) { return dmk(a.v * b.v, a.d * b.v + a.v * b.d); }
+static inline dual dexp(dual a) { double e = exp(a.v); return dmk(e, e * a.d); }
+static inline dual dsin(dual a) { return dmk(sin(a.v), cos(a.v) * a.d); }
+static inline dual dcos(dual a) { return dmk(cos(a.v), -sin(a.v) * a.d); }
+static inline dual ddiv(dual a, dual b) { return dmk(a.v / b.v, (a.d * b.v - a.v * b.d) / (b.v * b.v)); }
+
+int oracle_fisp_jvp_f64(double *sig, double *dsig, double *loss, double *dloss, double T1, double T2, double B1,
+                        double dT1, double dT2, double dB1, const float *mrf, const double *dalpha, size_t nreps,
+                        int nstates, int shift, const double *y)
+{
+    int w = nstates;
+    dual *fp = (dual *)calloc(3 * (size_t)w, sizeof(dual));
+    if (!fp) return -3;
+    dual *fm = fp + w, *z = fm + w;
+    const float *alpha = mrf, *TR = mrf + 2 * nreps, *TE = mrf + 3 * nreps;
+    z[0] = dmk(1, 0);
+    dual t1 = dmk(T1, dT1), t2 = dmk(T2, dT2), b1 = dmk(B1, dB1);
+    dual L = dmk(0, 0);
+    for (size_t i = 0; i < nreps; i++) {
+        dual a = dmul(dmk(alpha[i], dalpha ? dalpha[i] : 0), b1);
+        dual sa = dsin(a), ca = dcos(a);
+        dual c2 = dmul(dadd(dmk(1, 0), ca), dmk(0.5, 0)), s2 = dmul(dadd(dmk(1, 0), dmk(-ca.v, -ca.d)), dmk(0.5, 0));
+        dual hs = dmul(sa, dmk(0.5, 0));
+        for (int k = 0; k < w; k++) {
+            dual p = fp[k], m = fm[k], q = z[k];
+            fp[k] = dadd(dadd(dmul(c2, p), dmul(s2, m)), dmul(dmk(-sa.v, -sa.d), q));
+            fm[k] = dadd(dadd(dmul(s2, p), dmul(c2, m)), dmul(sa, q));
+            z[k] = dadd(dadd(dmul(hs, p), dmul(dmk(-hs.v, -hs.d), m)), dmul(ca, q));
+        }
+        double ta = (double)TE[i], tb = (double)TR[i] - (double)TE[i];
+        for (int pass = 0; pass < 2; pass++) {
+            double t = pass == 0 ? ta : tb;
+            dual E1 = dexp(ddiv(dmk(-t, 0), t1)), E2 = dexp(ddiv(dmk(-t, 0), t2));
+            for (int k = 0; k < w; k++) {
+                fp[k] = dmul(fp[k], E2);
+                fm[k] = dmul(fm[k], E2);
+                z[k] = dmul(z[k], E1);
+            }
+            z[0] = dadd(z[0], dmk(1 - E1.v, -E1.d));
+            if (pass == 0) {
+                sig[i] = fp[0].v;
+                dsig[i] = fp[0].d;
+                if (y) {
+                    double re = -(double)y[2 * i], im = fp[0].v - y[2 * i + 1];
+                    L.v += re * re + im * im;
+                    L.d += 2 * im * fp[0].d;
+                }
+                if (shift) {
+                    for (int k = w - 1; k >= 1; k--) fp[k] = fp[k - 1];
+                    dual f0 = fm[0];
+                    for (int k = 0; k <= w - 2; k++) fm[k] = fm[k + 1];
+                    fp[0] = dmk(-(w == 1 ? f0.v : fm[0].v), -(w == 1 ? f0.d : fm[0].d));
+                    fm[w - 1] = dmk(0, 0);
+                }
+            }
+        }
+    }
+    if (loss) *loss = L.v;
+    if (dloss) *dloss = L.d;
+    free(fp);
+    return 0;
+}

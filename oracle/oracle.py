@@ -93,3 +93,33 @@ def match(img, atoms, params, nreps: int, natoms: int | None = None, b1map=None,
     if r != 0:
         raise RuntimeError(f"oracle_match failed: {r}")
     return maps, idx
+
+
+def fisp_jvp(theta, tangent, h_mrf, nstates: int = 101, echo: str = "epg_fisp", dalpha=None, y=None):
+    """FP64 forward-mode derivative of the real FISP / SR recursion (every
+    RF phase 0) along one direction.
+
+    theta = (T1, T2, B1), tangent = (dT1, dT2, dB1), optional dalpha [T]
+    (direction in the flip-angle schedule), optional targets y complex [T].
+    Returns (Im s [T], d Im s [T], loss, dloss) with loss = sum |s - y|^2
+    (0, 0 without y)."""
+    h_mrf = np.ascontiguousarray(h_mrf, np.float32)
+    T = h_mrf.shape[-1]
+    sig = np.zeros(T, np.float64)
+    dsig = np.zeros(T, np.float64)
+    loss = C.c_double(0)
+    dloss = C.c_double(0)
+    da = None if dalpha is None else np.ascontiguousarray(dalpha, np.float64)
+    yy = None if y is None else np.ascontiguousarray(np.stack([np.real(y), np.imag(y)], -1), np.float64)
+    if echo not in ("epg_fisp", "epg_sr"):
+        raise ValueError("fisp_jvp covers epg_fisp and epg_sr")
+    f = lib().oracle_fisp_jvp_f64
+    f.restype = C.c_int
+    f.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p] + [C.c_double] * 6 + \
+        [C.c_void_p, C.c_void_p, C.c_size_t, C.c_int, C.c_int, C.c_void_p]
+    r = f(sig.ctypes.data, dsig.ctypes.data, C.byref(loss), C.byref(dloss), *map(float, theta),
+          *map(float, tangent), h_mrf.ctypes.data, None if da is None else da.ctypes.data, T, nstates,
+          1 if echo == "epg_fisp" else 0, None if yy is None else yy.ctypes.data)
+    if r != 0:
+        raise RuntimeError(f"oracle_fisp_jvp failed: {r}")
+    return sig, dsig, loss.value, dloss.value

@@ -101,6 +101,10 @@ def lib() -> C.CDLL:
                                         C.POINTER(MatchOpts), vp]
         L.snapmrf_mrf_match_noalloc.argtypes = [vp, vp, sz, vp, sz, vp, sz, sz, sz, sz, C.c_int, C.c_int,
                                                 vp, vp, vp]
+        L.snapmrf_epg_adjoint.argtypes = [vp, C.c_int, vp, sz, sz, sz, C.c_int, C.c_char_p, vp, vp, vp,
+                                          vp, vp, C.c_int, vp]
+        L.snapmrf_refine_gn.argtypes = [vp, vp, sz, vp, sz, sz, sz, C.c_int, C.c_char_p, C.c_int,
+                                        C.c_float, vp, vp, vp]
         _lib = L
     return _lib
 
@@ -333,3 +337,39 @@ def MRF_match_noalloc(d_maps, d_img, d_atoms, d_params, NREPS: int, nreps: int, 
     _check(lib().snapmrf_mrf_match_noalloc(_ptr(d_maps), _ptr(d_img), img_stride, _ptr(d_atoms), NREPS,
                                            _ptr(d_params), nreps, NATOMS, natoms, nvoxels, nparams, nmaps,
                                            _ptr(d_b1map), _ptr(d_index), _stream_ptr(stream)))
+
+
+# ---------------------------------------------------------------------------
+# derivatives (no counterpart in the reference)
+# ---------------------------------------------------------------------------
+
+def _schedule(h_mrf, NREPS: int) -> np.ndarray:
+    h_mrf = np.ascontiguousarray(h_mrf, np.float32)
+    if h_mrf.size < 4 * NREPS:
+        raise SnapMRFError(1, "h_mrf must hold 4*NREPS values")
+    return h_mrf
+
+
+def epg_adjoint(d_params, h_mrf, nreps: int, NREPS: int, natoms: int, d_grad_signal, d_grad_params,
+                nparams: int = NPARAMS, nstates: int = 101, echo_type: str = "epg_fisp", *,
+                d_signal=None, d_grad_alpha=None, d_grad_alpha_atoms=None, checkpoint_every: int = 0,
+                stream=None) -> None:
+    """Reverse-mode derivative of the real FISP / SR recursion: given
+    dL/ds (device complex64 [natoms][nreps]) writes dL/d(T1, T2, B1) into
+    d_grad_params [natoms][3] and, optionally, dL/dalpha_t."""
+    h_mrf = _schedule(h_mrf, NREPS)
+    _check(lib().snapmrf_epg_adjoint(_ptr(d_params), nparams, h_mrf.ctypes.data, nreps, NREPS, natoms,
+                                     nstates, echo_type.encode(), _ptr(d_grad_signal), _ptr(d_signal),
+                                     _ptr(d_grad_params), _ptr(d_grad_alpha), _ptr(d_grad_alpha_atoms),
+                                     checkpoint_every, _stream_ptr(stream)))
+
+
+def refine_gn(d_theta, d_img, h_mrf, nreps: int, NREPS: int, nvoxels: int, nstates: int = 101,
+              echo_type: str = "epg_fisp", *, iterations: int = 2, max_rel_step: float = 0.2,
+              img_stride: int = 0, d_pd=None, d_m0=None, stream=None) -> None:
+    """Gauss-Newton refinement of matched (T1, T2): d_theta device float32
+    [nvoxels][3] (T1, T2, B1) in/out; d_img device complex64 voxels."""
+    h_mrf = _schedule(h_mrf, NREPS)
+    _check(lib().snapmrf_refine_gn(_ptr(d_theta), _ptr(d_img), img_stride, h_mrf.ctypes.data, nreps, NREPS,
+                                   nvoxels, nstates, echo_type.encode(), iterations, max_rel_step, _ptr(d_pd),
+                                   _ptr(d_m0), _stream_ptr(stream)))

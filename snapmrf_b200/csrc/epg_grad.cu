@@ -1,0 +1,615 @@
+// Derivatives of the EPG recursion on sm_100a: a reverse-mode (adjoint)
+// kernel with checkpointing, and a forward-mode kernel with two tangents
+// that drives a per-voxel Gauss-Newton refinement of (T1, T2).
+//
+// Both work on the real-valued FISP / SR recursion (every RF phase 0, the
+// form of the benchmark dictionaries): per EPG state f+ = Im F+,
+// f- = Im F-, z = Re Z; flip angle a_t = alpha_t * B1; per step
+//   RF    f+' = c f+ + s f- - S z,  f-' = s f+ + c f- + S z,
+//         z'  = S/2 f+ - S/2 f- + C z      (C = cos a, S = sin a,
+//                                          c = (1 + C)/2, s = (1 - C)/2)
+//   relax f+- *= E2(TE), z *= E1(TE), z0 += 1 - E1(TE)
+//   read  s_t = i f+[0]
+//   shift (FISP only) F+ up, F- down, f+[0] = -f-[0], F-[w-1] = 0
+//   relax over TR - TE
+// which is the reference's epg_fisp / epg_sr (src/functions.cu:687-739,
+// 878-933) with the B1 extension (flip angle times the atom's B1).
+//
+// Layout: one atom (or voxel) per group of L lanes, S states per lane, as in
+// the dictionary kernels; states k >= w are kept exactly zero so that they
+// never enter a gradient.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "common.h"
+
+namespace snapmrf {
+namespace grad {
+
+constexpr int kThreads = 128;
+constexpr int kMaxS = 8;
+
+struct Schedule {
+    const float *alpha;  // [nreps] raw flip angles (rad)
+    const float *TR;     // [nreps] ms
+    const float *TE;     // [nreps] ms
+    int nreps;
+};
+
+// Per-step constants of the recursion for one flip angle a.
+struct StepRF {
+    float C, S, c, s, hS;  // cos a, sin a, (1+C)/2, (1-C)/2, S/2
+};
+
+__device__ __forceinline__ StepRF step_rf(float a) {
+    StepRF r;
+    __sincosf(a, &r.S, &r.C);
+    r.c = (1 + r.C) / 2;
+    r.s = (1 - r.C) / 2;
+    r.hS = 0.5f * r.S;
+    return r;
+}
+
+template <int S>
+struct St {
+    float p[S], m[S], z[S];
+};
+
+template <int S>
+__device__ __forceinline__ void rf_fwd(St<S> &x, const StepRF &r) {
+#pragma unroll
+    for (int j = 0; j < S; j++) {
+        const float p = x.p[j], m = x.m[j], q = x.z[j];
+        x.p[j] = fmaf(-r.S, q, fmaf(r.s, m, r.c * p));
+        x.m[j] = fmaf(r.S, q, fmaf(r.c, m, r.s * p));
+        x.z[j] = fmaf(r.C, q, fmaf(-r.hS, m, r.hS * p));
+    }
+}
+
+template <int S>
+__device__ __forceinline__ void relax_fwd(St<S> &x, float E1, float E2, bool lane0) {
+#pragma unroll
+    for (int j = 0; j < S; j++) {
+        x.p[j] *= E2;
+        x.m[j] *= E2;
+        x.z[j] *= E1;
+    }
+    if (lane0) x.z[0] += 1 - E1;
+}
+
+// Shift with padding kept at zero (see dephase_gradients).
+template <int S>
+__device__ __forceinline__ void shift_fwd(St<S> &x, int gl, int L, int w) {
+    const unsigned full = 0xffffffffu;
+    const float up = __shfl_up_sync(full, x.p[S - 1], 1, L);
+    const float dn = __shfl_down_sync(full, x.m[0], 1, L);
+    const float old_m0 = x.m[0];
+#pragma unroll
+    for (int j = S - 1; j >= 1; j--) x.p[j] = x.p[j - 1];
+    x.p[0] = up;
+#pragma unroll
+    for (int j = 0; j < S - 1; j++) x.m[j] = x.m[j + 1];
+    x.m[S - 1] = (gl == L - 1) ? 0.f : dn;
+    if (gl == 0) x.p[0] = -((w == 1) ? old_m0 : x.m[0]);
+#pragma unroll
+    for (int j = 0; j < S; j++) {
+        const int k = gl * S + j;
+        if (k >= w) x.p[j] = x.m[j] = 0.f;
+        if (k == w - 1) x.m[j] = 0.f;
+    }
+}
+
+// Transpose of shift_fwd acting on an adjoint state: lambda_f+ moves down a
+// slot, lambda_f- up a slot, lambda_f-[1] (or [0] for w = 1) receives
+// -lambda_f+[0]; lambda_f+[w-1] and lambda_f-[k >= w] vanish.
+template <int S>
+__device__ __forceinline__ void shift_adj(St<S> &l, int gl, int L, int w) {
+    const unsigned full = 0xffffffffu;
+    const float lp0 = l.p[0];
+    const float lp0_all = __shfl_sync(full, lp0, 0, L);   // lambda_f+[0] of the group
+    const float dn = __shfl_down_sync(full, l.p[0], 1, L);
+    const float up = __shfl_up_sync(full, l.m[S - 1], 1, L);
+#pragma unroll
+    for (int j = 0; j < S - 1; j++) l.p[j] = l.p[j + 1];
+    l.p[S - 1] = (gl == L - 1) ? 0.f : dn;
+#pragma unroll
+    for (int j = S - 1; j >= 1; j--) l.m[j] = l.m[j - 1];
+    l.m[0] = (gl == 0) ? 0.f : up;
+    // f+[0] = -f-[1] (w >= 2) or -f-[0] (w == 1) before the shift
+    const int kk = (w == 1) ? 0 : 1;
+#pragma unroll
+    for (int j = 0; j < S; j++) {
+        const int k = gl * S + j;
+        if (k == kk) l.m[j] -= lp0_all;
+        if (k == w - 1) l.p[j] = 0.f;
+        if (k >= w) l.m[j] = 0.f;
+    }
+}
+
+__device__ __forceinline__ float group_sum(float v, int L) {
+    for (int o = L / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o, L);
+    return v;
+}
+
+// --------------------------------------------------------------------------
+// Adjoint
+// --------------------------------------------------------------------------
+struct AdjArgs {
+    Schedule sch;
+    const float *params;      // [n][nparams]: T1, T2, (B0), B1
+    int nparams;
+    long long n;
+    int w, L, shift;
+    const float2 *gsig;       // [n][nreps] dL/d(Re s_t, Im s_t)
+    float2 *sig;              // optional out [n][nreps]
+    float *gparams;           // [n][3]: dL/dT1, dL/dT2, dL/dB1
+    float *galpha_atoms;      // [n][nreps] dL/dalpha_t per atom
+    float *ckpt;              // [n][nckpt][3][L*S]
+    float *seg;               // [n][C][3][L*S]
+    int C, nckpt;
+};
+
+// A saved state is [3][S][L] floats: for each register slot the L lanes of
+// the group touch consecutive words.
+template <int S>
+__device__ __forceinline__ void store_state(float *dst, int L, int gl, const St<S> &x) {
+#pragma unroll
+    for (int j = 0; j < S; j++) {
+        dst[j * L + gl] = x.p[j];
+        dst[(S + j) * L + gl] = x.m[j];
+        dst[(2 * S + j) * L + gl] = x.z[j];
+    }
+}
+
+template <int S>
+__device__ __forceinline__ void load_state(const float *src, int L, int gl, St<S> &x) {
+#pragma unroll
+    for (int j = 0; j < S; j++) {
+        x.p[j] = src[j * L + gl];
+        x.m[j] = src[(S + j) * L + gl];
+        x.z[j] = src[(2 * S + j) * L + gl];
+    }
+}
+
+__device__ __forceinline__ void relax_factors(const Schedule &sc, int t, float T1, float T2, float *E1a, float *E2a,
+                                              float *E1b, float *E2b, float *ta, float *tb) {
+    const float tr = sc.TR[t], te = sc.TE[t];
+    *ta = te;
+    *tb = tr - te;
+    *E1a = expf(-*ta / T1);
+    *E2a = expf(-*ta / T2);
+    *E1b = expf(-*tb / T1);
+    *E2b = expf(-*tb / T2);
+}
+
+template <int S>
+__global__ void __launch_bounds__(kThreads) adjoint_kernel(AdjArgs a) {
+    const int L = a.L, LS = L * S;
+    const int g = threadIdx.x / L, gl = threadIdx.x % L;
+    const long long atom = (long long)blockIdx.x * (kThreads / L) + g;
+    const bool active = atom < a.n;
+    const long long at = active ? atom : 0;
+    const bool lane0 = gl == 0;
+    const float *pp = a.params + at * a.nparams;
+    const float T1 = pp[0], T2 = pp[1], B1 = pp[3];
+    const int T = a.sch.nreps, w = a.w;
+    float *ck = a.ckpt + at * (long long)a.nckpt * 3 * LS;
+    float *sg = a.seg + at * (long long)a.C * 3 * LS;
+
+    // forward with checkpoints
+    St<S> x;
+#pragma unroll
+    for (int j = 0; j < S; j++) x.p[j] = x.m[j] = x.z[j] = 0.f;
+    if (lane0) x.z[0] = 1.f;
+    for (int t = 0; t < T; t++) {
+        if (t % a.C == 0 && active) store_state<S>(ck + (long long)(t / a.C) * 3 * LS, L, gl, x);
+        float E1a, E2a, E1b, E2b, ta, tb;
+        relax_factors(a.sch, t, T1, T2, &E1a, &E2a, &E1b, &E2b, &ta, &tb);
+        rf_fwd<S>(x, step_rf(a.sch.alpha[t] * B1));
+        relax_fwd<S>(x, E1a, E2a, lane0);
+        if (lane0 && active && a.sig) a.sig[at * T + t] = make_float2(0.f, x.p[0]);
+        if (a.shift) shift_fwd<S>(x, gl, L, w);
+        relax_fwd<S>(x, E1b, E2b, lane0);
+    }
+    __syncwarp();
+
+    // reverse sweep, one checkpoint segment at a time
+    St<S> l;
+#pragma unroll
+    for (int j = 0; j < S; j++) l.p[j] = l.m[j] = l.z[j] = 0.f;
+    float gT1 = 0.f, gT2 = 0.f, gB1 = 0.f;
+    for (int c = a.nckpt - 1; c >= 0; c--) {
+        const int t0 = c * a.C, t1 = min(T, t0 + a.C);
+        if (active) load_state<S>(ck + (long long)c * 3 * LS, L, gl, x);
+        for (int t = t0; t < t1; t++) {
+            if (active) store_state<S>(sg + (long long)(t - t0) * 3 * LS, L, gl, x);
+            float E1a, E2a, E1b, E2b, ta, tb;
+            relax_factors(a.sch, t, T1, T2, &E1a, &E2a, &E1b, &E2b, &ta, &tb);
+            rf_fwd<S>(x, step_rf(a.sch.alpha[t] * B1));
+            relax_fwd<S>(x, E1a, E2a, lane0);
+            if (a.shift) shift_fwd<S>(x, gl, L, w);
+            relax_fwd<S>(x, E1b, E2b, lane0);
+        }
+        __syncwarp();
+        for (int t = t1 - 1; t >= t0; t--) {
+            St<S> x0, xr, xs;
+            if (active) load_state<S>(sg + (long long)(t - t0) * 3 * LS, L, gl, x0);
+            else {
+#pragma unroll
+                for (int j = 0; j < S; j++) x0.p[j] = x0.m[j] = x0.z[j] = 0.f;
+            }
+            float E1a, E2a, E1b, E2b, ta, tb;
+            relax_factors(a.sch, t, T1, T2, &E1a, &E2a, &E1b, &E2b, &ta, &tb);
+            const float at_ = a.sch.alpha[t] * B1;
+            const StepRF r = step_rf(at_);
+            xr = x0;
+            rf_fwd<S>(xr, r);          // state after RF
+            xs = xr;
+            relax_fwd<S>(xs, E1a, E2a, lane0);
+            if (a.shift) shift_fwd<S>(xs, gl, L, w);   // state entering relax over TR-TE
+
+            // relax(TR-TE)^T
+            float gE1 = 0.f, gE2 = 0.f;
+#pragma unroll
+            for (int j = 0; j < S; j++) {
+                gE2 += l.p[j] * xs.p[j] + l.m[j] * xs.m[j];
+                gE1 += l.z[j] * xs.z[j];
+            }
+            if (lane0) gE1 -= l.z[0];
+            gT1 += gE1 * E1b * tb / (T1 * T1);
+            gT2 += gE2 * E2b * tb / (T2 * T2);
+#pragma unroll
+            for (int j = 0; j < S; j++) {
+                l.p[j] *= E2b;
+                l.m[j] *= E2b;
+                l.z[j] *= E1b;
+            }
+            if (a.shift) shift_adj<S>(l, gl, L, w);
+            // readout s_t = i f+[0] after relax(TE)
+            if (lane0 && active) l.p[0] += a.gsig[at * T + t].y;
+            // relax(TE)^T, pre-op state xr
+            gE1 = 0.f;
+            gE2 = 0.f;
+#pragma unroll
+            for (int j = 0; j < S; j++) {
+                gE2 += l.p[j] * xr.p[j] + l.m[j] * xr.m[j];
+                gE1 += l.z[j] * xr.z[j];
+            }
+            if (lane0) gE1 -= l.z[0];
+            gT1 += gE1 * E1a * ta / (T1 * T1);
+            gT2 += gE2 * E2a * ta / (T2 * T2);
+#pragma unroll
+            for (int j = 0; j < S; j++) {
+                l.p[j] *= E2a;
+                l.m[j] *= E2a;
+                l.z[j] *= E1a;
+            }
+            // RF^T with pre-op state x0; derivative of the matrix w.r.t. a
+            float ga = 0.f;
+#pragma unroll
+            for (int j = 0; j < S; j++) {
+                const float p = x0.p[j], m = x0.m[j], q = x0.z[j];
+                const float dp = -r.hS * p + r.hS * m - r.C * q;
+                const float dm = r.hS * p - r.hS * m + r.C * q;
+                const float dz = 0.5f * r.C * p - 0.5f * r.C * m - r.S * q;
+                ga += l.p[j] * dp + l.m[j] * dm + l.z[j] * dz;
+                const float lp = l.p[j], lm = l.m[j], lz = l.z[j];
+                l.p[j] = r.c * lp + r.s * lm + r.hS * lz;
+                l.m[j] = r.s * lp + r.c * lm - r.hS * lz;
+                l.z[j] = -r.S * lp + r.S * lm + r.C * lz;
+            }
+            ga = group_sum(ga, L);
+            if (lane0 && active) a.galpha_atoms[at * T + t] = ga * B1;
+            gB1 += ga * a.sch.alpha[t];
+        }
+        __syncwarp();
+    }
+    gT1 = group_sum(gT1, L);
+    gT2 = group_sum(gT2, L);
+    if (lane0 && active) {
+        a.gparams[at * 3 + 0] = gT1;
+        a.gparams[at * 3 + 1] = gT2;
+        a.gparams[at * 3 + 2] = gB1;
+    }
+}
+
+// Column sums of the per-atom schedule gradients in two deterministic
+// passes: kSplits row ranges into partial sums, then the partials.
+constexpr int kSplits = 512;
+
+__global__ void sum_columns_partial_kernel(float *part, const float *in, long long n, int T) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= T) return;
+    const long long r0 = n * blockIdx.y / kSplits, r1 = n * (blockIdx.y + 1) / kSplits;
+    float s = 0.f;
+    for (long long i = r0; i < r1; i++) s += in[i * T + t];
+    part[(long long)blockIdx.y * T + t] = s;
+}
+
+__global__ void sum_columns_final_kernel(float *out, const float *part, int T) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= T) return;
+    float s = 0.f;
+    for (int k = 0; k < kSplits; k++) s += part[(long long)k * T + t];
+    out[t] = s;
+}
+
+// --------------------------------------------------------------------------
+// Gauss-Newton refinement (forward mode, tangents d/dT1 and d/dT2)
+// --------------------------------------------------------------------------
+struct GnArgs {
+    Schedule sch;
+    long long nvox;
+    int w, L, shift;
+    const float2 *img;        // [nvox][img_stride]
+    long long img_stride;
+    float *theta;             // [nvox][3] in/out: T1, T2, B1 (B1 fixed)
+    float *pd;                // optional out [nvox]: |<s, x>| / ||s||
+    float *m0;                // optional out [nvox]: |rho| with x ~ rho * s
+    float max_rel_step;
+    int update;               // 0: only evaluate pd / m0
+};
+
+template <int S>
+struct Dual3 {
+    St<S> v, d1, d2;
+};
+
+template <int S>
+__global__ void __launch_bounds__(kThreads) gn_step_kernel(GnArgs a) {
+    const int L = a.L;
+    const int g = threadIdx.x / L, gl = threadIdx.x % L;
+    const long long vox = (long long)blockIdx.x * (kThreads / L) + g;
+    const bool active = vox < a.nvox;
+    const long long v = active ? vox : 0;
+    const bool lane0 = gl == 0;
+    const float T1 = a.theta[v * 3], T2 = a.theta[v * 3 + 1], B1 = a.theta[v * 3 + 2];
+    const int T = a.sch.nreps, w = a.w;
+    const float2 *x = a.img + v * a.img_stride;
+
+    Dual3<S> s;
+#pragma unroll
+    for (int j = 0; j < S; j++) {
+        s.v.p[j] = s.v.m[j] = s.v.z[j] = 0.f;
+        s.d1.p[j] = s.d1.m[j] = s.d1.z[j] = 0.f;
+        s.d2.p[j] = s.d2.m[j] = s.d2.z[j] = 0.f;
+    }
+    if (lane0) s.v.z[0] = 1.f;
+    // inner products (lane 0): Ss = <s,s>, P = <s,x>, G_j = <s,J_j>,
+    // H_jk = <J_j,J_k>, Q_j = <J_j,x>; s_t = i f, J_jt = i df_j
+    float Ss = 0.f, Pr = 0.f, Pi = 0.f, G1 = 0.f, G2 = 0.f, H11 = 0.f, H12 = 0.f, H22 = 0.f;
+    float Q1r = 0.f, Q1i = 0.f, Q2r = 0.f, Q2i = 0.f;
+    for (int t = 0; t < T; t++) {
+        const StepRF r = step_rf(a.sch.alpha[t] * B1);
+        rf_fwd<S>(s.v, r);
+        rf_fwd<S>(s.d1, r);
+        rf_fwd<S>(s.d2, r);
+        const float tr = a.sch.TR[t], te = a.sch.TE[t];
+        for (int pass = 0; pass < 2; pass++) {
+            const float tt = pass == 0 ? te : tr - te;
+            const float E1 = expf(-tt / T1), E2 = expf(-tt / T2);
+            const float dE1 = E1 * tt / (T1 * T1), dE2 = E2 * tt / (T2 * T2);  // dE1/dT1, dE2/dT2
+#pragma unroll
+            for (int j = 0; j < S; j++) {
+                // product rule: d(E x) = dE x + E dx
+                s.d1.p[j] = E2 * s.d1.p[j];
+                s.d1.m[j] = E2 * s.d1.m[j];
+                s.d1.z[j] = fmaf(dE1, s.v.z[j], E1 * s.d1.z[j]);
+                s.d2.p[j] = fmaf(dE2, s.v.p[j], E2 * s.d2.p[j]);
+                s.d2.m[j] = fmaf(dE2, s.v.m[j], E2 * s.d2.m[j]);
+                s.d2.z[j] = E1 * s.d2.z[j];
+            }
+            relax_fwd<S>(s.v, E1, E2, lane0);
+            if (lane0) s.d1.z[0] -= dE1;
+            if (pass == 0) {
+                if (lane0) {
+                    const float f = s.v.p[0], d1 = s.d1.p[0], d2 = s.d2.p[0];
+                    const float2 xv = x[t];
+                    Ss = fmaf(f, f, Ss);
+                    Pr = fmaf(f, xv.y, Pr);
+                    Pi = fmaf(-f, xv.x, Pi);
+                    G1 = fmaf(f, d1, G1);
+                    G2 = fmaf(f, d2, G2);
+                    H11 = fmaf(d1, d1, H11);
+                    H12 = fmaf(d1, d2, H12);
+                    H22 = fmaf(d2, d2, H22);
+                    Q1r = fmaf(d1, xv.y, Q1r);
+                    Q1i = fmaf(-d1, xv.x, Q1i);
+                    Q2r = fmaf(d2, xv.y, Q2r);
+                    Q2i = fmaf(-d2, xv.x, Q2i);
+                }
+                if (a.shift) {
+                    shift_fwd<S>(s.v, gl, L, w);
+                    shift_fwd<S>(s.d1, gl, L, w);
+                    shift_fwd<S>(s.d2, gl, L, w);
+                }
+            }
+        }
+    }
+    if (!(lane0 && active)) return;
+    // variable projection: rho = P / Ss; A_jk = |rho|^2 (H_jk - G_j G_k / Ss),
+    // b_j = Re(conj(rho) (Q_j - G_j P / Ss)); delta = A^-1 b
+    if (!(Ss > 0.f)) return;
+    const float rr = Pr / Ss, ri = Pi / Ss, r2 = rr * rr + ri * ri;
+    const float A11 = r2 * (H11 - G1 * G1 / Ss), A12 = r2 * (H12 - G1 * G2 / Ss), A22 = r2 * (H22 - G2 * G2 / Ss);
+    const float c1r = Q1r - G1 * Pr / Ss, c1i = Q1i - G1 * Pi / Ss;
+    const float c2r = Q2r - G2 * Pr / Ss, c2i = Q2i - G2 * Pi / Ss;
+    const float b1 = rr * c1r + ri * c1i, b2 = rr * c2r + ri * c2i;
+    const float det = A11 * A22 - A12 * A12;
+    if (a.pd) a.pd[v] = sqrtf(Pr * Pr + Pi * Pi) / sqrtf(Ss);
+    if (a.m0) a.m0[v] = sqrtf(r2);
+    if (!a.update || !(fabsf(det) > 0.f) || !isfinite(det)) return;
+    float d1 = (A22 * b1 - A12 * b2) / det, d2 = (A11 * b2 - A12 * b1) / det;
+    // trust region: at most max_rel_step of each parameter per iteration
+    const float lim1 = a.max_rel_step * T1, lim2 = a.max_rel_step * T2;
+    d1 = fminf(fmaxf(d1, -lim1), lim1);
+    d2 = fminf(fmaxf(d2, -lim2), lim2);
+    if (!isfinite(d1) || !isfinite(d2)) return;
+    float n1 = T1 + d1, n2 = T2 + d2;
+    n2 = fmaxf(n2, 1e-3f);
+    n1 = fmaxf(n1, n2 * (1.f + 1e-4f));  // keep T1 > T2 > 0
+    a.theta[v * 3] = n1;
+    a.theta[v * 3 + 1] = n2;
+}
+
+static void choose(int w, int *L, int *S) {
+    int bL = 32, bS = kMaxS, pad = 1 << 30;
+    for (int s = kMaxS; s >= 1; s--)
+        for (int l = 1; l <= 32; l *= 2)
+            if (l * s >= w) {
+                if (l * s - w < pad) { pad = l * s - w; bL = l; bS = s; }
+                break;
+            }
+    *L = bL;
+    *S = bS;
+}
+
+#define SNAPMRF_GRAD_DISPATCH(KERNEL, S, GRID, ST, ARGS)                   \
+    switch (S) {                                                          \
+    case 1: KERNEL<1><<<GRID, kThreads, 0, ST>>>(ARGS); break;            \
+    case 2: KERNEL<2><<<GRID, kThreads, 0, ST>>>(ARGS); break;            \
+    case 3: KERNEL<3><<<GRID, kThreads, 0, ST>>>(ARGS); break;            \
+    case 4: KERNEL<4><<<GRID, kThreads, 0, ST>>>(ARGS); break;            \
+    case 5: KERNEL<5><<<GRID, kThreads, 0, ST>>>(ARGS); break;            \
+    case 6: KERNEL<6><<<GRID, kThreads, 0, ST>>>(ARGS); break;            \
+    case 7: KERNEL<7><<<GRID, kThreads, 0, ST>>>(ARGS); break;            \
+    default: KERNEL<8><<<GRID, kThreads, 0, ST>>>(ARGS); break;           \
+    }
+
+// Schedule of the real-valued recursion on the device; fails unless every
+// RF phase is 0.
+static int upload_schedule(DeviceScratch &buf, Schedule *sc, const float *h_mrf, size_t nreps, size_t NREPS,
+                           cudaStream_t st, const char *who) {
+    for (size_t t = 0; t < nreps; t++)
+        if (h_mrf[NREPS + t] != 0.f)
+            SNAPMRF_FAIL(SNAPMRF_ERR_UNSUPPORTED, "%s: RF phases must all be 0 (real-valued recursion)", who);
+    SNAPMRF_CUDA(buf.alloc(3 * nreps * sizeof(float), st));
+    float *h = static_cast<float *>(stage_acquire(3 * nreps * sizeof(float)));
+    if (!h) SNAPMRF_FAIL(SNAPMRF_ERR_ALLOC, "%s: cannot allocate a pinned staging buffer", who);
+    memcpy(h, h_mrf, nreps * sizeof(float));
+    memcpy(h + nreps, h_mrf + 2 * NREPS, nreps * sizeof(float));
+    memcpy(h + 2 * nreps, h_mrf + 3 * NREPS, nreps * sizeof(float));
+    SNAPMRF_CUDA(cudaMemcpyAsync(buf.ptr, h, 3 * nreps * sizeof(float), cudaMemcpyHostToDevice, st));
+    SNAPMRF_CUDA(stage_release(st));
+    sc->alpha = buf.as<float>();
+    sc->TR = sc->alpha + nreps;
+    sc->TE = sc->TR + nreps;
+    sc->nreps = (int)nreps;
+    return SNAPMRF_OK;
+}
+
+// 1 for epg_fisp (dephasing shift every TR), 0 for epg_sr, -1 otherwise.
+static int echo_shift(const char *echo_type) {
+    if (echo_type && !strcmp(echo_type, "epg_fisp")) return 1;
+    if (echo_type && !strcmp(echo_type, "epg_sr")) return 0;
+    return -1;
+}
+
+}  // namespace grad
+}  // namespace snapmrf
+
+using namespace snapmrf;
+using namespace snapmrf::grad;
+
+extern "C" int snapmrf_epg_adjoint(const float *d_params, int nparams, const float *h_mrf, size_t nreps,
+                                   size_t NREPS, size_t natoms, int nstates, const char *echo_type,
+                                   const float *d_grad_signal, float *d_signal, float *d_grad_params,
+                                   float *d_grad_alpha, float *d_grad_alpha_atoms, int checkpoint_every,
+                                   void *stream) {
+    cudaStream_t st = (cudaStream_t)stream;
+    if (!d_params || !h_mrf || !d_grad_signal || !d_grad_params)
+        SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "epg_adjoint: null pointer");
+    if (nparams < 4 || nreps == 0 || nreps > NREPS || natoms == 0 || nstates < 1 || nstates > 32 * kMaxS)
+        SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "epg_adjoint: bad sizes");
+    if (nreps > 0x7fffffff) SNAPMRF_FAIL(SNAPMRF_ERR_UNSUPPORTED, "epg_adjoint: too many time points");
+    const int shift = echo_shift(echo_type);
+    if (shift < 0) SNAPMRF_FAIL(SNAPMRF_ERR_ECHO_TYPE, "epg_adjoint: echo type must be epg_fisp or epg_sr");
+    DeviceScratch sbuf;
+    Schedule sc;
+    int rc = upload_schedule(sbuf, &sc, h_mrf, nreps, NREPS, st, "epg_adjoint");
+    if (rc) return rc;
+    int L, S;
+    choose(nstates, &L, &S);
+    int C = checkpoint_every > 0 ? checkpoint_every : (int)std::max(1.0, std::ceil(std::sqrt((double)nreps)));
+    int nckpt = (int)((nreps + C - 1) / C);
+    const long long LS = (long long)L * S;
+    DeviceScratch work;
+    size_t ck = (size_t)natoms * nckpt * 3 * LS, sg = (size_t)natoms * C * 3 * LS;
+    size_t ga = d_grad_alpha_atoms ? 0 : (size_t)natoms * nreps;
+    size_t part = d_grad_alpha ? (size_t)kSplits * nreps : 0;
+    SNAPMRF_CUDA(work.alloc((ck + sg + ga + part) * sizeof(float), st));
+    AdjArgs a;
+    a.sch = sc;
+    a.params = d_params;
+    a.nparams = nparams;
+    a.n = (long long)natoms;
+    a.w = nstates;
+    a.L = L;
+    a.shift = shift;
+    a.gsig = reinterpret_cast<const float2 *>(d_grad_signal);
+    a.sig = reinterpret_cast<float2 *>(d_signal);
+    a.gparams = d_grad_params;
+    a.ckpt = work.as<float>();
+    a.seg = a.ckpt + ck;
+    a.galpha_atoms = d_grad_alpha_atoms ? d_grad_alpha_atoms : a.seg + sg;
+    a.C = C;
+    a.nckpt = nckpt;
+    const int apc = kThreads / L;
+    dim3 grid((unsigned)((natoms + apc - 1) / apc));
+    SNAPMRF_GRAD_DISPATCH(adjoint_kernel, S, grid, st, a);
+    SNAPMRF_LAUNCH_CHECK();
+    if (d_grad_alpha) {
+        float *partial = a.ckpt + ck + sg + ga;
+        dim3 pg((unsigned)((nreps + 127) / 128), kSplits);
+        sum_columns_partial_kernel<<<pg, 128, 0, st>>>(partial, a.galpha_atoms, (long long)natoms, (int)nreps);
+        SNAPMRF_LAUNCH_CHECK();
+        sum_columns_final_kernel<<<(unsigned)((nreps + 127) / 128), 128, 0, st>>>(d_grad_alpha, partial, (int)nreps);
+        SNAPMRF_LAUNCH_CHECK();
+    }
+    return SNAPMRF_OK;
+}
+
+extern "C" int snapmrf_refine_gn(float *d_theta, const float *img, size_t img_stride, const float *h_mrf,
+                                 size_t nreps, size_t NREPS, size_t nvoxels, int nstates, const char *echo_type,
+                                 int iterations, float max_rel_step, float *d_pd, float *d_m0, void *stream) {
+    cudaStream_t st = (cudaStream_t)stream;
+    if (!d_theta || !img || !h_mrf) SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "refine_gn: null pointer");
+    if (nreps == 0 || nreps > NREPS || nvoxels == 0 || nstates < 1 || nstates > 32 * kMaxS || iterations < 0)
+        SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "refine_gn: bad sizes");
+    if (!img_stride) img_stride = nreps;
+    const int shift = echo_shift(echo_type);
+    if (shift < 0) SNAPMRF_FAIL(SNAPMRF_ERR_ECHO_TYPE, "refine_gn: echo type must be epg_fisp or epg_sr");
+    DeviceScratch sbuf;
+    Schedule sc;
+    int rc = upload_schedule(sbuf, &sc, h_mrf, nreps, NREPS, st, "refine_gn");
+    if (rc) return rc;
+    int L, S;
+    choose(nstates, &L, &S);
+    GnArgs a;
+    a.sch = sc;
+    a.nvox = (long long)nvoxels;
+    a.w = nstates;
+    a.L = L;
+    a.shift = shift;
+    a.img = reinterpret_cast<const float2 *>(img);
+    a.img_stride = (long long)img_stride;
+    a.theta = d_theta;
+    a.max_rel_step = max_rel_step > 0.f ? max_rel_step : 0.2f;
+    const int apc = kThreads / L;
+    dim3 grid((unsigned)((nvoxels + apc - 1) / apc));
+    for (int it = 0; it <= iterations; it++) {
+        // the last pass only evaluates PD and M0 at the final parameters
+        const bool last = it == iterations;
+        if (last && !d_pd && !d_m0) break;
+        a.pd = last ? d_pd : nullptr;
+        a.m0 = last ? d_m0 : nullptr;
+        a.update = last ? 0 : 1;
+        SNAPMRF_GRAD_DISPATCH(gn_step_kernel, S, grid, st, a);
+        SNAPMRF_LAUNCH_CHECK();
+    }
+    return SNAPMRF_OK;
+}

@@ -1,0 +1,253 @@
+"""Derivative kernels on the GPU (snapmrf_epg_adjoint, snapmrf_refine_gn)
+against the FP64 forward-mode oracle, central differences and
+torch.autograd.gradcheck."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def schedule(T, seed=0, sr=False):
+    rng = np.random.default_rng(seed)
+    a = np.deg2rad(5 + 55 * np.abs(np.sin(np.pi * np.arange(T) / 230)) + rng.uniform(0, 3, T))
+    if sr:
+        a[::50] = np.deg2rad(90)
+    tr = rng.uniform(11, 15, T)
+    te = tr * rng.uniform(0.3, 0.6, T)
+    return np.array([a, np.zeros(T), tr, te], np.float32)
+
+
+def atoms_params(n, seed=1):
+    rng = np.random.default_rng(seed)
+    t1 = rng.uniform(300, 2500, n)
+    t2 = rng.uniform(20, 250, n)
+    b1 = rng.uniform(0.7, 1.2, n)
+    return np.stack([t1, t2, np.zeros(n), b1], 1).astype(np.float32)
+
+
+def run_adjoint(snap, params, h, nstates, echo, gsig, checkpoint_every=0, per_atom=True):
+    import torch
+    n, T = params.shape[0], h.shape[1]
+    d_params = torch.from_numpy(params).cuda()
+    d_g = torch.from_numpy(np.ascontiguousarray(gsig.astype(np.complex64)).view(np.float32)).cuda()
+    d_sig = torch.full((n, T, 2), 7.0, device="cuda")
+    d_gp = torch.full((n, 3), 7.0, device="cuda")
+    d_ga = torch.full((T,), 7.0, device="cuda")
+    d_gaa = torch.full((n, T), 7.0, device="cuda") if per_atom else None
+    snap.epg_adjoint(d_params, h, T, T, n, d_g, d_gp, 4, nstates, echo, d_signal=d_sig, d_grad_alpha=d_ga,
+                     d_grad_alpha_atoms=d_gaa, checkpoint_every=checkpoint_every)
+    torch.cuda.synchronize()
+    s = d_sig.cpu().numpy()
+    return (s[..., 0] + 1j * s[..., 1], d_gp.cpu().numpy(), d_ga.cpu().numpy(),
+            None if d_gaa is None else d_gaa.cpu().numpy())
+
+
+@pytest.mark.parametrize("echo", ["epg_fisp", "epg_sr"])
+@pytest.mark.parametrize("nstates", [1, 2, 7, 30, 50])
+def test_adjoint_matches_fp64_forward_mode(snap, oracle, echo, nstates):
+    """dL/dT1, dL/dT2, dL/dB1 and dL/dalpha (along a random direction) of
+    L = sum |s - y|^2 agree with the FP64 dual-number oracle to 1e-3 of the
+    gradient's scale."""
+    T = 400
+    h = schedule(T, seed=nstates, sr=echo == "epg_sr")
+    params = atoms_params(5, seed=nstates)
+    rng = np.random.default_rng(7)
+    ys, ref_sig = [], []
+    for p in params:
+        s, _, _, _ = oracle.fisp_jvp((p[0], p[1], p[3]), (0, 0, 0), h, nstates=nstates, echo=echo)
+        ref_sig.append(s)
+        ys.append(1j * s * rng.uniform(0.5, 1.5) + 0.02 * (rng.standard_normal(T) + 1j * rng.standard_normal(T)))
+    ys = np.array(ys)
+    ref_sig = np.array(ref_sig)
+    # dL/ds = 2 (s - y), with s the oracle's signal
+    gsig = 2 * (1j * ref_sig - ys)
+    sig, gp, ga, gaa = run_adjoint(snap, params, h, nstates, echo, gsig)
+    assert np.abs(sig.real).max() == 0
+    np.testing.assert_allclose(sig.imag, ref_sig, rtol=0, atol=2e-5 * np.abs(ref_sig).max())
+    v = rng.standard_normal(T)
+    for i, p in enumerate(params):
+        th = (p[0], p[1], p[3])
+        for k, tg in enumerate(((1, 0, 0), (0, 1, 0), (0, 0, 1))):
+            _, ds, _, w = oracle.fisp_jvp(th, tg, h, nstates=nstates, echo=echo, y=ys[i])
+            # scale of the sum's terms, for gradients that cancel to near 0
+            scale = float(np.abs(gsig[i].imag) @ np.abs(ds))
+            assert abs(gp[i, k] - w) <= 1e-3 * abs(w) + 1e-4 * scale, (i, k, gp[i, k], w, scale)
+        wa = oracle.fisp_jvp(th, (0, 0, 0), h, nstates=nstates, echo=echo, dalpha=v, y=ys[i])[3]
+        got = float(np.dot(gaa[i].astype(np.float64), v))
+        scale = float(np.abs(gaa[i]).astype(np.float64) @ np.abs(v))
+        assert abs(got - wa) <= 1e-3 * scale, (i, got, wa, scale)
+    np.testing.assert_allclose(ga, gaa.astype(np.float64).sum(0), rtol=1e-5, atol=1e-5 * np.abs(gaa).max())
+
+
+def test_adjoint_checkpoint_interval_does_not_change_results(snap):
+    T, w = 257, 20
+    h = schedule(T, seed=3)
+    params = atoms_params(37, seed=3)
+    rng = np.random.default_rng(3)
+    gsig = rng.standard_normal((37, T)) + 1j * rng.standard_normal((37, T))
+    base = run_adjoint(snap, params, h, w, "epg_fisp", gsig, checkpoint_every=0)
+    for c in (1, 5, 64, T, 10 * T):
+        other = run_adjoint(snap, params, h, w, "epg_fisp", gsig, checkpoint_every=c)
+        for a, b in zip(base, other):
+            np.testing.assert_array_equal(a, b)
+
+
+def test_adjoint_signal_equals_dictionary(snap):
+    """The adjoint's forward sweep gives the atoms snapmrf_mrf_dict gives
+    (one B1 block per atom)."""
+    from gpu_util import run_dict
+    T, w = 300, 40
+    h = schedule(T, seed=4)
+    params = atoms_params(50, seed=4)
+    sig, _, _, _ = run_adjoint(snap, params, h, w, "epg_fisp", np.zeros((50, T)))
+    ref = run_dict(snap, "epg_fisp", params, h, T, natoms=1, nstates=w, flags=snap.DICT_ALL_B1_BLOCKS)
+    rel = np.abs(sig - ref).max(axis=1) / np.abs(ref).max(axis=1)
+    assert rel.max() < 2e-6
+
+
+def test_adjoint_vs_central_differences_of_the_dictionary(snap):
+    """Gradient of L = sum_t w_t Im s_t against central differences of
+    snapmrf_mrf_dict itself (FP32, relative steps 1e-3)."""
+    from gpu_util import run_dict
+    T, w = 300, 25
+    h = schedule(T, seed=5)
+    params = atoms_params(4, seed=5)
+    rng = np.random.default_rng(5)
+    wt = rng.standard_normal(T)
+    _, gp, _, _ = run_adjoint(snap, params, h, w, "epg_fisp", np.broadcast_to(1j * wt, (4, T)))
+    for k, col in enumerate((0, 1, 3)):
+        hp, hm = params.copy(), params.copy()
+        step = 1e-3 * params[:, col]
+        hp[:, col] += step
+        hm[:, col] -= step
+        sp = run_dict(snap, "epg_fisp", hp, h, T, natoms=1, nstates=w, flags=snap.DICT_ALL_B1_BLOCKS)
+        sm = run_dict(snap, "epg_fisp", hm, h, T, natoms=1, nstates=w, flags=snap.DICT_ALL_B1_BLOCKS)
+        fd = ((sp.imag.astype(np.float64) - sm.imag) @ wt) / (hp[:, col].astype(np.float64) - hm[:, col])
+        np.testing.assert_allclose(gp[:, k], fd, rtol=1e-2, atol=1e-3 * np.abs(fd).max())
+
+
+def test_autograd_gradcheck(snap):
+    import torch
+    from snapmrf_b200.autograd import EPGSignal
+    T, w = 48, 12
+    h = schedule(T, seed=6)
+    base = torch.tensor(atoms_params(2, seed=6), device="cuda")
+    scale = torch.tensor([1000.0, 100.0, 1.0, 1.0], device="cuda")
+    u = (base / scale).clone().requires_grad_(True)
+    alpha = torch.tensor(h[0], device="cuda").requires_grad_(True)
+
+    def f(u_, a_):
+        return EPGSignal.apply(u_ * scale, a_, h, w, "epg_fisp")
+
+    assert torch.autograd.gradcheck(f, (u, alpha), eps=1e-3, atol=2e-3, rtol=2e-2, check_undefined_grad=False)
+    # and the same through a scalar loss, against the oracle
+    from oracle import oracle as orc
+    y = torch.randn((2, T, 2), device="cuda", generator=torch.Generator("cuda").manual_seed(0))
+    loss = ((f(u, alpha) - y) ** 2).sum()
+    loss.backward()
+    p = (u.detach() * scale).cpu().numpy()
+    yc = y.cpu().numpy()
+    yc = yc[..., 0] + 1j * yc[..., 1]
+    for i in range(2):
+        want = orc.fisp_jvp((p[i, 0], p[i, 1], p[i, 3]), (1000.0, 0, 0), h, nstates=w, y=yc[i])[3]
+        assert abs(u.grad[i, 0].item() - want) <= 1e-3 * abs(want) + 1e-4
+
+
+def test_adjoint_rejects_unsupported_inputs(snap):
+    import torch
+    T = 20
+    h = schedule(T)
+    d_params = torch.from_numpy(atoms_params(2)).cuda()
+    g = torch.zeros((2, T, 2), device="cuda")
+    gp = torch.zeros((2, 3), device="cuda")
+    with pytest.raises(snap.SnapMRFError):
+        snap.epg_adjoint(d_params, h, T, T, 2, g, gp, 4, 10, "epg_ssfp")
+    hp = h.copy()
+    hp[1, 3] = 0.5
+    with pytest.raises(snap.SnapMRFError):
+        snap.epg_adjoint(d_params, hp, T, T, 2, g, gp, 4, 10, "epg_fisp")
+    with pytest.raises(snap.SnapMRFError):
+        snap.epg_adjoint(d_params, h, T, T, 2, g, gp, 4, 300, "epg_fisp")
+
+
+# --------------------------------------------------------------------------
+# Gauss-Newton refinement
+# --------------------------------------------------------------------------
+
+def gn_step_fp64(orc, theta, x, h, w, echo="epg_fisp"):
+    """One projected Gauss-Newton step in FP64 from the oracle's tangents."""
+    s, d1, _, _ = orc.fisp_jvp(theta, (1, 0, 0), h, nstates=w, echo=echo)
+    _, d2, _, _ = orc.fisp_jvp(theta, (0, 1, 0), h, nstates=w, echo=echo)
+    s, J = 1j * s, np.stack([1j * d1, 1j * d2], 1)
+    rho = np.vdot(s, x) / np.vdot(s, s)
+    ss = np.vdot(s, s).real
+    Pj = J - np.outer(s, (s.conj() @ J) / ss)
+    A = (abs(rho) ** 2) * (Pj.conj().T @ Pj).real
+    b = (np.conj(rho) * (Pj.conj().T @ x)).real
+    return np.linalg.solve(A, b), abs(rho), abs(np.vdot(s, x)) / np.sqrt(ss)
+
+
+def run_gn(snap, theta, img, h, w, iterations, echo="epg_fisp", max_rel_step=0.2):
+    import torch
+    d_theta = torch.from_numpy(np.ascontiguousarray(theta, np.float32)).cuda()
+    d_img = torch.from_numpy(np.ascontiguousarray(img.astype(np.complex64)).view(np.float32)).cuda()
+    n = theta.shape[0]
+    d_pd = torch.full((n,), -1.0, device="cuda")
+    d_m0 = torch.full((n,), -1.0, device="cuda")
+    snap.refine_gn(d_theta, d_img, h, h.shape[1], h.shape[1], n, w, echo, iterations=iterations,
+                   max_rel_step=max_rel_step, d_pd=d_pd, d_m0=d_m0)
+    torch.cuda.synchronize()
+    return d_theta.cpu().numpy(), d_pd.cpu().numpy(), d_m0.cpu().numpy()
+
+
+def synthetic_voxels(orc, n, h, w, seed, echo="epg_fisp", noise=0.0):
+    rng = np.random.default_rng(seed)
+    truth = atoms_params(n, seed=seed)
+    rho = rng.uniform(0.5, 2, n) * np.exp(1j * rng.uniform(0, 6.28, n))
+    x = []
+    for p, r in zip(truth, rho):
+        s, _, _, _ = orc.fisp_jvp((p[0], p[1], p[3]), (0, 0, 0), h, nstates=w, echo=echo)
+        x.append(r * 1j * s + noise * (rng.standard_normal(len(s)) + 1j * rng.standard_normal(len(s))))
+    return truth, rho, np.array(x)
+
+
+@pytest.mark.parametrize("echo", ["epg_fisp", "epg_sr"])
+def test_gn_step_matches_fp64_step(snap, oracle, echo):
+    T, w = 300, 30
+    h = schedule(T, seed=8, sr=echo == "epg_sr")
+    truth, rho, x = synthetic_voxels(oracle, 6, h, w, seed=8, echo=echo, noise=0.01)
+    rng = np.random.default_rng(9)
+    theta0 = np.stack([truth[:, 0] * rng.uniform(0.95, 1.05, 6), truth[:, 1] * rng.uniform(0.95, 1.05, 6),
+                       truth[:, 3]], 1).astype(np.float32)
+    got, _, _ = run_gn(snap, theta0, x, h, w, 1, echo=echo, max_rel_step=1e6)
+    for i in range(6):
+        d, _, _ = gn_step_fp64(oracle, tuple(theta0[i].astype(np.float64)), x[i], h, w, echo)
+        step = got[i, :2].astype(np.float64) - theta0[i, :2]
+        np.testing.assert_allclose(step, d, rtol=2e-3, atol=2e-3 * np.abs(d).max() + 1e-3)
+        assert got[i, 2] == theta0[i, 2]
+
+
+def test_gn_recovers_off_grid_parameters(snap, oracle):
+    T, w = 500, 40
+    h = schedule(T, seed=10)
+    truth, rho, x = synthetic_voxels(oracle, 64, h, w, seed=10)
+    rng = np.random.default_rng(11)
+    theta0 = np.stack([truth[:, 0] * rng.uniform(0.9, 1.1, 64), truth[:, 1] * rng.uniform(0.9, 1.1, 64),
+                       truth[:, 3]], 1).astype(np.float32)
+    got, pd, m0 = run_gn(snap, theta0, x, h, w, 5)
+    np.testing.assert_allclose(got[:, 0], truth[:, 0], rtol=2e-3)
+    np.testing.assert_allclose(got[:, 1], truth[:, 1], rtol=2e-3)
+    np.testing.assert_allclose(m0, np.abs(rho), rtol=2e-3)
+    for i in range(64):
+        s, _, _, _ = oracle.fisp_jvp((truth[i, 0], truth[i, 1], truth[i, 3]), (0, 0, 0), h, nstates=w)
+        assert abs(pd[i] - abs(rho[i]) * np.linalg.norm(s)) <= 2e-3 * pd[i]
+
+
+def test_gn_zero_iterations_only_evaluates(snap, oracle):
+    T, w = 200, 20
+    h = schedule(T, seed=12)
+    truth, rho, x = synthetic_voxels(oracle, 10, h, w, seed=12)
+    theta0 = np.stack([truth[:, 0], truth[:, 1], truth[:, 3]], 1).astype(np.float32)
+    got, pd, m0 = run_gn(snap, theta0, x, h, w, 0)
+    np.testing.assert_array_equal(got, theta0)
+    np.testing.assert_allclose(m0, np.abs(rho), rtol=1e-4)

@@ -68,3 +68,47 @@ def test_oracle_b1_blocks_and_normalize(oracle):
     h2[0] = (h[0] * np.float32(0.8)).astype(np.float32)
     single = oracle.dict_atoms("epg_fisp", base[:, :] + [0, 0, 0, 1], h2, 50, nstates=20)
     np.testing.assert_allclose(atoms[0] * norms[0], single[0], rtol=1e-12, atol=1e-15)
+
+
+@pytest.mark.parametrize("echo", ["epg_fisp", "epg_sr"])
+def test_oracle_forward_mode_matches_dictionary_and_differences(oracle, echo):
+    """The FP64 dual-number recursion (the derivative oracle) gives the
+    dictionary oracle's atoms, and its tangents agree with central
+    differences of itself."""
+    rng = np.random.default_rng(0)
+    T, w = 300, 30
+    a = np.deg2rad(10 + 50 * np.abs(np.sin(np.pi * np.arange(T) / 250)))
+    tr = rng.uniform(11, 15, T)
+    h = np.array([a, np.zeros(T), tr, tr / 2], np.float32)
+    th = (900.0, 60.0, 0.95)
+    s, _, _, _ = oracle.fisp_jvp(th, (0, 0, 0), h, nstates=w, echo=echo)
+    params = np.array([[th[0], th[1], 0, th[2]]], np.float32)
+    at = oracle.dict_atoms(echo, params, h, T, nstates=w, flags=oracle.ALL_B1_BLOCKS)[0]
+    assert np.abs(at.real).max() == 0
+    assert np.abs(at.imag - s).max() < 1e-6 * np.abs(s).max()
+    y = s * 0.8j + 0.01 * rng.standard_normal(T)
+    for i, step in ((0, 1.0), (1, 0.1), (2, 1e-4)):
+        tg = [0.0, 0.0, 0.0]
+        tg[i] = 1.0
+        _, ds, L, dL = oracle.fisp_jvp(th, tg, h, nstates=w, echo=echo, y=y)
+        tp, tm = list(th), list(th)
+        tp[i] += step
+        tm[i] -= step
+        sp, _, Lp, _ = oracle.fisp_jvp(tp, (0, 0, 0), h, nstates=w, echo=echo, y=y)
+        sm, _, Lm, _ = oracle.fisp_jvp(tm, (0, 0, 0), h, nstates=w, echo=echo, y=y)
+        assert np.abs(ds - (sp - sm) / (2 * step)).max() < 1e-5 * np.abs(ds).max()
+        assert abs(dL - (Lp - Lm) / (2 * step)) < 1e-5 * abs(dL) + 1e-9
+    v = rng.standard_normal(T)
+    _, ds, _, _ = oracle.fisp_jvp(th, (0, 0, 0), h, nstates=w, echo=echo, dalpha=v)
+    hp, hm = h.astype(np.float64).copy(), h.astype(np.float64).copy()
+    # alpha is read as float32: difference along v with a step float32 resolves
+    e = 1e-3
+    hp[0] += e * v
+    hm[0] -= e * v
+    sp, _, _, _ = oracle.fisp_jvp(th, (0, 0, 0), hp.astype(np.float32), nstates=w, echo=echo)
+    sm, _, _, _ = oracle.fisp_jvp(th, (0, 0, 0), hm.astype(np.float32), nstates=w, echo=echo)
+    dv = (hp[0].astype(np.float32).astype(np.float64) - hm[0].astype(np.float32)) / (2 * e)
+    # the float32 rounding of the perturbed angles changes the effective direction
+    _, ds2, _, _ = oracle.fisp_jvp(th, (0, 0, 0), h, nstates=w, echo=echo, dalpha=dv)
+    assert np.abs(ds2 - (sp - sm) / (2 * e)).max() < 1e-4 * np.abs(ds2).max()
+    assert np.abs(ds2 - ds).max() < 1e-3 * np.abs(ds).max()
