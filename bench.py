@@ -242,7 +242,7 @@ def run_ours(args) -> None:
 
     d_index = torch.empty(nvox, dtype=torch.int64, device=dev)
 
-    def step(precision, ev=None):
+    def step(precision, ev=None, gn=0):
         if ev is not None:
             ev[0].record(stream)
         snap.MRF_dict(d_atoms, d_params, h_mrf, T, T, NATOMS, natoms, 4, NSTATES, "epg_fisp", flags=flags)
@@ -253,19 +253,25 @@ def run_ours(args) -> None:
                        topk=args.topk)
         if ev is not None:
             ev[2].record(stream)
+        if gn:
+            # Gauss-Newton refinement of the matched (T1, T2) at the B1 map
+            snap.refine_gn(d_maps, d_img, h_mrf, T, T, nvox, NSTATES, "epg_fisp", iterations=gn,
+                           d_b1map=d_b1)
+        if ev is not None:
+            ev[3].record(stream)
 
     def barrier():
         if world > 1:
             dist.barrier()
 
-    def timed(precision):
+    def timed(precision, gn=0):
         """W warm-up steps, then K steps between barriers and device syncs."""
         for _ in range(args.warmup):
-            step(precision)
+            step(precision, gn=gn)
         torch.cuda.synchronize()
         barrier()
         torch.cuda.synchronize()
-        evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+        evs = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
         launches0 = snap.kernel_launches()
         clk = ClockSampler(local)
         clk.start()
@@ -273,7 +279,7 @@ def run_ours(args) -> None:
         t_end = torch.cuda.Event(enable_timing=True)
         t_start.record(stream)
         for k in range(args.steps):
-            step(precision, evs[k])
+            step(precision, evs[k], gn=gn)
         t_end.record(stream)
         torch.cuda.synchronize()
         barrier()
@@ -282,11 +288,15 @@ def run_ours(args) -> None:
              "elapsed_ms": t_start.elapsed_time(t_end),
              "dict_ms": float(np.mean([e[0].elapsed_time(e[1]) for e in evs])),
              "match_ms": float(np.mean([e[1].elapsed_time(e[2]) for e in evs])),
+             "gn_ms": float(np.mean([e[2].elapsed_time(e[3]) for e in evs])),
              "maps": d_maps.cpu().numpy(), "index": d_index.cpu().numpy()}
         return r
 
     PRECS = {"fp32": snap.PREC_FP32, "bf16": snap.PREC_BF16, "fp16": snap.PREC_FP16}
     forms = {name: timed(p) for name, p in PRECS.items()}
+    # the tensor-core forms followed by Gauss-Newton refinement of (T1, T2)
+    gn_forms = {f"{name}+gn": timed(PRECS[name], gn=args.gn_iters) for name in ("bf16", "fp16")} \
+        if args.gn_iters > 0 else {}
     # argmax agreement with the FP32 form, counting a different atom as agreeing
     # when its exact FP32 score is within 1e-6 of the FP32 form's pick (an FP32
     # near-tie, where the FP32 form itself depends on summation order)
@@ -357,15 +367,20 @@ def run_ours(args) -> None:
 
     # max over ranks
     names = list(PRECS)
+    gnames = list(gn_forms)
     t = torch.tensor([elapsed_ms, e2e_ms, dict_ms, match_ms] +
-                     [forms[f]["elapsed_ms"] for f in names] + [forms[f]["match_ms"] for f in names],
+                     [forms[f]["elapsed_ms"] for f in names] + [forms[f]["match_ms"] for f in names] +
+                     [gn_forms[f]["elapsed_ms"] for f in gnames] + [gn_forms[f]["gn_ms"] for f in gnames],
                      dtype=torch.float64, device=dev)
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     t = t.tolist()
     elapsed_ms, e2e_ms, dict_ms, match_ms = t[:4]
     form_ms = dict(zip(names, t[4:4 + len(names)]))
-    form_match_ms = dict(zip(names, t[4 + len(names):]))
+    form_match_ms = dict(zip(names, t[4 + len(names):4 + 2 * len(names)]))
+    o = 4 + 2 * len(names)
+    gn_ms = dict(zip(gnames, t[o:o + len(gnames)]))
+    gn_stage_ms = dict(zip(gnames, t[o + len(gnames):]))
 
     if rank == 0:
         ms_per_step = elapsed_ms / args.steps
@@ -428,10 +443,16 @@ def run_ours(args) -> None:
             "gpu_launches": int(launches),
             "clocks": clocks,
             "maps_error_vs_truth": {
-                f: {"t1_median_rel": round(float(np.median(np.abs(forms[f]["maps"][:, 0] - vt1) / vt1)), 5),
-                    "t2_median_rel": round(float(np.median(np.abs(forms[f]["maps"][:, 1] - vt2) / vt2)), 5)}
-                for f in names},
+                f: {"t1_median_rel": round(float(np.median(np.abs(fm[f]["maps"][:, 0] - vt1) / vt1)), 5),
+                    "t2_median_rel": round(float(np.median(np.abs(fm[f]["maps"][:, 1] - vt2) / vt2)), 5)}
+                for fm in (forms, gn_forms) for f in fm},
         }
+        if gn_forms:
+            line["forms_refined"] = {
+                f: {"voxels_per_s": round(world * nvox / (gn_ms[f] / args.steps / 1e3), 1),
+                    "ms_per_step": round(gn_ms[f] / args.steps, 3), "gn_ms": round(gn_stage_ms[f], 3),
+                    "gn_iterations": args.gn_iters,
+                    "speedup_vs_fp32_form": round(form_ms["fp32"] / gn_ms[f], 3)} for f in gnames}
         if args.b1_blocks != 41 or args.nx != NX:
             line["config"]["workload"] = f"{WORKLOAD} reduced: {NATOMS // natoms} B1 blocks, {args.nx}x{args.nx} voxels"
         if not args.no_cpu_baseline:
@@ -530,6 +551,8 @@ def main() -> None:
     ap.add_argument("--b1-blocks", type=int, default=41,
                     help="reduced case for profiling: keep this many B1 blocks around 1.0")
     ap.add_argument("--nx", type=int, default=NX, help="reduced case for profiling: nx x nx voxels")
+    ap.add_argument("--gn-iters", type=int, default=2,
+                    help="Gauss-Newton iterations of the refined forms (0: skip them)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":

@@ -273,21 +273,28 @@ int snapmrf_epg_adjoint(const float *d_params, int nparams, const float *h_mrf, 
                         float *d_grad_alpha, float *d_grad_alpha_atoms, int checkpoint_every,
                         void *stream);
 
-/* Per-voxel Gauss-Newton refinement of (T1, T2) after matching.
+/* Per-voxel Gauss-Newton refinement of matched (T1, T2), in place.
  *
  * Model: voxel x = rho * s(T1, T2, B1) with rho complex, eliminated by
  * variable projection (rho = <s, x> / <s, s>); each iteration runs the
  * forward recursion with the tangents ds/dT1 and ds/dT2, then solves the
  * 2x2 normal equations of the projected residual.  Steps are clipped to
  * max_rel_step (0: 0.2) times the current value, and T1 > T2 > 0 is kept.
- * d_theta: device in/out [nvoxels][3] = T1, T2, B1 (B1 is not changed);
+ *
+ * d_maps: device in/out [nvoxels][nmaps] as snapmrf_mrf_match writes them
+ * (T1, T2, B0, B1, PD): T1 and T2 are refined at the voxel's B1, taken from
+ * d_b1map (optional device [nvoxels], the measured B1 map, then also written
+ * to column 3) or else from column 3 (1 when nmaps < 4); with nmaps >= 5
+ * column 4 is replaced by the PD of the refined signal, |<s, x>| / ||s||
+ * (the matching PD of a unit-norm atom).  Voxels whose maps are not finite
+ * or do not hold T1 > T2 > 0 are left as they are.
  * img: device complex [nvoxels][img_stride] (0 = nreps);
- * d_pd (optional out [nvoxels]): |<s, x>| / ||s||, the matching PD of a
- * normalised atom; d_m0 (optional out [nvoxels]): |rho|.  These two cost
- * one more forward pass at the final parameters. */
-int snapmrf_refine_gn(float *d_theta, const float *img, size_t img_stride, const float *h_mrf,
-                      size_t nreps, size_t NREPS, size_t nvoxels, int nstates, const char *echo_type,
-                      int iterations, float max_rel_step, float *d_pd, float *d_m0, void *stream);
+ * d_m0: optional out [nvoxels], |rho|.  PD, M0 and the B1 column cost one
+ * value-only forward pass at the final parameters. */
+int snapmrf_refine_gn(float *d_maps, int nmaps, const float *img, size_t img_stride,
+                      const float *d_b1map, const float *h_mrf, size_t nreps, size_t NREPS, size_t nvoxels, int nstates,
+                      const char *echo_type, int iterations, float max_rel_step, float *d_m0,
+                      void *stream);
 
 #ifdef __cplusplus
 }

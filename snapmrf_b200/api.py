@@ -103,8 +103,8 @@ def lib() -> C.CDLL:
                                                 vp, vp, vp]
         L.snapmrf_epg_adjoint.argtypes = [vp, C.c_int, vp, sz, sz, sz, C.c_int, C.c_char_p, vp, vp, vp,
                                           vp, vp, C.c_int, vp]
-        L.snapmrf_refine_gn.argtypes = [vp, vp, sz, vp, sz, sz, sz, C.c_int, C.c_char_p, C.c_int,
-                                        C.c_float, vp, vp, vp]
+        L.snapmrf_refine_gn.argtypes = [vp, C.c_int, vp, sz, vp, vp, sz, sz, sz, C.c_int, C.c_char_p, C.c_int,
+                                        C.c_float, vp, vp]
         _lib = L
     return _lib
 
@@ -364,12 +364,16 @@ def epg_adjoint(d_params, h_mrf, nreps: int, NREPS: int, natoms: int, d_grad_sig
                                      checkpoint_every, _stream_ptr(stream)))
 
 
-def refine_gn(d_theta, d_img, h_mrf, nreps: int, NREPS: int, nvoxels: int, nstates: int = 101,
-              echo_type: str = "epg_fisp", *, iterations: int = 2, max_rel_step: float = 0.2,
-              img_stride: int = 0, d_pd=None, d_m0=None, stream=None) -> None:
-    """Gauss-Newton refinement of matched (T1, T2): d_theta device float32
-    [nvoxels][3] (T1, T2, B1) in/out; d_img device complex64 voxels."""
+def refine_gn(d_maps, d_img, h_mrf, nreps: int, NREPS: int, nvoxels: int, nstates: int = 101,
+              echo_type: str = "epg_fisp", *, nmaps: int = NMAPS, iterations: int = 2,
+              max_rel_step: float = 0.2, img_stride: int = 0, d_b1map=None, d_m0=None,
+              stream=None) -> None:
+    """Gauss-Newton refinement of matched (T1, T2) in place: d_maps device
+    float32 [nvoxels][nmaps] (T1, T2, B0, B1, PD) as MRF_match writes them;
+    d_img device complex64 voxels; d_b1map optional device B1 map (else the
+    maps' B1 column)."""
     h_mrf = _schedule(h_mrf, NREPS)
-    _check(lib().snapmrf_refine_gn(_ptr(d_theta), _ptr(d_img), img_stride, h_mrf.ctypes.data, nreps, NREPS,
-                                   nvoxels, nstates, echo_type.encode(), iterations, max_rel_step, _ptr(d_pd),
+    _check(lib().snapmrf_refine_gn(_ptr(d_maps), nmaps, _ptr(d_img), img_stride, _ptr(d_b1map),
+                                   h_mrf.ctypes.data, nreps,
+                                   NREPS, nvoxels, nstates, echo_type.encode(), iterations, max_rel_step,
                                    _ptr(d_m0), _stream_ptr(stream)))

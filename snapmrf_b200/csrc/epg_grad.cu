@@ -347,113 +347,136 @@ struct GnArgs {
     int w, L, shift;
     const float2 *img;        // [nvox][img_stride]
     long long img_stride;
-    float *theta;             // [nvox][3] in/out: T1, T2, B1 (B1 fixed)
-    float *pd;                // optional out [nvox]: |<s, x>| / ||s||
+    float *maps;              // [nvox][nmaps] in/out: T1, T2, B0, B1, PD
+    int nmaps;
+    const float *b1map;       // optional [nvox]: B1 of each voxel
     float *m0;                // optional out [nvox]: |rho| with x ~ rho * s
     float max_rel_step;
-    int update;               // 0: only evaluate pd / m0
 };
 
-template <int S>
-struct Dual3 {
-    St<S> v, d1, d2;
-};
+// A voxel whose map holds no usable start (not finite, T2 <= 0, T1 <= T2)
+// is left as matched.
+__device__ __forceinline__ bool usable(float T1, float T2, float B1) {
+    return isfinite(T1) && isfinite(T2) && isfinite(B1) && T2 > 0.f && T1 > T2;
+}
 
-template <int S>
-__global__ void __launch_bounds__(kThreads) gn_step_kernel(GnArgs a) {
+// One Gauss-Newton iteration per voxel (TANGENTS) or, without tangents, the
+// final evaluation of PD and M0 at the current parameters.
+template <int S, bool TANGENTS>
+__global__ void __launch_bounds__(kThreads) gn_kernel(GnArgs a) {
     const int L = a.L;
     const int g = threadIdx.x / L, gl = threadIdx.x % L;
     const long long vox = (long long)blockIdx.x * (kThreads / L) + g;
-    const bool active = vox < a.nvox;
-    const long long v = active ? vox : 0;
+    const long long v = vox < a.nvox ? vox : a.nvox - 1;
     const bool lane0 = gl == 0;
-    const float T1 = a.theta[v * 3], T2 = a.theta[v * 3 + 1], B1 = a.theta[v * 3 + 2];
+    float *mp = a.maps + v * a.nmaps;
+    const float T1 = mp[0], T2 = mp[1];
+    const float B1 = a.b1map ? a.b1map[v] : (a.nmaps >= 4 ? mp[3] : 1.f);
+    // whole groups leave together, so the shuffles below see full groups
+    if (vox >= a.nvox || !usable(T1, T2, B1)) return;
     const int T = a.sch.nreps, w = a.w;
     const float2 *x = a.img + v * a.img_stride;
 
-    Dual3<S> s;
+    St<S> sv, s1, s2;
 #pragma unroll
     for (int j = 0; j < S; j++) {
-        s.v.p[j] = s.v.m[j] = s.v.z[j] = 0.f;
-        s.d1.p[j] = s.d1.m[j] = s.d1.z[j] = 0.f;
-        s.d2.p[j] = s.d2.m[j] = s.d2.z[j] = 0.f;
+        sv.p[j] = sv.m[j] = sv.z[j] = 0.f;
+        s1.p[j] = s1.m[j] = s1.z[j] = 0.f;
+        s2.p[j] = s2.m[j] = s2.z[j] = 0.f;
     }
-    if (lane0) s.v.z[0] = 1.f;
+    if (lane0) sv.z[0] = 1.f;
     // inner products (lane 0): Ss = <s,s>, P = <s,x>, G_j = <s,J_j>,
     // H_jk = <J_j,J_k>, Q_j = <J_j,x>; s_t = i f, J_jt = i df_j
     float Ss = 0.f, Pr = 0.f, Pi = 0.f, G1 = 0.f, G2 = 0.f, H11 = 0.f, H12 = 0.f, H22 = 0.f;
     float Q1r = 0.f, Q1i = 0.f, Q2r = 0.f, Q2i = 0.f;
+    const float r1 = 1.f / T1, r2 = 1.f / T2;
     for (int t = 0; t < T; t++) {
         const StepRF r = step_rf(a.sch.alpha[t] * B1);
-        rf_fwd<S>(s.v, r);
-        rf_fwd<S>(s.d1, r);
-        rf_fwd<S>(s.d2, r);
+        rf_fwd<S>(sv, r);
+        if (TANGENTS) {
+            rf_fwd<S>(s1, r);
+            rf_fwd<S>(s2, r);
+        }
         const float tr = a.sch.TR[t], te = a.sch.TE[t];
+#pragma unroll
         for (int pass = 0; pass < 2; pass++) {
             const float tt = pass == 0 ? te : tr - te;
-            const float E1 = expf(-tt / T1), E2 = expf(-tt / T2);
-            const float dE1 = E1 * tt / (T1 * T1), dE2 = E2 * tt / (T2 * T2);  // dE1/dT1, dE2/dT2
+            const float E1 = __expf(-tt * r1), E2 = __expf(-tt * r2);
+            if (TANGENTS) {
+                const float dE1 = E1 * tt * r1 * r1, dE2 = E2 * tt * r2 * r2;  // dE1/dT1, dE2/dT2
 #pragma unroll
-            for (int j = 0; j < S; j++) {
-                // product rule: d(E x) = dE x + E dx
-                s.d1.p[j] = E2 * s.d1.p[j];
-                s.d1.m[j] = E2 * s.d1.m[j];
-                s.d1.z[j] = fmaf(dE1, s.v.z[j], E1 * s.d1.z[j]);
-                s.d2.p[j] = fmaf(dE2, s.v.p[j], E2 * s.d2.p[j]);
-                s.d2.m[j] = fmaf(dE2, s.v.m[j], E2 * s.d2.m[j]);
-                s.d2.z[j] = E1 * s.d2.z[j];
+                for (int j = 0; j < S; j++) {
+                    // product rule: d(E x) = dE x + E dx
+                    s1.p[j] = E2 * s1.p[j];
+                    s1.m[j] = E2 * s1.m[j];
+                    s1.z[j] = fmaf(dE1, sv.z[j], E1 * s1.z[j]);
+                    s2.p[j] = fmaf(dE2, sv.p[j], E2 * s2.p[j]);
+                    s2.m[j] = fmaf(dE2, sv.m[j], E2 * s2.m[j]);
+                    s2.z[j] = E1 * s2.z[j];
+                }
+                if (lane0) s1.z[0] -= dE1;
             }
-            relax_fwd<S>(s.v, E1, E2, lane0);
-            if (lane0) s.d1.z[0] -= dE1;
+            relax_fwd<S>(sv, E1, E2, lane0);
             if (pass == 0) {
                 if (lane0) {
-                    const float f = s.v.p[0], d1 = s.d1.p[0], d2 = s.d2.p[0];
+                    const float f = sv.p[0];
                     const float2 xv = x[t];
                     Ss = fmaf(f, f, Ss);
                     Pr = fmaf(f, xv.y, Pr);
                     Pi = fmaf(-f, xv.x, Pi);
-                    G1 = fmaf(f, d1, G1);
-                    G2 = fmaf(f, d2, G2);
-                    H11 = fmaf(d1, d1, H11);
-                    H12 = fmaf(d1, d2, H12);
-                    H22 = fmaf(d2, d2, H22);
-                    Q1r = fmaf(d1, xv.y, Q1r);
-                    Q1i = fmaf(-d1, xv.x, Q1i);
-                    Q2r = fmaf(d2, xv.y, Q2r);
-                    Q2i = fmaf(-d2, xv.x, Q2i);
+                    if (TANGENTS) {
+                        const float d1 = s1.p[0], d2 = s2.p[0];
+                        G1 = fmaf(f, d1, G1);
+                        G2 = fmaf(f, d2, G2);
+                        H11 = fmaf(d1, d1, H11);
+                        H12 = fmaf(d1, d2, H12);
+                        H22 = fmaf(d2, d2, H22);
+                        Q1r = fmaf(d1, xv.y, Q1r);
+                        Q1i = fmaf(-d1, xv.x, Q1i);
+                        Q2r = fmaf(d2, xv.y, Q2r);
+                        Q2i = fmaf(-d2, xv.x, Q2i);
+                    }
                 }
                 if (a.shift) {
-                    shift_fwd<S>(s.v, gl, L, w);
-                    shift_fwd<S>(s.d1, gl, L, w);
-                    shift_fwd<S>(s.d2, gl, L, w);
+                    shift_fwd<S>(sv, gl, L, w);
+                    if (TANGENTS) {
+                        shift_fwd<S>(s1, gl, L, w);
+                        shift_fwd<S>(s2, gl, L, w);
+                    }
                 }
             }
         }
     }
-    if (!(lane0 && active)) return;
+    if (!lane0 || !(Ss > 0.f)) return;
+    if (!TANGENTS) {
+        // PD of a unit-norm atom (what matching reports) and |rho|
+        const float ip = sqrtf(Pr * Pr + Pi * Pi);
+        if (a.b1map && a.nmaps >= 4) mp[3] = B1;
+        if (a.nmaps >= 5) mp[4] = ip / sqrtf(Ss);
+        if (a.m0) a.m0[v] = ip / Ss;
+        return;
+    }
     // variable projection: rho = P / Ss; A_jk = |rho|^2 (H_jk - G_j G_k / Ss),
     // b_j = Re(conj(rho) (Q_j - G_j P / Ss)); delta = A^-1 b
-    if (!(Ss > 0.f)) return;
-    const float rr = Pr / Ss, ri = Pi / Ss, r2 = rr * rr + ri * ri;
-    const float A11 = r2 * (H11 - G1 * G1 / Ss), A12 = r2 * (H12 - G1 * G2 / Ss), A22 = r2 * (H22 - G2 * G2 / Ss);
+    const float rr = Pr / Ss, ri = Pi / Ss, rho2 = rr * rr + ri * ri;
+    const float A11 = rho2 * (H11 - G1 * G1 / Ss), A12 = rho2 * (H12 - G1 * G2 / Ss);
+    const float A22 = rho2 * (H22 - G2 * G2 / Ss);
     const float c1r = Q1r - G1 * Pr / Ss, c1i = Q1i - G1 * Pi / Ss;
     const float c2r = Q2r - G2 * Pr / Ss, c2i = Q2i - G2 * Pi / Ss;
     const float b1 = rr * c1r + ri * c1i, b2 = rr * c2r + ri * c2i;
     const float det = A11 * A22 - A12 * A12;
-    if (a.pd) a.pd[v] = sqrtf(Pr * Pr + Pi * Pi) / sqrtf(Ss);
-    if (a.m0) a.m0[v] = sqrtf(r2);
-    if (!a.update || !(fabsf(det) > 0.f) || !isfinite(det)) return;
+    if (!(fabsf(det) > 0.f) || !isfinite(det)) return;
     float d1 = (A22 * b1 - A12 * b2) / det, d2 = (A11 * b2 - A12 * b1) / det;
+    if (!isfinite(d1) || !isfinite(d2)) return;
     // trust region: at most max_rel_step of each parameter per iteration
     const float lim1 = a.max_rel_step * T1, lim2 = a.max_rel_step * T2;
     d1 = fminf(fmaxf(d1, -lim1), lim1);
     d2 = fminf(fmaxf(d2, -lim2), lim2);
-    if (!isfinite(d1) || !isfinite(d2)) return;
     float n1 = T1 + d1, n2 = T2 + d2;
     n2 = fmaxf(n2, 1e-3f);
     n1 = fmaxf(n1, n2 * (1.f + 1e-4f));  // keep T1 > T2 > 0
-    a.theta[v * 3] = n1;
-    a.theta[v * 3 + 1] = n2;
+    mp[0] = n1;
+    mp[1] = n2;
 }
 
 static void choose(int w, int *L, int *S) {
@@ -478,6 +501,18 @@ static void choose(int w, int *L, int *S) {
     case 6: KERNEL<6><<<GRID, kThreads, 0, ST>>>(ARGS); break;            \
     case 7: KERNEL<7><<<GRID, kThreads, 0, ST>>>(ARGS); break;            \
     default: KERNEL<8><<<GRID, kThreads, 0, ST>>>(ARGS); break;           \
+    }
+
+#define SNAPMRF_GRAD_DISPATCH2(KERNEL, S, B, GRID, ST, ARGS)                \
+    switch (S) {                                                          \
+    case 1: KERNEL<1, B><<<GRID, kThreads, 0, ST>>>(ARGS); break;         \
+    case 2: KERNEL<2, B><<<GRID, kThreads, 0, ST>>>(ARGS); break;         \
+    case 3: KERNEL<3, B><<<GRID, kThreads, 0, ST>>>(ARGS); break;         \
+    case 4: KERNEL<4, B><<<GRID, kThreads, 0, ST>>>(ARGS); break;         \
+    case 5: KERNEL<5, B><<<GRID, kThreads, 0, ST>>>(ARGS); break;         \
+    case 6: KERNEL<6, B><<<GRID, kThreads, 0, ST>>>(ARGS); break;         \
+    case 7: KERNEL<7, B><<<GRID, kThreads, 0, ST>>>(ARGS); break;         \
+    default: KERNEL<8, B><<<GRID, kThreads, 0, ST>>>(ARGS); break;        \
     }
 
 // Schedule of the real-valued recursion on the device; fails unless every
@@ -573,14 +608,18 @@ extern "C" int snapmrf_epg_adjoint(const float *d_params, int nparams, const flo
     return SNAPMRF_OK;
 }
 
-extern "C" int snapmrf_refine_gn(float *d_theta, const float *img, size_t img_stride, const float *h_mrf,
-                                 size_t nreps, size_t NREPS, size_t nvoxels, int nstates, const char *echo_type,
-                                 int iterations, float max_rel_step, float *d_pd, float *d_m0, void *stream) {
+extern "C" int snapmrf_refine_gn(float *d_maps, int nmaps, const float *img, size_t img_stride,
+                                 const float *d_b1map, const float *h_mrf, size_t nreps, size_t NREPS, size_t nvoxels, int nstates,
+                                 const char *echo_type, int iterations, float max_rel_step, float *d_m0,
+                                 void *stream) {
     cudaStream_t st = (cudaStream_t)stream;
-    if (!d_theta || !img || !h_mrf) SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "refine_gn: null pointer");
-    if (nreps == 0 || nreps > NREPS || nvoxels == 0 || nstates < 1 || nstates > 32 * kMaxS || iterations < 0)
+    if (!d_maps || !img || !h_mrf) SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "refine_gn: null pointer");
+    if (nmaps < 2 || nreps == 0 || nreps > NREPS || nvoxels == 0 || nstates < 1 || nstates > 32 * kMaxS ||
+        iterations < 0)
         SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "refine_gn: bad sizes");
+    if (nreps > 0x7fffffff) SNAPMRF_FAIL(SNAPMRF_ERR_UNSUPPORTED, "refine_gn: too many time points");
     if (!img_stride) img_stride = nreps;
+    if (img_stride < nreps) SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "refine_gn: img_stride < nreps");
     const int shift = echo_shift(echo_type);
     if (shift < 0) SNAPMRF_FAIL(SNAPMRF_ERR_ECHO_TYPE, "refine_gn: echo type must be epg_fisp or epg_sr");
     DeviceScratch sbuf;
@@ -597,18 +636,19 @@ extern "C" int snapmrf_refine_gn(float *d_theta, const float *img, size_t img_st
     a.shift = shift;
     a.img = reinterpret_cast<const float2 *>(img);
     a.img_stride = (long long)img_stride;
-    a.theta = d_theta;
+    a.maps = d_maps;
+    a.nmaps = nmaps;
+    a.b1map = d_b1map;
+    a.m0 = d_m0;
     a.max_rel_step = max_rel_step > 0.f ? max_rel_step : 0.2f;
     const int apc = kThreads / L;
     dim3 grid((unsigned)((nvoxels + apc - 1) / apc));
-    for (int it = 0; it <= iterations; it++) {
-        // the last pass only evaluates PD and M0 at the final parameters
-        const bool last = it == iterations;
-        if (last && !d_pd && !d_m0) break;
-        a.pd = last ? d_pd : nullptr;
-        a.m0 = last ? d_m0 : nullptr;
-        a.update = last ? 0 : 1;
-        SNAPMRF_GRAD_DISPATCH(gn_step_kernel, S, grid, st, a);
+    for (int it = 0; it < iterations; it++) {
+        SNAPMRF_GRAD_DISPATCH2(gn_kernel, S, true, grid, st, a);
+        SNAPMRF_LAUNCH_CHECK();
+    }
+    if (nmaps >= 5 || d_m0 || (d_b1map && nmaps >= 4)) {
+        SNAPMRF_GRAD_DISPATCH2(gn_kernel, S, false, grid, st, a);
         SNAPMRF_LAUNCH_CHECK();
     }
     return SNAPMRF_OK;

@@ -107,7 +107,7 @@ def test_adjoint_signal_equals_dictionary(snap):
 
 def test_adjoint_vs_central_differences_of_the_dictionary(snap):
     """Gradient of L = sum_t w_t Im s_t against central differences of
-    snapmrf_mrf_dict itself (FP32, relative steps 1e-3)."""
+    snapmrf_mrf_dict itself (FP32)."""
     from gpu_util import run_dict
     T, w = 300, 25
     h = schedule(T, seed=5)
@@ -115,15 +115,16 @@ def test_adjoint_vs_central_differences_of_the_dictionary(snap):
     rng = np.random.default_rng(5)
     wt = rng.standard_normal(T)
     _, gp, _, _ = run_adjoint(snap, params, h, w, "epg_fisp", np.broadcast_to(1j * wt, (4, T)))
-    for k, col in enumerate((0, 1, 3)):
+    # relative steps large enough for FP32 differences of ~1e-5 gradients
+    for k, (col, rel) in enumerate(((0, 1e-2), (1, 1e-2), (3, 1e-3))):
         hp, hm = params.copy(), params.copy()
-        step = 1e-3 * params[:, col]
+        step = rel * params[:, col]
         hp[:, col] += step
         hm[:, col] -= step
         sp = run_dict(snap, "epg_fisp", hp, h, T, natoms=1, nstates=w, flags=snap.DICT_ALL_B1_BLOCKS)
         sm = run_dict(snap, "epg_fisp", hm, h, T, natoms=1, nstates=w, flags=snap.DICT_ALL_B1_BLOCKS)
         fd = ((sp.imag.astype(np.float64) - sm.imag) @ wt) / (hp[:, col].astype(np.float64) - hm[:, col])
-        np.testing.assert_allclose(gp[:, k], fd, rtol=1e-2, atol=1e-3 * np.abs(fd).max())
+        np.testing.assert_allclose(gp[:, k], fd, rtol=1e-2, atol=1e-2 * np.abs(fd).max())
 
 
 def test_autograd_gradcheck(snap):
@@ -187,17 +188,22 @@ def gn_step_fp64(orc, theta, x, h, w, echo="epg_fisp"):
     return np.linalg.solve(A, b), abs(rho), abs(np.vdot(s, x)) / np.sqrt(ss)
 
 
-def run_gn(snap, theta, img, h, w, iterations, echo="epg_fisp", max_rel_step=0.2):
+def run_gn(snap, theta, img, h, w, iterations, echo="epg_fisp", max_rel_step=0.2, b1map=None):
+    """theta [n][3] = (T1, T2, B1) -> (T1, T2, B1) [n][3], PD, M0."""
     import torch
-    d_theta = torch.from_numpy(np.ascontiguousarray(theta, np.float32)).cuda()
-    d_img = torch.from_numpy(np.ascontiguousarray(img.astype(np.complex64)).view(np.float32)).cuda()
     n = theta.shape[0]
-    d_pd = torch.full((n,), -1.0, device="cuda")
+    maps = np.zeros((n, 5), np.float32)
+    maps[:, 0], maps[:, 1], maps[:, 3], maps[:, 4] = theta[:, 0], theta[:, 1], theta[:, 2], -1
+    d_maps = torch.from_numpy(maps).cuda()
+    d_img = torch.from_numpy(np.ascontiguousarray(img.astype(np.complex64)).view(np.float32)).cuda()
     d_m0 = torch.full((n,), -1.0, device="cuda")
-    snap.refine_gn(d_theta, d_img, h, h.shape[1], h.shape[1], n, w, echo, iterations=iterations,
-                   max_rel_step=max_rel_step, d_pd=d_pd, d_m0=d_m0)
+    d_b1 = None if b1map is None else torch.from_numpy(np.ascontiguousarray(b1map, np.float32)).cuda()
+    snap.refine_gn(d_maps, d_img, h, h.shape[1], h.shape[1], n, w, echo, iterations=iterations,
+                   max_rel_step=max_rel_step, d_b1map=d_b1, d_m0=d_m0)
     torch.cuda.synchronize()
-    return d_theta.cpu().numpy(), d_pd.cpu().numpy(), d_m0.cpu().numpy()
+    out = d_maps.cpu().numpy()
+    assert np.all(out[:, 2] == 0)
+    return out[:, [0, 1, 3]], out[:, 4], d_m0.cpu().numpy()
 
 
 def synthetic_voxels(orc, n, h, w, seed, echo="epg_fisp", noise=0.0):
@@ -251,3 +257,31 @@ def test_gn_zero_iterations_only_evaluates(snap, oracle):
     got, pd, m0 = run_gn(snap, theta0, x, h, w, 0)
     np.testing.assert_array_equal(got, theta0)
     np.testing.assert_allclose(m0, np.abs(rho), rtol=1e-4)
+
+
+def test_gn_leaves_unusable_voxels(snap, oracle):
+    T, w = 100, 10
+    h = schedule(T, seed=13)
+    truth, rho, x = synthetic_voxels(oracle, 5, h, w, seed=13)
+    theta0 = np.stack([truth[:, 0], truth[:, 1], truth[:, 3]], 1).astype(np.float32)
+    theta0[0, 0] = np.nan
+    theta0[1, 1] = 0
+    theta0[2, 0] = theta0[2, 1]  # T1 == T2
+    got, pd, m0 = run_gn(snap, theta0, x, h, w, 2)
+    np.testing.assert_array_equal(got[:3], theta0[:3])
+    assert np.all(pd[:3] == -1) and np.all(m0[:3] == -1)
+    assert np.all(pd[3:] > 0)
+
+
+def test_gn_uses_the_b1_map(snap, oracle):
+    """Maps matched at a quantised B1 block value, refined at the measured B1."""
+    T, w = 400, 30
+    h = schedule(T, seed=14)
+    truth, rho, x = synthetic_voxels(oracle, 32, h, w, seed=14)
+    rng = np.random.default_rng(15)
+    theta0 = np.stack([truth[:, 0] * rng.uniform(0.95, 1.05, 32), truth[:, 1] * rng.uniform(0.95, 1.05, 32),
+                       np.round(truth[:, 3] / 0.05) * 0.05], 1).astype(np.float32)
+    got, _, _ = run_gn(snap, theta0, x, h, w, 4, b1map=truth[:, 3])
+    np.testing.assert_array_equal(got[:, 2], truth[:, 3])
+    np.testing.assert_allclose(got[:, 0], truth[:, 0], rtol=2e-3)
+    np.testing.assert_allclose(got[:, 1], truth[:, 1], rtol=2e-3)
