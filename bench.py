@@ -551,7 +551,7 @@ def main() -> None:
     ap.add_argument("--b1-blocks", type=int, default=41,
                     help="reduced case for profiling: keep this many B1 blocks around 1.0")
     ap.add_argument("--nx", type=int, default=NX, help="reduced case for profiling: nx x nx voxels")
-    ap.add_argument("--gn-iters", type=int, default=2,
+    ap.add_argument("--gn-iters", type=int, default=1,
                     help="Gauss-Newton iterations of the refined forms (0: skip them)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)

@@ -22,6 +22,8 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -360,102 +362,220 @@ __device__ __forceinline__ bool usable(float T1, float T2, float B1) {
     return isfinite(T1) && isfinite(T2) && isfinite(B1) && T2 > 0.f && T1 > T2;
 }
 
-// One Gauss-Newton iteration per voxel (TANGENTS) or, without tangents, the
-// final evaluation of PD and M0 at the current parameters.
-template <int S, bool TANGENTS>
-__global__ void __launch_bounds__(kThreads) gn_kernel(GnArgs a) {
-    const int L = a.L;
-    const int g = threadIdx.x / L, gl = threadIdx.x % L;
-    const long long vox = (long long)blockIdx.x * (kThreads / L) + g;
-    const long long v = vox < a.nvox ? vox : a.nvox - 1;
-    const bool lane0 = gl == 0;
-    float *mp = a.maps + v * a.nmaps;
-    const float T1 = mp[0], T2 = mp[1];
-    const float B1 = a.b1map ? a.b1map[v] : (a.nmaps >= 4 ? mp[3] : 1.f);
-    // whole groups leave together, so the shuffles below see full groups
-    if (vox >= a.nvox || !usable(T1, T2, B1)) return;
-    const int T = a.sch.nreps, w = a.w;
-    const float2 *x = a.img + v * a.img_stride;
+// Packed state of the refinement: P pairs of EPG states per lane (slot
+// j = 2i + h of pair i is state k = gl * 2P + j), one set for the signal and
+// one for each tangent; two-wide FP32 instructions update a pair at once.
+template <int P>
+struct Pair3 {
+    float2 p[P], m[P], z[P];
+};
 
-    St<S> sv, s1, s2;
+template <int P>
+__device__ __forceinline__ void pz(Pair3<P> &x) {
 #pragma unroll
-    for (int j = 0; j < S; j++) {
-        sv.p[j] = sv.m[j] = sv.z[j] = 0.f;
-        s1.p[j] = s1.m[j] = s1.z[j] = 0.f;
-        s2.p[j] = s2.m[j] = s2.z[j] = 0.f;
+    for (int i = 0; i < P; i++) x.p[i] = x.m[i] = x.z[i] = make_float2(0.f, 0.f);
+}
+
+template <int P>
+__device__ __forceinline__ void p_rf(Pair3<P> &x, float2 c, float2 s, float2 S, float2 nS, float2 hS,
+                                     float2 nhS, float2 C) {
+#pragma unroll
+    for (int i = 0; i < P; i++) {
+        const float2 p = x.p[i], m = x.m[i], q = x.z[i];
+        x.p[i] = __ffma2_rn(nS, q, __ffma2_rn(s, m, __fmul2_rn(c, p)));
+        x.m[i] = __ffma2_rn(S, q, __ffma2_rn(c, m, __fmul2_rn(s, p)));
+        x.z[i] = __ffma2_rn(C, q, __ffma2_rn(nhS, m, __fmul2_rn(hS, p)));
     }
-    if (lane0) sv.z[0] = 1.f;
+}
+
+// Shift of one packed stream.  States k >= w hold zeros: F- needs no mask
+// (F-[w-1] takes the zero of F-[w]), F+ takes F+[w-1] into slot w, which
+// keep[] (0 at slot w, 1 elsewhere) clears.
+template <int P>
+__device__ __forceinline__ void p_shift(Pair3<P> &x, int gl, int L, int w, const float2 *keep) {
+    const unsigned full = 0xffffffffu;
+    const float up = __shfl_up_sync(full, x.p[P - 1].y, 1, L);
+    const float dn = __shfl_down_sync(full, x.m[0].x, 1, L);
+    const float old_m0 = x.m[0].x;
+#pragma unroll
+    for (int i = P - 1; i >= 1; i--) x.p[i] = make_float2(x.p[i - 1].y, x.p[i].x);
+    x.p[0] = make_float2(up, x.p[0].x);
+#pragma unroll
+    for (int i = 0; i < P - 1; i++) x.m[i] = make_float2(x.m[i].y, x.m[i + 1].x);
+    x.m[P - 1] = make_float2(x.m[P - 1].y, (gl == L - 1) ? 0.f : dn);
+    if (gl == 0) x.p[0].x = -((w == 1) ? old_m0 : x.m[0].x);
+#pragma unroll
+    for (int i = 0; i < P; i++) x.p[i] = __fmul2_rn(x.p[i], keep[i]);
+}
+
+// Per-step constants of one voxel, staged in shared memory per chunk.
+// Relaxation is diagonal in the EPG states with one factor for F+ and F-,
+// so it commutes with the dephasing shift: relax(TE), shift, relax(TR-TE)
+// equals shift, relax(TR), and the readout after relax(TE) is E2(TE) f+[0]
+// taken right after the RF pulse.
+struct GnStep {
+    float C, S;            // cos, sin of alpha_t * B1
+    float E1, E2;          // relaxation over TR
+    float dE1, dE2;        // dE1/dT1, dE2/dT2
+    float Ea, dEa;         // E2 over TE (readout) and dEa/dT2
+    float xr, xi;          // voxel sample
+};
+
+constexpr int kGnChunk = 16;
+
+// One Gauss-Newton iteration per voxel (TANGENTS) or, without tangents, the
+// final evaluation of PD and M0 at the current parameters.  L lanes per
+// voxel; a block of kThreads handles kThreads / L voxels in lockstep over
+// chunks of `chunk` steps.
+template <int P, bool TANGENTS>
+__global__ void __launch_bounds__(kThreads) gn_kernel(GnArgs a, int chunk) {
+    extern __shared__ __align__(16) unsigned char gn_smem[];
+    const int L = a.L, apc = kThreads / L;
+    const int tid = threadIdx.x, g = tid / L, gl = tid % L;
+    const bool lane0 = gl == 0;
+    GnStep *sQ = reinterpret_cast<GnStep *>(gn_smem);              // [apc][chunk]
+    float *sV = reinterpret_cast<float *>(sQ + apc * chunk);       // [apc][4]: T1, T2, B1, ok
+    const long long vox0 = (long long)blockIdx.x * apc;
+    for (int i = tid; i < apc; i += kThreads) {
+        const long long v = vox0 + i;
+        float T1 = 2.f, T2 = 1.f, B1 = 1.f, ok = 0.f;
+        if (v < a.nvox) {
+            const float *mp = a.maps + v * a.nmaps;
+            const float t1 = mp[0], t2 = mp[1];
+            const float b1 = a.b1map ? a.b1map[v] : (a.nmaps >= 4 ? mp[3] : 1.f);
+            if (usable(t1, t2, b1)) {
+                T1 = t1;
+                T2 = t2;
+                B1 = b1;
+                ok = 1.f;
+            }
+        }
+        sV[4 * i] = T1;
+        sV[4 * i + 1] = T2;
+        sV[4 * i + 2] = B1;
+        sV[4 * i + 3] = ok;
+    }
+    __syncthreads();
+    const long long v = vox0 + g;
+    const bool active = sV[4 * g + 3] != 0.f;
+    const int T = a.sch.nreps, w = a.w;
+    const int k0 = gl * 2 * P;
+    float2 keep[P];
+#pragma unroll
+    for (int i = 0; i < P; i++)
+        keep[i] = make_float2(k0 + 2 * i == w ? 0.f : 1.f, k0 + 2 * i + 1 == w ? 0.f : 1.f);
+
+    Pair3<P> sv, s1, s2;
+    pz<P>(sv);
+    if (TANGENTS) {
+        pz<P>(s1);
+        pz<P>(s2);
+    }
+    if (lane0) sv.z[0].x = 1.f;
     // inner products (lane 0): Ss = <s,s>, P = <s,x>, G_j = <s,J_j>,
     // H_jk = <J_j,J_k>, Q_j = <J_j,x>; s_t = i f, J_jt = i df_j
     float Ss = 0.f, Pr = 0.f, Pi = 0.f, G1 = 0.f, G2 = 0.f, H11 = 0.f, H12 = 0.f, H22 = 0.f;
     float Q1r = 0.f, Q1i = 0.f, Q2r = 0.f, Q2i = 0.f;
-    const float r1 = 1.f / T1, r2 = 1.f / T2;
-    for (int t = 0; t < T; t++) {
-        const StepRF r = step_rf(a.sch.alpha[t] * B1);
-        rf_fwd<S>(sv, r);
-        if (TANGENTS) {
-            rf_fwd<S>(s1, r);
-            rf_fwd<S>(s2, r);
+    for (int t0 = 0; t0 < T; t0 += chunk) {
+        const int nch = min(chunk, T - t0);
+        __syncthreads();
+        for (int idx = tid; idx < apc * nch; idx += kThreads) {
+            const int ga = idx / nch, i = idx - ga * nch;
+            const float T1 = sV[4 * ga], T2 = sV[4 * ga + 1], B1 = sV[4 * ga + 2];
+            const int t = t0 + i;
+            GnStep q;
+            __sincosf(a.sch.alpha[t] * B1, &q.S, &q.C);
+            const float ta = a.sch.TE[t], tr = a.sch.TR[t];
+            const float r1 = 1.f / T1, r2 = 1.f / T2;
+            q.E1 = __expf(-tr * r1);
+            q.E2 = __expf(-tr * r2);
+            q.dE1 = q.E1 * tr * r1 * r1;
+            q.dE2 = q.E2 * tr * r2 * r2;
+            q.Ea = __expf(-ta * r2);
+            q.dEa = q.Ea * ta * r2 * r2;
+            const long long vv = vox0 + ga;
+            float2 xv = make_float2(0.f, 0.f);
+            if (vv < a.nvox) xv = a.img[vv * a.img_stride + t];
+            q.xr = xv.x;
+            q.xi = xv.y;
+            sQ[ga * chunk + i] = q;
         }
-        const float tr = a.sch.TR[t], te = a.sch.TE[t];
-#pragma unroll
-        for (int pass = 0; pass < 2; pass++) {
-            const float tt = pass == 0 ? te : tr - te;
-            const float E1 = __expf(-tt * r1), E2 = __expf(-tt * r2);
+        __syncthreads();
+        const GnStep *qs = sQ + g * chunk;
+        for (int i = 0; i < nch; i++) {
+            const GnStep q = qs[i];
+            const float cc = (1 + q.C) / 2, ss = (1 - q.C) / 2, hS = 0.5f * q.S;
+            const float2 kc = make_float2(cc, cc), ks = make_float2(ss, ss), kS = make_float2(q.S, q.S),
+                         knS = make_float2(-q.S, -q.S), khS = make_float2(hS, hS), knhS = make_float2(-hS, -hS),
+                         kC = make_float2(q.C, q.C);
+            p_rf<P>(sv, kc, ks, kS, knS, khS, knhS, kC);
             if (TANGENTS) {
-                const float dE1 = E1 * tt * r1 * r1, dE2 = E2 * tt * r2 * r2;  // dE1/dT1, dE2/dT2
+                p_rf<P>(s1, kc, ks, kS, knS, khS, knhS, kC);
+                p_rf<P>(s2, kc, ks, kS, knS, khS, knhS, kC);
+            }
+            if (lane0) {
+                // readout s_t = i Ea f+[0] (relaxation over TE)
+                const float f = q.Ea * sv.p[0].x;
+                Ss = fmaf(f, f, Ss);
+                Pr = fmaf(f, q.xi, Pr);
+                Pi = fmaf(-f, q.xr, Pi);
+                if (TANGENTS) {
+                    const float d1 = q.Ea * s1.p[0].x;
+                    const float d2 = fmaf(q.dEa, sv.p[0].x, q.Ea * s2.p[0].x);
+                    G1 = fmaf(f, d1, G1);
+                    G2 = fmaf(f, d2, G2);
+                    H11 = fmaf(d1, d1, H11);
+                    H12 = fmaf(d1, d2, H12);
+                    H22 = fmaf(d2, d2, H22);
+                    Q1r = fmaf(d1, q.xi, Q1r);
+                    Q1i = fmaf(-d1, q.xr, Q1i);
+                    Q2r = fmaf(d2, q.xi, Q2r);
+                    Q2i = fmaf(-d2, q.xr, Q2i);
+                }
+            }
+            if (a.shift) {
+                p_shift<P>(sv, gl, L, w, keep);
+                if (TANGENTS) {
+                    p_shift<P>(s1, gl, L, w, keep);
+                    p_shift<P>(s2, gl, L, w, keep);
+                }
+            }
+            // relaxation over TR
+            const float2 e1 = make_float2(q.E1, q.E1), e2 = make_float2(q.E2, q.E2);
+            if (TANGENTS) {
+                const float2 de1 = make_float2(q.dE1, q.dE1), de2 = make_float2(q.dE2, q.dE2);
 #pragma unroll
-                for (int j = 0; j < S; j++) {
-                    // product rule: d(E x) = dE x + E dx
-                    s1.p[j] = E2 * s1.p[j];
-                    s1.m[j] = E2 * s1.m[j];
-                    s1.z[j] = fmaf(dE1, sv.z[j], E1 * s1.z[j]);
-                    s2.p[j] = fmaf(dE2, sv.p[j], E2 * s2.p[j]);
-                    s2.m[j] = fmaf(dE2, sv.m[j], E2 * s2.m[j]);
-                    s2.z[j] = E1 * s2.z[j];
+                for (int j = 0; j < P; j++) {
+                    // product rule on the pre-relaxation signal: d(E x) = dE x + E dx
+                    s1.p[j] = __fmul2_rn(e2, s1.p[j]);
+                    s1.m[j] = __fmul2_rn(e2, s1.m[j]);
+                    s1.z[j] = __ffma2_rn(de1, sv.z[j], __fmul2_rn(e1, s1.z[j]));
+                    s2.p[j] = __ffma2_rn(de2, sv.p[j], __fmul2_rn(e2, s2.p[j]));
+                    s2.m[j] = __ffma2_rn(de2, sv.m[j], __fmul2_rn(e2, s2.m[j]));
+                    s2.z[j] = __fmul2_rn(e1, s2.z[j]);
                 }
-                if (lane0) s1.z[0] -= dE1;
+                if (lane0) s1.z[0].x -= q.dE1;
             }
-            relax_fwd<S>(sv, E1, E2, lane0);
-            if (pass == 0) {
-                if (lane0) {
-                    const float f = sv.p[0];
-                    const float2 xv = x[t];
-                    Ss = fmaf(f, f, Ss);
-                    Pr = fmaf(f, xv.y, Pr);
-                    Pi = fmaf(-f, xv.x, Pi);
-                    if (TANGENTS) {
-                        const float d1 = s1.p[0], d2 = s2.p[0];
-                        G1 = fmaf(f, d1, G1);
-                        G2 = fmaf(f, d2, G2);
-                        H11 = fmaf(d1, d1, H11);
-                        H12 = fmaf(d1, d2, H12);
-                        H22 = fmaf(d2, d2, H22);
-                        Q1r = fmaf(d1, xv.y, Q1r);
-                        Q1i = fmaf(-d1, xv.x, Q1i);
-                        Q2r = fmaf(d2, xv.y, Q2r);
-                        Q2i = fmaf(-d2, xv.x, Q2i);
-                    }
-                }
-                if (a.shift) {
-                    shift_fwd<S>(sv, gl, L, w);
-                    if (TANGENTS) {
-                        shift_fwd<S>(s1, gl, L, w);
-                        shift_fwd<S>(s2, gl, L, w);
-                    }
-                }
+#pragma unroll
+            for (int j = 0; j < P; j++) {
+                sv.p[j] = __fmul2_rn(e2, sv.p[j]);
+                sv.m[j] = __fmul2_rn(e2, sv.m[j]);
+                sv.z[j] = __fmul2_rn(e1, sv.z[j]);
             }
+            if (lane0) sv.z[0].x += 1 - q.E1;
         }
     }
-    if (!lane0 || !(Ss > 0.f)) return;
+    if (!lane0 || !active || !(Ss > 0.f)) return;
+    float *mp = a.maps + v * a.nmaps;
     if (!TANGENTS) {
         // PD of a unit-norm atom (what matching reports) and |rho|
         const float ip = sqrtf(Pr * Pr + Pi * Pi);
-        if (a.b1map && a.nmaps >= 4) mp[3] = B1;
+        if (a.b1map && a.nmaps >= 4) mp[3] = sV[4 * g + 2];
         if (a.nmaps >= 5) mp[4] = ip / sqrtf(Ss);
         if (a.m0) a.m0[v] = ip / Ss;
         return;
     }
+    const float T1 = sV[4 * g], T2 = sV[4 * g + 1];
     // variable projection: rho = P / Ss; A_jk = |rho|^2 (H_jk - G_j G_k / Ss),
     // b_j = Re(conj(rho) (Q_j - G_j P / Ss)); delta = A^-1 b
     const float rr = Pr / Ss, ri = Pi / Ss, rho2 = rr * rr + ri * ri;
@@ -477,6 +597,36 @@ __global__ void __launch_bounds__(kThreads) gn_kernel(GnArgs a) {
     n1 = fmaxf(n1, n2 * (1.f + 1e-4f));  // keep T1 > T2 > 0
     mp[0] = n1;
     mp[1] = n2;
+}
+
+constexpr int kGnMaxPairs = 7;  // 8 pairs with both tangents exceed 255 registers
+
+// Lanes per voxel and state pairs per lane for the refinement: the fewest
+// padded states, then the most pairs per lane (fewer shuffles per state).
+// SNAPMRF_GN_LAYOUT="L,P" overrides the choice when it covers w states.
+static void choose_pairs(int w, int *L, int *P) {
+    if (const char *e = getenv("SNAPMRF_GN_LAYOUT")) {
+        int l = 0, p = 0;
+        if (sscanf(e, "%d,%d", &l, &p) == 2 && l >= 1 && l <= 32 && (l & (l - 1)) == 0 && p >= 1 &&
+            p <= kGnMaxPairs && l * 2 * p >= w) {
+            *L = l;
+            *P = p;
+            return;
+        }
+    }
+    int bL = 32, bP = kGnMaxPairs, best = 1 << 30;
+    for (int p = 1; p <= kGnMaxPairs; p++) {
+        int l = 1;
+        while (l < 32 && l * 2 * p < w) l *= 2;
+        if (l * 2 * p < w) continue;
+        if (l * 2 * p <= best) {
+            best = l * 2 * p;
+            bL = l;
+            bP = p;
+        }
+    }
+    *L = bL;
+    *P = bP;
 }
 
 static void choose(int w, int *L, int *S) {
@@ -503,16 +653,15 @@ static void choose(int w, int *L, int *S) {
     default: KERNEL<8><<<GRID, kThreads, 0, ST>>>(ARGS); break;           \
     }
 
-#define SNAPMRF_GRAD_DISPATCH2(KERNEL, S, B, GRID, ST, ARGS)                \
-    switch (S) {                                                          \
-    case 1: KERNEL<1, B><<<GRID, kThreads, 0, ST>>>(ARGS); break;         \
-    case 2: KERNEL<2, B><<<GRID, kThreads, 0, ST>>>(ARGS); break;         \
-    case 3: KERNEL<3, B><<<GRID, kThreads, 0, ST>>>(ARGS); break;         \
-    case 4: KERNEL<4, B><<<GRID, kThreads, 0, ST>>>(ARGS); break;         \
-    case 5: KERNEL<5, B><<<GRID, kThreads, 0, ST>>>(ARGS); break;         \
-    case 6: KERNEL<6, B><<<GRID, kThreads, 0, ST>>>(ARGS); break;         \
-    case 7: KERNEL<7, B><<<GRID, kThreads, 0, ST>>>(ARGS); break;         \
-    default: KERNEL<8, B><<<GRID, kThreads, 0, ST>>>(ARGS); break;        \
+#define SNAPMRF_GN_DISPATCH(P, B, GRID, SMEM, ST, ARGS, CHUNK)                      \
+    switch (P) {                                                                    \
+    case 1: gn_kernel<1, B><<<GRID, kThreads, SMEM, ST>>>(ARGS, CHUNK); break;      \
+    case 2: gn_kernel<2, B><<<GRID, kThreads, SMEM, ST>>>(ARGS, CHUNK); break;      \
+    case 3: gn_kernel<3, B><<<GRID, kThreads, SMEM, ST>>>(ARGS, CHUNK); break;      \
+    case 4: gn_kernel<4, B><<<GRID, kThreads, SMEM, ST>>>(ARGS, CHUNK); break;      \
+    case 5: gn_kernel<5, B><<<GRID, kThreads, SMEM, ST>>>(ARGS, CHUNK); break;      \
+    case 6: gn_kernel<6, B><<<GRID, kThreads, SMEM, ST>>>(ARGS, CHUNK); break;      \
+    default: gn_kernel<7, B><<<GRID, kThreads, SMEM, ST>>>(ARGS, CHUNK); break;     \
     }
 
 // Schedule of the real-valued recursion on the device; fails unless every
@@ -614,8 +763,8 @@ extern "C" int snapmrf_refine_gn(float *d_maps, int nmaps, const float *img, siz
                                  void *stream) {
     cudaStream_t st = (cudaStream_t)stream;
     if (!d_maps || !img || !h_mrf) SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "refine_gn: null pointer");
-    if (nmaps < 2 || nreps == 0 || nreps > NREPS || nvoxels == 0 || nstates < 1 || nstates > 32 * kMaxS ||
-        iterations < 0)
+    if (nmaps < 2 || nreps == 0 || nreps > NREPS || nvoxels == 0 || nstates < 1 ||
+        nstates > 32 * 2 * kGnMaxPairs || iterations < 0)
         SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "refine_gn: bad sizes");
     if (nreps > 0x7fffffff) SNAPMRF_FAIL(SNAPMRF_ERR_UNSUPPORTED, "refine_gn: too many time points");
     if (!img_stride) img_stride = nreps;
@@ -626,8 +775,8 @@ extern "C" int snapmrf_refine_gn(float *d_maps, int nmaps, const float *img, siz
     Schedule sc;
     int rc = upload_schedule(sbuf, &sc, h_mrf, nreps, NREPS, st, "refine_gn");
     if (rc) return rc;
-    int L, S;
-    choose(nstates, &L, &S);
+    int L, P;
+    choose_pairs(nstates, &L, &P);
     GnArgs a;
     a.sch = sc;
     a.nvox = (long long)nvoxels;
@@ -642,13 +791,17 @@ extern "C" int snapmrf_refine_gn(float *d_maps, int nmaps, const float *img, siz
     a.m0 = d_m0;
     a.max_rel_step = max_rel_step > 0.f ? max_rel_step : 0.2f;
     const int apc = kThreads / L;
+    // steps staged per chunk: at most kGnChunk, within 48 KB of shared memory
+    const size_t smem_cap = 48 * 1024 - (size_t)apc * 4 * sizeof(float);
+    const int chunk = (int)std::min<size_t>(kGnChunk, smem_cap / ((size_t)apc * sizeof(GnStep)));
+    const size_t smem = (size_t)apc * chunk * sizeof(GnStep) + (size_t)apc * 4 * sizeof(float);
     dim3 grid((unsigned)((nvoxels + apc - 1) / apc));
     for (int it = 0; it < iterations; it++) {
-        SNAPMRF_GRAD_DISPATCH2(gn_kernel, S, true, grid, st, a);
+        SNAPMRF_GN_DISPATCH(P, true, grid, smem, st, a, chunk);
         SNAPMRF_LAUNCH_CHECK();
     }
     if (nmaps >= 5 || d_m0 || (d_b1map && nmaps >= 4)) {
-        SNAPMRF_GRAD_DISPATCH2(gn_kernel, S, false, grid, st, a);
+        SNAPMRF_GN_DISPATCH(P, false, grid, smem, st, a, chunk);
         SNAPMRF_LAUNCH_CHECK();
     }
     return SNAPMRF_OK;
