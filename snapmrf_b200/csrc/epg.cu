@@ -102,10 +102,10 @@ static cudaError_t dispatch_states(const EpgArgs &a, int S, dim3 grid, cudaStrea
     }
 }
 
-template <int ECHO, int S>
+template <int ECHO, int S, bool TAIL = false>
 static cudaError_t launch_epg_real(const EpgArgs &a, dim3 grid, cudaStream_t st) {
     size_t smem = epg_real_smem_bytes(a.L);
-    auto k = epg_real_kernel<ECHO, S>;
+    auto k = epg_real_kernel<ECHO, S, TAIL>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     k<<<grid, kEpgThreads, smem, st>>>(a);
@@ -113,9 +113,30 @@ static cudaError_t launch_epg_real(const EpgArgs &a, dim3 grid, cudaStream_t st)
     return cudaGetLastError();
 }
 
-// P = pairs of states per lane (S = 2P).
+// P = pairs of states per lane (S = 2P).  FISP layouts that pad at most two
+// states take the TAIL form of the shift.
 template <int ECHO>
 static cudaError_t dispatch_real(const EpgArgs &a, int P, dim3 grid, cudaStream_t st) {
+    if constexpr (ECHO == ECHO_FISP) {
+        if (a.L * 2 * P - a.nstates <= 2) switch (P) {
+        case 1: return launch_epg_real<ECHO, 1, true>(a, grid, st);
+        case 2: return launch_epg_real<ECHO, 2, true>(a, grid, st);
+        case 3: return launch_epg_real<ECHO, 3, true>(a, grid, st);
+        case 4: return launch_epg_real<ECHO, 4, true>(a, grid, st);
+        case 5: return launch_epg_real<ECHO, 5, true>(a, grid, st);
+        case 6: return launch_epg_real<ECHO, 6, true>(a, grid, st);
+        case 7: return launch_epg_real<ECHO, 7, true>(a, grid, st);
+        case 8: return launch_epg_real<ECHO, 8, true>(a, grid, st);
+        case 9: return launch_epg_real<ECHO, 9, true>(a, grid, st);
+        case 10: return launch_epg_real<ECHO, 10, true>(a, grid, st);
+        case 11: return launch_epg_real<ECHO, 11, true>(a, grid, st);
+        case 12: return launch_epg_real<ECHO, 12, true>(a, grid, st);
+        case 13: return launch_epg_real<ECHO, 13, true>(a, grid, st);
+        case 14: return launch_epg_real<ECHO, 14, true>(a, grid, st);
+        case 15: return launch_epg_real<ECHO, 15, true>(a, grid, st);
+        default: return launch_epg_real<ECHO, 16, true>(a, grid, st);
+            }
+    }
     switch (P) {
     case 1: return launch_epg_real<ECHO, 1>(a, grid, st);
     case 2: return launch_epg_real<ECHO, 2>(a, grid, st);

@@ -403,8 +403,15 @@ __device__ __forceinline__ void rl2_relax(RealLane2<P> &s, float E1, float E2, b
 // Gradient shift of the paired real state (see st_shift): F+ up one slot,
 // F- down one slot, f+[0] = -f-[0] (Im of conj), F-[w-1] = 0, slots k >= w
 // zero; with w = 1 the unshifted f-[0] is used.
-template <int P>
-__device__ __forceinline__ void rl2_shift(RealLane2<P> &s, int gl, int L, int w) {
+//
+// TAIL: the layout pads at most two slots (w >= 2P L - 2).  Slots k >= w
+// then hold zeros before the shift, so F-[w-1] takes the zero of F-[w] and
+// only F+[w], which receives F+[w-1], must be cleared.  That slot lies in the
+// last pair of the last lane, and tail_keep (0 there, 1 elsewhere) clears it
+// with one multiply instead of a compare per slot; every non-zero value is
+// the same as with the per-slot masks.
+template <int P, bool TAIL = false>
+__device__ __forceinline__ void rl2_shift(RealLane2<P> &s, int gl, int L, int w, float2 tail_keep = {1.f, 1.f}) {
     const unsigned full = 0xffffffffu;
     const float up = __shfl_up_sync(full, s.fp[P - 1].y, 1, L);
     const float dn = __shfl_down_sync(full, s.fm[0].x, 1, L);
@@ -416,6 +423,10 @@ __device__ __forceinline__ void rl2_shift(RealLane2<P> &s, int gl, int L, int w)
     for (int i = 0; i < P - 1; i++) s.fm[i] = make_float2(s.fm[i].y, s.fm[i + 1].x);
     s.fm[P - 1] = make_float2(s.fm[P - 1].y, (gl == L - 1) ? 0.f : dn);
     if (gl == 0) s.fp[0].x = -((w == 1) ? old_fm0 : s.fm[0].x);
+    if (TAIL) {
+        s.fp[P - 1] = __fmul2_rn(s.fp[P - 1], tail_keep);
+        return;
+    }
     const int k0 = gl * 2 * P;
 #pragma unroll
     for (int i = 0; i < P; i++) {
@@ -432,7 +443,7 @@ inline size_t epg_real_smem_bytes(int L) {
            (size_t)apc * kReadoutStride * sizeof(float2) + (size_t)apc * 3 * sizeof(float);
 }
 
-template <int ECHO, int P>
+template <int ECHO, int P, bool TAIL>
 __global__ void __launch_bounds__(kEpgThreads) epg_real_kernel(EpgArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr int NF = 4;
@@ -474,6 +485,12 @@ __global__ void __launch_bounds__(kEpgThreads) epg_real_kernel(EpgArgs a) {
     const float *TR = a.sched + 2 * nreps;
     const float *TE = a.sched + 3 * nreps;
     const int w = a.nstates;
+    // TAIL layouts: 0 at slot w (cleared after each shift), 1 elsewhere
+    float2 tail_keep = make_float2(1.f, 1.f);
+    if (TAIL && gl == L - 1) {
+        const int pad = L * 2 * P - w;
+        tail_keep = make_float2(pad == 2 ? 0.f : 1.f, pad >= 1 ? 0.f : 1.f);
+    }
 
     // init_rf_pulse with alpha = phi = 0, TI = 0 (the expression of st_init)
     RealLane2<P> s;
@@ -515,7 +532,7 @@ __global__ void __launch_bounds__(kEpgThreads) epg_real_kernel(EpgArgs a) {
                 // the complex path adds round(0*0 + v*v) = round(v*v)
                 nrm = __fadd_rn(nrm, __fmul_rn(v, v));
             }
-            if (ECHO == ECHO_FISP) rl2_shift<P>(s, gl, L, w);
+            if (ECHO == ECHO_FISP) rl2_shift<P, TAIL>(s, gl, L, w, tail_keep);
             rl2_relax<P>(s, f.z, f.w, lane0);
         }
         __syncwarp();

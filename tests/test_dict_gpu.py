@@ -165,7 +165,7 @@ def test_normalize_entry_point(snap):
 
 
 @pytest.mark.parametrize("echo", ["epg_fisp", "epg_sr"])
-@pytest.mark.parametrize("nstates", [1, 7, 20, 50, 101, 256])
+@pytest.mark.parametrize("nstates", [1, 2, 7, 20, 49, 50, 51, 101, 256])
 def test_real_path_bit_identical_to_complex_path(snap, echo, nstates):
     """With every RF phase 0 the real-valued recursion (default) must give
     exactly the complex recursion's atoms (SNAPMRF_DICT_REFERENCE_ORDER)."""
