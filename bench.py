@@ -50,7 +50,17 @@ T = 1000
 NSTATES = 50
 NX = NY = 240
 SNR = 40.0
-FLOP_PER_STATE_STEP = 66        # RF 54 + two relaxations 6 + 6
+# Algorithmic work of the dictionary per EPG state and time step, by the
+# fixed convention of the complex recursion: RF 54 + two relaxations 6 + 6.
+FLOP_PER_STATE_STEP = 66
+# Work the real-valued recursion actually executes when every RF phase is 0
+# (this schedule): RF 9 FMA (18 flop) + two relaxations of 3 multiplies.
+FLOP_PER_STATE_STEP_EXECUTED = 24
+# DRAM bytes per dictionary atom (T = 1000, w = 50, normalised) measured by
+# ncu on the reduced workload (5 B1 blocks, 34,690 atoms: 164.7 MB read +
+# 486.2 MB written in one launch); traffic grows with the atom count, so a
+# full launch moves this times NATOMS.
+DICT_DRAM_BYTES_PER_ATOM = (164.743424e6 + 486.182656e6) / 34690
 PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
 
 
@@ -136,18 +146,62 @@ def make_inputs(snap, torch, seed: int, b1_blocks: int = 41, nx: int = NX):
 # ---------------------------------------------------------------------------
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    """SM clock, power and clock-event (throttle) reasons sampled through NVML
+    every 2 ms from a host thread; only samples taken between mark_start()
+    and mark_end() (the timed region) are reported.  Falls back to
+    `nvidia-smi -lms 50` when NVML is unavailable."""
+    FIELDS = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clock-event reason bits
+    REASONS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20,
+               "hw_thermal_slowdown": 0x40, "hw_power_brake_slowdown": 0x80}
 
     def __init__(self, device_index: int):
         self.idx = device_index
-        self.proc = None
-        self.lines: list[str] = []
+        self.samples: list[tuple] = []
+        self.stop_flag = threading.Event()
         self.thread = None
+        self.proc = None
+        self.t0 = self.t1 = None
+        self.nvml = None
+        self.max_mhz = None
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        props = torch.cuda.get_device_properties(self.idx)
+        try:
+            bus = f"{props.pci_domain_id:08x}:{props.pci_bus_id:02x}:{props.pci_device_id:02x}.0"
+            h = pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.idx)
+        return pynvml, h
 
     def start(self):
+        try:
+            self.nvml = self._nvml_handle()
+        except Exception:
+            self.nvml = None
+        if self.nvml is not None:
+            nv, h = self.nvml
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            get_reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                nv.nvmlDeviceGetCurrentClocksThrottleReasons
+
+            def loop():
+                while not self.stop_flag.is_set():
+                    t = time.perf_counter()
+                    try:
+                        self.samples.append((t, float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)),
+                                             nv.nvmlDeviceGetPowerUsage(h) / 1000.0, int(get_reasons(h))))
+                    except Exception:
+                        pass
+                    time.sleep(0.002)
+            self.thread = threading.Thread(target=loop, daemon=True)
+            self.thread.start()
+            return
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}",
@@ -156,42 +210,61 @@ class ClockSampler:
         except (FileNotFoundError, OSError):
             self.proc = None
             return
-        self.thread = threading.Thread(target=self._read, daemon=True)
-        self.thread.start()
 
-    def _read(self):
-        for ln in self.proc.stdout:
-            self.lines.append(ln.strip())
+        def read():
+            for ln in self.proc.stdout:
+                self.samples.append((time.perf_counter(), ln.strip()))
+        self.thread = threading.Thread(target=read, daemon=True)
+        self.thread.start()
+        time.sleep(0.5)  # nvidia-smi start-up
+
+    def mark_start(self):
+        self.t0 = time.perf_counter()
+
+    def mark_end(self):
+        self.t1 = time.perf_counter()
+
+    def _window(self):
+        t0 = self.t0 if self.t0 is not None else -1e30
+        t1 = self.t1 if self.t1 is not None else 1e30
+        return [s for s in self.samples if t0 <= s[0] <= t1]
 
     def stop(self) -> dict:
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
+        if self.nvml is None and self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvml and nvidia-smi unavailable"]}
+        self.stop_flag.set()
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
         if self.thread:
             self.thread.join(timeout=2)
-        sm, mx, pw, reasons = [], [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            f = [x.strip() for x in ln.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                sm.append(float(f[1]))
-                mx.append(float(f[2]))
-                pw.append(float(f[3]))
-            except ValueError:
-                continue
-            for n, v in zip(names, f[5:9]):
-                if v.lower() == "active":
-                    reasons.add(n)
-        return {"sm_mhz": float(np.median(sm)) if sm else None,
-                "sm_max_mhz": max(mx) if mx else None,
-                "power_w_max": max(pw) if pw else None,
-                "samples": len(sm), "reasons": sorted(reasons)}
+        win = self._window()
+        sm, pw, reasons = [], [], set()
+        mx = self.max_mhz
+        if self.nvml is not None:
+            for _, clk, p, bits in win:
+                sm.append(clk)
+                pw.append(p)
+                reasons.update(n for n, b in self.REASONS.items() if bits & b)
+        else:
+            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            for _, ln in win:
+                f = [x.strip() for x in ln.split(",")]
+                if len(f) < 10:
+                    continue
+                try:
+                    sm.append(float(f[2]))
+                    mx = float(f[3])
+                    pw.append(float(f[4]))
+                except ValueError:
+                    continue
+                reasons.update(n for n, v in zip(names, f[6:10]) if v.lower() == "active")
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
+                "power_w_max": max(pw) if pw else None, "samples": len(sm), "reasons": sorted(reasons),
+                "source": "nvml, 2 ms" if self.nvml is not None else "nvidia-smi -lms 50"}
 
 
 def peaks() -> dict:
@@ -256,7 +329,7 @@ def run_ours(args) -> None:
         if gn:
             # Gauss-Newton refinement of the matched (T1, T2) at the B1 map
             snap.refine_gn(d_maps, d_img, h_mrf, T, T, nvox, NSTATES, "epg_fisp", iterations=gn,
-                           d_b1map=d_b1)
+                           tol=args.gn_tol, d_b1map=d_b1)
         if ev is not None:
             ev[3].record(stream)
 
@@ -266,6 +339,8 @@ def run_ours(args) -> None:
 
     def timed(precision, gn=0):
         """W warm-up steps, then K steps between barriers and device syncs."""
+        clk = ClockSampler(local)
+        clk.start()
         for _ in range(args.warmup):
             step(precision, gn=gn)
         torch.cuda.synchronize()
@@ -273,15 +348,15 @@ def run_ours(args) -> None:
         torch.cuda.synchronize()
         evs = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
         launches0 = snap.kernel_launches()
-        clk = ClockSampler(local)
-        clk.start()
         t_start = torch.cuda.Event(enable_timing=True)
         t_end = torch.cuda.Event(enable_timing=True)
+        clk.mark_start()
         t_start.record(stream)
         for k in range(args.steps):
             step(precision, evs[k], gn=gn)
         t_end.record(stream)
         torch.cuda.synchronize()
+        clk.mark_end()
         barrier()
         torch.cuda.synchronize()
         r = {"clocks": clk.stop(), "launches": snap.kernel_launches() - launches0,
@@ -393,9 +468,18 @@ def run_ours(args) -> None:
         match_flops = nvox * 8.0 * T * natoms
         dict_tf = dict_flops / (dict_ms / 1e3) / 1e12
         match_tf = match_flops / (match_ms / 1e3) / 1e12
-        rl_dict = {"kernel": "epg_fisp dictionary", "bound": "fp32", "achieved": round(dict_tf, 2),
-                   "peak": round(fp32_peak, 2), "unit": "TFLOP/s", "frac": round(dict_tf / fp32_peak, 4),
-                   "traffic": None, "algorithmic_flop_per_launch": dict_flops, "ms": round(dict_ms, 3)}
+        rl_dict = {"kernel": "epg_real_kernel (epg_fisp dictionary, real-valued recursion)", "bound": "fp32",
+                   "achieved": round(dict_tf, 2), "peak": round(fp32_peak, 2), "unit": "TFLOP/s",
+                   "frac": round(dict_tf / fp32_peak, 4),
+                   "executed_tflops": round(dict_tf * FLOP_PER_STATE_STEP_EXECUTED / FLOP_PER_STATE_STEP, 2),
+                   "executed_frac": round(dict_tf * FLOP_PER_STATE_STEP_EXECUTED / FLOP_PER_STATE_STEP / fp32_peak, 4),
+                   "note": "achieved counts 66 flop per state-step (complex recursion convention); the "
+                           "real-valued recursion executes 24, hence frac > 1 is possible; executed_frac is "
+                           "the FP32-pipe utilisation",
+                   "traffic": round(DICT_DRAM_BYTES_PER_ATOM * NATOMS),
+                   "traffic_note": "ncu DRAM bytes of the reduced case scaled by atoms; algorithmic output "
+                                   f"{NATOMS * T * 8} B",
+                   "algorithmic_flop_per_launch": dict_flops, "ms": round(dict_ms, 3)}
         if headline != "fp32":
             mpk = pk["bf16_tflops"]
             rl_match = {"kernel": f"{headline} tcgen05 B1-bin match + fp32 top-16 rescoring", "bound": "tensor",
@@ -428,8 +512,8 @@ def run_ours(args) -> None:
             "match_voxels_per_s": round(world * nvox / (match_ms / 1e3), 1),
             "stage_ms": {"dict": round(dict_ms, 3), "match": round(match_ms, 3)},
             "roofline": dominant, "roofline_other": other,
-            "peak_note": "fp32 peak = 148 SMs x 128 lanes x 2 flop x max SM clock (nominal); "
-                         f"HBM/bf16 peaks {pk['source']}",
+            "peak_note": "fp32 peak = 148 SMs x 128 FMA lanes x 2 flop x max SM clock (nominal, no "
+                         f"measured FP32 figure exists); bf16 peak {pk['source']} (burst)",
             "e2e": {"value": round(e2e_value, 1) if e2e_value else None, "unit": "voxels/s",
                     "h2d_bytes_per_step": int(params.nbytes + img.nbytes + b1map.nbytes + h_mrf.nbytes),
                     "d2h_bytes_per_step": int(nvox * 5 * 4)},
@@ -451,7 +535,7 @@ def run_ours(args) -> None:
             line["forms_refined"] = {
                 f: {"voxels_per_s": round(world * nvox / (gn_ms[f] / args.steps / 1e3), 1),
                     "ms_per_step": round(gn_ms[f] / args.steps, 3), "gn_ms": round(gn_stage_ms[f], 3),
-                    "gn_iterations": args.gn_iters,
+                    "gn_iterations_max": args.gn_iters, "gn_tol": args.gn_tol,
                     "speedup_vs_fp32_form": round(form_ms["fp32"] / gn_ms[f], 3)} for f in gnames}
         if args.b1_blocks != 41 or args.nx != NX:
             line["config"]["workload"] = f"{WORKLOAD} reduced: {NATOMS // natoms} B1 blocks, {args.nx}x{args.nx} voxels"
@@ -551,8 +635,10 @@ def main() -> None:
     ap.add_argument("--b1-blocks", type=int, default=41,
                     help="reduced case for profiling: keep this many B1 blocks around 1.0")
     ap.add_argument("--nx", type=int, default=NX, help="reduced case for profiling: nx x nx voxels")
-    ap.add_argument("--gn-iters", type=int, default=1,
-                    help="Gauss-Newton iterations of the refined forms (0: skip them)")
+    ap.add_argument("--gn-iters", type=int, default=3,
+                    help="Gauss-Newton iterations (at most, per voxel) of the refined forms (0: skip them)")
+    ap.add_argument("--gn-tol", type=float, default=1e-4,
+                    help="a voxel stops refining once a step moves T1 and T2 by at most this (relative)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":

@@ -290,11 +290,14 @@ int snapmrf_epg_adjoint(const float *d_params, int nparams, const float *h_mrf, 
  * or do not hold T1 > T2 > 0 are left as they are.
  * img: device complex [nvoxels][img_stride] (0 = nreps);
  * d_m0: optional out [nvoxels], |rho|.  PD, M0 and the B1 column cost one
- * value-only forward pass at the final parameters. */
+ * value-only forward pass at the final parameters.
+ * iterations: at most this many Gauss-Newton steps per voxel; with tol > 0 a
+ * voxel stops once a step changed both T1 and T2 by at most tol of their
+ * values (later iterations run only over the voxels still moving). */
 int snapmrf_refine_gn(float *d_maps, int nmaps, const float *img, size_t img_stride,
-                      const float *d_b1map, const float *h_mrf, size_t nreps, size_t NREPS, size_t nvoxels, int nstates,
-                      const char *echo_type, int iterations, float max_rel_step, float *d_m0,
-                      void *stream);
+                      const float *d_b1map, const float *h_mrf, size_t nreps, size_t NREPS,
+                      size_t nvoxels, int nstates, const char *echo_type, int iterations,
+                      float max_rel_step, float tol, float *d_m0, void *stream);
 
 #ifdef __cplusplus
 }

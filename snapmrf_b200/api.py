@@ -104,7 +104,7 @@ def lib() -> C.CDLL:
         L.snapmrf_epg_adjoint.argtypes = [vp, C.c_int, vp, sz, sz, sz, C.c_int, C.c_char_p, vp, vp, vp,
                                           vp, vp, C.c_int, vp]
         L.snapmrf_refine_gn.argtypes = [vp, C.c_int, vp, sz, vp, vp, sz, sz, sz, C.c_int, C.c_char_p, C.c_int,
-                                        C.c_float, vp, vp]
+                                        C.c_float, C.c_float, vp, vp]
         _lib = L
     return _lib
 
@@ -365,15 +365,16 @@ def epg_adjoint(d_params, h_mrf, nreps: int, NREPS: int, natoms: int, d_grad_sig
 
 
 def refine_gn(d_maps, d_img, h_mrf, nreps: int, NREPS: int, nvoxels: int, nstates: int = 101,
-              echo_type: str = "epg_fisp", *, nmaps: int = NMAPS, iterations: int = 2,
-              max_rel_step: float = 0.2, img_stride: int = 0, d_b1map=None, d_m0=None,
-              stream=None) -> None:
+              echo_type: str = "epg_fisp", *, nmaps: int = NMAPS, iterations: int = 3,
+              max_rel_step: float = 0.2, tol: float = 1e-4, img_stride: int = 0, d_b1map=None,
+              d_m0=None, stream=None) -> None:
     """Gauss-Newton refinement of matched (T1, T2) in place: d_maps device
     float32 [nvoxels][nmaps] (T1, T2, B0, B1, PD) as MRF_match writes them;
     d_img device complex64 voxels; d_b1map optional device B1 map (else the
-    maps' B1 column)."""
+    maps' B1 column).  At most `iterations` steps per voxel; a voxel stops
+    once a step moved T1 and T2 by at most tol (relative; 0: never early)."""
     h_mrf = _schedule(h_mrf, NREPS)
     _check(lib().snapmrf_refine_gn(_ptr(d_maps), nmaps, _ptr(d_img), img_stride, _ptr(d_b1map),
                                    h_mrf.ctypes.data, nreps,
                                    NREPS, nvoxels, nstates, echo_type.encode(), iterations, max_rel_step,
-                                   _ptr(d_m0), _stream_ptr(stream)))
+                                   tol, _ptr(d_m0), _stream_ptr(stream)))

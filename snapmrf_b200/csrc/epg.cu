@@ -13,6 +13,8 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -65,6 +67,17 @@ static int parse_echo(const char *s) {
 // Lanes per atom (power of two) and states per lane (<= smax, a multiple of
 // `step`) for w states: least padding first, then more states per lane.
 static void choose_layout(int w, int smax, int step, int *L, int *S) {
+    // SNAPMRF_DICT_LAYOUT="L,S" (lanes per atom, states per lane) overrides
+    // the choice when it is a valid layout for w states
+    if (const char *e = getenv("SNAPMRF_DICT_LAYOUT")) {
+        int l = 0, s = 0;
+        if (sscanf(e, "%d,%d", &l, &s) == 2 && l >= 1 && l <= 32 && (l & (l - 1)) == 0 && s >= step &&
+            s <= smax && s % step == 0 && l * s >= w) {
+            *L = l;
+            *S = s;
+            return;
+        }
+    }
     int bestL = 32, bestS = smax, bestPad = 1 << 30;
     for (int s = smax; s >= step; s -= step)
         for (int l = 1; l <= 32; l *= 2)

@@ -354,6 +354,13 @@ struct GnArgs {
     const float *b1map;       // optional [nvox]: B1 of each voxel
     float *m0;                // optional out [nvox]: |rho| with x ~ rho * s
     float max_rel_step;
+    // early exit: voxels of list_in[0 .. *count_in) (all voxels when null);
+    // voxels whose step exceeds tol of T1 or T2 are appended to list_out
+    const int *list_in;
+    const int *count_in;
+    int *list_out;
+    int *count_out;
+    float tol;
 };
 
 // A voxel whose map holds no usable start (not finite, T2 <= 0, T1 <= T2)
@@ -435,11 +442,16 @@ __global__ void __launch_bounds__(kThreads) gn_kernel(GnArgs a, int chunk) {
     const bool lane0 = gl == 0;
     GnStep *sQ = reinterpret_cast<GnStep *>(gn_smem);              // [apc][chunk]
     float *sV = reinterpret_cast<float *>(sQ + apc * chunk);       // [apc][4]: T1, T2, B1, ok
+    long long *sI = reinterpret_cast<long long *>(sV + apc * 4);  // [apc]: voxel or -1
     const long long vox0 = (long long)blockIdx.x * apc;
+    const long long nlist = a.list_in ? (long long)*a.count_in : a.nvox;
     for (int i = tid; i < apc; i += kThreads) {
-        const long long v = vox0 + i;
+        const long long slot = vox0 + i;
+        long long v = -1;
+        if (slot < nlist) v = a.list_in ? (long long)a.list_in[slot] : slot;
+        sI[i] = v;
         float T1 = 2.f, T2 = 1.f, B1 = 1.f, ok = 0.f;
-        if (v < a.nvox) {
+        if (v >= 0) {
             const float *mp = a.maps + v * a.nmaps;
             const float t1 = mp[0], t2 = mp[1];
             const float b1 = a.b1map ? a.b1map[v] : (a.nmaps >= 4 ? mp[3] : 1.f);
@@ -455,8 +467,9 @@ __global__ void __launch_bounds__(kThreads) gn_kernel(GnArgs a, int chunk) {
         sV[4 * i + 2] = B1;
         sV[4 * i + 3] = ok;
     }
-    __syncthreads();
-    const long long v = vox0 + g;
+    // a block without a usable voxel leaves at once (uniformly)
+    if (!__syncthreads_or(tid < apc && sV[4 * tid + 3] != 0.f)) return;
+    const long long v = sI[g];
     const bool active = sV[4 * g + 3] != 0.f;
     const int T = a.sch.nreps, w = a.w;
     const int k0 = gl * 2 * P;
@@ -493,9 +506,9 @@ __global__ void __launch_bounds__(kThreads) gn_kernel(GnArgs a, int chunk) {
             q.dE2 = q.E2 * tr * r2 * r2;
             q.Ea = __expf(-ta * r2);
             q.dEa = q.Ea * ta * r2 * r2;
-            const long long vv = vox0 + ga;
+            const long long vv = sI[ga];
             float2 xv = make_float2(0.f, 0.f);
-            if (vv < a.nvox) xv = a.img[vv * a.img_stride + t];
+            if (vv >= 0) xv = a.img[vv * a.img_stride + t];
             q.xr = xv.x;
             q.xi = xv.y;
             sQ[ga * chunk + i] = q;
@@ -597,6 +610,8 @@ __global__ void __launch_bounds__(kThreads) gn_kernel(GnArgs a, int chunk) {
     n1 = fmaxf(n1, n2 * (1.f + 1e-4f));  // keep T1 > T2 > 0
     mp[0] = n1;
     mp[1] = n2;
+    if (a.list_out && !(fabsf(n1 - T1) <= a.tol * T1 && fabsf(n2 - T2) <= a.tol * T2))
+        a.list_out[atomicAdd(a.count_out, 1)] = (int)v;
 }
 
 constexpr int kGnMaxPairs = 7;  // 8 pairs with both tangents exceed 255 registers
@@ -758,15 +773,16 @@ extern "C" int snapmrf_epg_adjoint(const float *d_params, int nparams, const flo
 }
 
 extern "C" int snapmrf_refine_gn(float *d_maps, int nmaps, const float *img, size_t img_stride,
-                                 const float *d_b1map, const float *h_mrf, size_t nreps, size_t NREPS, size_t nvoxels, int nstates,
-                                 const char *echo_type, int iterations, float max_rel_step, float *d_m0,
-                                 void *stream) {
+                                 const float *d_b1map, const float *h_mrf, size_t nreps, size_t NREPS,
+                                 size_t nvoxels, int nstates, const char *echo_type, int iterations,
+                                 float max_rel_step, float tol, float *d_m0, void *stream) {
     cudaStream_t st = (cudaStream_t)stream;
     if (!d_maps || !img || !h_mrf) SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "refine_gn: null pointer");
     if (nmaps < 2 || nreps == 0 || nreps > NREPS || nvoxels == 0 || nstates < 1 ||
         nstates > 32 * 2 * kGnMaxPairs || iterations < 0)
         SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "refine_gn: bad sizes");
-    if (nreps > 0x7fffffff) SNAPMRF_FAIL(SNAPMRF_ERR_UNSUPPORTED, "refine_gn: too many time points");
+    if (nreps > 0x7fffffff || nvoxels > 0x7fffffff)
+        SNAPMRF_FAIL(SNAPMRF_ERR_UNSUPPORTED, "refine_gn: too many time points or voxels");
     if (!img_stride) img_stride = nreps;
     if (img_stride < nreps) SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "refine_gn: img_stride < nreps");
     const int shift = echo_shift(echo_type);
@@ -790,17 +806,40 @@ extern "C" int snapmrf_refine_gn(float *d_maps, int nmaps, const float *img, siz
     a.b1map = d_b1map;
     a.m0 = d_m0;
     a.max_rel_step = max_rel_step > 0.f ? max_rel_step : 0.2f;
+    a.tol = tol;
+    a.list_in = a.count_in = nullptr;
+    a.list_out = a.count_out = nullptr;
+    // voxel lists of the early exit: two lists and two counters
+    const bool early = tol > 0.f && iterations > 1;
+    DeviceScratch lists;
+    int *lst[2] = {nullptr, nullptr}, *cnt[2] = {nullptr, nullptr};
+    if (early) {
+        SNAPMRF_CUDA(lists.alloc((2 * nvoxels + 2) * sizeof(int), st));
+        lst[0] = lists.as<int>();
+        lst[1] = lst[0] + nvoxels;
+        cnt[0] = lst[1] + nvoxels;
+        cnt[1] = cnt[0] + 1;
+    }
     const int apc = kThreads / L;
     // steps staged per chunk: at most kGnChunk, within 48 KB of shared memory
-    const size_t smem_cap = 48 * 1024 - (size_t)apc * 4 * sizeof(float);
-    const int chunk = (int)std::min<size_t>(kGnChunk, smem_cap / ((size_t)apc * sizeof(GnStep)));
-    const size_t smem = (size_t)apc * chunk * sizeof(GnStep) + (size_t)apc * 4 * sizeof(float);
+    const size_t fixed = (size_t)apc * (4 * sizeof(float) + sizeof(long long));
+    const int chunk = (int)std::min<size_t>(kGnChunk, (48 * 1024 - fixed) / ((size_t)apc * sizeof(GnStep)));
+    const size_t smem = (size_t)apc * chunk * sizeof(GnStep) + fixed;
     dim3 grid((unsigned)((nvoxels + apc - 1) / apc));
     for (int it = 0; it < iterations; it++) {
+        if (early) {
+            a.list_in = it == 0 ? nullptr : lst[(it - 1) & 1];
+            a.count_in = it == 0 ? nullptr : cnt[(it - 1) & 1];
+            a.list_out = it + 1 < iterations ? lst[it & 1] : nullptr;
+            a.count_out = it + 1 < iterations ? cnt[it & 1] : nullptr;
+            if (a.count_out) SNAPMRF_CUDA(cudaMemsetAsync(a.count_out, 0, sizeof(int), st));
+        }
         SNAPMRF_GN_DISPATCH(P, true, grid, smem, st, a, chunk);
         SNAPMRF_LAUNCH_CHECK();
     }
     if (nmaps >= 5 || d_m0 || (d_b1map && nmaps >= 4)) {
+        a.list_in = a.count_in = nullptr;
+        a.list_out = a.count_out = nullptr;
         SNAPMRF_GN_DISPATCH(P, false, grid, smem, st, a, chunk);
         SNAPMRF_LAUNCH_CHECK();
     }

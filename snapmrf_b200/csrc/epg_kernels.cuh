@@ -443,8 +443,16 @@ inline size_t epg_real_smem_bytes(int L) {
            (size_t)apc * kReadoutStride * sizeof(float2) + (size_t)apc * 3 * sizeof(float);
 }
 
+// (An explicit minimum of 1 block per SM lets ptxas use more registers and
+// costs a resident block per SM; SNAPMRF_EPG_REAL_MIN_BLOCKS is for tuning.)
+#ifdef SNAPMRF_EPG_REAL_MIN_BLOCKS
+#define SNAPMRF_EPG_REAL_BOUNDS __launch_bounds__(kEpgThreads, SNAPMRF_EPG_REAL_MIN_BLOCKS)
+#else
+#define SNAPMRF_EPG_REAL_BOUNDS __launch_bounds__(kEpgThreads)
+#endif
+
 template <int ECHO, int P, bool TAIL>
-__global__ void __launch_bounds__(kEpgThreads) epg_real_kernel(EpgArgs a) {
+__global__ void SNAPMRF_EPG_REAL_BOUNDS epg_real_kernel(EpgArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr int NF = 4;
     constexpr int FS = epg_f_stride(ECHO_FISP);
@@ -478,12 +486,12 @@ __global__ void __launch_bounds__(kEpgThreads) epg_real_kernel(EpgArgs a) {
         sP[3 * i + 1] = t2;
         sP[3 * i + 2] = 0.f;
     }
-    __syncthreads();
 
     const float *alpha = a.alpha + blk * nreps;
     const float *phi = a.sched + nreps;
     const float *TR = a.sched + 2 * nreps;
     const float *TE = a.sched + 3 * nreps;
+    __syncthreads();
     const int w = a.nstates;
     // TAIL layouts: 0 at slot w (cleared after each shift), 1 elsewhere
     float2 tail_keep = make_float2(1.f, 1.f);

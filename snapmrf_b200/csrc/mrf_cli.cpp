@@ -53,6 +53,9 @@ static void usage() {
             "\t    --topk 8|16\t\t\t candidates rescored in FP32 (tensor-core forms)\n"
             "\t    --all-b1-blocks\t\t generate every B1 block for non-SSFP echo types\n"
             "\t    --normalize\t\t\t unit-norm every atom\n"
+            "\t    --refine n\t\t\t Gauss-Newton refinement of T1/T2 after matching, at\n"
+            "\t\t\t\t\t most n iterations per voxel (epg_fisp / epg_sr with\n"
+            "\t\t\t\t\t every RF phase 0; flip angle x B1 as --all-b1-blocks)\n"
             "\t-h, --help\t\t\t show this help\n");
 }
 
@@ -83,9 +86,9 @@ int main(int argc, char **argv) {
     const char *T1 = "20:20:3000", *T2 = "20:10:1000", *B0 = "0", *B1 = "1", *echo_type = "epg_ssfp";
     int nparams = 4, nmaps = 5, nstates = 101;
     size_t nreps = 1500, NATOMS_req = 0;
-    int precision = SNAPMRF_PREC_FP32, topk = 0;
+    int precision = SNAPMRF_PREC_FP32, topk = 0, refine = 0;
     unsigned dict_flags = 0;
-    enum { OPT_PREC = 1000, OPT_TOPK, OPT_ALLB1, OPT_NORM };
+    enum { OPT_PREC = 1000, OPT_TOPK, OPT_ALLB1, OPT_NORM, OPT_REFINE };
     static struct option longopts[] = {
         {"b1map", 1, NULL, 'M'},      {"atoms", 1, NULL, 'a'},       {"map", 1, NULL, 'm'},
         {"maps", 1, NULL, 'm'},       {"params", 1, NULL, 'p'},      {"T1", 1, NULL, 't'},
@@ -94,7 +97,8 @@ int main(int argc, char **argv) {
         {"nreps", 1, NULL, 'T'},      {"timepoints", 1, NULL, 'T'},  {"gridsize", 1, NULL, 'G'},
         {"blocksize", 1, NULL, 'B'},  {"NATOMS", 1, NULL, 'N'},      {"help", 0, NULL, 'h'},
         {"precision", 1, NULL, OPT_PREC}, {"topk", 1, NULL, OPT_TOPK},
-        {"all-b1-blocks", 0, NULL, OPT_ALLB1}, {"normalize", 0, NULL, OPT_NORM}, {NULL, 0, NULL, 0}};
+        {"all-b1-blocks", 0, NULL, OPT_ALLB1}, {"normalize", 0, NULL, OPT_NORM},
+        {"refine", 1, NULL, OPT_REFINE},  {NULL, 0, NULL, 0}};
     opterr = 0;
     int c;
     while ((c = getopt_long(argc, argv, "M:N:a:m:p:t:s:b:r:w:e:T:G:B:h", longopts, NULL)) != -1) {
@@ -121,6 +125,7 @@ int main(int argc, char **argv) {
         case OPT_TOPK: topk = atoi(optarg); break;
         case OPT_ALLB1: dict_flags |= SNAPMRF_DICT_ALL_B1_BLOCKS; break;
         case OPT_NORM: dict_flags |= SNAPMRF_DICT_NORMALIZE; break;
+        case OPT_REFINE: refine = atoi(optarg); break;
         case 'h':
         default: usage(); return 1;
         }
@@ -230,6 +235,30 @@ int main(int argc, char **argv) {
         cuda_check(cudaStreamSynchronize(st), "matching");
         cudaEventElapsedTime(&ms, e0, e1);
         printf("Elapsed matching time: %.4f s\n\n", ms / 1e3);
+        if (refine > 0) {
+            // the voxels and the B1 map on the device, then Gauss-Newton in place
+            float *d_img = NULL, *d_b1 = NULL;
+            const size_t m = nreps < nt ? nreps : nt;
+            cuda_check(cudaMalloc((void **)&d_img, nvoxels * nt * 2 * sizeof(float)), "cudaMalloc");
+            cuda_check(cudaMemcpyAsync(d_img, img.data, nvoxels * nt * 2 * sizeof(float), cudaMemcpyHostToDevice,
+                                       st), "cudaMemcpy");
+            if (in_b1map) {
+                cuda_check(cudaMalloc((void **)&d_b1, nvoxels * sizeof(float)), "cudaMalloc");
+                cuda_check(cudaMemcpyAsync(d_b1, b1ra.data, nvoxels * sizeof(float), cudaMemcpyHostToDevice, st),
+                           "cudaMemcpy");
+            }
+            printf("Refining (Gauss-Newton, at most %d iterations)...\n", refine);
+            cudaEventRecord(e0, st);
+            check(snapmrf_refine_gn(d_maps, nmaps, d_img, nt, d_b1, h_mrf.data(), m, NREPS, nvoxels, nstates,
+                                    echo_type, refine, 0.2f, 1e-4f, NULL, st),
+                  "refine_gn");
+            cudaEventRecord(e1, st);
+            cuda_check(cudaStreamSynchronize(st), "refinement");
+            cudaEventElapsedTime(&ms, e0, e1);
+            printf("Elapsed refinement time: %.4f s\n\n", ms / 1e3);
+            cudaFree(d_img);
+            if (d_b1) cudaFree(d_b1);
+        }
         if (!out_maps) out_maps = "../result/maps.ra";
         printf("Output maps: %s\n", out_maps);
         std::vector<float> h_maps(nmaps * nvoxels);

@@ -188,7 +188,7 @@ def gn_step_fp64(orc, theta, x, h, w, echo="epg_fisp"):
     return np.linalg.solve(A, b), abs(rho), abs(np.vdot(s, x)) / np.sqrt(ss)
 
 
-def run_gn(snap, theta, img, h, w, iterations, echo="epg_fisp", max_rel_step=0.2, b1map=None):
+def run_gn(snap, theta, img, h, w, iterations, echo="epg_fisp", max_rel_step=0.2, b1map=None, tol=1e-4):
     """theta [n][3] = (T1, T2, B1) -> (T1, T2, B1) [n][3], PD, M0."""
     import torch
     n = theta.shape[0]
@@ -199,7 +199,7 @@ def run_gn(snap, theta, img, h, w, iterations, echo="epg_fisp", max_rel_step=0.2
     d_m0 = torch.full((n,), -1.0, device="cuda")
     d_b1 = None if b1map is None else torch.from_numpy(np.ascontiguousarray(b1map, np.float32)).cuda()
     snap.refine_gn(d_maps, d_img, h, h.shape[1], h.shape[1], n, w, echo, iterations=iterations,
-                   max_rel_step=max_rel_step, d_b1map=d_b1, d_m0=d_m0)
+                   max_rel_step=max_rel_step, tol=tol, d_b1map=d_b1, d_m0=d_m0)
     torch.cuda.synchronize()
     out = d_maps.cpu().numpy()
     assert np.all(out[:, 2] == 0)
@@ -285,3 +285,21 @@ def test_gn_uses_the_b1_map(snap, oracle):
     np.testing.assert_array_equal(got[:, 2], truth[:, 3])
     np.testing.assert_allclose(got[:, 0], truth[:, 0], rtol=2e-3)
     np.testing.assert_allclose(got[:, 1], truth[:, 1], rtol=2e-3)
+
+
+def test_gn_early_exit_agrees_with_full_iterations(snap, oracle):
+    """Voxels that stop once their step is below tol end where running every
+    iteration on every voxel ends (to well within tol's effect); 333 voxels
+    exercise partly filled blocks of the compacted voxel lists."""
+    T, w = 300, 25
+    h = schedule(T, seed=16)
+    truth, rho, x = synthetic_voxels(oracle, 333, h, w, seed=16, noise=0.003)
+    rng = np.random.default_rng(17)
+    theta0 = np.stack([truth[:, 0] * rng.uniform(0.9, 1.1, 333), truth[:, 1] * rng.uniform(0.9, 1.1, 333),
+                       truth[:, 3]], 1).astype(np.float32)
+    full, pd_f, _ = run_gn(snap, theta0, x, h, w, 4, tol=0.0)
+    early, pd_e, _ = run_gn(snap, theta0, x, h, w, 4, tol=1e-4)
+    np.testing.assert_allclose(early[:, :2], full[:, :2], rtol=5e-4)
+    np.testing.assert_allclose(pd_e, pd_f, rtol=1e-5)
+    one, _, _ = run_gn(snap, theta0, x, h, w, 1, tol=1e-4)
+    assert not np.allclose(one[:, :2], full[:, :2], rtol=5e-4)
