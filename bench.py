@@ -275,6 +275,18 @@ def peaks() -> dict:
     return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0, "source": "fallback"}
 
 
+def reduce_over_ranks(values, op: str, device, world: int) -> list:
+    """Element-wise max or min of `values` over all ranks (identity for one
+    rank); every rank calls it at the same point with the same length."""
+    if world <= 1:
+        return [float(v) for v in values]
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.MIN)
+    return t.tolist()
+
+
 def fp32_peak_tflops(sm_mhz: float) -> float:
     """FP32 FMA peak of 148 SMs x 128 lanes x 2 flop at the given clock."""
     return 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
@@ -382,11 +394,9 @@ def run_ours(args) -> None:
         tie = forms[f]["maps"][:, 4] >= pd32 * (1 - 1e-6)
         raw[f] = float(np.mean(same))
         agree[f] = float(np.mean(same | tie))
-    if world > 1:
-        a = torch.tensor([agree["bf16"], agree["fp16"], raw["bf16"], raw["fp16"]], dtype=torch.float64, device=dev)
-        dist.all_reduce(a, op=dist.ReduceOp.MIN)
-        agree = {"bf16": float(a[0]), "fp16": float(a[1])}
-        raw = {"bf16": float(a[2]), "fp16": float(a[3])}
+    a = reduce_over_ranks([agree["bf16"], agree["fp16"], raw["bf16"], raw["fp16"]], "min", dev, world)
+    agree = {"bf16": a[0], "fp16": a[1]}
+    raw = {"bf16": a[2], "fp16": a[3]}
     # headline: the fastest tensor-core form whose argmax agrees with the FP32
     # form on >= 99.9 % of voxels in this very run, else the FP32 form
     ok = [f for f in ("bf16", "fp16") if agree[f] >= 0.999]
@@ -443,13 +453,10 @@ def run_ours(args) -> None:
     # max over ranks
     names = list(PRECS)
     gnames = list(gn_forms)
-    t = torch.tensor([elapsed_ms, e2e_ms, dict_ms, match_ms] +
-                     [forms[f]["elapsed_ms"] for f in names] + [forms[f]["match_ms"] for f in names] +
-                     [gn_forms[f]["elapsed_ms"] for f in gnames] + [gn_forms[f]["gn_ms"] for f in gnames],
-                     dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    t = t.tolist()
+    t = reduce_over_ranks([elapsed_ms, e2e_ms, dict_ms, match_ms] +
+                          [forms[f]["elapsed_ms"] for f in names] + [forms[f]["match_ms"] for f in names] +
+                          [gn_forms[f]["elapsed_ms"] for f in gnames] + [gn_forms[f]["gn_ms"] for f in gnames],
+                          "max", dev, world)
     elapsed_ms, e2e_ms, dict_ms, match_ms = t[:4]
     form_ms = dict(zip(names, t[4:4 + len(names)]))
     form_match_ms = dict(zip(names, t[4 + len(names):4 + 2 * len(names)]))

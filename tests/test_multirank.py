@@ -1,0 +1,88 @@
+"""Multi-rank logic of bench.py on the CPU: the cross-rank reductions over a
+world-size-2 gloo group, the per-rank slices, and the reference arm under
+torchrun (rank 0 alone prints one line)."""
+import json
+import os
+import socket
+import subprocess
+import sys
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+ROOT = Path(__file__).resolve().parent.parent
+
+
+def _free_port() -> int:
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _reduce_worker(rank, world, port, out_dir):
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    sys.path.insert(0, str(ROOT))
+    import bench
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        dev = torch.device("cpu")
+        mx = bench.reduce_over_ranks([rank, -rank, 10.0 * rank + 1], "max", dev, world)
+        mn = bench.reduce_over_ranks([rank, -rank, 10.0 * rank + 1], "min", dev, world)
+        (Path(out_dir) / f"r{rank}.json").write_text(json.dumps({"max": mx, "min": mn}))
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_reduce_over_ranks_gloo(tmp_path):
+    import torch.multiprocessing as mp
+    port = _free_port()
+    mp.start_processes(_reduce_worker, args=(2, port, str(tmp_path)), nprocs=2, start_method="spawn")
+    for r in range(2):
+        d = json.loads((tmp_path / f"r{r}.json").read_text())
+        assert d["max"] == [1.0, 0.0, 11.0]
+        assert d["min"] == [0.0, -1.0, 1.0]
+
+
+def test_reduce_over_ranks_single_rank_is_identity():
+    sys.path.insert(0, str(ROOT))
+    import bench
+    assert bench.reduce_over_ranks([3, 1.5], "max", None, 1) == [3.0, 1.5]
+
+
+def test_each_rank_gets_its_own_slice():
+    """Weak scaling: rank r simulates the slice seeded by r; the same rank
+    always gets the same slice, and the B1 field is the same on every rank."""
+    sys.path.insert(0, str(ROOT))
+    import bench
+    a0 = bench.phantom(0, nx=32)
+    a0b = bench.phantom(0, nx=32)
+    a1 = bench.phantom(1, nx=32)
+    for x, y in zip(a0, a0b):
+        np.testing.assert_array_equal(x, y)
+    assert not np.array_equal(a0[1], a1[1])
+    np.testing.assert_array_equal(a0[0], a1[0])
+
+
+@pytest.mark.timeout(600)
+def test_reference_arm_under_torchrun_prints_one_line():
+    port = _free_port()
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
+           "--master-addr", "127.0.0.1", "--master-port", str(port), str(ROOT / "bench.py"),
+           "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "3", "--cpu-seconds", "0.3"]
+    env = dict(os.environ, OMP_NUM_THREADS="2")
+    r = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=540, env=env,
+                       stdin=subprocess.DEVNULL)
+    assert r.returncode == 0, r.stderr[-3000:]
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1, r.stdout
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["n_gpus"] == 2
+    assert d["value"] > 0 and d["e2e"]["h2d_bytes_per_step"] == 0
+    assert d["cpu_baseline"]["kind"] == "port"
