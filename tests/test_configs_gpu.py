@@ -24,12 +24,16 @@ def _scores(atoms, img):
 
 
 def _assert_indices_equal_where_separated(idx, ref_idx, scores, gap=2e-5):
-    """The FP32 matching against the FP64 oracle: equal picks wherever the
-    exact best score leads the runner-up by more than `gap` (relative), a
-    margin above the rounding of a 1000-term FP32 dot product."""
+    """The FP32 matching against the FP64 oracle: every pick scores within
+    `gap` (relative) of the exact best, a margin above the rounding of a
+    1000-term FP32 dot product, and the picks are equal wherever the exact
+    best leads the runner-up by more than that."""
+    n = scores.shape[0]
+    best = scores.max(axis=1)
+    assert np.all(scores[np.arange(n), idx] >= best * (1 - gap))
     srt = np.sort(scores, axis=1)
     sure = (srt[:, -1] - srt[:, -2]) > gap * srt[:, -1]
-    assert sure.mean() > 0.9
+    assert sure.mean() > 0.5
     np.testing.assert_array_equal(idx[sure], ref_idx[sure])
 
 
