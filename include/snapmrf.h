@@ -172,6 +172,11 @@ int snapmrf_normalize(float *d_atoms, size_t nreps, size_t NATOMS, float *d_norm
 #define SNAPMRF_PREC_BF16 1
 /* The same with FP16 operands (8x finer mantissa than BF16, same rate). */
 #define SNAPMRF_PREC_FP16 2
+/* The same with FP8-E4M3 operands (twice the BF16 rate, 3 mantissa bits):
+ * each atom row and each voxel row is scaled so its largest component is
+ * 448, scores are divided by the atom's squared scale before the top-k
+ * (16 by default), and the k candidates are rescored in FP32. */
+#define SNAPMRF_PREC_FP8 3
 
 /* Skip the device check that every B1 block holds one B1 value (true for
  * any params table built by trans_params); without the flag the call

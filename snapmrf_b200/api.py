@@ -32,6 +32,7 @@ DICT_REFERENCE_ORDER = 0x4
 PREC_FP32 = 0
 PREC_BF16 = 1
 PREC_FP16 = 2
+PREC_FP8 = 3
 MATCH_ASSUME_UNIFORM_B1 = 0x1
 
 ECHO_TYPES = ("epg_ssfp", "roa_ssfp", "epg_sr", "epg_se", "epg_tse1", "epg_tse2", "epg_fisp")

@@ -4,7 +4,7 @@
 // this library unchanged.  Each function cites the reference function whose
 // behaviour it keeps; every computation goes through libsnapmrf.so.
 //
-// Environment: SNAPMRF_PRECISION = fp32 (default) | bf16 | fp16 selects the
+// Environment: SNAPMRF_PRECISION = fp32 (default) | bf16 | fp16 | fp8 selects the
 // matching form used by MRF_match.
 #include <cerrno>
 #include <cmath>
@@ -198,7 +198,8 @@ static int env_precision() {
     if (!p || !strcmp(p, "fp32")) return SNAPMRF_PREC_FP32;
     if (!strcmp(p, "bf16")) return SNAPMRF_PREC_BF16;
     if (!strcmp(p, "fp16")) return SNAPMRF_PREC_FP16;
-    fprintf(stderr, "SNAPMRF_PRECISION must be fp32, bf16 or fp16\n");
+    if (!strcmp(p, "fp8")) return SNAPMRF_PREC_FP8;
+    fprintf(stderr, "SNAPMRF_PRECISION must be fp32, bf16, fp16 or fp8\n");
     exit(EX_USAGE);
 }
 

@@ -178,7 +178,8 @@ extern "C" int snapmrf_mrf_match(float *d_maps, const float *img, int img_on_hos
         SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "MRF_match: bad sizes (nreps %zu, nvoxels %zu, NATOMS %zu, natoms %zu)",
                      nreps, nvoxels, NATOMS, natoms);
     int precision = opts ? opts->precision : SNAPMRF_PREC_FP32;
-    if (precision != SNAPMRF_PREC_FP32 && precision != SNAPMRF_PREC_BF16 && precision != SNAPMRF_PREC_FP16)
+    if (precision != SNAPMRF_PREC_FP32 && precision != SNAPMRF_PREC_BF16 && precision != SNAPMRF_PREC_FP16 &&
+        precision != SNAPMRF_PREC_FP8)
         SNAPMRF_FAIL(SNAPMRF_ERR_UNSUPPORTED, "MRF_match: unknown precision %d", precision);
     size_t img_stride = (opts && opts->img_stride) ? opts->img_stride : nreps;
     size_t atom_stride = (opts && opts->atom_stride) ? opts->atom_stride : nreps;
@@ -229,7 +230,7 @@ extern "C" int snapmrf_mrf_match(float *d_maps, const float *img, int img_on_hos
     }
 
     const long long nvox = (long long)nvoxels;
-    if (precision == SNAPMRF_PREC_BF16 || precision == SNAPMRF_PREC_FP16) {
+    if (precision == SNAPMRF_PREC_BF16 || precision == SNAPMRF_PREC_FP16 || precision == SNAPMRF_PREC_FP8) {
         if (general)
             SNAPMRF_FAIL(SNAPMRF_ERR_UNSUPPORTED,
                          "MRF_match: tensor-core matching needs every B1 block to hold one B1 value");
@@ -248,8 +249,8 @@ extern "C" int snapmrf_mrf_match(float *d_maps, const float *img, int img_on_hos
         q.nvox = nvox;
         q.nblocks = (int)nblocks;
         q.b1map = d_b1;
-        q.half = precision == SNAPMRF_PREC_FP16;
-        q.topk = (opts && opts->topk) ? opts->topk : (q.half ? 8 : 16);
+        q.fmt = precision == SNAPMRF_PREC_FP16 ? 1 : precision == SNAPMRF_PREC_FP8 ? 2 : 0;
+        q.topk = (opts && opts->topk) ? opts->topk : (q.fmt == 1 ? 8 : 16);
         if (q.topk != 8 && q.topk != 16)
             SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "MRF_match: topk must be 8 or 16 (got %d)", q.topk);
         return match_bf16(q, st);

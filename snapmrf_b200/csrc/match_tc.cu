@@ -1,4 +1,4 @@
-// Tensor-core matching on sm_100a: BF16 (or FP16) real-stacked scores on
+// Tensor-core matching on sm_100a: BF16, FP16 or FP8-E4M3 real-stacked scores on
 // tcgen05 with FP32 accumulation in TMEM, a per-voxel running top-k (8 or
 // 16) in the epilogue, then exact FP32 rescoring of the k candidates (the maps then follow the
 // reference's rules: first argmax of |s| among them, PD = |s|).
@@ -27,6 +27,7 @@
 #include <cuda_runtime.h>
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
+#include <cuda_fp8.h>
 
 #include <algorithm>
 #include <mutex>
@@ -49,6 +50,8 @@ constexpr int BM = 128;                 // voxels per tile (TMEM lanes)
 constexpr int BA = 128;                 // atoms per tile
 constexpr int BN = 2 * BA;              // B rows per tile
 constexpr int BK = 64;                  // bf16 per 128-byte swizzled row
+constexpr int BK8 = 128;                // e4m3 per 128-byte swizzled row
+constexpr float E4M3_MAX = 448.f;       // largest finite E4M3 value
 constexpr int STAGES = 4;
 constexpr int A_BYTES = BM * BK * 2;    // 16 KB
 constexpr int B_BYTES = BN * BK * 2;    // 32 KB
@@ -66,6 +69,7 @@ struct Args {
     long long bin_natoms;
     int nk;                       // K chunks of BK
     uint32_t idesc;               // tcgen05 instruction descriptor
+    const float *ascale2;         // E4M3: [NATOMS] 1 / (atom scale)^2
     float *top_s;                 // [slots][TOPK]
     int *top_i;                   // [slots][TOPK]
     int *err;
@@ -96,9 +100,12 @@ __device__ __forceinline__ void topk_insert(float *ts, int *ti, float s, int i) 
     }
 }
 
-template <int TOPK>
+// FP8: E4M3 operands on kind::f8f6f4, one 128-byte row holding 128 elements
+// of K, and scores divided by the atom's squared scale before the top-k.
+template <int TOPK, bool FP8>
 __global__ void __launch_bounds__(THREADS, 1)
 match_bf16_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, Args p) {
+    constexpr int BKE = FP8 ? BK8 : BK;   // K elements per stage
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t full[STAGES], empty[STAGES], tfull[2], tempty[2], mma_done;
     __shared__ uint32_t tmem_base_sh;
@@ -151,8 +158,8 @@ match_bf16_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
                         }
                         sm100::mbar_arrive_expect_tx(&full[stage], STAGE_BYTES);
                         unsigned char *sa = smem + stage * STAGE_BYTES;
-                        sm100::tma_load_2d(sa, &tmA, &full[stage], kc * BK, vrow);
-                        sm100::tma_load_2d(sa + A_BYTES, &tmB, &full[stage], kc * BK, brow);
+                        sm100::tma_load_2d(sa, &tmA, &full[stage], kc * BKE, vrow);
+                        sm100::tma_load_2d(sa + A_BYTES, &tmB, &full[stage], kc * BKE, brow);
                         issued[stage] = (int)phase;
                         if (++stage == STAGES) {
                             stage = 0;
@@ -189,11 +196,18 @@ match_bf16_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
                         sm100::tc_fence_after();
                         const uint32_t a_addr = sm100::smem_u32(smem + stage * STAGE_BYTES);
                         const uint32_t b_addr = a_addr + A_BYTES;
+                        // four MMAs of 32 bytes of K each (16 bf16 / 32 e4m3)
 #pragma unroll
-                        for (int k = 0; k < BK / 16; k++)
-                            sm100::mma_bf16(d, sm100::make_sw128_desc(a_addr + k * 32),
-                                            sm100::make_sw128_desc(b_addr + k * 32), idesc,
-                                            (kc > 0 || k > 0) ? 1u : 0u);
+                        for (int k = 0; k < 4; k++) {
+                            if (FP8)
+                                sm100::mma_f8f6f4(d, sm100::make_sw128_desc(a_addr + k * 32),
+                                                  sm100::make_sw128_desc(b_addr + k * 32), idesc,
+                                                  (kc > 0 || k > 0) ? 1u : 0u);
+                            else
+                                sm100::mma_bf16(d, sm100::make_sw128_desc(a_addr + k * 32),
+                                                sm100::make_sw128_desc(b_addr + k * 32), idesc,
+                                                (kc > 0 || k > 0) ? 1u : 0u);
+                        }
                         sm100::mma_commit(&empty[stage]);
                         if (++stage == STAGES) {
                             stage = 0;
@@ -219,6 +233,8 @@ match_bf16_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
         uint32_t aphase = 0;
         bool ok = true;
         for (long long item = blockIdx.x; item < total && ok; item += gridDim.x) {
+            const float *asc = nullptr;
+            if (FP8) asc = p.ascale2 + (long long)find_bin(p.tile_start, p.nbins, item) * p.bin_natoms;
             float ts[TOPK];
             int ti[TOPK];
 #pragma unroll
@@ -245,8 +261,10 @@ match_bf16_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
 #pragma unroll
                     for (int j = 0; j < 16; j++) {
                         const int atom = abase + c * 16 + j;
-                        const float sc = fmaf(v[2 * j], v[2 * j], v[2 * j + 1] * v[2 * j + 1]);
-                        if (sc > ts[TOPK - 1] && (full_tile || atom < p.bin_natoms)) topk_insert<TOPK>(ts, ti, sc, atom);
+                        const bool valid = full_tile || atom < p.bin_natoms;
+                        float sc = fmaf(v[2 * j], v[2 * j], v[2 * j + 1] * v[2 * j + 1]);
+                        if (FP8) sc *= valid ? __ldg(asc + atom) : 0.f;
+                        if (sc > ts[TOPK - 1] && valid) topk_insert<TOPK>(ts, ti, sc, atom);
                     }
                 }
                 sm100::tc_fence_before();
@@ -354,6 +372,67 @@ __global__ void pack_atoms_kernel(void *B, const float2 *atoms, long long atom_s
     }
 }
 
+// E4M3 A rows: voxel perm[slot] scaled so that its largest component is
+// E4M3_MAX (the argmax over atoms does not depend on the voxel's scale),
+// interleaved (Re, Im), zero padded to Kp bytes.  One warp per slot.
+__global__ void pack_voxels_e4m3_kernel(unsigned char *A, const float2 *img, long long img_stride,
+                                        const long long *perm, long long nslots, long long nreps, long long Kp) {
+    const long long slot = (blockIdx.x * (long long)blockDim.x + threadIdx.x) / 32;
+    const int lane = threadIdx.x % 32;
+    if (slot >= nslots) return;
+    const long long v = perm[slot];
+    const float2 *x = img + (v >= 0 ? v : 0) * img_stride;
+    float mx = 0.f;
+    if (v >= 0)
+        for (long long t = lane; t < nreps; t += 32) mx = fmaxf(mx, fmaxf(fabsf(x[t].x), fabsf(x[t].y)));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    const float sc = mx > 0.f ? E4M3_MAX / mx : 0.f;
+    __nv_fp8x2_storage_t *row = reinterpret_cast<__nv_fp8x2_storage_t *>(A + slot * Kp);
+    for (long long t = lane; t < Kp / 2; t += 32) {
+        float2 xv = make_float2(0.f, 0.f);
+        if (v >= 0 && t < nreps) xv = x[t];
+        row[t] = __nv_cvt_float2_to_fp8x2(make_float2(xv.x * sc, xv.y * sc), __NV_SATFINITE, __NV_E4M3);
+    }
+}
+
+// E4M3 B rows: atom a scaled by s_a = E4M3_MAX / (largest component) into
+// row 2a (Re d, Im d) and row 2a+1 (-Im d, Re d); ascale2[a] = 1 / s_a^2
+// undoes the scale on |s|^2.  One warp per atom, eight samples (16 bytes)
+// per lane and step.
+__global__ void pack_atoms_e4m3_kernel(unsigned char *B, float *ascale2, const float2 *atoms,
+                                       long long atom_stride, long long natoms, long long nreps, long long Kp) {
+    const long long a = (blockIdx.x * (long long)blockDim.x + threadIdx.x) / 32;
+    const int lane = threadIdx.x % 32;
+    if (a >= natoms) return;
+    const float2 *src = atoms + a * atom_stride;
+    float mx = 0.f;
+    for (long long t = lane; t < nreps; t += 32) mx = fmaxf(mx, fmaxf(fabsf(src[t].x), fabsf(src[t].y)));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    const float sc = mx > 0.f ? E4M3_MAX / mx : 0.f;
+    if (lane == 0) ascale2[a] = mx > 0.f ? 1.f / (sc * sc) : 0.f;
+    unsigned char *r0 = B + (2 * a) * Kp;
+    unsigned char *r1 = r0 + Kp;
+    for (long long t = 8 * lane; t < Kp / 2; t += 256) {
+        uint32_t o0[4], o1[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            float2 d0 = make_float2(0.f, 0.f), d1 = make_float2(0.f, 0.f);
+            if (t + 2 * u < nreps) d0 = src[t + 2 * u];
+            if (t + 2 * u + 1 < nreps) d1 = src[t + 2 * u + 1];
+            const uint32_t p0 = __nv_cvt_float2_to_fp8x2(make_float2(d0.x * sc, d0.y * sc), __NV_SATFINITE, __NV_E4M3);
+            const uint32_t p1 = __nv_cvt_float2_to_fp8x2(make_float2(d1.x * sc, d1.y * sc), __NV_SATFINITE, __NV_E4M3);
+            const uint32_t q0 = __nv_cvt_float2_to_fp8x2(make_float2(-d0.y * sc, d0.x * sc), __NV_SATFINITE, __NV_E4M3);
+            const uint32_t q1 = __nv_cvt_float2_to_fp8x2(make_float2(-d1.y * sc, d1.x * sc), __NV_SATFINITE, __NV_E4M3);
+            o0[u] = p0 | (p1 << 16);
+            o1[u] = q0 | (q1 << 16);
+        }
+        *reinterpret_cast<uint4 *>(r0 + 2 * t) = make_uint4(o0[0], o0[1], o0[2], o0[3]);
+        *reinterpret_cast<uint4 *>(r1 + 2 * t) = make_uint4(o1[0], o1[1], o1[2], o1[3]);
+    }
+}
+
 // Exact FP32 rescoring of the top-k (k <= 16) per voxel; one warp per slot.  The map
 // gets the candidate with the largest |s| (lowest atom index on ties,
 // nothing unless |s| > 0, like generate_maps' strict '>' from 0).
@@ -443,14 +522,19 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
     return fn;
 }
 
-int make_map(CUtensorMap *m, const void *base, long long rows, long long Kp, int box_rows, bool half) {
+// fmt: 0 bf16, 1 fp16, 2 e4m3 (as bytes); the box is one 128-byte row of K.
+int make_map(CUtensorMap *m, const void *base, long long rows, long long Kp, int box_rows, int fmt) {
     auto enc = encode_fn();
     if (!enc) SNAPMRF_FAIL(SNAPMRF_ERR_CUDA, "MRF_match: cuTensorMapEncodeTiled is not available");
+    const int eb = fmt == 2 ? 1 : 2;
     cuuint64_t dims[2] = {(cuuint64_t)Kp, (cuuint64_t)rows};
-    cuuint64_t strides[1] = {(cuuint64_t)(Kp * 2)};
-    cuuint32_t box[2] = {(cuuint32_t)BK, (cuuint32_t)box_rows};
+    cuuint64_t strides[1] = {(cuuint64_t)(Kp * eb)};
+    cuuint32_t box[2] = {(cuuint32_t)(128 / eb), (cuuint32_t)box_rows};
     cuuint32_t estr[2] = {1, 1};
-    CUresult r = enc(m, half ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(base), dims, strides, box, estr,
+    const CUtensorMapDataType ty = fmt == 2   ? CU_TENSOR_MAP_DATA_TYPE_UINT8
+                                   : fmt == 1 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16
+                                              : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
+    CUresult r = enc(m, ty, 2, const_cast<void *>(base), dims, strides, box, estr,
                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) SNAPMRF_FAIL(SNAPMRF_ERR_CUDA, "MRF_match: cuTensorMapEncodeTiled failed (%d)", (int)r);
@@ -466,7 +550,11 @@ int match_bf16(const TcMatchRequest &q, cudaStream_t st) {
     const long long nvox = q.nvox;
     const int nbins = q.b1map ? q.nblocks : 1;
     const long long bin_natoms = q.b1map ? q.natoms : q.NATOMS;
-    const long long Kp = ((2 * q.nreps + BK - 1) / BK) * BK;
+    const int fmt = q.fmt;
+    const bool fp8 = fmt == 2;
+    const int eb = fp8 ? 1 : 2;           // bytes per element
+    const int bke = fp8 ? BK8 : BK;       // K elements per 128-byte row
+    const long long Kp = ((2 * q.nreps + bke - 1) / bke) * bke;
     const long long cap = ((nvox + BM - 1) / BM + nbins) * BM;  // padded slots, upper bound
     const long long brows = 2 * q.NATOMS;
     if (cap > 0x7fffffffll || brows > 0x7fffffffll || Kp > 0x7fffffffll)
@@ -478,7 +566,8 @@ int match_bf16(const TcMatchRequest &q, cudaStream_t st) {
         bytes += (n + 255) & ~size_t(255);
         return off;
     };
-    const size_t oA = take((size_t)cap * Kp * 2), oB = take((size_t)brows * Kp * 2);
+    const size_t oA = take((size_t)cap * Kp * eb), oB = take((size_t)brows * Kp * eb);
+    const size_t oSc = take(fp8 ? (size_t)q.NATOMS * 4 : 0);
     const size_t oTs = take((size_t)cap * TOPK_MAX * 4), oTi = take((size_t)cap * TOPK_MAX * 4);
     const size_t oPerm = take((size_t)cap * 8), oTile = take((size_t)(nbins + 1) * 8);
     const size_t oCur = take((size_t)(nbins + 1) * 8), oVb = take((size_t)nvox * 4);
@@ -488,7 +577,8 @@ int match_bf16(const TcMatchRequest &q, cudaStream_t st) {
     unsigned char *b = s.as<unsigned char>();
     void *A = b + oA;
     void *B = b + oB;
-    const bool half = q.half;
+    float *ascale2 = reinterpret_cast<float *>(b + oSc);
+    const bool half = fmt == 1;
     float *top_s = reinterpret_cast<float *>(b + oTs);
     int *top_i = reinterpret_cast<int *>(b + oTi);
     long long *perm = reinterpret_cast<long long *>(b + oPerm);
@@ -513,7 +603,17 @@ int match_bf16(const TcMatchRequest &q, cudaStream_t st) {
         global_bin_kernel<<<nblk(cap, 256), 256, 0, st>>>(tile_start, perm, nvox, cap);
         SNAPMRF_LAUNCH_CHECK();
     }
-    {
+    if (fp8) {
+        pack_voxels_e4m3_kernel<<<nblk(cap * 32, 256), 256, 0, st>>>(static_cast<unsigned char *>(A), q.img,
+                                                                      q.img_stride, perm, cap, q.nreps, Kp);
+        SNAPMRF_LAUNCH_CHECK();
+        // Kp is a multiple of 128 bytes, so every 16-byte group of a row is
+        // whole and aligned
+        pack_atoms_e4m3_kernel<<<nblk(q.NATOMS * 32, 256), 256, 0, st>>>(static_cast<unsigned char *>(B), ascale2,
+                                                                          q.atoms, q.atom_stride, q.NATOMS,
+                                                                          q.nreps, Kp);
+        SNAPMRF_LAUNCH_CHECK();
+    } else {
         if (half)
             pack_voxels_kernel<true><<<nblk(cap * 32, 256), 256, 0, st>>>(A, q.img, q.img_stride, perm, cap, q.nreps, Kp);
         else
@@ -530,22 +630,24 @@ int match_bf16(const TcMatchRequest &q, cudaStream_t st) {
         SNAPMRF_LAUNCH_CHECK();
     }
     CUtensorMap mA, mB;
-    int rc = make_map(&mA, A, cap, Kp, BM, half);
+    int rc = make_map(&mA, A, cap, Kp, BM, fmt);
     if (rc) return rc;
-    rc = make_map(&mB, B, brows, Kp, BN, half);
+    rc = make_map(&mB, B, brows, Kp, BN, fmt);
     if (rc) return rc;
 
     int num_sms = 0, dev = 0;
     SNAPMRF_CUDA(cudaGetDevice(&dev));
     SNAPMRF_CUDA(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev));
-    auto kern = q.topk > 8 ? match_bf16_kernel<16> : match_bf16_kernel<8>;
+    auto kern = fp8 ? (q.topk > 8 ? match_bf16_kernel<16, true> : match_bf16_kernel<8, true>)
+                    : (q.topk > 8 ? match_bf16_kernel<16, false> : match_bf16_kernel<8, false>);
     SNAPMRF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
     Args a;
     a.tile_start = tile_start;
     a.nbins = nbins;
     a.bin_natoms = bin_natoms;
-    a.nk = (int)(Kp / BK);
-    a.idesc = half ? sm100::make_idesc_f16(BM, BN) : sm100::make_idesc_bf16(BM, BN);
+    a.nk = (int)(Kp / bke);
+    a.idesc = fp8 ? sm100::make_idesc_e4m3(BM, BN) : half ? sm100::make_idesc_f16(BM, BN) : sm100::make_idesc_bf16(BM, BN);
+    a.ascale2 = fp8 ? ascale2 : nullptr;
     a.top_s = top_s;
     a.top_i = top_i;
     a.err = err;

@@ -17,11 +17,11 @@ struct TcMatchRequest {
     long long nreps, NATOMS, natoms, nvox;
     int nblocks;
     const float *b1map;      // device [nvox] or null
-    bool half;               // fp16 operands instead of bf16
+    int fmt;                 // operands: 0 bf16, 1 fp16, 2 e4m3 (per-row scales)
     int topk;                // candidates rescored in FP32: 8 or 16
 };
 
-// BF16 / FP16 tcgen05 scores + top-k + FP32 rescoring; enqueued on st.
+// BF16 / FP16 / E4M3 tcgen05 scores + top-k + FP32 rescoring; enqueued on st.
 int match_bf16(const TcMatchRequest &q, cudaStream_t st);
 
 }  // namespace snapmrf

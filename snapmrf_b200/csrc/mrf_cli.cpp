@@ -49,7 +49,7 @@ static void usage() {
             "\t\t\t\t\t epg_tse1, epg_tse2, epg_fisp)\n"
             "\t-T, --nreps, --timepoints n\t number of time points\n"
             "\t-G, --gridsize n, -B, --blocksize n  accepted, unused\n"
-            "\t    --precision fp32|bf16|fp16\t matching form (default fp32)\n"
+            "\t    --precision fp32|bf16|fp16|fp8 matching form (default fp32)\n"
             "\t    --topk 8|16\t\t\t candidates rescored in FP32 (tensor-core forms)\n"
             "\t    --all-b1-blocks\t\t generate every B1 block for non-SSFP echo types\n"
             "\t    --normalize\t\t\t unit-norm every atom\n"
@@ -120,7 +120,8 @@ int main(int argc, char **argv) {
             if (!strcmp(optarg, "fp32")) precision = SNAPMRF_PREC_FP32;
             else if (!strcmp(optarg, "bf16")) precision = SNAPMRF_PREC_BF16;
             else if (!strcmp(optarg, "fp16")) precision = SNAPMRF_PREC_FP16;
-            else errx(EX_USAGE, "--precision must be fp32, bf16 or fp16");
+            else if (!strcmp(optarg, "fp8")) precision = SNAPMRF_PREC_FP8;
+            else errx(EX_USAGE, "--precision must be fp32, bf16, fp16 or fp8");
             break;
         case OPT_TOPK: topk = atoi(optarg); break;
         case OPT_ALLB1: dict_flags |= SNAPMRF_DICT_ALL_B1_BLOCKS; break;

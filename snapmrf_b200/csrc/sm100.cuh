@@ -101,6 +101,17 @@ __device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t adesc, uint64
         ::"r"(d_tmem), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
 }
 
+// D (+)= A * B^T with 8-bit A and B (E4M3 / E5M2 as the descriptor says), FP32
+// accumulation; one instruction covers K = 32 (32 bytes of a 128-byte row).
+__device__ __forceinline__ void mma_f8f6f4(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                           uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f8f6f4 [%0], %1, %2, %3, p;\n\t}"
+        ::"r"(d_tmem), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+}
+
 // Arrives on the mbarrier once all prior tcgen05 operations of this thread complete.
 __device__ __forceinline__ void mma_commit(uint64_t *bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
@@ -147,6 +158,11 @@ __host__ __device__ constexpr uint32_t make_idesc_bf16(int M, int N) {
 }
 // The same with fp16 A and B (format code 0).
 __host__ __device__ constexpr uint32_t make_idesc_f16(int M, int N) {
+    return (1u << 4) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+// kind::f8f6f4 with E4M3 A and B (format code 0 in bits 7-9 and 10-12), FP32
+// accumulator.
+__host__ __device__ constexpr uint32_t make_idesc_e4m3(int M, int N) {
     return (1u << 4) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
 
