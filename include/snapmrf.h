@@ -135,6 +135,12 @@ void snapmrf_ra_free(snapmrf_ra *a);
 /* Use the reference's operation order (complex state, separate relaxation
  * and RF steps) even where the real-valued fast recursion applies. */
 #define SNAPMRF_DICT_REFERENCE_ORDER 0x4u
+/* Real-valued recursion (FISP / SR with every RF phase 0) with the
+ * reference's two relaxations per step, bit-identical to the complex
+ * recursion.  By default that recursion folds each step's relaxation over
+ * TR into the next step's RF instead (relaxation commutes with the
+ * dephasing shift), which changes results by rounding only (~1e-7). */
+#define SNAPMRF_DICT_SEPARATE_RELAX 0x8u
 
 typedef struct snapmrf_dict_opts {
     unsigned flags;  /* SNAPMRF_DICT_* */

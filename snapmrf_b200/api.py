@@ -28,6 +28,7 @@ NMAPS = 5    # src/mrf.cu:59
 DICT_ALL_B1_BLOCKS = 0x1
 DICT_NORMALIZE = 0x2
 DICT_REFERENCE_ORDER = 0x4
+DICT_SEPARATE_RELAX = 0x8
 # matching
 PREC_FP32 = 0
 PREC_BF16 = 1

@@ -151,11 +151,16 @@ size_t compute_natoms(float *h_t1, float *h_t2, size_t l_t1, size_t l_t2, size_t
 }
 
 // MRF_dict (src/functions.cu:1224-1315); returns after the device work.
+// The reference's two relaxations per step are kept (bit-identical FISP / SR
+// atoms, as its drivers' golden checks expect).
 void MRF_dict(float2 *d_atoms, float *d_params, float *h_mrf, size_t nreps, size_t NREPS, size_t NATOMS,
               size_t natoms, int nparams, int nstates, const char *echo_type) {
     printf("Constructing dictionary...\n");
+    snapmrf_dict_opts o;
+    memset(&o, 0, sizeof o);
+    o.flags = SNAPMRF_DICT_SEPARATE_RELAX;
     int rc = snapmrf_mrf_dict(reinterpret_cast<float *>(d_atoms), d_params, h_mrf, nreps, NREPS, NATOMS, natoms,
-                              nparams, nstates, echo_type, NULL, stream[0]);
+                              nparams, nstates, echo_type, &o, stream[0]);
     if (rc == SNAPMRF_ERR_ECHO_TYPE) errx(EX_USAGE, "Please put in correct echo types.");
     if (rc) die(rc, "MRF_dict");
     gpuAssert(cudaStreamSynchronize(stream[0]), __FILE__, __LINE__);

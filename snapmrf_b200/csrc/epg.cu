@@ -115,10 +115,10 @@ static cudaError_t dispatch_states(const EpgArgs &a, int S, dim3 grid, cudaStrea
     }
 }
 
-template <int ECHO, int S, bool TAIL = false>
+template <int ECHO, int S, bool TAIL, bool FOLD>
 static cudaError_t launch_epg_real(const EpgArgs &a, dim3 grid, cudaStream_t st) {
     size_t smem = epg_real_smem_bytes(a.L);
-    auto k = epg_real_kernel<ECHO, S, TAIL>;
+    auto k = epg_real_kernel<ECHO, S, TAIL, FOLD>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     k<<<grid, kEpgThreads, smem, st>>>(a);
@@ -128,46 +128,51 @@ static cudaError_t launch_epg_real(const EpgArgs &a, dim3 grid, cudaStream_t st)
 
 // P = pairs of states per lane (S = 2P).  FISP layouts that pad at most two
 // states take the TAIL form of the shift.
-template <int ECHO>
-static cudaError_t dispatch_real(const EpgArgs &a, int P, dim3 grid, cudaStream_t st) {
+template <int ECHO, bool FOLD>
+static cudaError_t dispatch_real_p(const EpgArgs &a, int P, dim3 grid, cudaStream_t st) {
     if constexpr (ECHO == ECHO_FISP) {
         if (a.L * 2 * P - a.nstates <= 2) switch (P) {
-        case 1: return launch_epg_real<ECHO, 1, true>(a, grid, st);
-        case 2: return launch_epg_real<ECHO, 2, true>(a, grid, st);
-        case 3: return launch_epg_real<ECHO, 3, true>(a, grid, st);
-        case 4: return launch_epg_real<ECHO, 4, true>(a, grid, st);
-        case 5: return launch_epg_real<ECHO, 5, true>(a, grid, st);
-        case 6: return launch_epg_real<ECHO, 6, true>(a, grid, st);
-        case 7: return launch_epg_real<ECHO, 7, true>(a, grid, st);
-        case 8: return launch_epg_real<ECHO, 8, true>(a, grid, st);
-        case 9: return launch_epg_real<ECHO, 9, true>(a, grid, st);
-        case 10: return launch_epg_real<ECHO, 10, true>(a, grid, st);
-        case 11: return launch_epg_real<ECHO, 11, true>(a, grid, st);
-        case 12: return launch_epg_real<ECHO, 12, true>(a, grid, st);
-        case 13: return launch_epg_real<ECHO, 13, true>(a, grid, st);
-        case 14: return launch_epg_real<ECHO, 14, true>(a, grid, st);
-        case 15: return launch_epg_real<ECHO, 15, true>(a, grid, st);
-        default: return launch_epg_real<ECHO, 16, true>(a, grid, st);
+            case 1: return launch_epg_real<ECHO, 1, true, FOLD>(a, grid, st);
+            case 2: return launch_epg_real<ECHO, 2, true, FOLD>(a, grid, st);
+            case 3: return launch_epg_real<ECHO, 3, true, FOLD>(a, grid, st);
+            case 4: return launch_epg_real<ECHO, 4, true, FOLD>(a, grid, st);
+            case 5: return launch_epg_real<ECHO, 5, true, FOLD>(a, grid, st);
+            case 6: return launch_epg_real<ECHO, 6, true, FOLD>(a, grid, st);
+            case 7: return launch_epg_real<ECHO, 7, true, FOLD>(a, grid, st);
+            case 8: return launch_epg_real<ECHO, 8, true, FOLD>(a, grid, st);
+            case 9: return launch_epg_real<ECHO, 9, true, FOLD>(a, grid, st);
+            case 10: return launch_epg_real<ECHO, 10, true, FOLD>(a, grid, st);
+            case 11: return launch_epg_real<ECHO, 11, true, FOLD>(a, grid, st);
+            case 12: return launch_epg_real<ECHO, 12, true, FOLD>(a, grid, st);
+            case 13: return launch_epg_real<ECHO, 13, true, FOLD>(a, grid, st);
+            case 14: return launch_epg_real<ECHO, 14, true, FOLD>(a, grid, st);
+            case 15: return launch_epg_real<ECHO, 15, true, FOLD>(a, grid, st);
+            default: return launch_epg_real<ECHO, 16, true, FOLD>(a, grid, st);
             }
     }
     switch (P) {
-    case 1: return launch_epg_real<ECHO, 1>(a, grid, st);
-    case 2: return launch_epg_real<ECHO, 2>(a, grid, st);
-    case 3: return launch_epg_real<ECHO, 3>(a, grid, st);
-    case 4: return launch_epg_real<ECHO, 4>(a, grid, st);
-    case 5: return launch_epg_real<ECHO, 5>(a, grid, st);
-    case 6: return launch_epg_real<ECHO, 6>(a, grid, st);
-    case 7: return launch_epg_real<ECHO, 7>(a, grid, st);
-    case 8: return launch_epg_real<ECHO, 8>(a, grid, st);
-    case 9: return launch_epg_real<ECHO, 9>(a, grid, st);
-    case 10: return launch_epg_real<ECHO, 10>(a, grid, st);
-    case 11: return launch_epg_real<ECHO, 11>(a, grid, st);
-    case 12: return launch_epg_real<ECHO, 12>(a, grid, st);
-    case 13: return launch_epg_real<ECHO, 13>(a, grid, st);
-    case 14: return launch_epg_real<ECHO, 14>(a, grid, st);
-    case 15: return launch_epg_real<ECHO, 15>(a, grid, st);
-    default: return launch_epg_real<ECHO, 16>(a, grid, st);
+    case 1: return launch_epg_real<ECHO, 1, false, FOLD>(a, grid, st);
+    case 2: return launch_epg_real<ECHO, 2, false, FOLD>(a, grid, st);
+    case 3: return launch_epg_real<ECHO, 3, false, FOLD>(a, grid, st);
+    case 4: return launch_epg_real<ECHO, 4, false, FOLD>(a, grid, st);
+    case 5: return launch_epg_real<ECHO, 5, false, FOLD>(a, grid, st);
+    case 6: return launch_epg_real<ECHO, 6, false, FOLD>(a, grid, st);
+    case 7: return launch_epg_real<ECHO, 7, false, FOLD>(a, grid, st);
+    case 8: return launch_epg_real<ECHO, 8, false, FOLD>(a, grid, st);
+    case 9: return launch_epg_real<ECHO, 9, false, FOLD>(a, grid, st);
+    case 10: return launch_epg_real<ECHO, 10, false, FOLD>(a, grid, st);
+    case 11: return launch_epg_real<ECHO, 11, false, FOLD>(a, grid, st);
+    case 12: return launch_epg_real<ECHO, 12, false, FOLD>(a, grid, st);
+    case 13: return launch_epg_real<ECHO, 13, false, FOLD>(a, grid, st);
+    case 14: return launch_epg_real<ECHO, 14, false, FOLD>(a, grid, st);
+    case 15: return launch_epg_real<ECHO, 15, false, FOLD>(a, grid, st);
+    default: return launch_epg_real<ECHO, 16, false, FOLD>(a, grid, st);
     }
+}
+
+template <int ECHO>
+static cudaError_t dispatch_real(const EpgArgs &a, int P, bool fold, dim3 grid, cudaStream_t st) {
+    return fold ? dispatch_real_p<ECHO, true>(a, P, grid, st) : dispatch_real_p<ECHO, false>(a, P, grid, st);
 }
 
 static cudaError_t launch_epg(int echo, const EpgArgs &a, int S, dim3 grid, cudaStream_t st) {
@@ -298,8 +303,9 @@ extern "C" int snapmrf_mrf_dict(float *d_atoms, const float *d_params, const flo
     dim3 grid((unsigned)((natoms + apc - 1) / apc), (unsigned)gen_blocks);
     if (grid.x > 0x7fffffffu) SNAPMRF_FAIL(SNAPMRF_ERR_UNSUPPORTED, "MRF_dict: grid too large");
     if (real_path) {
-        SNAPMRF_CUDA(echo == ECHO_FISP ? dispatch_real<ECHO_FISP>(a, S / 2, grid, st)
-                                       : dispatch_real<ECHO_SR>(a, S / 2, grid, st));
+        const bool fold = !(flags & SNAPMRF_DICT_SEPARATE_RELAX);
+        SNAPMRF_CUDA(echo == ECHO_FISP ? dispatch_real<ECHO_FISP>(a, S / 2, fold, grid, st)
+                                       : dispatch_real<ECHO_SR>(a, S / 2, fold, grid, st));
     } else {
         SNAPMRF_CUDA(launch_epg(echo, a, S, grid, st));
     }

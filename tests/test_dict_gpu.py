@@ -167,19 +167,28 @@ def test_normalize_entry_point(snap):
 @pytest.mark.parametrize("echo", ["epg_fisp", "epg_sr"])
 @pytest.mark.parametrize("nstates", [1, 2, 7, 20, 49, 50, 51, 101, 256])
 def test_real_path_bit_identical_to_complex_path(snap, echo, nstates):
-    """With every RF phase 0 the real-valued recursion (default) must give
-    exactly the complex recursion's atoms (SNAPMRF_DICT_REFERENCE_ORDER)."""
+    """With every RF phase 0 the real-valued recursion with the reference's
+    two relaxations per step (SNAPMRF_DICT_SEPARATE_RELAX) gives exactly the
+    complex recursion's atoms (SNAPMRF_DICT_REFERENCE_ORDER); the default,
+    with each relaxation folded into the next RF, differs by rounding only:
+    within the 1e-5 parity bar (measured <= 5.4e-6; FP32 itself sits
+    ~2e-5 from FP64 on long schedules)."""
     T = 300
     h = mrf_schedule(T, seed=6)
     params = _grid(np.geomspace(100, 4000, 10), np.geomspace(10, 1500, 8), b1s=(0.9, 1.1))
     natoms = params.shape[0] // 2
     flags = snap.DICT_ALL_B1_BLOCKS | snap.DICT_NORMALIZE
-    fast, n1 = run_dict(snap, echo, params, h, T, natoms=natoms, nstates=nstates, flags=flags,
-                        want_norms=True)
+    exact, n1 = run_dict(snap, echo, params, h, T, natoms=natoms, nstates=nstates,
+                         flags=flags | snap.DICT_SEPARATE_RELAX, want_norms=True)
     ref, n2 = run_dict(snap, echo, params, h, T, natoms=natoms, nstates=nstates,
                        flags=flags | snap.DICT_REFERENCE_ORDER, want_norms=True)
-    assert np.array_equal(fast, ref)
+    assert np.array_equal(exact, ref)
     assert np.array_equal(n1, n2)
+    fast, n3 = run_dict(snap, echo, params, h, T, natoms=natoms, nstates=nstates, flags=flags, want_norms=True)
+    rel = rel_err_per_atom(fast, ref)
+    print(f"{echo} w={nstates}: folded relaxation vs complex recursion, max rel {rel.max():.2e}")
+    assert rel.max() < 1e-5
+    np.testing.assert_allclose(n3, n2, rtol=1e-5)
 
 
 def test_real_path_large_state_count(snap, oracle):
