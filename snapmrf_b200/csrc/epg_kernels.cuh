@@ -444,7 +444,7 @@ __device__ __forceinline__ void rl2_shift(RealLane2<P> &s, int gl, int L, int w,
 inline size_t epg_real_smem_bytes(int L) {
     int apc = kEpgThreads / L;
     return (size_t)kChunk * 10 * sizeof(float2) + (size_t)apc * epg_f_stride(ECHO_FISP) * sizeof(float) +
-           (size_t)apc * kReadoutStride * sizeof(float2) + (size_t)apc * 3 * sizeof(float);
+           (size_t)apc * kReadoutStride * sizeof(float2) + (size_t)apc * 4 * sizeof(float);
 }
 
 // (An explicit minimum of 1 block per SM lets ptxas use more registers and
@@ -494,9 +494,10 @@ __global__ void SNAPMRF_EPG_REAL_BOUNDS epg_real_kernel(EpgArgs a) {
             t1 = p[0];
             t2 = p[1];
         }
-        sP[3 * i] = t1;
-        sP[3 * i + 1] = t2;
-        sP[3 * i + 2] = 0.f;
+        sP[4 * i] = t1;
+        sP[4 * i + 1] = t2;
+        sP[4 * i + 2] = 1.f / t1;
+        sP[4 * i + 3] = 1.f / t2;
     }
 
     const float *alpha = a.alpha + blk * nreps;
@@ -521,7 +522,7 @@ __global__ void SNAPMRF_EPG_REAL_BOUNDS epg_real_kernel(EpgArgs a) {
         s.zz[i] = make_float2(0.f, 0.f);
     }
     if (lane0) {
-        const float T1 = sP[3 * g];
+        const float T1 = sP[4 * g];
         float e1 = expf(-0.f / T1), sa, ca;
         __sincosf((float)(0.f * M_PI / 180.f), &sa, &ca);
         s.zz[0].x = e1 * ca + 1 - e1;
@@ -535,15 +536,18 @@ __global__ void SNAPMRF_EPG_REAL_BOUNDS epg_real_kernel(EpgArgs a) {
         for (int i = tid; i < nch; i += kEpgThreads) rf_real_coeffs2(alpha[t0 + i], phi[t0 + i], sC + 10 * i);
         for (int idx = tid; idx < apc * nch; idx += kEpgThreads) {
             int ga = idx / nch, i = idx - ga * nch;
-            float t1 = sP[3 * ga], t2 = sP[3 * ga + 1];
+            float t1 = sP[4 * ga], t2 = sP[4 * ga + 1];
             float4 f;
             if (FOLD) {
                 // (E1, E2) over the previous step's TR (1 before the first
-                // step), E2 over this step's TE, and Z0's recovery 1 - E1
+                // step), E2 over this step's TE, and Z0's recovery 1 - E1;
+                // rates as reciprocals (|t / T| < 1, so the argument's
+                // rounding moves exp by far less than an ulp)
                 const long long t = t0 + i;
                 const float trp = t > 0 ? TR[t - 1] : 0.f;
-                const float e1 = t > 0 ? expf(-trp / t1) : 1.f, e2 = t > 0 ? expf(-trp / t2) : 1.f;
-                f = make_float4(e1, e2, expf(-TE[t] / t2), 1.f - e1);
+                const float r1 = sP[4 * ga + 2], r2 = sP[4 * ga + 3];
+                const float e1 = t > 0 ? expf(-trp * r1) : 1.f, e2 = t > 0 ? expf(-trp * r2) : 1.f;
+                f = make_float4(e1, e2, expf(-TE[t] * r2), 1.f - e1);
             } else {
                 float tr = TR[t0 + i], te = TE[t0 + i];
                 float ta = te, tb = tr - te;

@@ -433,9 +433,11 @@ __global__ void pack_atoms_e4m3_kernel(unsigned char *B, float *ascale2, const f
     }
 }
 
-// Exact FP32 rescoring of the top-k (k <= 16) per voxel; one warp per slot.  The map
-// gets the candidate with the largest |s| (lowest atom index on ties,
-// nothing unless |s| > 0, like generate_maps' strict '>' from 0).
+// Exact FP32 rescoring of the top-k per voxel (TOPK of the TOPK_MAX slots);
+// one warp per slot.  The map gets the candidate with the largest |s| (lowest
+// atom index on ties, nothing unless |s| > 0, like generate_maps' strict '>'
+// from 0).  VEC: two samples per 16-byte load (strides even, rows aligned).
+template <int TOPK, bool VEC>
 __global__ void rescore_kernel(float *maps, long long *index_out, const float *top_s, const int *top_i,
                                const long long *perm, const long long *tile_start, int nbins, const int *vox_bin,
                                const float2 *atoms, long long atom_stride, const float2 *img, long long img_stride,
@@ -447,29 +449,49 @@ __global__ void rescore_kernel(float *maps, long long *index_out, const float *t
     const long long v = perm[slot];
     if (v < 0) return;
     const long long bin = vox_bin ? vox_bin[v] : 0;
-    int cand = lane < TOPK_MAX ? top_i[slot * TOPK_MAX + lane] : -1;
-    int ci[TOPK_MAX];
+    int cand = lane < TOPK ? top_i[slot * TOPK_MAX + lane] : -1;
+    int ci[TOPK];
+    const float2 *row[TOPK];
 #pragma unroll
-    for (int k = 0; k < TOPK_MAX; k++) ci[k] = __shfl_sync(0xffffffffu, cand, k);
-    float re[TOPK_MAX], im[TOPK_MAX];
+    for (int k = 0; k < TOPK; k++) {
+        ci[k] = __shfl_sync(0xffffffffu, cand, k);
+        row[k] = atoms + (bin * bin_natoms + (ci[k] >= 0 ? ci[k] : 0)) * atom_stride;
+    }
+    float re[TOPK], im[TOPK];
 #pragma unroll
-    for (int k = 0; k < TOPK_MAX; k++) {
+    for (int k = 0; k < TOPK; k++) {
         re[k] = 0.f;
         im[k] = 0.f;
     }
     const float2 *x = img + v * img_stride;
-    for (long long t = lane; t < nreps; t += 32) {
-        const float2 xv = x[t];
+    if (VEC) {
+        const long long n2 = nreps / 2;
+        for (long long t = lane; t < n2; t += 32) {
+            const float4 xv = reinterpret_cast<const float4 *>(x)[t];
 #pragma unroll
-        for (int k = 0; k < TOPK_MAX; k++) {
-            if (ci[k] < 0) continue;
-            const float2 d = atoms[(bin * bin_natoms + ci[k]) * atom_stride + t];
-            re[k] += d.x * xv.x + d.y * xv.y;
-            im[k] += d.x * xv.y - d.y * xv.x;
+            for (int k = 0; k < TOPK; k++) {
+                if (ci[k] < 0) continue;
+                const float4 d = reinterpret_cast<const float4 *>(row[k])[t];
+                re[k] += d.x * xv.x + d.y * xv.y;
+                im[k] += d.x * xv.y - d.y * xv.x;
+                re[k] += d.z * xv.z + d.w * xv.w;
+                im[k] += d.z * xv.w - d.w * xv.z;
+            }
+        }
+    } else {
+        for (long long t = lane; t < nreps; t += 32) {
+            const float2 xv = x[t];
+#pragma unroll
+            for (int k = 0; k < TOPK; k++) {
+                if (ci[k] < 0) continue;
+                const float2 d = row[k][t];
+                re[k] += d.x * xv.x + d.y * xv.y;
+                im[k] += d.x * xv.y - d.y * xv.x;
+            }
         }
     }
 #pragma unroll
-    for (int k = 0; k < TOPK_MAX; k++) {
+    for (int k = 0; k < TOPK; k++) {
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             re[k] += __shfl_xor_sync(0xffffffffu, re[k], o);
@@ -480,7 +502,7 @@ __global__ void rescore_kernel(float *maps, long long *index_out, const float *t
     int best = -1;
     float bs = 0.f, bre = 0.f, bim = 0.f;
 #pragma unroll
-    for (int k = 0; k < TOPK_MAX; k++) {
+    for (int k = 0; k < TOPK; k++) {
         if (ci[k] < 0) continue;
         const float sc = re[k] * re[k] + im[k] * im[k];
         if (sc > bs || (sc == bs && best >= 0 && ci[k] < best)) {
@@ -655,9 +677,14 @@ int match_bf16(const TcMatchRequest &q, cudaStream_t st) {
     const unsigned grid = (unsigned)std::max<long long>(1, std::min<long long>(num_sms, max_items));
     kern<<<grid, THREADS, SMEM_BYTES, st>>>(mA, mB, a);
     SNAPMRF_LAUNCH_CHECK();
-    rescore_kernel<<<nblk(cap * 32, 256), 256, 0, st>>>(q.maps, q.index_out, top_s, top_i, perm, tile_start, nbins,
-                                                        q.b1map ? vox_bin : nullptr, q.atoms, q.atom_stride, q.img,
-                                                        q.img_stride, q.nreps, q.params, q.nparams, bin_natoms, err);
+    // two samples per 16-byte load when every row starts 16-byte aligned
+    const bool vec = q.nreps % 2 == 0 && q.atom_stride % 2 == 0 && q.img_stride % 2 == 0 &&
+                     reinterpret_cast<uintptr_t>(q.atoms) % 16 == 0 && reinterpret_cast<uintptr_t>(q.img) % 16 == 0;
+    auto rk = q.topk > 8 ? (vec ? rescore_kernel<16, true> : rescore_kernel<16, false>)
+                         : (vec ? rescore_kernel<8, true> : rescore_kernel<8, false>);
+    rk<<<nblk(cap * 32, 256), 256, 0, st>>>(q.maps, q.index_out, top_s, top_i, perm, tile_start, nbins,
+                                            q.b1map ? vox_bin : nullptr, q.atoms, q.atom_stride, q.img,
+                                            q.img_stride, q.nreps, q.params, q.nparams, bin_natoms, err);
     SNAPMRF_LAUNCH_CHECK();
     publish_error_kernel<<<1, 1, 0, st>>>(err);
     SNAPMRF_LAUNCH_CHECK();
