@@ -188,6 +188,13 @@ int snapmrf_normalize(float *d_atoms, size_t nreps, size_t NATOMS, float *d_norm
  * any params table built by trans_params); without the flag the call
  * synchronises `stream` once to read the check's result. */
 #define SNAPMRF_MATCH_ASSUME_UNIFORM_B1 0x1u
+/* The atoms are purely imaginary (every Re d_t is 0), as the FISP / SR
+ * dictionaries of schedules whose RF phases are all 0 are.  The BF16 / FP16
+ * forms then score |s|^2 = (sum Im d x_r)^2 + (sum Im d x_i)^2 with one
+ * operand row per atom: half the tensor-core work.  An atom with a non-zero
+ * real part makes the call's maps NaN and sets the device error word
+ * (snapmrf_device_error() == 7).  Other precisions ignore the flag. */
+#define SNAPMRF_MATCH_IMAG_ATOMS 0x2u
 
 typedef struct snapmrf_match_opts {
     int precision;          /* SNAPMRF_PREC_* */

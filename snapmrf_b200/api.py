@@ -35,6 +35,7 @@ PREC_BF16 = 1
 PREC_FP16 = 2
 PREC_FP8 = 3
 MATCH_ASSUME_UNIFORM_B1 = 0x1
+MATCH_IMAG_ATOMS = 0x2
 
 ECHO_TYPES = ("epg_ssfp", "roa_ssfp", "epg_sr", "epg_se", "epg_tse1", "epg_tse2", "epg_fisp")
 

@@ -102,7 +102,13 @@ __device__ __forceinline__ void topk_insert(float *ts, int *ti, float s, int i) 
 
 // FP8: E4M3 operands on kind::f8f6f4, one 128-byte row holding 128 elements
 // of K, and scores divided by the atom's squared scale before the top-k.
-template <int TOPK, bool FP8>
+// IMAG: purely imaginary atoms d = i v.  Then s = -i sum v x, |s|^2 =
+// (sum v x_r)^2 + (sum v x_i)^2: a voxel gives two A rows (x_r, x_i) in
+// neighbouring TMEM lanes, an atom one B row v, K = T: half the MMA work.
+// A tile is 64 voxels x 256 atoms; the two lanes of a voxel swap halves of
+// each 32-column load and keep a top-k each over half the atoms, merged at
+// the end of the item.
+template <int TOPK, bool FP8, bool IMAG>
 __global__ void __launch_bounds__(THREADS, 1)
 match_bf16_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, Args p) {
     constexpr int BKE = FP8 ? BK8 : BK;   // K elements per stage
@@ -112,8 +118,10 @@ match_bf16_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
     unsigned char *smem = reinterpret_cast<unsigned char *>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
-    const long long total = p.tile_start[p.nbins];
-    const int natiles = (int)((p.bin_natoms + BA - 1) / BA);
+    constexpr int IPT = IMAG ? 2 : 1;       // work items per 128-slot tile
+    constexpr int APT = IMAG ? BN : BA;     // atoms per B tile
+    const long long total = p.tile_start[p.nbins] * IPT;
+    const int natiles = (int)((p.bin_natoms + APT - 1) / APT);
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < STAGES; s++) {
@@ -147,10 +155,11 @@ match_bf16_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
             for (int s = 0; s < STAGES; s++) issued[s] = -1;
             bool ok = true;
             for (long long item = blockIdx.x; item < total && ok; item += gridDim.x) {
-                const int bin = find_bin(p.tile_start, p.nbins, item);
+                const int bin = find_bin(p.tile_start, p.nbins, item / IPT);
                 const int vrow = (int)(item * BM);
                 for (int at = 0; at < natiles && ok; at++) {
-                    const int brow = (int)(2 * ((long long)bin * p.bin_natoms + (long long)at * BA));
+                    const int brow = IMAG ? (int)((long long)bin * p.bin_natoms + (long long)at * APT)
+                                          : (int)(2 * ((long long)bin * p.bin_natoms + (long long)at * BA));
                     for (int kc = 0; kc < p.nk; kc++) {
                         if (!sm100::mbar_wait(&empty[stage], phase ^ 1, p.err, 1)) {
                             ok = false;
@@ -234,7 +243,7 @@ match_bf16_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
         bool ok = true;
         for (long long item = blockIdx.x; item < total && ok; item += gridDim.x) {
             const float *asc = nullptr;
-            if (FP8) asc = p.ascale2 + (long long)find_bin(p.tile_start, p.nbins, item) * p.bin_natoms;
+            if (FP8) asc = p.ascale2 + (long long)find_bin(p.tile_start, p.nbins, item / IPT) * p.bin_natoms;
             float ts[TOPK];
             int ti[TOPK];
 #pragma unroll
@@ -252,12 +261,26 @@ match_bf16_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
                 }
                 sm100::tc_fence_after();
                 const uint32_t taddr = tmem + (uint32_t)(acc * BN) + ((uint32_t)(lg * 32) << 16);
-                const int abase = at * BA;
-                const bool full_tile = (long long)abase + BA <= p.bin_natoms;
+                const int abase = at * APT;
+                const bool full_tile = (long long)abase + APT <= p.bin_natoms;
 #pragma unroll 1
                 for (int c = 0; c < BN / 32; c++) {
                     float v[32];
                     sm100::tmem_ld32(taddr + c * 32, v);
+                    if (IMAG) {
+                        // lane pair (2m, 2m+1) = voxel m's (x_r, x_i) rows: the
+                        // even lane scores columns 0-15, the odd lane 16-31
+                        const int part = lane & 1;
+#pragma unroll
+                        for (int j = 0; j < 16; j++) {
+                            const float mine = part ? v[16 + j] : v[j];
+                            const float other = __shfl_xor_sync(0xffffffffu, part ? v[j] : v[16 + j], 1);
+                            const int atom = abase + c * 32 + (part ? 16 + j : j);
+                            const float sc = fmaf(mine, mine, other * other);
+                            if (sc > ts[TOPK - 1] && (full_tile || atom < p.bin_natoms)) topk_insert<TOPK>(ts, ti, sc, atom);
+                        }
+                        continue;
+                    }
 #pragma unroll
                     for (int j = 0; j < 16; j++) {
                         const int atom = abase + c * 16 + j;
@@ -272,12 +295,30 @@ match_bf16_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
                 acc ^= 1;
                 if (acc == 0) aphase ^= 1;
             }
-            const long long slot = item * BM + row;
+            if (IMAG) {
+                // the odd lane's list into the even lane's: the top-k of the union
+                float os[TOPK];
+                int oi[TOPK];
 #pragma unroll
-            for (int k = 0; k < TOPK_MAX; k++) {
-                p.top_s[slot * TOPK_MAX + k] = k < TOPK ? ts[k] : 0.f;
-                p.top_i[slot * TOPK_MAX + k] = k < TOPK ? ti[k] : -1;
+                for (int k = 0; k < TOPK; k++) {
+                    os[k] = __shfl_xor_sync(0xffffffffu, ts[k], 1);
+                    oi[k] = __shfl_xor_sync(0xffffffffu, ti[k], 1);
+                }
+                if (!(lane & 1)) {
+#pragma unroll
+                    for (int k = 0; k < TOPK; k++)
+                        if (oi[k] >= 0 && os[k] > ts[TOPK - 1]) topk_insert<TOPK>(ts, ti, os[k], oi[k]);
+                }
             }
+            if (!IMAG || !(lane & 1)) {
+                const long long slot = IMAG ? item * (BM / 2) + row / 2 : item * BM + row;
+#pragma unroll
+                for (int k = 0; k < TOPK_MAX; k++) {
+                    p.top_s[slot * TOPK_MAX + k] = k < TOPK ? ts[k] : 0.f;
+                    p.top_i[slot * TOPK_MAX + k] = k < TOPK ? ti[k] : -1;
+                }
+            }
+            __syncwarp();
         }
     }
     __syncthreads();
@@ -370,6 +411,65 @@ __global__ void pack_atoms_kernel(void *B, const float2 *atoms, long long atom_s
         *reinterpret_cast<uint4 *>(r0 + t) = make_uint4(o0[0], o0[1], o0[2], o0[3]);
         *reinterpret_cast<uint4 *>(r1 + t) = make_uint4(o1[0], o1[1], o1[2], o1[3]);
     }
+}
+
+// A rows for purely imaginary atoms: voxel perm[slot] at unit norm as two
+// rows, 2 slot = (Re x_t) and 2 slot + 1 = (Im x_t), zero padded to Kp.
+// One warp per slot.
+template <bool HALF>
+__global__ void pack_voxels_split_kernel(void *A, const float2 *img, long long img_stride, const long long *perm,
+                                         long long nslots, long long nreps, long long Kp) {
+    using P = Pair<HALF>;
+    const long long slot = (blockIdx.x * (long long)blockDim.x + threadIdx.x) / 32;
+    const int lane = threadIdx.x % 32;
+    if (slot >= nslots) return;
+    const long long v = perm[slot];
+    const float2 *x = img + (v >= 0 ? v : 0) * img_stride;
+    float n = 0.f;
+    if (v >= 0)
+        for (long long t = lane; t < nreps; t += 32) n += x[t].x * x[t].x + x[t].y * x[t].y;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) n += __shfl_xor_sync(0xffffffffu, n, o);
+    const float inv = n > 0.f ? rsqrtf(n) : 0.f;
+    typename P::T *rr = reinterpret_cast<typename P::T *>(A) + (2 * slot) * (Kp / 2);
+    typename P::T *ri = rr + Kp / 2;
+    for (long long t = lane; t < Kp / 2; t += 32) {
+        float2 a = make_float2(0.f, 0.f), b = make_float2(0.f, 0.f);
+        if (v >= 0 && 2 * t < nreps) a = x[2 * t];
+        if (v >= 0 && 2 * t + 1 < nreps) b = x[2 * t + 1];
+        rr[t] = P::make(a.x * inv, b.x * inv);
+        ri[t] = P::make(a.y * inv, b.y * inv);
+    }
+}
+
+// B rows for purely imaginary atoms: row a = (Im d_t), zero padded to Kp;
+// an atom with a non-zero real part sets the error word (code 7), which
+// turns the call's maps to NaN.  One warp per atom, eight samples (16
+// bytes) per lane and step.
+template <bool HALF>
+__global__ void pack_atoms_imag_kernel(void *B, const float2 *atoms, long long atom_stride, long long natoms,
+                                       long long nreps, long long Kp, int *err) {
+    using P = Pair<HALF>;
+    const long long a = (blockIdx.x * (long long)blockDim.x + threadIdx.x) / 32;
+    const int lane = threadIdx.x % 32;
+    if (a >= natoms) return;
+    typename P::T *row = reinterpret_cast<typename P::T *>(B) + a * (Kp / 2);
+    const float2 *src = atoms + a * atom_stride;
+    bool real_part = false;
+    for (long long t = 8 * lane; t < Kp; t += 256) {
+        uint32_t o[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            float2 d0 = make_float2(0.f, 0.f), d1 = make_float2(0.f, 0.f);
+            if (t + 2 * u < nreps) d0 = src[t + 2 * u];
+            if (t + 2 * u + 1 < nreps) d1 = src[t + 2 * u + 1];
+            real_part |= d0.x != 0.f || d1.x != 0.f;
+            typename P::T q = P::make(d0.y, d1.y);
+            o[u] = *reinterpret_cast<const uint32_t *>(&q);
+        }
+        *reinterpret_cast<uint4 *>(row + t / 2) = make_uint4(o[0], o[1], o[2], o[3]);
+    }
+    if (__any_sync(0xffffffffu, real_part) && lane == 0) atomicCAS(err, 0, 7);
 }
 
 // E4M3 A rows: voxel perm[slot] scaled so that its largest component is
@@ -574,12 +674,14 @@ int match_bf16(const TcMatchRequest &q, cudaStream_t st) {
     const long long bin_natoms = q.b1map ? q.natoms : q.NATOMS;
     const int fmt = q.fmt;
     const bool fp8 = fmt == 2;
+    const bool imag = q.imag && !fp8;     // one real row per atom, K = T
     const int eb = fp8 ? 1 : 2;           // bytes per element
     const int bke = fp8 ? BK8 : BK;       // K elements per 128-byte row
-    const long long Kp = ((2 * q.nreps + bke - 1) / bke) * bke;
+    const long long Kp = (((imag ? 1 : 2) * q.nreps + bke - 1) / bke) * bke;
     const long long cap = ((nvox + BM - 1) / BM + nbins) * BM;  // padded slots, upper bound
-    const long long brows = 2 * q.NATOMS;
-    if (cap > 0x7fffffffll || brows > 0x7fffffffll || Kp > 0x7fffffffll)
+    const long long brows = (imag ? 1 : 2) * q.NATOMS;
+    const long long arows = (imag ? 2 : 1) * cap;
+    if (arows > 0x7fffffffll || brows > 0x7fffffffll || Kp > 0x7fffffffll)
         SNAPMRF_FAIL(SNAPMRF_ERR_UNSUPPORTED, "MRF_match: problem too large for the tensor-core path");
 
     size_t bytes = 0;
@@ -588,7 +690,7 @@ int match_bf16(const TcMatchRequest &q, cudaStream_t st) {
         bytes += (n + 255) & ~size_t(255);
         return off;
     };
-    const size_t oA = take((size_t)cap * Kp * eb), oB = take((size_t)brows * Kp * eb);
+    const size_t oA = take((size_t)arows * Kp * eb), oB = take((size_t)brows * Kp * eb);
     const size_t oSc = take(fp8 ? (size_t)q.NATOMS * 4 : 0);
     const size_t oTs = take((size_t)cap * TOPK_MAX * 4), oTi = take((size_t)cap * TOPK_MAX * 4);
     const size_t oPerm = take((size_t)cap * 8), oTile = take((size_t)(nbins + 1) * 8);
@@ -635,6 +737,23 @@ int match_bf16(const TcMatchRequest &q, cudaStream_t st) {
                                                                           q.atoms, q.atom_stride, q.NATOMS,
                                                                           q.nreps, Kp);
         SNAPMRF_LAUNCH_CHECK();
+    } else if (imag) {
+        if (half)
+            pack_voxels_split_kernel<true><<<nblk(cap * 32, 256), 256, 0, st>>>(A, q.img, q.img_stride, perm, cap,
+                                                                                q.nreps, Kp);
+        else
+            pack_voxels_split_kernel<false><<<nblk(cap * 32, 256), 256, 0, st>>>(A, q.img, q.img_stride, perm, cap,
+                                                                                 q.nreps, Kp);
+        SNAPMRF_LAUNCH_CHECK();
+        // Kp is a multiple of 64, so every 8-element group of a row is whole
+        // and 16-byte aligned
+        if (half)
+            pack_atoms_imag_kernel<true><<<nblk(q.NATOMS * 32, 256), 256, 0, st>>>(B, q.atoms, q.atom_stride,
+                                                                                   q.NATOMS, q.nreps, Kp, err);
+        else
+            pack_atoms_imag_kernel<false><<<nblk(q.NATOMS * 32, 256), 256, 0, st>>>(B, q.atoms, q.atom_stride,
+                                                                                    q.NATOMS, q.nreps, Kp, err);
+        SNAPMRF_LAUNCH_CHECK();
     } else {
         if (half)
             pack_voxels_kernel<true><<<nblk(cap * 32, 256), 256, 0, st>>>(A, q.img, q.img_stride, perm, cap, q.nreps, Kp);
@@ -652,7 +771,7 @@ int match_bf16(const TcMatchRequest &q, cudaStream_t st) {
         SNAPMRF_LAUNCH_CHECK();
     }
     CUtensorMap mA, mB;
-    int rc = make_map(&mA, A, cap, Kp, BM, fmt);
+    int rc = make_map(&mA, A, arows, Kp, BM, fmt);
     if (rc) return rc;
     rc = make_map(&mB, B, brows, Kp, BN, fmt);
     if (rc) return rc;
@@ -660,8 +779,9 @@ int match_bf16(const TcMatchRequest &q, cudaStream_t st) {
     int num_sms = 0, dev = 0;
     SNAPMRF_CUDA(cudaGetDevice(&dev));
     SNAPMRF_CUDA(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev));
-    auto kern = fp8 ? (q.topk > 8 ? match_bf16_kernel<16, true> : match_bf16_kernel<8, true>)
-                    : (q.topk > 8 ? match_bf16_kernel<16, false> : match_bf16_kernel<8, false>);
+    auto kern = fp8    ? (q.topk > 8 ? match_bf16_kernel<16, true, false> : match_bf16_kernel<8, true, false>)
+                : imag ? (q.topk > 8 ? match_bf16_kernel<16, false, true> : match_bf16_kernel<8, false, true>)
+                       : (q.topk > 8 ? match_bf16_kernel<16, false, false> : match_bf16_kernel<8, false, false>);
     SNAPMRF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
     Args a;
     a.tile_start = tile_start;
@@ -673,7 +793,7 @@ int match_bf16(const TcMatchRequest &q, cudaStream_t st) {
     a.top_s = top_s;
     a.top_i = top_i;
     a.err = err;
-    const long long max_items = cap / BM;
+    const long long max_items = (imag ? 2 : 1) * cap / BM;
     const unsigned grid = (unsigned)std::max<long long>(1, std::min<long long>(num_sms, max_items));
     kern<<<grid, THREADS, SMEM_BYTES, st>>>(mA, mB, a);
     SNAPMRF_LAUNCH_CHECK();

@@ -76,19 +76,28 @@ def test_tc_reference_selftest(snap, golden, prec):
     assert snap.device_error(reset=True) == 0
 
 
+IMAG = pytest.mark.parametrize("imag", [False, True], ids=["complex", "imag"])
+
+
+def _flags(snap, imag):
+    return snap.MATCH_IMAG_ATOMS if imag else 0
+
+
 @PRECS
+@IMAG
 @pytest.mark.parametrize("T", [200, 1000])
-def test_tc_global_vs_fp32(snap, T, prec):
+def test_tc_global_vs_fp32(snap, T, prec, imag):
     atoms, params, natoms = _dictionary(snap, T, (0.8, 1.0, 1.2))
     img = _voxels(atoms, 900, 1)
     m32, i32 = run_match(snap, img, atoms, params, natoms=natoms)
-    m16, i16 = run_match(snap, img, atoms, params, natoms=natoms, precision=prec)
+    m16, i16 = run_match(snap, img, atoms, params, natoms=natoms, precision=prec, flags=_flags(snap, imag))
     compare(img, atoms, params, m32, i32, m16, i16, *LIMITS[prec])
     assert snap.device_error(reset=True) == 0
 
 
 @PRECS
-def test_tc_b1map_vs_fp32(snap, prec):
+@IMAG
+def test_tc_b1map_vs_fp32(snap, prec, imag):
     b1s = np.float32([0.6, 0.75, 0.9, 1.05, 1.2, 1.35])
     atoms, params, natoms = _dictionary(snap, 300, b1s, nt1=16, nt2=14)
     nvox = 1500
@@ -96,20 +105,22 @@ def test_tc_b1map_vs_fp32(snap, prec):
     b1map = np.random.default_rng(3).uniform(0.5, 1.5, nvox).astype(np.float32)
     b1map[:4] = [0.0, 0.675, 11.0, np.nan]
     m32, i32 = run_match(snap, img, atoms, params, natoms=natoms, b1map=b1map)
-    m16, i16 = run_match(snap, img, atoms, params, natoms=natoms, b1map=b1map, precision=prec)
+    m16, i16 = run_match(snap, img, atoms, params, natoms=natoms, b1map=b1map, precision=prec,
+                         flags=_flags(snap, imag))
     assert np.all(i16 // natoms == i32 // natoms)
     compare(img, atoms, params, m32, i32, m16, i16, *LIMITS[prec])
     assert snap.device_error(reset=True) == 0
 
 
 @PRECS
-def test_tc_ragged_tiles(snap, prec):
-    """Atom and voxel counts off the 128-wide tiles, K not a multiple of 64."""
+@IMAG
+def test_tc_ragged_tiles(snap, prec, imag):
+    """Atom and voxel counts off the 128- and 256-wide tiles, K not a multiple of 64."""
     atoms, params, natoms = _dictionary(snap, 77, (1.0,))
     atoms, params = atoms[:131], params[:131]
     img = _voxels(atoms, 67, 8)
     m32, i32 = run_match(snap, img, atoms, params)
-    m16, i16 = run_match(snap, img, atoms, params, precision=prec)
+    m16, i16 = run_match(snap, img, atoms, params, precision=prec, flags=_flags(snap, imag))
     compare(img, atoms, params, m32, i32, m16, i16, min_agree=min(0.97, LIMITS[prec][0]),
             max_loss=LIMITS[prec][1])
     assert snap.device_error(reset=True) == 0
@@ -129,3 +140,20 @@ def test_tc_zero_nan_and_duplicate_atoms(snap, prec):
     assert got[1] == 0 and maps[1, 4] == 0
     assert got[2] == 0 and maps[2, 4] == 0
     assert snap.device_error(reset=True) == 0
+
+
+@pytest.mark.parametrize("prec", [BF16, FP16], ids=["bf16", "fp16"])
+def test_tc_imag_flag_on_complex_atoms_fails_loudly(snap, prec):
+    """SNAPMRF_MATCH_IMAG_ATOMS asserts Re d = 0; atoms with a real part turn
+    the maps to NaN and set the device error word (7) instead of matching
+    against half of each atom."""
+    atoms, params, natoms = _dictionary(snap, 64, (1.0,))
+    atoms = atoms.copy()
+    atoms[5] = atoms[5] + 0.01
+    img = _voxels(atoms, 40, 9)
+    maps, _ = run_match(snap, img, atoms, params, precision=prec, flags=snap.MATCH_IMAG_ATOMS)
+    assert np.all(np.isnan(maps))
+    assert snap.device_error(reset=True) == 7
+    assert snap.device_error() == 0
+    maps, _ = run_match(snap, img, atoms, params, precision=prec)
+    assert np.all(np.isfinite(maps))
