@@ -47,6 +47,9 @@ namespace snapmrf {
 // uploads, so that cudaMemcpyAsync stays asynchronous.  stage_acquire waits
 // for the previous upload from the buffer (stage_release records it).
 void *stage_acquire(size_t bytes);
+// Copies `bytes` from the staging buffer to device memory on `st` with a
+// kernel that reads the page-locked host memory directly (no copy engine).
+cudaError_t stage_upload(void *d_dst, const void *h_stage, size_t bytes, cudaStream_t st);
 cudaError_t stage_release(cudaStream_t st);
 
 // The library's stream-ordered memory pool on the current device.  Its

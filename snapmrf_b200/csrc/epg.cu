@@ -247,7 +247,7 @@ extern "C" int snapmrf_mrf_dict(float *d_atoms, const float *d_params, const flo
     float *h_stage = static_cast<float *>(stage_acquire(4 * nreps * sizeof(float)));
     if (!h_stage) SNAPMRF_FAIL(SNAPMRF_ERR_ALLOC, "MRF_dict: cannot allocate a pinned staging buffer");
     memcpy(h_stage, sched.data(), 4 * nreps * sizeof(float));
-    SNAPMRF_CUDA(cudaMemcpyAsync(d_sched, h_stage, 4 * nreps * sizeof(float), cudaMemcpyHostToDevice, st));
+    SNAPMRF_CUDA(stage_upload(d_sched, h_stage, 4 * nreps * sizeof(float), st));
     SNAPMRF_CUDA(stage_release(st));
     int mode = (echo == ECHO_SSFP) ? 0 : (all_blocks ? 1 : 2);
     prepare_alpha_kernel<<<(unsigned)((nreps + 255) / 256), 256, 0, st>>>(

@@ -692,7 +692,7 @@ static int upload_schedule(DeviceScratch &buf, Schedule *sc, const float *h_mrf,
     memcpy(h, h_mrf, nreps * sizeof(float));
     memcpy(h + nreps, h_mrf + 2 * NREPS, nreps * sizeof(float));
     memcpy(h + 2 * nreps, h_mrf + 3 * NREPS, nreps * sizeof(float));
-    SNAPMRF_CUDA(cudaMemcpyAsync(buf.ptr, h, 3 * nreps * sizeof(float), cudaMemcpyHostToDevice, st));
+    SNAPMRF_CUDA(stage_upload(buf.ptr, h, 3 * nreps * sizeof(float), st));
     SNAPMRF_CUDA(stage_release(st));
     sc->alpha = buf.as<float>();
     sc->TR = sc->alpha + nreps;

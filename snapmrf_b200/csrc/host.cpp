@@ -4,6 +4,7 @@
 // values (and therefore atom order and map values) are bit-identical; the
 // differences are that failures return a status instead of asserting or
 // crashing.
+#include <algorithm>
 #include <atomic>
 #include <cmath>
 #include <cstdio>
@@ -19,10 +20,20 @@
 
 namespace snapmrf {
 
-struct Stage {
+// Page-locked staging slots of this thread per device, used in turn.  A slot
+// is reused only after the copy that read it has run (its event), so the
+// host blocks only when it is kStageSlots calls ahead of the device.
+constexpr int kStageSlots = 4;
+
+struct StageSlot {
     void *p = nullptr;
     size_t cap = 0;
     cudaEvent_t ev = nullptr;
+};
+
+struct Stage {
+    StageSlot slot[kStageSlots];
+    int cur = 0;
 };
 
 static thread_local std::map<int, Stage> g_stage;
@@ -30,19 +41,57 @@ static thread_local std::map<int, Stage> g_stage;
 void *stage_acquire(size_t bytes) {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
-    Stage &s = g_stage[dev];
+    Stage &st = g_stage[dev];
+    st.cur = (st.cur + 1) % kStageSlots;
+    StageSlot &s = st.slot[st.cur];
     if (s.ev) cudaEventSynchronize(s.ev);
     if (s.cap < bytes) {
         if (s.p) cudaFreeHost(s.p);
         s.cap = 0;
         size_t want = bytes < 65536 ? 65536 : bytes;
-        if (cudaMallocHost(&s.p, want) != cudaSuccess) {
+        if (cudaHostAlloc(&s.p, want, cudaHostAllocMapped | cudaHostAllocPortable) != cudaSuccess) {
             s.p = nullptr;
             return nullptr;
         }
         s.cap = want;
     }
     return s.p;
+}
+
+// Reads the staged words straight from page-locked host memory (mapped into
+// the device's address space), so the upload does not queue on the copy
+// engine behind large transfers of other streams.
+__global__ void stage_copy_kernel(uint32_t *dst, const uint32_t *src, long long n) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        dst[i] = src[i];
+}
+
+cudaError_t stage_upload(void *d_dst, const void *h_stage, size_t bytes, cudaStream_t st) {
+    // the slot's address in the device's address space; without one (memory
+    // not mapped), an ordinary copy
+    void *src = nullptr;
+    if (bytes % 4 != 0 || cudaHostGetDevicePointer(&src, const_cast<void *>(h_stage), 0) != cudaSuccess || !src) {
+        cudaGetLastError();
+        return cudaMemcpyAsync(d_dst, h_stage, bytes, cudaMemcpyHostToDevice, st);
+    }
+    const long long n = (long long)(bytes / 4);
+    const unsigned blocks = (unsigned)std::min<long long>(64, (n + 255) / 256);
+    stage_copy_kernel<<<blocks > 0 ? blocks : 1, 256, 0, st>>>(static_cast<uint32_t *>(d_dst),
+                                                               static_cast<const uint32_t *>(src), n);
+    note_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t stage_release(cudaStream_t st) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    StageSlot &s = g_stage[dev].slot[g_stage[dev].cur];
+    if (!s.ev) {
+        e = cudaEventCreateWithFlags(&s.ev, cudaEventDisableTiming);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaEventRecord(s.ev, st);
 }
 
 static std::mutex g_pool_mu;
@@ -72,18 +121,6 @@ cudaError_t device_pool(cudaMemPool_t *pool) {
     g_pools[dev] = p;
     *pool = p;
     return cudaSuccess;
-}
-
-cudaError_t stage_release(cudaStream_t st) {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return e;
-    Stage &s = g_stage[dev];
-    if (!s.ev) {
-        e = cudaEventCreateWithFlags(&s.ev, cudaEventDisableTiming);
-        if (e != cudaSuccess) return e;
-    }
-    return cudaEventRecord(s.ev, st);
 }
 
 static thread_local std::string g_last_error;
