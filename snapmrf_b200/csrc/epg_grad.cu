@@ -361,6 +361,7 @@ struct GnArgs {
     int *list_out;
     int *count_out;
     float tol;
+    int finish;               // a voxel that stops in this pass writes PD, M0, B1
 };
 
 // A voxel whose map holds no usable start (not finite, T2 <= 0, T1 <= T2)
@@ -580,12 +581,16 @@ __global__ void __launch_bounds__(kThreads) gn_kernel(GnArgs a, int chunk) {
     }
     if (!lane0 || !active || !(Ss > 0.f)) return;
     float *mp = a.maps + v * a.nmaps;
-    if (!TANGENTS) {
-        // PD of a unit-norm atom (what matching reports) and |rho|
-        const float ip = sqrtf(Pr * Pr + Pi * Pi);
+    // PD of a unit-norm atom (what matching reports), |rho| and the B1 used,
+    // from <s, x> = (pr, pi) and <s, s> = ss
+    auto finish = [&](float pr, float pi, float ss) {
+        const float ip = sqrtf(pr * pr + pi * pi);
         if (a.b1map && a.nmaps >= 4) mp[3] = sV[4 * g + 2];
-        if (a.nmaps >= 5) mp[4] = ip / sqrtf(Ss);
-        if (a.m0) a.m0[v] = ip / Ss;
+        if (a.nmaps >= 5) mp[4] = ss > 0.f ? ip / sqrtf(ss) : 0.f;
+        if (a.m0) a.m0[v] = ss > 0.f ? ip / ss : 0.f;
+    };
+    if (!TANGENTS) {
+        finish(Pr, Pi, Ss);
         return;
     }
     const float T1 = sV[4 * g], T2 = sV[4 * g + 1];
@@ -598,9 +603,12 @@ __global__ void __launch_bounds__(kThreads) gn_kernel(GnArgs a, int chunk) {
     const float c2r = Q2r - G2 * Pr / Ss, c2i = Q2i - G2 * Pi / Ss;
     const float b1 = rr * c1r + ri * c1i, b2 = rr * c2r + ri * c2i;
     const float det = A11 * A22 - A12 * A12;
-    if (!(fabsf(det) > 0.f) || !isfinite(det)) return;
-    float d1 = (A22 * b1 - A12 * b2) / det, d2 = (A11 * b2 - A12 * b1) / det;
-    if (!isfinite(d1) || !isfinite(d2)) return;
+    float d1 = 0.f, d2 = 0.f;
+    if (fabsf(det) > 0.f && isfinite(det)) {
+        d1 = (A22 * b1 - A12 * b2) / det;
+        d2 = (A11 * b2 - A12 * b1) / det;
+    }
+    if (!isfinite(d1) || !isfinite(d2)) d1 = d2 = 0.f;
     // trust region: at most max_rel_step of each parameter per iteration
     const float lim1 = a.max_rel_step * T1, lim2 = a.max_rel_step * T2;
     d1 = fminf(fmaxf(d1, -lim1), lim1);
@@ -608,10 +616,23 @@ __global__ void __launch_bounds__(kThreads) gn_kernel(GnArgs a, int chunk) {
     float n1 = T1 + d1, n2 = T2 + d2;
     n2 = fmaxf(n2, 1e-3f);
     n1 = fmaxf(n1, n2 * (1.f + 1e-4f));  // keep T1 > T2 > 0
+    d1 = n1 - T1;
+    d2 = n2 - T2;
     mp[0] = n1;
     mp[1] = n2;
-    if (a.list_out && !(fabsf(n1 - T1) <= a.tol * T1 && fabsf(n2 - T2) <= a.tol * T2))
+    const bool moving = !(fabsf(d1) <= a.tol * T1 && fabsf(d2) <= a.tol * T2);
+    if (a.list_out && moving) {
         a.list_out[atomicAdd(a.count_out, 1)] = (int)v;
+        return;
+    }
+    if (a.finish) {
+        // the voxel stops here: PD and M0 at the updated parameters from the
+        // linear model s(T + d) = s + J d, exact to first order in d:
+        // <s + J d, x> = P + Q d, ||s + J d||^2 = Ss + 2 G d + d^T H d
+        const float pr = Pr + Q1r * d1 + Q2r * d2, pi = Pi + Q1i * d1 + Q2i * d2;
+        const float ss = Ss + 2.f * (G1 * d1 + G2 * d2) + H11 * d1 * d1 + 2.f * H12 * d1 * d2 + H22 * d2 * d2;
+        finish(pr, pi, ss);
+    }
 }
 
 constexpr int kGnMaxPairs = 7;  // 8 pairs with both tangents exceed 255 registers
@@ -826,20 +847,29 @@ extern "C" int snapmrf_refine_gn(float *d_maps, int nmaps, const float *img, siz
     const int chunk = (int)std::min<size_t>(kGnChunk, (48 * 1024 - fixed) / ((size_t)apc * sizeof(GnStep)));
     const size_t smem = (size_t)apc * chunk * sizeof(GnStep) + fixed;
     dim3 grid((unsigned)((nvoxels + apc - 1) / apc));
+    // PD, M0 and the B1 column: written by each voxel in the pass where it
+    // stops (early exit, or the last iteration); with no iteration at all, by
+    // one value-only pass
+    const bool outputs = nmaps >= 5 || d_m0 || (d_b1map && nmaps >= 4);
     for (int it = 0; it < iterations; it++) {
+        const bool last = it + 1 == iterations;
+        a.list_in = a.count_in = nullptr;
+        a.list_out = a.count_out = nullptr;
         if (early) {
             a.list_in = it == 0 ? nullptr : lst[(it - 1) & 1];
             a.count_in = it == 0 ? nullptr : cnt[(it - 1) & 1];
-            a.list_out = it + 1 < iterations ? lst[it & 1] : nullptr;
-            a.count_out = it + 1 < iterations ? cnt[it & 1] : nullptr;
+            a.list_out = last ? nullptr : lst[it & 1];
+            a.count_out = last ? nullptr : cnt[it & 1];
             if (a.count_out) SNAPMRF_CUDA(cudaMemsetAsync(a.count_out, 0, sizeof(int), st));
         }
+        a.finish = outputs && (early || last) ? 1 : 0;
         SNAPMRF_GN_DISPATCH(P, true, grid, smem, st, a, chunk);
         SNAPMRF_LAUNCH_CHECK();
     }
-    if (nmaps >= 5 || d_m0 || (d_b1map && nmaps >= 4)) {
+    if (outputs && iterations == 0) {
         a.list_in = a.count_in = nullptr;
         a.list_out = a.count_out = nullptr;
+        a.finish = 1;
         SNAPMRF_GN_DISPATCH(P, false, grid, smem, st, a, chunk);
         SNAPMRF_LAUNCH_CHECK();
     }

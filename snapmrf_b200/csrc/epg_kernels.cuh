@@ -441,10 +441,16 @@ __device__ __forceinline__ void rl2_shift(RealLane2<P> &s, int gl, int L, int w,
     }
 }
 
+// The real-valued kernel stages 32 steps per chunk (half the barriers of 16;
+// its per-step shared data is small).
+constexpr int kRealChunk = 32;
+constexpr int kRealFS = kRealChunk * 4 + 4;          // floats per atom of relaxation factors
+constexpr int kRealReadoutStride = kRealChunk + 1;  // float2 per group
+
 inline size_t epg_real_smem_bytes(int L) {
     int apc = kEpgThreads / L;
-    return (size_t)kChunk * 10 * sizeof(float2) + (size_t)apc * epg_f_stride(ECHO_FISP) * sizeof(float) +
-           (size_t)apc * kReadoutStride * sizeof(float2) + (size_t)apc * 4 * sizeof(float);
+    return (size_t)kRealChunk * 10 * sizeof(float2) + (size_t)apc * kRealFS * sizeof(float) +
+           (size_t)apc * kRealReadoutStride * sizeof(float2) + (size_t)apc * 4 * sizeof(float);
 }
 
 // (An explicit minimum of 1 block per SM lets ptxas use more registers and
@@ -467,7 +473,7 @@ template <int ECHO, int P, bool TAIL, bool FOLD>
 __global__ void SNAPMRF_EPG_REAL_BOUNDS epg_real_kernel(EpgArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr int NF = 4;
-    constexpr int FS = epg_f_stride(ECHO_FISP);
+    constexpr int FS = kRealFS;
     const int L = a.L;
     const int apc = kEpgThreads / L;
     const int tid = threadIdx.x;
@@ -481,10 +487,10 @@ __global__ void SNAPMRF_EPG_REAL_BOUNDS epg_real_kernel(EpgArgs a) {
     const bool active = ab < a.natoms;
     const long long gatom = blk * a.natoms + ab;
 
-    float2 *sC = reinterpret_cast<float2 *>(smem_raw);        // [kChunk][10]
-    float *sF = reinterpret_cast<float *>(sC + kChunk * 10);   // [apc][FS]
-    float2 *sR = reinterpret_cast<float2 *>(sF + apc * FS);    // [apc][kReadoutStride]
-    float *sP = reinterpret_cast<float *>(sR + apc * kReadoutStride);
+    float2 *sC = reinterpret_cast<float2 *>(smem_raw);        // [kRealChunk][10]
+    float *sF = reinterpret_cast<float *>(sC + kRealChunk * 10);   // [apc][FS]
+    float2 *sR = reinterpret_cast<float2 *>(sF + apc * FS);    // [apc][kRealReadoutStride]
+    float *sP = reinterpret_cast<float *>(sR + apc * kRealReadoutStride);
 
     for (int i = tid; i < apc; i += kEpgThreads) {
         long long at = atom0 + i;
@@ -530,8 +536,8 @@ __global__ void SNAPMRF_EPG_REAL_BOUNDS epg_real_kernel(EpgArgs a) {
 
     float nrm = 0.f;
     float2 *out = a.atoms + gatom * nreps;
-    for (long long t0 = 0; t0 < nreps; t0 += kChunk) {
-        const int nch = (int)min((long long)kChunk, nreps - t0);
+    for (long long t0 = 0; t0 < nreps; t0 += kRealChunk) {
+        const int nch = (int)min((long long)kRealChunk, nreps - t0);
         __syncthreads();
         for (int i = tid; i < nch; i += kEpgThreads) rf_real_coeffs2(alpha[t0 + i], phi[t0 + i], sC + 10 * i);
         for (int idx = tid; idx < apc * nch; idx += kEpgThreads) {
@@ -570,7 +576,7 @@ __global__ void SNAPMRF_EPG_REAL_BOUNDS epg_real_kernel(EpgArgs a) {
                     s.fm[0].x = fmaf(c[5].x, f.w, s.fm[0].x);
                     s.zz[0].x = fmaf(c[8].x, f.w, s.zz[0].x);
                     const float v = f.z * s.fp[0].x;
-                    sR[g * kReadoutStride + i] = make_float2(0.f, v);
+                    sR[g * kRealReadoutStride + i] = make_float2(0.f, v);
                     nrm = fmaf(v, v, nrm);
                 }
                 if (ECHO == ECHO_FISP) rl2_shift<P, TAIL>(s, gl, L, w, tail_keep);
@@ -579,7 +585,7 @@ __global__ void SNAPMRF_EPG_REAL_BOUNDS epg_real_kernel(EpgArgs a) {
                 rl2_relax<P>(s, f.x, f.y, lane0);
                 if (lane0) {
                     const float v = s.fp[0].x;
-                    sR[g * kReadoutStride + i] = make_float2(0.f, v);
+                    sR[g * kRealReadoutStride + i] = make_float2(0.f, v);
                     // the complex path adds round(0*0 + v*v) = round(v*v)
                     nrm = __fadd_rn(nrm, __fmul_rn(v, v));
                 }
@@ -589,7 +595,7 @@ __global__ void SNAPMRF_EPG_REAL_BOUNDS epg_real_kernel(EpgArgs a) {
         }
         __syncwarp();
         if (active)
-            for (int q = gl; q < nch; q += L) out[t0 + q] = sR[g * kReadoutStride + q];
+            for (int q = gl; q < nch; q += L) out[t0 + q] = sR[g * kRealReadoutStride + q];
     }
     if (a.normalize || a.norms) {
         nrm = __shfl_sync(0xffffffffu, nrm, 0, L);
