@@ -267,27 +267,37 @@ match_bf16_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
                 for (int c = 0; c < BN / 32; c++) {
                     float v[32];
                     sm100::tmem_ld32(taddr + c * 32, v);
+                    // the 16 scores of this load, then one test of their
+                    // maximum against the current k-th best before any insertion
+                    float sc[16];
+                    int a0;
                     if (IMAG) {
                         // lane pair (2m, 2m+1) = voxel m's (x_r, x_i) rows: the
                         // even lane scores columns 0-15, the odd lane 16-31
                         const int part = lane & 1;
+                        a0 = abase + c * 32 + (part ? 16 : 0);
 #pragma unroll
                         for (int j = 0; j < 16; j++) {
                             const float mine = part ? v[16 + j] : v[j];
                             const float other = __shfl_xor_sync(0xffffffffu, part ? v[j] : v[16 + j], 1);
-                            const int atom = abase + c * 32 + (part ? 16 + j : j);
-                            const float sc = fmaf(mine, mine, other * other);
-                            if (sc > ts[TOPK - 1] && (full_tile || atom < p.bin_natoms)) topk_insert<TOPK>(ts, ti, sc, atom);
+                            sc[j] = fmaf(mine, mine, other * other);
                         }
-                        continue;
-                    }
+                    } else {
+                        a0 = abase + c * 16;
 #pragma unroll
-                    for (int j = 0; j < 16; j++) {
-                        const int atom = abase + c * 16 + j;
-                        const bool valid = full_tile || atom < p.bin_natoms;
-                        float sc = fmaf(v[2 * j], v[2 * j], v[2 * j + 1] * v[2 * j + 1]);
-                        if (FP8) sc *= valid ? __ldg(asc + atom) : 0.f;
-                        if (sc > ts[TOPK - 1] && valid) topk_insert<TOPK>(ts, ti, sc, atom);
+                        for (int j = 0; j < 16; j++) {
+                            sc[j] = fmaf(v[2 * j], v[2 * j], v[2 * j + 1] * v[2 * j + 1]);
+                            if (FP8) sc[j] *= (full_tile || a0 + j < p.bin_natoms) ? __ldg(asc + a0 + j) : 0.f;
+                        }
+                    }
+                    float mx = sc[0];
+#pragma unroll
+                    for (int j = 1; j < 16; j++) mx = fmaxf(mx, sc[j]);
+                    if (mx > ts[TOPK - 1]) {
+#pragma unroll
+                        for (int j = 0; j < 16; j++)
+                            if (sc[j] > ts[TOPK - 1] && (full_tile || a0 + j < p.bin_natoms))
+                                topk_insert<TOPK>(ts, ti, sc[j], a0 + j);
                     }
                 }
                 sm100::tc_fence_before();
