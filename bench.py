@@ -331,15 +331,24 @@ def run_ours(args) -> None:
     # atoms are purely imaginary (the tensor-core forms use half the MMA work)
     MATCH_FLAGS = snap.MATCH_ASSUME_UNIFORM_B1 | snap.MATCH_IMAG_ATOMS
 
+    # the BF16 / FP16 forms take the matching operand (one 16-bit row of Im d
+    # per atom) from the dictionary kernel instead of packing the atoms again
+    d_packed = torch.empty((NATOMS, snap.packed_pitch(T)), dtype=torch.int16, device=dev)
+
+    def packs(precision):
+        return precision in (snap.PREC_BF16, snap.PREC_FP16)
+
     def step(precision, ev=None, gn=0):
         if ev is not None:
             ev[0].record(stream)
-        snap.MRF_dict(d_atoms, d_params, h_mrf, T, T, NATOMS, natoms, 4, NSTATES, "epg_fisp", flags=flags)
+        pk = packs(precision)
+        snap.MRF_dict(d_atoms, d_params, h_mrf, T, T, NATOMS, natoms, 4, NSTATES, "epg_fisp", flags=flags,
+                      d_packed=d_packed if pk else None, packed_precision=precision if pk else 0)
         if ev is not None:
             ev[1].record(stream)
         snap.MRF_match(d_maps, d_img, d_atoms, d_params, T, T, NATOMS, natoms, nvox, in_b1map=d_b1,
                        flags=MATCH_FLAGS, precision=precision, d_index=d_index,
-                       topk=args.topk)
+                       topk=args.topk, packed_atoms=d_packed if pk else None)
         if ev is not None:
             ev[2].record(stream)
         if gn:
@@ -448,10 +457,13 @@ def run_ours(args) -> None:
             e2e_b1[b].copy_(h_b1, non_blocking=True)
             ev_img[b].record(up_stream)
         stream.wait_event(ev_par[b])
-        snap.MRF_dict(e2e_atoms, e2e_par[b], h_mrf, T, T, NATOMS, natoms, 4, NSTATES, "epg_fisp", flags=flags)
+        pk = packs(prec)
+        snap.MRF_dict(e2e_atoms, e2e_par[b], h_mrf, T, T, NATOMS, natoms, 4, NSTATES, "epg_fisp", flags=flags,
+                      d_packed=d_packed if pk else None, packed_precision=prec if pk else 0)
         stream.wait_event(ev_img[b])
         snap.MRF_match(d_maps, e2e_img[b], e2e_atoms, e2e_par[b], T, T, NATOMS, natoms, nvox, in_b1map=e2e_b1[b],
-                       img_stride=T, flags=MATCH_FLAGS, precision=prec, topk=args.topk)
+                       img_stride=T, flags=MATCH_FLAGS, precision=prec, topk=args.topk,
+                       packed_atoms=d_packed if pk else None)
         ev_free[b].record(stream)
         h_maps.copy_(d_maps, non_blocking=True)
 

@@ -146,7 +146,18 @@ typedef struct snapmrf_dict_opts {
     unsigned flags;  /* SNAPMRF_DICT_* */
     int n_iso;       /* ROA isochromats per atom, dephased across 2*pi per TR (1 = reference) */
     float *d_norms;  /* optional out [NATOMS]: l2 norm of each generated atom before normalisation */
+    /* Optional out, device [NATOMS][snapmrf_packed_pitch(nreps)] 16-bit
+     * (packed_precision SNAPMRF_PREC_BF16 or _FP16): the imaginary part of
+     * each generated atom (as written to d_atoms), zero padded, which
+     * snapmrf_mrf_match takes as snapmrf_match_opts.packed_atoms instead of
+     * packing the atoms itself.  Only for the real-valued recursion (epg_fisp
+     * / epg_sr with every RF phase 0, whose atoms are purely imaginary). */
+    void *d_packed;
+    int packed_precision;
 } snapmrf_dict_opts;
+
+/* Row pitch (elements) of packed atoms for nreps time points. */
+size_t snapmrf_packed_pitch(size_t nreps);
 
 /* d_atoms: out, device [NATOMS][nreps] complex (blocks the echo type does
  *          not generate are left untouched, as in the reference)
@@ -205,6 +216,12 @@ typedef struct snapmrf_match_opts {
     int b1map_on_host;      /* b1map is host memory */
     int64_t *d_index;       /* optional out [nvoxels]: chosen global atom index */
     int topk;               /* tensor-core forms: candidates rescored in FP32, 8 or 16 (0: default) */
+    /* Optional: the atoms packed by snapmrf_mrf_dict (snapmrf_dict_opts.d_packed)
+     * in this call's precision (BF16 or FP16) for these same nreps
+     * (packed_nreps == nreps); needs SNAPMRF_MATCH_IMAG_ATOMS.  The FP32
+     * atoms are still read for the exact rescoring. */
+    const void *packed_atoms;
+    size_t packed_nreps;
 } snapmrf_match_opts;
 
 /* d_maps: out, device [nvoxels][nmaps] (nmaps == 5, nparams == 4)

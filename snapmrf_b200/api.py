@@ -51,13 +51,15 @@ class SnapMRFError(RuntimeError):
 
 
 class DictOpts(C.Structure):
-    _fields_ = [("flags", C.c_uint), ("n_iso", C.c_int), ("d_norms", C.c_void_p)]
+    _fields_ = [("flags", C.c_uint), ("n_iso", C.c_int), ("d_norms", C.c_void_p), ("d_packed", C.c_void_p),
+                ("packed_precision", C.c_int)]
 
 
 class MatchOpts(C.Structure):
     _fields_ = [("precision", C.c_int), ("flags", C.c_uint), ("img_stride", C.c_size_t),
                 ("atom_stride", C.c_size_t), ("b1map", C.c_void_p), ("b1map_on_host", C.c_int),
-                ("d_index", C.c_void_p), ("topk", C.c_int)]
+                ("d_index", C.c_void_p), ("topk", C.c_int), ("packed_atoms", C.c_void_p),
+                ("packed_nreps", C.c_size_t)]
 
 
 class RA(C.Structure):
@@ -100,6 +102,8 @@ def lib() -> C.CDLL:
         L.snapmrf_mrf_dict.argtypes = [vp, vp, vp, sz, sz, sz, sz, C.c_int, C.c_int, C.c_char_p,
                                        C.POINTER(DictOpts), vp]
         L.snapmrf_normalize.argtypes = [vp, sz, sz, vp, vp]
+        L.snapmrf_packed_pitch.restype = sz
+        L.snapmrf_packed_pitch.argtypes = [sz]
         L.snapmrf_mrf_match.argtypes = [vp, vp, C.c_int, vp, vp, sz, sz, sz, sz, C.c_int, C.c_int,
                                         C.POINTER(MatchOpts), vp]
         L.snapmrf_mrf_match_noalloc.argtypes = [vp, vp, sz, vp, sz, vp, sz, sz, sz, sz, C.c_int, C.c_int,
@@ -269,7 +273,8 @@ def ra_write(path: str, arr: np.ndarray) -> None:
 
 def MRF_dict(d_atoms, d_params, h_mrf, nreps: int, NREPS: int, NATOMS: int, natoms: int,
              nparams: int = NPARAMS, nstates: int = 101, echo_type: str = "epg_ssfp", *,
-             flags: int = 0, n_iso: int = 1, d_norms=None, stream=None) -> None:
+             flags: int = 0, n_iso: int = 1, d_norms=None, d_packed=None, packed_precision: int = 0,
+             stream=None) -> None:
     """Dictionary generation (src/functions.cu:1224-1315).
 
     d_atoms: device complex64 [NATOMS][nreps] (out); d_params: device float32
@@ -277,7 +282,7 @@ def MRF_dict(d_atoms, d_params, h_mrf, nreps: int, NREPS: int, NATOMS: int, nato
     h_mrf = np.ascontiguousarray(h_mrf, np.float32)
     if h_mrf.size < 4 * NREPS:
         raise SnapMRFError(1, "h_mrf must hold 4*NREPS values")
-    opts = DictOpts(flags, n_iso, _ptr(d_norms))
+    opts = DictOpts(flags, n_iso, _ptr(d_norms), _ptr(d_packed), packed_precision)
     _check(lib().snapmrf_mrf_dict(_ptr(d_atoms), _ptr(d_params), h_mrf.ctypes.data, nreps, NREPS,
                                   NATOMS, natoms, nparams, nstates, echo_type.encode(),
                                   C.byref(opts), _stream_ptr(stream)))
@@ -291,7 +296,7 @@ def normalize(d_atoms, nreps: int, NATOMS: int, d_norms=None, stream=None) -> No
 def MRF_match(d_maps, img, d_atoms, d_params, NREPS: int, nreps: int, NATOMS: int, natoms: int,
               nvoxels: int, nparams: int = NPARAMS, nmaps: int = NMAPS, in_b1map=None, *,
               precision: int = PREC_FP32, flags: int = 0, img_stride: int = 0,
-              d_index=None, topk: int = 0, stream=None) -> None:
+              d_index=None, topk: int = 0, packed_atoms=None, stream=None) -> None:
     """Template matching (src/functions.cu:1493-1584).
 
     img: host numpy complex64 [nvoxels][stride] or a device tensor; NREPS is
@@ -315,7 +320,8 @@ def MRF_match(d_maps, img, d_atoms, d_params, NREPS: int, nreps: int, NATOMS: in
         elif hasattr(in_b1map, "device") and in_b1map.device.type == "cpu":
             b1_host = 1
         b1 = in_b1map
-    opts = MatchOpts(precision, flags, img_stride, NREPS, _ptr(b1), b1_host, _ptr(d_index), topk)
+    opts = MatchOpts(precision, flags, img_stride, NREPS, _ptr(b1), b1_host, _ptr(d_index), topk,
+                     _ptr(packed_atoms), nreps if packed_atoms is not None else 0)
     _check(lib().snapmrf_mrf_match(_ptr(d_maps), _ptr(img), 1 if on_host else 0, _ptr(d_atoms),
                                    _ptr(d_params), nreps, NATOMS, natoms, nvoxels, nparams, nmaps,
                                    C.byref(opts), _stream_ptr(stream)))
@@ -381,3 +387,8 @@ def refine_gn(d_maps, d_img, h_mrf, nreps: int, NREPS: int, nvoxels: int, nstate
                                    h_mrf.ctypes.data, nreps,
                                    NREPS, nvoxels, nstates, echo_type.encode(), iterations, max_rel_step,
                                    tol, _ptr(d_m0), _stream_ptr(stream)))
+
+
+def packed_pitch(nreps: int) -> int:
+    """Row pitch (elements) of atoms packed by MRF_dict(d_packed=...)."""
+    return int(lib().snapmrf_packed_pitch(nreps))

@@ -275,8 +275,14 @@ extern "C" int snapmrf_mrf_dict(float *d_atoms, const float *d_params, const flo
                        : (echo == ECHO_SE || echo == ECHO_TSE) ? 90.f : 0.f;
     a.init_phi_deg = (echo == ECHO_SE || echo == ECHO_TSE) ? 90.f : 0.f;
     a.init_ti = (echo == ECHO_SSFP) ? 40.f : 0.f;
+    a.packed = nullptr;
+    a.packed_half = 0;
+    a.packed_pitch = 0;
+    void *d_packed = opts ? opts->d_packed : nullptr;
 
     if (echo == ECHO_ROA) {
+        if (d_packed)
+            SNAPMRF_FAIL(SNAPMRF_ERR_UNSUPPORTED, "MRF_dict: d_packed needs epg_fisp / epg_sr with every RF phase 0");
         if (n_iso > 32 * 8) SNAPMRF_FAIL(SNAPMRF_ERR_UNSUPPORTED, "MRF_dict: n_iso must be <= 256");
         a.L = 1;
         SNAPMRF_CUDA(launch_roa(a, (long long)natoms, (unsigned)gen_blocks, st));
@@ -293,6 +299,16 @@ extern "C" int snapmrf_mrf_dict(float *d_atoms, const float *d_params, const flo
                      "MRF_dict: nstates must be in [1, %d] for this echo type and schedule "
                      "(up to %d for epg_fisp / epg_sr with all RF phases 0)",
                      32 * kMaxStatesPerLane, 32 * kMaxRealStatesPerLane);
+    if (d_packed) {
+        if (!real_path)
+            SNAPMRF_FAIL(SNAPMRF_ERR_UNSUPPORTED,
+                         "MRF_dict: d_packed needs epg_fisp / epg_sr with every RF phase 0 (purely imaginary atoms)");
+        if (opts->packed_precision != SNAPMRF_PREC_BF16 && opts->packed_precision != SNAPMRF_PREC_FP16)
+            SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "MRF_dict: packed_precision must be SNAPMRF_PREC_BF16 or _FP16");
+        a.packed = d_packed;
+        a.packed_half = opts->packed_precision == SNAPMRF_PREC_FP16 ? 1 : 0;
+        a.packed_pitch = (long long)snapmrf_packed_pitch(nreps);
+    }
     int L, S;
     if (real_path)
         choose_layout(nstates, kMaxRealStatesPerLane, 2, &L, &S);
@@ -333,6 +349,8 @@ __global__ void normalize_kernel(float2 *atoms, float *norms, long long nreps, l
 }
 
 }  // namespace snapmrf
+
+extern "C" size_t snapmrf_packed_pitch(size_t nreps) { return (nreps + 63) / 64 * 64; }
 
 extern "C" int snapmrf_normalize(float *d_atoms, size_t nreps, size_t NATOMS, float *d_norms,
                                  void *stream) {

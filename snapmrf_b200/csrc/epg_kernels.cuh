@@ -1,6 +1,9 @@
 // EPG / ROA device kernels (reference operation order).
 #pragma once
 
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
 #include <cuda_runtime.h>
 
 #include "common.h"
@@ -31,6 +34,10 @@ struct EpgArgs {
     // run time like the reference's kernel arguments, so that __sincosf is
     // evaluated on the device rather than folded at compile time.
     float init_alpha_deg, init_phi_deg, init_ti;
+    // optional 16-bit copy of Im(atom), [blocks][natoms][packed_pitch]
+    void *packed;
+    int packed_half;      // 1: fp16, 0: bf16
+    long long packed_pitch;
 };
 
 // Number of per-(atom, step) factors staged: E1/E2 at TE and at TR-TE, plus
@@ -461,6 +468,15 @@ inline size_t epg_real_smem_bytes(int L) {
 #define SNAPMRF_EPG_REAL_BOUNDS __launch_bounds__(kEpgThreads)
 #endif
 
+// One element of the optional 16-bit copy of Im(atom) (the tensor-core
+// matching operand, one row per atom).
+__device__ __forceinline__ void store_packed(const EpgArgs &a, long long atom, long long q, float v) {
+    if (a.packed_half)
+        reinterpret_cast<__half *>(a.packed)[atom * a.packed_pitch + q] = __float2half_rn(v);
+    else
+        reinterpret_cast<__nv_bfloat16 *>(a.packed)[atom * a.packed_pitch + q] = __float2bfloat16_rn(v);
+}
+
 // FOLD: relaxation is diagonal with one factor for F+ and F- (and Z0's
 // recovery only touches state 0), so it commutes with the dephasing shift:
 // relax(TE), shift, relax(TR - TE) equals shift followed by one relaxation
@@ -595,7 +611,11 @@ __global__ void SNAPMRF_EPG_REAL_BOUNDS epg_real_kernel(EpgArgs a) {
         }
         __syncwarp();
         if (active)
-            for (int q = gl; q < nch; q += L) out[t0 + q] = sR[g * kRealReadoutStride + q];
+            for (int q = gl; q < nch; q += L) {
+                const float2 o = sR[g * kRealReadoutStride + q];
+                out[t0 + q] = o;
+                if (a.packed && !a.normalize) store_packed(a, gatom, t0 + q, o.y);
+            }
     }
     if (a.normalize || a.norms) {
         nrm = __shfl_sync(0xffffffffu, nrm, 0, L);
@@ -605,9 +625,15 @@ __global__ void SNAPMRF_EPG_REAL_BOUNDS epg_real_kernel(EpgArgs a) {
             float inv = nrm;
             if (inv > 0.f) inv = 1.f / sqrtf(inv);
             if (active)
-                for (long long q = gl; q < nreps; q += L) out[q] = c_scale(out[q], inv);
+                for (long long q = gl; q < nreps; q += L) {
+                    const float2 o = c_scale(out[q], inv);
+                    out[q] = o;
+                    if (a.packed) store_packed(a, gatom, q, o.y);
+                }
         }
     }
+    if (a.packed && active)
+        for (long long q = nreps + gl; q < a.packed_pitch; q += L) store_packed(a, gatom, q, 0.f);
 }
 
 // ROA (src/functions.cu:1021-1222).  State m = (Mx, My, Mz).  Per step:

@@ -251,6 +251,10 @@ extern "C" int snapmrf_mrf_match(float *d_maps, const float *img, int img_on_hos
         q.b1map = d_b1;
         q.fmt = precision == SNAPMRF_PREC_FP16 ? 1 : precision == SNAPMRF_PREC_FP8 ? 2 : 0;
         q.imag = (flags & SNAPMRF_MATCH_IMAG_ATOMS) != 0;
+        q.packed = opts ? opts->packed_atoms : nullptr;
+        if (q.packed && (!q.imag || q.fmt == 2 || opts->packed_nreps != nreps))
+            SNAPMRF_FAIL(SNAPMRF_ERR_INVALID,
+                         "MRF_match: packed_atoms need SNAPMRF_MATCH_IMAG_ATOMS, BF16 / FP16 and packed_nreps == nreps");
         q.topk = (opts && opts->topk) ? opts->topk : (q.fmt == 1 ? 8 : 16);
         if (q.topk != 8 && q.topk != 16)
             SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "MRF_match: topk must be 8 or 16 (got %d)", q.topk);

@@ -700,7 +700,8 @@ int match_bf16(const TcMatchRequest &q, cudaStream_t st) {
         bytes += (n + 255) & ~size_t(255);
         return off;
     };
-    const size_t oA = take((size_t)arows * Kp * eb), oB = take((size_t)brows * Kp * eb);
+    const bool prepacked = imag && q.packed;
+    const size_t oA = take((size_t)arows * Kp * eb), oB = take(prepacked ? 0 : (size_t)brows * Kp * eb);
     const size_t oSc = take(fp8 ? (size_t)q.NATOMS * 4 : 0);
     const size_t oTs = take((size_t)cap * TOPK_MAX * 4), oTi = take((size_t)cap * TOPK_MAX * 4);
     const size_t oPerm = take((size_t)cap * 8), oTile = take((size_t)(nbins + 1) * 8);
@@ -710,7 +711,7 @@ int match_bf16(const TcMatchRequest &q, cudaStream_t st) {
     SNAPMRF_CUDA(s.alloc(bytes, st));
     unsigned char *b = s.as<unsigned char>();
     void *A = b + oA;
-    void *B = b + oB;
+    void *B = prepacked ? const_cast<void *>(q.packed) : static_cast<void *>(b + oB);
     float *ascale2 = reinterpret_cast<float *>(b + oSc);
     const bool half = fmt == 1;
     float *top_s = reinterpret_cast<float *>(b + oTs);
@@ -757,13 +758,15 @@ int match_bf16(const TcMatchRequest &q, cudaStream_t st) {
         SNAPMRF_LAUNCH_CHECK();
         // Kp is a multiple of 64, so every 8-element group of a row is whole
         // and 16-byte aligned
-        if (half)
-            pack_atoms_imag_kernel<true><<<nblk(q.NATOMS * 32, 256), 256, 0, st>>>(B, q.atoms, q.atom_stride,
-                                                                                   q.NATOMS, q.nreps, Kp, err);
-        else
-            pack_atoms_imag_kernel<false><<<nblk(q.NATOMS * 32, 256), 256, 0, st>>>(B, q.atoms, q.atom_stride,
-                                                                                    q.NATOMS, q.nreps, Kp, err);
-        SNAPMRF_LAUNCH_CHECK();
+        if (!prepacked) {
+            if (half)
+                pack_atoms_imag_kernel<true><<<nblk(q.NATOMS * 32, 256), 256, 0, st>>>(B, q.atoms, q.atom_stride,
+                                                                                       q.NATOMS, q.nreps, Kp, err);
+            else
+                pack_atoms_imag_kernel<false><<<nblk(q.NATOMS * 32, 256), 256, 0, st>>>(B, q.atoms, q.atom_stride,
+                                                                                        q.NATOMS, q.nreps, Kp, err);
+            SNAPMRF_LAUNCH_CHECK();
+        }
     } else {
         if (half)
             pack_voxels_kernel<true><<<nblk(cap * 32, 256), 256, 0, st>>>(A, q.img, q.img_stride, perm, cap, q.nreps, Kp);

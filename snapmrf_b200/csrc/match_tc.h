@@ -19,6 +19,7 @@ struct TcMatchRequest {
     const float *b1map;      // device [nvox] or null
     int fmt;                 // operands: 0 bf16, 1 fp16, 2 e4m3 (per-row scales)
     bool imag;               // atoms purely imaginary (bf16 / fp16: half the MMA work)
+    const void *packed;      // optional: the atoms' imaginary rows, already packed (imag)
     int topk;                // candidates rescored in FP32: 8 or 16
 };
 

@@ -157,3 +157,71 @@ def test_tc_imag_flag_on_complex_atoms_fails_loudly(snap, prec):
     assert snap.device_error() == 0
     maps, _ = run_match(snap, img, atoms, params, precision=prec)
     assert np.all(np.isfinite(maps))
+
+
+@pytest.mark.parametrize("prec", [BF16, FP16], ids=["bf16", "fp16"])
+@pytest.mark.parametrize("normalize", [False, True])
+def test_dictionary_packs_atoms_for_matching(snap, prec, normalize):
+    """MRF_dict(d_packed=...) writes each atom's imaginary part as one 16-bit
+    row (the matching operand); MRF_match(packed_atoms=...) then skips its own
+    packing and gives identical maps and indices."""
+    import torch
+    T = 300
+    h = mrf_schedule(T, seed=21)
+    b1s = (0.9, 1.0, 1.1)
+    rows = [(a, b, 0.0, d) for d in b1s for b in np.geomspace(10, 800, 12)
+            for a in np.geomspace(100, 3000, 14) if a > b]
+    params = np.array(rows, np.float32)
+    NATOMS = params.shape[0]
+    natoms = NATOMS // len(b1s)
+    pitch = snap.packed_pitch(T)
+    assert pitch % 64 == 0 and pitch >= T
+    flags = snap.DICT_ALL_B1_BLOCKS | (snap.DICT_NORMALIZE if normalize else 0)
+    d_params = torch.from_numpy(params).cuda()
+    d_atoms = torch.empty((NATOMS, T, 2), device="cuda")
+    d_packed = torch.full((NATOMS, pitch), 12345, dtype=torch.int16, device="cuda")
+    snap.MRF_dict(d_atoms, d_params, h, T, T, NATOMS, natoms, 4, 20, "epg_fisp", flags=flags,
+                  d_packed=d_packed, packed_precision=prec)
+    torch.cuda.synchronize()
+    a = d_atoms.cpu().numpy()
+    assert np.all(a[..., 0] == 0)
+    dt = torch.float16 if prec == FP16 else torch.bfloat16
+    want = torch.zeros((NATOMS, pitch), dtype=dt)
+    want[:, :T] = torch.from_numpy(a[..., 1]).to(dt)
+    assert torch.equal(d_packed.cpu().view(dt), want)
+    atoms = (a[..., 0] + 1j * a[..., 1]).astype(np.complex64)
+    img = _voxels(atoms, 700, 22)
+    b1map = np.random.default_rng(23).uniform(0.85, 1.15, 700).astype(np.float32)
+    runs = []
+    for packed in (None, d_packed):
+        d_maps = torch.full((700, 5), -7.0, device="cuda")
+        d_index = torch.full((700,), -1, dtype=torch.int64, device="cuda")
+        snap.MRF_match(d_maps, img, d_atoms, d_params, T, T, NATOMS, natoms, 700, in_b1map=b1map,
+                       precision=prec, flags=snap.MATCH_IMAG_ATOMS, d_index=d_index, img_stride=T,
+                       packed_atoms=packed)
+        torch.cuda.synchronize()
+        runs.append((d_maps.cpu().numpy(), d_index.cpu().numpy()))
+    np.testing.assert_array_equal(runs[0][1], runs[1][1])
+    np.testing.assert_array_equal(runs[0][0], runs[1][0])
+    assert snap.device_error(reset=True) == 0
+
+
+def test_packed_atoms_are_rejected_where_they_do_not_apply(snap):
+    import torch
+    T = 40
+    h = mrf_schedule(T, seed=24)
+    params = np.array([(500.0, 50.0, 0.0, 1.0), (900.0, 80.0, 0.0, 1.0)], np.float32)
+    d_params = torch.from_numpy(params).cuda()
+    d_atoms = torch.empty((2, T, 2), device="cuda")
+    d_packed = torch.empty((2, snap.packed_pitch(T)), dtype=torch.int16, device="cuda")
+    with pytest.raises(snap.SnapMRFError):   # complex recursion: atoms not purely imaginary
+        snap.MRF_dict(d_atoms, d_params, h, T, T, 2, 2, 4, 10, "epg_ssfp", d_packed=d_packed,
+                      packed_precision=FP16)
+    with pytest.raises(snap.SnapMRFError):   # FP8 has no packed form
+        snap.MRF_dict(d_atoms, d_params, h, T, T, 2, 2, 4, 10, "epg_fisp", d_packed=d_packed,
+                      packed_precision=FP8)
+    snap.MRF_dict(d_atoms, d_params, h, T, T, 2, 2, 4, 10, "epg_fisp", d_packed=d_packed, packed_precision=FP16)
+    img = np.ones((3, T), np.complex64)
+    d_maps = torch.empty((3, 5), device="cuda")
+    with pytest.raises(snap.SnapMRFError):   # packed atoms need the imaginary-atom form
+        snap.MRF_match(d_maps, img, d_atoms, d_params, T, T, 2, 2, 3, precision=FP16, packed_atoms=d_packed)
