@@ -334,6 +334,25 @@ int snapmrf_refine_gn(float *d_maps, int nmaps, const float *img, size_t img_str
                       size_t nvoxels, int nstates, const char *echo_type, int iterations,
                       float max_rel_step, float tol, float *d_m0, void *stream);
 
+/* Cramer-Rao bound of (T1, T2) and its gradient with respect to the flip-angle
+ * schedule, for designing schedules.  No counterpart in the reference.
+ *
+ * For each tissue i (d_params row: T1, T2, B0, B1; real FISP / SR recursion
+ * with flip angle alpha_t * B1, every RF phase 0) the signal s = i f and its
+ * tangents f1 = df/dT1, f2 = df/dT2 give the Fisher matrix M = V^T V of
+ * V = [f1, f2, f] (unit noise variance, a real proton-density factor as the
+ * nuisance parameter) and
+ *   d_loss[i] = [M^-1]_00 / T1^2 + [M^-1]_11 / T2^2,
+ * the normalised CRBs of T1 and T2 (NaN when M is singular).
+ * d_grad_alpha (out [nreps]) = d(sum_i d_loss[i]) / d alpha_t, by reverse
+ * mode through the recursion and its tangents, with states kept every
+ * checkpoint_every steps (0: ceil(sqrt(nreps))).
+ * d_signals (optional out [ntissues][3][nreps]): f, f1, f2. */
+int snapmrf_crb_gradient(const float *d_params, int nparams, const float *h_mrf, size_t nreps,
+                         size_t NREPS, size_t ntissues, int nstates, const char *echo_type,
+                         float *d_loss, float *d_grad_alpha, float *d_signals, int checkpoint_every,
+                         void *stream);
+
 #ifdef __cplusplus
 }
 #endif

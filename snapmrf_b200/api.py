@@ -110,6 +110,8 @@ def lib() -> C.CDLL:
                                                 vp, vp, vp]
         L.snapmrf_epg_adjoint.argtypes = [vp, C.c_int, vp, sz, sz, sz, C.c_int, C.c_char_p, vp, vp, vp,
                                           vp, vp, C.c_int, vp]
+        L.snapmrf_crb_gradient.argtypes = [vp, C.c_int, vp, sz, sz, sz, C.c_int, C.c_char_p, vp, vp, vp,
+                                           C.c_int, vp]
         L.snapmrf_refine_gn.argtypes = [vp, C.c_int, vp, sz, vp, vp, sz, sz, sz, C.c_int, C.c_char_p, C.c_int,
                                         C.c_float, C.c_float, vp, vp]
         _lib = L
@@ -392,3 +394,16 @@ def refine_gn(d_maps, d_img, h_mrf, nreps: int, NREPS: int, nvoxels: int, nstate
 def packed_pitch(nreps: int) -> int:
     """Row pitch (elements) of atoms packed by MRF_dict(d_packed=...)."""
     return int(lib().snapmrf_packed_pitch(nreps))
+
+
+def crb_gradient(d_params, h_mrf, nreps: int, NREPS: int, ntissues: int, d_loss, d_grad_alpha,
+                 nparams: int = NPARAMS, nstates: int = 101, echo_type: str = "epg_fisp", *,
+                 d_signals=None, checkpoint_every: int = 0, stream=None) -> None:
+    """Normalised Cramer-Rao bounds of (T1, T2) per tissue (d_loss [ntissues])
+    and the gradient of their sum with respect to the flip angles
+    (d_grad_alpha [nreps]); d_signals optional [ntissues][3][nreps] = f,
+    df/dT1, df/dT2 of the real FISP / SR signal s = i f."""
+    h_mrf = _schedule(h_mrf, NREPS)
+    _check(lib().snapmrf_crb_gradient(_ptr(d_params), nparams, h_mrf.ctypes.data, nreps, NREPS, ntissues,
+                                      nstates, echo_type.encode(), _ptr(d_loss), _ptr(d_grad_alpha),
+                                      _ptr(d_signals), checkpoint_every, _stream_ptr(stream)))

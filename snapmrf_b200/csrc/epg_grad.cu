@@ -665,6 +665,307 @@ static void choose_pairs(int w, int *L, int *P) {
     *P = bP;
 }
 
+// --------------------------------------------------------------------------
+// Cramer-Rao bound of (T1, T2) and its gradient with respect to the schedule
+// --------------------------------------------------------------------------
+// Per tissue the signal f (s = i f) and its tangents f1 = df/dT1, f2 = df/dT2
+// give the Fisher matrix M = V^T V of V = [f1, f2, f] (unit noise, a real
+// proton-density factor as the nuisance parameter), and the loss
+//   L = [M^-1]_00 / T1^2 + [M^-1]_11 / T2^2,
+// the sum of the normalised CRBs of T1 and T2.  dL/dV = 2 V G with
+// G = -M^-1 W M^-1, W = diag(1/T1^2, 1/T2^2, 0); these gradients are carried
+// back through the recursion with its tangents (three adjoint streams) to
+// dL/dalpha_t.  Relaxation over TR after the shift, readout E2(TE) f+[0] after
+// the RF, as in the Gauss-Newton kernel.
+struct CrbArgs {
+    Schedule sch;
+    const float *params;      // [n][nparams]: T1, T2, (B0), B1
+    int nparams;
+    long long n;
+    int w, L, shift;
+    float *fvec;              // [n][3][T]: f, f1, f2
+    const float *gvec;        // [n][3][T]: dL/df, dL/df1, dL/df2
+    float *ckpt;              // [n][nckpt][9][L*S]
+    float *seg;               // [n][C][9][L*S]
+    float *galpha;            // [n][T]: dL/dalpha_t per tissue
+    int C, nckpt;
+};
+
+// Relaxation constants of step t: E1, E2 over TR, their T1 / T2 derivatives,
+// and E2 over TE (the readout) with its T2 derivative.
+struct CrbStep {
+    float E1, E2, dE1, dE2, Ea, dEa;
+};
+
+__device__ __forceinline__ CrbStep crb_step(const Schedule &sc, int t, float T1, float T2) {
+    CrbStep c;
+    const float tr = sc.TR[t], te = sc.TE[t];
+    c.E1 = expf(-tr / T1);
+    c.E2 = expf(-tr / T2);
+    c.dE1 = c.E1 * tr / (T1 * T1);
+    c.dE2 = c.E2 * tr / (T2 * T2);
+    c.Ea = expf(-te / T2);
+    c.dEa = c.Ea * te / (T2 * T2);
+    return c;
+}
+
+template <int S>
+struct Aug {
+    St<S> v, d1, d2;
+};
+
+template <int S>
+__device__ __forceinline__ void aug_zero(Aug<S> &x) {
+#pragma unroll
+    for (int j = 0; j < S; j++) {
+        x.v.p[j] = x.v.m[j] = x.v.z[j] = 0.f;
+        x.d1.p[j] = x.d1.m[j] = x.d1.z[j] = 0.f;
+        x.d2.p[j] = x.d2.m[j] = x.d2.z[j] = 0.f;
+    }
+}
+
+template <int S>
+__device__ __forceinline__ void aug_store(float *dst, int L, int gl, const Aug<S> &x) {
+    const int LS3 = 3 * L * S;
+    store_state<S>(dst, L, gl, x.v);
+    store_state<S>(dst + LS3, L, gl, x.d1);
+    store_state<S>(dst + 2 * LS3, L, gl, x.d2);
+}
+
+template <int S>
+__device__ __forceinline__ void aug_load(const float *src, int L, int gl, Aug<S> &x) {
+    const int LS3 = 3 * L * S;
+    load_state<S>(src, L, gl, x.v);
+    load_state<S>(src + LS3, L, gl, x.d1);
+    load_state<S>(src + 2 * LS3, L, gl, x.d2);
+}
+
+// One step forward: RF, readout (f, f1, f2 on the group's first lane), shift,
+// relaxation over TR with the product rule for the tangents.
+template <int S>
+__device__ __forceinline__ void aug_step(Aug<S> &x, const StepRF &r, const CrbStep &c, bool lane0, int gl, int L,
+                                         int w, int shift, float *f3) {
+    rf_fwd<S>(x.v, r);
+    rf_fwd<S>(x.d1, r);
+    rf_fwd<S>(x.d2, r);
+    if (f3 && lane0) {
+        f3[0] = c.Ea * x.v.p[0];
+        f3[1] = c.Ea * x.d1.p[0];
+        f3[2] = fmaf(c.dEa, x.v.p[0], c.Ea * x.d2.p[0]);
+    }
+    if (shift) {
+        shift_fwd<S>(x.v, gl, L, w);
+        shift_fwd<S>(x.d1, gl, L, w);
+        shift_fwd<S>(x.d2, gl, L, w);
+    }
+#pragma unroll
+    for (int j = 0; j < S; j++) {
+        x.d1.p[j] *= c.E2;
+        x.d1.m[j] *= c.E2;
+        x.d1.z[j] = fmaf(c.dE1, x.v.z[j], c.E1 * x.d1.z[j]);
+        x.d2.p[j] = fmaf(c.dE2, x.v.p[j], c.E2 * x.d2.p[j]);
+        x.d2.m[j] = fmaf(c.dE2, x.v.m[j], c.E2 * x.d2.m[j]);
+        x.d2.z[j] *= c.E1;
+    }
+    if (lane0) x.d1.z[0] -= c.dE1;
+    relax_fwd<S>(x.v, c.E1, c.E2, lane0);
+}
+
+template <int S>
+__global__ void __launch_bounds__(kThreads) crb_forward_kernel(CrbArgs a) {
+    const int L = a.L, LS = L * S;
+    const int g = threadIdx.x / L, gl = threadIdx.x % L;
+    const long long tis = (long long)blockIdx.x * (kThreads / L) + g;
+    const bool active = tis < a.n;
+    const long long at = active ? tis : 0;
+    const bool lane0 = gl == 0;
+    const float *pp = a.params + at * a.nparams;
+    const float T1 = pp[0], T2 = pp[1], B1 = pp[3];
+    const int T = a.sch.nreps;
+    float *ck = a.ckpt + at * (long long)a.nckpt * 9 * LS;
+    float *fv = a.fvec + at * 3LL * T;
+    Aug<S> x;
+    aug_zero<S>(x);
+    if (lane0) x.v.z[0] = 1.f;
+    for (int t = 0; t < T; t++) {
+        if (t % a.C == 0 && active) aug_store<S>(ck + (long long)(t / a.C) * 9 * LS, L, gl, x);
+        float f3[3];
+        aug_step<S>(x, step_rf(a.sch.alpha[t] * B1), crb_step(a.sch, t, T1, T2), lane0, gl, L, a.w, a.shift, f3);
+        if (lane0 && active) {
+            fv[t] = f3[0];
+            fv[T + t] = f3[1];
+            fv[2 * T + t] = f3[2];
+        }
+    }
+}
+
+// One block per tissue: the Fisher matrix, the loss and dL/d(f, f1, f2).
+__global__ void crb_loss_kernel(const float *fvec, float *gvec, float *loss, const float *params, int nparams,
+                                int T) {
+    const long long tis = blockIdx.x;
+    const float *f = fvec + tis * 3LL * T, *f1 = f + T, *f2 = f + 2 * T;
+    double acc[6] = {0, 0, 0, 0, 0, 0};  // M00 M01 M02 M11 M12 M22 over V = [f1, f2, f]
+    for (int t = threadIdx.x; t < T; t += blockDim.x) {
+        const double a = f1[t], b = f2[t], c = f[t];
+        acc[0] += a * a;
+        acc[1] += a * b;
+        acc[2] += a * c;
+        acc[3] += b * b;
+        acc[4] += b * c;
+        acc[5] += c * c;
+    }
+    __shared__ double red[6][32];
+    __shared__ double Gs[9];
+    __shared__ int bad;
+    const int lane = threadIdx.x % 32, warp = threadIdx.x / 32;
+#pragma unroll
+    for (int k = 0; k < 6; k++) {
+        double v = acc[k];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) red[k][warp] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double m[6];
+        for (int k = 0; k < 6; k++) {
+            m[k] = 0;
+            for (int i = 0; i < (int)(blockDim.x / 32); i++) m[k] += red[k][i];
+        }
+        const double M[3][3] = {{m[0], m[1], m[2]}, {m[1], m[3], m[4]}, {m[2], m[4], m[5]}};
+        // inverse by cofactors
+        double C[3][3];
+        C[0][0] = M[1][1] * M[2][2] - M[1][2] * M[2][1];
+        C[0][1] = M[1][2] * M[2][0] - M[1][0] * M[2][2];
+        C[0][2] = M[1][0] * M[2][1] - M[1][1] * M[2][0];
+        C[1][0] = M[0][2] * M[2][1] - M[0][1] * M[2][2];
+        C[1][1] = M[0][0] * M[2][2] - M[0][2] * M[2][0];
+        C[1][2] = M[0][1] * M[2][0] - M[0][0] * M[2][1];
+        C[2][0] = M[0][1] * M[1][2] - M[0][2] * M[1][1];
+        C[2][1] = M[0][2] * M[1][0] - M[0][0] * M[1][2];
+        C[2][2] = M[0][0] * M[1][1] - M[0][1] * M[1][0];
+        const double det = M[0][0] * C[0][0] + M[0][1] * C[0][1] + M[0][2] * C[0][2];
+        bad = !(fabs(det) > 0.0) || !isfinite(det);
+        const double T1 = params[tis * nparams], T2 = params[tis * nparams + 1];
+        const double Wd[3] = {1.0 / (T1 * T1), 1.0 / (T2 * T2), 0.0};
+        double Mi[3][3];
+        for (int i = 0; i < 3; i++)
+            for (int j = 0; j < 3; j++) Mi[i][j] = C[j][i] / det;
+        loss[tis] = bad ? __int_as_float(0x7fc00000) : (float)(Mi[0][0] * Wd[0] + Mi[1][1] * Wd[1]);
+        // G = -Mi W Mi
+        for (int i = 0; i < 3; i++)
+            for (int j = 0; j < 3; j++) {
+                double g = 0;
+                for (int k = 0; k < 3; k++) g += Mi[i][k] * Wd[k] * Mi[k][j];
+                Gs[3 * i + j] = -g;
+            }
+    }
+    __syncthreads();
+    float *g = gvec + tis * 3LL * T;  // [dL/df, dL/df1, dL/df2]
+    for (int t = threadIdx.x; t < T; t += blockDim.x) {
+        const double a = f1[t], b = f2[t], c = f[t];
+        const double g1 = 2 * (a * Gs[0] + b * Gs[3] + c * Gs[6]);
+        const double g2 = 2 * (a * Gs[1] + b * Gs[4] + c * Gs[7]);
+        const double g0 = 2 * (a * Gs[2] + b * Gs[5] + c * Gs[8]);
+        g[t] = bad ? 0.f : (float)g0;
+        g[T + t] = bad ? 0.f : (float)g1;
+        g[2 * T + t] = bad ? 0.f : (float)g2;
+    }
+}
+
+// lambda^T (dR/da) x for one stream pair (the RF derivative as in the adjoint).
+template <int S>
+__device__ __forceinline__ float rf_dadj(const St<S> &l, const St<S> &x0, const StepRF &r) {
+    float ga = 0.f;
+#pragma unroll
+    for (int j = 0; j < S; j++) {
+        const float p = x0.p[j], m = x0.m[j], q = x0.z[j];
+        const float dp = -r.hS * p + r.hS * m - r.C * q;
+        const float dm = r.hS * p - r.hS * m + r.C * q;
+        const float dz = 0.5f * r.C * p - 0.5f * r.C * m - r.S * q;
+        ga += l.p[j] * dp + l.m[j] * dm + l.z[j] * dz;
+    }
+    return ga;
+}
+
+template <int S>
+__device__ __forceinline__ void rf_transpose(St<S> &l, const StepRF &r) {
+#pragma unroll
+    for (int j = 0; j < S; j++) {
+        const float lp = l.p[j], lm = l.m[j], lz = l.z[j];
+        l.p[j] = r.c * lp + r.s * lm + r.hS * lz;
+        l.m[j] = r.s * lp + r.c * lm - r.hS * lz;
+        l.z[j] = -r.S * lp + r.S * lm + r.C * lz;
+    }
+}
+
+template <int S>
+__global__ void __launch_bounds__(kThreads) crb_adjoint_kernel(CrbArgs a) {
+    const int L = a.L, LS = L * S;
+    const int g = threadIdx.x / L, gl = threadIdx.x % L;
+    const long long tis = (long long)blockIdx.x * (kThreads / L) + g;
+    const bool active = tis < a.n;
+    const long long at = active ? tis : 0;
+    const bool lane0 = gl == 0;
+    const float *pp = a.params + at * a.nparams;
+    const float T1 = pp[0], T2 = pp[1], B1 = pp[3];
+    const int T = a.sch.nreps, w = a.w;
+    const float *ck = a.ckpt + at * (long long)a.nckpt * 9 * LS;
+    float *sg = a.seg + at * (long long)a.C * 9 * LS;
+    const float *gv = a.gvec + at * 3LL * T;
+    Aug<S> l, x;
+    aug_zero<S>(l);
+    for (int c = a.nckpt - 1; c >= 0; c--) {
+        const int t0 = c * a.C, t1 = min(T, t0 + a.C);
+        if (active) aug_load<S>(ck + (long long)c * 9 * LS, L, gl, x);
+        else aug_zero<S>(x);
+        for (int t = t0; t < t1; t++) {
+            if (active) aug_store<S>(sg + (long long)(t - t0) * 9 * LS, L, gl, x);
+            aug_step<S>(x, step_rf(a.sch.alpha[t] * B1), crb_step(a.sch, t, T1, T2), lane0, gl, L, w, a.shift,
+                        nullptr);
+        }
+        __syncwarp();
+        for (int t = t1 - 1; t >= t0; t--) {
+            Aug<S> x0;
+            if (active) aug_load<S>(sg + (long long)(t - t0) * 9 * LS, L, gl, x0);
+            else aug_zero<S>(x0);
+            const CrbStep cs = crb_step(a.sch, t, T1, T2);
+            const StepRF r = step_rf(a.sch.alpha[t] * B1);
+            // relaxation over TR, transposed: the signal's adjoint gathers the
+            // tangents' product-rule terms
+#pragma unroll
+            for (int j = 0; j < S; j++) {
+                l.v.p[j] = fmaf(cs.dE2, l.d2.p[j], cs.E2 * l.v.p[j]);
+                l.v.m[j] = fmaf(cs.dE2, l.d2.m[j], cs.E2 * l.v.m[j]);
+                l.v.z[j] = fmaf(cs.dE1, l.d1.z[j], cs.E1 * l.v.z[j]);
+                l.d1.p[j] *= cs.E2;
+                l.d1.m[j] *= cs.E2;
+                l.d1.z[j] *= cs.E1;
+                l.d2.p[j] *= cs.E2;
+                l.d2.m[j] *= cs.E2;
+                l.d2.z[j] *= cs.E1;
+            }
+            if (a.shift) {
+                shift_adj<S>(l.v, gl, L, w);
+                shift_adj<S>(l.d1, gl, L, w);
+                shift_adj<S>(l.d2, gl, L, w);
+            }
+            if (lane0 && active) {
+                const float g0 = gv[t], g1 = gv[T + t], g2 = gv[2 * T + t];
+                l.v.p[0] += fmaf(cs.Ea, g0, cs.dEa * g2);
+                l.d1.p[0] += cs.Ea * g1;
+                l.d2.p[0] += cs.Ea * g2;
+            }
+            float ga = rf_dadj<S>(l.v, x0.v, r) + rf_dadj<S>(l.d1, x0.d1, r) + rf_dadj<S>(l.d2, x0.d2, r);
+            rf_transpose<S>(l.v, r);
+            rf_transpose<S>(l.d1, r);
+            rf_transpose<S>(l.d2, r);
+            ga = group_sum(ga, L);
+            if (lane0 && active) a.galpha[at * T + t] = ga * B1;
+        }
+        __syncwarp();
+    }
+}
+
 static void choose(int w, int *L, int *S) {
     int bL = 32, bS = kMaxS, pad = 1 << 30;
     for (int s = kMaxS; s >= 1; s--)
@@ -873,5 +1174,63 @@ extern "C" int snapmrf_refine_gn(float *d_maps, int nmaps, const float *img, siz
         SNAPMRF_GN_DISPATCH(P, false, grid, smem, st, a, chunk);
         SNAPMRF_LAUNCH_CHECK();
     }
+    return SNAPMRF_OK;
+}
+
+extern "C" int snapmrf_crb_gradient(const float *d_params, int nparams, const float *h_mrf, size_t nreps,
+                                    size_t NREPS, size_t ntissues, int nstates, const char *echo_type, float *d_loss,
+                                    float *d_grad_alpha, float *d_signals, int checkpoint_every, void *stream) {
+    cudaStream_t st = (cudaStream_t)stream;
+    if (!d_params || !h_mrf || !d_loss || !d_grad_alpha) SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "crb_gradient: null pointer");
+    if (nparams < 4 || nreps == 0 || nreps > NREPS || ntissues == 0 || nstates < 1 || nstates > 32 * kMaxS)
+        SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "crb_gradient: bad sizes");
+    if (nreps > 0x7fffffff || ntissues > 0x7fffffff)
+        SNAPMRF_FAIL(SNAPMRF_ERR_UNSUPPORTED, "crb_gradient: too many time points or tissues");
+    const int shift = echo_shift(echo_type);
+    if (shift < 0) SNAPMRF_FAIL(SNAPMRF_ERR_ECHO_TYPE, "crb_gradient: echo type must be epg_fisp or epg_sr");
+    DeviceScratch sbuf;
+    Schedule sc;
+    int rc = upload_schedule(sbuf, &sc, h_mrf, nreps, NREPS, st, "crb_gradient");
+    if (rc) return rc;
+    int L, S;
+    choose(nstates, &L, &S);
+    const int C = checkpoint_every > 0 ? checkpoint_every : (int)std::max(1.0, std::ceil(std::sqrt((double)nreps)));
+    const int nckpt = (int)((nreps + C - 1) / C);
+    const long long LS = (long long)L * S;
+    const size_t n = ntissues;
+    const size_t nf = n * 3 * nreps, ck = n * (size_t)nckpt * 9 * LS, sg = n * (size_t)C * 9 * LS,
+                 ga = n * nreps, part = (size_t)kSplits * nreps;
+    DeviceScratch work;
+    SNAPMRF_CUDA(work.alloc((2 * nf + ck + sg + ga + part) * sizeof(float), st));
+    float *base = work.as<float>();
+    CrbArgs a;
+    a.sch = sc;
+    a.params = d_params;
+    a.nparams = nparams;
+    a.n = (long long)n;
+    a.w = nstates;
+    a.L = L;
+    a.shift = shift;
+    a.fvec = d_signals ? d_signals : base;
+    a.gvec = base + nf;
+    a.ckpt = base + 2 * nf;
+    a.seg = a.ckpt + ck;
+    a.galpha = a.seg + sg;
+    a.C = C;
+    a.nckpt = nckpt;
+    float *partial = a.galpha + ga;
+    const int apc = kThreads / L;
+    dim3 grid((unsigned)((n + apc - 1) / apc));
+    SNAPMRF_GRAD_DISPATCH(crb_forward_kernel, S, grid, st, a);
+    SNAPMRF_LAUNCH_CHECK();
+    crb_loss_kernel<<<(unsigned)n, 256, 0, st>>>(a.fvec, base + nf, d_loss, d_params, nparams, (int)nreps);
+    SNAPMRF_LAUNCH_CHECK();
+    SNAPMRF_GRAD_DISPATCH(crb_adjoint_kernel, S, grid, st, a);
+    SNAPMRF_LAUNCH_CHECK();
+    dim3 pg((unsigned)((nreps + 127) / 128), kSplits);
+    sum_columns_partial_kernel<<<pg, 128, 0, st>>>(partial, a.galpha, (long long)n, (int)nreps);
+    SNAPMRF_LAUNCH_CHECK();
+    sum_columns_final_kernel<<<(unsigned)((nreps + 127) / 128), 128, 0, st>>>(d_grad_alpha, partial, (int)nreps);
+    SNAPMRF_LAUNCH_CHECK();
     return SNAPMRF_OK;
 }

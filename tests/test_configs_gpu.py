@@ -192,3 +192,57 @@ def test_c4_roa_100_isochromats(snap, oracle):
     rel = rel_err_per_atom(got[:ref.shape[0]], ref)
     print(f"C4 ROA n_iso=100: max rel vs FP64 oracle {rel.max():.2e}")
     assert rel.max() < 1e-4
+
+
+def _crb_loss_fp64(oracle, tissues, h, w):
+    """sum_i [M^-1]_00 / T1^2 + [M^-1]_11 / T2^2 from the FP64 forward mode."""
+    total, per, sig = 0.0, [], []
+    for (t1, t2, b1) in tissues:
+        f, f1, _, _ = oracle.fisp_jvp((t1, t2, b1), (1, 0, 0), h, nstates=w)
+        _, f2, _, _ = oracle.fisp_jvp((t1, t2, b1), (0, 1, 0), h, nstates=w)
+        V = np.stack([f1, f2, f], 1)
+        Mi = np.linalg.inv(V.T @ V)
+        li = Mi[0, 0] / t1 ** 2 + Mi[1, 1] / t2 ** 2
+        per.append(li)
+        sig.append(np.stack([f, f1, f2]))
+        total += li
+    return total, np.array(per), np.array(sig)
+
+
+def test_c3_crb_schedule_gradient_three_tissues(snap, oracle):
+    """The CRB loss of three tissues and its gradient with respect to every
+    flip angle (T = 1000, w = 50, checkpoints every 32 steps) against the
+    FP64 forward-mode oracle and central differences of its loss along
+    random directions."""
+    import torch
+    T, w = 1000, 50
+    h = mrf_schedule(T, seed=30, inversion=False)
+    tissues = [(1000.0, 80.0, 1.0), (1500.0, 150.0, 0.9), (800.0, 50.0, 1.1)]
+    params = np.array([(a, b, 0.0, c) for a, b, c in tissues], np.float32)
+    d_p = torch.from_numpy(params).cuda()
+    d_loss = torch.empty(3, device="cuda")
+    d_ga = torch.empty(T, device="cuda")
+    d_sig = torch.empty((3, 3, T), device="cuda")
+    snap.crb_gradient(d_p, h, T, T, 3, d_loss, d_ga, 4, w, "epg_fisp", d_signals=d_sig, checkpoint_every=32)
+    torch.cuda.synchronize()
+    total, per, sig = _crb_loss_fp64(oracle, [tuple(map(float, p[[0, 1, 3]])) for p in params], h, w)
+    err = np.abs(d_sig.cpu().numpy() - sig).max(axis=2) / np.abs(sig).max(axis=2)
+    print(f"f, df/dT1, df/dT2 vs FP64: max rel {err.max():.2e}; loss {d_loss.cpu().numpy()} vs {per}")
+    assert err.max() < 1e-4
+    np.testing.assert_allclose(d_loss.cpu().numpy(), per, rtol=2e-3)
+    g = d_ga.cpu().numpy().astype(np.float64)
+    rng = np.random.default_rng(31)
+    for trial in range(3):
+        v = rng.standard_normal(T)
+        e = 2e-3
+        hp, hm = h.copy(), h.copy()
+        hp[0] = (h[0].astype(np.float64) + e * v).astype(np.float32)
+        hm[0] = (h[0].astype(np.float64) - e * v).astype(np.float32)
+        dv = (hp[0].astype(np.float64) - hm[0]) / (2 * e)   # the direction the float32 angles take
+        tl = [tuple(map(float, p[[0, 1, 3]])) for p in params]
+        lp, _, _ = _crb_loss_fp64(oracle, tl, hp, w)
+        lm, _, _ = _crb_loss_fp64(oracle, tl, hm, w)
+        fd = (lp - lm) / (2 * e)
+        got = float(g @ dv)
+        print(f"CRB gradient along a random direction: adjoint {got:.6e}, FP64 difference {fd:.6e}")
+        assert abs(got - fd) <= 5e-3 * abs(fd) + 1e-3 * float(np.abs(g) @ np.abs(dv))
