@@ -1,11 +1,13 @@
-"""torch.autograd binding of the EPG derivative kernels.
+"""torch.autograd bindings of the EPG derivative kernels.
 
 EPGSignal maps per-atom parameters (T1, T2, B0, B1) and a flip-angle
 schedule to the FISP / SR signal on the GPU: the forward pass is
 snapmrf_mrf_dict (one B1 block per atom, so every atom uses its own B1), the
-backward pass is snapmrf_epg_adjoint.  It exists for gradient checks
-(torch.autograd.gradcheck against central differences) and for prototypes
-that optimise a schedule; dictionary generation and matching do not use it.
+backward pass is snapmrf_epg_adjoint.  CRBLoss gives the Cramer-Rao bound
+loss of a set of tissues with its flip-angle gradient (snapmrf_crb_gradient).
+They serve gradient checks (torch.autograd.gradcheck against central
+differences) and schedule design; dictionary generation and matching do not
+use them.
 """
 from __future__ import annotations
 
@@ -52,3 +54,32 @@ class EPGSignal(torch.autograd.Function):
         grad_params[:, 1] = gp[:, 1]
         grad_params[:, 3] = gp[:, 2]
         return grad_params, ga.to(ctx.alpha_device), None, None, None
+
+
+class CRBLoss(torch.autograd.Function):
+    """loss = CRBLoss.apply(params, alpha, schedule, nstates, echo_type)
+
+    The sum over tissues of the normalised Cramer-Rao bounds of T1 and T2
+    (snapmrf_crb_gradient), differentiable in the flip angles: a schedule
+    design loop is a torch optimiser over `alpha`.
+    params: CUDA float32 [n][4] tissues (T1, T2, B0, B1); alpha: float32 [T]
+    flip angles in radians; schedule: host float32 [4][T] (row 0 is replaced
+    by alpha, RF phases must be 0); returns a 0-d CUDA tensor."""
+
+    @staticmethod
+    def forward(ctx, params, alpha, schedule, nstates: int = 50, echo_type: str = "epg_fisp"):
+        params = params.detach().to(torch.float32).contiguous()
+        n, T = params.shape[0], alpha.shape[0]
+        h = np.array(schedule, np.float32, copy=True).reshape(4, -1)[:, :T].copy()
+        h[0] = alpha.detach().to("cpu", torch.float32).numpy()
+        loss = torch.empty(n, dtype=torch.float32, device=params.device)
+        grad = torch.empty(T, dtype=torch.float32, device=params.device)
+        api.crb_gradient(params, h, T, T, n, loss, grad, 4, nstates, echo_type)
+        ctx.save_for_backward(grad)
+        ctx.alpha_device = alpha.device
+        return loss.sum()
+
+    @staticmethod
+    def backward(ctx, grad_out):
+        (grad,) = ctx.saved_tensors
+        return None, (grad * grad_out).to(ctx.alpha_device), None, None, None

@@ -53,6 +53,8 @@ static void usage() {
             "\t    --topk 8|16\t\t\t candidates rescored in FP32 (tensor-core forms)\n"
             "\t    --all-b1-blocks\t\t generate every B1 block for non-SSFP echo types\n"
             "\t    --normalize\t\t\t unit-norm every atom\n"
+            "\t    --load-atoms <rafile>\t match against a saved dictionary (with --load-params)\n"
+            "\t    --load-params <rafile>\t its parameter table; no dictionary is generated\n"
             "\t    --refine n\t\t\t Gauss-Newton refinement of T1/T2 after matching, at\n"
             "\t\t\t\t\t most n iterations per voxel (epg_fisp / epg_sr with\n"
             "\t\t\t\t\t every RF phase 0; flip angle x B1 as --all-b1-blocks)\n"
@@ -88,7 +90,8 @@ int main(int argc, char **argv) {
     size_t nreps = 1500, NATOMS_req = 0;
     int precision = SNAPMRF_PREC_FP32, topk = 0, refine = 0;
     unsigned dict_flags = 0;
-    enum { OPT_PREC = 1000, OPT_TOPK, OPT_ALLB1, OPT_NORM, OPT_REFINE };
+    enum { OPT_PREC = 1000, OPT_TOPK, OPT_ALLB1, OPT_NORM, OPT_REFINE, OPT_LOADA, OPT_LOADP };
+    const char *load_atoms = NULL, *load_params = NULL;
     static struct option longopts[] = {
         {"b1map", 1, NULL, 'M'},      {"atoms", 1, NULL, 'a'},       {"map", 1, NULL, 'm'},
         {"maps", 1, NULL, 'm'},       {"params", 1, NULL, 'p'},      {"T1", 1, NULL, 't'},
@@ -98,7 +101,8 @@ int main(int argc, char **argv) {
         {"blocksize", 1, NULL, 'B'},  {"NATOMS", 1, NULL, 'N'},      {"help", 0, NULL, 'h'},
         {"precision", 1, NULL, OPT_PREC}, {"topk", 1, NULL, OPT_TOPK},
         {"all-b1-blocks", 0, NULL, OPT_ALLB1}, {"normalize", 0, NULL, OPT_NORM},
-        {"refine", 1, NULL, OPT_REFINE},  {NULL, 0, NULL, 0}};
+        {"refine", 1, NULL, OPT_REFINE},  {"load-atoms", 1, NULL, OPT_LOADA},
+        {"load-params", 1, NULL, OPT_LOADP}, {NULL, 0, NULL, 0}};
     opterr = 0;
     int c;
     while ((c = getopt_long(argc, argv, "M:N:a:m:p:t:s:b:r:w:e:T:G:B:h", longopts, NULL)) != -1) {
@@ -127,6 +131,8 @@ int main(int argc, char **argv) {
         case OPT_ALLB1: dict_flags |= SNAPMRF_DICT_ALL_B1_BLOCKS; break;
         case OPT_NORM: dict_flags |= SNAPMRF_DICT_NORMALIZE; break;
         case OPT_REFINE: refine = atoi(optarg); break;
+        case OPT_LOADA: load_atoms = optarg; break;
+        case OPT_LOADP: load_params = optarg; break;
         case 'h':
         default: usage(); return 1;
         }
@@ -139,9 +145,23 @@ int main(int argc, char **argv) {
     }
     printf("\nnstates : %d\nEcho : %s\n\n", nstates, echo_type);
 
-    // parameter grids (src/mrf.cu:168-232)
+    if ((load_atoms != NULL) != (load_params != NULL)) errx(EX_USAGE, "--load-atoms and --load-params go together");
+    const bool loading = load_atoms != NULL;
+    // parameter grids (src/mrf.cu:168-232), or a saved parameter table
     std::vector<float> t1, t2, b0, b1;
-    if (NATOMS_req != 0) {
+    snapmrf_ra ra_atoms, ra_params;
+    memset(&ra_atoms, 0, sizeof ra_atoms);
+    memset(&ra_params, 0, sizeof ra_params);
+    if (loading) {
+        printf("Loading dictionary...\nAtoms : %s\nParams : %s\n", load_atoms, load_params);
+        check(snapmrf_ra_read(&ra_params, load_params, 0), "ra_read");
+        check(snapmrf_ra_read(&ra_atoms, load_atoms, 0), "ra_read");
+        if (ra_params.eltype != 3 || ra_params.elbyte != 4 || ra_params.ndims < 2 || ra_params.dims[0] != 4)
+            errx(EX_DATAERR, "%s: expected a float (4, NATOMS) parameter table", load_params);
+        if (ra_atoms.eltype != 4 || ra_atoms.elbyte != 8 || ra_atoms.ndims < 2 || ra_atoms.dims[1] != ra_params.dims[1])
+            errx(EX_DATAERR, "%s: expected complex (T, %llu) atoms", load_atoms,
+                 (unsigned long long)ra_params.dims[1]);
+    } else if (NATOMS_req != 0) {
         printf("Hard coding for parameters...\n");
         size_t l_b1 = 11, l_b0 = 21;
         size_t l_t = (size_t)roundf(sqrtf((float)(NATOMS_req / l_b0 / l_b1)));
@@ -155,14 +175,28 @@ int main(int argc, char **argv) {
         printf("Parsing parameters...\nT1 : %s\nT2 : %s\nB0 : %s\nB1 : %s\n", T1, T2, B0, B1);
         t1 = grid_values(T1); t2 = grid_values(T2); b0 = grid_values(B0); b1 = grid_values(B1);
     }
-    size_t NATOMS = snapmrf_compute_natoms(t1.data(), t2.data(), t1.size(), t2.size(), b0.size(), b1.size());
-    size_t natoms = NATOMS / b1.size();
-    printf("l_t1: %zu, l_t2: %zu, l_b0: %zu, l_b1: %zu\nNATOMS: %zu, natoms: %zu\n", t1.size(), t2.size(),
-           b0.size(), b1.size(), NATOMS, natoms);
-    if (NATOMS == 0) errx(EX_SOFTWARE, "Number of atoms is 0!");
-    std::vector<float> h_params(NATOMS * nparams);
-    check(snapmrf_trans_params(h_params.data(), t1.data(), t2.data(), b0.data(), b1.data(), t1.size(), t2.size(),
-                               b0.size(), b1.size(), NATOMS, nparams), "trans_params");
+    size_t NATOMS, natoms;
+    std::vector<float> h_params;
+    if (loading) {
+        NATOMS = (size_t)ra_params.dims[1];
+        const float *pr = reinterpret_cast<const float *>(ra_params.data);
+        h_params.assign(pr, pr + NATOMS * nparams);
+        // B1 blocks: the table's leading run of one B1 value (trans_params order)
+        natoms = 1;
+        while (natoms < NATOMS && pr[natoms * nparams + 3] == pr[3]) natoms++;
+        if (NATOMS % natoms != 0) errx(EX_DATAERR, "%s: B1 blocks of unequal size", load_params);
+        printf("NATOMS: %zu, natoms: %zu\n", NATOMS, natoms);
+    } else {
+        NATOMS = snapmrf_compute_natoms(t1.data(), t2.data(), t1.size(), t2.size(), b0.size(), b1.size());
+        natoms = NATOMS / b1.size();
+        printf("l_t1: %zu, l_t2: %zu, l_b0: %zu, l_b1: %zu\nNATOMS: %zu, natoms: %zu\n", t1.size(), t2.size(),
+               b0.size(), b1.size(), NATOMS, natoms);
+        if (NATOMS == 0) errx(EX_SOFTWARE, "Number of atoms is 0!");
+        h_params.resize(NATOMS * nparams);
+        check(snapmrf_trans_params(h_params.data(), t1.data(), t2.data(), b0.data(), b1.data(), t1.size(),
+                                   t2.size(), b0.size(), b1.size(), NATOMS, nparams),
+              "trans_params");
+    }
 
     // schedule (src/mrf.cu:260-276)
     printf("Input mrf: %s\n", in_mrf);
@@ -170,6 +204,10 @@ int main(int argc, char **argv) {
     if (lines == (size_t)-1 || lines < 2) errx(EX_NOINPUT, "cannot read schedule %s", in_mrf);
     size_t NREPS = lines - 1;
     if (nreps > NREPS) nreps = NREPS;
+    if (loading) {
+        if ((size_t)ra_atoms.dims[0] > NREPS) errx(EX_DATAERR, "%s: more time points than the schedule", load_atoms);
+        nreps = (size_t)ra_atoms.dims[0];
+    }
     printf("NREPS: %zu, nreps: %zu\n\n", NREPS, nreps);
     std::vector<float> h_mrf(NREPS * 4);
     check(snapmrf_csv_read(h_mrf.data(), NREPS, in_mrf), "csv_read");
@@ -187,16 +225,27 @@ int main(int argc, char **argv) {
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
 
-    snapmrf_dict_opts dopt = {dict_flags, 1, NULL};
-    printf("Constructing dictionary...\n");
-    cudaEventRecord(e0, st);
-    check(snapmrf_mrf_dict(d_atoms, d_params, h_mrf.data(), nreps, NREPS, NATOMS, natoms, nparams, nstates,
-                           echo_type, &dopt, st), "MRF_dict");
-    cudaEventRecord(e1, st);
-    cuda_check(cudaStreamSynchronize(st), "dictionary");
     float ms = 0;
-    cudaEventElapsedTime(&ms, e0, e1);
-    printf("Elapsed dictionary time: %.4f s\n\n", ms / 1e3);
+    if (loading) {
+        cuda_check(cudaMemcpyAsync(d_atoms, ra_atoms.data, nreps * NATOMS * 2 * sizeof(float), cudaMemcpyHostToDevice,
+                                   st), "cudaMemcpy");
+        cuda_check(cudaStreamSynchronize(st), "dictionary upload");
+        snapmrf_ra_free(&ra_atoms);
+        snapmrf_ra_free(&ra_params);
+    } else {
+        snapmrf_dict_opts dopt;
+        memset(&dopt, 0, sizeof dopt);
+        dopt.flags = dict_flags;
+        dopt.n_iso = 1;
+        printf("Constructing dictionary...\n");
+        cudaEventRecord(e0, st);
+        check(snapmrf_mrf_dict(d_atoms, d_params, h_mrf.data(), nreps, NREPS, NATOMS, natoms, nparams, nstates,
+                               echo_type, &dopt, st), "MRF_dict");
+        cudaEventRecord(e1, st);
+        cuda_check(cudaStreamSynchronize(st), "dictionary");
+        cudaEventElapsedTime(&ms, e0, e1);
+        printf("Elapsed dictionary time: %.4f s\n\n", ms / 1e3);
+    }
 
     if (!in_img && out_maps) printf("NO data specified! Abort matching!\n");
     if (in_img) {
