@@ -57,11 +57,11 @@ FLOP_PER_STATE_STEP = 66
 # (this schedule) with each relaxation folded into the next RF: the RF's 9
 # FMA (18 flop) per state and step (plus 9 multiplies per lane and step).
 FLOP_PER_STATE_STEP_EXECUTED = 18
-# DRAM bytes per dictionary atom (T = 1000, w = 50, normalised) measured by
-# ncu on the reduced workload (5 B1 blocks, 34,690 atoms: 164.7 MB read +
-# 486.2 MB written in one launch); traffic grows with the atom count, so a
-# full launch moves this times NATOMS.
-DICT_DRAM_BYTES_PER_ATOM = (164.743424e6 + 486.182656e6) / 34690
+# DRAM bytes per dictionary atom (T = 1000, w = 50, normalised, writing the
+# FP16 matching operand too) measured by ncu on the reduced workload (5 B1
+# blocks, 34,690 atoms: 184.2 MB read + 487.7 MB written in one launch);
+# traffic grows with the atom count, so a full launch moves this times NATOMS.
+DICT_DRAM_BYTES_PER_ATOM = (184.245248e6 + 487.704064e6) / 34690
 PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
 
 
