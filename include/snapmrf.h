@@ -222,6 +222,28 @@ typedef struct snapmrf_match_opts {
      * atoms are still read for the exact rescoring. */
     const void *packed_atoms;
     size_t packed_nreps;
+    /* Optional: compressed matching against a low-rank dictionary from
+     * snapmrf_svd_compress.  basis: device complex
+     * [nblocks][basis_rows][basis_stride] (the r leading left singular
+     * vectors of each B1 block, over nreps samples); coeffs: device complex
+     * [NATOMS][coeff_stride] (each atom's r coordinates in its block's
+     * basis); rank: r.  Each voxel is projected onto its B1 block's basis and
+     * scored against the coordinates (r instead of nreps products per pair).
+     * FP32: the maps come from the compressed scores (PD = |<c, U^H x>|), as
+     * matching against the MATLAB code's dict_compress does.  BF16 / FP16 /
+     * FP8: the top-k candidates of the compressed scores are rescored
+     * exactly in FP32 against d_atoms and the voxels (against the
+     * coordinates and projected voxels when d_atoms is NULL).  Needs a B1
+     * map (with one B1 value per block) or a single block; with
+     * SNAPMRF_MATCH_IMAG_ATOMS the basis is taken as real (its imaginary
+     * parts are not read) and the coordinates must be purely imaginary, as
+     * snapmrf_svd_compress writes them for such atoms.  Not combinable with
+     * packed_atoms. */
+    const float *basis;
+    size_t basis_rows, basis_stride;
+    const float *coeffs;
+    size_t coeff_stride;
+    int rank;
 } snapmrf_match_opts;
 
 /* d_maps: out, device [nvoxels][nmaps] (nmaps == 5, nparams == 4)
@@ -235,6 +257,53 @@ int snapmrf_mrf_match(float *d_maps, const float *img, int img_on_host,
                       const float *d_atoms, const float *d_params, size_t nreps,
                       size_t NATOMS, size_t natoms, size_t nvoxels, int nparams, int nmaps,
                       const snapmrf_match_opts *opts, void *stream);
+
+/* ------------------------------------------------------------------------
+ * Low-rank (SVD) compression of a dictionary per B1 block, the method of
+ * McGivney et al. (IEEE TMI 2014) as matlab/MRF_dict_B1.m:127-159 applies it
+ * (input.reduce = 1): each block's atoms D_b (nreps x natoms, columns as
+ * stored) are represented by their coordinates C_b = U_r^H D_b in the span
+ * of the block's r leading left singular vectors U_r.  The rank comes from
+ * block 0 with the MATLAB rule r = #{i : (s_1^2 + ... + s_i^2) /
+ * ||D_0||_F^2 <= sfrac}, and every block keeps r vectors.  The reference's
+ * CUDA path has no counterpart.
+ *
+ * The singular vectors are computed by subspace iteration: k = max_rank +
+ * oversample vectors (k <= SNAPMRF_SVD_MAX_SUBSPACE), a seeded random
+ * start, power_iters rounds of D D^H with FP64 Gram matrices and FP64
+ * Jacobi eigensolvers for the k x k problems, then a Rayleigh-Ritz step.
+ * Deterministic for a given seed.
+ * ---------------------------------------------------------------------- */
+#define SNAPMRF_SVD_MAX_SUBSPACE 80
+/* The atoms are purely imaginary (every Re d_t is 0, as for
+ * SNAPMRF_MATCH_IMAG_ATOMS): the singular vectors are computed in real
+ * arithmetic, the basis is real (imaginary parts 0) and the coordinates
+ * purely imaginary (real parts 0). */
+#define SNAPMRF_SVD_IMAG_ATOMS 0x2u
+
+typedef struct snapmrf_svd_opts {
+    unsigned flags;         /* SNAPMRF_SVD_* */
+    size_t atom_stride;     /* complex samples between atoms (0 = nreps) */
+    double sfrac;           /* energy fraction kept (the MATLAB rule) when rank == 0 */
+    int rank;               /* > 0: keep exactly this many vectors (<= max_rank) */
+    int oversample;         /* subspace vectors beyond max_rank (0: 8) */
+    int power_iters;        /* rounds of D D^H (0: 3; < 0: none) */
+    unsigned long long seed;/* random start of the subspace */
+} snapmrf_svd_opts;
+
+/* d_atoms: device complex [NATOMS][atom_stride], NATOMS = nblocks * natoms;
+ * d_basis: out, device complex [nblocks][max_rank][basis_stride]: row i of
+ *   block b is u_i over the nreps samples (rows >= r are zero);
+ * d_coeffs: out, device complex [NATOMS][coeff_stride] (coeff_stride >=
+ *   max_rank): c_j = U_r^H d_j in columns [0, r), zero in [r, max_rank);
+ * rank: out, r;
+ * h_sv: optional out, host [nblocks][max_rank]: each block's leading
+ *   singular values (Ritz values), descending.
+ * Synchronises `stream` once (to choose r).  Returns SNAPMRF_ERR_INVALID when
+ * sfrac keeps no vector or more than max_rank. */
+int snapmrf_svd_compress(const float *d_atoms, size_t nreps, size_t NATOMS, size_t natoms, int max_rank,
+                         float *d_basis, size_t basis_stride, float *d_coeffs, size_t coeff_stride,
+                         int *rank, double *h_sv, const snapmrf_svd_opts *opts, void *stream);
 
 /* Device-side error word of the tensor-core kernels (a bounded wait that
  * ran out sets it; the maps of that call are then NaN).  Synchronises the

@@ -123,3 +123,74 @@ def fisp_jvp(theta, tangent, h_mrf, nstates: int = 101, echo: str = "epg_fisp", 
     if r != 0:
         raise RuntimeError(f"oracle_fisp_jvp failed: {r}")
     return sig, dsig, loss.value, dloss.value
+
+
+def svd_compress(atoms, natoms: int, sfrac: float | None = None, rank: int | None = None):
+    """Low-rank compression per B1 block, restated from matlab/MRF_dict_B1.m:127-159
+    (input.reduce = 1) in FP64 numpy:
+
+      per block b (ii = 1..numel(B1_v)): [U, S, ~] = svd(dict_norm_b, 'econ');
+      block 0 only: fNRG_v = cumsum(s.^2) ./ sum(s.^2),
+                    nDictSpace = sum(fNRG_v <= sfrac)              (:143-147)
+      U_r = U(:, 1:nDictSpace); dict_compress = U_r' * dict_norm_b   (:149-150)
+
+    atoms: [NATOMS][nreps] complex, block b = rows [b*natoms, (b+1)*natoms)
+    (the columns of MATLAB's nreps x natoms dict_norm).  A fixed `rank`
+    replaces the sfrac rule.  Returns (basis [nb][r][nreps] with row i = u_i,
+    coeffs [NATOMS][r] = U_r^H d_j, r, singular values [nb][min(nreps, natoms)]).
+    """
+    atoms = np.asarray(atoms, np.complex128)
+    nb = atoms.shape[0] // natoms
+    us, ss = [], []
+    for b in range(nb):
+        D = atoms[b * natoms:(b + 1) * natoms].T
+        U, s, _ = np.linalg.svd(D, full_matrices=False)
+        us.append(U)
+        ss.append(s)
+    if rank is None:
+        f = np.cumsum(ss[0] ** 2) / np.sum(ss[0] ** 2)
+        rank = int(np.sum(f <= sfrac))
+    basis = np.stack([U[:, :rank].T for U in us])
+    coeffs = np.concatenate([atoms[b * natoms:(b + 1) * natoms] @ np.conj(us[b][:, :rank])
+                             for b in range(nb)])
+    return basis, coeffs, rank, np.stack(ss)
+
+
+def match_compressed(img, basis, coeffs, params, natoms: int, b1map=None):
+    """Matching in the compressed space (FP64): each voxel is projected onto
+    the basis of the B1 block nearest its B1 (the reference's merge rule,
+    src/functions.cu:1351-1384: strict '<' from 10, ties to the lower block;
+    block 0 without a map) and the first atom of that block with the largest
+    |c_j^H U^H x| wins; PD = that modulus.  Returns (maps [nvox][5], index)."""
+    img = np.asarray(img, np.complex128)
+    coeffs = np.asarray(coeffs, np.complex128)
+    params = np.asarray(params, np.float32).reshape(-1, 4)
+    nb = coeffs.shape[0] // natoms
+    nvox = img.shape[0]
+    bins = np.zeros(nvox, np.int64)
+    if b1map is not None:
+        b1 = np.asarray(b1map, np.float32).reshape(-1)
+        heads = params[np.arange(nb) * natoms, 3]
+        for v in range(nvox):
+            best, dist = 0, np.float32(10.0)
+            for k in range(nb):
+                d = np.float32(abs(b1[v] - heads[k]))
+                if d < dist:
+                    best, dist = k, d
+            bins[v] = best
+    maps = np.zeros((nvox, 5), np.float32)
+    idx = np.zeros(nvox, np.int64)
+    r = basis.shape[1]
+    for b in range(nb):
+        sel = np.nonzero(bins == b)[0]
+        if sel.size == 0:
+            continue
+        xc = img[sel, :basis.shape[2]] @ np.conj(np.asarray(basis[b], np.complex128)).T
+        C = coeffs[b * natoms:(b + 1) * natoms, :r]
+        s = np.abs(xc @ np.conj(C).T)
+        j = np.argmax(s, axis=1)
+        g = b * natoms + j
+        maps[sel, :4] = params[g]
+        maps[sel, 4] = s[np.arange(sel.size), j]
+        idx[sel] = g
+    return maps, idx

@@ -59,7 +59,14 @@ class MatchOpts(C.Structure):
     _fields_ = [("precision", C.c_int), ("flags", C.c_uint), ("img_stride", C.c_size_t),
                 ("atom_stride", C.c_size_t), ("b1map", C.c_void_p), ("b1map_on_host", C.c_int),
                 ("d_index", C.c_void_p), ("topk", C.c_int), ("packed_atoms", C.c_void_p),
-                ("packed_nreps", C.c_size_t)]
+                ("packed_nreps", C.c_size_t), ("basis", C.c_void_p), ("basis_rows", C.c_size_t),
+                ("basis_stride", C.c_size_t), ("coeffs", C.c_void_p), ("coeff_stride", C.c_size_t),
+                ("rank", C.c_int)]
+
+
+class SvdOpts(C.Structure):
+    _fields_ = [("flags", C.c_uint), ("atom_stride", C.c_size_t), ("sfrac", C.c_double), ("rank", C.c_int),
+                ("oversample", C.c_int), ("power_iters", C.c_int), ("seed", C.c_ulonglong)]
 
 
 class RA(C.Structure):
@@ -106,6 +113,8 @@ def lib() -> C.CDLL:
         L.snapmrf_packed_pitch.argtypes = [sz]
         L.snapmrf_mrf_match.argtypes = [vp, vp, C.c_int, vp, vp, sz, sz, sz, sz, C.c_int, C.c_int,
                                         C.POINTER(MatchOpts), vp]
+        L.snapmrf_svd_compress.argtypes = [vp, sz, sz, sz, C.c_int, vp, sz, vp, sz, C.POINTER(C.c_int),
+                                           vp, C.POINTER(SvdOpts), vp]
         L.snapmrf_mrf_match_noalloc.argtypes = [vp, vp, sz, vp, sz, vp, sz, sz, sz, sz, C.c_int, C.c_int,
                                                 vp, vp, vp]
         L.snapmrf_epg_adjoint.argtypes = [vp, C.c_int, vp, sz, sz, sz, C.c_int, C.c_char_p, vp, vp, vp,
@@ -298,12 +307,15 @@ def normalize(d_atoms, nreps: int, NATOMS: int, d_norms=None, stream=None) -> No
 def MRF_match(d_maps, img, d_atoms, d_params, NREPS: int, nreps: int, NATOMS: int, natoms: int,
               nvoxels: int, nparams: int = NPARAMS, nmaps: int = NMAPS, in_b1map=None, *,
               precision: int = PREC_FP32, flags: int = 0, img_stride: int = 0,
-              d_index=None, topk: int = 0, packed_atoms=None, stream=None) -> None:
+              d_index=None, topk: int = 0, packed_atoms=None, compressed=None, stream=None) -> None:
     """Template matching (src/functions.cu:1493-1584).
 
     img: host numpy complex64 [nvoxels][stride] or a device tensor; NREPS is
     the dictionary's time points (atom stride), nreps the matched time points.
-    in_b1map: None, a path to an RA B1 map, a host array or a device tensor."""
+    in_b1map: None, a path to an RA B1 map, a host array or a device tensor.
+    compressed: a Compressed from svd_compress: match in its rank-r space
+    (d_atoms may then be None; with atoms the tensor-core forms rescore
+    their candidates against them)."""
     on_host = isinstance(img, np.ndarray) or (hasattr(img, "device") and img.device.type == "cpu")
     if isinstance(img, np.ndarray):
         img = np.ascontiguousarray(img, np.complex64)
@@ -322,11 +334,51 @@ def MRF_match(d_maps, img, d_atoms, d_params, NREPS: int, nreps: int, NATOMS: in
         elif hasattr(in_b1map, "device") and in_b1map.device.type == "cpu":
             b1_host = 1
         b1 = in_b1map
+    cb = compressed
     opts = MatchOpts(precision, flags, img_stride, NREPS, _ptr(b1), b1_host, _ptr(d_index), topk,
-                     _ptr(packed_atoms), nreps if packed_atoms is not None else 0)
+                     _ptr(packed_atoms), nreps if packed_atoms is not None else 0,
+                     _ptr(cb.basis) if cb else None, cb.max_rank if cb else 0, cb.basis_stride if cb else 0,
+                     _ptr(cb.coeffs) if cb else None, cb.coeff_stride if cb else 0, cb.rank if cb else 0)
     _check(lib().snapmrf_mrf_match(_ptr(d_maps), _ptr(img), 1 if on_host else 0, _ptr(d_atoms),
                                    _ptr(d_params), nreps, NATOMS, natoms, nvoxels, nparams, nmaps,
                                    C.byref(opts), _stream_ptr(stream)))
+
+
+SVD_MAX_SUBSPACE = 80
+SVD_IMAG_ATOMS = 0x2
+
+
+class Compressed:
+    """A dictionary compressed per B1 block by svd_compress: the bases
+    (device complex64 [nblocks][max_rank][basis_stride]), the atoms'
+    coordinates (device complex64 [NATOMS][coeff_stride]), the rank r and
+    the singular values (numpy [nblocks][max_rank])."""
+
+    def __init__(self, basis, coeffs, rank: int, max_rank: int, basis_stride: int, coeff_stride: int, sv):
+        self.basis, self.coeffs, self.rank, self.max_rank = basis, coeffs, rank, max_rank
+        self.basis_stride, self.coeff_stride, self.sv = basis_stride, coeff_stride, sv
+
+
+def svd_compress(d_atoms, nreps: int, NATOMS: int, natoms: int, *, sfrac: float = 0.0, rank: int = 0,
+                 max_rank: int = 64, imag_atoms: bool = False, oversample: int = 0, power_iters: int = 0,
+                 seed: int = 0, atom_stride: int = 0, stream=None) -> Compressed:
+    """Low-rank compression of each B1 block (matlab/MRF_dict_B1.m:127-159):
+    the rank from block 0's energy fraction sfrac (or a fixed rank), the
+    r leading left singular vectors of each block and the atoms'
+    coordinates in them.  d_atoms: device complex64 [NATOMS][atom_stride]."""
+    import torch
+    nb = NATOMS // natoms
+    dev = d_atoms.device if hasattr(d_atoms, "device") else torch.device("cuda")
+    bstride = nreps
+    basis = torch.empty((nb, max_rank, bstride, 2), dtype=torch.float32, device=dev)
+    coeffs = torch.empty((NATOMS, max_rank, 2), dtype=torch.float32, device=dev)
+    sv = np.zeros((nb, max_rank), np.float64)
+    r = C.c_int(0)
+    o = SvdOpts(SVD_IMAG_ATOMS if imag_atoms else 0, atom_stride, sfrac, rank, oversample, power_iters, seed)
+    _check(lib().snapmrf_svd_compress(_ptr(d_atoms), nreps, NATOMS, natoms, max_rank, _ptr(basis), bstride,
+                                      _ptr(coeffs), max_rank, C.byref(r), sv.ctypes.data, C.byref(o),
+                                      _stream_ptr(stream)))
+    return Compressed(basis, coeffs, r.value, max_rank, bstride, max_rank, sv)
 
 
 NOALLOC_MAX_VOXELS = 65536

@@ -21,6 +21,7 @@
 #include "common.h"
 #include "match_kernels.cuh"
 #include "match_tc.h"
+#include "svd.h"
 
 namespace snapmrf {
 
@@ -170,7 +171,8 @@ extern "C" int snapmrf_mrf_match(float *d_maps, const float *img, int img_on_hos
                                  size_t NATOMS, size_t natoms, size_t nvoxels, int nparams,
                                  int nmaps, const snapmrf_match_opts *opts, void *stream) {
     cudaStream_t st = (cudaStream_t)stream;
-    if (!d_maps || !img || !d_atoms || !d_params)
+    const bool comp = opts && opts->basis;
+    if (!d_maps || !img || (!d_atoms && !comp) || !d_params)
         SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "MRF_match: null pointer");
     if (nmaps != 5 || nparams < 4)
         SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "MRF_match: nmaps must be 5 and nparams >= 4");
@@ -192,6 +194,18 @@ extern "C" int snapmrf_mrf_match(float *d_maps, const float *img, int img_on_hos
     if (nblocks > 65535) SNAPMRF_FAIL(SNAPMRF_ERR_UNSUPPORTED, "MRF_match: more than 65535 B1 blocks");
     unsigned flags = opts ? opts->flags : 0u;
     int64_t *d_index = opts ? opts->d_index : nullptr;
+    if (comp) {
+        if (!opts->coeffs || opts->rank < 1 || opts->basis_rows < (size_t)opts->rank ||
+            opts->basis_stride < nreps || opts->coeff_stride < (size_t)opts->rank)
+            SNAPMRF_FAIL(SNAPMRF_ERR_INVALID,
+                         "MRF_match: compressed matching needs coeffs, rank >= 1, basis_rows and coeff_stride >= rank "
+                         "and basis_stride >= nreps");
+        if (opts->packed_atoms)
+            SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "MRF_match: packed_atoms and a compressed basis are exclusive");
+        if (!b1map && nblocks > 1)
+            SNAPMRF_FAIL(SNAPMRF_ERR_UNSUPPORTED,
+                         "MRF_match: compressed matching of several B1 blocks needs a B1 map (one basis per block)");
+    }
 
     // Image on the device: one strided 2D copy instead of one copy per voxel
     // (src/functions.cu:1524-1530).
@@ -230,6 +244,9 @@ extern "C" int snapmrf_mrf_match(float *d_maps, const float *img, int img_on_hos
     }
 
     const long long nvox = (long long)nvoxels;
+    if (comp && general)
+        SNAPMRF_FAIL(SNAPMRF_ERR_UNSUPPORTED,
+                     "MRF_match: compressed matching needs every B1 block to hold one B1 value");
     if (precision == SNAPMRF_PREC_BF16 || precision == SNAPMRF_PREC_FP16 || precision == SNAPMRF_PREC_FP8) {
         if (general)
             SNAPMRF_FAIL(SNAPMRF_ERR_UNSUPPORTED,
@@ -255,6 +272,12 @@ extern "C" int snapmrf_mrf_match(float *d_maps, const float *img, int img_on_hos
         if (q.packed && (!q.imag || q.fmt == 2 || opts->packed_nreps != nreps))
             SNAPMRF_FAIL(SNAPMRF_ERR_INVALID,
                          "MRF_match: packed_atoms need SNAPMRF_MATCH_IMAG_ATOMS, BF16 / FP16 and packed_nreps == nreps");
+        q.basis = comp ? reinterpret_cast<const float2 *>(opts->basis) : nullptr;
+        q.basis_rows = comp ? (long long)opts->basis_rows : 0;
+        q.basis_stride = comp ? (long long)opts->basis_stride : 0;
+        q.coeffs = comp ? reinterpret_cast<const float2 *>(opts->coeffs) : nullptr;
+        q.coeff_stride = comp ? (long long)opts->coeff_stride : 0;
+        q.rank = comp ? opts->rank : 0;
         q.topk = (opts && opts->topk) ? opts->topk : (q.fmt == 1 ? 8 : 16);
         if (q.topk != 8 && q.topk != 16)
             SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "MRF_match: topk must be 8 or 16 (got %d)", q.topk);
@@ -330,6 +353,25 @@ extern "C" int snapmrf_mrf_match(float *d_maps, const float *img, int img_on_hos
     m.slot_start = slot_start;
     m.tile_start = tile_start;
 
+    // Compressed: score the rank-r coordinates of the atoms against the
+    // voxels projected onto their bin's basis; the maps' PD is the
+    // compressed |s|.
+    DeviceScratch s_cimg;
+    if (comp) {
+        const long long rs = (opts->rank + 1) & ~1ll;
+        SNAPMRF_CUDA(s_cimg.alloc((size_t)nvox * rs * sizeof(float2), st));
+        int rc = project_voxels(s_cimg.as<float2>(), rs, d_img, istride, nvox, (long long)nreps,
+                                d_b1 ? vox_bin : nullptr, nbins, reinterpret_cast<const float2 *>(opts->basis),
+                                (long long)opts->basis_rows, (long long)opts->basis_stride, opts->rank,
+                                (flags & SNAPMRF_MATCH_IMAG_ATOMS) != 0, st);
+        if (rc) return rc;
+        m.img = s_cimg.as<float2>();
+        m.img_stride = rs;
+        m.atoms = reinterpret_cast<const float2 *>(opts->coeffs);
+        m.atom_stride = (long long)opts->coeff_stride;
+        m.nreps = opts->rank;
+    }
+
     // Grid: y walks voxel tiles (bin-major, so concurrent CTAs share a bin's
     // atoms in L2), x splits a bin's atom tiles so that small voxel counts
     // still fill the 148 SMs.
@@ -361,7 +403,7 @@ extern "C" int snapmrf_mrf_match(float *d_maps, const float *img, int img_on_hos
     }
     finalize_maps_kernel<<<nblk(nvox * 32, 256), 256, 0, st>>>(
         d_maps, (long long *)d_index, fkeys, d_b1 ? perm : nullptr, d_b1 ? vox_bin : nullptr, m.atoms,
-        m.atom_stride, d_img, istride, (long long)nreps, d_params, nparams, per_bin_atoms, nvox);
+        m.atom_stride, m.img, m.img_stride, m.nreps, d_params, nparams, per_bin_atoms, nvox);
     SNAPMRF_LAUNCH_CHECK();
     return SNAPMRF_OK;
 }

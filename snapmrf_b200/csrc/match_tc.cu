@@ -11,14 +11,16 @@
 // column pairs of 128 atoms per tile: the top-k update needs no cross-thread
 // reduction.
 //
-// Kernel (one persistent CTA per SM, 192 threads):
+// Kernel (one persistent CTA per SM, 320 threads):
 //   warp 0     TMA producer: voxel tile (128 x 64 bf16) + atom tile
 //              (256 x 64 bf16) per K-chunk into a 4-stage ring, 128-byte
 //              swizzle;
 //   warp 1     allocates 512 TMEM columns, issues tcgen05.mma (M 128, N 256,
 //              K 16) into one of two accumulators, commits to mbarriers;
-//   warps 2-5  epilogue: tcgen05.ld of the finished accumulator, |s|^2,
-//              top-k insertion, release of the accumulator.
+//   warps 2-9  epilogue, two warps per TMEM lane group, each on half of the
+//              accumulator's columns: tcgen05.ld, |s|^2, top-k insertion,
+//              release of the accumulator.  Each voxel leaves two top-k
+//              lists; the rescoring kernel takes the k best of their union.
 // Work items are (B1 block, 128-voxel tile); each item loops over all atom
 // tiles of its block.  Every mbarrier wait is bounded (sm100.cuh) and sets a
 // device error word instead of hanging.
@@ -35,6 +37,7 @@
 #include "common.h"
 #include "match_tc.h"
 #include "sm100.cuh"
+#include "svd.h"
 
 namespace snapmrf {
 
@@ -57,7 +60,8 @@ constexpr int A_BYTES = BM * BK * 2;    // 16 KB
 constexpr int B_BYTES = BN * BK * 2;    // 32 KB
 constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
 constexpr int TOPK_MAX = 16;
-constexpr int THREADS = 192;
+constexpr int NLISTS = 2;               // top-k lists per voxel (one per half tile)
+constexpr int THREADS = 320;
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024;
 constexpr uint32_t TMEM_COLS = 512;
 
@@ -130,7 +134,7 @@ match_bf16_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
         }
         for (int a = 0; a < 2; a++) {
             sm100::mbar_init(&tfull[a], 1);
-            sm100::mbar_init(&tempty[a], 128);
+            sm100::mbar_init(&tempty[a], 256);
         }
         sm100::mbar_init(&mma_done, 1);
         sm100::fence_mbar_init();
@@ -236,7 +240,12 @@ match_bf16_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
         __syncwarp();
     } else {
         // ---------------- epilogue ----------------
+        // two warps per TMEM lane group, each taking half of the columns of
+        // every accumulator and keeping its own top-k (merged by the
+        // rescoring kernel), so that two warps per SM sub-partition hide
+        // each other's tcgen05.ld and shuffle latencies
         const int lg = warp % 4;           // TMEM lane group of this warp
+        const int half = (warp - 2) / 4;   // columns [half * BN / 2, (half + 1) * BN / 2)
         const int row = lg * 32 + lane;    // voxel row within the tile
         int acc = 0;
         uint32_t aphase = 0;
@@ -264,7 +273,7 @@ match_bf16_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
                 const int abase = at * APT;
                 const bool full_tile = (long long)abase + APT <= p.bin_natoms;
 #pragma unroll 1
-                for (int c = 0; c < BN / 32; c++) {
+                for (int c = half * (BN / 64); c < (half + 1) * (BN / 64); c++) {
                     float v[32];
                     sm100::tmem_ld32(taddr + c * 32, v);
                     // the 16 scores of this load, then one test of their
@@ -322,10 +331,11 @@ match_bf16_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
             }
             if (!IMAG || !(lane & 1)) {
                 const long long slot = IMAG ? item * (BM / 2) + row / 2 : item * BM + row;
+                const long long o = (slot * NLISTS + half) * TOPK_MAX;
 #pragma unroll
                 for (int k = 0; k < TOPK_MAX; k++) {
-                    p.top_s[slot * TOPK_MAX + k] = k < TOPK ? ts[k] : 0.f;
-                    p.top_i[slot * TOPK_MAX + k] = k < TOPK ? ti[k] : -1;
+                    p.top_s[o + k] = k < TOPK ? ts[k] : 0.f;
+                    p.top_i[o + k] = k < TOPK ? ti[k] : -1;
                 }
             }
             __syncwarp();
@@ -482,6 +492,105 @@ __global__ void pack_atoms_imag_kernel(void *B, const float2 *atoms, long long a
     if (__any_sync(0xffffffffu, real_part) && lane == 0) atomicCAS(err, 0, 7);
 }
 
+// Compressed operands (rank-r coordinates), each value split into 16-bit
+// parts hi = rn(v), lo = rn(v - hi): an A row holds [hi(a), lo(a), hi(a)]
+// and a B row [hi(b), hi(b), lo(b)], so the MMA sums hi(a) hi(b) +
+// lo(a) hi(b) + hi(a) lo(b) = a b - lo(a) lo(b): the product to ~2^-22
+// (FP16) or ~2^-16 (BF16) relative, at K = 3L (L = r, or 2r interleaved),
+// which for r <= 21 still fits the one 64-wide K chunk.  Few coordinates
+// carry most of a score, so unlike K = nreps the rounding of single
+// products does not average out.
+template <bool HALF> struct Half16;
+template <> struct Half16<false> {
+    using T = __nv_bfloat16;
+    static __device__ __forceinline__ T make(float a) { return __float2bfloat16_rn(a); }
+    static __device__ __forceinline__ float back(T a) { return __bfloat162float(a); }
+};
+template <> struct Half16<true> {
+    using T = __half;
+    static __device__ __forceinline__ T make(float a) { return __float2half_rn(a); }
+    static __device__ __forceinline__ float back(T a) { return __half2float(a); }
+};
+
+template <bool HALF>
+__device__ __forceinline__ typename Half16<HALF>::T split_part(float v, int seg, bool atom) {
+    using H = Half16<HALF>;
+    const typename H::T hi = H::make(v);
+    const bool lo = atom ? seg == 2 : seg == 1;
+    return lo ? H::make(v - H::back(hi)) : hi;
+}
+
+// A rows of compressed voxels (r coordinates, unit norm): IMAG gives two
+// rows (Re, Im) per slot, otherwise one interleaved row.  One warp per slot.
+template <bool HALF, bool IMAG>
+__global__ void pack_voxels_comp_kernel(void *A, const float2 *img, long long img_stride, const long long *perm,
+                                        long long nslots, long long r, long long Kp) {
+    using H = Half16<HALF>;
+    const long long slot = (blockIdx.x * (long long)blockDim.x + threadIdx.x) / 32;
+    const int lane = threadIdx.x % 32;
+    if (slot >= nslots) return;
+    const long long v = perm[slot];
+    const float2 *x = img + (v >= 0 ? v : 0) * img_stride;
+    float n = 0.f;
+    if (v >= 0)
+        for (long long i = lane; i < r; i += 32) n += x[i].x * x[i].x + x[i].y * x[i].y;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) n += __shfl_xor_sync(0xffffffffu, n, o);
+    const float inv = n > 0.f ? rsqrtf(n) : 0.f;
+    const long long L = IMAG ? r : 2 * r;
+    typename H::T *row = reinterpret_cast<typename H::T *>(A) + (IMAG ? 2 * slot : slot) * Kp;
+    for (long long e = lane; e < Kp; e += 32) {
+        const int seg = (int)(e / L);
+        const long long i = e % L;
+        float a0 = 0.f, a1 = 0.f;
+        if (v >= 0 && seg < 3) {
+            if (IMAG) {
+                a0 = x[i].x * inv;
+                a1 = x[i].y * inv;
+            } else {
+                a0 = ((i & 1) ? x[i / 2].y : x[i / 2].x) * inv;
+            }
+        }
+        row[e] = seg < 3 ? split_part<HALF>(a0, seg, false) : H::make(0.f);
+        if (IMAG) row[Kp + e] = seg < 3 ? split_part<HALF>(a1, seg, false) : H::make(0.f);
+    }
+}
+
+// B rows of compressed atoms: IMAG one row (Im c; a non-zero Re c sets the
+// error word to 7), otherwise two rows (Re c, Im c) and (-Im c, Re c)
+// interleaved.  One warp per atom.
+template <bool HALF, bool IMAG>
+__global__ void pack_atoms_comp_kernel(void *B, const float2 *coeffs, long long stride, long long natoms, long long r,
+                                       long long Kp, int *err) {
+    using H = Half16<HALF>;
+    const long long a = (blockIdx.x * (long long)blockDim.x + threadIdx.x) / 32;
+    const int lane = threadIdx.x % 32;
+    if (a >= natoms) return;
+    const float2 *c = coeffs + a * stride;
+    const long long L = IMAG ? r : 2 * r;
+    typename H::T *row = reinterpret_cast<typename H::T *>(B) + (IMAG ? a : 2 * a) * Kp;
+    bool real_part = false;
+    for (long long e = lane; e < Kp; e += 32) {
+        const int seg = (int)(e / L);
+        const long long i = e % L;
+        float b0 = 0.f, b1 = 0.f;
+        if (seg < 3) {
+            if (IMAG) {
+                const float2 cv = c[i];
+                real_part |= cv.x != 0.f;
+                b0 = cv.y;
+            } else {
+                const float2 cv = c[i / 2];
+                b0 = (i & 1) ? cv.y : cv.x;
+                b1 = (i & 1) ? cv.x : -cv.y;
+            }
+        }
+        row[e] = seg < 3 ? split_part<HALF>(b0, seg, true) : H::make(0.f);
+        if (!IMAG) row[Kp + e] = seg < 3 ? split_part<HALF>(b1, seg, true) : H::make(0.f);
+    }
+    if (IMAG && __any_sync(0xffffffffu, real_part) && lane == 0) atomicCAS(err, 0, 7);
+}
+
 // E4M3 A rows: voxel perm[slot] scaled so that its largest component is
 // E4M3_MAX (the argmax over atoms does not depend on the voxel's scale),
 // interleaved (Re, Im), zero padded to Kp bytes.  One warp per slot.
@@ -543,8 +652,10 @@ __global__ void pack_atoms_e4m3_kernel(unsigned char *B, float *ascale2, const f
     }
 }
 
-// Exact FP32 rescoring of the top-k per voxel (TOPK of the TOPK_MAX slots);
-// one warp per slot.  The map gets the candidate with the largest |s| (lowest
+// Exact FP32 rescoring of the top-k per voxel; one warp per slot.  The
+// scoring kernel leaves NLISTS lists of TOPK (by approximate score) per
+// voxel, one per half of the atom tiles; their TOPK best (ties to the lower
+// atom index) are rescored.  The map gets the candidate with the largest |s| (lowest
 // atom index on ties, nothing unless |s| > 0, like generate_maps' strict '>'
 // from 0).  VEC: two samples per 16-byte load (strides even, rows aligned).
 template <int TOPK, bool VEC>
@@ -559,7 +670,25 @@ __global__ void rescore_kernel(float *maps, long long *index_out, const float *t
     const long long v = perm[slot];
     if (v < 0) return;
     const long long bin = vox_bin ? vox_bin[v] : 0;
-    int cand = lane < TOPK ? top_i[slot * TOPK_MAX + lane] : -1;
+    static_assert(NLISTS * TOPK <= 32, "one lane per listed candidate");
+    const bool listed = lane < NLISTS * TOPK;
+    const long long o = (slot * NLISTS + lane / TOPK) * TOPK_MAX + lane % TOPK;
+    const int li = listed ? top_i[o] : -1;
+    const float ls = listed && li >= 0 ? top_s[o] : -1.f;
+    int rank = 0;
+#pragma unroll
+    for (int j = 0; j < NLISTS * TOPK; j++) {
+        const float sj = __shfl_sync(0xffffffffu, ls, j);
+        const int ij = __shfl_sync(0xffffffffu, li, j);
+        rank += sj > ls || (sj == ls && (ij < li || (ij == li && j < lane)));
+    }
+    int cand = -1;
+#pragma unroll
+    for (int k = 0; k < TOPK; k++) {
+        const unsigned m = __ballot_sync(0xffffffffu, listed && rank == k);
+        const int ik = __shfl_sync(0xffffffffu, li, m ? __ffs(m) - 1 : 0);
+        if (lane == k) cand = m ? ik : -1;
+    }
     int ci[TOPK];
     const float2 *row[TOPK];
 #pragma unroll
@@ -687,7 +816,14 @@ int match_bf16(const TcMatchRequest &q, cudaStream_t st) {
     const bool imag = q.imag && !fp8;     // one real row per atom, K = T
     const int eb = fp8 ? 1 : 2;           // bytes per element
     const int bke = fp8 ? BK8 : BK;       // K elements per 128-byte row
-    const long long Kp = (((imag ? 1 : 2) * q.nreps + bke - 1) / bke) * bke;
+    // compressed matching scores rank-r coordinates: projected voxels
+    // [nvox][rs] (rs even, for the two-sample loads of the rescoring)
+    const bool comp = q.basis != nullptr;
+    const long long kn = comp ? q.rank : q.nreps;
+    const long long rs = comp ? ((q.rank + 1) & ~1ll) : 0;
+    // BF16 / FP16 compressed operands are split into hi + lo parts (K = 3L)
+    const bool split = comp && !fp8;
+    const long long Kp = (((imag ? 1 : 2) * kn * (split ? 3 : 1) + bke - 1) / bke) * bke;
     const long long cap = ((nvox + BM - 1) / BM + nbins) * BM;  // padded slots, upper bound
     const long long brows = (imag ? 1 : 2) * q.NATOMS;
     const long long arows = (imag ? 2 : 1) * cap;
@@ -703,10 +839,11 @@ int match_bf16(const TcMatchRequest &q, cudaStream_t st) {
     const bool prepacked = imag && q.packed;
     const size_t oA = take((size_t)arows * Kp * eb), oB = take(prepacked ? 0 : (size_t)brows * Kp * eb);
     const size_t oSc = take(fp8 ? (size_t)q.NATOMS * 4 : 0);
-    const size_t oTs = take((size_t)cap * TOPK_MAX * 4), oTi = take((size_t)cap * TOPK_MAX * 4);
+    const size_t oTs = take((size_t)cap * NLISTS * TOPK_MAX * 4), oTi = take((size_t)cap * NLISTS * TOPK_MAX * 4);
     const size_t oPerm = take((size_t)cap * 8), oTile = take((size_t)(nbins + 1) * 8);
     const size_t oCur = take((size_t)(nbins + 1) * 8), oVb = take((size_t)nvox * 4);
     const size_t oCnt = take((size_t)nbins * 4), oErr = take(4);
+    const size_t oCimg = take(comp ? (size_t)nvox * rs * sizeof(float2) : 0);
     DeviceScratch s;
     SNAPMRF_CUDA(s.alloc(bytes, st));
     unsigned char *b = s.as<unsigned char>();
@@ -722,7 +859,13 @@ int match_bf16(const TcMatchRequest &q, cudaStream_t st) {
     int *vox_bin = reinterpret_cast<int *>(b + oVb);
     int *counts = reinterpret_cast<int *>(b + oCnt);
     int *err = reinterpret_cast<int *>(b + oErr);
+    float2 *cimg = reinterpret_cast<float2 *>(b + oCimg);
     SNAPMRF_CUDA(cudaMemsetAsync(err, 0, 4, st));
+    // operands of the scores: the samples, or the rank-r coordinates
+    const float2 *pimg = comp ? cimg : q.img;
+    const long long pis = comp ? rs : q.img_stride;
+    const float2 *patoms = comp ? q.coeffs : q.atoms;
+    const long long pas = comp ? q.coeff_stride : q.atom_stride;
 
     if (q.b1map) {
         SNAPMRF_CUDA(cudaMemsetAsync(counts, 0, (size_t)nbins * 4, st));
@@ -738,49 +881,74 @@ int match_bf16(const TcMatchRequest &q, cudaStream_t st) {
         global_bin_kernel<<<nblk(cap, 256), 256, 0, st>>>(tile_start, perm, nvox, cap);
         SNAPMRF_LAUNCH_CHECK();
     }
-    if (fp8) {
-        pack_voxels_e4m3_kernel<<<nblk(cap * 32, 256), 256, 0, st>>>(static_cast<unsigned char *>(A), q.img,
-                                                                      q.img_stride, perm, cap, q.nreps, Kp);
+    if (comp) {
+        int rc = project_voxels(cimg, rs, q.img, q.img_stride, nvox, q.nreps, q.b1map ? vox_bin : nullptr, nbins,
+                                q.basis, q.basis_rows, q.basis_stride, q.rank, q.imag, st);
+        if (rc) return rc;
+    }
+    if (split) {
+        const unsigned gv = nblk(cap * 32, 256), ga = nblk(q.NATOMS * 32, 256);
+        if (imag && half) {
+            pack_voxels_comp_kernel<true, true><<<gv, 256, 0, st>>>(A, pimg, pis, perm, cap, kn, Kp);
+            SNAPMRF_LAUNCH_CHECK();
+            pack_atoms_comp_kernel<true, true><<<ga, 256, 0, st>>>(B, patoms, pas, q.NATOMS, kn, Kp, err);
+        } else if (imag) {
+            pack_voxels_comp_kernel<false, true><<<gv, 256, 0, st>>>(A, pimg, pis, perm, cap, kn, Kp);
+            SNAPMRF_LAUNCH_CHECK();
+            pack_atoms_comp_kernel<false, true><<<ga, 256, 0, st>>>(B, patoms, pas, q.NATOMS, kn, Kp, err);
+        } else if (half) {
+            pack_voxels_comp_kernel<true, false><<<gv, 256, 0, st>>>(A, pimg, pis, perm, cap, kn, Kp);
+            SNAPMRF_LAUNCH_CHECK();
+            pack_atoms_comp_kernel<true, false><<<ga, 256, 0, st>>>(B, patoms, pas, q.NATOMS, kn, Kp, err);
+        } else {
+            pack_voxels_comp_kernel<false, false><<<gv, 256, 0, st>>>(A, pimg, pis, perm, cap, kn, Kp);
+            SNAPMRF_LAUNCH_CHECK();
+            pack_atoms_comp_kernel<false, false><<<ga, 256, 0, st>>>(B, patoms, pas, q.NATOMS, kn, Kp, err);
+        }
+        SNAPMRF_LAUNCH_CHECK();
+    } else if (fp8) {
+        pack_voxels_e4m3_kernel<<<nblk(cap * 32, 256), 256, 0, st>>>(static_cast<unsigned char *>(A), pimg,
+                                                                      pis, perm, cap, kn, Kp);
         SNAPMRF_LAUNCH_CHECK();
         // Kp is a multiple of 128 bytes, so every 16-byte group of a row is
         // whole and aligned
         pack_atoms_e4m3_kernel<<<nblk(q.NATOMS * 32, 256), 256, 0, st>>>(static_cast<unsigned char *>(B), ascale2,
-                                                                          q.atoms, q.atom_stride, q.NATOMS,
-                                                                          q.nreps, Kp);
+                                                                          patoms, pas, q.NATOMS,
+                                                                          kn, Kp);
         SNAPMRF_LAUNCH_CHECK();
     } else if (imag) {
         if (half)
-            pack_voxels_split_kernel<true><<<nblk(cap * 32, 256), 256, 0, st>>>(A, q.img, q.img_stride, perm, cap,
-                                                                                q.nreps, Kp);
+            pack_voxels_split_kernel<true><<<nblk(cap * 32, 256), 256, 0, st>>>(A, pimg, pis, perm, cap,
+                                                                                kn, Kp);
         else
-            pack_voxels_split_kernel<false><<<nblk(cap * 32, 256), 256, 0, st>>>(A, q.img, q.img_stride, perm, cap,
-                                                                                 q.nreps, Kp);
+            pack_voxels_split_kernel<false><<<nblk(cap * 32, 256), 256, 0, st>>>(A, pimg, pis, perm, cap,
+                                                                                 kn, Kp);
         SNAPMRF_LAUNCH_CHECK();
         // Kp is a multiple of 64, so every 8-element group of a row is whole
         // and 16-byte aligned
         if (!prepacked) {
             if (half)
-                pack_atoms_imag_kernel<true><<<nblk(q.NATOMS * 32, 256), 256, 0, st>>>(B, q.atoms, q.atom_stride,
-                                                                                       q.NATOMS, q.nreps, Kp, err);
+                pack_atoms_imag_kernel<true><<<nblk(q.NATOMS * 32, 256), 256, 0, st>>>(B, patoms, pas,
+                                                                                       q.NATOMS, kn, Kp, err);
             else
-                pack_atoms_imag_kernel<false><<<nblk(q.NATOMS * 32, 256), 256, 0, st>>>(B, q.atoms, q.atom_stride,
-                                                                                        q.NATOMS, q.nreps, Kp, err);
+                pack_atoms_imag_kernel<false><<<nblk(q.NATOMS * 32, 256), 256, 0, st>>>(B, patoms, pas,
+                                                                                        q.NATOMS, kn, Kp, err);
             SNAPMRF_LAUNCH_CHECK();
         }
     } else {
         if (half)
-            pack_voxels_kernel<true><<<nblk(cap * 32, 256), 256, 0, st>>>(A, q.img, q.img_stride, perm, cap, q.nreps, Kp);
+            pack_voxels_kernel<true><<<nblk(cap * 32, 256), 256, 0, st>>>(A, pimg, pis, perm, cap, kn, Kp);
         else
-            pack_voxels_kernel<false><<<nblk(cap * 32, 256), 256, 0, st>>>(A, q.img, q.img_stride, perm, cap, q.nreps, Kp);
+            pack_voxels_kernel<false><<<nblk(cap * 32, 256), 256, 0, st>>>(A, pimg, pis, perm, cap, kn, Kp);
         SNAPMRF_LAUNCH_CHECK();
         // Kp is a multiple of 64, so every 4-pair group of a row is whole and
         // 16-byte aligned (row pitch Kp * 2 bytes)
         if (half)
-            pack_atoms_kernel<true><<<nblk(q.NATOMS * 32, 256), 256, 0, st>>>(B, q.atoms, q.atom_stride, q.NATOMS,
-                                                                                q.nreps, Kp);
+            pack_atoms_kernel<true><<<nblk(q.NATOMS * 32, 256), 256, 0, st>>>(B, patoms, pas, q.NATOMS,
+                                                                                kn, Kp);
         else
-            pack_atoms_kernel<false><<<nblk(q.NATOMS * 32, 256), 256, 0, st>>>(B, q.atoms, q.atom_stride, q.NATOMS,
-                                                                                 q.nreps, Kp);
+            pack_atoms_kernel<false><<<nblk(q.NATOMS * 32, 256), 256, 0, st>>>(B, patoms, pas, q.NATOMS,
+                                                                                 kn, Kp);
         SNAPMRF_LAUNCH_CHECK();
     }
     CUtensorMap mA, mB;
@@ -811,13 +979,19 @@ int match_bf16(const TcMatchRequest &q, cudaStream_t st) {
     kern<<<grid, THREADS, SMEM_BYTES, st>>>(mA, mB, a);
     SNAPMRF_LAUNCH_CHECK();
     // two samples per 16-byte load when every row starts 16-byte aligned
-    const bool vec = q.nreps % 2 == 0 && q.atom_stride % 2 == 0 && q.img_stride % 2 == 0 &&
-                     reinterpret_cast<uintptr_t>(q.atoms) % 16 == 0 && reinterpret_cast<uintptr_t>(q.img) % 16 == 0;
+    // rescoring operands: the atoms and samples, or (compressed, no atoms)
+    // the coordinates and projected voxels
+    const bool rfull = !comp || q.atoms;
+    const float2 *ratoms = rfull ? q.atoms : q.coeffs, *rimg = rfull ? q.img : cimg;
+    const long long ras = rfull ? q.atom_stride : q.coeff_stride, ris = rfull ? q.img_stride : rs;
+    const long long rn = rfull ? q.nreps : q.rank;
+    const bool vec = rn % 2 == 0 && ras % 2 == 0 && ris % 2 == 0 && reinterpret_cast<uintptr_t>(ratoms) % 16 == 0 &&
+                     reinterpret_cast<uintptr_t>(rimg) % 16 == 0;
     auto rk = q.topk > 8 ? (vec ? rescore_kernel<16, true> : rescore_kernel<16, false>)
                          : (vec ? rescore_kernel<8, true> : rescore_kernel<8, false>);
     rk<<<nblk(cap * 32, 256), 256, 0, st>>>(q.maps, q.index_out, top_s, top_i, perm, tile_start, nbins,
-                                            q.b1map ? vox_bin : nullptr, q.atoms, q.atom_stride, q.img,
-                                            q.img_stride, q.nreps, q.params, q.nparams, bin_natoms, err);
+                                            q.b1map ? vox_bin : nullptr, ratoms, ras, rimg, ris, rn, q.params,
+                                            q.nparams, bin_natoms, err);
     SNAPMRF_LAUNCH_CHECK();
     publish_error_kernel<<<1, 1, 0, st>>>(err);
     SNAPMRF_LAUNCH_CHECK();

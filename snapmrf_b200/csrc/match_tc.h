@@ -21,6 +21,14 @@ struct TcMatchRequest {
     bool imag;               // atoms purely imaginary (bf16 / fp16: half the MMA work)
     const void *packed;      // optional: the atoms' imaginary rows, already packed (imag)
     int topk;                // candidates rescored in FP32: 8 or 16
+    // compressed matching (basis != null): voxels are projected onto their
+    // bin's rank-r basis and scored against the atoms' coordinates; the
+    // candidates are rescored against `atoms` (the coordinates when null)
+    const float2 *basis;     // device [nblocks][basis_rows][basis_stride]
+    long long basis_rows, basis_stride;
+    const float2 *coeffs;    // device [NATOMS][coeff_stride]
+    long long coeff_stride;
+    int rank;
 };
 
 // BF16 / FP16 / E4M3 tcgen05 scores + top-k + FP32 rescoring; enqueued on st.

@@ -112,3 +112,50 @@ def test_oracle_forward_mode_matches_dictionary_and_differences(oracle, echo):
     _, ds2, _, _ = oracle.fisp_jvp(th, (0, 0, 0), h, nstates=w, echo=echo, dalpha=dv)
     assert np.abs(ds2 - (sp - sm) / (2 * e)).max() < 1e-4 * np.abs(ds2).max()
     assert np.abs(ds2 - ds).max() < 1e-3 * np.abs(ds).max()
+
+
+def _with_spectrum(rng, T, n, s):
+    """A T x n complex matrix with singular values s (returned as n atoms)."""
+    qa, _ = np.linalg.qr(rng.standard_normal((T, len(s))) + 1j * rng.standard_normal((T, len(s))))
+    qb, _ = np.linalg.qr(rng.standard_normal((n, len(s))) + 1j * rng.standard_normal((n, len(s))))
+    return ((qa * s) @ np.conj(qb).T).T
+
+
+def test_oracle_svd_rank_rule(oracle):
+    """nDictSpace = sum(cumsum(s.^2)./sum(s.^2) <= sfrac) on block 0, kept for
+    every block (matlab/MRF_dict_B1.m:143-150)."""
+    rng = np.random.default_rng(0)
+    s0 = np.sqrt([0.5, 0.3, 0.15, 0.05])          # cumulative energy 0.5 0.8 0.95 1.0
+    s1 = np.sqrt([0.9, 0.06, 0.03, 0.01])
+    atoms = np.concatenate([_with_spectrum(rng, 12, 9, s0), _with_spectrum(rng, 12, 9, s1)])
+    for sfrac, r in [(0.49, 0), (0.6, 1), (0.9, 2), (0.97, 3), (0.9999, 3)]:
+        basis, coeffs, rank, sv = oracle.svd_compress(atoms, 9, sfrac=sfrac)
+        assert rank == r, (sfrac, rank)
+        assert basis.shape == (2, r, 12) and coeffs.shape == (18, r)
+    np.testing.assert_allclose(sv[0, :4], s0, rtol=1e-12)
+    np.testing.assert_allclose(sv[1, :4], s1, rtol=1e-12)
+    # the coordinates hold the kept energy of each block
+    basis, coeffs, rank, sv = oracle.svd_compress(atoms, 9, sfrac=0.9)
+    for b in range(2):
+        np.testing.assert_allclose(np.sum(np.abs(coeffs[9 * b:9 * b + 9]) ** 2), np.sum(sv[b, :2] ** 2),
+                                   rtol=1e-12)
+
+
+def test_oracle_compressed_match_full_rank_is_exact(oracle):
+    """At full rank the projection is exact, so compressed matching equals
+    the oracle's MRF_match (picks and PD)."""
+    rng = np.random.default_rng(1)
+    T, natoms, nb, nvox = 40, 16, 3, 50
+    atoms = rng.standard_normal((nb * natoms, T)) + 1j * rng.standard_normal((nb * natoms, T))
+    atoms /= np.linalg.norm(atoms, axis=1, keepdims=True)
+    params = np.array([(100.0 + i, 10.0 + i % 7, 0.0, 0.8 + 0.2 * (i // natoms)) for i in range(nb * natoms)],
+                      np.float32)
+    img = (atoms[rng.integers(0, nb * natoms, nvox)] * 2.0
+           + 0.05 * (rng.standard_normal((nvox, T)) + 1j * rng.standard_normal((nvox, T))))
+    b1 = params[rng.integers(0, nb * natoms, nvox), 3] + rng.uniform(-0.05, 0.05, nvox).astype(np.float32)
+    basis, coeffs, rank, _ = oracle.svd_compress(atoms, natoms, rank=natoms)
+    mc, ic = oracle.match_compressed(img, basis, coeffs, params, natoms, b1map=b1)
+    m, i = oracle.match(img.astype(np.complex64), atoms.astype(np.complex64), params, T, natoms=natoms,
+                        b1map=b1)
+    np.testing.assert_array_equal(ic, i)
+    np.testing.assert_allclose(mc[:, 4], m[:, 4], rtol=1e-5)
