@@ -32,7 +32,9 @@
 #include <cuda_fp8.h>
 
 #include <algorithm>
+#include <cmath>
 #include <mutex>
+#include <numeric>
 
 #include "common.h"
 #include "match_tc.h"
@@ -72,6 +74,7 @@ struct Args {
     int nbins;
     long long bin_natoms;
     int nk;                       // K chunks of BK
+    int tile_stride;              // atom tiles visited in the order (at * tile_stride) % natiles
     uint32_t idesc;               // tcgen05 instruction descriptor
     const float *ascale2;         // E4M3: [NATOMS] 1 / (atom scale)^2
     float *top_s;                 // [slots][TOPK]
@@ -162,8 +165,9 @@ match_bf16_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
                 const int bin = find_bin(p.tile_start, p.nbins, item / IPT);
                 const int vrow = (int)(item * BM);
                 for (int at = 0; at < natiles && ok; at++) {
-                    const int brow = IMAG ? (int)((long long)bin * p.bin_natoms + (long long)at * APT)
-                                          : (int)(2 * ((long long)bin * p.bin_natoms + (long long)at * BA));
+                    const long long pt = (long long)at * p.tile_stride % natiles;
+                    const int brow = IMAG ? (int)((long long)bin * p.bin_natoms + pt * APT)
+                                          : (int)(2 * ((long long)bin * p.bin_natoms + pt * BA));
                     for (int kc = 0; kc < p.nk; kc++) {
                         if (!sm100::mbar_wait(&empty[stage], phase ^ 1, p.err, 1)) {
                             ok = false;
@@ -270,7 +274,7 @@ match_bf16_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
                 }
                 sm100::tc_fence_after();
                 const uint32_t taddr = tmem + (uint32_t)(acc * BN) + ((uint32_t)(lg * 32) << 16);
-                const int abase = at * APT;
+                const int abase = (int)((long long)at * p.tile_stride % natiles) * APT;
                 const bool full_tile = (long long)abase + APT <= p.bin_natoms;
 #pragma unroll 1
                 for (int c = half * (BN / 64); c < (half + 1) * (BN / 64); c++) {
@@ -969,6 +973,17 @@ int match_bf16(const TcMatchRequest &q, cudaStream_t st) {
     a.nbins = nbins;
     a.bin_natoms = bin_natoms;
     a.nk = (int)(Kp / bke);
+    // Atom tiles in a golden-ratio stride order (coprime to their count):
+    // the dictionary's (T1, T2) order makes consecutive tiles' scores rise
+    // smoothly toward a voxel's best, so visiting tiles spread over the grid
+    // first raises the k-th best early and saves top-k insertions.
+    {
+        const long long natiles = (bin_natoms + (imag ? BN : BA) - 1) / (imag ? BN : BA);
+        long long st_ = std::max(1ll, (long long)std::llround(0.618034 * (double)natiles));
+        while (std::gcd(st_, natiles) != 1) st_++;
+        a.tile_stride = natiles > 1 ? (int)(st_ % natiles) : 1;
+        if (a.tile_stride == 0) a.tile_stride = 1;
+    }
     a.idesc = fp8 ? sm100::make_idesc_e4m3(BM, BN) : half ? sm100::make_idesc_f16(BM, BN) : sm100::make_idesc_bf16(BM, BN);
     a.ascale2 = fp8 ? ascale2 : nullptr;
     a.top_s = top_s;

@@ -7,8 +7,11 @@
 //     -w/--nstates n  -e/--echo_type name     -T/--nreps n
 //     -G/--gridsize, -B/--blocksize (accepted, unused)  -h/--help
 // The usage text's spellings --maps, --states and --timepoints are accepted
-// too.  Additive options: --precision fp32|bf16|fp16, --topk 8|16,
-// --all-b1-blocks (non-SSFP echo types over every B1 block), --normalize.
+// too.  Additive options: --precision fp32|bf16|fp16|fp8, --topk 8|16,
+// --all-b1-blocks (non-SSFP echo types over every B1 block), --normalize,
+// --load-atoms / --load-params, --refine n, and --compress sfrac (with
+// --max-rank, --out-basis, --out-compressed) for matching in the
+// SVD-compressed space of each B1 block.
 // Times are wall-clock (CUDA events), not the reference's CPU clock().
 #include <cmath>
 #include <cstdio>
@@ -55,6 +58,12 @@ static void usage() {
             "\t    --normalize\t\t\t unit-norm every atom\n"
             "\t    --load-atoms <rafile>\t match against a saved dictionary (with --load-params)\n"
             "\t    --load-params <rafile>\t its parameter table; no dictionary is generated\n"
+            "\t    --compress sfrac\t\t match in the SVD-compressed space of each B1 block,\n"
+            "\t\t\t\t\t keeping the energy fraction sfrac of block 0\n"
+            "\t\t\t\t\t (McGivney et al.; matlab/MRF_dict_B1.m input.reduce)\n"
+            "\t    --max-rank r\t\t largest rank --compress may keep (default 64)\n"
+            "\t    --out-basis <rafile>\t the bases U_r, complex (nreps, r x B1 blocks)\n"
+            "\t    --out-compressed <rafile>\t the compressed atoms, complex (r, NATOMS)\n"
             "\t    --refine n\t\t\t Gauss-Newton refinement of T1/T2 after matching, at\n"
             "\t\t\t\t\t most n iterations per voxel (epg_fisp / epg_sr with\n"
             "\t\t\t\t\t every RF phase 0; flip angle x B1 as --all-b1-blocks)\n"
@@ -88,9 +97,12 @@ int main(int argc, char **argv) {
     const char *T1 = "20:20:3000", *T2 = "20:10:1000", *B0 = "0", *B1 = "1", *echo_type = "epg_ssfp";
     int nparams = 4, nmaps = 5, nstates = 101;
     size_t nreps = 1500, NATOMS_req = 0;
-    int precision = SNAPMRF_PREC_FP32, topk = 0, refine = 0;
+    int precision = SNAPMRF_PREC_FP32, topk = 0, refine = 0, max_rank = 64;
+    double compress = 0.0;
+    const char *out_basis = NULL, *out_compressed = NULL;
     unsigned dict_flags = 0;
-    enum { OPT_PREC = 1000, OPT_TOPK, OPT_ALLB1, OPT_NORM, OPT_REFINE, OPT_LOADA, OPT_LOADP };
+    enum { OPT_PREC = 1000, OPT_TOPK, OPT_ALLB1, OPT_NORM, OPT_REFINE, OPT_LOADA, OPT_LOADP, OPT_COMP, OPT_MAXR,
+           OPT_OBAS, OPT_OCMP };
     const char *load_atoms = NULL, *load_params = NULL;
     static struct option longopts[] = {
         {"b1map", 1, NULL, 'M'},      {"atoms", 1, NULL, 'a'},       {"map", 1, NULL, 'm'},
@@ -102,7 +114,9 @@ int main(int argc, char **argv) {
         {"precision", 1, NULL, OPT_PREC}, {"topk", 1, NULL, OPT_TOPK},
         {"all-b1-blocks", 0, NULL, OPT_ALLB1}, {"normalize", 0, NULL, OPT_NORM},
         {"refine", 1, NULL, OPT_REFINE},  {"load-atoms", 1, NULL, OPT_LOADA},
-        {"load-params", 1, NULL, OPT_LOADP}, {NULL, 0, NULL, 0}};
+        {"load-params", 1, NULL, OPT_LOADP}, {"compress", 1, NULL, OPT_COMP},
+        {"max-rank", 1, NULL, OPT_MAXR},      {"out-basis", 1, NULL, OPT_OBAS},
+        {"out-compressed", 1, NULL, OPT_OCMP}, {NULL, 0, NULL, 0}};
     opterr = 0;
     int c;
     while ((c = getopt_long(argc, argv, "M:N:a:m:p:t:s:b:r:w:e:T:G:B:h", longopts, NULL)) != -1) {
@@ -133,6 +147,10 @@ int main(int argc, char **argv) {
         case OPT_REFINE: refine = atoi(optarg); break;
         case OPT_LOADA: load_atoms = optarg; break;
         case OPT_LOADP: load_params = optarg; break;
+        case OPT_COMP: compress = atof(optarg); break;
+        case OPT_MAXR: max_rank = atoi(optarg); break;
+        case OPT_OBAS: out_basis = optarg; break;
+        case OPT_OCMP: out_compressed = optarg; break;
         case 'h':
         default: usage(); return 1;
         }
@@ -247,6 +265,44 @@ int main(int argc, char **argv) {
         printf("Elapsed dictionary time: %.4f s\n\n", ms / 1e3);
     }
 
+    // low-rank compression per B1 block (the MATLAB code's input.reduce)
+    float *d_basis = NULL, *d_coeffs = NULL;
+    int svd_rank = 0;
+    if (compress > 0.0) {
+        const size_t nb = NATOMS / natoms;
+        cuda_check(cudaMalloc((void **)&d_basis, nb * max_rank * nreps * 2 * sizeof(float)), "cudaMalloc");
+        cuda_check(cudaMalloc((void **)&d_coeffs, NATOMS * max_rank * 2 * sizeof(float)), "cudaMalloc");
+        snapmrf_svd_opts so;
+        memset(&so, 0, sizeof so);
+        so.sfrac = compress;
+        printf("Compressing dictionary (SVD per B1 block, sfrac %g)...\n", compress);
+        cudaEventRecord(e0, st);
+        check(snapmrf_svd_compress(d_atoms, nreps, NATOMS, natoms, max_rank, d_basis, nreps, d_coeffs,
+                                   (size_t)max_rank, &svd_rank, NULL, &so, st), "svd_compress");
+        cudaEventRecord(e1, st);
+        cuda_check(cudaStreamSynchronize(st), "compression");
+        cudaEventElapsedTime(&ms, e0, e1);
+        printf("Rank: %d\nElapsed compression time: %.4f s\n\n", svd_rank, ms / 1e3);
+        if (out_basis) {
+            // MATLAB's U_r: the blocks' r vectors side by side, (nreps, r * nb)
+            printf("Output basis: %s\n", out_basis);
+            std::vector<float> h(nb * max_rank * nreps * 2), o(nb * svd_rank * nreps * 2);
+            cuda_check(cudaMemcpy(h.data(), d_basis, h.size() * sizeof(float), cudaMemcpyDeviceToHost), "cudaMemcpy");
+            for (size_t b = 0; b < nb; b++)
+                memcpy(&o[b * svd_rank * nreps * 2], &h[b * max_rank * nreps * 2], svd_rank * nreps * 2 * sizeof(float));
+            save_ra(o.data(), 4, 8, out_basis, nreps, nb * svd_rank);
+        }
+        if (out_compressed) {
+            // MATLAB's dict_compress: (r, NATOMS)
+            printf("Output compressed atoms: %s\n", out_compressed);
+            std::vector<float> h(NATOMS * max_rank * 2), o(NATOMS * svd_rank * 2);
+            cuda_check(cudaMemcpy(h.data(), d_coeffs, h.size() * sizeof(float), cudaMemcpyDeviceToHost), "cudaMemcpy");
+            for (size_t j = 0; j < NATOMS; j++)
+                memcpy(&o[j * svd_rank * 2], &h[j * max_rank * 2], svd_rank * 2 * sizeof(float));
+            save_ra(o.data(), 4, 8, out_compressed, svd_rank, NATOMS);
+        }
+    }
+
     if (!in_img && out_maps) printf("NO data specified! Abort matching!\n");
     if (in_img) {
         printf("Input img: %s\n", in_img);
@@ -264,6 +320,14 @@ int main(int argc, char **argv) {
         mopt.img_stride = nt;
         mopt.atom_stride = nreps;
         mopt.topk = topk;
+        if (d_basis) {
+            mopt.basis = d_basis;
+            mopt.basis_rows = (size_t)max_rank;
+            mopt.basis_stride = nreps;
+            mopt.coeffs = d_coeffs;
+            mopt.coeff_stride = (size_t)max_rank;
+            mopt.rank = svd_rank;
+        }
         snapmrf_ra b1ra;
         memset(&b1ra, 0, sizeof b1ra);
         if (in_b1map) {
@@ -331,6 +395,8 @@ int main(int argc, char **argv) {
     }
     cudaFree(d_atoms);
     cudaFree(d_params);
+    if (d_basis) cudaFree(d_basis);
+    if (d_coeffs) cudaFree(d_coeffs);
     cudaStreamDestroy(st);
     return 0;
 }

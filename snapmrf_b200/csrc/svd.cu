@@ -294,19 +294,21 @@ __global__ void __launch_bounds__(THREADS) project64_kernel(const float2 *x, lon
 }
 
 // Projection of voxels onto their bin's basis for the compressed matching,
-// where the rank is small: one warp per tile of PT voxels of one bin (WPB
+// where the rank is small: one warp per tile of PT voxels of one bin (VWPB
 // independent warps per CTA, no CTA barrier), a lane per voxel holding the
-// KC columns [c0, c0 + KC) of one pass in registers (columns >= k read zero
-// basis values), two columns per packed two-wide FMA with the basis read as
-// broadcast float4s.  FP32 sums per chunk of PT samples, FP64 across chunks.
-// RB: real basis (imaginary parts not read).
+// VKC columns [c0, c0 + VKC) of one pass in registers (columns >= k read
+// zero basis values), two columns per packed two-wide FMA.  The basis chunk
+// is kept as [column][sample] (conflict-free stores) and read as broadcast
+// float4s of four samples.  FP32 sums per chunk of PT samples, FP64 across
+// chunks.  RB: real basis (imaginary parts not read).
 constexpr int VKC = 16;  // columns per pass
 constexpr int VWPB = 2;  // warps (tiles) per CTA
+constexpr int VLD = PT + 4;  // basis row pitch (16-byte aligned rows)
 template <bool RB>
 __global__ void __launch_bounds__(VWPB * 32) project_voxels_kernel(ProjArgs a, int c0, long long ntiles) {
     __shared__ float sxr[VWPB][PT][PT + 1], sxi[VWPB][PT][PT + 1];
-    __shared__ __align__(16) float sbr[VWPB][PT][VKC];
-    __shared__ __align__(16) float sbi[VWPB][RB ? 1 : PT][VKC];
+    __shared__ __align__(16) float sbr[VWPB][VKC][VLD];
+    __shared__ __align__(16) float sbi[VWPB][RB ? 1 : VKC][VLD];
     const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
     const long long g = (long long)blockIdx.x * VWPB + warp;
     if (g >= ntiles) return;  // warp-uniform; no CTA-wide barrier follows
@@ -342,31 +344,40 @@ __global__ void __launch_bounds__(VWPB * 32) project_voxels_kernel(ProjArgs a, i
         for (int c = 0; c < VKC; c++) {
             float2 v = make_float2(0.f, 0.f);
             if (c0 + c < a.k && tin) v = B[(long long)(c0 + c) * a.basis_stride + t];
-            sbr[warp][lane][c] = v.x;
-            if constexpr (!RB) sbi[warp][lane][c] = v.y;
+            sbr[warp][c][lane] = v.x;
+            if constexpr (!RB) sbi[warp][c][lane] = v.y;
         }
         __syncwarp();
-#pragma unroll 2
-        for (int tt = 0; tt < PT; tt++) {
-            const float xr = sxr[warp][lane][tt], xi = sxi[warp][lane][tt];
-            const float2 xr2 = make_float2(xr, xr), xi2 = make_float2(xi, xi);
+#pragma unroll 1
+        for (int t4 = 0; t4 < PT; t4 += 4) {
+            float xr[4], xi[4];
 #pragma unroll
-            for (int q = 0; q < VKC / 4; q++) {
-                const float4 b = *reinterpret_cast<const float4 *>(&sbr[warp][tt][4 * q]);
-                const float2 b01 = make_float2(b.x, b.y), b23 = make_float2(b.z, b.w);
-                ar[2 * q] = __ffma2_rn(b01, xr2, ar[2 * q]);
-                ar[2 * q + 1] = __ffma2_rn(b23, xr2, ar[2 * q + 1]);
-                ai[2 * q] = __ffma2_rn(b01, xi2, ai[2 * q]);
-                ai[2 * q + 1] = __ffma2_rn(b23, xi2, ai[2 * q + 1]);
+            for (int u = 0; u < 4; u++) {
+                xr[u] = sxr[warp][lane][t4 + u];
+                xi[u] = sxi[warp][lane][t4 + u];
+            }
+#pragma unroll
+            for (int q = 0; q < VKC / 2; q++) {
+                const float4 b0 = *reinterpret_cast<const float4 *>(&sbr[warp][2 * q][t4]);
+                const float4 b1 = *reinterpret_cast<const float4 *>(&sbr[warp][2 * q + 1][t4]);
+                const float2 bb[4] = {make_float2(b0.x, b1.x), make_float2(b0.y, b1.y), make_float2(b0.z, b1.z),
+                                      make_float2(b0.w, b1.w)};
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    ar[q] = __ffma2_rn(bb[u], make_float2(xr[u], xr[u]), ar[q]);
+                    ai[q] = __ffma2_rn(bb[u], make_float2(xi[u], xi[u]), ai[q]);
+                }
                 if constexpr (!RB) {
                     // conj(b) x: Re += bi xi, Im -= bi xr
-                    const float4 c = *reinterpret_cast<const float4 *>(&sbi[warp][tt][4 * q]);
-                    const float2 c01 = make_float2(c.x, c.y), c23 = make_float2(c.z, c.w);
-                    const float2 nxr2 = make_float2(-xr, -xr);
-                    ar[2 * q] = __ffma2_rn(c01, xi2, ar[2 * q]);
-                    ar[2 * q + 1] = __ffma2_rn(c23, xi2, ar[2 * q + 1]);
-                    ai[2 * q] = __ffma2_rn(c01, nxr2, ai[2 * q]);
-                    ai[2 * q + 1] = __ffma2_rn(c23, nxr2, ai[2 * q + 1]);
+                    const float4 c0v = *reinterpret_cast<const float4 *>(&sbi[warp][2 * q][t4]);
+                    const float4 c1v = *reinterpret_cast<const float4 *>(&sbi[warp][2 * q + 1][t4]);
+                    const float2 cc[4] = {make_float2(c0v.x, c1v.x), make_float2(c0v.y, c1v.y),
+                                          make_float2(c0v.z, c1v.z), make_float2(c0v.w, c1v.w)};
+#pragma unroll
+                    for (int u = 0; u < 4; u++) {
+                        ar[q] = __ffma2_rn(cc[u], make_float2(xi[u], xi[u]), ar[q]);
+                        ai[q] = __ffma2_rn(cc[u], make_float2(-xr[u], -xr[u]), ai[q]);
+                    }
                 }
             }
         }

@@ -54,3 +54,49 @@ def test_cli_saved_dictionary_and_refinement(snap, tmp_path):
     assert np.all(m_ref[:, 1] > 0) and np.all(m_ref[:, 0] > m_ref[:, 1])
     np.testing.assert_allclose(m_ref[:, 0], m_gen[:, 0], rtol=0.2)
     assert np.mean(m_ref[:, 0] != m_gen[:, 0]) > 0.5
+
+
+def test_cli_compressed_matching(snap, tmp_path):
+    """--compress: the bases and compressed atoms written in MATLAB's layouts
+    (U_r as (nreps, r x blocks), dict_compress as (r, NATOMS)), orthonormal
+    bases, coordinates U_r^H d, and FP16 compressed matching (rescored in
+    FP32) picking the uncompressed FP32 run's atoms."""
+    T = 200
+    rng = np.random.default_rng(41)
+    a = np.deg2rad(10 + 50 * np.abs(np.sin(np.pi * np.arange(T) / 70)))
+    tr = rng.uniform(11, 15, T)
+    sched = np.array([a, np.zeros(T), tr, tr / 2], np.float32)
+    rows = "\n".join(",".join(repr(float(v)) for v in sched[:, t]) for t in range(T))
+    (tmp_path / "sched.csv").write_text(HEADER + "\n" + rows + "\n")
+    grid = ["-e", "epg_fisp", "-t", "300:100:2000", "-s", "30:10:200", "-b", "0", "-r", "0.9:0.1:1.1",
+            "-w", "20", "-T", str(T), "--all-b1-blocks", "--normalize"]
+    _run(grid + ["sched.csv", "-a", "atoms.ra", "-p", "params.ra"], tmp_path)
+    atoms = snap.ra_read(str(tmp_path / "atoms.ra")).astype(np.complex128)
+    params = snap.ra_read(str(tmp_path / "params.ra"))
+    n = 200
+    pick = rng.integers(0, atoms.shape[0], n)
+    img = atoms[pick] * (rng.uniform(0.5, 1, n) * np.exp(1j * rng.uniform(0, 6.28, n)))[:, None]
+    img = (img + 0.003 * (rng.standard_normal(img.shape) + 1j * rng.standard_normal(img.shape))).astype(np.complex64)
+    snap.ra_write(str(tmp_path / "img.ra"), img.reshape(10, 20, T))
+    snap.ra_write(str(tmp_path / "b1.ra"), params[pick, 3].astype(np.float32).reshape(10, 20))
+    _run(grid + ["sched.csv", "img.ra", "-M", "b1.ra", "-m", "maps32.ra"], tmp_path)
+    out = _run(grid + ["sched.csv", "img.ra", "-M", "b1.ra", "-m", "maps_c.ra", "--precision", "fp16",
+                       "--compress", "0.99999", "--max-rank", "32", "--out-basis", "basis.ra",
+                       "--out-compressed", "comp.ra"], tmp_path)
+    r = int(out.split("Rank: ")[1].split()[0])
+    nb = 3
+    natoms = atoms.shape[0] // nb
+    basis = snap.ra_read(str(tmp_path / "basis.ra")).astype(np.complex128)
+    comp = snap.ra_read(str(tmp_path / "comp.ra")).astype(np.complex128)
+    assert 1 <= r <= 32 and basis.shape == (nb * r, T) and comp.shape == (atoms.shape[0], r)
+    for b in range(nb):
+        U = basis[b * r:(b + 1) * r]
+        np.testing.assert_allclose(U @ np.conj(U).T, np.eye(r), atol=1e-5)
+        want = atoms[b * natoms:(b + 1) * natoms] @ np.conj(U).T
+        assert np.max(np.abs(comp[b * natoms:(b + 1) * natoms] - want)) <= 1e-5
+    m32 = snap.ra_read(str(tmp_path / "maps32.ra")).reshape(-1, 5)
+    mc = snap.ra_read(str(tmp_path / "maps_c.ra")).reshape(-1, 5)
+    same = np.all(m32[:, :4] == mc[:, :4], axis=1)
+    print(f"rank {r}: {same.mean():.4f} of the picks equal the FP32 run's")
+    assert same.mean() >= 0.97
+    np.testing.assert_allclose(mc[same, 4], m32[same, 4], rtol=1e-5)
