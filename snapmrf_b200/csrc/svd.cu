@@ -294,27 +294,31 @@ __global__ void __launch_bounds__(THREADS) project64_kernel(const float2 *x, lon
 }
 
 // Projection of voxels onto their bin's basis for the compressed matching,
-// where the rank is small: one warp per tile of PT voxels of one bin (VWPB
-// independent warps per CTA, no CTA barrier), a lane per voxel holding the
-// VKC columns [c0, c0 + VKC) of one pass in registers (columns >= k read
-// zero basis values), two columns per packed two-wide FMA.  The basis chunk
-// is kept as [column][sample] (conflict-free stores) and read as broadcast
-// float4s of four samples.  FP32 sums per chunk of PT samples, FP64 across
-// chunks.  RB: real basis (imaginary parts not read).
-constexpr int VKC = 16;  // columns per pass
-constexpr int VWPB = 2;  // warps (tiles) per CTA
+// where the rank is small.  A CTA takes a tile of PT voxels of one bin and
+// its VTS warps split the samples (chunks of PT, round-robin), so that even
+// 25,600 voxels give enough warps to hide the image loads; a lane holds one
+// voxel's VKC columns [c0, c0 + VKC) of one pass (columns >= k read zero
+// basis values), two columns per packed two-wide FMA.  Each warp's basis
+// chunk is kept as [column][sample] (conflict-free stores) and read as
+// broadcast float4s of four samples.  The warps' partial sums are added in
+// shared memory at the end.  RB: real basis (imaginary parts not read).
+constexpr int VKC = 16;   // columns per pass
+constexpr int VTS = 4;    // warps per tile (sample split)
 constexpr int VLD = PT + 4;  // basis row pitch (16-byte aligned rows)
+struct VoxSmem {
+    float xr[VTS][PT][PT + 1], xi[VTS][PT][PT + 1];
+    __align__(16) float br[VTS][VKC][VLD];
+    __align__(16) float bi[VTS][VKC][VLD];
+};
 template <bool RB>
-__global__ void __launch_bounds__(VWPB * 32) project_voxels_kernel(ProjArgs a, int c0, long long ntiles) {
-    __shared__ float sxr[VWPB][PT][PT + 1], sxi[VWPB][PT][PT + 1];
-    __shared__ __align__(16) float sbr[VWPB][VKC][VLD];
-    __shared__ __align__(16) float sbi[VWPB][RB ? 1 : VKC][VLD];
+__global__ void __launch_bounds__(VTS * 32) project_voxels_kernel(ProjArgs a, int c0) {
+    extern __shared__ __align__(16) unsigned char vsm_raw[];
+    VoxSmem &sm = *reinterpret_cast<VoxSmem *>(vsm_raw);
     const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
-    const long long g = (long long)blockIdx.x * VWPB + warp;
-    if (g >= ntiles) return;  // warp-uniform; no CTA-wide barrier follows
+    const long long g = blockIdx.x;
     long long bin, row;
     if (a.perm) {
-        if (g >= a.tile_start[a.nbins]) return;
+        if (g >= a.tile_start[a.nbins]) return;  // uniform per CTA
         const int b = find_bin(a.tile_start, a.nbins, g);
         bin = b;
         const long long sl = a.slot_start[b] + (g - a.tile_start[b]) * PT + lane;
@@ -325,27 +329,24 @@ __global__ void __launch_bounds__(VWPB * 32) project_voxels_kernel(ProjArgs a, i
     }
     const float2 *B = a.basis + bin * a.basis_rows * a.basis_stride;
     float2 ar[VKC / 2], ai[VKC / 2];
-    double sr[VKC], si[VKC];
 #pragma unroll
     for (int j = 0; j < VKC / 2; j++) ar[j] = ai[j] = make_float2(0.f, 0.f);
-#pragma unroll
-    for (int j = 0; j < VKC; j++) sr[j] = si[j] = 0.0;
-    for (long long t0 = 0; t0 < a.nreps; t0 += PT) {
+    for (long long t0 = (long long)warp * PT; t0 < a.nreps; t0 += (long long)VTS * PT) {
         const long long t = t0 + lane;
         const bool tin = t < a.nreps;
         for (int r = 0; r < PT; r++) {
             const long long rr = __shfl_sync(0xffffffffu, row, r);
             float2 v = make_float2(0.f, 0.f);
             if (rr >= 0 && tin) v = a.x[rr * a.x_stride + t];
-            sxr[warp][r][lane] = v.x;
-            sxi[warp][r][lane] = v.y;
+            sm.xr[warp][r][lane] = v.x;
+            sm.xi[warp][r][lane] = v.y;
         }
 #pragma unroll
         for (int c = 0; c < VKC; c++) {
             float2 v = make_float2(0.f, 0.f);
             if (c0 + c < a.k && tin) v = B[(long long)(c0 + c) * a.basis_stride + t];
-            sbr[warp][c][lane] = v.x;
-            if constexpr (!RB) sbi[warp][c][lane] = v.y;
+            sm.br[warp][c][lane] = v.x;
+            if constexpr (!RB) sm.bi[warp][c][lane] = v.y;
         }
         __syncwarp();
 #pragma unroll 1
@@ -353,13 +354,13 @@ __global__ void __launch_bounds__(VWPB * 32) project_voxels_kernel(ProjArgs a, i
             float xr[4], xi[4];
 #pragma unroll
             for (int u = 0; u < 4; u++) {
-                xr[u] = sxr[warp][lane][t4 + u];
-                xi[u] = sxi[warp][lane][t4 + u];
+                xr[u] = sm.xr[warp][lane][t4 + u];
+                xi[u] = sm.xi[warp][lane][t4 + u];
             }
 #pragma unroll
             for (int q = 0; q < VKC / 2; q++) {
-                const float4 b0 = *reinterpret_cast<const float4 *>(&sbr[warp][2 * q][t4]);
-                const float4 b1 = *reinterpret_cast<const float4 *>(&sbr[warp][2 * q + 1][t4]);
+                const float4 b0 = *reinterpret_cast<const float4 *>(&sm.br[warp][2 * q][t4]);
+                const float4 b1 = *reinterpret_cast<const float4 *>(&sm.br[warp][2 * q + 1][t4]);
                 const float2 bb[4] = {make_float2(b0.x, b1.x), make_float2(b0.y, b1.y), make_float2(b0.z, b1.z),
                                       make_float2(b0.w, b1.w)};
 #pragma unroll
@@ -369,8 +370,8 @@ __global__ void __launch_bounds__(VWPB * 32) project_voxels_kernel(ProjArgs a, i
                 }
                 if constexpr (!RB) {
                     // conj(b) x: Re += bi xi, Im -= bi xr
-                    const float4 c0v = *reinterpret_cast<const float4 *>(&sbi[warp][2 * q][t4]);
-                    const float4 c1v = *reinterpret_cast<const float4 *>(&sbi[warp][2 * q + 1][t4]);
+                    const float4 c0v = *reinterpret_cast<const float4 *>(&sm.bi[warp][2 * q][t4]);
+                    const float4 c1v = *reinterpret_cast<const float4 *>(&sm.bi[warp][2 * q + 1][t4]);
                     const float2 cc[4] = {make_float2(c0v.x, c1v.x), make_float2(c0v.y, c1v.y),
                                           make_float2(c0v.z, c1v.z), make_float2(c0v.w, c1v.w)};
 #pragma unroll
@@ -382,21 +383,36 @@ __global__ void __launch_bounds__(VWPB * 32) project_voxels_kernel(ProjArgs a, i
             }
         }
         __syncwarp();
-#pragma unroll
-        for (int j = 0; j < VKC / 2; j++) {
-            sr[2 * j] += ar[j].x;
-            sr[2 * j + 1] += ar[j].y;
-            si[2 * j] += ai[j].x;
-            si[2 * j + 1] += ai[j].y;
-            ar[j] = ai[j] = make_float2(0.f, 0.f);
-        }
     }
-    if (row < 0) return;
-    float2 *out = static_cast<float2 *>(a.out) + row * a.out_stride;
+    // the warps' partial sums: [warp][voxel][column] in the x buffers
+    __syncthreads();
+    float2 *red = reinterpret_cast<float2 *>(&sm.xr[0][0][0]);  // VTS * PT * VKC float2 fit in xr + xi
 #pragma unroll
-    for (int c = 0; c < VKC; c++)
-        if (c0 + c < a.k) out[c0 + c] = make_float2((float)sr[c], (float)si[c]);
+    for (int j = 0; j < VKC / 2; j++) {
+        red[(warp * PT + lane) * VKC + 2 * j] = make_float2(ar[j].x, ai[j].x);
+        red[(warp * PT + lane) * VKC + 2 * j + 1] = make_float2(ar[j].y, ai[j].y);
+    }
+    __syncthreads();
+    const long long vrow = __shfl_sync(0xffffffffu, row, lane);
+    if (vrow < 0) return;
+    // warp w adds columns [w * VKC / VTS, (w + 1) * VKC / VTS) over the warps
+    float2 *out = static_cast<float2 *>(a.out) + vrow * a.out_stride;
+#pragma unroll
+    for (int cc = 0; cc < VKC / VTS; cc++) {
+        const int c = warp * (VKC / VTS) + cc;
+        if (c0 + c >= a.k) continue;
+        float sr = 0.f, si = 0.f;
+#pragma unroll
+        for (int w = 0; w < VTS; w++) {
+            const float2 v = red[(w * PT + lane) * VKC + c];
+            sr += v.x;
+            si += v.y;
+        }
+        out[c0 + c] = make_float2(sr, si);
+    }
 }
+static_assert(sizeof(float) * 2 * VTS * PT * (PT + 1) >= sizeof(float2) * VTS * PT * VKC,
+              "the partial sums fit in the sample buffers");
 
 // ---- Y = D Z: partial sums over a split of each block's atoms ---------------
 struct RangeArgs {
@@ -944,10 +960,12 @@ int project_voxels(float2 *out, long long out_stride, const float2 *img, long lo
         a.nbins = nbins;
         ntiles = (nvox + PT - 1) / PT + nbins;  // upper bound on the tiles
     }
-    const unsigned grid = nblk(ntiles, VWPB);
+    const size_t vsm = sizeof(VoxSmem);
+    SNAPMRF_CUDA(allow_smem(project_voxels_kernel<true>, vsm));
+    SNAPMRF_CUDA(allow_smem(project_voxels_kernel<false>, vsm));
     for (int c0 = 0; c0 < rank; c0 += VKC) {
-        if (real_basis) project_voxels_kernel<true><<<grid, VWPB * 32, 0, st>>>(a, c0, ntiles);
-        else project_voxels_kernel<false><<<grid, VWPB * 32, 0, st>>>(a, c0, ntiles);
+        if (real_basis) project_voxels_kernel<true><<<(unsigned)ntiles, VTS * 32, vsm, st>>>(a, c0);
+        else project_voxels_kernel<false><<<(unsigned)ntiles, VTS * 32, vsm, st>>>(a, c0);
         SNAPMRF_LAUNCH_CHECK();
     }
     return SNAPMRF_OK;
