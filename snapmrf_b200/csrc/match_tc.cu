@@ -306,10 +306,15 @@ match_bf16_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
                     float mx = sc[0];
 #pragma unroll
                     for (int j = 1; j < 16; j++) mx = fmaxf(mx, sc[j]);
-                    if (mx > ts[TOPK - 1]) {
+                    // IMAG: the lane pair keeps two lists of one voxel; each
+                    // list's k-th best bounds the voxel's k-th best from
+                    // below, so a score must beat the larger of the two
+                    float thr = ts[TOPK - 1];
+                    if (IMAG) thr = fmaxf(thr, __shfl_xor_sync(0xffffffffu, thr, 1));
+                    if (mx > thr) {
 #pragma unroll
                         for (int j = 0; j < 16; j++)
-                            if (sc[j] > ts[TOPK - 1] && (full_tile || a0 + j < p.bin_natoms))
+                            if (sc[j] > fmaxf(thr, ts[TOPK - 1]) && (full_tile || a0 + j < p.bin_natoms))
                                 topk_insert<TOPK>(ts, ti, sc[j], a0 + j);
                     }
                 }
