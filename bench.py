@@ -553,7 +553,7 @@ def run_ours(args) -> None:
 
     # max over ranks
     def topk_of(form):
-        return args.topk or (8 if form == "fp16" else 16)
+        return args.topk or (4 if form == "fp16" else 16)
 
     names = list(PRECS)
     gnames = list(gn_forms)
@@ -750,7 +750,7 @@ def main() -> None:
                     help="approximate CPU seconds of the bounded CPU sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
-    ap.add_argument("--topk", type=int, default=0, choices=[0, 8, 16],
+    ap.add_argument("--topk", type=int, default=0, choices=[0, 4, 8, 16],
                     help="tensor-core forms: candidates rescored in FP32 (0: library default, "
                          "16 for BF16, 8 for FP16)")
     ap.add_argument("--b1-blocks", type=int, default=41,

@@ -181,8 +181,8 @@ int snapmrf_normalize(float *d_atoms, size_t nreps, size_t NATOMS, float *d_norm
  * ---------------------------------------------------------------------- */
 #define SNAPMRF_PREC_FP32 0  /* FP32 scores (the reference's cublasCgemm form) */
 /* BF16 scores on the tensor cores (FP32 accumulation, each voxel scaled to
- * unit norm first), a per-voxel top-k (snapmrf_match_opts.topk, 8 or 16;
- * 16 by default for BF16, 8 for FP16),
+ * unit norm first), a per-voxel top-k (snapmrf_match_opts.topk, 4, 8 or 16;
+ * 16 by default for BF16, 4 for FP16),
  * then exact FP32 rescoring of those k atoms: the map is the FP32 first
  * argmax among them.  Needs B1 blocks holding one B1 value each when a B1
  * map is given. */
@@ -215,7 +215,7 @@ typedef struct snapmrf_match_opts {
     const float *b1map;     /* optional [nvoxels] B1 map: match within the nearest B1 block */
     int b1map_on_host;      /* b1map is host memory */
     int64_t *d_index;       /* optional out [nvoxels]: chosen global atom index */
-    int topk;               /* tensor-core forms: candidates rescored in FP32, 8 or 16 (0: default) */
+    int topk;               /* tensor-core forms: candidates rescored in FP32, 4, 8 or 16 (0: default) */
     /* Optional: the atoms packed by snapmrf_mrf_dict (snapmrf_dict_opts.d_packed)
      * in this call's precision (BF16 or FP16) for these same nreps
      * (packed_nreps == nreps); needs SNAPMRF_MATCH_IMAG_ATOMS.  The FP32

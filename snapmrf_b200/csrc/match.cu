@@ -278,9 +278,9 @@ extern "C" int snapmrf_mrf_match(float *d_maps, const float *img, int img_on_hos
         q.coeffs = comp ? reinterpret_cast<const float2 *>(opts->coeffs) : nullptr;
         q.coeff_stride = comp ? (long long)opts->coeff_stride : 0;
         q.rank = comp ? opts->rank : 0;
-        q.topk = (opts && opts->topk) ? opts->topk : (q.fmt == 1 ? 8 : 16);
-        if (q.topk != 8 && q.topk != 16)
-            SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "MRF_match: topk must be 8 or 16 (got %d)", q.topk);
+        q.topk = (opts && opts->topk) ? opts->topk : (q.fmt == 1 ? 4 : 16);
+        if (q.topk != 4 && q.topk != 8 && q.topk != 16)
+            SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "MRF_match: topk must be 4, 8 or 16 (got %d)", q.topk);
         return match_bf16(q, st);
     }
     int nbins;

@@ -969,9 +969,13 @@ int match_bf16(const TcMatchRequest &q, cudaStream_t st) {
     int num_sms = 0, dev = 0;
     SNAPMRF_CUDA(cudaGetDevice(&dev));
     SNAPMRF_CUDA(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev));
-    auto kern = fp8    ? (q.topk > 8 ? match_bf16_kernel<16, true, false> : match_bf16_kernel<8, true, false>)
-                : imag ? (q.topk > 8 ? match_bf16_kernel<16, false, true> : match_bf16_kernel<8, false, true>)
-                       : (q.topk > 8 ? match_bf16_kernel<16, false, false> : match_bf16_kernel<8, false, false>);
+    auto pick = [&](auto k16, auto k8, auto k4) { return q.topk > 8 ? k16 : q.topk > 4 ? k8 : k4; };
+    auto kern = fp8    ? pick(match_bf16_kernel<16, true, false>, match_bf16_kernel<8, true, false>,
+                              match_bf16_kernel<4, true, false>)
+                : imag ? pick(match_bf16_kernel<16, false, true>, match_bf16_kernel<8, false, true>,
+                              match_bf16_kernel<4, false, true>)
+                       : pick(match_bf16_kernel<16, false, false>, match_bf16_kernel<8, false, false>,
+                              match_bf16_kernel<4, false, false>);
     SNAPMRF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
     Args a;
     a.tile_start = tile_start;
@@ -1007,8 +1011,8 @@ int match_bf16(const TcMatchRequest &q, cudaStream_t st) {
     const long long rn = rfull ? q.nreps : q.rank;
     const bool vec = rn % 2 == 0 && ras % 2 == 0 && ris % 2 == 0 && reinterpret_cast<uintptr_t>(ratoms) % 16 == 0 &&
                      reinterpret_cast<uintptr_t>(rimg) % 16 == 0;
-    auto rk = q.topk > 8 ? (vec ? rescore_kernel<16, true> : rescore_kernel<16, false>)
-                         : (vec ? rescore_kernel<8, true> : rescore_kernel<8, false>);
+    auto rk = vec ? pick(rescore_kernel<16, true>, rescore_kernel<8, true>, rescore_kernel<4, true>)
+                  : pick(rescore_kernel<16, false>, rescore_kernel<8, false>, rescore_kernel<4, false>);
     rk<<<nblk(cap * 32, 256), 256, 0, st>>>(q.maps, q.index_out, top_s, top_i, perm, tile_start, nbins,
                                             q.b1map ? vox_bin : nullptr, ratoms, ras, rimg, ris, rn, q.params,
                                             q.nparams, bin_natoms, err);

@@ -53,7 +53,7 @@ static void usage() {
             "\t-T, --nreps, --timepoints n\t number of time points\n"
             "\t-G, --gridsize n, -B, --blocksize n  accepted, unused\n"
             "\t    --precision fp32|bf16|fp16|fp8 matching form (default fp32)\n"
-            "\t    --topk 8|16\t\t\t candidates rescored in FP32 (tensor-core forms)\n"
+            "\t    --topk 4|8|16\t\t candidates rescored in FP32 (tensor-core forms)\n"
             "\t    --all-b1-blocks\t\t generate every B1 block for non-SSFP echo types\n"
             "\t    --normalize\t\t\t unit-norm every atom\n"
             "\t    --load-atoms <rafile>\t match against a saved dictionary (with --load-params)\n"
