@@ -121,7 +121,7 @@ static cudaError_t launch_epg_real(const EpgArgs &a, dim3 grid, cudaStream_t st)
     auto k = epg_real_kernel<ECHO, S, TAIL, FOLD>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    k<<<grid, kEpgThreads, smem, st>>>(a);
+    k<<<grid, kRealThreads, smem, st>>>(a);
     note_launches(1);
     return cudaGetLastError();
 }
@@ -315,7 +315,7 @@ extern "C" int snapmrf_mrf_dict(float *d_atoms, const float *d_params, const flo
     else
         choose_layout(nstates, kMaxStatesPerLane, 1, &L, &S);
     a.L = L;
-    const int apc = kEpgThreads / L;
+    const int apc = (real_path ? kRealThreads : kEpgThreads) / L;
     dim3 grid((unsigned)((natoms + apc - 1) / apc), (unsigned)gen_blocks);
     if (grid.x > 0x7fffffffu) SNAPMRF_FAIL(SNAPMRF_ERR_UNSUPPORTED, "MRF_dict: grid too large");
     if (real_path) {

@@ -451,11 +451,22 @@ __device__ __forceinline__ void rl2_shift(RealLane2<P> &s, int gl, int L, int w,
 // The real-valued kernel stages 32 steps per chunk (half the barriers of 16;
 // its per-step shared data is small).
 constexpr int kRealChunk = 32;
+// Threads per CTA of the real-valued kernel: one warp.  Its occupancy is
+// fixed by registers (12 warps per SM), so a dictionary fills a whole number
+// of waves plus a fraction, and the last wave runs nearly empty for one
+// CTA's duration, which shrinks with the CTA (C1: 7.82 ms with 128 threads,
+// 7.79 with 64, 7.63 with 32; the atoms are bit-identical).
+// SNAPMRF_EPG_REAL_THREADS overrides it for tuning (a multiple of 32).
+#ifndef SNAPMRF_EPG_REAL_THREADS
+#define SNAPMRF_EPG_REAL_THREADS 32
+#endif
+constexpr int kRealThreads = SNAPMRF_EPG_REAL_THREADS;
+static_assert(kRealThreads % 32 == 0, "whole warps");
 constexpr int kRealFS = kRealChunk * 4 + 4;          // floats per atom of relaxation factors
 constexpr int kRealReadoutStride = kRealChunk + 1;  // float2 per group
 
 inline size_t epg_real_smem_bytes(int L) {
-    int apc = kEpgThreads / L;
+    int apc = kRealThreads / L;
     return (size_t)kRealChunk * 10 * sizeof(float2) + (size_t)apc * kRealFS * sizeof(float) +
            (size_t)apc * kRealReadoutStride * sizeof(float2) + (size_t)apc * 4 * sizeof(float);
 }
@@ -463,9 +474,9 @@ inline size_t epg_real_smem_bytes(int L) {
 // (An explicit minimum of 1 block per SM lets ptxas use more registers and
 // costs a resident block per SM; SNAPMRF_EPG_REAL_MIN_BLOCKS is for tuning.)
 #ifdef SNAPMRF_EPG_REAL_MIN_BLOCKS
-#define SNAPMRF_EPG_REAL_BOUNDS __launch_bounds__(kEpgThreads, SNAPMRF_EPG_REAL_MIN_BLOCKS)
+#define SNAPMRF_EPG_REAL_BOUNDS __launch_bounds__(kRealThreads, SNAPMRF_EPG_REAL_MIN_BLOCKS)
 #else
-#define SNAPMRF_EPG_REAL_BOUNDS __launch_bounds__(kEpgThreads)
+#define SNAPMRF_EPG_REAL_BOUNDS __launch_bounds__(kRealThreads)
 #endif
 
 // One element of the optional 16-bit copy of Im(atom) (the tensor-core
@@ -491,7 +502,7 @@ __global__ void SNAPMRF_EPG_REAL_BOUNDS epg_real_kernel(EpgArgs a) {
     constexpr int NF = 4;
     constexpr int FS = kRealFS;
     const int L = a.L;
-    const int apc = kEpgThreads / L;
+    const int apc = kRealThreads / L;
     const int tid = threadIdx.x;
     const int g = tid / L;
     const int gl = tid % L;
@@ -508,7 +519,7 @@ __global__ void SNAPMRF_EPG_REAL_BOUNDS epg_real_kernel(EpgArgs a) {
     float2 *sR = reinterpret_cast<float2 *>(sF + apc * FS);    // [apc][kRealReadoutStride]
     float *sP = reinterpret_cast<float *>(sR + apc * kRealReadoutStride);
 
-    for (int i = tid; i < apc; i += kEpgThreads) {
+    for (int i = tid; i < apc; i += kRealThreads) {
         long long at = atom0 + i;
         float t1 = 1.f, t2 = 1.f;
         if (at < a.natoms) {
@@ -555,8 +566,8 @@ __global__ void SNAPMRF_EPG_REAL_BOUNDS epg_real_kernel(EpgArgs a) {
     for (long long t0 = 0; t0 < nreps; t0 += kRealChunk) {
         const int nch = (int)min((long long)kRealChunk, nreps - t0);
         __syncthreads();
-        for (int i = tid; i < nch; i += kEpgThreads) rf_real_coeffs2(alpha[t0 + i], phi[t0 + i], sC + 10 * i);
-        for (int idx = tid; idx < apc * nch; idx += kEpgThreads) {
+        for (int i = tid; i < nch; i += kRealThreads) rf_real_coeffs2(alpha[t0 + i], phi[t0 + i], sC + 10 * i);
+        for (int idx = tid; idx < apc * nch; idx += kRealThreads) {
             int ga = idx / nch, i = idx - ga * nch;
             float t1 = sP[4 * ga], t2 = sP[4 * ga + 1];
             float4 f;
