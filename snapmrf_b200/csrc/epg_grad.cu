@@ -33,6 +33,15 @@ namespace snapmrf {
 namespace grad {
 
 constexpr int kThreads = 128;
+// Threads per CTA of gn_kernel: one warp.  Its occupancy is fixed by
+// registers (8 warps per SM), so a pass fills whole waves plus a fraction,
+// and the last wave runs nearly empty for one CTA's duration, which shrinks
+// with the CTA.  SNAPMRF_GN_THREADS overrides it for tuning.
+#ifndef SNAPMRF_GN_THREADS
+#define SNAPMRF_GN_THREADS 32
+#endif
+constexpr int kGnThreads = SNAPMRF_GN_THREADS;
+static_assert(kGnThreads % 32 == 0, "whole warps");
 constexpr int kMaxS = 8;
 
 struct Schedule {
@@ -433,12 +442,12 @@ constexpr int kGnChunk = 16;
 
 // One Gauss-Newton iteration per voxel (TANGENTS) or, without tangents, the
 // final evaluation of PD and M0 at the current parameters.  L lanes per
-// voxel; a block of kThreads handles kThreads / L voxels in lockstep over
+// voxel; a block of kGnThreads handles kGnThreads / L voxels in lockstep over
 // chunks of `chunk` steps.
 template <int P, bool TANGENTS>
-__global__ void __launch_bounds__(kThreads) gn_kernel(GnArgs a, int chunk) {
+__global__ void __launch_bounds__(kGnThreads) gn_kernel(GnArgs a, int chunk) {
     extern __shared__ __align__(16) unsigned char gn_smem[];
-    const int L = a.L, apc = kThreads / L;
+    const int L = a.L, apc = kGnThreads / L;
     const int tid = threadIdx.x, g = tid / L, gl = tid % L;
     const bool lane0 = gl == 0;
     GnStep *sQ = reinterpret_cast<GnStep *>(gn_smem);              // [apc][chunk]
@@ -446,7 +455,7 @@ __global__ void __launch_bounds__(kThreads) gn_kernel(GnArgs a, int chunk) {
     long long *sI = reinterpret_cast<long long *>(sV + apc * 4);  // [apc]: voxel or -1
     const long long vox0 = (long long)blockIdx.x * apc;
     const long long nlist = a.list_in ? (long long)*a.count_in : a.nvox;
-    for (int i = tid; i < apc; i += kThreads) {
+    for (int i = tid; i < apc; i += kGnThreads) {
         const long long slot = vox0 + i;
         long long v = -1;
         if (slot < nlist) v = a.list_in ? (long long)a.list_in[slot] : slot;
@@ -493,7 +502,7 @@ __global__ void __launch_bounds__(kThreads) gn_kernel(GnArgs a, int chunk) {
     for (int t0 = 0; t0 < T; t0 += chunk) {
         const int nch = min(chunk, T - t0);
         __syncthreads();
-        for (int idx = tid; idx < apc * nch; idx += kThreads) {
+        for (int idx = tid; idx < apc * nch; idx += kGnThreads) {
             const int ga = idx / nch, i = idx - ga * nch;
             const float T1 = sV[4 * ga], T2 = sV[4 * ga + 1], B1 = sV[4 * ga + 2];
             const int t = t0 + i;
@@ -992,13 +1001,13 @@ static void choose(int w, int *L, int *S) {
 
 #define SNAPMRF_GN_DISPATCH(P, B, GRID, SMEM, ST, ARGS, CHUNK)                      \
     switch (P) {                                                                    \
-    case 1: gn_kernel<1, B><<<GRID, kThreads, SMEM, ST>>>(ARGS, CHUNK); break;      \
-    case 2: gn_kernel<2, B><<<GRID, kThreads, SMEM, ST>>>(ARGS, CHUNK); break;      \
-    case 3: gn_kernel<3, B><<<GRID, kThreads, SMEM, ST>>>(ARGS, CHUNK); break;      \
-    case 4: gn_kernel<4, B><<<GRID, kThreads, SMEM, ST>>>(ARGS, CHUNK); break;      \
-    case 5: gn_kernel<5, B><<<GRID, kThreads, SMEM, ST>>>(ARGS, CHUNK); break;      \
-    case 6: gn_kernel<6, B><<<GRID, kThreads, SMEM, ST>>>(ARGS, CHUNK); break;      \
-    default: gn_kernel<7, B><<<GRID, kThreads, SMEM, ST>>>(ARGS, CHUNK); break;     \
+    case 1: gn_kernel<1, B><<<GRID, kGnThreads, SMEM, ST>>>(ARGS, CHUNK); break;      \
+    case 2: gn_kernel<2, B><<<GRID, kGnThreads, SMEM, ST>>>(ARGS, CHUNK); break;      \
+    case 3: gn_kernel<3, B><<<GRID, kGnThreads, SMEM, ST>>>(ARGS, CHUNK); break;      \
+    case 4: gn_kernel<4, B><<<GRID, kGnThreads, SMEM, ST>>>(ARGS, CHUNK); break;      \
+    case 5: gn_kernel<5, B><<<GRID, kGnThreads, SMEM, ST>>>(ARGS, CHUNK); break;      \
+    case 6: gn_kernel<6, B><<<GRID, kGnThreads, SMEM, ST>>>(ARGS, CHUNK); break;      \
+    default: gn_kernel<7, B><<<GRID, kGnThreads, SMEM, ST>>>(ARGS, CHUNK); break;     \
     }
 
 // Schedule of the real-valued recursion on the device; fails unless every
@@ -1142,7 +1151,7 @@ extern "C" int snapmrf_refine_gn(float *d_maps, int nmaps, const float *img, siz
         cnt[0] = lst[1] + nvoxels;
         cnt[1] = cnt[0] + 1;
     }
-    const int apc = kThreads / L;
+    const int apc = kGnThreads / L;
     // steps staged per chunk: at most kGnChunk, within 48 KB of shared memory
     const size_t fixed = (size_t)apc * (4 * sizeof(float) + sizeof(long long));
     const int chunk = (int)std::min<size_t>(kGnChunk, (48 * 1024 - fixed) / ((size_t)apc * sizeof(GnStep)));
