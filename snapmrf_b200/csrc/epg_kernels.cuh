@@ -451,11 +451,10 @@ __device__ __forceinline__ void rl2_shift(RealLane2<P> &s, int gl, int L, int w,
 // The real-valued kernel stages 32 steps per chunk (half the barriers of 16;
 // its per-step shared data is small).
 constexpr int kRealChunk = 32;
-// Threads per CTA of the real-valued kernel: one warp.  Its occupancy is
-// fixed by registers (12 warps per SM), so a dictionary fills a whole number
-// of waves plus a fraction, and the last wave runs nearly empty for one
-// CTA's duration, which shrinks with the CTA (C1: 7.82 ms with 128 threads,
-// 7.79 with 64, 7.63 with 32; the atoms are bit-identical).
+// Threads per CTA of the real-valued kernel: one warp, so that no CTA
+// barrier makes the warps of a CTA wait for each other at every chunk (C1:
+// 7.82 ms with 128 threads, 7.79 with 64, 7.63 with 32; the atoms are
+// bit-identical).
 // SNAPMRF_EPG_REAL_THREADS overrides it for tuning (a multiple of 32).
 #ifndef SNAPMRF_EPG_REAL_THREADS
 #define SNAPMRF_EPG_REAL_THREADS 32
