@@ -108,7 +108,7 @@ struct ProjArgs {
     const float2 *x;            // rows [*][x_stride] complex
     long long x_stride;
     long long rows_per_block;   // contiguous mode: rows b * rpb + [0, rpb), grid.y = block
-    const long long *perm;      // binned mode (non-null): slot -> row (voxel)
+    const long long *perm;      // binned mode (voxel projection, non-null): slot -> row
     const long long *tile_start;  // [nbins + 1] first PT-slot tile of each bin
     const long long *slot_start;  // [nbins + 1] first slot of each bin
     int nbins;
@@ -125,31 +125,19 @@ struct ProjArgs {
 // MODE 0: complex basis and rows; 1: real basis, complex rows; 2: real
 // basis, purely imaginary rows d = i v: the value sum_t u_c[t] v[t] (real),
 // written as a float (OUTF2 false) or as the complex (0, value).
-// A CTA takes PT rows of one bin; lane = row, warp w the columns w + NW j.
+// A CTA takes PT rows of one B1 block (rows b * rows_per_block + [0,
+// rows_per_block), grid.y = b); lane = row, warp w the columns w + NW j.
 template <int MODE, bool OUTF2>
 __global__ void __launch_bounds__(THREADS) project_kernel(ProjArgs a) {
     __shared__ float sxr[PT][PT + 1], sxi[PT][PT + 1];
     __shared__ float sbr[KMAX][PT + 1], sbi[MODE == 0 ? KMAX : 1][PT + 1];
     __shared__ long long srow[PT], slocal[PT];
     const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
-    long long bin;
-    if (a.perm) {
-        const long long g = blockIdx.x;
-        if (g >= a.tile_start[a.nbins]) return;  // uniform per CTA
-        const int b = find_bin(a.tile_start, a.nbins, g);
-        bin = b;
-        if (threadIdx.x < PT) {
-            const long long sl = a.slot_start[b] + (g - a.tile_start[b]) * PT + threadIdx.x;
-            srow[threadIdx.x] = sl < a.slot_start[b + 1] ? a.perm[sl] : -1;
-            slocal[threadIdx.x] = -1;
-        }
-    } else {
-        bin = blockIdx.y;
-        if (threadIdx.x < PT) {
-            const long long l = (long long)blockIdx.x * PT + threadIdx.x;
-            srow[threadIdx.x] = l < a.rows_per_block ? bin * a.rows_per_block + l : -1;
-            slocal[threadIdx.x] = l;
-        }
+    const long long bin = blockIdx.y;
+    if (threadIdx.x < PT) {
+        const long long l = (long long)blockIdx.x * PT + threadIdx.x;
+        srow[threadIdx.x] = l < a.rows_per_block ? bin * a.rows_per_block + l : -1;
+        slocal[threadIdx.x] = l;
     }
     __syncthreads();
     const float2 *B = a.basis + bin * a.basis_rows * a.basis_stride;
