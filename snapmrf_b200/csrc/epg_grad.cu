@@ -393,15 +393,20 @@ __device__ __forceinline__ void pz(Pair3<P> &x) {
     for (int i = 0; i < P; i++) x.p[i] = x.m[i] = x.z[i] = make_float2(0.f, 0.f);
 }
 
+// RF pulse on one packed stream: F+' = c F+ + s F- - S Z, F-' = s F+ + c F-
+// + S Z, Z' = hS (F+ - F-) + C Z (hS = S / 2 with its sign), computed as
+// F-' = (c + s)(F+ + F-) - F+': 8 packed operations per pair instead of 9.
 template <int P>
-__device__ __forceinline__ void p_rf(Pair3<P> &x, float2 c, float2 s, float2 S, float2 nS, float2 hS,
-                                     float2 nhS, float2 C) {
+__device__ __forceinline__ void p_rf(Pair3<P> &x, float2 c, float2 s, float2 nS, float2 hS, float2 C) {
+    const float2 cs = __fadd2_rn(c, s);
 #pragma unroll
     for (int i = 0; i < P; i++) {
         const float2 p = x.p[i], m = x.m[i], q = x.z[i];
-        x.p[i] = __ffma2_rn(nS, q, __ffma2_rn(s, m, __fmul2_rn(c, p)));
-        x.m[i] = __ffma2_rn(S, q, __ffma2_rn(c, m, __fmul2_rn(s, p)));
-        x.z[i] = __ffma2_rn(C, q, __ffma2_rn(nhS, m, __fmul2_rn(hS, p)));
+        const float2 np = __ffma2_rn(nS, q, __ffma2_rn(s, m, __fmul2_rn(c, p)));
+        const float2 d = __fadd2_rn(p, make_float2(-m.x, -m.y));
+        x.z[i] = __ffma2_rn(C, q, __fmul2_rn(hS, d));
+        x.m[i] = __ffma2_rn(cs, p, __ffma2_rn(cs, m, make_float2(-np.x, -np.y)));
+        x.p[i] = np;
     }
 }
 
@@ -528,13 +533,12 @@ __global__ void __launch_bounds__(kGnThreads) gn_kernel(GnArgs a, int chunk) {
         for (int i = 0; i < nch; i++) {
             const GnStep q = qs[i];
             const float cc = (1 + q.C) / 2, ss = (1 - q.C) / 2, hS = 0.5f * q.S;
-            const float2 kc = make_float2(cc, cc), ks = make_float2(ss, ss), kS = make_float2(q.S, q.S),
-                         knS = make_float2(-q.S, -q.S), khS = make_float2(hS, hS), knhS = make_float2(-hS, -hS),
-                         kC = make_float2(q.C, q.C);
-            p_rf<P>(sv, kc, ks, kS, knS, khS, knhS, kC);
+            const float2 kc = make_float2(cc, cc), ks = make_float2(ss, ss), knS = make_float2(-q.S, -q.S),
+                         khS = make_float2(hS, hS), kC = make_float2(q.C, q.C);
+            p_rf<P>(sv, kc, ks, knS, khS, kC);
             if (TANGENTS) {
-                p_rf<P>(s1, kc, ks, kS, knS, khS, knhS, kC);
-                p_rf<P>(s2, kc, ks, kS, knS, khS, knhS, kC);
+                p_rf<P>(s1, kc, ks, knS, khS, kC);
+                p_rf<P>(s2, kc, ks, knS, khS, kC);
             }
             if (lane0) {
                 // readout s_t = i Ea f+[0] (relaxation over TE)

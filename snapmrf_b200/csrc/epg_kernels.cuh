@@ -393,6 +393,32 @@ __device__ __forceinline__ void rl2_rf_k(RealLane2<P> &s, float2 c0, float2 c1, 
     }
 }
 
+// The same RF with the structure of a phi = 0 pulse (c3 = c1, c4 = c0,
+// c5 = -c2, c7 = -c6, as rf_real_coeffs2 produces them and the folded
+// relaxation keeps them): F-' = (c0 + c1)(F+ + F-) - F+' and
+// Z' = c6 (F+ - F-) + c8 Z, 8 packed operations per pair instead of 9.  It
+// rounds differently from the reference's order (unit-norm C1 atoms move by
+// at most 6e-8) and is used by the folded recursion only.
+template <int P>
+__device__ __forceinline__ void rl2_rf_k8(RealLane2<P> &s, float2 c0, float2 c1, float2 c2, float2 c6, float2 c8) {
+    const float2 cs = __fadd2_rn(c0, c1);
+#pragma unroll
+    for (int i = 0; i < P; i++) {
+        const float2 p = s.fp[i], m = s.fm[i], z = s.zz[i];
+        float2 np = __fmul2_rn(c0, p);
+        np = __ffma2_rn(c1, m, np);
+        np = __ffma2_rn(c2, z, np);
+        const float2 d = __fadd2_rn(p, make_float2(-m.x, -m.y));
+        float2 nz = __fmul2_rn(c6, d);
+        nz = __ffma2_rn(c8, z, nz);
+        float2 nm = __ffma2_rn(cs, m, make_float2(-np.x, -np.y));
+        nm = __ffma2_rn(cs, p, nm);
+        s.fp[i] = np;
+        s.fm[i] = nm;
+        s.zz[i] = nz;
+    }
+}
+
 template <int P>
 __device__ __forceinline__ void rl2_rf(RealLane2<P> &s, const float2 *c) {
     rl2_rf_k<P>(s, c[0], c[1], c[2], c[3], c[4], c[5], c[6], c[7], c[8]);
@@ -593,9 +619,8 @@ __global__ void SNAPMRF_EPG_REAL_BOUNDS epg_real_kernel(EpgArgs a) {
             if (FOLD) {
                 const float2 *c = sC + 10 * i;
                 const float2 e1 = make_float2(f.x, f.x), e2 = make_float2(f.y, f.y);
-                rl2_rf_k<P>(s, __fmul2_rn(c[0], e2), __fmul2_rn(c[1], e2), __fmul2_rn(c[2], e1),
-                            __fmul2_rn(c[3], e2), __fmul2_rn(c[4], e2), __fmul2_rn(c[5], e1),
-                            __fmul2_rn(c[6], e2), __fmul2_rn(c[7], e2), __fmul2_rn(c[8], e1));
+                rl2_rf_k8<P>(s, __fmul2_rn(c[0], e2), __fmul2_rn(c[1], e2), __fmul2_rn(c[2], e1),
+                             __fmul2_rn(c[6], e2), __fmul2_rn(c[8], e1));
                 if (lane0) {
                     // the recovery term (1 - E1) of Z0 through the RF's Z column
                     s.fp[0].x = fmaf(c[2].x, f.w, s.fp[0].x);
