@@ -500,6 +500,8 @@ inline size_t epg_real_smem_bytes(int L) {
 // costs a resident block per SM; SNAPMRF_EPG_REAL_MIN_BLOCKS is for tuning.)
 #ifdef SNAPMRF_EPG_REAL_MIN_BLOCKS
 #define SNAPMRF_EPG_REAL_BOUNDS __launch_bounds__(kRealThreads, SNAPMRF_EPG_REAL_MIN_BLOCKS)
+#elif defined(SNAPMRF_EPG_REAL_MAXNREG)
+#define SNAPMRF_EPG_REAL_BOUNDS __maxnreg__(SNAPMRF_EPG_REAL_MAXNREG)
 #else
 #define SNAPMRF_EPG_REAL_BOUNDS __launch_bounds__(kRealThreads)
 #endif
