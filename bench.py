@@ -61,9 +61,9 @@ FLOP_PER_STATE_STEP = 66
 FLOP_PER_STATE_STEP_EXECUTED = 16
 # DRAM bytes per dictionary atom (T = 1000, w = 50, normalised, writing the
 # FP16 matching operand too) measured by ncu on the reduced workload (5 B1
-# blocks, 34,690 atoms: 184.2 MB read + 489.3 MB written in one launch);
+# blocks, 34,690 atoms: 194.7 MB read + 488.3 MB written in one launch);
 # traffic grows with the atom count, so a full launch moves this times NATOMS.
-DICT_DRAM_BYTES_PER_ATOM = (184.247296e6 + 489.294848e6) / 34690
+DICT_DRAM_BYTES_PER_ATOM = (194.683648e6 + 488.295936e6) / 34690
 PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
 
 
