@@ -257,3 +257,20 @@ def test_compressed_match_errors(snap):
         snap.MRF_match(d_maps, img, d, d_params, 120, 120, atoms.shape[0], natoms, 100, in_b1map=b1,
                        precision=2, flags=snap.MATCH_IMAG_ATOMS, packed_atoms=packed, compressed=c)
     assert e.value.status == ERR_INVALID
+
+
+def test_svd_blocks_smaller_than_subspace(snap, oracle_mod):
+    """Blocks of 6 atoms with a subspace of 16 vectors (and 40 samples): the
+    Gram matrices are rank-deficient, the directions beyond 6 drop out, and a
+    fixed rank of 4 still matches LAPACK."""
+    torch = torch_cuda()
+    rng = np.random.default_rng(21)
+    T, natoms, nb = 40, 6, 3
+    atoms = rng.standard_normal((nb * natoms, T)) + 1j * rng.standard_normal((nb * natoms, T))
+    atoms = (atoms / np.linalg.norm(atoms, axis=1, keepdims=True)).astype(np.complex64)
+    c, _, basis, coeffs = _compress(snap, atoms, natoms, rank=4, max_rank=8)
+    assert c.rank == 4
+    ref_basis, _, _, ref_sv = oracle_mod.svd_compress(atoms, natoms, rank=4)
+    assert np.all(np.isfinite(basis)) and np.all(np.isfinite(coeffs))
+    np.testing.assert_allclose(c.sv[:, 6:], 0.0, atol=1e-3)
+    _check_basis(atoms, natoms, c, basis, coeffs, ref_basis, ref_sv)
