@@ -86,3 +86,87 @@ def test_reference_arm_under_torchrun_prints_one_line():
     assert d["impl"] == "reference" and d["n_gpus"] == 2
     assert d["value"] > 0 and d["e2e"]["h2d_bytes_per_step"] == 0
     assert d["cpu_baseline"]["kind"] == "port"
+
+
+def _shard_maps(r, nvox=64):
+    """Synthetic per-shard matching results (shard r of 2) with ties built in:
+    the B1 values of the shard's blocks, PDs that repeat across shards."""
+    rng = np.random.default_rng(100 + r)
+    maps = np.zeros((nvox, 5), np.float32)
+    maps[:, 0] = rng.uniform(100, 3000, nvox)
+    maps[:, 1] = rng.uniform(10, 90, nvox)
+    maps[:, 3] = np.float32([0.8, 0.9][r]) + np.float32(0.1) * (np.arange(nvox) % 2)
+    maps[:, 4] = np.round(rng.uniform(0, 4, nvox)).astype(np.float32)   # few distinct values: ties
+    index = (r * 1000 + np.arange(nvox)).astype(np.int64)
+    return maps, index
+
+
+def _reference_merge(maps_list, index_list, b1):
+    """merge_maps restated (src/functions.cu:1351-1384): nearest B1 from an
+    initial 10 with strict '<', else the largest PD with strict '>'."""
+    nvox = maps_list[0].shape[0]
+    out = np.zeros_like(maps_list[0])
+    idx = np.zeros(nvox, np.int64)
+    for v in range(nvox):
+        k = 0
+        if b1 is not None:
+            best = np.float32(10.0)
+            for r, m in enumerate(maps_list):
+                d = np.float32(abs(np.float32(b1[v]) - m[v, 3]))
+                if d < best:
+                    best, k = d, r
+        else:
+            best = maps_list[0][v, 4]
+            for r, m in enumerate(maps_list[1:], start=1):
+                if m[v, 4] > best:
+                    best, k = m[v, 4], r
+        out[v] = maps_list[k][v]
+        idx[v] = index_list[k][v]
+    return out, idx
+
+
+def _b1_for(nvox=64):
+    b1 = np.linspace(0.7, 1.2, nvox).astype(np.float32)
+    b1[5] = np.nan
+    b1[6] = 50.0
+    b1[7] = np.float32(0.85)  # equidistant from 0.8 and 0.9 within rounding
+    return b1
+
+
+def _sharded_worker(rank, world, port, out_dir):
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    sys.path.insert(0, str(ROOT))
+    from snapmrf_b200 import sharded
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        m, i = _shard_maps(rank)
+        res = {}
+        for name, b1 in (("pd", None), ("b1", _b1_for())):
+            maps, index = sharded.exchange_and_merge(torch.from_numpy(m), torch.from_numpy(i),
+                                                     None if b1 is None else torch.from_numpy(b1))
+            res[name] = (maps.numpy().tolist(), index.numpy().tolist())
+        (Path(out_dir) / f"s{rank}.json").write_text(json.dumps(res))
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_sharded_merge_gloo(tmp_path):
+    """Two ranks, each with the matching results of its half of the B1
+    blocks: one all_gather and the reference's merge rule give every rank the
+    same maps, equal to merge_maps restated over both shards."""
+    import torch.multiprocessing as mp
+    port = _free_port()
+    mp.start_processes(_sharded_worker, args=(2, port, str(tmp_path)), nprocs=2, start_method="spawn")
+    shards = [_shard_maps(r) for r in range(2)]
+    for name, b1 in (("pd", None), ("b1", _b1_for())):
+        want_maps, want_idx = _reference_merge([s[0] for s in shards], [s[1] for s in shards], b1)
+        for r in range(2):
+            got_maps, got_idx = json.loads((tmp_path / f"s{r}.json").read_text())[name]
+            np.testing.assert_array_equal(np.array(got_maps, np.float32), want_maps)
+            np.testing.assert_array_equal(np.array(got_idx, np.int64), want_idx)
