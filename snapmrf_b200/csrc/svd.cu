@@ -19,17 +19,24 @@
 //     Z = D^H Q W L^-1/2             combine_kernel from P (orthonormal)
 //     Y = D Z                        range_kernel, a pass over the atoms
 //     Q = orth(Y)                    gram + jacobi + combine on Y (FP64)
-//   P = Q^H D, M = P P^H = W L W^H: Ritz values L ~ s^2, vectors U = Q W
+//   P = Q^H D in FP64, M = P P^H = W L W^H: Ritz values L ~ s^2, vectors
+//     U = Q W                        project64_kernel, a pass over the atoms
 //   C = U_r^H D                      project_kernel, a pass over the atoms
 //
 // orth(A) is the eigen-decomposition form of the Gram-matrix orthonormalisation:
 // A^H A = V S V^H (FP64 Jacobi), Q = A V S^-1/2, dropping directions with
 // S below 1e-12 of the largest (numerically absent: rank-deficient blocks,
 // nreps or natoms below k).  ||D_0||_F^2, the rank rule's denominator, is
-// summed over block 0's atoms in FP64.  The passes over the atoms read FP32
-// and accumulate in FP32 per 32-element chunk; every Gram, eigenproblem and
-// basis rotation is FP64.  All reductions have a fixed order: the result is
-// deterministic for a given seed.
+// summed over block 0's atoms in FP64.  The passes of the iteration read
+// FP32 and accumulate in FP32 per 32-element chunk, FP64 across chunks; the
+// Rayleigh-Ritz projection, every Gram, eigenproblem and basis rotation is
+// FP64, so the Ritz values the rank rule sums are exact for the computed
+// subspace.  All reductions have a fixed order: the result is deterministic
+// for a given seed.
+//
+// Compressed matching projects each voxel onto its bin's basis
+// (project_voxels_kernel; the scores and rescoring are in match_tc.cu and
+// match.cu).
 //
 // Purely imaginary atoms (SNAPMRF_SVD_IMAG_ATOMS) d = i v run the same
 // iteration in real arithmetic on v (REAL = true); then U is real and
