@@ -1,0 +1,59 @@
+"""The reference's own mrf, rebuilt for sm_100a from its sources
+(oracle/_ref/mrf_ref), against this package's mrf CLI on one C1-size B1 block
+on the same GPU: 6,659 atoms (-t 100:55:5000 -s 10:22:2000, epg_fisp, w = 50,
+T = 1000) and 240 x 240 noisy voxels, no B1 map.  Criteria: the same
+(T1, T2, B0, B1) on >= 99.9 % of the voxels, and this package's dictionary
+and matching (FP32, CUDA events, first-call costs and the image upload
+included) each faster than the reference's (its clock() times).  The
+timings are printed.  Skipped where oracle/_ref was not built."""
+import re
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+ROOT = Path(__file__).resolve().parent.parent
+REF = ROOT / "oracle" / "_ref" / "mrf_ref"
+CLI = ROOT / "snapmrf_b200" / "mrf"
+pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not REF.exists() or not CLI.exists(),
+                                                  reason="oracle/_ref/mrf_ref or the mrf CLI not built")]
+HEADER = "flip_angle_(fraction_of_nominal),rf_phase_(deg),extension_of_base_TR_(ms),extension_of_base_TE_(ms)"
+
+
+def _run(exe, args, cwd):
+    r = subprocess.run([str(exe), *args], cwd=cwd, stdin=subprocess.DEVNULL, capture_output=True, text=True,
+                       timeout=900)
+    assert r.returncode == 0, (exe.name, r.stdout[-1500:], r.stderr[-1500:])
+    return {k: float(v) for k, v in re.findall(r"Elapsed (dictionary|matching) time: ([0-9.eE+-]+)", r.stdout)}
+
+
+@pytest.mark.timeout(900)
+def test_mrf_faster_than_rebuilt_reference_same_maps(snap, tmp_path):
+    T = 1000
+    rng = np.random.default_rng(7)
+    sched = np.array([0.1 + 0.8 * np.abs(np.sin(np.pi * np.arange(T) / 250)), np.zeros(T),
+                      rng.uniform(-3, -1, T), rng.uniform(-1, 1, T)], np.float32)
+    rows = "\n".join(",".join(repr(float(v)) for v in sched[:, t]) for t in range(T))
+    (tmp_path / "sched.csv").write_text(HEADER + "\n" + rows + "\n")
+    grid = ["-e", "epg_fisp", "-t", "100:55:5000", "-s", "10:22:2000", "-b", "0", "-r", "1", "-w", "50",
+            "-T", str(T)]
+    _run(CLI, grid + ["sched.csv", "-a", "atoms.ra"], tmp_path)
+    atoms = snap.ra_read(str(tmp_path / "atoms.ra"))
+    assert atoms.shape == (6659, T)
+    nv = 240 * 240
+    pick = rng.integers(0, atoms.shape[0], nv)
+    img = atoms[pick] * (rng.uniform(0.5, 1, nv) * np.exp(1j * rng.uniform(0, 6.28, nv)))[:, None]
+    noise = 0.002 * np.abs(img).mean() * (rng.standard_normal(img.shape) + 1j * rng.standard_normal(img.shape))
+    snap.ra_write(str(tmp_path / "img.ra"), (img + noise).astype(np.complex64).reshape(240, 240, T))
+    del img, noise
+    ref = _run(REF, grid + ["sched.csv", "img.ra", "-m", "maps_ref.ra"], tmp_path)
+    ours = _run(CLI, grid + ["sched.csv", "img.ra", "-m", "maps_ours.ra"], tmp_path)
+    print(f"reference (rebuilt, clock()): {ref}; this package (CUDA events): {ours}")
+    mr = snap.ra_read(str(tmp_path / "maps_ref.ra")).reshape(-1, 5)
+    mo = snap.ra_read(str(tmp_path / "maps_ours.ra")).reshape(-1, 5)
+    same = np.mean(np.all(mr[:, :4] == mo[:, :4], axis=1))
+    print(f"same (T1, T2, B0, B1) on {same:.5f} of the voxels")
+    assert same >= 0.999
+    assert ours["dictionary"] < ref["dictionary"]
+    assert ours["matching"] < ref["matching"]
