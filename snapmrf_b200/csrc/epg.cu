@@ -12,6 +12,7 @@
 // steps, and the readout is staged in shared memory and written coalesced.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -115,15 +116,87 @@ static cudaError_t dispatch_states(const EpgArgs &a, int S, dim3 grid, cudaStrea
     }
 }
 
+// Fine-tail plan of the real-valued kernel.  A CTA carries its atoms through
+// every step whatever its layout, so a grid of C CTAs on R resident ones
+// takes ceil(C / R) rounds, and a last round holding only a few CTAs costs a
+// good part of a full one (C1, 41 B1 blocks x 434 CTAs on 1,776 resident:
+// the 41 CTAs past 10 rounds add 0.17 ms to 7.04).  When the CTAs past the
+// last whole round number at most the blocks (one partial CTA each), or the
+// whole grid is smaller than one round, each block's trailing atoms go to
+// the fine layout (kFineL lanes per atom, kFineP pairs of states per lane:
+// w <= 64), provided its CTAs number at most R / 2.  *bulk_cpb / *fine_cpb:
+// CTAs per block of the chosen and the fine layout (*fine_cpb = 0: no
+// split).  SNAPMRF_DICT_FINE_ATOMS = n forces n fine atoms per block (rounded
+// up to whole CTAs of the chosen layout; 0 turns the split off); an explicit
+// SNAPMRF_DICT_LAYOUT turns it off too.
+static void plan_fine_tail(const EpgArgs &a, int P, long long nblocks, const void *kernel, size_t smem,
+                           long long *bulk_cpb, long long *fine_cpb) {
+    const long long apc = kRealThreads / a.L, apc_f = kRealThreads / kFineL;
+    const long long n = a.natoms, B = nblocks;
+    *bulk_cpb = (n + apc - 1) / apc;
+    *fine_cpb = 0;
+    if (P <= kFineP || a.nstates > 2 * kFineP * kFineL || kRealThreads % 32 || getenv("SNAPMRF_DICT_LAYOUT"))
+        return;
+    long long bulk;
+    if (const char *e = getenv("SNAPMRF_DICT_FINE_ATOMS")) {
+        const long long nf = atoll(e);
+        if (nf <= 0) return;
+        bulk = nf >= n ? 0 : (n - nf) / apc;
+    } else {
+        int dev = 0, sms = 0, per_sm = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kRealThreads, smem) != cudaSuccess ||
+            sms <= 0 || per_sm <= 0) {
+            cudaGetLastError();
+            return;
+        }
+        const long long R = (long long)sms * per_sm;
+        const long long C = B * *bulk_cpb;
+        const long long rounds = C / R;
+        if (rounds && (C % R == 0 || C % R > B)) return;
+        bulk = rounds ? std::min(rounds * R / B, n / apc) : 0;
+        if (B * ((n - bulk * apc + apc_f - 1) / apc_f) > R / 2) return;
+    }
+    if (n - bulk * apc <= 0) return;
+    *bulk_cpb = bulk;
+    *fine_cpb = (n - bulk * apc + apc_f - 1) / apc_f;
+}
+
 template <int ECHO, int S, bool TAIL, bool FOLD>
-static cudaError_t launch_epg_real(const EpgArgs &a, dim3 grid, cudaStream_t st) {
+static cudaError_t launch_epg_real(EpgArgs a, dim3 grid, cudaStream_t st) {
     size_t smem = epg_real_smem_bytes(a.L);
     auto k = epg_real_kernel<ECHO, S, TAIL, FOLD>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    k<<<grid, kRealThreads, smem, st>>>(a);
+    long long bulk_cpb = grid.x, fine_cpb = 0;
+    plan_fine_tail(a, S, grid.y, (const void *)k, smem, &bulk_cpb, &fine_cpb);
+    if (bulk_cpb > 0) {
+        k<<<dim3((unsigned)bulk_cpb, grid.y), kRealThreads, smem, st>>>(a);
+        note_launches(1);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    if (fine_cpb == 0) return cudaSuccess;
+    // the fine tail, a programmatic dependent of the main grid (see
+    // epg_real_fine_kernel)
+    a.fine_first = bulk_cpb * (kRealThreads / a.L);
+    auto kf = epg_real_fine_kernel<ECHO, FOLD>;
+    const size_t smem_f = epg_real_smem_bytes(kFineL);
+    if ((e = cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_f)) != cudaSuccess)
+        return e;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)fine_cpb, grid.y);
+    cfg.blockDim = dim3(kRealThreads);
+    cfg.dynamicSmemBytes = smem_f;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = bulk_cpb > 0 ? 1 : 0;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    e = cudaLaunchKernelEx(&cfg, kf, a);
     note_launches(1);
-    return cudaGetLastError();
+    return e != cudaSuccess ? e : cudaGetLastError();
 }
 
 // P = pairs of states per lane (S = 2P).  FISP layouts that pad at most two
@@ -278,6 +351,7 @@ extern "C" int snapmrf_mrf_dict(float *d_atoms, const float *d_params, const flo
     a.packed = nullptr;
     a.packed_half = 0;
     a.packed_pitch = 0;
+    a.fine_first = 0;
     void *d_packed = opts ? opts->d_packed : nullptr;
 
     if (echo == ECHO_ROA) {

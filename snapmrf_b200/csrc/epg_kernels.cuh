@@ -38,6 +38,8 @@ struct EpgArgs {
     void *packed;
     int packed_half;      // 1: fp16, 0: bf16
     long long packed_pitch;
+    // first atom of each B1 block in the fine tail of the real-valued kernel
+    long long fine_first;
 };
 
 // Number of per-(atom, step) factors staged: E1/E2 at TE and at TR-TE, plus
@@ -523,20 +525,21 @@ __device__ __forceinline__ void store_packed(const EpgArgs &a, long long atom, l
 // The readout after relax(TE) is E2(TE) f+[0] right after the RF.  Two
 // multiplies per state and step fewer, and one exp fewer per atom and step;
 // the result differs from the separate relaxations only by rounding.
+//
+// One CTA's work: atoms atom0 .. atom0 + kRealThreads / L - 1 of B1 block
+// blk, L lanes per atom, P pairs of states per lane.
 template <int ECHO, int P, bool TAIL, bool FOLD>
-__global__ void SNAPMRF_EPG_REAL_BOUNDS epg_real_kernel(EpgArgs a) {
+__device__ __forceinline__ void epg_real_cta(const EpgArgs &a, const int L, const long long blk,
+                                             const long long atom0) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr int NF = 4;
     constexpr int FS = kRealFS;
-    const int L = a.L;
     const int apc = kRealThreads / L;
     const int tid = threadIdx.x;
     const int g = tid / L;
     const int gl = tid % L;
     const bool lane0 = (gl == 0);
-    const long long blk = blockIdx.y;
     const long long nreps = a.nreps;
-    const long long atom0 = (long long)blockIdx.x * apc;
     const long long ab = atom0 + g;
     const bool active = ab < a.natoms;
     const long long gatom = blk * a.natoms + ab;
@@ -671,6 +674,44 @@ __global__ void SNAPMRF_EPG_REAL_BOUNDS epg_real_kernel(EpgArgs a) {
     }
     if (a.packed && active)
         for (long long q = nreps + gl; q < a.packed_pitch; q += L) store_packed(a, gatom, q, 0.f);
+}
+
+// Fine layout of the real-valued recursion: kFineP pairs of states per lane
+// and kFineL = 32 / kFineP lanes per atom (64 states, so w <= 64).  Two
+// pairs measured best on C1's tail (one: a lone warp is latency-bound on the
+// shuffles; four: more instructions per step).
+#ifndef SNAPMRF_EPG_FINE_P
+#define SNAPMRF_EPG_FINE_P 2
+#endif
+constexpr int kFineP = SNAPMRF_EPG_FINE_P;
+constexpr int kFineL = 32 / kFineP;
+static_assert(kFineP == 1 || kFineP == 2 || kFineP == 4 || kFineP == 8, "fine layout");
+
+// Grid: x = CTA within the B1 block, y = block.  Each CTA signals at once
+// that a grid launched after it as a programmatic dependent (the fine tail
+// below) may start: that grid then starts when every CTA of this one has
+// started, i.e. during its last round.
+template <int ECHO, int P, bool TAIL, bool FOLD>
+__global__ void SNAPMRF_EPG_REAL_BOUNDS epg_real_kernel(EpgArgs a) {
+    asm volatile("griddepcontrol.launch_dependents;");
+    epg_real_cta<ECHO, P, TAIL, FOLD>(a, a.L, blockIdx.y, (long long)blockIdx.x * (kRealThreads / a.L));
+}
+
+// Fine tail: atoms a.fine_first .. natoms - 1 of each B1 block in the fine
+// layout.  A CTA carries its atoms through every step whatever its layout,
+// and the fine CTAs, a few times shorter than those of the chosen layout,
+// fill the slots that the chosen layout's last, partial round of resident
+// CTAs leaves free instead of a few full-length CTAs running alone.  Every
+// layout performs the same operations on each state in the same order, so
+// the atoms do not depend on the split.  Launched as a programmatic
+// dependent of the main grid, this grid must not complete before it (work
+// after it on the stream reads the whole dictionary), hence the wait at the
+// end; launched alone, the wait returns at once.
+template <int ECHO, bool FOLD>
+__global__ void __launch_bounds__(kRealThreads, 1) epg_real_fine_kernel(EpgArgs a) {
+    epg_real_cta<ECHO, kFineP, false, FOLD>(a, kFineL, blockIdx.y,
+                                            a.fine_first + (long long)blockIdx.x * (kRealThreads / kFineL));
+    asm volatile("griddepcontrol.wait;" ::: "memory");
 }
 
 // ROA (src/functions.cu:1021-1222).  State m = (Mx, My, Mz).  Per step:

@@ -199,3 +199,46 @@ def test_real_path_large_state_count(snap, oracle):
     got = run_dict(snap, "epg_fisp", params, h, T, nstates=400)
     ref = oracle.dict_atoms("epg_fisp", params, h, T, nstates=400)
     assert rel_err_per_atom(got, ref).max() < 2e-5
+
+
+def _dict_with_packed(snap, params, h, T, natoms, nstates, flags):
+    from gpu_util import torch_cuda
+    torch = torch_cuda()
+    NATOMS = params.shape[0]
+    d_params = torch.from_numpy(params).cuda()
+    d_atoms = torch.full((NATOMS, T, 2), 7.0, dtype=torch.float32, device="cuda")
+    d_norms = torch.full((NATOMS,), -1.0, dtype=torch.float32, device="cuda")
+    d_packed = torch.full((NATOMS, snap.packed_pitch(T)), 3, dtype=torch.int16, device="cuda")
+    snap.MRF_dict(d_atoms, d_params, np.ascontiguousarray(h, np.float32), T, T, NATOMS, natoms, 4, nstates,
+                  "epg_fisp", flags=flags, d_norms=d_norms, d_packed=d_packed, packed_precision=snap.PREC_FP16)
+    torch.cuda.synchronize()
+    return d_atoms.cpu().numpy(), d_norms.cpu().numpy(), d_packed.cpu().numpy()
+
+
+@pytest.mark.parametrize("nstates", [3, 20, 50, 64])
+@pytest.mark.parametrize("fold", [True, False], ids=["fold", "separate_relax"])
+def test_fine_tail_gives_the_same_atoms(snap, monkeypatch, nstates, fold):
+    """Each B1 block's trailing atoms on CTAs of 32 lanes per atom (the fine
+    tail of the real-valued kernel): 1, 10, 37 and all atoms of each block
+    fine, and the automatic choice, against the unsplit grid.  Criteria: the
+    atoms, norms and FP16 operand equal (as numbers), every element written."""
+    T = 120
+    h = mrf_schedule(T, seed=3)
+    b1s = (0.7, 0.85, 1.0, 1.2, 1.3)
+    params = _grid(np.geomspace(100, 3000, 11), np.geomspace(10, 1500, 9), b1s=b1s)
+    natoms = params.shape[0] // len(b1s)
+    flags = snap.DICT_ALL_B1_BLOCKS | snap.DICT_NORMALIZE | (0 if fold else snap.DICT_SEPARATE_RELAX)
+    monkeypatch.delenv("SNAPMRF_DICT_LAYOUT", raising=False)
+    monkeypatch.setenv("SNAPMRF_DICT_FINE_ATOMS", "0")
+    base = _dict_with_packed(snap, params, h, T, natoms, nstates, flags)
+    assert np.allclose(np.sqrt((base[0] ** 2).sum(axis=(1, 2))), 1, atol=1e-5) and np.all(base[1] > 0)
+    assert np.all(base[2][:, T:] == 0)
+    for nf in ("1", "10", "37", str(natoms), None):
+        if nf is None:
+            monkeypatch.delenv("SNAPMRF_DICT_FINE_ATOMS")
+        else:
+            monkeypatch.setenv("SNAPMRF_DICT_FINE_ATOMS", nf)
+        got = _dict_with_packed(snap, params, h, T, natoms, nstates, flags)
+        for b, g in zip(base, got):
+            assert np.array_equal(b, g), (nf, nstates)
+    assert snap.device_error(reset=True) == 0
