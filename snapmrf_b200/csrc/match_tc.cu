@@ -280,6 +280,23 @@ match_bf16_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant
                 for (int c = half * (BN / 64); c < (half + 1) * (BN / 64); c++) {
                     float v[32];
                     sm100::tmem_ld32(taddr + c * 32, v);
+                    if (IMAG) {
+                        // Bound first: each lane holds one component (x_r or
+                        // x_i sum) of all 32 atoms of the load, so every
+                        // score of the pair is at most max|own|^2 +
+                        // max|partner's|^2 (inflated by 2^-20 to cover
+                        // rounding).  When no pair of the warp can beat its
+                        // k-th best, the load needs no shuffles.  A voxel's
+                        // two sums share one phase over all atoms, so the
+                        // bound sits close to the best score of the load.
+                        float am = 0.f;
+#pragma unroll
+                        for (int j = 0; j < 32; j++) am = fmaxf(am, fabsf(v[j]));
+                        const float own = am * am;
+                        const float bound = (own + __shfl_xor_sync(0xffffffffu, own, 1)) * (1.f + 0x1p-20f);
+                        const float thr = fmaxf(ts[TOPK - 1], __shfl_xor_sync(0xffffffffu, ts[TOPK - 1], 1));
+                        if (!__any_sync(0xffffffffu, bound > thr)) continue;
+                    }
                     // the 16 scores of this load, then one test of their
                     // maximum against the current k-th best before any insertion
                     float sc[16];
