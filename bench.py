@@ -59,11 +59,12 @@ FLOP_PER_STATE_STEP = 66
 # counted as 2 flop each, the pipe's rate (plus 10 operations per lane and
 # step for the folded coefficients).
 FLOP_PER_STATE_STEP_EXECUTED = 16
-# DRAM bytes per dictionary atom (T = 1000, w = 50, normalised, writing the
-# FP16 matching operand too) measured by ncu on the reduced workload (5 B1
-# blocks, 34,690 atoms: 194.7 MB read + 488.3 MB written in one launch);
-# traffic grows with the atom count, so a full launch moves this times NATOMS.
-DICT_DRAM_BYTES_PER_ATOM = (194.683648e6 + 488.295936e6) / 34690
+# DRAM bytes per dictionary atom of the headline form (T = 1000, w = 50, the
+# FP16 matching operand normalised, the FP32 atoms as generated) measured by
+# ncu on the reduced workload (5 B1 blocks, 34,690 atoms: 241.1 MB read +
+# 306.0 MB written in one launch); traffic grows with the atom count, so a
+# full launch moves this times NATOMS.
+DICT_DRAM_BYTES_PER_ATOM = (241.051904e6 + 305.966080e6) / 34690
 PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
 
 
@@ -337,6 +338,12 @@ def run_ours(args) -> None:
     # per atom) from the dictionary kernel instead of packing the atoms again
     d_packed = torch.empty((NATOMS, snap.packed_pitch(T)), dtype=torch.int16, device=dev)
 
+    # ... and with it, the dictionary normalises only that operand: the FP32
+    # atoms stay as generated, with their norms, which the exact rescoring
+    # divides by (the same maps as unit-norm atoms, without rewriting 2.3 GB)
+    d_norms = torch.empty(NATOMS, dtype=torch.float32, device=dev)
+    flags_packed = snap.DICT_ALL_B1_BLOCKS | snap.DICT_NORMALIZE_OPERAND
+
     def packs(precision):
         return precision in (snap.PREC_BF16, snap.PREC_FP16)
 
@@ -344,13 +351,14 @@ def run_ours(args) -> None:
         if ev is not None:
             ev[0].record(stream)
         pk = packs(precision)
-        snap.MRF_dict(d_atoms, d_params, h_mrf, T, T, NATOMS, natoms, 4, NSTATES, "epg_fisp", flags=flags,
+        snap.MRF_dict(d_atoms, d_params, h_mrf, T, T, NATOMS, natoms, 4, NSTATES, "epg_fisp",
+                      flags=flags_packed if pk else flags, d_norms=d_norms if pk else None,
                       d_packed=d_packed if pk else None, packed_precision=precision if pk else 0)
         if ev is not None:
             ev[1].record(stream)
         snap.MRF_match(d_maps, d_img, d_atoms, d_params, T, T, NATOMS, natoms, nvox, in_b1map=d_b1,
                        flags=MATCH_FLAGS, precision=precision, d_index=d_index,
-                       topk=args.topk, packed_atoms=d_packed if pk else None)
+                       topk=args.topk, packed_atoms=d_packed if pk else None, atom_norms=d_norms if pk else None)
         if ev is not None:
             ev[2].record(stream)
         if gn:
@@ -428,7 +436,8 @@ def run_ours(args) -> None:
     if args.svd_sfrac > 0:
         comp = {"sfrac": args.svd_sfrac}
         try:
-            step(snap.PREC_FP16)  # the dictionary in d_atoms
+            # the unit-norm dictionary in d_atoms
+            snap.MRF_dict(d_atoms, d_params, h_mrf, T, T, NATOMS, natoms, 4, NSTATES, "epg_fisp", flags=flags)
             torch.cuda.synchronize()
             c0 = torch.cuda.Event(enable_timing=True)
             c1 = torch.cuda.Event(enable_timing=True)
@@ -517,12 +526,13 @@ def run_ours(args) -> None:
             ev_img[b].record(up_stream)
         stream.wait_event(ev_par[b])
         pk = packs(prec)
-        snap.MRF_dict(e2e_atoms, e2e_par[b], h_mrf, T, T, NATOMS, natoms, 4, NSTATES, "epg_fisp", flags=flags,
+        snap.MRF_dict(e2e_atoms, e2e_par[b], h_mrf, T, T, NATOMS, natoms, 4, NSTATES, "epg_fisp",
+                      flags=flags_packed if pk else flags, d_norms=d_norms if pk else None,
                       d_packed=d_packed if pk else None, packed_precision=prec if pk else 0)
         stream.wait_event(ev_img[b])
         snap.MRF_match(d_maps, e2e_img[b], e2e_atoms, e2e_par[b], T, T, NATOMS, natoms, nvox, in_b1map=e2e_b1[b],
                        img_stride=T, flags=MATCH_FLAGS, precision=prec, topk=args.topk,
-                       packed_atoms=d_packed if pk else None)
+                       packed_atoms=d_packed if pk else None, atom_norms=d_norms if pk else None)
         ev_free[b].record(stream)
         h_maps.copy_(d_maps, non_blocking=True)
 

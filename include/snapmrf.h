@@ -141,6 +141,12 @@ void snapmrf_ra_free(snapmrf_ra *a);
  * TR into the next step's RF instead (relaxation commutes with the
  * dephasing shift), which changes results by rounding only (~1e-7). */
 #define SNAPMRF_DICT_SEPARATE_RELAX 0x8u
+/* With d_packed (and without SNAPMRF_DICT_NORMALIZE): write the 16-bit
+ * operand of the unit-norm atoms, bit-identical to the one written with
+ * SNAPMRF_DICT_NORMALIZE, while d_atoms keeps the atoms as generated; with
+ * d_norms, their norms.  snapmrf_mrf_match takes such a dictionary with
+ * snapmrf_match_opts.atom_norms.  Saves rewriting the FP32 atoms. */
+#define SNAPMRF_DICT_NORMALIZE_OPERAND 0x10u
 
 typedef struct snapmrf_dict_opts {
     unsigned flags;  /* SNAPMRF_DICT_* */
@@ -244,6 +250,13 @@ typedef struct snapmrf_match_opts {
     const float *coeffs;
     size_t coeff_stride;
     int rank;
+    /* Optional, device [NATOMS]: the l2 norm of each atom of d_atoms, which
+     * are then taken as not normalised (a dictionary made with
+     * SNAPMRF_DICT_NORMALIZE_OPERAND): the exact FP32 rescoring divides each
+     * candidate's inner product by its atom's norm, so the maps are those of
+     * unit-norm atoms.  BF16 / FP16 with packed_atoms only (the candidates
+     * come from the unit-norm packed operand). */
+    const float *atom_norms;
 } snapmrf_match_opts;
 
 /* d_maps: out, device [nvoxels][nmaps] (nmaps == 5, nparams == 4)

@@ -29,6 +29,7 @@ DICT_ALL_B1_BLOCKS = 0x1
 DICT_NORMALIZE = 0x2
 DICT_REFERENCE_ORDER = 0x4
 DICT_SEPARATE_RELAX = 0x8
+DICT_NORMALIZE_OPERAND = 0x10
 # matching
 PREC_FP32 = 0
 PREC_BF16 = 1
@@ -61,7 +62,7 @@ class MatchOpts(C.Structure):
                 ("d_index", C.c_void_p), ("topk", C.c_int), ("packed_atoms", C.c_void_p),
                 ("packed_nreps", C.c_size_t), ("basis", C.c_void_p), ("basis_rows", C.c_size_t),
                 ("basis_stride", C.c_size_t), ("coeffs", C.c_void_p), ("coeff_stride", C.c_size_t),
-                ("rank", C.c_int)]
+                ("rank", C.c_int), ("atom_norms", C.c_void_p)]
 
 
 class SvdOpts(C.Structure):
@@ -307,7 +308,8 @@ def normalize(d_atoms, nreps: int, NATOMS: int, d_norms=None, stream=None) -> No
 def MRF_match(d_maps, img, d_atoms, d_params, NREPS: int, nreps: int, NATOMS: int, natoms: int,
               nvoxels: int, nparams: int = NPARAMS, nmaps: int = NMAPS, in_b1map=None, *,
               precision: int = PREC_FP32, flags: int = 0, img_stride: int = 0,
-              d_index=None, topk: int = 0, packed_atoms=None, compressed=None, stream=None) -> None:
+              d_index=None, topk: int = 0, packed_atoms=None, compressed=None, atom_norms=None,
+              stream=None) -> None:
     """Template matching (src/functions.cu:1493-1584).
 
     img: host numpy complex64 [nvoxels][stride] or a device tensor; NREPS is
@@ -315,7 +317,10 @@ def MRF_match(d_maps, img, d_atoms, d_params, NREPS: int, nreps: int, NATOMS: in
     in_b1map: None, a path to an RA B1 map, a host array or a device tensor.
     compressed: a Compressed from svd_compress: match in its rank-r space
     (d_atoms may then be None; with atoms the tensor-core forms rescore
-    their candidates against them)."""
+    their candidates against them).
+    atom_norms: device float32 [NATOMS], the norms of d_atoms when they are
+    not normalised (MRF_dict with DICT_NORMALIZE_OPERAND); BF16 / FP16 with
+    packed_atoms only."""
     on_host = isinstance(img, np.ndarray) or (hasattr(img, "device") and img.device.type == "cpu")
     if isinstance(img, np.ndarray):
         img = np.ascontiguousarray(img, np.complex64)
@@ -338,7 +343,8 @@ def MRF_match(d_maps, img, d_atoms, d_params, NREPS: int, nreps: int, NATOMS: in
     opts = MatchOpts(precision, flags, img_stride, NREPS, _ptr(b1), b1_host, _ptr(d_index), topk,
                      _ptr(packed_atoms), nreps if packed_atoms is not None else 0,
                      _ptr(cb.basis) if cb else None, cb.max_rank if cb else 0, cb.basis_stride if cb else 0,
-                     _ptr(cb.coeffs) if cb else None, cb.coeff_stride if cb else 0, cb.rank if cb else 0)
+                     _ptr(cb.coeffs) if cb else None, cb.coeff_stride if cb else 0, cb.rank if cb else 0,
+                     _ptr(atom_norms))
     _check(lib().snapmrf_mrf_match(_ptr(d_maps), _ptr(img), 1 if on_host else 0, _ptr(d_atoms),
                                    _ptr(d_params), nreps, NATOMS, natoms, nvoxels, nparams, nmaps,
                                    C.byref(opts), _stream_ptr(stream)))

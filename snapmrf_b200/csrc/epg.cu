@@ -294,6 +294,11 @@ extern "C" int snapmrf_mrf_dict(float *d_atoms, const float *d_params, const flo
     const bool all_blocks = (echo == ECHO_SSFP) || (flags & SNAPMRF_DICT_ALL_B1_BLOCKS);
     const size_t gen_blocks = all_blocks ? nblocks : 1;
     const bool normalize = echo == ECHO_SSFP || echo == ECHO_ROA || (flags & SNAPMRF_DICT_NORMALIZE);
+    const bool pack_normalized = (flags & SNAPMRF_DICT_NORMALIZE_OPERAND) != 0;
+    if (pack_normalized && (normalize || !(opts && opts->d_packed)))
+        SNAPMRF_FAIL(SNAPMRF_ERR_INVALID,
+                     "MRF_dict: SNAPMRF_DICT_NORMALIZE_OPERAND needs d_packed and atoms that are not normalised "
+                     "(no SNAPMRF_DICT_NORMALIZE; not epg_ssfp / roa_ssfp)");
 
     // Converted schedule (MRF_dict, src/functions.cu:1229-1291): SSFP and ROA
     // take the CSV's flip fraction of 60 deg, phase in degrees and TR/TE
@@ -352,6 +357,7 @@ extern "C" int snapmrf_mrf_dict(float *d_atoms, const float *d_params, const flo
     a.packed_half = 0;
     a.packed_pitch = 0;
     a.fine_first = 0;
+    a.pack_normalized = pack_normalized ? 1 : 0;
     void *d_packed = opts ? opts->d_packed : nullptr;
 
     if (echo == ECHO_ROA) {

@@ -40,6 +40,8 @@ struct EpgArgs {
     long long packed_pitch;
     // first atom of each B1 block in the fine tail of the real-valued kernel
     long long fine_first;
+    // 16-bit operand of the unit-norm atoms while the atoms stay as generated
+    int pack_normalized;
 };
 
 // Number of per-(atom, step) factors staged: E1/E2 at TE and at TR-TE, plus
@@ -654,22 +656,29 @@ __device__ __forceinline__ void epg_real_cta(const EpgArgs &a, const int L, cons
             for (int q = gl; q < nch; q += L) {
                 const float2 o = sR[g * kRealReadoutStride + q];
                 out[t0 + q] = o;
-                if (a.packed && !a.normalize) store_packed(a, gatom, t0 + q, o.y);
+                if (a.packed && !a.normalize && !a.pack_normalized) store_packed(a, gatom, t0 + q, o.y);
             }
     }
-    if (a.normalize || a.norms) {
+    if (a.normalize || a.norms || a.pack_normalized) {
         nrm = __shfl_sync(0xffffffffu, nrm, 0, L);
         if (a.norms && lane0 && active) a.norms[gatom] = sqrtf(nrm);
-        if (a.normalize) {
+        if (a.normalize || a.pack_normalized) {
             __syncwarp();
             float inv = nrm;
             if (inv > 0.f) inv = 1.f / sqrtf(inv);
-            if (active)
-                for (long long q = gl; q < nreps; q += L) {
-                    const float2 o = c_scale(out[q], inv);
-                    out[q] = o;
-                    if (a.packed) store_packed(a, gatom, q, o.y);
+            if (active) {
+                if (a.normalize) {
+                    for (long long q = gl; q < nreps; q += L) {
+                        const float2 o = c_scale(out[q], inv);
+                        out[q] = o;
+                        if (a.packed) store_packed(a, gatom, q, o.y);
+                    }
+                } else {
+                    // the operand of the unit-norm atom (the same product
+                    // as above); the atom itself is not rewritten
+                    for (long long q = gl; q < nreps; q += L) store_packed(a, gatom, q, c_scale(out[q], inv).y);
                 }
+            }
         }
     }
     if (a.packed && active)

@@ -194,6 +194,10 @@ extern "C" int snapmrf_mrf_match(float *d_maps, const float *img, int img_on_hos
     if (nblocks > 65535) SNAPMRF_FAIL(SNAPMRF_ERR_UNSUPPORTED, "MRF_match: more than 65535 B1 blocks");
     unsigned flags = opts ? opts->flags : 0u;
     int64_t *d_index = opts ? opts->d_index : nullptr;
+    const float *atom_norms = opts ? opts->atom_norms : nullptr;
+    if (atom_norms && (comp || !opts->packed_atoms ||
+                       (precision != SNAPMRF_PREC_BF16 && precision != SNAPMRF_PREC_FP16)))
+        SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "MRF_match: atom_norms needs BF16 / FP16 matching with packed_atoms");
     if (comp) {
         if (!opts->coeffs || opts->rank < 1 || opts->basis_rows < (size_t)opts->rank ||
             opts->basis_stride < nreps || opts->coeff_stride < (size_t)opts->rank)
@@ -269,6 +273,7 @@ extern "C" int snapmrf_mrf_match(float *d_maps, const float *img, int img_on_hos
         q.fmt = precision == SNAPMRF_PREC_FP16 ? 1 : precision == SNAPMRF_PREC_FP8 ? 2 : 0;
         q.imag = (flags & SNAPMRF_MATCH_IMAG_ATOMS) != 0;
         q.packed = opts ? opts->packed_atoms : nullptr;
+        q.atom_norms = atom_norms;
         if (q.packed && (!q.imag || q.fmt == 2 || opts->packed_nreps != nreps))
             SNAPMRF_FAIL(SNAPMRF_ERR_INVALID,
                          "MRF_match: packed_atoms need SNAPMRF_MATCH_IMAG_ATOMS, BF16 / FP16 and packed_nreps == nreps");

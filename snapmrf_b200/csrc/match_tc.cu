@@ -689,7 +689,7 @@ __global__ void rescore_kernel(float *maps, long long *index_out, const float *t
                                const long long *perm, const long long *tile_start, int nbins, const int *vox_bin,
                                const float2 *atoms, long long atom_stride, const float2 *img, long long img_stride,
                                long long nreps, const float *params, int nparams, long long bin_natoms,
-                               const int *err) {
+                               const int *err, const float *atom_norms) {
     const long long slot = (blockIdx.x * (long long)blockDim.x + threadIdx.x) / 32;
     const int lane = threadIdx.x % 32;
     if (slot >= tile_start[nbins] * BM) return;
@@ -764,6 +764,18 @@ __global__ void rescore_kernel(float *maps, long long *index_out, const float *t
         }
     }
     if (lane != 0) return;
+    if (atom_norms) {
+        // atoms as generated: the inner products of the unit-norm atoms,
+        // with 1 / ||d|| formed as the dictionary's normalisation forms it
+#pragma unroll
+        for (int k = 0; k < TOPK; k++) {
+            if (ci[k] < 0) continue;
+            const float n = atom_norms[bin * bin_natoms + ci[k]];
+            const float inv = n > 0.f ? 1.f / n : 0.f;
+            re[k] *= inv;
+            im[k] *= inv;
+        }
+    }
     int best = -1;
     float bs = 0.f, bre = 0.f, bim = 0.f;
 #pragma unroll
@@ -1032,7 +1044,7 @@ int match_bf16(const TcMatchRequest &q, cudaStream_t st) {
                   : pick(rescore_kernel<16, false>, rescore_kernel<8, false>, rescore_kernel<4, false>);
     rk<<<nblk(cap * 32, 256), 256, 0, st>>>(q.maps, q.index_out, top_s, top_i, perm, tile_start, nbins,
                                             q.b1map ? vox_bin : nullptr, ratoms, ras, rimg, ris, rn, q.params,
-                                            q.nparams, bin_natoms, err);
+                                            q.nparams, bin_natoms, err, rfull ? q.atom_norms : nullptr);
     SNAPMRF_LAUNCH_CHECK();
     publish_error_kernel<<<1, 1, 0, st>>>(err);
     SNAPMRF_LAUNCH_CHECK();

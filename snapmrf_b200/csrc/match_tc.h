@@ -29,6 +29,9 @@ struct TcMatchRequest {
     const float2 *coeffs;    // device [NATOMS][coeff_stride]
     long long coeff_stride;
     int rank;
+    // optional device [NATOMS]: norms of `atoms`, which are not normalised;
+    // the rescoring divides each candidate's inner product by its norm
+    const float *atom_norms = nullptr;
 };
 
 // BF16 / FP16 / E4M3 tcgen05 scores + top-k + FP32 rescoring; enqueued on st.

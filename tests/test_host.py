@@ -155,3 +155,23 @@ def test_match_argument_errors_without_gpu(snap):
         snap.MRF_match(1, img, 1, 1, 10, 10, 4, 4, 4, nmaps=4, stream=0)
     with pytest.raises(snap.SnapMRFError, match="precision"):
         snap.MRF_match(1, img, 1, 1, 10, 10, 4, 4, 4, precision=9, stream=0)
+
+
+def test_normalize_operand_argument_errors_without_gpu(snap):
+    """DICT_NORMALIZE_OPERAND needs the packed operand and atoms that are not
+    normalised; atom_norms needs BF16 / FP16 matching of packed atoms.  Both
+    are checked before any device work."""
+    h = np.zeros((4, 10), np.float32)
+    with pytest.raises(snap.SnapMRFError, match="NORMALIZE_OPERAND"):
+        snap.MRF_dict(1, 1, h, 10, 10, 4, 4, echo_type="epg_fisp", flags=snap.DICT_NORMALIZE_OPERAND, stream=0)
+    with pytest.raises(snap.SnapMRFError, match="NORMALIZE_OPERAND"):
+        snap.MRF_dict(1, 1, h, 10, 10, 4, 4, echo_type="epg_fisp", d_packed=1,
+                      flags=snap.DICT_NORMALIZE_OPERAND | snap.DICT_NORMALIZE, stream=0)
+    with pytest.raises(snap.SnapMRFError, match="NORMALIZE_OPERAND"):
+        snap.MRF_dict(1, 1, h, 10, 10, 4, 4, echo_type="epg_ssfp", d_packed=1,
+                      flags=snap.DICT_NORMALIZE_OPERAND, stream=0)
+    img = np.zeros((4, 10), np.complex64)
+    for kw in (dict(precision=snap.PREC_FP32, packed_atoms=1), dict(precision=snap.PREC_FP8, packed_atoms=1),
+               dict(precision=snap.PREC_FP16)):
+        with pytest.raises(snap.SnapMRFError, match="atom_norms"):
+            snap.MRF_match(1, img, 1, 1, 10, 10, 4, 4, 4, atom_norms=1, stream=0, **kw)
