@@ -728,6 +728,24 @@ __global__ void rescore_kernel(float *maps, long long *index_out, const float *t
         re[k] = 0.f;
         im[k] = 0.f;
     }
+    // Atoms as generated (atom_norms): 1 / ||d|| per candidate, formed as the
+    // dictionary's normalisation forms it, loaded ahead of the inner products
+    // so that the loads' latency is hidden.  Top-16: every lane loads and
+    // forms all 16; top-4 / 8: lane k loads candidate k's norm and forms its
+    // inverse after the inner products (each the faster on C1).
+    float inv[TOPK];
+    if constexpr (TOPK == 16) {
+#pragma unroll
+        for (int k = 0; k < TOPK; k++) {
+            inv[k] = 1.f;
+            if (atom_norms && ci[k] >= 0) {
+                const float n = atom_norms[bin * bin_natoms + ci[k]];
+                inv[k] = n > 0.f ? 1.f / n : 0.f;
+            }
+        }
+    }
+    const bool scaled = TOPK != 16 && atom_norms && lane < TOPK && cand >= 0;
+    const float my_norm = scaled ? atom_norms[bin * bin_natoms + cand] : 1.f;
     const float2 *x = img + v * img_stride;
     if (VEC) {
         const long long n2 = nreps / 2;
@@ -763,17 +781,17 @@ __global__ void rescore_kernel(float *maps, long long *index_out, const float *t
             im[k] += __shfl_xor_sync(0xffffffffu, im[k], o);
         }
     }
+    if constexpr (TOPK != 16) {
+        const float my_inv = scaled ? (my_norm > 0.f ? 1.f / my_norm : 0.f) : 1.f;
+#pragma unroll
+        for (int k = 0; k < TOPK; k++) inv[k] = __shfl_sync(0xffffffffu, my_inv, k);
+    }
     if (lane != 0) return;
     if (atom_norms) {
-        // atoms as generated: the inner products of the unit-norm atoms,
-        // with 1 / ||d|| formed as the dictionary's normalisation forms it
 #pragma unroll
         for (int k = 0; k < TOPK; k++) {
-            if (ci[k] < 0) continue;
-            const float n = atom_norms[bin * bin_natoms + ci[k]];
-            const float inv = n > 0.f ? 1.f / n : 0.f;
-            re[k] *= inv;
-            im[k] *= inv;
+            re[k] *= inv[k];
+            im[k] *= inv[k];
         }
     }
     int best = -1;
