@@ -44,3 +44,30 @@ def test_header_compiles_as_c(tmp_path):
     src.write_text('#include "snapmrf.h"\nint main(void){ return snapmrf_version() == 0; }\n')
     subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-fsyntax-only", f"-I{ROOT / 'include'}",
                     str(src)], check=True)
+
+
+STRUCTS = {"DictOpts": "snapmrf_dict_opts", "MatchOpts": "snapmrf_match_opts", "SvdOpts": "snapmrf_svd_opts",
+           "RA": "snapmrf_ra"}
+
+
+@pytest.mark.parametrize("py_name", sorted(STRUCTS))
+def test_ctypes_structs_match_the_header(snap, tmp_path, py_name):
+    """Every ctypes mirror of an option / RA struct has the header's size and
+    field offsets (a field added on one side only would shift the rest)."""
+    import ctypes
+    cls = getattr(snap.api, py_name)
+    c_name = STRUCTS[py_name]
+    fields = [f[0] for f in cls._fields_]
+    lines = [f'printf("sizeof() %zu\\n", sizeof({c_name}));']
+    lines += [f'printf("{f} %zu\\n", offsetof({c_name}, {f}));' for f in fields]
+    src = tmp_path / "s.c"
+    src.write_text('#include <stddef.h>\n#include <stdio.h>\n#include "snapmrf.h"\nint main(void){\n'
+                   + "\n".join(lines) + "\nreturn 0; }\n")
+    exe = tmp_path / "s"
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", f"-I{ROOT / 'include'}", str(src), "-o", str(exe)],
+                   check=True)
+    out = dict(ln.split() for ln in subprocess.run([str(exe)], capture_output=True, text=True,
+                                                   check=True).stdout.splitlines())
+    assert int(out["sizeof()"]) == ctypes.sizeof(cls)
+    for f in fields:
+        assert int(out[f]) == getattr(cls, f).offset, f
