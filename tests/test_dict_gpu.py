@@ -217,21 +217,29 @@ def _dict_with_packed(snap, params, h, T, natoms, nstates, flags):
 
 @pytest.mark.parametrize("nstates", [3, 20, 50, 64])
 @pytest.mark.parametrize("fold", [True, False], ids=["fold", "separate_relax"])
-def test_fine_tail_gives_the_same_atoms(snap, monkeypatch, nstates, fold):
-    """Each B1 block's trailing atoms on CTAs of 32 lanes per atom (the fine
-    tail of the real-valued kernel): 1, 10, 37 and all atoms of each block
-    fine, and the automatic choice, against the unsplit grid.  Criteria: the
-    atoms, norms and FP16 operand equal (as numbers), every element written."""
+@pytest.mark.parametrize("mode", ["normalize", "operand"])
+def test_fine_tail_gives_the_same_atoms(snap, monkeypatch, nstates, fold, mode):
+    """Each B1 block's trailing atoms on the fine layout (the fine tail of the
+    real-valued kernel, 16 lanes per atom): 1, 10, 37 and all atoms of each
+    block fine, and the automatic choice, against the unsplit grid, with the
+    atoms normalised or only the operand (DICT_NORMALIZE_OPERAND).  Criteria:
+    the atoms, norms and FP16 operand equal (as numbers), every element
+    written."""
     T = 120
     h = mrf_schedule(T, seed=3)
     b1s = (0.7, 0.85, 1.0, 1.2, 1.3)
     params = _grid(np.geomspace(100, 3000, 11), np.geomspace(10, 1500, 9), b1s=b1s)
     natoms = params.shape[0] // len(b1s)
-    flags = snap.DICT_ALL_B1_BLOCKS | snap.DICT_NORMALIZE | (0 if fold else snap.DICT_SEPARATE_RELAX)
+    norm_flag = snap.DICT_NORMALIZE if mode == "normalize" else snap.DICT_NORMALIZE_OPERAND
+    flags = snap.DICT_ALL_B1_BLOCKS | norm_flag | (0 if fold else snap.DICT_SEPARATE_RELAX)
     monkeypatch.delenv("SNAPMRF_DICT_LAYOUT", raising=False)
     monkeypatch.setenv("SNAPMRF_DICT_FINE_ATOMS", "0")
     base = _dict_with_packed(snap, params, h, T, natoms, nstates, flags)
-    assert np.allclose(np.sqrt((base[0] ** 2).sum(axis=(1, 2))), 1, atol=1e-5) and np.all(base[1] > 0)
+    norms = np.sqrt((base[0].astype(np.float64) ** 2).sum(axis=(1, 2)))
+    if mode == "normalize":
+        assert np.allclose(norms, 1, atol=1e-5) and np.all(base[1] > 0)
+    else:
+        assert np.allclose(base[1], norms, rtol=1e-5) and np.all(base[1] > 0)
     assert np.all(base[2][:, T:] == 0)
     for nf in ("1", "10", "37", str(natoms), None):
         if nf is None:
