@@ -54,6 +54,10 @@ const char *snapmrf_version(void);
 /* Number of CUDA kernels this library has launched in this process (all
  * threads, all devices): an exact count for benchmarks and tests. */
 uint64_t snapmrf_kernel_launches(void);
+/* Number of device scratch allocations this library has made in this
+ * process (stream-ordered, from the pool below): a diagnostic that lets a
+ * caller check that a call allocated nothing. */
+uint64_t snapmrf_scratch_allocations(void);
 /* Scratch memory is taken from a per-device pool that keeps freed blocks
  * for reuse by later calls; this returns the cached memory of the current
  * device to the driver (it synchronises the device first). */
@@ -318,10 +322,12 @@ int snapmrf_svd_compress(const float *d_atoms, size_t nreps, size_t NATOMS, size
                          float *d_basis, size_t basis_stride, float *d_coeffs, size_t coeff_stride,
                          int *rank, double *h_sv, const snapmrf_svd_opts *opts, void *stream);
 
-/* Device-side error word of the tensor-core kernels (a bounded wait that
- * ran out sets it; the maps of that call are then NaN).  Synchronises the
- * current device; returns 0 when no error was recorded, and clears the word
- * when reset != 0. */
+/* Device-side error word (0 when no error was recorded).  Codes: 1-6 a
+ * bounded wait of the tensor-core matching kernel ran out (the maps of that
+ * call are NaN); 7 SNAPMRF_MATCH_IMAG_ATOMS was given atoms with a non-zero
+ * real part (NaN maps); 9 snapmrf_mrf_match_noalloc was given a B1 map and
+ * a B1 block holding several B1 values (NaN maps, indices -1).
+ * Synchronises the current device; clears the word when reset != 0. */
 int snapmrf_device_error(int reset);
 
 /* Largest request snapmrf_mrf_match_noalloc accepts: its working arrays live
@@ -348,10 +354,14 @@ int snapmrf_device_error(int reset);
  *     NATOMS / natoms <= SNAPMRF_NOALLOC_MAX_B1_BLOCKS; larger requests
  *     return SNAPMRF_ERR_INVALID (split the image into several calls);
  *   - with a B1 map every B1 block must hold a single B1 value, as every
- *     table built by snapmrf_trans_params does (no check is made);
- *   - the first call on a device looks up the array's device address
- *     (cudaGetSymbolAddress, with that device current): make that first
- *     call before any stream capture;
+ *     table built by snapmrf_trans_params does; this is checked on the
+ *     device without waiting for it: when a block holds several values the
+ *     call's maps are NaN, its indices -1, and snapmrf_device_error()
+ *     returns 9;
+ *   - each call looks up the array's device address on the current device
+ *     (cudaGetSymbolAddress: host-side work, nothing enqueued); the first
+ *     call on a device also makes the runtime load the array, so make that
+ *     first call before any stream capture;
  *   - all calls on a device share the array and it keeps the previous
  *     call's contents (each call clears what must start at zero): calls
  *     whose device work overlaps race and give wrong maps, so issue them in

@@ -90,6 +90,7 @@ def lib() -> C.CDLL:
         L.snapmrf_last_error.restype = C.c_char_p
         L.snapmrf_version.restype = C.c_char_p
         L.snapmrf_kernel_launches.restype = C.c_uint64
+        L.snapmrf_scratch_allocations.restype = C.c_uint64
         L.snapmrf_device_error.argtypes = [C.c_int]
         L.snapmrf_csv_dim.restype = sz
         L.snapmrf_csv_dim.argtypes = [C.c_char_p]
@@ -136,6 +137,11 @@ def device_error(reset: bool = False) -> int:
 def kernel_launches() -> int:
     """Kernels launched by libsnapmrf.so so far in this process."""
     return lib().snapmrf_kernel_launches()
+
+
+def scratch_allocations() -> int:
+    """Device scratch allocations libsnapmrf.so has made so far in this process."""
+    return lib().snapmrf_scratch_allocations()
 
 
 def _check(rc: int) -> None:
@@ -401,8 +407,11 @@ def MRF_match_noalloc(d_maps, d_img, d_atoms, d_params, NREPS: int, nreps: int, 
     arrays come from a fixed ~1.3 MiB array the library reserves per GPU, so
     at most NOALLOC_MAX_VOXELS voxels (and NOALLOC_MAX_B1_BLOCKS B1 blocks
     with a B1 map) per call.  Calls share that array: do not let two calls
-    run on the GPU at the same time.  The first call on a device sets up
-    the array's address and should precede any stream capture."""
+    run on the GPU at the same time.  Each call looks up the array's device
+    address on the current device; the first call on a device also makes
+    the runtime load the array and should precede any stream capture.  With
+    a B1 map, a B1 block holding several B1 values gives NaN maps, indices
+    -1 and device_error() == 9."""
     _check(lib().snapmrf_mrf_match_noalloc(_ptr(d_maps), _ptr(d_img), img_stride, _ptr(d_atoms), NREPS,
                                            _ptr(d_params), nreps, NATOMS, natoms, nvoxels, nparams, nmaps,
                                            _ptr(d_b1map), _ptr(d_index), _stream_ptr(stream)))

@@ -16,6 +16,8 @@ int set_error(int code, const char *fmt, ...);
 void clear_error();
 // Adds n to the process-wide kernel launch counter.
 void note_launches(unsigned n);
+// Counts one device scratch allocation (snapmrf_scratch_allocations).
+void note_scratch_alloc();
 
 }  // namespace snapmrf
 
@@ -70,6 +72,7 @@ struct DeviceScratch {
         cudaMemPool_t pool;
         cudaError_t e = device_pool(&pool);
         if (e != cudaSuccess) return e;
+        note_scratch_alloc();
         return cudaMallocFromPoolAsync(&ptr, bytes ? bytes : 16, pool, s);
     }
     ~DeviceScratch() {

@@ -141,6 +141,10 @@ static std::atomic<uint64_t> g_launches{0};
 
 void note_launches(unsigned n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
+static std::atomic<uint64_t> g_scratch_allocs{0};
+
+void note_scratch_alloc() { g_scratch_allocs.fetch_add(1, std::memory_order_relaxed); }
+
 }  // namespace snapmrf
 
 using snapmrf::set_error;
@@ -150,6 +154,8 @@ extern "C" const char *snapmrf_last_error(void) { return snapmrf::g_last_error.c
 extern "C" const char *snapmrf_version(void) { return "snapmrf-b200 0.1 (sm_100a)"; }
 
 extern "C" uint64_t snapmrf_kernel_launches(void) { return snapmrf::g_launches.load(); }
+
+extern "C" uint64_t snapmrf_scratch_allocations(void) { return snapmrf::g_scratch_allocs.load(); }
 
 // Returns the scratch memory cached by the library's pool on the current
 // device to the driver (after the device finishes its pending work).

@@ -288,6 +288,10 @@ extern "C" int snapmrf_mrf_match(float *d_maps, const float *img, int img_on_hos
             SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "MRF_match: topk must be 4, 8 or 16 (got %d)", q.topk);
         return match_bf16(q, st);
     }
+    // the FP32 kernels carry an atom's index within its bin as an int
+    if (!d_b1 && NATOMS >= 0x7fffffffull)
+        SNAPMRF_FAIL(SNAPMRF_ERR_UNSUPPORTED,
+                     "MRF_match: FP32 matching without a B1 map takes fewer than 2^31 - 1 atoms (got %zu)", NATOMS);
     int nbins;
     long long per_bin_atoms, nslots;
     if (!d_b1) {

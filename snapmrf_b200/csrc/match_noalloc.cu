@@ -18,7 +18,6 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
-#include <mutex>
 
 #include "common.h"
 #define SNAPMRF_MATCH_KERNEL_DECLARATION_ONLY
@@ -35,6 +34,8 @@ __global__ void scatter_bins_kernel(long long *perm, long long *cursor, const in
                                     long long nvox);
 __global__ void uniform_bins_kernel(long long *slot_start, long long *tile_start, int nbins,
                                     long long nvox, long long vt);
+__global__ void check_uniform_b1_kernel(int *bad, const float *params, int nparams, long long natoms,
+                                        long long NATOMS);
 __global__ void finalize_maps_kernel(float *maps, long long *index_out, const unsigned long long *keys,
                                      const long long *perm, const int *vox_bin, const float2 *atoms,
                                      long long atom_stride, const float2 *img, long long img_stride,
@@ -44,50 +45,68 @@ __global__ void finalize_maps_kernel(float *maps, long long *index_out, const un
 namespace {
 
 // Layout of the scratch array: keys[V] u64 | perm[V] i64 | slot_start,
-// tile_start, cursor [B+1] i64 | vox_bin[V] i32 | counts[B] i32.
+// tile_start, cursor [B+1] i64 | vox_bin[V] i32 | counts[B] i32 | flag i32
+// (set when a B1 block holds several B1 values).
 constexpr size_t kMaxVoxels = SNAPMRF_NOALLOC_MAX_VOXELS;
 constexpr size_t kMaxBlocks = SNAPMRF_NOALLOC_MAX_B1_BLOCKS;
 constexpr size_t kScratchBytes = kMaxVoxels * 8 + kMaxVoxels * 8 + 3 * (kMaxBlocks + 1) * 8 +
-                                 kMaxVoxels * 4 + kMaxBlocks * 4;
+                                 kMaxVoxels * 4 + kMaxBlocks * 4 + 16;
 
 __device__ __align__(256) unsigned char g_match_scratch[kScratchBytes];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_mu;
-void *g_scratch_addr[kMaxDevices] = {};
+// Error word of this path (read by snapmrf_device_error).
+__device__ int g_noalloc_error;
 
 // Device address of g_match_scratch on the current device.  In host code
 // the symbol names a host-side shadow, not device memory, so the address is
-// looked up once per device (with that device current) and cached.
+// looked up (with the device current) on every call: a host-side query that
+// enqueues nothing, and that stays right after a device reset re-creates the
+// context and loads the array again.
 int scratch_address(void **out) {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess)
-        SNAPMRF_FAIL(SNAPMRF_ERR_CUDA, "MRF_match_noalloc: cudaGetDevice failed: %s", cudaGetErrorString(e));
-    if (dev < 0 || dev >= kMaxDevices)
-        SNAPMRF_FAIL(SNAPMRF_ERR_UNSUPPORTED, "MRF_match_noalloc: device ordinal %d >= %d", dev, kMaxDevices);
-    std::lock_guard<std::mutex> lock(g_mu);
-    if (!g_scratch_addr[dev]) {
-        void *p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_match_scratch);
-        if (e != cudaSuccess || !p)
-            SNAPMRF_FAIL(SNAPMRF_ERR_CUDA, "MRF_match_noalloc: cudaGetSymbolAddress failed: %s",
-                         cudaGetErrorString(e));
-        g_scratch_addr[dev] = p;
-    }
-    *out = g_scratch_addr[dev];
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_match_scratch);
+    if (e != cudaSuccess || !p)
+        SNAPMRF_FAIL(SNAPMRF_ERR_CUDA, "MRF_match_noalloc: cudaGetSymbolAddress failed: %s",
+                     cudaGetErrorString(e));
+    *out = p;
     return SNAPMRF_OK;
 }
 
-__global__ void clear_scratch_kernel(unsigned long long *keys, long long nkeys, int *counts, int ncounts) {
+__global__ void clear_scratch_kernel(unsigned long long *keys, long long nkeys, int *counts, int ncounts,
+                                     int *flag) {
     long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (i < nkeys) keys[i] = 0ull;
     if (i < ncounts) counts[i] = 0;
+    if (i == 0) *flag = 0;
+}
+
+// A B1 block with several B1 values cannot be matched by nearest-B1 bins:
+// such a call's maps become NaN, its indices -1, and the error word 9.
+__global__ void reject_mixed_b1_kernel(float *maps, long long *index_out, long long nvox, const int *flag) {
+    if (!*flag) return;
+    long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (v == 0) atomicCAS(&g_noalloc_error, 0, 9);
+    if (v >= nvox) return;
+    const float nan = __int_as_float(0x7fc00000);
+    for (int k = 0; k < 5; k++) maps[v * 5 + k] = nan;
+    if (index_out) index_out[v] = -1;
 }
 
 inline unsigned nblk(long long n, int t) { return (unsigned)((n + t - 1) / t); }
 
 }  // namespace
+
+// Reads (and with reset clears) this path's error word; snapmrf_device_error
+// reports it beside the tensor-core kernels' word.
+cudaError_t noalloc_device_error(int *value, int reset) {
+    cudaError_t e = cudaMemcpyFromSymbol(value, g_noalloc_error, sizeof(int));
+    if (e == cudaSuccess && reset) {
+        int z = 0;
+        e = cudaMemcpyToSymbol(g_noalloc_error, &z, sizeof(int));
+    }
+    return e;
+}
+
 }  // namespace snapmrf
 
 using namespace snapmrf;
@@ -134,10 +153,17 @@ extern "C" int snapmrf_mrf_match_noalloc(float *d_maps, const float *d_img, size
     long long *cursor = tile_start + (kMaxBlocks + 1);
     int *vox_bin = reinterpret_cast<int *>(cursor + (kMaxBlocks + 1));
     int *counts = vox_bin + kMaxVoxels;
+    int *flag = counts + kMaxBlocks;
 
-    // keys and the per-bin counts start at zero on every call
-    clear_scratch_kernel<<<nblk(std::max<long long>(nvox, nbins), 256), 256, 0, st>>>(keys, nvox, counts, nbins);
+    // keys, the per-bin counts and the flag start at zero on every call
+    clear_scratch_kernel<<<nblk(std::max<long long>(nvox, nbins), 256), 256, 0, st>>>(keys, nvox, counts, nbins,
+                                                                                      flag);
     SNAPMRF_LAUNCH_CHECK();
+    if (d_b1map && nblocks > 1) {
+        check_uniform_b1_kernel<<<nblk((long long)NATOMS, 256), 256, 0, st>>>(flag, d_params, nparams,
+                                                                              (long long)natoms, (long long)NATOMS);
+        SNAPMRF_LAUNCH_CHECK();
+    }
 
     MatchArgs m;
     m.atoms = reinterpret_cast<const float2 *>(d_atoms);
@@ -179,5 +205,9 @@ extern "C" int snapmrf_mrf_match_noalloc(float *d_maps, const float *d_img, size
         d_maps, (long long *)d_index, keys, d_b1map ? perm : nullptr, d_b1map ? vox_bin : nullptr, m.atoms,
         m.atom_stride, m.img, m.img_stride, (long long)nreps, d_params, nparams, m.bin_natoms, nvox);
     SNAPMRF_LAUNCH_CHECK();
+    if (d_b1map && nblocks > 1) {
+        reject_mixed_b1_kernel<<<nblk(nvox, 256), 256, 0, st>>>(d_maps, (long long *)d_index, nvox, flag);
+        SNAPMRF_LAUNCH_CHECK();
+    }
     return SNAPMRF_OK;
 }

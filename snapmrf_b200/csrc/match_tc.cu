@@ -1071,12 +1071,17 @@ int match_bf16(const TcMatchRequest &q, cudaStream_t st) {
 
 }  // namespace snapmrf
 
+namespace snapmrf {
+cudaError_t noalloc_device_error(int *value, int reset);
+}
+
 extern "C" int snapmrf_device_error(int reset) {
-    int v = 0;
+    int v = 0, w = 0;
     SNAPMRF_CUDA(cudaMemcpyFromSymbol(&v, snapmrf::tc::g_device_error, sizeof(int)));
     if (reset) {
         int z = 0;
         SNAPMRF_CUDA(cudaMemcpyToSymbol(snapmrf::tc::g_device_error, &z, sizeof(int)));
     }
-    return v;
+    SNAPMRF_CUDA(snapmrf::noalloc_device_error(&w, reset));
+    return v ? v : w;
 }

@@ -95,6 +95,25 @@ def mrf_schedule(T: int, seed: int, fa_deg=lambda t: 10.0 + 50.0 * abs(math.sin(
     return np.array([np.deg2rad(a), np.deg2rad(ph), TR, TR / 2], np.float32)
 
 
+def c4_ssfp_csv(T: int = 500, seed: int = 4) -> np.ndarray:
+    """The bSSFP schedule of the large off-resonance configuration:
+    alpha_t = 5 + 55 |sin(pi t / 200)| deg, phase alternating 0 / 180 deg,
+    TR ~ U[10, 14] ms, TE = TR / 2, written in the epg_ssfp / roa_ssfp CSV
+    convention (fraction of 60 deg, deg, TR - 16, TE - 3.5;
+    src/functions.cu:1240-1261)."""
+    rng = np.random.default_rng(seed)
+    t = np.arange(T)
+    fa = (5.0 + 55.0 * np.abs(np.sin(np.pi * t / 200.0))) / 60.0
+    ph = np.where(t % 2 == 0, 0.0, 180.0)
+    tr = rng.uniform(10.0, 14.0, T)
+    return np.array([fa, ph, tr - 16.0, tr / 2 - 3.5], np.float32)
+
+
+def geometric_grid(lo: float, hi: float, ratio: float = 1.05) -> np.ndarray:
+    """lo * ratio^k <= hi (the 5 % relaxation-time grids)."""
+    return np.array([lo * ratio ** k for k in range(400) if lo * ratio ** k <= hi], np.float32)
+
+
 def rel_err_per_atom(a: np.ndarray, b: np.ndarray) -> np.ndarray:
     """max_t |a - b| / max_t |b| per atom (rows)."""
     num = np.abs(a - b).max(axis=-1)

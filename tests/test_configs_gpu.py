@@ -7,7 +7,7 @@ the configurations' shapes and distributions."""
 import numpy as np
 import pytest
 
-from cases import mrf_schedule, rel_err_per_atom
+from cases import c4_ssfp_csv, mrf_schedule, rel_err_per_atom
 from gpu_util import run_dict, run_match
 
 pytestmark = pytest.mark.gpu
@@ -143,15 +143,7 @@ def test_c3_adjoint_4096_atoms(snap, oracle):
 # --------------------------------------------------------------------------
 
 def _c4_csv(T=500, seed=4):
-    """alpha_t = 5 + 55 |sin(pi t / 200)| deg, phase alternating 0 / 180 deg,
-    TR ~ U[10, 14] ms, TE = TR / 2, written in the epg_ssfp / roa_ssfp CSV
-    convention (fraction of 60 deg, deg, TR - 16, TE - 3.5)."""
-    rng = np.random.default_rng(seed)
-    t = np.arange(T)
-    fa = (5.0 + 55.0 * np.abs(np.sin(np.pi * t / 200.0))) / 60.0
-    ph = np.where(t % 2 == 0, 0.0, 180.0)
-    tr = rng.uniform(10.0, 14.0, T)
-    return np.array([fa, ph, tr - 16.0, tr / 2 - 3.5], np.float32)
+    return c4_ssfp_csv(T, seed)
 
 
 def test_c4_ssfp_b0_b1_grid_and_max_pd_matching(snap, oracle):

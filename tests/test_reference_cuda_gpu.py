@@ -9,7 +9,7 @@ from pathlib import Path
 import numpy as np
 import pytest
 
-from cases import mrf_schedule, rel_err_per_atom
+from cases import c4_ssfp_csv, geometric_grid, mrf_schedule, rel_err_per_atom
 from gpu_util import run_dict, run_match
 
 HARNESS = Path(__file__).resolve().parent.parent / "oracle" / "_ref" / "ref_harness"
@@ -120,3 +120,285 @@ def test_goldens_sum_vs_rebuilt_reference(snap, golden, tmp_path, name):
     s_pair = np.abs(got.astype(np.complex128) - ref).sum()
     print(f"{name}: sum|ref-golden| {s_ref:.3e}  sum|ours-golden| {s_got:.3e}  sum|ours-ref| {s_pair:.3e}")
     assert s_got <= max(1e-6, 2 * s_ref)
+
+
+# --------------------------------------------------------------------------
+# Parity at the benchmark's own shapes
+# --------------------------------------------------------------------------
+
+def ref_normalize(tmp, atoms):
+    """The reference's normalize kernel (src/functions.cu:670-685) on atoms."""
+    i, o = tmp / "n_in.c64", tmp / "n_out.c64"
+    np.ascontiguousarray(atoms, np.complex64).tofile(i)
+    r = subprocess.run([str(HARNESS), "normalize", str(i), str(atoms.shape[1]), str(atoms.shape[0]), str(o)],
+                       stdin=subprocess.DEVNULL, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    return np.fromfile(o, np.complex64).reshape(atoms.shape)
+
+
+def ref_match(snap, tmp, img, atoms, params, natoms, b1map=None):
+    """The reference's MRF_match (src/functions.cu:1493-1584) on the same
+    inputs; returns maps [nvox][5]."""
+    ia, aa, pa, o, bm = (tmp / n for n in ("m_i.c64", "m_a.c64", "m_p.f32", "m_o.f32", "m_b1.ra"))
+    np.ascontiguousarray(img, np.complex64).tofile(ia)
+    np.ascontiguousarray(atoms, np.complex64).tofile(aa)
+    np.ascontiguousarray(params, np.float32).tofile(pa)
+    if b1map is not None:
+        snap.ra_write(str(bm), np.ascontiguousarray(b1map, np.float32))
+    T, nvox = atoms.shape[1], img.shape[0]
+    r = subprocess.run([str(HARNESS), "match", str(ia), str(aa), str(pa), str(T), str(T), str(params.shape[0]),
+                        str(natoms), str(nvox), str(bm) if b1map is not None else "-", str(o)],
+                       stdin=subprocess.DEVNULL, capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    return np.fromfile(o, np.float32).reshape(nvox, 5)
+
+
+def top2_fp64(img, atoms, chunk=4096):
+    """Best and runner-up |<atom, voxel>| per voxel in FP64 over atom chunks,
+    and the index of the best (first on ties)."""
+    x = img.astype(np.complex128)
+    best = np.full(len(x), -1.0)
+    second = np.full(len(x), -1.0)
+    arg = np.zeros(len(x), np.int64)
+    rows = np.arange(len(x))
+    for a0 in range(0, atoms.shape[0], chunk):
+        d = atoms[a0:a0 + chunk].astype(np.complex128)
+        s = np.abs(x @ d.conj().T)
+        j = np.argmax(s, axis=1)
+        sb = s[rows, j]
+        s[rows, j] = -1.0
+        s2 = s.max(axis=1)
+        win = sb > best
+        second = np.where(win, np.maximum(best, s2), np.maximum(second, sb))
+        arg = np.where(win, a0 + j, arg)
+        best = np.where(win, sb, best)
+    return best, second, arg
+
+
+def decided(img, dicts, blocks=None, natoms=None, gap=1e-6):
+    """Voxels whose matched atom is decided by the exact (FP64) scores of
+    every dictionary in `dicts` (the reference's and this implementation's
+    atoms, which differ by FP32 rounding): the same first argmax under each,
+    leading the runner-up by more than `gap` (relative) under each.  With
+    `blocks`, each voxel is scored within its B1 block only."""
+    n = img.shape[0]
+    ok = np.ones(n, bool)
+    first = None
+    for d in dicts:
+        if blocks is None:
+            b, s, a = top2_fp64(img, d)
+        else:
+            b, s, a = np.zeros(n), np.zeros(n), np.zeros(n, np.int64)
+            for j in np.unique(blocks):
+                sel = blocks == j
+                b[sel], s[sel], a[sel] = top2_fp64(img[sel], d[j * natoms:(j + 1) * natoms])
+                a[sel] += j * natoms
+        ok &= (b - s) > gap * b
+        if first is None:
+            first = a
+        else:
+            ok &= a == first
+    return ok
+
+
+def nearest_block(b1map, b1s):
+    """merge_maps' rule with a B1 map (src/functions.cu:1351-1384): strict '<'
+    from 10, ties to the lower block."""
+    out = np.zeros(len(b1map), np.int64)
+    for v, g in enumerate(b1map):
+        best, babs = 0, 10.0
+        for k, b in enumerate(b1s):
+            d = abs(np.float32(g) - np.float32(b))
+            if d < babs:
+                best, babs = k, d
+        out[v] = best
+    return out
+
+
+C1_B1 = (0.60, 0.80, 1.00, 1.20, 1.40)
+
+
+@pytest.fixture(scope="module")
+def c1_blocks(snap, tmp_path_factory):
+    """Five B1 blocks of the 240x240 B1-mapped FISP workload (6,938 T1/T2
+    pairs each, T = 1000, w = 50, its schedule with the 180 deg row 0) from
+    the rebuilt reference: one epg_fisp run per block with the flip-angle
+    column multiplied by the block's B1, the rule the B1 extension follows
+    (epg_ssfp's FA x b1, src/functions.cu:970-973)."""
+    import bench
+    tmp = tmp_path_factory.mktemp("c1")
+    h = bench.schedule(1)
+    t1, t2, b0, _ = bench.grid()
+    b1 = np.array(C1_B1, np.float32)
+    params = snap.trans_params(t1, t2, b0, b1)
+    natoms = params.shape[0] // len(b1)
+    assert natoms == 6938
+    blocks = []
+    for j, v in enumerate(b1):
+        hj = h.copy()
+        hj[0] = h[0] * v
+        blocks.append(ref_dict(tmp, "epg_fisp", params[j * natoms:(j + 1) * natoms], hj, bench.T, natoms,
+                               bench.NSTATES))
+    return h, params, natoms, np.concatenate(blocks), tmp
+
+
+def _headline_dict(snap, params, h, natoms, T, w, precision):
+    """The benchmark's headline dictionary call: folded relaxation, the
+    eight-operation RF, the 16-bit operand of the unit-norm atoms, the norms,
+    FP32 atoms as generated."""
+    import torch
+    N = params.shape[0]
+    d_params = torch.from_numpy(params).cuda()
+    d_atoms = torch.zeros((N, T, 2), dtype=torch.float32, device="cuda")
+    d_norms = torch.empty(N, dtype=torch.float32, device="cuda")
+    d_packed = torch.zeros((N, snap.packed_pitch(T)), dtype=torch.int16, device="cuda")
+    snap.MRF_dict(d_atoms, d_params, h, T, T, N, natoms, 4, w, "epg_fisp",
+                  flags=snap.DICT_ALL_B1_BLOCKS | snap.DICT_NORMALIZE_OPERAND, d_norms=d_norms,
+                  d_packed=d_packed, packed_precision=precision)
+    torch.cuda.synchronize()
+    return d_params, d_atoms, d_norms, d_packed
+
+
+def test_c1_shape_dictionary_headline_mode_vs_reference_cuda(snap, c1_blocks):
+    """Atoms of the benchmark's headline dictionary mode within 1e-5
+    (per-atom max-norm relative) of the rebuilt reference's epg_fisp, at the
+    benchmark's T = 1000, w = 50; the norms within 1e-5 and the FP16 operand
+    within FP16 rounding of the reference atoms scaled to unit norm."""
+    import torch
+    h, params, natoms, ref, _ = c1_blocks
+    T = ref.shape[1]
+    _, d_atoms, d_norms, d_packed = _headline_dict(snap, params, h, natoms, T, 50, snap.PREC_FP16)
+    a = d_atoms.cpu().numpy()
+    got = (a[..., 0] + 1j * a[..., 1]).astype(np.complex64)
+    rel = rel_err_per_atom(got, ref)
+    print(f"C1 shape, headline mode: max rel vs reference CUDA {rel.max():.3e} (median {np.median(rel):.3e})")
+    assert rel.max() < 1e-5
+    nref = np.linalg.norm(ref.astype(np.complex128), axis=1)
+    nrel = np.abs(d_norms.cpu().numpy() - nref) / nref
+    print(f"norms: max rel {nrel.max():.3e}")
+    assert nrel.max() < 1e-5
+    pk = d_packed.cpu().numpy().view(np.float16)[:, :T].astype(np.float64)
+    want = ref.imag.astype(np.float64) / nref[:, None]
+    perr = np.abs(pk - want).max(axis=1) / np.abs(want).max(axis=1)
+    print(f"FP16 operand: max rel {perr.max():.3e}")
+    assert perr.max() < 1e-3
+    del torch
+
+
+def test_c1_shape_matching_vs_reference_cuda(snap, c1_blocks):
+    """4,096 voxels of the benchmark phantom (SNR 40, B1 map) matched within
+    their nearest B1 block: the FP32 form and the headline FP16 form
+    (tcgen05, purely imaginary atoms, top-4 rescored in FP32 against atoms
+    as generated and their norms) give the (T1, T2, B0, B1) of the
+    reference's MRF_match on its own normalised atoms wherever the FP64
+    score gap to the runner-up exceeds 1e-6."""
+    import torch
+    import bench
+    h, params, natoms, ref, tmp = c1_blocks
+    T, w = ref.shape[1], bench.NSTATES
+    b1s = np.array(C1_B1, np.float32)
+    b1map, vt1, vt2, m0, ph = bench.phantom(0, 64)
+    n = b1map.size
+    vp = np.stack([vt1, vt2, np.zeros(n, np.float32), b1map], 1).astype(np.float32)
+    sig = run_dict(snap, "epg_fisp", vp, h, T, natoms=1, nstates=w, flags=snap.DICT_ALL_B1_BLOCKS)
+    sig = sig * (m0 * np.exp(1j * ph))[:, None]
+    rng = np.random.default_rng(2024)
+    sigma = np.linalg.norm(sig, axis=1, keepdims=True) / np.sqrt(T) / 40.0
+    img = (sig + sigma / np.sqrt(2) * (rng.standard_normal(sig.shape) + 1j * rng.standard_normal(sig.shape)))
+    img = img.astype(np.complex64)
+
+    ref_unit = ref_normalize(tmp, ref)
+    ref_maps = ref_match(snap, tmp, img, ref_unit, params, natoms, b1map)
+    blk = nearest_block(b1map, b1s)
+
+    # FP32 form on the unit-norm dictionary
+    atoms = run_dict(snap, "epg_fisp", params, h, T, natoms=natoms, nstates=w,
+                     flags=snap.DICT_ALL_B1_BLOCKS | snap.DICT_NORMALIZE)
+    sure = decided(img, (ref_unit, atoms), blk, natoms)
+    print(f"voxels decided by a gap > 1e-6 under both dictionaries: {sure.mean():.4f}")
+    assert sure.mean() > 0.9
+    maps, _ = run_match(snap, img, atoms, params, natoms=natoms, b1map=b1map, b1_device=True)
+    diff = (maps[:, :4] != ref_maps[:, :4]).any(axis=1)
+    print(f"FP32 form: {diff.sum()} of {n} voxels differ from the reference ({(diff & sure).sum()} decided)")
+    np.testing.assert_array_equal(maps[sure, :4], ref_maps[sure, :4])
+    np.testing.assert_allclose(maps[:, 4], ref_maps[:, 4], rtol=1e-5)
+
+    # headline FP16 form
+    d_params, d_atoms, d_norms, d_packed = _headline_dict(snap, params, h, natoms, T, w, snap.PREC_FP16)
+    d_img = torch.from_numpy(img.view(np.float32).reshape(n, T, 2)).cuda()
+    d_b1 = torch.from_numpy(b1map).cuda()
+    d_maps = torch.full((n, 5), -7.0, device="cuda")
+    snap.MRF_match(d_maps, d_img, d_atoms, d_params, T, T, params.shape[0], natoms, n, in_b1map=d_b1,
+                   precision=snap.PREC_FP16, flags=snap.MATCH_IMAG_ATOMS | snap.MATCH_ASSUME_UNIFORM_B1,
+                   packed_atoms=d_packed, atom_norms=d_norms)
+    torch.cuda.synchronize()
+    assert snap.device_error(reset=True) == 0
+    m16 = d_maps.cpu().numpy()
+    a = d_atoms.cpu().numpy()
+    head = (a[..., 0] + 1j * a[..., 1]) / d_norms.cpu().numpy()[:, None]
+    sure = decided(img, (ref_unit, head), blk, natoms)
+    diff = (m16[:, :4] != ref_maps[:, :4]).any(axis=1)
+    print(f"FP16 headline form: {diff.sum()} of {n} voxels differ from the reference "
+          f"({(diff & sure).sum()} decided)")
+    np.testing.assert_array_equal(m16[sure, :4], ref_maps[sure, :4])
+    np.testing.assert_allclose(m16[:, 4], ref_maps[:, 4], rtol=1e-5)
+
+
+def test_c4_shape_ssfp_vs_reference_cuda(snap, tmp_path):
+    """The large off-resonance configuration's bSSFP dictionary at its shape
+    (T = 500, w = 50, the 6,938 T1/T2 pairs x B0 in [-100, 100] Hz x two B1
+    blocks = 69,380 atoms) against the rebuilt reference's epg_ssfp within
+    1e-5; then 4,096 noisy voxels matched without a B1 map (the reference
+    merges its blocks by the largest PD: a global first argmax) in FP32 and
+    on the tensor cores with complex [Re; Im] operands, equal to the
+    reference's MRF_match wherever the FP64 score gap exceeds 1e-6."""
+    import torch
+    T, w = 500, 50
+    h = c4_ssfp_csv(T)
+    t1, t2 = geometric_grid(100.0, 5000.0), geometric_grid(10.0, 2000.0)
+    b0 = np.array([-100.0, -48.0, 0.0, 52.0, 100.0], np.float32)
+    b1 = np.array([0.9, 1.1], np.float32)
+    params = snap.trans_params(t1, t2, b0, b1)
+    natoms = params.shape[0] // len(b1)
+    assert params.shape[0] == 69380
+    ref = ref_dict(tmp_path, "epg_ssfp", params, h, T, natoms, w)
+    got = run_dict(snap, "epg_ssfp", params, h, T, natoms=natoms, nstates=w)
+    rel = rel_err_per_atom(got, ref)
+    print(f"C4 shape SSFP: max rel vs reference CUDA {rel.max():.3e} (median {np.median(rel):.3e})")
+    assert rel.max() < 1e-5
+
+    rng = np.random.default_rng(44)
+    n = 4096
+    vt1 = np.exp(rng.uniform(np.log(200), np.log(4000), n)).astype(np.float32)
+    vt2 = np.minimum(np.exp(rng.uniform(np.log(20), np.log(400), n)), 0.5 * vt1).astype(np.float32)
+    vb0 = b0[rng.integers(0, len(b0), n)]
+    vb1 = b1[rng.integers(0, len(b1), n)]
+    sig = np.zeros((n, T), np.complex64)
+    for v in b1:
+        sel = np.flatnonzero(vb1 == v)
+        vp = np.stack([vt1[sel], vt2[sel], vb0[sel], np.full(len(sel), v, np.float32)], 1)
+        sig[sel] = run_dict(snap, "epg_ssfp", vp, h, T, natoms=len(sel), nstates=w)
+    sig = sig * (rng.uniform(0.6, 1.0, n) * np.exp(1j * rng.uniform(0, 2 * np.pi, n)))[:, None]
+    sigma = np.linalg.norm(sig, axis=1, keepdims=True) / np.sqrt(T) / 40.0
+    img = (sig + sigma / np.sqrt(2) * (rng.standard_normal(sig.shape) + 1j * rng.standard_normal(sig.shape)))
+    img = img.astype(np.complex64)
+
+    ref_maps = ref_match(snap, tmp_path, img, ref, params, natoms)
+    sure = decided(img, (ref, got))
+    print(f"voxels decided by a gap > 1e-6 under both dictionaries: {sure.mean():.4f}")
+    assert sure.mean() > 0.9
+    maps, _ = run_match(snap, img, got, params, natoms=natoms)
+    np.testing.assert_array_equal(maps[sure, :4], ref_maps[sure, :4])
+    np.testing.assert_allclose(maps[:, 4], ref_maps[:, 4], rtol=1e-5)
+    # the tensor-core forms pick among their top-k by exact FP32 rescoring:
+    # FP16 (11-bit significands) keeps the decided voxel's best in its list
+    # on >= 99.9 % of voxels; BF16 (8 bits) on complex bSSFP atoms, whose
+    # neighbours in T1 / T2 score closer than its rounding, on >= 99.5 %
+    for prec, name, bar in ((snap.PREC_FP16, "fp16", 0.999), (snap.PREC_BF16, "bf16", 0.995)):
+        m, _ = run_match(snap, img, got, params, natoms=natoms, precision=prec)
+        assert snap.device_error(reset=True) == 0
+        same = (m[:, :4] == ref_maps[:, :4]).all(axis=1)
+        print(f"C4 shape {name} (complex operands): equal to the reference on {same[sure].mean():.5f} "
+              f"of the decided voxels")
+        assert same[sure].mean() >= bar
+    del torch
