@@ -125,6 +125,54 @@ def fisp_jvp(theta, tangent, h_mrf, nstates: int = 101, echo: str = "epg_fisp", 
     return sig, dsig, loss.value, dloss.value
 
 
+def trans_params(t1, t2, b0, b1) -> np.ndarray:
+    """params[NATOMS][4] = {T1, T2, B0, B1} restated from trans_params
+    (src/functions.cu:355-391): B1 outermost, then B0, then T2, T1
+    innermost, keeping T1 > T2 strictly (compute_natoms, :393-414)."""
+    t1, t2, b0, b1 = (np.asarray(v, np.float32).reshape(-1) for v in (t1, t2, b0, b1))
+    rows = [(a, b, c, d) for d in b1 for c in b0 for b in t2 for a in t1 if a > b]
+    return np.array(rows, np.float32).reshape(-1, 4)
+
+
+def gn_step_f64(theta, x, h_mrf, nstates: int = 101, echo: str = "epg_fisp"):
+    """One projected Gauss-Newton step of (T1, T2) in FP64 for one voxel x
+    (complex [T]) under the model x = rho * s(T1, T2, B1), s = i f the real
+    FISP / SR signal, rho complex and eliminated by variable projection.  The
+    refinement has no counterpart in the reference; this is the checker's
+    FP64 statement of it, built on the forward-mode derivatives above.
+    theta = (T1, T2, B1).  Returns (step [2], |rho|, |<s, x>| / ||s||)."""
+    s, d1, _, _ = fisp_jvp(theta, (1, 0, 0), h_mrf, nstates=nstates, echo=echo)
+    _, d2, _, _ = fisp_jvp(theta, (0, 1, 0), h_mrf, nstates=nstates, echo=echo)
+    s, J = 1j * s, np.stack([1j * d1, 1j * d2], 1)
+    x = np.asarray(x, np.complex128)
+    rho = np.vdot(s, x) / np.vdot(s, s)
+    ss = np.vdot(s, s).real
+    Pj = J - np.outer(s, (s.conj() @ J) / ss)
+    A = (abs(rho) ** 2) * (Pj.conj().T @ Pj).real
+    b = (np.conj(rho) * (Pj.conj().T @ x)).real
+    return np.linalg.solve(A, b), abs(rho), abs(np.vdot(s, x)) / np.sqrt(ss)
+
+
+def refine_gn_f64(theta, x, h_mrf, nstates: int = 101, echo: str = "epg_fisp", iterations: int = 40,
+                  tol: float = 1e-12, max_rel_step: float = 0.2):
+    """FP64 Gauss-Newton of (T1, T2) from theta = (T1, T2, B1) iterated to
+    convergence (every step at most max_rel_step of each value, T1 > T2 > 0
+    kept): the least-squares fit of one voxel.  Returns (T1, T2, PD) with PD =
+    |<s, x>| / ||s|| at the result."""
+    t1, t2, b1 = (float(v) for v in theta)
+    for _ in range(iterations):
+        d, _, _ = gn_step_f64((t1, t2, b1), x, h_mrf, nstates, echo)
+        d = np.clip(d, [-max_rel_step * t1, -max_rel_step * t2], [max_rel_step * t1, max_rel_step * t2])
+        n2 = max(t2 + d[1], 1e-3)
+        n1 = max(t1 + d[0], n2 * (1 + 1e-4))
+        done = abs(n1 - t1) <= tol * t1 and abs(n2 - t2) <= tol * t2
+        t1, t2 = n1, n2
+        if done:
+            break
+    _, _, pd = gn_step_f64((t1, t2, b1), x, h_mrf, nstates, echo)
+    return t1, t2, pd
+
+
 def svd_compress(atoms, natoms: int, sfrac: float | None = None, rank: int | None = None):
     """Low-rank compression per B1 block, restated from matlab/MRF_dict_B1.m:127-159
     (input.reduce = 1) in FP64 numpy:

@@ -63,6 +63,8 @@ def _compile(src: str, verbose: bool, extra: list[str]) -> Path:
 
 
 COMPAT_LIB = PKG / "libsnapmrf_compat.so"
+# the benchmark's FP32 FMA throughput probe (not part of the product library)
+PROBE_LIB = PKG / "libsnapmrf_probe.so"
 CLI = PKG / "mrf"
 RPATH = ["-Xlinker", "-rpath", "-Xlinker", "$ORIGIN"]
 
@@ -88,11 +90,19 @@ def build(verbose: bool = False, extra: list[str] | None = None) -> Path:
     BUILD.mkdir(exist_ok=True)
     extra = list(extra or [])
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 2)) as ex:
-        objs = list(ex.map(lambda s: _compile(s, verbose, extra), SOURCES + ["compat.cpp", "mrf_cli.cpp"]))
-    core, compat_o, cli_o = objs[:len(SOURCES)], objs[-2], objs[-1]
+        objs = list(ex.map(lambda s: _compile(s, verbose, extra),
+                           SOURCES + ["compat.cpp", "mrf_cli.cpp", "fp32_probe.cu"]))
+    core, compat_o, cli_o, probe_o = objs[:len(SOURCES)], objs[-3], objs[-2], objs[-1]
     _link(LIB, core, ["-shared"])
     _link(COMPAT_LIB, [compat_o], ["-shared"])
     _link(CLI, [cli_o], [])
+    if _stale(PROBE_LIB, [probe_o]):
+        tmp = PROBE_LIB.with_name(PROBE_LIB.name + ".tmp")
+        r = subprocess.run([nvcc()] + ARCH + ["-shared", "-o", str(tmp), str(probe_o), "-lcudart"],
+                           capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"link of {PROBE_LIB.name} failed:\n{r.stdout}\n{r.stderr}")
+        os.replace(tmp, PROBE_LIB)
     return LIB
 
 

@@ -160,6 +160,21 @@ __global__ void merge_nearest_b1_kernel(unsigned long long *keys_out, int *vox_b
     keys_out[v] = keys[(long long)best * nvox + v];
 }
 
+// Maps of a call whose device-side check failed (*err != 0): NaN, index -1.
+__global__ void poison_maps_kernel(float *maps, long long *index_out, long long nvox, const int *err) {
+    if (!*err) return;
+    long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (v >= nvox) return;
+    const float nan = __int_as_float(0x7fc00000);
+    for (int k = 0; k < 5; k++) maps[v * 5 + k] = nan;
+    if (index_out) index_out[v] = -1;
+}
+
+namespace tc {
+// Copies a call's error code into the library's device error word (match_tc.cu).
+__global__ void publish_error_kernel(const int *err);
+}
+
 static inline unsigned nblk(long long n, int t) { return (unsigned)((n + t - 1) / t); }
 
 }  // namespace snapmrf
@@ -308,8 +323,10 @@ extern "C" int snapmrf_mrf_match(float *d_maps, const float *img, int img_on_hos
         nslots = nvox * (long long)nblocks;
     }
 
+    // purely imaginary atoms: half the products (the imaginary parts only)
+    const bool imag = (flags & SNAPMRF_MATCH_IMAG_ATOMS) != 0;
     // scratch: keys[nslots] u64 | perm[nvox] i64 | slot_start, tile_start,
-    // cursor [nbins+1] i64 | vox_bin[nvox] i32 | counts[nbins] i32
+    // cursor [nbins+1] i64 | vox_bin[nvox] i32 | counts[nbins] i32 | err i32
     size_t bytes = (size_t)nslots * 8 + (size_t)nvox * 8 + 3 * (size_t)(nbins + 1) * 8 +
                    (size_t)nvox * 4 + (size_t)nbins * 4 + 64;
     DeviceScratch s_work;
@@ -321,7 +338,9 @@ extern "C" int snapmrf_mrf_match(float *d_maps, const float *img, int img_on_hos
     long long *cursor = tile_start + (nbins + 1);
     int *vox_bin = reinterpret_cast<int *>(cursor + (nbins + 1));
     int *counts = vox_bin + nvox;
+    int *err = counts + nbins;
     SNAPMRF_CUDA(cudaMemsetAsync(keys, 0, (size_t)nslots * 8, st));
+    if (imag) SNAPMRF_CUDA(cudaMemsetAsync(err, 0, sizeof(int), st));
 
     MatchArgs m;
     m.atoms = reinterpret_cast<const float2 *>(d_atoms);
@@ -333,6 +352,7 @@ extern "C" int snapmrf_mrf_match(float *d_maps, const float *img, int img_on_hos
     m.bin_natoms = per_bin_atoms;
     m.nvox = nvox;
     m.keys = keys;
+    m.err = imag ? err : nullptr;
 
     if (!d_b1) {
         // one bin, identity permutation
@@ -381,19 +401,11 @@ extern "C" int snapmrf_mrf_match(float *d_maps, const float *img, int img_on_hos
         m.nreps = opts->rank;
     }
 
-    // Grid: y walks voxel tiles (bin-major, so concurrent CTAs share a bin's
-    // atoms in L2), x splits a bin's atom tiles so that small voxel counts
-    // still fill the 148 SMs.
     long long max_tiles = general ? (long long)nbins * ((nvox + kMatchVT - 1) / kMatchVT)
                                   : (nvox + kMatchVT - 1) / kMatchVT + nbins;
-    long long atiles = (per_bin_atoms + kMatchAT - 1) / kMatchAT;
     long long est_tiles = general ? max_tiles : (nvox + kMatchVT - 1) / kMatchVT;
-    long long target = 148 * 2 * 4;
-    long long splits = std::max(1ll, std::min(atiles, (target + est_tiles - 1) / std::max(1ll, est_tiles)));
-    m.atiles_per_split = (int)((atiles + splits - 1) / splits);
-    splits = (atiles + m.atiles_per_split - 1) / m.atiles_per_split;
-    dim3 grid((unsigned)splits, (unsigned)std::min(max_tiles, 65535ll));
-    SNAPMRF_CUDA(launch_match_fp32(m, grid, st));
+    dim3 grid = fp32_match_grid(m, est_tiles, max_tiles);
+    SNAPMRF_CUDA(launch_match_fp32(m, grid, imag, st));
 
     const unsigned long long *fkeys = keys;
     if (general) {
@@ -414,5 +426,12 @@ extern "C" int snapmrf_mrf_match(float *d_maps, const float *img, int img_on_hos
         d_maps, (long long *)d_index, fkeys, d_b1 ? perm : nullptr, d_b1 ? vox_bin : nullptr, m.atoms,
         m.atom_stride, m.img, m.img_stride, m.nreps, d_params, nparams, per_bin_atoms, nvox);
     SNAPMRF_LAUNCH_CHECK();
+    if (imag) {
+        // an atom with a real part: NaN maps, indices -1, error word 7
+        poison_maps_kernel<<<nblk(nvox, 256), 256, 0, st>>>(d_maps, (long long *)d_index, nvox, err);
+        SNAPMRF_LAUNCH_CHECK();
+        tc::publish_error_kernel<<<1, 1, 0, st>>>(err);
+        SNAPMRF_LAUNCH_CHECK();
+    }
     return SNAPMRF_OK;
 }

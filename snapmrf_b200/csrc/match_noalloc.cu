@@ -193,14 +193,9 @@ extern "C" int snapmrf_mrf_match_noalloc(float *d_maps, const float *d_img, size
         m.perm = nullptr;
     }
     const long long max_tiles = (nvox + kMatchVT - 1) / kMatchVT + nbins;
-    const long long atiles = (m.bin_natoms + kMatchAT - 1) / kMatchAT;
-    const long long vt = (nvox + kMatchVT - 1) / kMatchVT;
-    const long long target = 148 * 2 * 4;
-    long long splits = std::max(1ll, std::min(atiles, (target + vt - 1) / std::max(1ll, vt)));
-    m.atiles_per_split = (int)((atiles + splits - 1) / splits);
-    splits = (atiles + m.atiles_per_split - 1) / m.atiles_per_split;
-    dim3 grid((unsigned)splits, (unsigned)std::min(max_tiles, 65535ll));
-    SNAPMRF_CUDA(launch_match_fp32(m, grid, st));
+    dim3 grid = fp32_match_grid(m, (nvox + kMatchVT - 1) / kMatchVT, max_tiles);
+    m.err = nullptr;
+    SNAPMRF_CUDA(launch_match_fp32(m, grid, false, st));
     finalize_maps_kernel<<<nblk(nvox * 32, 256), 256, 0, st>>>(
         d_maps, (long long *)d_index, keys, d_b1map ? perm : nullptr, d_b1map ? vox_bin : nullptr, m.atoms,
         m.atom_stride, m.img, m.img_stride, (long long)nreps, d_params, nparams, m.bin_natoms, nvox);

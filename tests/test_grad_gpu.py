@@ -177,15 +177,7 @@ def test_adjoint_rejects_unsupported_inputs(snap):
 
 def gn_step_fp64(orc, theta, x, h, w, echo="epg_fisp"):
     """One projected Gauss-Newton step in FP64 from the oracle's tangents."""
-    s, d1, _, _ = orc.fisp_jvp(theta, (1, 0, 0), h, nstates=w, echo=echo)
-    _, d2, _, _ = orc.fisp_jvp(theta, (0, 1, 0), h, nstates=w, echo=echo)
-    s, J = 1j * s, np.stack([1j * d1, 1j * d2], 1)
-    rho = np.vdot(s, x) / np.vdot(s, s)
-    ss = np.vdot(s, s).real
-    Pj = J - np.outer(s, (s.conj() @ J) / ss)
-    A = (abs(rho) ** 2) * (Pj.conj().T @ Pj).real
-    b = (np.conj(rho) * (Pj.conj().T @ x)).real
-    return np.linalg.solve(A, b), abs(rho), abs(np.vdot(s, x)) / np.sqrt(ss)
+    return orc.gn_step_f64(theta, x, h, nstates=w, echo=echo)
 
 
 def run_gn(snap, theta, img, h, w, iterations, echo="epg_fisp", max_rel_step=0.2, b1map=None, tol=1e-4):

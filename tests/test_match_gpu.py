@@ -155,3 +155,46 @@ def test_pipeline_config0_like(snap, oracle):
     maps, got = run_match(snap, img, atoms, params)
     ref_maps, ref_idx = oracle.match(img, atoms, params, T, nthreads=8)
     check_parity(img, atoms, params, maps, got, ref_maps, ref_idx)
+
+
+@pytest.mark.parametrize("use_map,nreps,stride_pad", [(False, 300, 0), (True, 300, 0), (True, 213, 5),
+                                                      (False, 77, 3)])
+def test_fp32_imaginary_atom_form_equals_complex_form(snap, oracle, use_map, nreps, stride_pad):
+    """FISP atoms with every RF phase 0 are purely imaginary; with
+    SNAPMRF_MATCH_IMAG_ATOMS the FP32 form multiplies only their imaginary
+    parts (half the products), and its sums equal the complex form's
+    exactly (the real parts' products add exact zeros): same maps, indices
+    and PD bit for bit, for whole and partial time ranges, padded image
+    rows (odd strides take the 8-byte load path) and ragged tiles."""
+    b1s = np.float32([0.7, 0.85, 1.0, 1.15, 1.3])
+    atoms, params, natoms = _dictionary(snap, oracle, b1s=b1s, T=300)
+    assert np.abs(atoms.real).max() == 0
+    nvox = 777
+    img = _voxels(atoms, nvox, 11)
+    if stride_pad:
+        pad = np.zeros((nvox, 300 + stride_pad), np.complex64)
+        pad[:, :300] = img
+        img = pad
+    b1map = np.random.default_rng(12).uniform(0.6, 1.4, nvox).astype(np.float32) if use_map else None
+    a = run_match(snap, img, atoms, params, natoms=natoms, b1map=b1map, nreps=nreps, device_img=True)
+    b = run_match(snap, img, atoms, params, natoms=natoms, b1map=b1map, nreps=nreps, device_img=True,
+                  flags=snap.MATCH_IMAG_ATOMS)
+    assert snap.device_error(reset=True) == 0
+    np.testing.assert_array_equal(a[1], b[1])
+    np.testing.assert_array_equal(a[0], b[0])
+    ref_maps, ref_idx = oracle.match(img[:, :nreps], np.ascontiguousarray(atoms[:, :nreps]), params, nreps,
+                                     natoms=natoms, b1map=b1map, nthreads=8)
+    check_parity(img[:, :nreps], atoms[:, :nreps], params, b[0], b[1], ref_maps, ref_idx)
+
+
+def test_fp32_imaginary_atom_form_rejects_complex_atoms(snap, oracle):
+    """Atoms with a real part under SNAPMRF_MATCH_IMAG_ATOMS: NaN maps,
+    indices -1 and device error 7, as in the tensor-core forms."""
+    atoms, params, natoms = _dictionary(snap, oracle, nb1=1, T=100)
+    atoms = atoms.copy()
+    atoms[5] += 0.01
+    img = _voxels(atoms, 100, 13)
+    assert snap.device_error(reset=True) == 0
+    maps, got = run_match(snap, img, atoms, params, flags=snap.MATCH_IMAG_ATOMS)
+    assert snap.device_error(reset=True) == 7
+    assert np.isnan(maps).all() and (got == -1).all()

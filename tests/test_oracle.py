@@ -159,3 +159,30 @@ def test_oracle_compressed_match_full_rank_is_exact(oracle):
                         b1map=b1)
     np.testing.assert_array_equal(ic, i)
     np.testing.assert_allclose(mc[:, 4], m[:, 4], rtol=1e-5)
+
+
+def test_trans_params_restatement_matches_the_product_table(snap):
+    """The oracle's numpy trans_params (used by the CPU arm so that it loads
+    no product code) gives the table of the product's host code, which is
+    bit-identical to the reference's own (test_host)."""
+    from oracle import oracle as orc
+    for t1, t2, b0, b1 in [(np.arange(100, 3001, 100), np.arange(20, 301, 10), [0], [1]),
+                           ([100 * 1.05 ** k for k in range(81)], [10 * 1.05 ** k for k in range(109)], [0],
+                            [0.6 + 0.02 * k for k in range(41)]),
+                           ([300, 200, 100], [150, 50], [-5, 0, 5], [0.9, 1.1])]:
+        t1, t2, b0, b1 = (np.asarray(v, np.float32) for v in (t1, t2, b0, b1))
+        np.testing.assert_array_equal(orc.trans_params(t1, t2, b0, b1), snap.trans_params(t1, t2, b0, b1))
+
+
+def test_fp64_gauss_newton_converges_to_the_noiseless_truth(oracle):
+    """The FP64 refinement (the checker of the GPU refinement's maps) walks
+    from a 5 % grid offset to the parameters a noiseless voxel was made with."""
+    from cases import mrf_schedule
+    T, w = 200, 20
+    h = mrf_schedule(T, seed=3)
+    for t1, t2, b1 in [(900.0, 60.0, 1.0), (1500.0, 200.0, 0.85)]:
+        s, _, _, _ = oracle.fisp_jvp((t1, t2, b1), (0, 0, 0), h, nstates=w)
+        x = (0.7 - 0.4j) * 1j * s
+        g1, g2, pd = oracle.refine_gn_f64((t1 * 1.05, t2 / 1.05, b1), x, h, nstates=w)
+        assert abs(g1 - t1) < 1e-6 * t1 and abs(g2 - t2) < 1e-6 * t2
+        assert abs(pd - abs(0.7 - 0.4j) * np.linalg.norm(s)) < 1e-9 * pd
