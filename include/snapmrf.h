@@ -216,6 +216,13 @@ int snapmrf_normalize(float *d_atoms, size_t nreps, size_t NATOMS, float *d_norm
  * real part makes the call's maps NaN and sets the device error word
  * (snapmrf_device_error() == 7).  Other precisions ignore the flag. */
 #define SNAPMRF_MATCH_IMAG_ATOMS 0x2u
+/* With a host image (img_on_host) and snapmrf_match_opts.img_device_copy:
+ * the image upload may start at once, before the work already queued on
+ * `stream` (such as the dictionary generation whose atoms this call
+ * matches) has finished, so that the two overlap.  The caller guarantees
+ * that no work queued before this call still uses img_device_copy (for
+ * instance by alternating two buffers between calls). */
+#define SNAPMRF_MATCH_UPLOAD_EARLY 0x4u
 
 typedef struct snapmrf_match_opts {
     int precision;          /* SNAPMRF_PREC_* */
@@ -261,11 +268,21 @@ typedef struct snapmrf_match_opts {
      * unit-norm atoms.  BF16 / FP16 with packed_atoms only (the candidates
      * come from the unit-norm packed operand). */
     const float *atom_norms;
+    /* Optional, device [nvoxels][nreps] complex, with a host image: the
+     * upload lands here and stays for the caller (for instance for
+     * snapmrf_refine_gn), instead of in scratch freed by the call. */
+    float *img_device_copy;
 } snapmrf_match_opts;
 
 /* d_maps: out, device [nvoxels][nmaps] (nmaps == 5, nparams == 4)
- * img: [nvoxels][img_stride] complex, host memory when img_on_host != 0
- * (page-locked host memory makes the upload asynchronous);
+ * img: [nvoxels][img_stride] complex, host memory when img_on_host != 0.
+ * A host image is copied in up to 8 chunks of at least 16 MB on a copy
+ * stream of the library (one per host thread and device); the FP32 form
+ * matches each chunk as soon as it has arrived, while the next ones are in
+ * flight, and the tensor-core forms start once the whole image is there.
+ * Page-locked host memory makes the copies asynchronous: the call then
+ * returns before they finish, so keep the host image unchanged until the
+ * call's work on `stream` has completed;
  * nreps time points are matched.  Per B1 block the first atom with the
  * largest |<atom, voxel>| wins; blocks are merged by nearest B1 when a B1
  * map is given (ties to the lower block, differences >= 10 to block 0),

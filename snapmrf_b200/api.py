@@ -37,6 +37,7 @@ PREC_FP16 = 2
 PREC_FP8 = 3
 MATCH_ASSUME_UNIFORM_B1 = 0x1
 MATCH_IMAG_ATOMS = 0x2
+MATCH_UPLOAD_EARLY = 0x4
 
 ECHO_TYPES = ("epg_ssfp", "roa_ssfp", "epg_sr", "epg_se", "epg_tse1", "epg_tse2", "epg_fisp")
 
@@ -62,7 +63,7 @@ class MatchOpts(C.Structure):
                 ("d_index", C.c_void_p), ("topk", C.c_int), ("packed_atoms", C.c_void_p),
                 ("packed_nreps", C.c_size_t), ("basis", C.c_void_p), ("basis_rows", C.c_size_t),
                 ("basis_stride", C.c_size_t), ("coeffs", C.c_void_p), ("coeff_stride", C.c_size_t),
-                ("rank", C.c_int), ("atom_norms", C.c_void_p)]
+                ("rank", C.c_int), ("atom_norms", C.c_void_p), ("img_device_copy", C.c_void_p)]
 
 
 class SvdOpts(C.Structure):
@@ -315,7 +316,7 @@ def MRF_match(d_maps, img, d_atoms, d_params, NREPS: int, nreps: int, NATOMS: in
               nvoxels: int, nparams: int = NPARAMS, nmaps: int = NMAPS, in_b1map=None, *,
               precision: int = PREC_FP32, flags: int = 0, img_stride: int = 0,
               d_index=None, topk: int = 0, packed_atoms=None, compressed=None, atom_norms=None,
-              stream=None) -> None:
+              img_device_copy=None, upload_early: bool = False, stream=None) -> None:
     """Template matching (src/functions.cu:1493-1584).
 
     img: host numpy complex64 [nvoxels][stride] or a device tensor; NREPS is
@@ -326,7 +327,11 @@ def MRF_match(d_maps, img, d_atoms, d_params, NREPS: int, nreps: int, NATOMS: in
     their candidates against them).
     atom_norms: device float32 [NATOMS], the norms of d_atoms when they are
     not normalised (MRF_dict with DICT_NORMALIZE_OPERAND); BF16 / FP16 with
-    packed_atoms only."""
+    packed_atoms only.
+    img_device_copy: with a host image, a device complex64 [nvoxels][nreps]
+    buffer that receives the uploaded image and keeps it (e.g. for
+    refine_gn); upload_early (needs it) lets the upload overlap the work
+    already queued on the stream, which must not use that buffer."""
     on_host = isinstance(img, np.ndarray) or (hasattr(img, "device") and img.device.type == "cpu")
     if isinstance(img, np.ndarray):
         img = np.ascontiguousarray(img, np.complex64)
@@ -350,7 +355,9 @@ def MRF_match(d_maps, img, d_atoms, d_params, NREPS: int, nreps: int, NATOMS: in
                      _ptr(packed_atoms), nreps if packed_atoms is not None else 0,
                      _ptr(cb.basis) if cb else None, cb.max_rank if cb else 0, cb.basis_stride if cb else 0,
                      _ptr(cb.coeffs) if cb else None, cb.coeff_stride if cb else 0, cb.rank if cb else 0,
-                     _ptr(atom_norms))
+                     _ptr(atom_norms), _ptr(img_device_copy))
+    if upload_early:
+        opts.flags |= MATCH_UPLOAD_EARLY
     _check(lib().snapmrf_mrf_match(_ptr(d_maps), _ptr(img), 1 if on_host else 0, _ptr(d_atoms),
                                    _ptr(d_params), nreps, NATOMS, natoms, nvoxels, nparams, nmaps,
                                    C.byref(opts), _stream_ptr(stream)))

@@ -16,6 +16,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <map>
 #include <vector>
 
 #include "common.h"
@@ -177,6 +178,63 @@ __global__ void publish_error_kernel(const int *err);
 
 static inline unsigned nblk(long long n, int t) { return (unsigned)((n + t - 1) / t); }
 
+// Copy stream and chunk events of the calling thread on the current device.
+struct UploadContext {
+    cudaStream_t stream = nullptr;
+    cudaEvent_t start = nullptr;
+    std::vector<cudaEvent_t> ev;
+};
+
+// Chunks of one host-image upload: chunk c covers voxels [first(c), first(c+1)).
+struct ImageUpload {
+    int nchunks = 0;
+    long long per = 0, nvox = 0;
+    const cudaEvent_t *ev = nullptr;
+    long long first(int c) const { return std::min(nvox, (long long)c * per); }
+    cudaEvent_t done() const { return ev[nchunks - 1]; }
+};
+
+constexpr int kMaxUploadChunks = 8;
+constexpr size_t kUploadChunkBytes = 16u << 20;
+
+// Enqueues the copy of nvox host rows (stride `stride` samples, nreps copied)
+// into dst [nvox][nreps] on the thread's copy stream, as up to
+// kMaxUploadChunks 2D copies of at least kUploadChunkBytes, each followed by
+// an event.  The copy stream first waits for the work already on `st`
+// unless `early`.
+static int upload_image(ImageUpload *up, float2 *dst, const float2 *src, size_t stride, size_t nreps,
+                        size_t nvox, bool early, cudaStream_t st) {
+    static thread_local std::map<int, UploadContext> ctx;
+    int dev = 0;
+    SNAPMRF_CUDA(cudaGetDevice(&dev));
+    UploadContext &u = ctx[dev];
+    if (!u.stream) {
+        SNAPMRF_CUDA(cudaStreamCreateWithFlags(&u.stream, cudaStreamNonBlocking));
+        SNAPMRF_CUDA(cudaEventCreateWithFlags(&u.start, cudaEventDisableTiming));
+        u.ev.resize(kMaxUploadChunks);
+        for (auto &e : u.ev) SNAPMRF_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    const size_t row = nreps * sizeof(float2);
+    const size_t total = row * nvox;
+    int n = (int)std::min<size_t>(kMaxUploadChunks, std::max<size_t>(1, total / kUploadChunkBytes));
+    up->nvox = (long long)nvox;
+    up->per = ((long long)nvox + n - 1) / n;
+    n = (int)(((long long)nvox + up->per - 1) / up->per);
+    up->nchunks = n;
+    up->ev = u.ev.data();
+    if (!early) {
+        SNAPMRF_CUDA(cudaEventRecord(u.start, st));
+        SNAPMRF_CUDA(cudaStreamWaitEvent(u.stream, u.start, 0));
+    }
+    for (int c = 0; c < n; c++) {
+        const long long v0 = up->first(c), nv = up->first(c + 1) - v0;
+        SNAPMRF_CUDA(cudaMemcpy2DAsync(dst + v0 * (long long)nreps, row, src + v0 * (long long)stride,
+                                       stride * sizeof(float2), row, (size_t)nv, cudaMemcpyHostToDevice, u.stream));
+        SNAPMRF_CUDA(cudaEventRecord(u.ev[c], u.stream));
+    }
+    return SNAPMRF_OK;
+}
+
 }  // namespace snapmrf
 
 using namespace snapmrf;
@@ -226,16 +284,30 @@ extern "C" int snapmrf_mrf_match(float *d_maps, const float *img, int img_on_hos
                          "MRF_match: compressed matching of several B1 blocks needs a B1 map (one basis per block)");
     }
 
-    // Image on the device: one strided 2D copy instead of one copy per voxel
-    // (src/functions.cu:1524-1530).
+    // A host image is streamed to the device in chunks on the library's copy
+    // stream (one 2D copy per chunk instead of one copy per voxel,
+    // src/functions.cu:1524-1530), into img_device_copy or call scratch; the
+    // FP32 form matches each chunk as it arrives, the tensor-core forms wait
+    // for the whole image.
+    float *img_copy = opts ? opts->img_device_copy : nullptr;
+    const bool early = (flags & SNAPMRF_MATCH_UPLOAD_EARLY) != 0;
+    if (img_copy && !img_on_host)
+        SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "MRF_match: img_device_copy applies to a host image (img_on_host)");
+    if (early && !img_copy)
+        SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "MRF_match: SNAPMRF_MATCH_UPLOAD_EARLY needs img_device_copy");
     DeviceScratch s_img;
     const float2 *d_img = reinterpret_cast<const float2 *>(img);
     long long istride = (long long)img_stride;
+    ImageUpload up;
     if (img_on_host) {
-        SNAPMRF_CUDA(s_img.alloc(nvoxels * nreps * sizeof(float2), st));
-        SNAPMRF_CUDA(cudaMemcpy2DAsync(s_img.ptr, nreps * sizeof(float2), img, img_stride * sizeof(float2),
-                                       nreps * sizeof(float2), nvoxels, cudaMemcpyHostToDevice, st));
-        d_img = s_img.as<float2>();
+        float2 *dst = reinterpret_cast<float2 *>(img_copy);
+        if (!dst) {
+            SNAPMRF_CUDA(s_img.alloc(nvoxels * nreps * sizeof(float2), st));
+            dst = s_img.as<float2>();
+        }
+        int rc = upload_image(&up, dst, reinterpret_cast<const float2 *>(img), img_stride, nreps, nvoxels, early, st);
+        if (rc) return rc;
+        d_img = dst;
         istride = (long long)nreps;
     }
     DeviceScratch s_b1;
@@ -301,137 +373,162 @@ extern "C" int snapmrf_mrf_match(float *d_maps, const float *img, int img_on_hos
         q.topk = (opts && opts->topk) ? opts->topk : (q.fmt == 1 ? 4 : 16);
         if (q.topk != 4 && q.topk != 8 && q.topk != 16)
             SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "MRF_match: topk must be 4, 8 or 16 (got %d)", q.topk);
+        if (img_on_host) SNAPMRF_CUDA(cudaStreamWaitEvent(st, up.done(), 0));
         return match_bf16(q, st);
     }
     // the FP32 kernels carry an atom's index within its bin as an int
     if (!d_b1 && NATOMS >= 0x7fffffffull)
         SNAPMRF_FAIL(SNAPMRF_ERR_UNSUPPORTED,
                      "MRF_match: FP32 matching without a B1 map takes fewer than 2^31 - 1 atoms (got %zu)", NATOMS);
-    int nbins;
-    long long per_bin_atoms, nslots;
-    if (!d_b1) {
-        nbins = 1;
-        per_bin_atoms = (long long)NATOMS;
-        nslots = nvox;
-    } else if (!general) {
-        nbins = (int)nblocks;
-        per_bin_atoms = (long long)natoms;
-        nslots = nvox;
-    } else {
-        nbins = (int)nblocks;
-        per_bin_atoms = (long long)natoms;
-        nslots = nvox * (long long)nblocks;
-    }
+    // The FP32 path over voxels [v0, v0 + nvox): a host image streamed in
+    // chunks is matched chunk by chunk as each chunk arrives.
+    auto fp32_range = [&](long long v0, long long nvox, float *d_maps, int64_t *d_index, const float2 *d_img,
+                          const float *d_b1) -> int {
+        (void)v0;
+        int nbins;
+        long long per_bin_atoms, nslots;
+        if (!d_b1) {
+            nbins = 1;
+            per_bin_atoms = (long long)NATOMS;
+            nslots = nvox;
+        } else if (!general) {
+            nbins = (int)nblocks;
+            per_bin_atoms = (long long)natoms;
+            nslots = nvox;
+        } else {
+            nbins = (int)nblocks;
+            per_bin_atoms = (long long)natoms;
+            nslots = nvox * (long long)nblocks;
+        }
 
-    // purely imaginary atoms: half the products (the imaginary parts only)
-    const bool imag = (flags & SNAPMRF_MATCH_IMAG_ATOMS) != 0;
-    // scratch: keys[nslots] u64 | perm[nvox] i64 | slot_start, tile_start,
-    // cursor [nbins+1] i64 | vox_bin[nvox] i32 | counts[nbins] i32 | err i32
-    size_t bytes = (size_t)nslots * 8 + (size_t)nvox * 8 + 3 * (size_t)(nbins + 1) * 8 +
-                   (size_t)nvox * 4 + (size_t)nbins * 4 + 64;
-    DeviceScratch s_work;
-    SNAPMRF_CUDA(s_work.alloc(bytes, st));
-    unsigned long long *keys = s_work.as<unsigned long long>();
-    long long *perm = reinterpret_cast<long long *>(keys + nslots);
-    long long *slot_start = perm + nvox;
-    long long *tile_start = slot_start + (nbins + 1);
-    long long *cursor = tile_start + (nbins + 1);
-    int *vox_bin = reinterpret_cast<int *>(cursor + (nbins + 1));
-    int *counts = vox_bin + nvox;
-    int *err = counts + nbins;
-    SNAPMRF_CUDA(cudaMemsetAsync(keys, 0, (size_t)nslots * 8, st));
-    if (imag) SNAPMRF_CUDA(cudaMemsetAsync(err, 0, sizeof(int), st));
+        // purely imaginary atoms: half the products (the imaginary parts only)
+        const bool imag = (flags & SNAPMRF_MATCH_IMAG_ATOMS) != 0;
+        // scratch: keys[nslots] u64 | perm[nvox] i64 | slot_start, tile_start,
+        // cursor [nbins+1] i64 | vox_bin[nvox] i32 | counts[nbins] i32 | err i32
+        size_t bytes = (size_t)nslots * 8 + (size_t)nvox * 8 + 3 * (size_t)(nbins + 1) * 8 +
+                       (size_t)nvox * 4 + (size_t)nbins * 4 + 64;
+        DeviceScratch s_work;
+        SNAPMRF_CUDA(s_work.alloc(bytes, st));
+        unsigned long long *keys = s_work.as<unsigned long long>();
+        long long *perm = reinterpret_cast<long long *>(keys + nslots);
+        long long *slot_start = perm + nvox;
+        long long *tile_start = slot_start + (nbins + 1);
+        long long *cursor = tile_start + (nbins + 1);
+        int *vox_bin = reinterpret_cast<int *>(cursor + (nbins + 1));
+        int *counts = vox_bin + nvox;
+        int *err = counts + nbins;
+        SNAPMRF_CUDA(cudaMemsetAsync(keys, 0, (size_t)nslots * 8, st));
+        if (imag) SNAPMRF_CUDA(cudaMemsetAsync(err, 0, sizeof(int), st));
 
-    MatchArgs m;
-    m.atoms = reinterpret_cast<const float2 *>(d_atoms);
-    m.atom_stride = (long long)atom_stride;
-    m.img = d_img;
-    m.img_stride = istride;
-    m.nreps = (long long)nreps;
-    m.nbins = nbins;
-    m.bin_natoms = per_bin_atoms;
-    m.nvox = nvox;
-    m.keys = keys;
-    m.err = imag ? err : nullptr;
+        MatchArgs m;
+        m.atoms = reinterpret_cast<const float2 *>(d_atoms);
+        m.atom_stride = (long long)atom_stride;
+        m.img = d_img;
+        m.img_stride = istride;
+        m.nreps = (long long)nreps;
+        m.nbins = nbins;
+        m.bin_natoms = per_bin_atoms;
+        m.nvox = nvox;
+        m.keys = keys;
+        m.err = imag ? err : nullptr;
 
-    if (!d_b1) {
-        // one bin, identity permutation
-        uniform_bins_kernel<<<1, 256, 0, st>>>(slot_start, tile_start, 1, nvox,
-                                               (nvox + kMatchVT - 1) / kMatchVT);
-        SNAPMRF_LAUNCH_CHECK();
-        m.perm = nullptr;
-        m.perm_mod = 0;
-    } else if (!general) {
-        SNAPMRF_CUDA(cudaMemsetAsync(counts, 0, (size_t)nbins * 4, st));
-        assign_bins_kernel<<<nblk(nvox, 256), 256, 0, st>>>(vox_bin, counts, d_b1, d_params, nparams,
-                                                            (long long)natoms, nbins, nvox);
-        SNAPMRF_LAUNCH_CHECK();
-        scan_bins_kernel<<<1, 32, 0, st>>>(counts, slot_start, tile_start, cursor, nbins);
-        SNAPMRF_LAUNCH_CHECK();
-        scatter_bins_kernel<<<nblk(nvox, 256), 256, 0, st>>>(perm, cursor, vox_bin, nvox);
-        SNAPMRF_LAUNCH_CHECK();
-        m.perm = perm;
-        m.perm_mod = 0;
-    } else {
-        uniform_bins_kernel<<<nblk(nbins + 1, 256), 256, 0, st>>>(slot_start, tile_start, nbins, nvox,
-                                                                  (nvox + kMatchVT - 1) / kMatchVT);
-        SNAPMRF_LAUNCH_CHECK();
-        m.perm = nullptr;
-        m.perm_mod = nvox;
-    }
-    m.slot_start = slot_start;
-    m.tile_start = tile_start;
+        if (!d_b1) {
+            // one bin, identity permutation
+            uniform_bins_kernel<<<1, 256, 0, st>>>(slot_start, tile_start, 1, nvox,
+                                                   (nvox + kMatchVT - 1) / kMatchVT);
+            SNAPMRF_LAUNCH_CHECK();
+            m.perm = nullptr;
+            m.perm_mod = 0;
+        } else if (!general) {
+            SNAPMRF_CUDA(cudaMemsetAsync(counts, 0, (size_t)nbins * 4, st));
+            assign_bins_kernel<<<nblk(nvox, 256), 256, 0, st>>>(vox_bin, counts, d_b1, d_params, nparams,
+                                                                (long long)natoms, nbins, nvox);
+            SNAPMRF_LAUNCH_CHECK();
+            scan_bins_kernel<<<1, 32, 0, st>>>(counts, slot_start, tile_start, cursor, nbins);
+            SNAPMRF_LAUNCH_CHECK();
+            scatter_bins_kernel<<<nblk(nvox, 256), 256, 0, st>>>(perm, cursor, vox_bin, nvox);
+            SNAPMRF_LAUNCH_CHECK();
+            m.perm = perm;
+            m.perm_mod = 0;
+        } else {
+            uniform_bins_kernel<<<nblk(nbins + 1, 256), 256, 0, st>>>(slot_start, tile_start, nbins, nvox,
+                                                                      (nvox + kMatchVT - 1) / kMatchVT);
+            SNAPMRF_LAUNCH_CHECK();
+            m.perm = nullptr;
+            m.perm_mod = nvox;
+        }
+        m.slot_start = slot_start;
+        m.tile_start = tile_start;
 
-    // Compressed: score the rank-r coordinates of the atoms against the
-    // voxels projected onto their bin's basis; the maps' PD is the
-    // compressed |s|.
-    DeviceScratch s_cimg;
-    if (comp) {
-        const long long rs = (opts->rank + 1) & ~1ll;
-        SNAPMRF_CUDA(s_cimg.alloc((size_t)nvox * rs * sizeof(float2), st));
-        int rc = project_voxels(s_cimg.as<float2>(), rs, d_img, istride, nvox, (long long)nreps,
-                                d_b1 ? vox_bin : nullptr, nbins, reinterpret_cast<const float2 *>(opts->basis),
-                                (long long)opts->basis_rows, (long long)opts->basis_stride, opts->rank,
-                                (flags & SNAPMRF_MATCH_IMAG_ATOMS) != 0, st);
-        if (rc) return rc;
-        m.img = s_cimg.as<float2>();
-        m.img_stride = rs;
-        m.atoms = reinterpret_cast<const float2 *>(opts->coeffs);
-        m.atom_stride = (long long)opts->coeff_stride;
-        m.nreps = opts->rank;
-    }
+        // Compressed: score the rank-r coordinates of the atoms against the
+        // voxels projected onto their bin's basis; the maps' PD is the
+        // compressed |s|.
+        DeviceScratch s_cimg;
+        if (comp) {
+            const long long rs = (opts->rank + 1) & ~1ll;
+            SNAPMRF_CUDA(s_cimg.alloc((size_t)nvox * rs * sizeof(float2), st));
+            int rc = project_voxels(s_cimg.as<float2>(), rs, d_img, istride, nvox, (long long)nreps,
+                                    d_b1 ? vox_bin : nullptr, nbins, reinterpret_cast<const float2 *>(opts->basis),
+                                    (long long)opts->basis_rows, (long long)opts->basis_stride, opts->rank,
+                                    (flags & SNAPMRF_MATCH_IMAG_ATOMS) != 0, st);
+            if (rc) return rc;
+            m.img = s_cimg.as<float2>();
+            m.img_stride = rs;
+            m.atoms = reinterpret_cast<const float2 *>(opts->coeffs);
+            m.atom_stride = (long long)opts->coeff_stride;
+            m.nreps = opts->rank;
+        }
 
-    long long max_tiles = general ? (long long)nbins * ((nvox + kMatchVT - 1) / kMatchVT)
-                                  : (nvox + kMatchVT - 1) / kMatchVT + nbins;
-    long long est_tiles = general ? max_tiles : (nvox + kMatchVT - 1) / kMatchVT;
-    dim3 grid = fp32_match_grid(m, est_tiles, max_tiles);
-    SNAPMRF_CUDA(launch_match_fp32(m, grid, imag, st));
+        long long max_tiles = general ? (long long)nbins * ((nvox + kMatchVT - 1) / kMatchVT)
+                                      : (nvox + kMatchVT - 1) / kMatchVT + nbins;
+        long long est_tiles = general ? max_tiles : (nvox + kMatchVT - 1) / kMatchVT;
+        dim3 grid = fp32_match_grid(m, est_tiles, max_tiles);
+        SNAPMRF_CUDA(launch_match_fp32(m, grid, imag, st));
 
-    const unsigned long long *fkeys = keys;
-    if (general) {
-        DeviceScratch s_merged;
-        SNAPMRF_CUDA(s_merged.alloc((size_t)nvox * 8, st));
-        merge_nearest_b1_kernel<<<nblk(nvox, 256), 256, 0, st>>>(s_merged.as<unsigned long long>(), vox_bin,
-                                                                 keys, d_b1, d_params, nparams,
-                                                                 (long long)natoms, nbins, nvox);
-        SNAPMRF_LAUNCH_CHECK();
+        const unsigned long long *fkeys = keys;
+        if (general) {
+            DeviceScratch s_merged;
+            SNAPMRF_CUDA(s_merged.alloc((size_t)nvox * 8, st));
+            merge_nearest_b1_kernel<<<nblk(nvox, 256), 256, 0, st>>>(s_merged.as<unsigned long long>(), vox_bin,
+                                                                     keys, d_b1, d_params, nparams,
+                                                                     (long long)natoms, nbins, nvox);
+            SNAPMRF_LAUNCH_CHECK();
+            finalize_maps_kernel<<<nblk(nvox * 32, 256), 256, 0, st>>>(
+                d_maps, (long long *)d_index, s_merged.as<unsigned long long>(), nullptr, vox_bin,
+                m.atoms, m.atom_stride, d_img, istride, (long long)nreps, d_params, nparams,
+                (long long)natoms, nvox);
+            SNAPMRF_LAUNCH_CHECK();
+            if (imag) {
+                poison_maps_kernel<<<nblk(nvox, 256), 256, 0, st>>>(d_maps, (long long *)d_index, nvox, err);
+                SNAPMRF_LAUNCH_CHECK();
+                tc::publish_error_kernel<<<1, 1, 0, st>>>(err);
+                SNAPMRF_LAUNCH_CHECK();
+            }
+            return SNAPMRF_OK;
+        }
         finalize_maps_kernel<<<nblk(nvox * 32, 256), 256, 0, st>>>(
-            d_maps, (long long *)d_index, s_merged.as<unsigned long long>(), nullptr, vox_bin,
-            m.atoms, m.atom_stride, d_img, istride, (long long)nreps, d_params, nparams,
-            (long long)natoms, nvox);
+            d_maps, (long long *)d_index, fkeys, d_b1 ? perm : nullptr, d_b1 ? vox_bin : nullptr, m.atoms,
+            m.atom_stride, m.img, m.img_stride, m.nreps, d_params, nparams, per_bin_atoms, nvox);
         SNAPMRF_LAUNCH_CHECK();
+        if (imag) {
+            // an atom with a real part: NaN maps, indices -1, error word 7
+            poison_maps_kernel<<<nblk(nvox, 256), 256, 0, st>>>(d_maps, (long long *)d_index, nvox, err);
+            SNAPMRF_LAUNCH_CHECK();
+            tc::publish_error_kernel<<<1, 1, 0, st>>>(err);
+            SNAPMRF_LAUNCH_CHECK();
+        }
         return SNAPMRF_OK;
+    };
+    if (!img_on_host || up.nchunks <= 1 || comp || general) {
+        if (img_on_host) SNAPMRF_CUDA(cudaStreamWaitEvent(st, up.done(), 0));
+        return fp32_range(0, nvox, d_maps, d_index, d_img, d_b1);
     }
-    finalize_maps_kernel<<<nblk(nvox * 32, 256), 256, 0, st>>>(
-        d_maps, (long long *)d_index, fkeys, d_b1 ? perm : nullptr, d_b1 ? vox_bin : nullptr, m.atoms,
-        m.atom_stride, m.img, m.img_stride, m.nreps, d_params, nparams, per_bin_atoms, nvox);
-    SNAPMRF_LAUNCH_CHECK();
-    if (imag) {
-        // an atom with a real part: NaN maps, indices -1, error word 7
-        poison_maps_kernel<<<nblk(nvox, 256), 256, 0, st>>>(d_maps, (long long *)d_index, nvox, err);
-        SNAPMRF_LAUNCH_CHECK();
-        tc::publish_error_kernel<<<1, 1, 0, st>>>(err);
-        SNAPMRF_LAUNCH_CHECK();
+    for (int c = 0; c < up.nchunks; c++) {
+        const long long v0 = up.first(c), n = up.first(c + 1) - v0;
+        SNAPMRF_CUDA(cudaStreamWaitEvent(st, up.ev[c], 0));
+        int rc = fp32_range(v0, n, d_maps + 5 * v0, d_index ? d_index + v0 : nullptr, d_img + v0 * istride,
+                            d_b1 ? d_b1 + v0 : nullptr);
+        if (rc) return rc;
     }
     return SNAPMRF_OK;
 }

@@ -198,3 +198,59 @@ def test_fp32_imaginary_atom_form_rejects_complex_atoms(snap, oracle):
     maps, got = run_match(snap, img, atoms, params, flags=snap.MATCH_IMAG_ATOMS)
     assert snap.device_error(reset=True) == 7
     assert np.isnan(maps).all() and (got == -1).all()
+
+
+@pytest.mark.parametrize("prec", [0, 2])
+def test_host_image_streamed_in_chunks(snap, oracle, prec):
+    """A host image of 43 MB (three 16 MB chunks) with padded rows: the
+    library streams it to the device chunk by chunk on its copy stream and
+    (FP32) matches each chunk as it arrives; maps and indices equal the
+    device-image call's bit for bit, with and without a B1 map, pageable and
+    page-locked, and img_device_copy keeps the uploaded rows.  The
+    tensor-core form with SNAPMRF_MATCH_UPLOAD_EARLY (the upload overlapping
+    the work already queued) gives the same maps too."""
+    import torch
+    T = 600
+    b1s = np.float32([0.8, 1.0, 1.2])
+    atoms, params, natoms = _dictionary(snap, oracle, b1s=b1s, T=T)
+    nvox = 9000
+    img = np.zeros((nvox, T + 3), np.complex64)
+    img[:, :T] = _voxels(atoms, nvox, 21)
+    b1map = np.random.default_rng(22).uniform(0.7, 1.3, nvox).astype(np.float32)
+    d_atoms = torch.from_numpy(atoms.view(np.float32)).cuda()
+    d_params = torch.from_numpy(params).cuda()
+    d_img = torch.from_numpy(np.ascontiguousarray(img).view(np.float32)).cuda()
+    h_pinned = torch.from_numpy(np.ascontiguousarray(img).view(np.float32)).pin_memory()
+    flags = snap.MATCH_IMAG_ATOMS | snap.MATCH_ASSUME_UNIFORM_B1
+    for b1 in (None, torch.from_numpy(b1map).cuda()):
+        out = {}
+        for name, src in (("device", d_img), ("pageable", img), ("pinned", h_pinned)):
+            maps = torch.full((nvox, 5), -1.0, device="cuda")
+            idx = torch.full((nvox,), -1, dtype=torch.int64, device="cuda")
+            copy = torch.zeros((nvox, T, 2), device="cuda") if name != "device" else None
+            snap.MRF_match(maps, src, d_atoms, d_params, T, T, params.shape[0], natoms, nvox, in_b1map=b1,
+                           precision=prec, flags=flags, d_index=idx, img_stride=T + 3, img_device_copy=copy,
+                           upload_early=(prec != 0 and copy is not None))
+            torch.cuda.synchronize()
+            out[name] = (maps.cpu().numpy(), idx.cpu().numpy())
+            if copy is not None:
+                c = copy.cpu().numpy()
+                np.testing.assert_array_equal(c[..., 0] + 1j * c[..., 1], img[:, :T])
+        assert snap.device_error(reset=True) == 0
+        for name in ("pageable", "pinned"):
+            np.testing.assert_array_equal(out[name][1], out["device"][1])
+            np.testing.assert_array_equal(out[name][0], out["device"][0])
+
+
+def test_streamed_upload_options_are_checked(snap, oracle):
+    import torch
+    atoms, params, natoms = _dictionary(snap, oracle, nb1=1, T=64)
+    img = _voxels(atoms, 10, 23)
+    d_atoms = torch.from_numpy(atoms.view(np.float32)).cuda()
+    d_params = torch.from_numpy(params).cuda()
+    maps = torch.empty((10, 5), device="cuda")
+    with pytest.raises(snap.SnapMRFError, match="UPLOAD_EARLY needs img_device_copy"):
+        snap.MRF_match(maps, img, d_atoms, d_params, 64, 64, params.shape[0], natoms, 10, upload_early=True)
+    with pytest.raises(snap.SnapMRFError, match="applies to a host image"):
+        snap.MRF_match(maps, torch.from_numpy(img.view(np.float32)).cuda(), d_atoms, d_params, 64, 64,
+                       params.shape[0], natoms, 10, img_device_copy=torch.empty((10, 64, 2), device="cuda"))
