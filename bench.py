@@ -1,38 +1,53 @@
-"""Benchmark of the snapMRF hot path on B200: dictionary generation + B1-bin
-matching for one 240x240 B1-mapped MR-fingerprinting slice.
+"""Benchmark of the snapMRF hot path on B200: dictionary generation, matching
+and Gauss-Newton refinement of MR-fingerprinting images.
 
-Workload "fisp_b1map_240x240" (the full-size plain FP32 EPG-FISP form):
+Workload "fisp_b1map_240x240" (default; the full-size EPG-FISP form with a
+B1 map, and its BF16 + refine precision form):
   schedule  T = 1000, alpha_t = 10 + 50|sin(pi t / 250)| deg with alpha_0 =
             180 deg (inversion), phase 0, TR_t ~ U[11, 15] ms (seed 1),
             TE = TR / 2
   grid      T1 = 100 * 1.05^k <= 5000 ms (81) x T2 = 10 * 1.05^k <= 2000 ms
             (109), T1 > T2 -> 6938 pairs, x B1 = 0.60:0.02:1.40 (41 blocks)
-            = 284,458 atoms, w = 50 EPG states, atoms normalised
+            = 284,458 atoms, w = 50 EPG states
   voxels    240 x 240; B1 map 1 + 0.3 (x^2 + y^2 - 0.5) clipped to
             [0.6, 1.4]; 5 seeded elliptical tissue regions, +-5 % per-voxel
             T1/T2 jitter, M0 ~ U[0.6, 1], random phase, complex Gaussian
             noise at SNR 40 (sigma = ||s|| / sqrt(T) / 40); each voxel is
             matched within its nearest B1 block
-One step = MRF_dict (all 41 blocks) + MRF_match of every voxel, the two
-calls the reference's mrf CLI makes.  `value` is voxels/s with inputs
-resident in HBM; `e2e` runs the same step through the public API from pinned
-host buffers with the uploads and the map download inside the timed region.
+One step = MRF_dict (all 41 blocks) + MRF_match of every voxel (+ the
+Gauss-Newton refinement in the refined forms).  The headline form is the
+metric's own: BF16 matching with the top-16 rescored in FP32, then at most
+three Gauss-Newton iterations per voxel; `forms` times every other form
+(FP32, FP16, FP8, each tensor-core form with and without refinement) in the
+same run.  `value` is voxels/s with inputs resident in HBM; `e2e` runs the
+same step through the public API from pinned host buffers (parameter table,
+image and B1 map up, maps down) with the copies inside the timed region.
 Every input and output exceeds L2 (dictionary 2.28 GB, image 461 MB), so no
 flush is needed between steps.
+
+Workload "ssfp_b0_256x256x8" (--workload): the large bSSFP configuration
+with off-resonance: T = 500, alpha_t = 5 + 55|sin(pi t / 200)| deg, RF phase
+alternating 0 / 180 deg, TR_t ~ U[10, 14] ms, TE = TR / 2; the T1 / T2 grid
+above x B0 = -100:4:100 Hz x B1 = 0.8:0.1:1.2 = 1,769,190 atoms, w = 50; an
+EPG-SSFP dictionary and an ROA dictionary with 100 isochromats; 256 x 256 x 8
+voxels with a smooth B0 field (+-80 Hz, linear + quadratic) and tissue
+regions as above, matched without a B1 map (global MIP, the reference's
+max-PD merge).
 
 Multi-GPU (torchrun, one process per GPU): rank r processes its own slice
 (seeded by r) end to end, with no data-path collective; timing is the max
 over ranks of each rank's CUDA-event time.
 
 --impl reference times the reference algorithm's CPU implementation (the
-oracle, C, OpenMP over all host cores) on a bounded sample of the same
-workload and reports the same metric.
+oracle, C, OpenMP over all host cores): each step is one of the workload's
+41 B1 blocks (its 6,938 atoms generated, and 1/41 of the voxels matched
+against them), so the throughput it reports is measured, not extrapolated.
 """
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
-import math
 import os
 import subprocess
 import sys
@@ -46,24 +61,34 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 WORKLOAD = "fisp_b1map_240x240"
+WORKLOAD_C4 = "ssfp_b0_256x256x8"
+METRIC = "dict atoms/s + matched voxels/s (BF16+refine vs FP32, ≤1% T1/T2 err)"
 T = 1000
 NSTATES = 50
 NX = NY = 240
 SNR = 40.0
-# Algorithmic work of the dictionary per EPG state and time step, by the
-# fixed convention of the complex recursion: RF 54 + two relaxations 6 + 6.
+# Work per EPG state and time step.  Convention (the complex recursion):
+# RF 54 + two relaxations 6 + 6 flop.  Executed by the real-valued recursion
+# with every RF phase 0 and each relaxation folded into the next RF: eight
+# FP32-pipe operations (5 FMA, 2 multiplies, 1 add), 16 flop at the pipe's
+# rate of 2 flop per operation.
 FLOP_PER_STATE_STEP = 66
-# Work the real-valued recursion actually executes when every RF phase is 0
-# (this schedule) with each relaxation folded into the next RF: the RF's 8
-# FP32-pipe operations per state and step (5 FMA, 2 multiplies, 1 add),
-# counted as 2 flop each, the pipe's rate (plus 10 operations per lane and
-# step for the folded coefficients).
 FLOP_PER_STATE_STEP_EXECUTED = 16
-# DRAM bytes per dictionary atom of the headline form (T = 1000, w = 50, the
-# FP16 matching operand normalised, the FP32 atoms as generated) measured by
-# ncu on the reduced workload (5 B1 blocks, 34,690 atoms: 241.1 MB read +
-# 306.0 MB written in one launch); traffic grows with the atom count, so a
-# full launch moves this times NATOMS.
+# Gauss-Newton pass (signal + dT1 + dT2 tangents, packed two-wide): per state
+# and step 3 x 8 RF operations, 3 shift masks and 12 relaxation operations
+# with the tangents' product-rule terms = 39 FP32-pipe operations, 78 flop
+# at the pipe's rate.
+GN_FLOP_PER_STATE_STEP = 78
+# bSSFP (complex recursion with B0 precession), convention: RF 54 + two
+# relaxations 12 + two B0 precessions 24 flop; ROA: 31 flop per isochromat
+# and step.
+SSFP_FLOP_PER_STATE_STEP = 90
+ROA_FLOP_PER_ISO_STEP = 31
+# DRAM bytes per dictionary atom of the headline dictionary form (T = 1000,
+# w = 50, the 16-bit matching operand of the unit-norm atoms, FP32 atoms as
+# generated) measured by ncu on the reduced workload (5 B1 blocks, 34,690
+# atoms: 241.1 MB read + 306.0 MB written in one launch); traffic grows with
+# the atom count, so a full launch moves this times NATOMS.
 DICT_DRAM_BYTES_PER_ATOM = (241.051904e6 + 305.966080e6) / 34690
 PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
 
@@ -82,11 +107,14 @@ def schedule(seed: int = 1) -> np.ndarray:
     return np.array([np.deg2rad(a), np.zeros(T), tr, tr / 2], np.float32)
 
 
+def geometric(lo: float, hi: float) -> np.ndarray:
+    return np.array([lo * 1.05 ** k for k in range(400) if lo * 1.05 ** k <= hi], np.float32)
+
+
 def grid(b1_blocks: int = 41):
     """T1 / T2 / B0 / B1 grids; b1_blocks < 41 keeps the blocks nearest 1.0
     (a reduced case of the same workload, used for profiling)."""
-    t1 = np.array([100.0 * 1.05 ** k for k in range(200) if 100.0 * 1.05 ** k <= 5000.0], np.float32)
-    t2 = np.array([10.0 * 1.05 ** k for k in range(200) if 10.0 * 1.05 ** k <= 2000.0], np.float32)
+    t1, t2 = geometric(100.0, 5000.0), geometric(10.0, 2000.0)
     b1 = np.array([0.60 + 0.02 * k for k in range(41)], np.float32)
     if b1_blocks < 41:
         c = 20 - b1_blocks // 2
@@ -95,8 +123,8 @@ def grid(b1_blocks: int = 41):
 
 
 def phantom(seed: int, nx: int = NX):
-    """B1 map, true (T1, T2) and M0 per voxel (Fortran voxel order like the
-    reference's RA images: x fastest)."""
+    """B1 map, true (T1, T2), M0 and phase per voxel (Fortran voxel order
+    like the reference's RA images: x fastest)."""
     rng = np.random.default_rng(1000 + seed)
     y, x = np.meshgrid(np.linspace(-1, 1, nx), np.linspace(-1, 1, nx), indexing="ij")
     b1 = np.clip(1.0 + 0.3 * (x ** 2 + y ** 2 - 0.5), 0.6, 1.4).astype(np.float32)
@@ -118,6 +146,13 @@ def phantom(seed: int, nx: int = NX):
             m0.reshape(-1), ph.reshape(-1))
 
 
+def add_noise(sig: np.ndarray, seed: int, nreps: int) -> np.ndarray:
+    rng = np.random.default_rng(2000 + seed)
+    sigma = np.linalg.norm(sig, axis=1, keepdims=True) / np.sqrt(nreps) / SNR
+    noise = sigma / np.sqrt(2) * (rng.standard_normal(sig.shape) + 1j * rng.standard_normal(sig.shape))
+    return (sig + noise).astype(np.complex64)
+
+
 def make_inputs(snap, torch, seed: int, b1_blocks: int = 41, nx: int = NX):
     """Host inputs of one slice: (h_mrf, params, natoms, img, b1map, truth)."""
     h_mrf = schedule(1)
@@ -137,10 +172,7 @@ def make_inputs(snap, torch, seed: int, b1_blocks: int = 41, nx: int = NX):
     torch.cuda.synchronize()
     sig = d_sig.cpu().numpy()
     sig = (sig[..., 0] + 1j * sig[..., 1]) * (m0 * np.exp(1j * ph))[:, None]
-    rng = np.random.default_rng(2000 + seed)
-    sigma = np.linalg.norm(sig, axis=1, keepdims=True) / np.sqrt(T) / SNR
-    noise = sigma / np.sqrt(2) * (rng.standard_normal(sig.shape) + 1j * rng.standard_normal(sig.shape))
-    img = (sig + noise).astype(np.complex64)
+    img = add_noise(sig, seed, T)
     del d_sig, d_vp
     return h_mrf, params, natoms, img, b1map, (vt1, vt2, m0)
 
@@ -275,8 +307,27 @@ def peaks() -> dict:
     if PEAKS_FILE.exists():
         p = json.loads(PEAKS_FILE.read_text())
         return {"hbm_gbs": p.get("hbm_gbs"), "bf16_tflops": p.get("bf16_tflops"),
+                "bf16_tflops_sustained": p.get("bf16_tflops_sustained"),
                 "sm_max_mhz": p.get("sm_max_mhz", 1965.0), "source": "measured"}
-    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0, "source": "fallback"}
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0, "sm_max_mhz": 1965.0,
+            "source": "fallback"}
+
+
+def fp32_fma_peak() -> tuple[float, str]:
+    """FP32 FMA throughput measured on this GPU by the probe library (best of
+    5 launches of independent FMA chains), else the nominal 148 SMs x 128
+    lanes x 2 flop x 1.965 GHz."""
+    lib = ROOT / "snapmrf_b200" / "libsnapmrf_probe.so"
+    if lib.exists():
+        try:
+            L = ctypes.CDLL(str(lib))
+            L.snapmrf_probe_fp32_fma.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+            v = ctypes.c_double(0)
+            if L.snapmrf_probe_fp32_fma(5, ctypes.byref(v)) == 0 and v.value > 0:
+                return round(v.value, 2), "measured (FMA chains, best of 5)"
+        except OSError:
+            pass
+    return round(148 * 128 * 2 * 1.965e9 / 1e12, 2), "nominal"
 
 
 def reduce_over_ranks(values, op: str, device, world: int) -> list:
@@ -291,20 +342,68 @@ def reduce_over_ranks(values, op: str, device, world: int) -> list:
     return t.tolist()
 
 
-def fp32_peak_tflops(sm_mhz: float) -> float:
-    """FP32 FMA peak of 148 SMs x 128 lanes x 2 flop at the given clock."""
-    return 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
+def roofline(kernel: str, bound: str, flop: float, ms: float, peak: float, peak_note: str, **extra) -> dict:
+    """achieved = executed flop / duration; frac = achieved / peak."""
+    ach = flop / (ms / 1e3) / 1e12
+    r = {"kernel": kernel, "bound": bound, "achieved": round(ach, 2), "peak": round(peak, 2), "unit": "TFLOP/s",
+         "frac": round(ach / peak, 4), "peak_note": peak_note, "ms": round(ms, 3),
+         "executed_flop_per_launch": flop}
+    r.update(extra)
+    return r
+
+
+def median_rel(a, b) -> float:
+    return float(np.median(np.abs(np.asarray(a, np.float64) - b) / np.abs(b)))
+
+
+# ---------------------------------------------------------------------------
+# the FP64 oracle on a sample of voxels
+# ---------------------------------------------------------------------------
+
+def oracle_maps_sample(h_mrf, params, natoms, img, b1map, nsample: int, seed: int = 5):
+    """(voxel indices, T1, T2) of the FP64 oracle's pipeline on a sample:
+    each voxel matched within its nearest B1 block against an FP64 dictionary
+    of that block (first argmax of |<d, x>| on unit-norm atoms), then FP64
+    Gauss-Newton to convergence.  The sample is drawn from the two blocks
+    holding the most voxels."""
+    from concurrent.futures import ThreadPoolExecutor
+    from oracle import oracle as orc
+    nthr = orc.max_threads()
+    nb = params.shape[0] // natoms
+    heads = params[np.arange(nb) * natoms, 3]
+    blk = np.argmin(np.abs(b1map[:, None] - heads[None, :]), axis=1)
+    top = np.argsort(np.bincount(blk, minlength=nb))[::-1][:2]
+    rng = np.random.default_rng(seed)
+    picks = []
+    for b in top:
+        cand = np.flatnonzero(blk == b)
+        picks.append(rng.choice(cand, min(nsample // 2, cand.size), replace=False))
+    sel = np.concatenate(picks)
+    start = []
+    for b, p in zip(top, picks):
+        bp = params[b * natoms:(b + 1) * natoms]
+        d = orc.dict_atoms("epg_fisp", bp, h_mrf, T, natoms=natoms, nstates=NSTATES, precision="f64",
+                           flags=orc.ALL_B1_BLOCKS | orc.NORMALIZE, nthreads=nthr)
+        s = np.abs(img[p].astype(np.complex128) @ d.conj().T)
+        j = np.argmax(s, axis=1)
+        start += [(float(bp[k, 0]), float(bp[k, 1]), float(b1map[v])) for k, v in zip(j, p)]
+
+    def fit(i):
+        return orc.refine_gn_f64(start[i], img[sel[i]].astype(np.complex128), h_mrf, nstates=NSTATES)
+    with ThreadPoolExecutor(max_workers=nthr) as ex:
+        res = list(ex.map(fit, range(sel.size)))
+    t1 = np.array([r[0] for r in res])
+    t2 = np.array([r[1] for r in res])
+    return sel, t1, t2
 
 
 # ---------------------------------------------------------------------------
 # arms
 # ---------------------------------------------------------------------------
 
-def run_ours(args) -> None:
+def setup_dist():
     import torch
     import torch.distributed as dist
-    import snapmrf_b200 as snap
-
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -313,6 +412,15 @@ def run_ours(args) -> None:
         dist.init_process_group("nccl", init_method="env://",
                                 timeout=__import__("datetime").timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def run_ours(args) -> None:
+    import torch
+    import torch.distributed as dist
+    import snapmrf_b200 as snap
+
+    world, rank, local = setup_dist()
     dev = torch.device("cuda", local)
 
     h_mrf, params, natoms, img, b1map, truth = make_inputs(snap, torch, seed=rank,
@@ -331,34 +439,39 @@ def run_ours(args) -> None:
 
     d_index = torch.empty(nvox, dtype=torch.int64, device=dev)
     # every B1 block holds one B1 value (trans_params), and zero-phase FISP
-    # atoms are purely imaginary (the tensor-core forms use half the MMA work)
+    # atoms are purely imaginary (half the products in every form)
     MATCH_FLAGS = snap.MATCH_ASSUME_UNIFORM_B1 | snap.MATCH_IMAG_ATOMS
 
     # the BF16 / FP16 forms take the matching operand (one 16-bit row of Im d
-    # per atom) from the dictionary kernel instead of packing the atoms again
+    # per atom) from the dictionary kernel instead of packing the atoms again,
+    # and the dictionary normalises only that operand: the FP32 atoms stay as
+    # generated, with their norms, which the exact rescoring divides by
     d_packed = torch.empty((NATOMS, snap.packed_pitch(T)), dtype=torch.int16, device=dev)
-
-    # ... and with it, the dictionary normalises only that operand: the FP32
-    # atoms stay as generated, with their norms, which the exact rescoring
-    # divides by (the same maps as unit-norm atoms, without rewriting 2.3 GB)
     d_norms = torch.empty(NATOMS, dtype=torch.float32, device=dev)
     flags_packed = snap.DICT_ALL_B1_BLOCKS | snap.DICT_NORMALIZE_OPERAND
 
     def packs(precision):
         return precision in (snap.PREC_BF16, snap.PREC_FP16)
 
+    def dict_call(precision, params_dev):
+        pk = packs(precision)
+        snap.MRF_dict(d_atoms, params_dev, h_mrf, T, T, NATOMS, natoms, 4, NSTATES, "epg_fisp",
+                      flags=flags_packed if pk else flags, d_norms=d_norms if pk else None,
+                      d_packed=d_packed if pk else None, packed_precision=precision if pk else 0)
+
+    def match_kwargs(precision):
+        pk = packs(precision)
+        return dict(flags=MATCH_FLAGS, precision=precision, topk=args.topk,
+                    packed_atoms=d_packed if pk else None, atom_norms=d_norms if pk else None)
+
     def step(precision, ev=None, gn=0):
         if ev is not None:
             ev[0].record(stream)
-        pk = packs(precision)
-        snap.MRF_dict(d_atoms, d_params, h_mrf, T, T, NATOMS, natoms, 4, NSTATES, "epg_fisp",
-                      flags=flags_packed if pk else flags, d_norms=d_norms if pk else None,
-                      d_packed=d_packed if pk else None, packed_precision=precision if pk else 0)
+        dict_call(precision, d_params)
         if ev is not None:
             ev[1].record(stream)
         snap.MRF_match(d_maps, d_img, d_atoms, d_params, T, T, NATOMS, natoms, nvox, in_b1map=d_b1,
-                       flags=MATCH_FLAGS, precision=precision, d_index=d_index,
-                       topk=args.topk, packed_atoms=d_packed if pk else None, atom_norms=d_norms if pk else None)
+                       d_index=d_index, **match_kwargs(precision))
         if ev is not None:
             ev[2].record(stream)
         if gn:
@@ -394,23 +507,23 @@ def run_ours(args) -> None:
         clk.mark_end()
         barrier()
         torch.cuda.synchronize()
-        r = {"clocks": clk.stop(), "launches": snap.kernel_launches() - launches0,
-             "elapsed_ms": t_start.elapsed_time(t_end),
-             "dict_ms": float(np.mean([e[0].elapsed_time(e[1]) for e in evs])),
-             "match_ms": float(np.mean([e[1].elapsed_time(e[2]) for e in evs])),
-             "gn_ms": float(np.mean([e[2].elapsed_time(e[3]) for e in evs])),
-             "maps": d_maps.cpu().numpy(), "index": d_index.cpu().numpy()}
-        return r
+        return {"clocks": clk.stop(), "launches": snap.kernel_launches() - launches0,
+                "elapsed_ms": t_start.elapsed_time(t_end),
+                "dict_ms": float(np.mean([e[0].elapsed_time(e[1]) for e in evs])),
+                "match_ms": float(np.mean([e[1].elapsed_time(e[2]) for e in evs])),
+                "gn_ms": float(np.mean([e[2].elapsed_time(e[3]) for e in evs])),
+                "maps": d_maps.cpu().numpy(), "index": d_index.cpu().numpy()}
 
     PRECS = {"fp32": snap.PREC_FP32, "bf16": snap.PREC_BF16, "fp16": snap.PREC_FP16, "fp8": snap.PREC_FP8}
-    forms = {name: timed(p) for name, p in PRECS.items()}
-    # the tensor-core forms followed by Gauss-Newton refinement of (T1, T2)
     TC = ("bf16", "fp16", "fp8")
-    gn_forms = {f"{name}+gn": timed(PRECS[name], gn=args.gn_iters) for name in TC} \
-        if args.gn_iters > 0 else {}
-    # argmax agreement with the FP32 form, counting a different atom as agreeing
-    # when its exact FP32 score is within 1e-6 of the FP32 form's pick (an FP32
-    # near-tie, where the FP32 form itself depends on summation order)
+    HEAD = "bf16+gn"
+    forms = {name: timed(p) for name, p in PRECS.items()}
+    forms.update({f"{name}+gn": timed(PRECS[name], gn=args.gn_iters) for name in TC})
+
+    # argmax agreement with the FP32 form, counting a different atom as
+    # agreeing when its exact FP32 score is within 1e-6 of the FP32 form's
+    # pick (an FP32 near-tie, where the FP32 form itself depends on the
+    # summation order)
     pd32 = forms["fp32"]["maps"][:, 4]
     raw, agree = {}, {}
     for f in TC:
@@ -421,22 +534,32 @@ def run_ours(args) -> None:
     a = reduce_over_ranks([agree[f] for f in TC] + [raw[f] for f in TC], "min", dev, world)
     agree = dict(zip(TC, a[:len(TC)]))
     raw = dict(zip(TC, a[len(TC):]))
-    # headline: the fastest tensor-core form whose argmax agrees with the FP32
-    # form on >= 99.9 % of voxels in this very run, else the FP32 form
-    ok = [f for f in TC if agree[f] >= 0.999]
-    headline = min(ok, key=lambda f: forms[f]["elapsed_ms"]) if ok else "fp32"
-    prec = PRECS[headline]
-    hf = forms[headline]
 
-    # Compressed matching (per-B1-block SVD of the dictionary): the bases and
+    # per-kernel roofline of the refinement: one Gauss-Newton pass over every
+    # voxel (its first iteration, the largest launch), timed alone
+    d_maps_gn = torch.empty_like(d_maps)
+    step(snap.PREC_BF16)
+    gn_pass = []
+    for r in range(4):
+        d_maps_gn.copy_(d_maps)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        snap.refine_gn(d_maps_gn, d_img, h_mrf, T, T, nvox, NSTATES, "epg_fisp", iterations=1, tol=0.0,
+                       d_b1map=d_b1)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if r:
+            gn_pass.append(e0.elapsed_time(e1))
+    gn_pass_ms = float(np.mean(gn_pass))
+
+    # compressed matching (per-B1-block SVD of the dictionary): the bases and
     # coordinates are computed once per dictionary and reused for every
     # image, so the compression is timed once and the compressed FP16 match
-    # (rescored against the full atoms) alone over the K steps.
+    # (rescored against the full atoms) alone over the K steps
     comp = None
     if args.svd_sfrac > 0:
         comp = {"sfrac": args.svd_sfrac}
         try:
-            # the unit-norm dictionary in d_atoms
             snap.MRF_dict(d_atoms, d_params, h_mrf, T, T, NATOMS, natoms, 4, NSTATES, "epg_fisp", flags=flags)
             torch.cuda.synchronize()
             c0 = torch.cuda.Event(enable_timing=True)
@@ -476,277 +599,416 @@ def run_ours(args) -> None:
                         launches_per_match=(snap.kernel_launches() - l0) // args.steps,
                         argmax_agreement_vs_fp32=round(float(np.mean(same | tie)), 6),
                         argmax_agreement_vs_fp32_raw=round(float(np.mean(same)), 6),
-                        t1_median_rel=round(float(np.median(np.abs(cm[:, 0] - vt1) / vt1)), 5),
-                        t2_median_rel=round(float(np.median(np.abs(cm[:, 1] - vt2) / vt2)), 5),
+                        t1_median_rel=round(median_rel(cm[:, 0], vt1), 5),
+                        t2_median_rel=round(median_rel(cm[:, 1], vt2), 5),
                         singular_values_block0=[round(float(v), 4) for v in cmp.sv[0, :8]])
             del cmp
         except snap.SnapMRFError as e:
             comp["error"] = str(e)
-        # restore the headline form's maps for the lines below
-        step(prec)
-        torch.cuda.synchronize()
-    clocks, launches, elapsed_ms = hf["clocks"], hf["launches"], hf["elapsed_ms"]
-    dict_ms, match_ms, maps = hf["dict_ms"], hf["match_ms"], hf["maps"]
     dev_err = snap.device_error(reset=True)
 
-    # end to end through the public API from pinned host buffers
-    if args.no_e2e:
-        e2e_ms = float("nan")
+    # End to end through the public API from pinned host buffers.  The
+    # caller uploads the parameter table and the B1 map (MRF_dict takes
+    # device params, as the reference's does; the refinement needs the map on
+    # the device too); MRF_match takes the host image and streams it into a
+    # caller-owned device buffer on the library's copy stream, starting at
+    # once (the buffer alternates between steps, so nothing queued earlier
+    # still reads it) and overlapping the dictionary; the refinement reads
+    # that buffer; the maps come back down.
     h_params = torch.from_numpy(params).pin_memory()
     h_img = torch.from_numpy(img.view(np.float32).reshape(nvox, T, 2)).pin_memory()
     h_b1 = torch.from_numpy(b1map).pin_memory()
     h_maps = torch.empty((nvox, 5), dtype=torch.float32).pin_memory()
-    e2e_atoms = d_atoms  # output buffers are allocated once, like the reference's caller
-
-    # Uploads run on a second stream in the order params, image, B1 map, into
-    # one of two sets of device buffers (double buffering: step k+1's uploads
-    # overlap step k's dictionary and matching); the dictionary waits only
-    # for its params, matching for its image.  Every copy is inside the timed
-    # region.
-    up_stream = torch.cuda.Stream(device=dev)
     e2e_par = [torch.empty_like(d_params), torch.empty_like(d_params)]
-    e2e_img = [torch.empty_like(d_img), torch.empty_like(d_img)]
     e2e_b1 = [torch.empty_like(d_b1), torch.empty_like(d_b1)]
-    ev_free = [torch.cuda.Event(), torch.cuda.Event()]
-    ev_par = [torch.cuda.Event(), torch.cuda.Event()]
-    ev_img = [torch.cuda.Event(), torch.cuda.Event()]
-    for e in ev_free:
-        e.record(stream)
+    e2e_img = [torch.empty_like(d_img), torch.empty_like(d_img)]
     k_step = [0]
+    hprec = PRECS[HEAD.split("+")[0]]
 
     def e2e_step():
         b = k_step[0] % 2
         k_step[0] += 1
-        up_stream.wait_event(ev_free[b])
-        with torch.cuda.stream(up_stream):
-            e2e_par[b].copy_(h_params, non_blocking=True)
-            ev_par[b].record(up_stream)
-            e2e_img[b].copy_(h_img, non_blocking=True)
-            e2e_b1[b].copy_(h_b1, non_blocking=True)
-            ev_img[b].record(up_stream)
-        stream.wait_event(ev_par[b])
-        pk = packs(prec)
-        snap.MRF_dict(e2e_atoms, e2e_par[b], h_mrf, T, T, NATOMS, natoms, 4, NSTATES, "epg_fisp",
-                      flags=flags_packed if pk else flags, d_norms=d_norms if pk else None,
-                      d_packed=d_packed if pk else None, packed_precision=prec if pk else 0)
-        stream.wait_event(ev_img[b])
-        snap.MRF_match(d_maps, e2e_img[b], e2e_atoms, e2e_par[b], T, T, NATOMS, natoms, nvox, in_b1map=e2e_b1[b],
-                       img_stride=T, flags=MATCH_FLAGS, precision=prec, topk=args.topk,
-                       packed_atoms=d_packed if pk else None, atom_norms=d_norms if pk else None)
-        ev_free[b].record(stream)
+        e2e_par[b].copy_(h_params, non_blocking=True)
+        e2e_b1[b].copy_(h_b1, non_blocking=True)
+        dict_call(hprec, e2e_par[b])
+        snap.MRF_match(d_maps, h_img, d_atoms, e2e_par[b], T, T, NATOMS, natoms, nvox, in_b1map=e2e_b1[b],
+                       img_device_copy=e2e_img[b], upload_early=True, **match_kwargs(hprec))
+        snap.refine_gn(d_maps, e2e_img[b], h_mrf, T, T, nvox, NSTATES, "epg_fisp", iterations=args.gn_iters,
+                       tol=args.gn_tol, d_b1map=e2e_b1[b])
         h_maps.copy_(d_maps, non_blocking=True)
 
+    e2e_ms = float("nan")
     h2d_ms = float("nan")
+    e2e_err = None
+    e2e_same = None
     if not args.no_e2e:
-        # the image upload alone, for the link speed
-        u0 = torch.cuda.Event(enable_timing=True)
-        u1 = torch.cuda.Event(enable_timing=True)
-        torch.cuda.synchronize()
-        with torch.cuda.stream(up_stream):
-            u0.record(up_stream)
+        try:
+            u0 = torch.cuda.Event(enable_timing=True)
+            u1 = torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            u0.record(stream)
             for _ in range(3):
                 e2e_img[0].copy_(h_img, non_blocking=True)
-            u1.record(up_stream)
-        torch.cuda.synchronize()
-        h2d_ms = u0.elapsed_time(u1) / 3
-        for _ in range(max(1, args.warmup // 2)):
-            e2e_step()
-        torch.cuda.synchronize()
-        barrier()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(args.steps):
-            e2e_step()
-        e1.record(stream)
-        torch.cuda.synchronize()
-        barrier()
-        e2e_ms = e0.elapsed_time(e1)
+            u1.record(stream)
+            torch.cuda.synchronize()
+            h2d_ms = u0.elapsed_time(u1) / 3
+            for _ in range(args.warmup):
+                e2e_step()
+            torch.cuda.synchronize()
+            barrier()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(args.steps):
+                e2e_step()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            barrier()
+            e2e_ms = e0.elapsed_time(e1)
+            hm = forms[HEAD]["maps"][:, :2]
+            e2e_same = float(np.mean(np.all(np.abs(h_maps.numpy()[:, :2] - hm) <= 1e-6 * np.abs(hm), axis=1)))
+        except snap.SnapMRFError as e:
+            e2e_err = str(e)
 
     # max over ranks
-    def topk_of(form):
-        return args.topk or (4 if form == "fp16" else 16)
-
-    names = list(PRECS)
-    gnames = list(gn_forms)
-    t = reduce_over_ranks([elapsed_ms, e2e_ms, dict_ms, match_ms] +
-                          [forms[f]["elapsed_ms"] for f in names] + [forms[f]["match_ms"] for f in names] +
-                          [gn_forms[f]["elapsed_ms"] for f in gnames] + [gn_forms[f]["gn_ms"] for f in gnames],
-                          "max", dev, world)
-    elapsed_ms, e2e_ms, dict_ms, match_ms = t[:4]
-    form_ms = dict(zip(names, t[4:4 + len(names)]))
-    form_match_ms = dict(zip(names, t[4 + len(names):4 + 2 * len(names)]))
-    o = 4 + 2 * len(names)
-    gn_ms = dict(zip(gnames, t[o:o + len(gnames)]))
-    gn_stage_ms = dict(zip(gnames, t[o + len(gnames):]))
+    names = list(forms)
+    t = reduce_over_ranks([e2e_ms, gn_pass_ms] + [forms[f]["elapsed_ms"] for f in names] +
+                          [forms[f]["dict_ms"] for f in names] + [forms[f]["match_ms"] for f in names] +
+                          [forms[f]["gn_ms"] for f in names], "max", dev, world)
+    e2e_ms, gn_pass_ms = t[0], t[1]
+    n = len(names)
+    fms = {f: {"elapsed": t[2 + i], "dict": t[2 + n + i], "match": t[2 + 2 * n + i], "gn": t[2 + 3 * n + i]}
+           for i, f in enumerate(names)}
 
     if rank == 0:
-        ms_per_step = elapsed_ms / args.steps
+        hf = forms[HEAD]
+        ms_per_step = fms[HEAD]["elapsed"] / args.steps
         value = world * nvox / (ms_per_step / 1e3)
-        e2e_value = world * nvox / (e2e_ms / args.steps / 1e3) if not args.no_e2e else None
+        e2e_value = world * nvox / (e2e_ms / args.steps / 1e3) if e2e_ms == e2e_ms else None
         pk = peaks()
-        sm_mhz = clocks.get("sm_mhz") or pk["sm_max_mhz"]
-        fp32_peak = fp32_peak_tflops(pk["sm_max_mhz"])
-        dict_flops = NATOMS * T * NSTATES * FLOP_PER_STATE_STEP
-        match_flops = nvox * 8.0 * T * natoms
-        dict_tf = dict_flops / (dict_ms / 1e3) / 1e12
-        match_tf = match_flops / (match_ms / 1e3) / 1e12
-        rl_dict = {"kernel": "epg_real_kernel (epg_fisp dictionary, real-valued recursion)", "bound": "fp32",
-                   "achieved": round(dict_tf, 2), "peak": round(fp32_peak, 2), "unit": "TFLOP/s",
-                   "frac": round(dict_tf / fp32_peak, 4),
-                   "executed_tflops": round(dict_tf * FLOP_PER_STATE_STEP_EXECUTED / FLOP_PER_STATE_STEP, 2),
-                   "executed_frac": round(dict_tf * FLOP_PER_STATE_STEP_EXECUTED / FLOP_PER_STATE_STEP / fp32_peak, 4),
-                   "note": "achieved counts 66 flop per state-step (complex recursion convention); the "
-                           "real-valued recursion with folded relaxation executes 8 FP32-pipe operations (16 flop at the pipe's rate), hence frac > 1; "
-                           "executed_frac is the FP32-pipe utilisation",
-                   "traffic": round(DICT_DRAM_BYTES_PER_ATOM * NATOMS),
-                   "traffic_note": "ncu DRAM bytes of the reduced case scaled by atoms; algorithmic output "
-                                   f"{NATOMS * T * 8} B",
-                   "algorithmic_flop_per_launch": dict_flops, "ms": round(dict_ms, 3)}
-        if headline != "fp32":
-            # the E4M3 dense rate is twice the BF16 / FP16 rate (4.5 vs 2.25 PFLOP/s
-            # nominal); only the BF16 rate is measured
-            mpk = pk["bf16_tflops"] * (2 if headline == "fp8" else 1)
-            rl_match = {"kernel": f"{headline} tcgen05 B1-bin match + fp32 top-{topk_of(headline)} rescoring",
-                        "bound": "tensor",
-                        "peak_note": "2 x measured bf16" if headline == "fp8" else "measured bf16",
-                        "note": "achieved counts 8 T flop per voxel-atom pair (complex scores); with purely "
-                                "imaginary atoms (MATCH_IMAG_ATOMS) the MMAs execute half of that",
-                        "achieved": round(match_tf, 2), "peak": mpk, "unit": "TFLOP/s",
-                        "frac": round(match_tf / mpk, 4), "traffic": None,
-                        "algorithmic_flop_per_launch": match_flops, "ms": round(match_ms, 3)}
-        else:
-            rl_match = {"kernel": "fp32 B1-bin match", "bound": "fp32", "achieved": round(match_tf, 2),
-                        "peak": round(fp32_peak, 2), "unit": "TFLOP/s", "frac": round(match_tf / fp32_peak, 4),
-                        "traffic": None, "algorithmic_flop_per_launch": match_flops, "ms": round(match_ms, 3)}
-        dominant, other = (rl_match, rl_dict) if match_ms >= dict_ms else (rl_dict, rl_match)
-        # accuracy of the produced maps against the voxels' true parameters
+        fp32_peak, fp32_note = fp32_fma_peak()
         vt1, vt2, _ = truth
-        e1_ = np.abs(maps[:, 0] - vt1) / vt1
-        e2_ = np.abs(maps[:, 1] - vt2) / vt2
+
+        def topk_of(form):
+            return args.topk or (4 if form.startswith("fp16") else 16)
+
+        # rooflines of the headline step's kernels (executed work)
+        dict_ms, match_ms, gn_ms = fms[HEAD]["dict"], fms[HEAD]["match"], fms[HEAD]["gn"]
+        rl_dict = roofline("epg_real_kernel (+ fine tail): epg_fisp dictionary, real-valued recursion", "fp32",
+                           NATOMS * T * NSTATES * FLOP_PER_STATE_STEP_EXECUTED, dict_ms, fp32_peak, fp32_note,
+                           achieved_convention=round(NATOMS * T * NSTATES * FLOP_PER_STATE_STEP /
+                                                     (dict_ms / 1e3) / 1e12, 2),
+                           convention_note="66 flop per state-step (complex recursion); the real recursion "
+                                           "executes 16 (8 FP32-pipe operations)",
+                           traffic=round(DICT_DRAM_BYTES_PER_ATOM * NATOMS),
+                           traffic_note="ncu DRAM bytes of the reduced case scaled by atoms; algorithmic "
+                                        f"output {NATOMS * T * 8} B")
+        mm_flop = nvox * 4.0 * T * natoms   # purely imaginary atoms: 2 A rows x 1 B row x K = T
+        rl_match = roofline(f"bf16 tcgen05 B1-bin match (+ packing, fp32 top-{topk_of('bf16')} rescoring), "
+                            "whole call", "tensor", mm_flop, match_ms, pk["bf16_tflops"],
+                            f"bf16 dense, {pk['source']} (burst)",
+                            achieved_convention=round(nvox * 8.0 * T * natoms / (match_ms / 1e3) / 1e12, 2),
+                            convention_note="8 T flop per voxel-atom pair (complex scores); purely imaginary "
+                                            "atoms execute 4 T")
+        rl_gn = roofline("gn_kernel<7, tangents>: one Gauss-Newton pass over every voxel", "fp32",
+                         nvox * T * NSTATES * GN_FLOP_PER_STATE_STEP, gn_pass_ms, fp32_peak, fp32_note,
+                         note="78 flop per state-step at the pipe's rate (signal and two tangents); the "
+                              f"refinement runs up to {args.gn_iters} such passes over the voxels still moving "
+                              f"({gn_ms:.2f} ms in the step)")
+        rls = sorted([(gn_ms, rl_gn), (dict_ms, rl_dict), (match_ms, rl_match)], key=lambda x: -x[0])
+        rl_fp32 = roofline("match_fp32_kernel<imag>: FP32 B1-bin match (fp32 form), whole call", "fp32",
+                           nvox * 4.0 * T * natoms, fms["fp32"]["match"], fp32_peak, fp32_note)
+
+        oracle_cmp = None
+        if args.oracle_sample > 0:
+            sel, ot1, ot2 = oracle_maps_sample(h_mrf, params, natoms, img, b1map, args.oracle_sample)
+            hm = hf["maps"]
+            oracle_cmp = {"voxels": int(sel.size),
+                          "sample": "the two B1 blocks holding the most voxels; FP64 dictionary, match and "
+                                    "Gauss-Newton to convergence",
+                          "t1_median_rel": round(median_rel(hm[sel, 0], ot1), 6),
+                          "t2_median_rel": round(median_rel(hm[sel, 1], ot2), 6),
+                          "t1_max_rel": round(float(np.max(np.abs(hm[sel, 0] - ot1) / ot1)), 6),
+                          "t2_max_rel": round(float(np.max(np.abs(hm[sel, 1] - ot2) / ot2)), 6),
+                          "oracle_t1_median_rel_vs_truth": round(median_rel(ot1, vt1[sel]), 6),
+                          "oracle_t2_median_rel_vs_truth": round(median_rel(ot2, vt2[sel]), 6)}
         line = {
-            "metric": "dict atoms/s + matched voxels/s (voxels/s of the full dict+match step)",
+            "metric": METRIC,
             "value": round(value, 1), "unit": "voxels/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms_per_step, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
-            "dtype": (f"{headline} match (f32 accumulate, f32 top-{topk_of(headline)} rescoring), f32 dictionary"
-                      if headline != "fp32" else "f32"),
+            "dtype": f"bf16 match (f32 accumulate, f32 top-{topk_of('bf16')} rescoring), f32 dictionary and "
+                     "Gauss-Newton",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD, "T": T, "nstates": NSTATES, "atoms": NATOMS,
+            "config": {"workload": WORKLOAD, "form": HEAD, "T": T, "nstates": NSTATES, "atoms": NATOMS,
                        "atoms_per_b1_block": natoms, "b1_blocks": NATOMS // natoms, "voxels": nvox,
-                       "echo_type": "epg_fisp", "match": f"{headline}, nearest B1 block",
+                       "echo_type": "epg_fisp",
+                       "match": f"bf16 tcgen05, nearest B1 block, top-{topk_of('bf16')} rescored in fp32",
+                       "refine": f"Gauss-Newton, at most {args.gn_iters} iterations, tol {args.gn_tol}",
                        "l2": "inputs and outputs larger than L2 (no flush needed)",
                        "parallelism": f"{world} independent slices" if world > 1 else "single GPU"},
             "dict_atoms_per_s": round(world * NATOMS / (dict_ms / 1e3), 1),
             "match_voxels_per_s": round(world * nvox / (match_ms / 1e3), 1),
-            "stage_ms": {"dict": round(dict_ms, 3), "match": round(match_ms, 3)},
-            "roofline": dominant, "roofline_other": other,
-            "peak_note": "fp32 peak = 148 SMs x 128 FMA lanes x 2 flop x max SM clock (nominal, no "
-                         f"measured FP32 figure exists); bf16 peak {pk['source']} (burst)",
+            "stage_ms": {"dict": round(dict_ms, 3), "match": round(match_ms, 3), "refine": round(gn_ms, 3)},
+            "roofline": rls[0][1],
+            "roofline_other": [r for _, r in rls[1:]] + [rl_fp32],
+            "peaks": {"fp32_fma_tflops": fp32_peak, "fp32_note": fp32_note, "bf16_tflops": pk["bf16_tflops"],
+                      "hbm_gbs": pk["hbm_gbs"], "source": pk["source"]},
             "e2e": {"value": round(e2e_value, 1) if e2e_value else None, "unit": "voxels/s",
                     "h2d_bytes_per_step": int(params.nbytes + img.nbytes + b1map.nbytes + h_mrf.nbytes),
                     "d2h_bytes_per_step": int(nvox * 5 * 4),
+                    "path": "params and B1 map up by the caller, MRF_dict, MRF_match(host image streamed by the "
+                            "library into a caller-owned device buffer, overlapping the dictionary), refine_gn, "
+                            "maps to pinned host memory",
                     "image_upload_ms": round(h2d_ms, 3),
-                    "image_upload_gbs": round(img.nbytes / (h2d_ms / 1e3) / 1e9, 1) if h2d_ms == h2d_ms else None},
-            "forms": {**{f: {"voxels_per_s": round(world * nvox / (form_ms[f] / args.steps / 1e3), 1),
-                             "ms_per_step": round(form_ms[f] / args.steps, 3),
-                             "match_ms": round(form_match_ms[f], 3)} for f in names},
-                      "headline": headline, "topk": args.topk,
-                      "argmax_agreement_vs_fp32": {f: round(v, 6) for f, v in agree.items()},
-                      "argmax_agreement_vs_fp32_raw": {f: round(v, 6) for f, v in raw.items()}},
+                    "image_upload_gbs": round(img.nbytes / (h2d_ms / 1e3) / 1e9, 1) if h2d_ms == h2d_ms else None,
+                    "maps_equal_to_device_form": e2e_same, "error": e2e_err},
+            "forms": {f: {"voxels_per_s": round(world * nvox / (fms[f]["elapsed"] / args.steps / 1e3), 1),
+                          "ms_per_step": round(fms[f]["elapsed"] / args.steps, 3),
+                          "dict_ms": round(fms[f]["dict"], 3), "match_ms": round(fms[f]["match"], 3),
+                          "refine_ms": round(fms[f]["gn"], 3),
+                          "t1_median_rel_vs_truth": round(median_rel(forms[f]["maps"][:, 0], vt1), 5),
+                          "t2_median_rel_vs_truth": round(median_rel(forms[f]["maps"][:, 1], vt2), 5),
+                          **({"speedup_vs_fp32_form": round(fms["fp32"]["elapsed"] / fms[f]["elapsed"], 3)}
+                             if f != "fp32" else {})}
+                      for f in names},
+            "argmax_agreement_vs_fp32": {f: round(v, 6) for f, v in agree.items()},
+            "argmax_agreement_vs_fp32_raw": {f: round(v, 6) for f, v in raw.items()},
+            "maps_error_vs_fp64_oracle": oracle_cmp,
             "device_error": int(dev_err),
-            "gpu_launches": int(launches),
-            "clocks": clocks,
-            "maps_error_vs_truth": {
-                f: {"t1_median_rel": round(float(np.median(np.abs(fm[f]["maps"][:, 0] - vt1) / vt1)), 5),
-                    "t2_median_rel": round(float(np.median(np.abs(fm[f]["maps"][:, 1] - vt2) / vt2)), 5)}
-                for fm in (forms, gn_forms) for f in fm},
+            "gpu_launches": int(hf["launches"]),
+            "clocks": hf["clocks"],
         }
         if comp is not None:
             line["forms_compressed"] = comp
-        if gn_forms:
-            line["forms_refined"] = {
-                f: {"voxels_per_s": round(world * nvox / (gn_ms[f] / args.steps / 1e3), 1),
-                    "ms_per_step": round(gn_ms[f] / args.steps, 3), "gn_ms": round(gn_stage_ms[f], 3),
-                    "gn_iterations_max": args.gn_iters, "gn_tol": args.gn_tol,
-                    "speedup_vs_fp32_form": round(form_ms["fp32"] / gn_ms[f], 3)} for f in gnames}
         if args.b1_blocks != 41 or args.nx != NX:
             line["config"]["workload"] = f"{WORKLOAD} reduced: {NATOMS // natoms} B1 blocks, {args.nx}x{args.nx} voxels"
         if not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_baseline(args.cpu_seconds)
+            cb = cpu_step(0)
+            line["cpu_baseline"] = {"value": round(cb["voxels"] / cb["seconds"], 3), "unit": "voxels/s",
+                                    "cores": cb["threads"], "kind": "port", "sample": cb["sample"],
+                                    "sample_atoms": cb["atoms"], "sample_voxels": cb["voxels"],
+                                    "sample_seconds": round(cb["seconds"], 3), "extrapolated": False}
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
 
 
-def cpu_sample(seconds: float):
-    """Times the oracle's FP32 CPU path (all host threads) on a bounded
-    sample of the workload sized to about `seconds` of CPU time; returns
-    (step seconds extrapolated to the full workload, sample text, threads)."""
-    from oracle import oracle as orc
+# ---------------------------------------------------------------------------
+# the large bSSFP configuration
+# ---------------------------------------------------------------------------
+
+def c4_schedule(seed: int = 4, nreps: int = 500) -> np.ndarray:
+    """The bSSFP schedule in the epg_ssfp / roa_ssfp CSV convention (fraction
+    of 60 deg, deg, TR - 16, TE - 3.5; src/functions.cu:1240-1261)."""
+    rng = np.random.default_rng(seed)
+    t = np.arange(nreps)
+    fa = (5.0 + 55.0 * np.abs(np.sin(np.pi * t / 200.0))) / 60.0
+    ph = np.where(t % 2 == 0, 0.0, 180.0)
+    tr = rng.uniform(10.0, 14.0, nreps)
+    return np.array([fa, ph, tr - 16.0, tr / 2 - 3.5], np.float32)
+
+
+def run_c4(args) -> None:
+    """ssfp_b0_256x256x8: dictionaries (EPG-SSFP, and ROA with 100
+    isochromats) and global matching of 524,288 voxels (or --c4-slices
+    slices of 65,536) in FP16 / BF16 (complex [Re; Im] operands, top-k
+    rescored in FP32); the FP32 form on --c4-fp32-voxels voxels."""
+    import torch
     import snapmrf_b200 as snap
+    world, rank, local = setup_dist()
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream()
+    T4, w = 500, NSTATES
+    h = c4_schedule(4, T4)
+    t1, t2 = geometric(100.0, 5000.0), geometric(10.0, 2000.0)
+    b0 = np.array([-100.0 + 4.0 * k for k in range(51)], np.float32)
+    b1 = np.array([0.8, 0.9, 1.0, 1.1, 1.2], np.float32)
+    params = snap.trans_params(t1, t2, b0, b1)
+    NATOMS = params.shape[0]
+    natoms = NATOMS // len(b1)
+    nxy = 256
+    nvox = nxy * nxy * args.c4_slices
+    # voxels: per slice the tissue phantom (seeded per slice), a B0 field of
+    # +-80 Hz (linear + quadratic), and a B1 field 1 + 0.2 (x^2 + y^2 - 0.5)
+    # snapped to the dictionary's B1 values (the bSSFP recursion takes B1 per
+    # block); T1 / T2 / B0 off the grid
+    vt1, vt2, vb0, vb1, m0, ph = [], [], [], [], [], []
+    y, x = np.meshgrid(np.linspace(-1, 1, nxy), np.linspace(-1, 1, nxy), indexing="ij")
+    for s in range(args.c4_slices):
+        _, a1, a2, m, p = phantom(100 * rank + s, nxy)
+        zc = -1 + 2 * (s + 0.5) / max(args.c4_slices, 1)
+        f0 = np.clip(40.0 * x + 25.0 * y + 15.0 * (x ** 2 + y ** 2 + zc ** 2) - 10.0, -80.0, 80.0)
+        fb1 = np.clip(1.0 + 0.2 * (x ** 2 + y ** 2 - 0.5), 0.8, 1.2)
+        vt1.append(a1)
+        vt2.append(a2)
+        vb0.append(f0.reshape(-1).astype(np.float32))
+        vb1.append(b1[np.argmin(np.abs(fb1.reshape(-1)[:, None] - b1[None, :]), axis=1)])
+        m0.append(m)
+        ph.append(p)
+    vt1, vt2, vb0, vb1, m0, ph = (np.concatenate(v) for v in (vt1, vt2, vb0, vb1, m0, ph))
+    sig = np.zeros((nvox, T4), np.complex64)
+    for v in b1:
+        sel = np.flatnonzero(vb1 == v)
+        for c0 in range(0, sel.size, 65536):
+            cs = sel[c0:c0 + 65536]
+            vp = np.stack([vt1[cs], vt2[cs], vb0[cs], np.full(cs.size, v)], 1).astype(np.float32)
+            d_vp = torch.from_numpy(vp).to(dev)
+            d_s = torch.empty((cs.size, T4, 2), device=dev)
+            snap.MRF_dict(d_s, d_vp, h, T4, T4, cs.size, cs.size, 4, w, "epg_ssfp")
+            torch.cuda.synchronize()
+            a = d_s.cpu().numpy()
+            sig[cs] = a[..., 0] + 1j * a[..., 1]
+    img = add_noise(sig * (m0 * np.exp(1j * ph))[:, None], rank, T4)
+    del sig
+
+    d_params = torch.from_numpy(params).to(dev)
+    d_atoms = torch.empty((NATOMS, T4, 2), device=dev)
+    d_img = torch.from_numpy(img.view(np.float32).reshape(nvox, T4, 2)).to(dev)
+    d_maps = torch.empty((nvox, 5), device=dev)
+    d_index = torch.empty(nvox, dtype=torch.int64, device=dev)
+
+    def ev_time(fn, reps, warm):
+        for _ in range(warm):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0 = snap.kernel_launches()
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps, (snap.kernel_launches() - l0) // reps
+
+    out = {"workload": WORKLOAD_C4 if args.c4_slices == 8 else f"{WORKLOAD_C4} ({args.c4_slices} of 8 slices)",
+           "T": T4, "nstates": w, "atoms": NATOMS, "atoms_per_b1_block": natoms, "voxels": nvox,
+           "match": "global MIP (no B1 map; the reference's max-PD merge)"}
+    clk = ClockSampler(local)
+    clk.start()
+    clk.mark_start()
+    fp32_peak, fp32_note = fp32_fma_peak()
+    ssfp_ms, _ = ev_time(lambda: snap.MRF_dict(d_atoms, d_params, h, T4, T4, NATOMS, natoms, 4, w, "epg_ssfp"),
+                         args.steps, args.warmup)
+    out["ssfp_dict"] = roofline("epg_ref_kernel<SSFP>: bSSFP dictionary (complex recursion, B0)", "fp32",
+                                NATOMS * T4 * w * SSFP_FLOP_PER_STATE_STEP, ssfp_ms, fp32_peak, fp32_note,
+                                flop_note="90 flop per state-step by convention",
+                                atoms_per_s=round(NATOMS / (ssfp_ms / 1e3), 1))
+    d_roa = torch.empty((NATOMS, T4, 2), device=dev)
+    roa_ms, _ = ev_time(lambda: snap.MRF_dict(d_roa, d_params, h, T4, T4, NATOMS, natoms, 4, w, "roa_ssfp",
+                                              n_iso=100, flags=snap.DICT_ALL_B1_BLOCKS), args.steps, args.warmup)
+    out["roa_dict"] = roofline("roa_iso_kernel: ROA dictionary, 100 isochromats", "fp32",
+                               NATOMS * T4 * 100 * ROA_FLOP_PER_ISO_STEP, roa_ms, fp32_peak, fp32_note,
+                               atoms_per_s=round(NATOMS / (roa_ms / 1e3), 1))
+    del d_roa
+    snap.MRF_dict(d_atoms, d_params, h, T4, T4, NATOMS, natoms, 4, w, "epg_ssfp")
+    pk = peaks()
+    # matching: complex operands, K = 2T, 8 T flop per voxel-atom pair
+    res = {}
+    for name, prec, topk in (("fp16", snap.PREC_FP16, args.c4_topk16), ("bf16", snap.PREC_BF16, 16)):
+        ms, nl = ev_time(lambda: snap.MRF_match(d_maps, d_img, d_atoms, d_params, T4, T4, NATOMS, natoms, nvox,
+                                                precision=prec, topk=topk, d_index=d_index),
+                         args.c4_match_steps, 1)
+        res[name] = {"maps": d_maps.cpu().numpy(), "index": d_index.cpu().numpy()}
+        out[f"{name}_match"] = roofline(f"{name} tcgen05 global match + fp32 top-{topk} rescoring, whole call",
+                                        "tensor", nvox * 8.0 * T4 * NATOMS, ms, pk["bf16_tflops"],
+                                        f"bf16 dense, {pk['source']} (burst)", launches=nl,
+                                        voxels_per_s=round(nvox / (ms / 1e3), 1))
+    # FP32 on a voxel subset (the whole image takes about a minute per call)
+    nv32 = min(args.c4_fp32_voxels, nvox)
+    sel = np.sort(np.random.default_rng(9).choice(nvox, nv32, replace=False))
+    d_img32 = d_img[torch.from_numpy(sel).to(dev)].contiguous()
+    d_maps32 = torch.empty((nv32, 5), device=dev)
+    d_idx32 = torch.empty(nv32, dtype=torch.int64, device=dev)
+    ms32, _ = ev_time(lambda: snap.MRF_match(d_maps32, d_img32, d_atoms, d_params, T4, T4, NATOMS, natoms, nv32,
+                                             d_index=d_idx32), 1, 1)
+    clk.mark_end()
+    out["fp32_match"] = roofline("match_fp32_kernel<complex>: FP32 global match, whole call", "fp32",
+                                 nv32 * 8.0 * T4 * NATOMS, ms32, fp32_peak, fp32_note, voxels=nv32,
+                                 voxels_per_s=round(nv32 / (ms32 / 1e3), 1))
+    i32 = d_idx32.cpu().numpy()
+    m32 = d_maps32.cpu().numpy()
+    for name in res:
+        same = res[name]["index"][sel] == i32
+        tie = res[name]["maps"][sel, 4] >= m32[:, 4] * (1 - 1e-6)
+        r = out[f"{name}_match"]
+        r["argmax_agreement_vs_fp32"] = round(float(np.mean(same | tie)), 6)
+        r["argmax_agreement_vs_fp32_raw"] = round(float(np.mean(same)), 6)
+        mm = res[name]["maps"]
+        r["t1_median_rel_vs_truth"] = round(median_rel(mm[:, 0], vt1), 5)
+        r["t2_median_rel_vs_truth"] = round(median_rel(mm[:, 1], vt2), 5)
+        r["b0_median_abs_hz_vs_truth"] = round(float(np.median(np.abs(mm[:, 2] - vb0))), 3)
+    out["device_error"] = snap.device_error(reset=True)
+    clocks = clk.stop()
+    if rank == 0:
+        best = min(("fp16", "bf16"), key=lambda f: out[f"{f}_match"]["ms"])
+        step_ms = ssfp_ms + out[f"{best}_match"]["ms"]
+        line = {"metric": METRIC, "value": round(nvox / (step_ms / 1e3), 1), "unit": "voxels/s", "n_gpus": world,
+                "steps": args.c4_match_steps, "warmup": 1, "ms_per_step": round(step_ms, 3),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": f"{best} match (f32 accumulate, f32 rescoring), f32 dictionary", "data": "synthetic",
+                "config": out, "clocks": clocks}
+        print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# the reference algorithm on the host cores
+# ---------------------------------------------------------------------------
+
+def cpu_step(block: int, seed: int = 7) -> dict:
+    """One bounded slice of the workload on the host cores through the
+    oracle's FP32 C path (OpenMP, every host thread): B1 block `block`'s
+    6,938 atoms generated and normalised, and 1/41 of the voxels matched
+    against them.  Loads no product code."""
+    from oracle import oracle as orc
     nthr = orc.max_threads()
     h_mrf = schedule(1)
     t1, t2, b0, b1 = grid()
-    params = snap.trans_params(t1, t2, b0, b1)
-    natoms = params.shape[0] // len(b1)
-    NATOMS = params.shape[0]
-    nvox = NX * NY
-    rng = np.random.default_rng(7)
-
-    def run(na, nv):
-        t0 = time.perf_counter()
-        atoms = orc.dict_atoms("epg_fisp", params[:na], h_mrf, T, natoms=na, nstates=NSTATES,
-                               precision="f32", flags=orc.NORMALIZE, nthreads=nthr)
-        t_dict = time.perf_counter() - t0
-        # one full B1 block (natoms atoms) built from the generated atoms
-        blk = atoms.astype(np.complex64)[np.arange(natoms) % na]
-        vox = (blk[rng.integers(0, natoms, nv)] + np.complex64(0.01)).astype(np.complex64)
-        t0 = time.perf_counter()
-        orc.match(vox, blk, params[:natoms], T, precision="f32", nthreads=nthr)
-        return t_dict, time.perf_counter() - t0
-
-    na0, nv0 = 4 * nthr, nthr
-    td0, tm0 = run(na0, nv0)
-    na = int(min(natoms, max(na0, na0 * (seconds / 2) / max(td0, 1e-3))))
-    nv = int(min(nvox, max(nv0, nv0 * (seconds / 2) / max(tm0, 1e-3))))
-    t_dict, t_match = run(na, nv)
-    step_s = t_dict / na * NATOMS + t_match / nv * nvox
-    sample = (f"oracle FP32 C (OpenMP {nthr} threads): dictionary {na} of {NATOMS} atoms "
-              f"({t_dict:.2f} s), matching {nv} of {nvox} voxels against one {natoms}-atom B1 block "
-              f"({t_match:.2f} s); step time extrapolated linearly")
-    return step_s, sample, nthr
-
-
-def cpu_baseline(seconds: float) -> dict:
-    step_s, sample, nthr = cpu_sample(seconds)
-    return {"value": round(NX * NY / step_s, 3), "unit": "voxels/s", "cores": nthr, "kind": "port",
-            "sample": sample}
+    params = orc.trans_params(t1, t2, b0, b1)
+    nb = len(b1)
+    natoms = params.shape[0] // nb
+    nvox = -(-NX * NY // nb)
+    bp = params[block * natoms:(block + 1) * natoms]
+    t0 = time.perf_counter()
+    atoms = orc.dict_atoms("epg_fisp", bp, h_mrf, T, natoms=natoms, nstates=NSTATES, precision="f32",
+                           flags=orc.ALL_B1_BLOCKS | orc.NORMALIZE, nthreads=nthr).astype(np.complex64)
+    t_dict = time.perf_counter() - t0
+    rng = np.random.default_rng(seed + block)
+    vox = (atoms[rng.integers(0, natoms, nvox)] * np.complex64(0.8 - 0.3j)).astype(np.complex64)
+    vox += (0.01 * (rng.standard_normal(vox.shape) + 1j * rng.standard_normal(vox.shape))).astype(np.complex64)
+    t0 = time.perf_counter()
+    orc.match(vox, atoms, bp, T, precision="f32", nthreads=nthr)
+    t_match = time.perf_counter() - t0
+    return {"seconds": t_dict + t_match, "dict_s": t_dict, "match_s": t_match, "atoms": natoms, "voxels": nvox,
+            "threads": nthr,
+            "sample": f"one of {nb} B1 blocks per step: {natoms} atoms generated (FP32 EPG, {nthr} OpenMP "
+                      f"threads, {t_dict:.2f} s) and {nvox} voxels matched against them ({t_match:.2f} s)"}
 
 
 def run_reference(args) -> None:
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    for _ in range(args.warmup):
-        cpu_sample(args.cpu_seconds / 4)
-    times = []
-    sample = ""
-    nthr = 1
-    for _ in range(args.steps):
-        s, sample, nthr = cpu_sample(args.cpu_seconds)
-        times.append(s)
-    step_s = float(np.mean(times))
-    value = NX * NY / step_s
-    line = {"impl": "reference", "metric": "dict atoms/s + matched voxels/s (voxels/s of the full dict+match step)",
-            "value": round(value, 3), "unit": "voxels/s", "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(step_s * 1e3, 1),
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic", "config": {"workload": WORKLOAD, "T": T, "nstates": NSTATES,
-                                            "voxels": NX * NY, "echo_type": "epg_fisp"},
+    for k in range(args.warmup):
+        cpu_step(k % 41)
+    steps = [cpu_step((args.warmup + k) % 41) for k in range(args.steps)]
+    secs = sum(s["seconds"] for s in steps)
+    vox = sum(s["voxels"] for s in steps)
+    value = vox / secs
+    nthr = steps[0]["threads"]
+    line = {"impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": "voxels/s",
+            "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(secs / args.steps * 1e3, 1), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "form": "fp32 (the reference's own form)", "T": T, "nstates": NSTATES,
+                       "atoms": 284458, "atoms_per_b1_block": 6938, "b1_blocks": 41, "voxels": NX * NY,
+                       "echo_type": "epg_fisp", "match": "fp32, nearest B1 block",
+                       "l2": "host memory", "parallelism": f"{nthr} host threads"},
             "cpu_baseline": {"value": round(value, 3), "unit": "voxels/s", "cores": nthr, "kind": "port",
-                             "sample": sample},
+                             "sample": steps[0]["sample"], "sample_atoms": steps[0]["atoms"],
+                             "sample_voxels": steps[0]["voxels"],
+                             "sample_seconds": round(secs / args.steps, 3), "extrapolated": False},
             "e2e": {"value": round(value, 3), "unit": "voxels/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -758,27 +1020,34 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--cpu-seconds", type=float, default=6.0,
-                    help="approximate CPU seconds of the bounded CPU sample")
+    ap.add_argument("--workload", choices=[WORKLOAD, WORKLOAD_C4], default=WORKLOAD)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
     ap.add_argument("--topk", type=int, default=0, choices=[0, 4, 8, 16],
                     help="tensor-core forms: candidates rescored in FP32 (0: library default, "
-                         "16 for BF16, 8 for FP16)")
+                         "16 for BF16 and FP8, 4 for FP16)")
     ap.add_argument("--b1-blocks", type=int, default=41,
                     help="reduced case for profiling: keep this many B1 blocks around 1.0")
     ap.add_argument("--nx", type=int, default=NX, help="reduced case for profiling: nx x nx voxels")
     ap.add_argument("--gn-iters", type=int, default=3,
-                    help="Gauss-Newton iterations (at most, per voxel) of the refined forms (0: skip them)")
-    ap.add_argument("--svd-sfrac", type=float, default=0.99999,
-                    help="energy fraction of the compressed-matching form (0: skip it)")
+                    help="Gauss-Newton iterations (at most, per voxel) of the refined forms")
     ap.add_argument("--gn-tol", type=float, default=1e-3,
                     help="a voxel stops refining once a step moves T1 and T2 by at most this (relative); "
                          "1e-3 lies below the noise-limited error at SNR 40 (~1e-3 median)")
+    ap.add_argument("--svd-sfrac", type=float, default=0.99999,
+                    help="energy fraction of the compressed-matching form (0: skip it)")
+    ap.add_argument("--oracle-sample", type=int, default=64,
+                    help="voxels whose headline maps are compared with the FP64 oracle's (0: skip)")
+    ap.add_argument("--c4-slices", type=int, default=8, help="ssfp workload: 256x256 slices")
+    ap.add_argument("--c4-match-steps", type=int, default=2, help="ssfp workload: timed matching calls")
+    ap.add_argument("--c4-fp32-voxels", type=int, default=4096, help="ssfp workload: voxels of the FP32 form")
+    ap.add_argument("--c4-topk16", type=int, default=8, help="ssfp workload: FP16 candidates rescored")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == WORKLOAD_C4:
+        run_c4(args)
     else:
         run_ours(args)
 

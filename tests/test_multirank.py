@@ -75,7 +75,7 @@ def test_reference_arm_under_torchrun_prints_one_line():
     port = _free_port()
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
            "--master-addr", "127.0.0.1", "--master-port", str(port), str(ROOT / "bench.py"),
-           "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "3", "--cpu-seconds", "0.3"]
+           "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "3"]
     env = dict(os.environ, OMP_NUM_THREADS="2")
     r = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=540, env=env,
                        stdin=subprocess.DEVNULL)
@@ -85,7 +85,21 @@ def test_reference_arm_under_torchrun_prints_one_line():
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["n_gpus"] == 2
     assert d["value"] > 0 and d["e2e"]["h2d_bytes_per_step"] == 0
-    assert d["cpu_baseline"]["kind"] == "port"
+    assert d["cpu_baseline"]["kind"] == "port" and d["cpu_baseline"]["extrapolated"] is False
+    assert d["config"]["atoms"] == 284458 and d["config"]["voxels"] == 57600
+
+
+def test_reference_arm_loads_no_product_code():
+    """The CPU arm runs the oracle alone: after one of its steps neither the
+    product package nor its library is loaded in the process."""
+    code = ("import sys; sys.path.insert(0, '.'); import bench; r = bench.cpu_step(3); "
+            "assert r['atoms'] == 6938 and r['voxels'] == 1405, r; "
+            "assert not any(m.startswith('snapmrf_b200') for m in sys.modules), sorted(sys.modules); "
+            "maps = open('/proc/self/maps').read(); assert 'libsnapmrf' not in maps; print('ok')")
+    env = dict(os.environ, OMP_NUM_THREADS="2")
+    r = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True, timeout=300,
+                       env=env, stdin=subprocess.DEVNULL)
+    assert r.returncode == 0 and r.stdout.strip().endswith("ok"), r.stderr[-3000:]
 
 
 def _shard_maps(r, nvox=64):
