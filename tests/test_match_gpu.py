@@ -239,7 +239,11 @@ def test_host_image_streamed_in_chunks(snap, oracle, prec):
         assert snap.device_error(reset=True) == 0
         for name in ("pageable", "pinned"):
             np.testing.assert_array_equal(out[name][1], out["device"][1])
-            np.testing.assert_array_equal(out[name][0], out["device"][0])
+            np.testing.assert_array_equal(out[name][0][:, :4], out["device"][0][:, :4])
+            # the FP32 form's PD is bit-equal; the tensor-core rescoring sums
+            # two samples per load when rows are 16-byte aligned (the dense
+            # uploaded copy, not the padded device rows): last-bit changes
+            np.testing.assert_allclose(out[name][0][:, 4], out["device"][0][:, 4], rtol=0 if prec == 0 else 1e-6)
 
 
 def test_streamed_upload_options_are_checked(snap, oracle):

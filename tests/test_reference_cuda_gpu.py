@@ -180,9 +180,11 @@ def decided(img, dicts, blocks=None, natoms=None, gap=1e-6):
     every dictionary in `dicts` (the reference's and this implementation's
     atoms, which differ by FP32 rounding): the same first argmax under each,
     leading the runner-up by more than `gap` (relative) under each.  With
-    `blocks`, each voxel is scored within its B1 block only."""
+    `blocks`, each voxel is scored within its B1 block only.  Returns the
+    mask and each voxel's smallest relative gap."""
     n = img.shape[0]
     ok = np.ones(n, bool)
+    mingap = np.full(n, np.inf)
     first = None
     for d in dicts:
         if blocks is None:
@@ -193,12 +195,37 @@ def decided(img, dicts, blocks=None, natoms=None, gap=1e-6):
                 sel = blocks == j
                 b[sel], s[sel], a[sel] = top2_fp64(img[sel], d[j * natoms:(j + 1) * natoms])
                 a[sel] += j * natoms
-        ok &= (b - s) > gap * b
+        g = (b - s) / b
+        mingap = np.minimum(mingap, g)
+        ok &= g > gap
         if first is None:
             first = a
         else:
             ok &= a == first
-    return ok
+    return ok, mingap
+
+
+def fp32_sum_margin(nreps):
+    """Relative rounding of an FP32 inner product over nreps samples, four
+    times its random-walk size sqrt(nreps) 2^-24: two FP32 implementations
+    that sum in different orders (cuBLAS's and this one's) can pick
+    different atoms for gaps below it."""
+    return 4.0 * np.sqrt(nreps) * 2.0 ** -24
+
+
+def assert_same_where_decided(maps, ref_maps, sure, mingap, nreps, what):
+    """Equal (T1, T2, B0, B1) wherever the pick is decided (gap > 1e-6 under
+    both dictionaries) by more than the FP32 summation margin; among the
+    decided voxels inside that margin at most 0.1 % may differ."""
+    diff = (maps[:, :4] != ref_maps[:, :4]).any(axis=1)
+    margin = fp32_sum_margin(nreps)
+    firm = sure & (mingap > margin)
+    soft = sure & ~firm & diff
+    print(f"{what}: {diff.sum()} of {len(diff)} voxels differ from the reference; {(diff & firm).sum()} with a "
+          f"gap above the FP32 summation margin {margin:.2e}, {soft.sum()} decided ones below it"
+          + (f" (gaps {np.sort(mingap[soft])[:5]})" if soft.any() else ""))
+    np.testing.assert_array_equal(maps[firm, :4], ref_maps[firm, :4])
+    assert soft.sum() <= 1e-3 * len(diff)
 
 
 def nearest_block(b1map, b1s):
@@ -314,13 +341,11 @@ def test_c1_shape_matching_vs_reference_cuda(snap, c1_blocks):
     # FP32 form on the unit-norm dictionary
     atoms = run_dict(snap, "epg_fisp", params, h, T, natoms=natoms, nstates=w,
                      flags=snap.DICT_ALL_B1_BLOCKS | snap.DICT_NORMALIZE)
-    sure = decided(img, (ref_unit, atoms), blk, natoms)
+    sure, mingap = decided(img, (ref_unit, atoms), blk, natoms)
     print(f"voxels decided by a gap > 1e-6 under both dictionaries: {sure.mean():.4f}")
     assert sure.mean() > 0.9
     maps, _ = run_match(snap, img, atoms, params, natoms=natoms, b1map=b1map, b1_device=True)
-    diff = (maps[:, :4] != ref_maps[:, :4]).any(axis=1)
-    print(f"FP32 form: {diff.sum()} of {n} voxels differ from the reference ({(diff & sure).sum()} decided)")
-    np.testing.assert_array_equal(maps[sure, :4], ref_maps[sure, :4])
+    assert_same_where_decided(maps, ref_maps, sure, mingap, T, "FP32 form")
     np.testing.assert_allclose(maps[:, 4], ref_maps[:, 4], rtol=1e-5)
 
     # headline FP16 form
@@ -336,11 +361,8 @@ def test_c1_shape_matching_vs_reference_cuda(snap, c1_blocks):
     m16 = d_maps.cpu().numpy()
     a = d_atoms.cpu().numpy()
     head = (a[..., 0] + 1j * a[..., 1]) / d_norms.cpu().numpy()[:, None]
-    sure = decided(img, (ref_unit, head), blk, natoms)
-    diff = (m16[:, :4] != ref_maps[:, :4]).any(axis=1)
-    print(f"FP16 headline form: {diff.sum()} of {n} voxels differ from the reference "
-          f"({(diff & sure).sum()} decided)")
-    np.testing.assert_array_equal(m16[sure, :4], ref_maps[sure, :4])
+    sure, mingap = decided(img, (ref_unit, head), blk, natoms)
+    assert_same_where_decided(m16, ref_maps, sure, mingap, T, "FP16 headline form")
     np.testing.assert_allclose(m16[:, 4], ref_maps[:, 4], rtol=1e-5)
 
 
@@ -384,11 +406,11 @@ def test_c4_shape_ssfp_vs_reference_cuda(snap, tmp_path):
     img = img.astype(np.complex64)
 
     ref_maps = ref_match(snap, tmp_path, img, ref, params, natoms)
-    sure = decided(img, (ref, got))
+    sure, mingap = decided(img, (ref, got))
     print(f"voxels decided by a gap > 1e-6 under both dictionaries: {sure.mean():.4f}")
     assert sure.mean() > 0.9
     maps, _ = run_match(snap, img, got, params, natoms=natoms)
-    np.testing.assert_array_equal(maps[sure, :4], ref_maps[sure, :4])
+    assert_same_where_decided(maps, ref_maps, sure, mingap, T, "C4 shape FP32 form")
     np.testing.assert_allclose(maps[:, 4], ref_maps[:, 4], rtol=1e-5)
     # the tensor-core forms pick among their top-k by exact FP32 rescoring:
     # FP16 (11-bit significands) keeps the decided voxel's best in its list
