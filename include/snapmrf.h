@@ -343,9 +343,18 @@ int snapmrf_svd_compress(const float *d_atoms, size_t nreps, size_t NATOMS, size
  * bounded wait of the tensor-core matching kernel ran out (the maps of that
  * call are NaN); 7 SNAPMRF_MATCH_IMAG_ATOMS was given atoms with a non-zero
  * real part (NaN maps); 9 snapmrf_mrf_match_noalloc was given a B1 map and
- * a B1 block holding several B1 values (NaN maps, indices -1).
+ * a B1 block holding several B1 values (NaN maps, indices -1); 10 the
+ * bounded-wait self-test (snapmrf_selftest_bounded_wait).
  * Synchronises the current device; clears the word when reset != 0. */
 int snapmrf_device_error(int reset);
+
+/* Self-test of the bounded waits behind the device error word: launches one
+ * warp that waits, with a limit of limit_us microseconds (1 .. 2,000,000),
+ * on an mbarrier that nothing arrives on, the wait primitive of the
+ * tensor-core kernels.  The wait gives up, the kernel returns and the error
+ * word becomes 10 (snapmrf_device_error).  Nothing else is in flight in that
+ * kernel, so the device stays usable.  No counterpart in the reference. */
+int snapmrf_selftest_bounded_wait(unsigned limit_us, void *stream);
 
 /* Largest request snapmrf_mrf_match_noalloc accepts: its working arrays live
  * in one fixed array of about 1.3 MiB per GPU (sized for 65,536 voxels and

@@ -93,6 +93,7 @@ def lib() -> C.CDLL:
         L.snapmrf_kernel_launches.restype = C.c_uint64
         L.snapmrf_scratch_allocations.restype = C.c_uint64
         L.snapmrf_device_error.argtypes = [C.c_int]
+        L.snapmrf_selftest_bounded_wait.argtypes = [C.c_uint, C.c_void_p]
         L.snapmrf_csv_dim.restype = sz
         L.snapmrf_csv_dim.argtypes = [C.c_char_p]
         L.snapmrf_csv_read.argtypes = [vp, sz, C.c_char_p]
@@ -133,6 +134,13 @@ def lib() -> C.CDLL:
 def device_error(reset: bool = False) -> int:
     """Error word of the tensor-core kernels (0 = none); synchronises the device."""
     return lib().snapmrf_device_error(1 if reset else 0)
+
+
+def selftest_bounded_wait(limit_us: int = 1000, stream=None) -> None:
+    """Runs one warp that waits with a limit of limit_us on an mbarrier
+    nothing arrives on (the tensor-core kernels' wait primitive): the wait
+    gives up and device_error() then reads 10."""
+    _check(lib().snapmrf_selftest_bounded_wait(limit_us, _stream_ptr(stream)))
 
 
 def kernel_launches() -> int:

@@ -826,6 +826,21 @@ __global__ void publish_error_kernel(const int *err) {
     if (*err) atomicCAS(&g_device_error, 0, *err);
 }
 
+// Self-test of the bounded wait: an mbarrier that expects one arrival,
+// which nothing makes; thread 0 waits on it with a limit of limit_ns, the
+// wait gives up, records code 10 and the kernel returns.  No copy or MMA is
+// in flight, so giving up leaves nothing behind.
+__global__ void bounded_wait_selftest_kernel(int *err, unsigned long long limit_ns) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        sm100::mbar_init(&bar, 1);
+        sm100::fence_mbar_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) sm100::mbar_wait(&bar, 0, err, 10, limit_ns);
+    __syncthreads();
+}
+
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
     static std::once_flag once;
@@ -1073,6 +1088,22 @@ int match_bf16(const TcMatchRequest &q, cudaStream_t st) {
 
 namespace snapmrf {
 cudaError_t noalloc_device_error(int *value, int reset);
+}
+
+extern "C" int snapmrf_selftest_bounded_wait(unsigned limit_us, void *stream) {
+    using namespace snapmrf;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (limit_us == 0 || limit_us > 2000000u)
+        SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "selftest_bounded_wait: limit must be in [1, 2000000] us (got %u)",
+                     limit_us);
+    DeviceScratch s;
+    SNAPMRF_CUDA(s.alloc(sizeof(int), st));
+    SNAPMRF_CUDA(cudaMemsetAsync(s.ptr, 0, sizeof(int), st));
+    tc::bounded_wait_selftest_kernel<<<1, 32, 0, st>>>(s.as<int>(), 1000ull * limit_us);
+    SNAPMRF_LAUNCH_CHECK();
+    tc::publish_error_kernel<<<1, 1, 0, st>>>(s.as<int>());
+    SNAPMRF_LAUNCH_CHECK();
+    return SNAPMRF_OK;
 }
 
 extern "C" int snapmrf_device_error(int reset) {

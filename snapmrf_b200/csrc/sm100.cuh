@@ -51,14 +51,16 @@ __device__ __forceinline__ uint64_t globaltimer_ns() {
 }
 
 // Waits for the phase with the given parity to complete.  Gives up after
-// about two seconds, records `code` in *err and returns false, so that a
-// wrong arrival or byte count can never hang the GPU.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *err, int code) {
+// limit_ns (about two seconds by default), records `code` in *err and
+// returns false, so that a wrong arrival or byte count can never hang the
+// GPU.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *err, int code,
+                                          uint64_t limit_ns = 2000000000ull) {
     if (mbar_try_wait(bar, parity)) return true;
     const uint64_t t0 = globaltimer_ns();
     for (uint32_t it = 1;; ++it) {
         if (mbar_try_wait(bar, parity)) return true;
-        if ((it & 255u) == 0 && globaltimer_ns() - t0 > 2000000000ull) break;
+        if ((it & 255u) == 0 && globaltimer_ns() - t0 > limit_ns) break;
     }
     atomicCAS(err, 0, code);
     return false;

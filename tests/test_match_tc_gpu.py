@@ -225,3 +225,29 @@ def test_packed_atoms_are_rejected_where_they_do_not_apply(snap):
     d_maps = torch.empty((3, 5), device="cuda")
     with pytest.raises(snap.SnapMRFError):   # packed atoms need the imaginary-atom form
         snap.MRF_match(d_maps, img, d_atoms, d_params, T, T, 2, 2, 3, precision=FP16, packed_atoms=d_packed)
+
+
+def test_bounded_wait_runs_out_and_reports(snap):
+    """The wait primitive of the tensor-core kernels (an mbarrier wait bounded
+    by %globaltimer) made to run out: one warp waits 2 ms on an mbarrier that
+    nothing arrives on, gives up, returns, and the device error word reads
+    10; the device keeps working (a tensor-core match afterwards runs clean
+    and agrees with FP32)."""
+    import time
+    import torch
+    assert snap.device_error(reset=True) == 0
+    t0 = time.perf_counter()
+    snap.selftest_bounded_wait(2000)
+    torch.cuda.synchronize()
+    took = time.perf_counter() - t0
+    assert snap.device_error(reset=True) == 10
+    assert took < 5.0
+    assert snap.device_error(reset=True) == 0
+    with pytest.raises(snap.SnapMRFError, match="limit must be"):
+        snap.selftest_bounded_wait(0)
+    atoms, params, natoms = _dictionary(snap, 128, [1.0])
+    img = _voxels(atoms, 300, 31)
+    m32, i32 = run_match(snap, img, atoms, params)
+    m16, i16 = run_match(snap, img, atoms, params, precision=FP16)
+    assert snap.device_error(reset=True) == 0
+    compare(img, atoms, params, m32, i32, m16, i16)
