@@ -180,6 +180,21 @@ int snapmrf_mrf_dict(float *d_atoms, const float *d_params, const float *h_mrf,
                      int nparams, int nstates, const char *echo_type,
                      const snapmrf_dict_opts *opts, void *stream);
 
+/* Engine-level generation, as the reference's echo-type engines
+ * epg_sr / epg_se / epg_tse / epg_fisp / epg_ssfp / roa_ssfp run it
+ * (src/functions.h:89-113, src/functions.cu:687-1222): the schedule is
+ * already converted and in device memory, d_mrf [4][nreps] = {flip (rad),
+ * phase (rad), TR (ms), TE (ms)} (no CSV conversion), and the atoms are not
+ * normalised unless SNAPMRF_DICT_NORMALIZE asks for it (MRF_dict normalises
+ * the epg_ssfp / roa_ssfp atoms after the engine, src/functions.cu:1268,
+ * 1297).  ti: epg_ssfp's inversion delay in ms (MRF_dict passes 40); the
+ * other echo types ignore it.  Blocks, options and limits as for
+ * snapmrf_mrf_dict.  Synchronises `stream` once (the schedule is read back
+ * to choose the recursion). */
+int snapmrf_dict_engine(float *d_atoms, const float *d_params, const float *d_mrf, float ti,
+                        size_t nreps, size_t NATOMS, size_t natoms, int nparams, int nstates,
+                        const char *echo_type, const snapmrf_dict_opts *opts, void *stream);
+
 /* In-place unit-l2 normalisation of NATOMS atoms of nreps samples
  * (replaces the normalize kernel, src/functions.cu:670-685). */
 int snapmrf_normalize(float *d_atoms, size_t nreps, size_t NATOMS, float *d_norms,

@@ -51,6 +51,22 @@ void trans_params(float *h_params, float *h_t1, float *h_t2, float *h_b0, float 
 size_t compute_natoms(float *h_t1, float *h_t2, size_t l_t1, size_t l_t2, size_t l_b0, size_t l_b1);
 void MRF_dict(float2 *d_atoms, float *d_params, float *h_mrf, size_t nreps, size_t NREPS, size_t NATOMS,
               size_t natoms, int nparams, int nstates, const char *echo_type);
+void epg_sr(float2 *d_atoms, float *d_params, float *d_mrf, size_t nreps, size_t natoms, int nparams, int nstates);
+void epg_se(float2 *d_atoms, float *d_params, float *d_mrf, size_t nreps, size_t natoms, int nparams, int nstates);
+void epg_tse(float2 *d_atoms, float *d_params, float *d_mrf, size_t nreps, size_t natoms, int nparams, int nstates);
+void epg_fisp(float2 *d_atoms, float *d_params, float *d_mrf, size_t nreps, size_t natoms, int nparams,
+              int nstates);
+void epg_ssfp(float2 *d_atoms, float *d_params, float *d_mrf, float TI, size_t nreps, size_t NATOMS, size_t natoms,
+              int nparams, int nstates);
+void roa_ssfp(float2 *d_atoms, float *d_mrf, float *d_params, size_t nreps, size_t natoms, int nparams);
+#ifdef __CUDACC__
+/* the reference's kernel (src/functions.h:87): callers launch it with
+ * normalize<<<grid, block>>>(...) from code compiled without relocatable
+ * device code */
+__global__ void normalize(float2 *d_atoms, size_t nreps, size_t NATOMS);
+#endif
+void MRF_minimatch(float *d_maps, float2 *d_img, float2 *d_atoms, float2 *d_mat, float *d_params, size_t nreps,
+                   size_t NATOMS, size_t nminivoxels, int nparams, int nmaps);
 void compute_nsplits(size_t *nsplits, size_t *nminivoxels, size_t nvoxels, size_t NATOMS, int type);
 void MRF_match(float *d_maps, float2 *h_img, float2 *d_atoms, float *d_params, size_t NREPS, size_t nreps,
                size_t NATOMS, size_t natoms, size_t nvoxels, int nparams, int nmaps, const char *in_b1map);

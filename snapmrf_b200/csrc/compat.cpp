@@ -23,6 +23,8 @@ int blocksize = 64;
 int gridsize = 128;
 cudaStream_t stream[2];
 
+static int env_precision();
+
 static void die(int status, const char *what) {
     fprintf(stderr, "%s: %s\n", what, snapmrf_last_error());
     exit(status == SNAPMRF_ERR_ECHO_TYPE ? EX_USAGE : EXIT_FAILURE);
@@ -163,6 +165,89 @@ void MRF_dict(float2 *d_atoms, float *d_params, float *h_mrf, size_t nreps, size
                               nparams, nstates, echo_type, &o, stream[0]);
     if (rc == SNAPMRF_ERR_ECHO_TYPE) errx(EX_USAGE, "Please put in correct echo types.");
     if (rc) die(rc, "MRF_dict");
+    gpuAssert(cudaStreamSynchronize(stream[0]), __FILE__, __LINE__);
+}
+
+// The echo-type engines (src/functions.h:89-113): the schedule d_mrf is
+// already converted and on the device; the atoms are left as the recursion
+// produces them (MRF_dict normalises epg_ssfp / roa_ssfp afterwards).  They
+// return after the device work, as the reference's do.  The non-SSFP
+// engines fill natoms atoms of block 0; epg_ssfp fills every block.
+static void engine(const char *echo, float2 *d_atoms, float *d_params, float *d_mrf, float ti, size_t nreps,
+                   size_t NATOMS, size_t natoms, int nparams, int nstates) {
+    snapmrf_dict_opts o;
+    memset(&o, 0, sizeof o);
+    o.flags = SNAPMRF_DICT_SEPARATE_RELAX;
+    o.n_iso = 1;
+    int rc = snapmrf_dict_engine(reinterpret_cast<float *>(d_atoms), d_params, d_mrf, ti, nreps, NATOMS, natoms,
+                                 nparams, nstates, echo, &o, stream[0]);
+    if (rc) die(rc, echo);
+    gpuAssert(cudaStreamSynchronize(stream[0]), __FILE__, __LINE__);
+}
+
+// epg_sr (src/functions.cu:687-739)
+void epg_sr(float2 *d_atoms, float *d_params, float *d_mrf, size_t nreps, size_t natoms, int nparams, int nstates) {
+    engine("epg_sr", d_atoms, d_params, d_mrf, 0.f, nreps, natoms, natoms, nparams, nstates);
+}
+
+// epg_se (src/functions.cu:741-807)
+void epg_se(float2 *d_atoms, float *d_params, float *d_mrf, size_t nreps, size_t natoms, int nparams, int nstates) {
+    engine("epg_se", d_atoms, d_params, d_mrf, 0.f, nreps, natoms, natoms, nparams, nstates);
+}
+
+// epg_tse (src/functions.cu:809-876)
+void epg_tse(float2 *d_atoms, float *d_params, float *d_mrf, size_t nreps, size_t natoms, int nparams, int nstates) {
+    engine("epg_tse1", d_atoms, d_params, d_mrf, 0.f, nreps, natoms, natoms, nparams, nstates);
+}
+
+// epg_fisp (src/functions.cu:878-933)
+void epg_fisp(float2 *d_atoms, float *d_params, float *d_mrf, size_t nreps, size_t natoms, int nparams,
+              int nstates) {
+    engine("epg_fisp", d_atoms, d_params, d_mrf, 0.f, nreps, natoms, natoms, nparams, nstates);
+}
+
+// epg_ssfp (src/functions.cu:935-1019): every B1 block, inversion with delay TI
+void epg_ssfp(float2 *d_atoms, float *d_params, float *d_mrf, float TI, size_t nreps, size_t NATOMS, size_t natoms,
+              int nparams, int nstates) {
+    engine("epg_ssfp", d_atoms, d_params, d_mrf, TI, nreps, NATOMS, natoms, nparams, nstates);
+}
+
+// roa_ssfp (src/functions.cu:1155-1222): one isochromat, block 0
+void roa_ssfp(float2 *d_atoms, float *d_mrf, float *d_params, size_t nreps, size_t natoms, int nparams) {
+    engine("roa_ssfp", d_atoms, d_params, d_mrf, 0.f, nreps, natoms, natoms, nparams, 1);
+}
+
+// normalize (src/functions.cu:670-685), the reference's kernel, launched by
+// the caller with any grid and block: atoms are walked grid-stride, one
+// thread per atom, the squared moduli summed in time order.
+__global__ void normalize(float2 *d_atoms, size_t nreps, size_t NATOMS) {
+    for (size_t id = blockIdx.x * (size_t)blockDim.x + threadIdx.x; id < NATOMS;
+         id += (size_t)blockDim.x * gridDim.x) {
+        float2 *a = d_atoms + id * nreps;
+        float sum = 0.f;
+        for (size_t i = 0; i < nreps; i++) {
+            const float n2 = a[i].x * a[i].x + a[i].y * a[i].y;
+            sum += n2;
+        }
+        if (sum > 0.f) sum = 1.f / sqrtf(sum);
+        for (size_t i = 0; i < nreps; i++) a[i] = make_float2(a[i].x * sum, a[i].y * sum);
+    }
+}
+
+// MRF_minimatch (src/functions.cu:1464-1491): the first argmax of |<atom,
+// voxel>| over all NATOMS atoms for nminivoxels device voxels, maps written
+// as generate_maps does.  The matching never forms the score matrix, so
+// d_mat (the reference's cuBLAS output) is not written.
+void MRF_minimatch(float *d_maps, float2 *d_img, float2 *d_atoms, float2 *d_mat, float *d_params, size_t nreps,
+                   size_t NATOMS, size_t nminivoxels, int nparams, int nmaps) {
+    (void)d_mat;
+    snapmrf_match_opts o;
+    memset(&o, 0, sizeof o);
+    o.precision = env_precision();
+    int rc = snapmrf_mrf_match(d_maps, reinterpret_cast<const float *>(d_img), 0,
+                               reinterpret_cast<const float *>(d_atoms), d_params, nreps, NATOMS, NATOMS,
+                               nminivoxels, nparams, nmaps, &o, stream[0]);
+    if (rc) die(rc, "MRF_minimatch");
     gpuAssert(cudaStreamSynchronize(stream[0]), __FILE__, __LINE__);
 }
 

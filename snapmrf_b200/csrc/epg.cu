@@ -262,10 +262,14 @@ static cudaError_t launch_epg(int echo, const EpgArgs &a, int S, dim3 grid, cuda
 
 using namespace snapmrf;
 
-extern "C" int snapmrf_mrf_dict(float *d_atoms, const float *d_params, const float *h_mrf,
-                                size_t nreps, size_t NREPS, size_t NATOMS, size_t natoms,
-                                int nparams, int nstates, const char *echo_type,
-                                const snapmrf_dict_opts *opts, void *stream) {
+// MRF_dict and the engine-level entry point.  convert: apply MRF_dict's
+// schedule conversion for epg_ssfp / roa_ssfp (the engines take the
+// converted schedule); ti: epg_ssfp's inversion delay; engine: normalise only
+// on request (MRF_dict normalises the epg_ssfp / roa_ssfp atoms after the
+// engine has run, src/functions.cu:1268, 1297).
+static int dict_impl(float *d_atoms, const float *d_params, const float *h_mrf, size_t nreps, size_t NREPS,
+                     size_t NATOMS, size_t natoms, int nparams, int nstates, const char *echo_type,
+                     const snapmrf_dict_opts *opts, void *stream, bool convert, float ti, bool engine) {
     cudaStream_t st = (cudaStream_t)stream;
     int echo = parse_echo(echo_type);
     if (echo < 0)
@@ -293,7 +297,7 @@ extern "C" int snapmrf_mrf_dict(float *d_atoms, const float *d_params, const flo
     if (nblocks > 65535) SNAPMRF_FAIL(SNAPMRF_ERR_UNSUPPORTED, "MRF_dict: more than 65535 B1 blocks");
     const bool all_blocks = (echo == ECHO_SSFP) || (flags & SNAPMRF_DICT_ALL_B1_BLOCKS);
     const size_t gen_blocks = all_blocks ? nblocks : 1;
-    const bool normalize = echo == ECHO_SSFP || echo == ECHO_ROA || (flags & SNAPMRF_DICT_NORMALIZE);
+    const bool normalize = (!engine && (echo == ECHO_SSFP || echo == ECHO_ROA)) || (flags & SNAPMRF_DICT_NORMALIZE);
     const bool pack_normalized = (flags & SNAPMRF_DICT_NORMALIZE_OPERAND) != 0;
     if (pack_normalized && (normalize || !(opts && opts->d_packed)))
         SNAPMRF_FAIL(SNAPMRF_ERR_INVALID,
@@ -306,7 +310,7 @@ extern "C" int snapmrf_mrf_dict(float *d_atoms, const float *d_params, const flo
     std::vector<float> sched(4 * nreps);
     for (int r = 0; r < 4; r++)
         for (size_t t = 0; t < nreps; t++) sched[r * nreps + t] = h_mrf[r * NREPS + t];
-    if (echo == ECHO_SSFP || echo == ECHO_ROA) {
+    if (convert && (echo == ECHO_SSFP || echo == ECHO_ROA)) {
         const float nominal_flip = 60.f, TR_base = 16.f, TE_base = 3.5f;
         const float fa_scale = (float)(nominal_flip * M_PI / 180.f);
         const float ph_scale = (float)(M_PI / 180.f);
@@ -352,7 +356,7 @@ extern "C" int snapmrf_mrf_dict(float *d_atoms, const float *d_params, const flo
     a.init_alpha_deg = (echo == ECHO_SSFP || echo == ECHO_ROA) ? 180.f
                        : (echo == ECHO_SE || echo == ECHO_TSE) ? 90.f : 0.f;
     a.init_phi_deg = (echo == ECHO_SE || echo == ECHO_TSE) ? 90.f : 0.f;
-    a.init_ti = (echo == ECHO_SSFP) ? 40.f : 0.f;
+    a.init_ti = (echo == ECHO_SSFP) ? ti : 0.f;
     a.packed = nullptr;
     a.packed_half = 0;
     a.packed_pitch = 0;
@@ -406,6 +410,29 @@ extern "C" int snapmrf_mrf_dict(float *d_atoms, const float *d_params, const flo
         SNAPMRF_CUDA(launch_epg(echo, a, S, grid, st));
     }
     return SNAPMRF_OK;
+}
+
+extern "C" int snapmrf_mrf_dict(float *d_atoms, const float *d_params, const float *h_mrf,
+                                size_t nreps, size_t NREPS, size_t NATOMS, size_t natoms,
+                                int nparams, int nstates, const char *echo_type,
+                                const snapmrf_dict_opts *opts, void *stream) {
+    return dict_impl(d_atoms, d_params, h_mrf, nreps, NREPS, NATOMS, natoms, nparams, nstates, echo_type, opts,
+                     stream, true, 40.f, false);
+}
+
+extern "C" int snapmrf_dict_engine(float *d_atoms, const float *d_params, const float *d_mrf, float ti,
+                                   size_t nreps, size_t NATOMS, size_t natoms, int nparams, int nstates,
+                                   const char *echo_type, const snapmrf_dict_opts *opts, void *stream) {
+    if (!d_mrf || nreps == 0) SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "dict_engine: null schedule or nreps 0");
+    if (!(ti >= 0.f)) SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "dict_engine: TI must be >= 0");
+    // the schedule comes back to the host once: the real-valued recursion is
+    // chosen from its RF phases, and the kernels take it staged per call
+    std::vector<float> h(4 * nreps);
+    cudaStream_t st = (cudaStream_t)stream;
+    SNAPMRF_CUDA(cudaMemcpyAsync(h.data(), d_mrf, h.size() * sizeof(float), cudaMemcpyDeviceToHost, st));
+    SNAPMRF_CUDA(cudaStreamSynchronize(st));
+    return dict_impl(d_atoms, d_params, h.data(), nreps, nreps, NATOMS, natoms, nparams, nstates, echo_type, opts,
+                     stream, false, ti, true);
 }
 
 namespace snapmrf {

@@ -1,7 +1,7 @@
 """Regenerates tests/golden/golden.npz from the reference.
 
-Run in a container that has the reference tree (REF_ROOT, default
-/root/reference) and the reference harness built (`make -C oracle ref`):
+Run in a container that has the reference tree (REF_ROOT, default: a
+checkout named "reference" beside this repository) and the reference harness built (`make -C oracle ref`):
 
     python tests/golden/make_golden.py
 
@@ -30,7 +30,7 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 REPO = HERE.parent.parent
-REF = Path(os.environ.get("REF_ROOT", "/root/reference"))
+REF = Path(os.environ.get("REF_ROOT", str(Path(__file__).resolve().parents[3] / "reference")))
 HARNESS = REPO / "oracle" / "_ref" / "ref_harness"
 
 sys.path.insert(0, str(HERE.parent))

@@ -110,3 +110,34 @@ def test_mrf_cli_matches_reference(snap, tmp_path):
         assert rel.max() < 1e-5
         np.testing.assert_array_equal(maps[:, :4], ref_maps[:, :4])
         np.testing.assert_allclose(maps[:, 4], ref_maps[:, 4], rtol=1e-5)
+
+
+@pytest.mark.skipif(not (REF / "engine_on_snapmrf").exists(), reason="engine driver not built")
+def test_engine_entry_points_link_and_agree(tmp_path):
+    """A caller of the reference's engine-level functions (epg_sr / epg_se /
+    epg_tse / epg_fisp / epg_ssfp / roa_ssfp on a device schedule, the
+    normalize kernel launched with <<<gridsize, blocksize>>>, MRF_minimatch;
+    src/functions.h:87-134), compiled once from one source, linked against
+    the reference's own functions.o and against libsnapmrf_compat.so: atoms
+    within 1e-5 (per atom, max-norm relative), normalised atoms within 5e-6
+    and identical maps."""
+    outs = {}
+    for name in ("engine_ref", "engine_on_snapmrf"):
+        prefix = tmp_path / name
+        r = subprocess.run([str(REF / name), str(prefix)], stdin=subprocess.DEVNULL, capture_output=True,
+                           text=True, timeout=600)
+        assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+        outs[name] = prefix
+    for eng in ("sr", "se", "tse", "ssfp", "roa", "fisp", "norm"):
+        a = np.fromfile(f"{outs['engine_ref']}_{eng}.c64", np.complex64)
+        b = np.fromfile(f"{outs['engine_on_snapmrf']}_{eng}.c64", np.complex64)
+        assert a.size == b.size and a.size > 0
+        a, b = a.reshape(-1, 60), b.reshape(-1, 60)
+        scale = np.maximum(np.abs(a).max(axis=1), 1e-30)
+        rel = np.abs(a - b).max(axis=1) / scale
+        print(f"{eng}: {a.shape[0]} atoms, max rel {rel.max():.2e}")
+        assert rel.max() < (5e-6 if eng == "norm" else 1e-5)
+    ma = np.fromfile(f"{outs['engine_ref']}_maps.f32", np.float32).reshape(-1, 5)
+    mb = np.fromfile(f"{outs['engine_on_snapmrf']}_maps.f32", np.float32).reshape(-1, 5)
+    np.testing.assert_array_equal(ma[:, :4], mb[:, :4])
+    np.testing.assert_allclose(ma[:, 4], mb[:, 4], rtol=1e-5)
