@@ -517,8 +517,14 @@ def run_ours(args) -> None:
     PRECS = {"fp32": snap.PREC_FP32, "bf16": snap.PREC_BF16, "fp16": snap.PREC_FP16, "fp8": snap.PREC_FP8}
     TC = ("bf16", "fp16", "fp8")
     HEAD = "bf16+gn"
-    forms = {name: timed(p) for name, p in PRECS.items()}
-    forms.update({f"{name}+gn": timed(PRECS[name], gn=args.gn_iters) for name in TC})
+    # the FP32 form and the headline are always timed; --forms limits the rest
+    want = set(args.forms.split(",")) if args.forms else None
+
+    def wanted(f):
+        return want is None or f in want or f in ("fp32", HEAD)
+    forms = {name: timed(p) for name, p in PRECS.items() if wanted(name)}
+    forms.update({f"{name}+gn": timed(PRECS[name], gn=args.gn_iters) for name in TC if wanted(f"{name}+gn")})
+    TC = tuple(f for f in TC if f in forms)
 
     # argmax agreement with the FP32 form, counting a different atom as
     # agreeing when its exact FP32 score is within 1e-6 of the FP32 form's
@@ -595,7 +601,7 @@ def run_ours(args) -> None:
             tie = cm[:, 4] >= pd32 * (1 - 1e-6)
             vt1, vt2, _ = truth
             comp.update(match_ms=round(cms, 3), match_voxels_per_s=round(nvox / (cms / 1e3), 1),
-                        uncompressed_fp16_match_ms=round(forms["fp16"]["match_ms"], 3),
+                        uncompressed_fp16_match_ms=round(forms["fp16"]["match_ms"], 3) if "fp16" in forms else None,
                         launches_per_match=(snap.kernel_launches() - l0) // args.steps,
                         argmax_agreement_vs_fp32=round(float(np.mean(same | tie)), 6),
                         argmax_agreement_vs_fp32_raw=round(float(np.mean(same)), 6),
@@ -824,50 +830,54 @@ def run_c4(args) -> None:
     h = c4_schedule(4, T4)
     t1, t2 = geometric(100.0, 5000.0), geometric(10.0, 2000.0)
     b0 = np.array([-100.0 + 4.0 * k for k in range(51)], np.float32)
+    if args.c4_b0 < 51:   # a reduced case for profiling: every k-th B0 value
+        b0 = b0[::-(-51 // args.c4_b0)]
     b1 = np.array([0.8, 0.9, 1.0, 1.1, 1.2], np.float32)
     params = snap.trans_params(t1, t2, b0, b1)
     NATOMS = params.shape[0]
     natoms = NATOMS // len(b1)
     nxy = 256
     nvox = nxy * nxy * args.c4_slices
-    # voxels: per slice the tissue phantom (seeded per slice), a B0 field of
-    # +-80 Hz (linear + quadratic), and a B1 field 1 + 0.2 (x^2 + y^2 - 0.5)
-    # snapped to the dictionary's B1 values (the bSSFP recursion takes B1 per
-    # block); T1 / T2 / B0 off the grid
-    vt1, vt2, vb0, vb1, m0, ph = [], [], [], [], [], []
-    y, x = np.meshgrid(np.linspace(-1, 1, nxy), np.linspace(-1, 1, nxy), indexing="ij")
-    for s in range(args.c4_slices):
-        _, a1, a2, m, p = phantom(100 * rank + s, nxy)
-        zc = -1 + 2 * (s + 0.5) / max(args.c4_slices, 1)
-        f0 = np.clip(40.0 * x + 25.0 * y + 15.0 * (x ** 2 + y ** 2 + zc ** 2) - 10.0, -80.0, 80.0)
-        fb1 = np.clip(1.0 + 0.2 * (x ** 2 + y ** 2 - 0.5), 0.8, 1.2)
-        vt1.append(a1)
-        vt2.append(a2)
-        vb0.append(f0.reshape(-1).astype(np.float32))
-        vb1.append(b1[np.argmin(np.abs(fb1.reshape(-1)[:, None] - b1[None, :]), axis=1)])
-        m0.append(m)
-        ph.append(p)
-    vt1, vt2, vb0, vb1, m0, ph = (np.concatenate(v) for v in (vt1, vt2, vb0, vb1, m0, ph))
-    sig = np.zeros((nvox, T4), np.complex64)
-    for v in b1:
-        sel = np.flatnonzero(vb1 == v)
-        for c0 in range(0, sel.size, 65536):
-            cs = sel[c0:c0 + 65536]
-            vp = np.stack([vt1[cs], vt2[cs], vb0[cs], np.full(cs.size, v)], 1).astype(np.float32)
-            d_vp = torch.from_numpy(vp).to(dev)
-            d_s = torch.empty((cs.size, T4, 2), device=dev)
-            snap.MRF_dict(d_s, d_vp, h, T4, T4, cs.size, cs.size, 4, w, "epg_ssfp")
-            torch.cuda.synchronize()
-            a = d_s.cpu().numpy()
-            sig[cs] = a[..., 0] + 1j * a[..., 1]
-    img = add_noise(sig * (m0 * np.exp(1j * ph))[:, None], rank, T4)
-    del sig
+    if not args.c4_dict_only:
+        # voxels: per slice the tissue phantom (seeded per slice), a B0 field of
+        # +-80 Hz (linear + quadratic), and a B1 field 1 + 0.2 (x^2 + y^2 - 0.5)
+        # snapped to the dictionary's B1 values (the bSSFP recursion takes B1 per
+        # block); T1 / T2 / B0 off the grid
+        vt1, vt2, vb0, vb1, m0, ph = [], [], [], [], [], []
+        y, x = np.meshgrid(np.linspace(-1, 1, nxy), np.linspace(-1, 1, nxy), indexing="ij")
+        for s in range(args.c4_slices):
+            _, a1, a2, m, p = phantom(100 * rank + s, nxy)
+            zc = -1 + 2 * (s + 0.5) / max(args.c4_slices, 1)
+            f0 = np.clip(40.0 * x + 25.0 * y + 15.0 * (x ** 2 + y ** 2 + zc ** 2) - 10.0, -80.0, 80.0)
+            fb1 = np.clip(1.0 + 0.2 * (x ** 2 + y ** 2 - 0.5), 0.8, 1.2)
+            vt1.append(a1)
+            vt2.append(a2)
+            vb0.append(f0.reshape(-1).astype(np.float32))
+            vb1.append(b1[np.argmin(np.abs(fb1.reshape(-1)[:, None] - b1[None, :]), axis=1)])
+            m0.append(m)
+            ph.append(p)
+        vt1, vt2, vb0, vb1, m0, ph = (np.concatenate(v) for v in (vt1, vt2, vb0, vb1, m0, ph))
+        sig = np.zeros((nvox, T4), np.complex64)
+        for v in b1:
+            sel = np.flatnonzero(vb1 == v)
+            for c0 in range(0, sel.size, 65536):
+                cs = sel[c0:c0 + 65536]
+                vp = np.stack([vt1[cs], vt2[cs], vb0[cs], np.full(cs.size, v)], 1).astype(np.float32)
+                d_vp = torch.from_numpy(vp).to(dev)
+                d_s = torch.empty((cs.size, T4, 2), device=dev)
+                snap.MRF_dict(d_s, d_vp, h, T4, T4, cs.size, cs.size, 4, w, "epg_ssfp")
+                torch.cuda.synchronize()
+                a = d_s.cpu().numpy()
+                sig[cs] = a[..., 0] + 1j * a[..., 1]
+        img = add_noise(sig * (m0 * np.exp(1j * ph))[:, None], rank, T4)
+        del sig
 
     d_params = torch.from_numpy(params).to(dev)
     d_atoms = torch.empty((NATOMS, T4, 2), device=dev)
-    d_img = torch.from_numpy(img.view(np.float32).reshape(nvox, T4, 2)).to(dev)
-    d_maps = torch.empty((nvox, 5), device=dev)
-    d_index = torch.empty(nvox, dtype=torch.int64, device=dev)
+    if not args.c4_dict_only:
+        d_img = torch.from_numpy(img.view(np.float32).reshape(nvox, T4, 2)).to(dev)
+        d_maps = torch.empty((nvox, 5), device=dev)
+        d_index = torch.empty(nvox, dtype=torch.int64, device=dev)
 
     def ev_time(fn, reps, warm):
         for _ in range(warm):
@@ -882,7 +892,8 @@ def run_c4(args) -> None:
         torch.cuda.synchronize()
         return e0.elapsed_time(e1) / reps, (snap.kernel_launches() - l0) // reps
 
-    out = {"workload": WORKLOAD_C4 if args.c4_slices == 8 else f"{WORKLOAD_C4} ({args.c4_slices} of 8 slices)",
+    out = {"workload": WORKLOAD_C4 if args.c4_slices == 8 and args.c4_b0 == 51 else
+           f"{WORKLOAD_C4} reduced: {args.c4_slices} of 8 slices, {len(b0)} of 51 B0 values",
            "T": T4, "nstates": w, "atoms": NATOMS, "atoms_per_b1_block": natoms, "voxels": nvox,
            "match": "global MIP (no B1 map; the reference's max-PD merge)"}
     clk = ClockSampler(local)
@@ -902,6 +913,11 @@ def run_c4(args) -> None:
                                NATOMS * T4 * 100 * ROA_FLOP_PER_ISO_STEP, roa_ms, fp32_peak, fp32_note,
                                atoms_per_s=round(NATOMS / (roa_ms / 1e3), 1))
     del d_roa
+    if args.c4_dict_only:
+        clk.mark_end()
+        print(json.dumps({"workload": out["workload"], "atoms": NATOMS, "ssfp_dict": out["ssfp_dict"],
+                          "roa_dict": out["roa_dict"], "clocks": clk.stop()}), flush=True)
+        return
     snap.MRF_dict(d_atoms, d_params, h, T4, T4, NATOMS, natoms, 4, w, "epg_ssfp")
     pk = peaks()
     # matching: complex operands, K = 2T, 8 T flop per voxel-atom pair
@@ -1038,10 +1054,14 @@ def main() -> None:
                     help="energy fraction of the compressed-matching form (0: skip it)")
     ap.add_argument("--oracle-sample", type=int, default=64,
                     help="voxels whose headline maps are compared with the FP64 oracle's (0: skip)")
+    ap.add_argument("--forms", default="",
+                    help="comma-separated forms to time besides fp32 and the headline (default: all)")
     ap.add_argument("--c4-slices", type=int, default=8, help="ssfp workload: 256x256 slices")
     ap.add_argument("--c4-match-steps", type=int, default=2, help="ssfp workload: timed matching calls")
     ap.add_argument("--c4-fp32-voxels", type=int, default=4096, help="ssfp workload: voxels of the FP32 form")
     ap.add_argument("--c4-topk16", type=int, default=8, help="ssfp workload: FP16 candidates rescored")
+    ap.add_argument("--c4-b0", type=int, default=51, help="ssfp workload: B0 values (reduced case for profiling)")
+    ap.add_argument("--c4-dict-only", action="store_true", help="ssfp workload: the dictionaries alone")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
