@@ -62,7 +62,9 @@ void roa_ssfp(float2 *d_atoms, float *d_mrf, float *d_params, size_t nreps, size
 #ifdef __CUDACC__
 /* the reference's kernel (src/functions.h:87): callers launch it with
  * normalize<<<grid, block>>>(...) from code compiled without relocatable
- * device code */
+ * device code and linked with the shared CUDA runtime (nvcc -cudart
+ * shared), the runtime this library uses: the launch configuration the
+ * caller's <<<...>>> sets is read by the library's kernel stub */
 __global__ void normalize(float2 *d_atoms, size_t nreps, size_t NATOMS);
 #endif
 void MRF_minimatch(float *d_maps, float2 *d_img, float2 *d_atoms, float2 *d_mat, float *d_params, size_t nreps,

@@ -13,7 +13,7 @@ namespace snapmrf {
 enum Echo { ECHO_SSFP = 0, ECHO_ROA = 1, ECHO_SR = 2, ECHO_SE = 3, ECHO_TSE = 4, ECHO_FISP = 5 };
 
 constexpr int kEpgThreads = 128;      // threads per CTA
-constexpr int kChunk = 16;            // time steps staged per shared-memory chunk
+constexpr int kChunk = 16;            // time steps staged per shared-memory chunk (<= 32)
 constexpr int kMaxStatesPerLane = 8;  // register-resident EPG states per lane
 
 struct EpgArgs {
@@ -880,14 +880,21 @@ __global__ void __launch_bounds__(kEpgThreads) roa_iso_kernel(EpgArgs a) {
         const int nch = (int)min((long long)kChunk, nreps - t0);
         __syncthreads();
         for (int i = tid; i < nch; i += kEpgThreads) roa_matrix(alpha[t0 + i], phi[t0 + i], sT[i].T);
+        // the atom's relaxation and off-resonance factors of step t0 + l are
+        // computed once, by lane l (kChunk <= 32), and broadcast to the warp
+        float e1_l = 1.f, e2_l = 1.f, sb_l = 0.f, cb_l = 1.f;
+        if (lane < nch) {
+            const float tr = TR[t0 + lane];
+            e1_l = expf(-tr / t1);
+            e2_l = expf(-tr / t2);
+            const float beta = (float)(M_PI * b0 * tr / 1000.f);
+            __sincosf(beta, &sb_l, &cb_l);
+        }
         __syncthreads();
         for (int i = 0; i < nch; i++) {
             const float *T = sT[i].T;
-            float tr = TR[t0 + i];
-            float E1 = expf(-tr / t1), E2 = expf(-tr / t2);
-            float beta = (float)(M_PI * b0 * tr / 1000.f);
-            float sb, cb;
-            __sincosf(beta, &sb, &cb);
+            const float E1 = __shfl_sync(0xffffffffu, e1_l, i), E2 = __shfl_sync(0xffffffffu, e2_l, i);
+            const float sb = __shfl_sync(0xffffffffu, sb_l, i), cb = __shfl_sync(0xffffffffu, cb_l, i);
             float px = 0.f, py = 0.f;
 #pragma unroll
             for (int q = 0; q < IPL; q++) {
