@@ -931,6 +931,27 @@ def run_c4(args) -> None:
                                         "tensor", nvox * 8.0 * T4 * NATOMS, ms, pk["bf16_tflops"],
                                         f"bf16 dense, {pk['source']} (burst)", launches=nl,
                                         voxels_per_s=round(nvox / (ms / 1e3), 1))
+    # the refined form: the FP16 maps refined by Gauss-Newton on the complex
+    # bSSFP recursion (T1, T2, B0 and, with no B1 map, B1), at most
+    # --gn-iters iterations per voxel
+    if args.gn_iters > 0:
+        snap.MRF_match(d_maps, d_img, d_atoms, d_params, T4, T4, NATOMS, natoms, nvox, precision=snap.PREC_FP16,
+                       topk=args.c4_topk16, d_index=d_index)
+        d_maps16 = d_maps.clone()
+
+        def refine():
+            d_maps.copy_(d_maps16)
+            snap.refine_gn(d_maps, d_img, h, T4, T4, nvox, w, "epg_ssfp", iterations=args.gn_iters,
+                           tol=args.gn_tol)
+        gn_ms, _ = ev_time(refine, args.c4_match_steps, 1)
+        copy_ms, _ = ev_time(lambda: d_maps.copy_(d_maps16), 3, 1)
+        gm = d_maps.cpu().numpy()
+        out["gn_refine"] = {"ms": round(gn_ms - copy_ms, 3), "iterations_max": args.gn_iters, "tol": args.gn_tol,
+                            "refined": "T1, T2, B0, B1 (no B1 map)",
+                            "t1_median_rel_vs_truth": round(median_rel(gm[:, 0], vt1), 5),
+                            "t2_median_rel_vs_truth": round(median_rel(gm[:, 1], vt2), 5),
+                            "b0_median_abs_hz_vs_truth": round(float(np.median(np.abs(gm[:, 2] - vb0))), 3),
+                            "b1_median_abs_vs_truth": round(float(np.median(np.abs(gm[:, 3] - vb1))), 5)}
     # FP32 on a voxel subset (the whole image takes about a minute per call)
     nv32 = min(args.c4_fp32_voxels, nvox)
     sel = np.sort(np.random.default_rng(9).choice(nvox, nv32, replace=False))
@@ -958,7 +979,10 @@ def run_c4(args) -> None:
     out["device_error"] = snap.device_error(reset=True)
     clocks = clk.stop()
     if rank == 0:
-        best = min(("fp16", "bf16"), key=lambda f: out[f"{f}_match"]["ms"])
+        # the form whose argmax agrees with the FP32 form on >= 99.9 % of the
+        # sampled voxels, the faster one when both do
+        ok = [f for f in ("fp16", "bf16") if out[f"{f}_match"]["argmax_agreement_vs_fp32"] >= 0.999] or ["fp16"]
+        best = min(ok, key=lambda f: out[f"{f}_match"]["ms"])
         step_ms = ssfp_ms + out[f"{best}_match"]["ms"]
         line = {"metric": METRIC, "value": round(nvox / (step_ms / 1e3), 1), "unit": "voxels/s", "n_gpus": world,
                 "steps": args.c4_match_steps, "warmup": 1, "ms_per_step": round(step_ms, 3),

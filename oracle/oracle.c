@@ -168,3 +168,113 @@ int oracle_fisp_jvp_f64(double *sig, double *dsig, double *loss, double *dloss, 
     free(fp);
     return 0;
 }
+
+/* ------------------------------------------------------------------------
+ * FP64 forward mode (one tangent) for the complex bSSFP recursion of
+ * epg_ssfp (src/functions.cu:935-1019): inversion by init_rf_pulse with
+ * alpha = 180 deg, phi = 0 and delay TI (:456-481, 965-966); per step the RF
+ * matrix of fill_transition_matrix (:483-508) at flip alpha_t * B1 and phase
+ * phi_t, relaxation over TE (:530-583), B0 precession exp(+-i 2 pi B0 t /
+ * 1000) over TE (:585-607), readout F+[0] (:609-617), B0 precession over
+ * TR - TE, the dephasing shift (:619-668), relaxation over TR - TE.  The
+ * atoms are not normalised.  mrf is the converted compact [4][nreps]
+ * schedule (flip rad, phase rad, TR ms, TE ms).  Each quantity carries a
+ * value and a derivative along (dT1, dT2, dB0, dB1).
+ * Outputs: sig[2T] and dsig[2T], interleaved complex.
+ * ---------------------------------------------------------------------- */
+typedef struct { dual re, im; } cdual;
+
+static inline cdual cdmk(dual re, dual im) { cdual r; r.re = re; r.im = im; return r; }
+static inline cdual cdadd(cdual a, cdual b) { return cdmk(dadd(a.re, b.re), dadd(a.im, b.im)); }
+static inline cdual cdmul(cdual a, cdual b)
+{
+    return cdmk(dadd(dmul(a.re, b.re), dmul(dmk(-a.im.v, -a.im.d), b.im)),
+                dadd(dmul(a.re, b.im), dmul(a.im, b.re)));
+}
+static inline cdual cdscale(cdual a, dual s) { return cdmk(dmul(a.re, s), dmul(a.im, s)); }
+static inline cdual cdconj(cdual a) { return cdmk(a.re, dmk(-a.im.v, -a.im.d)); }
+static inline cdual cdzero(void) { return cdmk(dmk(0, 0), dmk(0, 0)); }
+
+int oracle_ssfp_jvp_f64(double *sig, double *dsig, double T1, double T2, double B0, double B1, double dT1,
+                        double dT2, double dB0, double dB1, const float *mrf, size_t nreps, int nstates, double TI)
+{
+    int w = nstates;
+    cdual *fp = (cdual *)calloc(3 * (size_t)w, sizeof(cdual));
+    if (!fp) return -3;
+    cdual *fm = fp + w, *z = fm + w;
+    for (int k = 0; k < 3 * w; k++) fp[k] = cdzero();
+    const float *alpha = mrf, *phi = mrf + nreps, *TR = mrf + 2 * nreps, *TE = mrf + 3 * nreps;
+    dual t1 = dmk(T1, dT1), t2 = dmk(T2, dT2), b0 = dmk(B0, dB0), b1 = dmk(B1, dB1);
+    /* inversion: F+0 = conj(q), F-0 = q with q = E2(TI) sin(a0) (sin p0 + i cos p0),
+     * Z0 = E1(TI) cos(a0) + 1 - E1(TI), a0 = pi, p0 = 0 */
+    {
+        dual e1 = dexp(ddiv(dmk(-TI, 0), t1)), e2 = dexp(ddiv(dmk(-TI, 0), t2));
+        double a0 = M_PI, p0 = 0.0;
+        cdual q = cdscale(cdmk(dmk(sin(p0), 0), dmk(cos(p0), 0)), dmul(e2, dmk(sin(a0), 0)));
+        fp[0] = cdconj(q);
+        fm[0] = q;
+        z[0] = cdmk(dadd(dmul(e1, dmk(cos(a0), 0)), dmk(1 - e1.v, -e1.d)), dmk(0, 0));
+    }
+    for (size_t i = 0; i < nreps; i++) {
+        dual a = dmul(dmk(alpha[i], 0), b1);
+        dual sa = dsin(a), ca = dcos(a);
+        dual sa2 = dmul(dadd(dmk(1, 0), dmk(-ca.v, -ca.d)), dmk(0.5, 0));
+        dual ca2 = dmul(dadd(dmk(1, 0), ca), dmk(0.5, 0));
+        cdual zz = cdmk(dmk(cos((double)phi[i]), 0), dmk(sin((double)phi[i]), 0)), zi = cdconj(zz);
+        cdual I = cdmk(dmk(0, 0), dmk(1, 0)), mI = cdmk(dmk(0, 0), dmk(-1, 0));
+        cdual M[9];
+        M[0] = cdmk(ca2, dmk(0, 0));
+        M[1] = cdscale(cdmul(zz, zz), sa2);
+        M[2] = cdscale(cdmul(mI, zz), sa);
+        M[3] = cdscale(cdmul(zi, zi), sa2);
+        M[4] = cdmk(ca2, dmk(0, 0));
+        M[5] = cdscale(cdmul(I, zi), sa);
+        M[6] = cdscale(cdmul(mI, zi), dmul(sa, dmk(0.5, 0)));
+        M[7] = cdscale(cdmul(I, zz), dmul(sa, dmk(0.5, 0)));
+        M[8] = cdmk(ca, dmk(0, 0));
+        for (int k = 0; k < w; k++) {
+            cdual p = fp[k], m = fm[k], q = z[k];
+            fp[k] = cdadd(cdadd(cdmul(M[0], p), cdmul(M[1], m)), cdmul(M[2], q));
+            fm[k] = cdadd(cdadd(cdmul(M[3], p), cdmul(M[4], m)), cdmul(M[5], q));
+            z[k] = cdadd(cdadd(cdmul(M[6], p), cdmul(M[7], m)), cdmul(M[8], q));
+        }
+        double ta = (double)TE[i], tb = (double)TR[i] - (double)TE[i];
+        for (int pass = 0; pass < 2; pass++) {
+            double t = pass == 0 ? ta : tb;
+            if (pass == 1) {
+                dual th = dmul(b0, dmk(2 * M_PI * t / 1000.0, 0));
+                cdual e = cdmk(dcos(th), dsin(th)), ec = cdconj(e);
+                for (int k = 0; k < w; k++) {
+                    fp[k] = cdmul(e, fp[k]);
+                    fm[k] = cdmul(ec, fm[k]);
+                }
+                for (int k = w - 1; k >= 1; k--) fp[k] = fp[k - 1];
+                cdual f0 = fm[0];
+                for (int k = 0; k <= w - 2; k++) fm[k] = fm[k + 1];
+                fp[0] = cdconj(w == 1 ? f0 : fm[0]);
+                fm[w - 1] = cdzero();
+            }
+            dual E1 = dexp(ddiv(dmk(-t, 0), t1)), E2 = dexp(ddiv(dmk(-t, 0), t2));
+            for (int k = 0; k < w; k++) {
+                fp[k] = cdscale(fp[k], E2);
+                fm[k] = cdscale(fm[k], E2);
+                z[k] = cdscale(z[k], E1);
+            }
+            z[0].re = dadd(z[0].re, dmk(1 - E1.v, -E1.d));
+            if (pass == 0) {
+                dual th = dmul(b0, dmk(2 * M_PI * t / 1000.0, 0));
+                cdual e = cdmk(dcos(th), dsin(th)), ec = cdconj(e);
+                for (int k = 0; k < w; k++) {
+                    fp[k] = cdmul(e, fp[k]);
+                    fm[k] = cdmul(ec, fm[k]);
+                }
+                sig[2 * i] = fp[0].re.v;
+                sig[2 * i + 1] = fp[0].im.v;
+                dsig[2 * i] = fp[0].re.d;
+                dsig[2 * i + 1] = fp[0].im.d;
+            }
+        }
+    }
+    free(fp);
+    return 0;
+}

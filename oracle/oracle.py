@@ -125,6 +125,58 @@ def fisp_jvp(theta, tangent, h_mrf, nstates: int = 101, echo: str = "epg_fisp", 
     return sig, dsig, loss.value, dloss.value
 
 
+def ssfp_schedule(h_csv, nreps: int | None = None) -> np.ndarray:
+    """The epg_ssfp conversion of a CSV schedule as MRF_dict does it
+    (src/functions.cu:1240-1261): flip fraction x 60 deg in rad, phase deg
+    -> rad, TR + 16 ms, TE + 3.5 ms, in float32."""
+    h = np.asarray(h_csv, np.float32)
+    n = nreps or h.shape[1]
+    fa_scale = np.float32(60.0 * np.pi / 180.0)
+    ph_scale = np.float32(np.pi / 180.0)
+    return np.array([h[0, :n] * fa_scale, h[1, :n] * ph_scale, h[2, :n] + np.float32(16.0),
+                     h[3, :n] + np.float32(3.5)], np.float32)
+
+
+def ssfp_jvp(theta, tangent, h_csv, nstates: int = 101, TI: float = 40.0):
+    """FP64 forward mode of the complex bSSFP recursion (epg_ssfp, no
+    normalisation) along one direction: theta = (T1, T2, B0, B1), tangent =
+    (dT1, dT2, dB0, dB1), h_csv the schedule in the CSV convention.
+    Returns (s [T] complex, ds [T] complex)."""
+    mrf = np.ascontiguousarray(ssfp_schedule(h_csv))
+    T = mrf.shape[1]
+    sig = np.zeros(2 * T, np.float64)
+    dsig = np.zeros(2 * T, np.float64)
+    f = lib().oracle_ssfp_jvp_f64
+    f.restype = C.c_int
+    f.argtypes = [C.c_void_p, C.c_void_p] + [C.c_double] * 8 + [C.c_void_p, C.c_size_t, C.c_int, C.c_double]
+    r = f(sig.ctypes.data, dsig.ctypes.data, *map(float, theta), *map(float, tangent), mrf.ctypes.data, T,
+          nstates, TI)
+    if r != 0:
+        raise RuntimeError(f"oracle_ssfp_jvp failed: {r}")
+    return sig[0::2] + 1j * sig[1::2], dsig[0::2] + 1j * dsig[1::2]
+
+
+def ssfp_gn_step_f64(theta, x, h_csv, nstates: int = 101, refine_b1: bool = True):
+    """One projected Gauss-Newton step of (T1, T2, B0[, B1]) in FP64 for one
+    voxel under x = rho * s(theta), s the bSSFP signal, rho complex and
+    eliminated by variable projection.  Returns (step, |rho|, |<s,x>|/||s||)."""
+    n = 4 if refine_b1 else 3
+    cols, s = [], None
+    for j in range(n):
+        tg = [0.0] * 4
+        tg[j] = 1.0
+        s, ds = ssfp_jvp(theta, tg, h_csv, nstates)
+        cols.append(ds)
+    J = np.stack(cols, 1)
+    x = np.asarray(x, np.complex128)
+    ss = np.vdot(s, s).real
+    rho = np.vdot(s, x) / ss
+    Pj = J - np.outer(s, (s.conj() @ J) / ss)
+    A = (abs(rho) ** 2) * (Pj.conj().T @ Pj).real
+    b = (np.conj(rho) * (Pj.conj().T @ x)).real
+    return np.linalg.solve(A, b), abs(rho), abs(np.vdot(s, x)) / np.sqrt(ss)
+
+
 def trans_params(t1, t2, b0, b1) -> np.ndarray:
     """params[NATOMS][4] = {T1, T2, B0, B1} restated from trans_params
     (src/functions.cu:355-391): B1 outermost, then B0, then T2, T1

@@ -1046,6 +1046,13 @@ static int echo_shift(const char *echo_type) {
 }  // namespace grad
 }  // namespace snapmrf
 
+namespace snapmrf {
+// epg_ssfp_grad.cu
+int refine_gn_ssfp(float *d_maps, int nmaps, const float *img, size_t img_stride, const float *d_b1map,
+                   const float *h_mrf, size_t nreps, size_t NREPS, size_t nvoxels, int nstates, int iterations,
+                   float max_rel_step, float tol, float *d_m0, cudaStream_t st);
+}
+
 using namespace snapmrf;
 using namespace snapmrf::grad;
 
@@ -1120,8 +1127,12 @@ extern "C" int snapmrf_refine_gn(float *d_maps, int nmaps, const float *img, siz
         SNAPMRF_FAIL(SNAPMRF_ERR_UNSUPPORTED, "refine_gn: too many time points or voxels");
     if (!img_stride) img_stride = nreps;
     if (img_stride < nreps) SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "refine_gn: img_stride < nreps");
+    if (echo_type && !strcmp(echo_type, "epg_ssfp"))
+        return refine_gn_ssfp(d_maps, nmaps, img, img_stride, d_b1map, h_mrf, nreps, NREPS, nvoxels, nstates,
+                              iterations, max_rel_step, tol, d_m0, st);
     const int shift = echo_shift(echo_type);
-    if (shift < 0) SNAPMRF_FAIL(SNAPMRF_ERR_ECHO_TYPE, "refine_gn: echo type must be epg_fisp or epg_sr");
+    if (shift < 0)
+        SNAPMRF_FAIL(SNAPMRF_ERR_ECHO_TYPE, "refine_gn: echo type must be epg_fisp, epg_sr or epg_ssfp");
     DeviceScratch sbuf;
     Schedule sc;
     int rc = upload_schedule(sbuf, &sc, h_mrf, nreps, NREPS, st, "refine_gn");

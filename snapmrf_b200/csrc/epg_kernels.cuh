@@ -763,6 +763,11 @@ __device__ __forceinline__ void roa_init(float t1, float t2, float &m0, float &m
     m2 = e1 * ca + 1 - e1;
 }
 
+#ifndef SNAPMRF_EPG_DEVICE_HELPERS_ONLY
+// (the non-template kernel below is defined once, in epg.cu; other sources
+// that need only the device helpers above define
+// SNAPMRF_EPG_DEVICE_HELPERS_ONLY)
+
 // Single isochromat (the reference's roa_ssfp): one thread per atom.
 __global__ void __launch_bounds__(kEpgThreads) roa_kernel(EpgArgs a) {
     __shared__ RoaStep sT[kChunk];
@@ -958,5 +963,7 @@ inline cudaError_t launch_roa(const EpgArgs &a, long long natoms, unsigned gen_b
     note_launches(1);
     return cudaGetLastError();
 }
+
+#endif  // SNAPMRF_EPG_DEVICE_HELPERS_ONLY
 
 }  // namespace snapmrf

@@ -295,3 +295,87 @@ def test_gn_early_exit_agrees_with_full_iterations(snap, oracle):
     np.testing.assert_allclose(pd_e, pd_f, rtol=1e-5)
     one, _, _ = run_gn(snap, theta0, x, h, w, 1, tol=1e-4)
     assert not np.allclose(one[:, :2], full[:, :2], rtol=5e-4)
+
+
+# --------------------------------------------------------------------------
+# Gauss-Newton on the complex bSSFP recursion
+# --------------------------------------------------------------------------
+
+def _ssfp_voxels(orc, n, h, w, seed, noise=0.0):
+    rng = np.random.default_rng(seed)
+    t1 = np.exp(rng.uniform(np.log(300), np.log(2500), n))
+    t2 = np.minimum(np.exp(rng.uniform(np.log(30), np.log(300), n)), 0.5 * t1)
+    b0 = rng.uniform(-60, 60, n)
+    b1 = rng.uniform(0.85, 1.15, n)
+    truth = np.stack([t1, t2, b0, b1], 1)
+    rho = rng.uniform(0.5, 2, n) * np.exp(1j * rng.uniform(0, 6.28, n))
+    x = []
+    for p, r in zip(truth, rho):
+        s, _ = orc.ssfp_jvp(tuple(p), (0, 0, 0, 0), h, nstates=w)
+        x.append(r * s + noise * (rng.standard_normal(len(s)) + 1j * rng.standard_normal(len(s))))
+    return truth, rho, np.array(x)
+
+
+def _run_gn_ssfp(snap, start, img, h, w, iterations, b1map=None, tol=0.0, max_rel_step=0.2):
+    import torch
+    n = start.shape[0]
+    maps = np.zeros((n, 5), np.float32)
+    maps[:, :4] = start
+    maps[:, 4] = -1
+    d_maps = torch.from_numpy(maps).cuda()
+    d_img = torch.from_numpy(np.ascontiguousarray(img.astype(np.complex64)).view(np.float32)).cuda()
+    d_m0 = torch.full((n,), -1.0, device="cuda")
+    d_b1 = None if b1map is None else torch.from_numpy(np.ascontiguousarray(b1map, np.float32)).cuda()
+    snap.refine_gn(d_maps, d_img, h, h.shape[1], h.shape[1], n, w, "epg_ssfp", iterations=iterations,
+                   max_rel_step=max_rel_step, tol=tol, d_b1map=d_b1, d_m0=d_m0)
+    torch.cuda.synchronize()
+    return d_maps.cpu().numpy(), d_m0.cpu().numpy()
+
+
+def test_gn_ssfp_step_matches_fp64_step(snap, oracle):
+    """One Gauss-Newton step of (T1, T2, B0, B1) on the complex bSSFP
+    recursion against the FP64 projected step from the oracle's forward
+    mode (noisy voxels, starts off by a few percent, no trust region)."""
+    from cases import c4_ssfp_csv
+    T, w = 200, 30
+    h = c4_ssfp_csv(T, seed=41)
+    truth, rho, x = _ssfp_voxels(oracle, 6, h, w, seed=42, noise=0.002)
+    rng = np.random.default_rng(43)
+    start = (truth * np.stack([rng.uniform(0.97, 1.03, 6), rng.uniform(0.97, 1.03, 6), np.ones(6),
+                               rng.uniform(0.98, 1.02, 6)], 1)).astype(np.float32)
+    start[:, 2] += rng.uniform(-1.5, 1.5, 6).astype(np.float32)
+    got, _ = _run_gn_ssfp(snap, start, x, h, w, 1, max_rel_step=1e6)
+    for i in range(6):
+        d, _, _ = oracle.ssfp_gn_step_f64(tuple(start[i].astype(np.float64)), x[i], h, nstates=w)
+        step = got[i, :4].astype(np.float64) - start[i].astype(np.float64)
+        print(i, step, d)
+        np.testing.assert_allclose(step, d, rtol=5e-3, atol=5e-3 * np.abs(d).max() + 1e-4)
+
+
+@pytest.mark.parametrize("with_map", [False, True])
+def test_gn_ssfp_recovers_off_grid_parameters(snap, oracle, with_map):
+    """Noiseless bSSFP voxels from off-grid (T1, T2, B0, B1), started a grid
+    step away (5 % in T1 and T2, 2 Hz, 0.04 in B1; with a B1 map, B1 exact
+    and kept): six iterations recover the parameters, and PD / M0 are those
+    of the exact fit."""
+    from cases import c4_ssfp_csv
+    T, w = 300, 40
+    h = c4_ssfp_csv(T, seed=44)
+    n = 24
+    truth, rho, x = _ssfp_voxels(oracle, n, h, w, seed=45)
+    sign = np.where(np.arange(n) % 2 == 0, 1.0, -1.0)
+    start = truth.copy()
+    start[:, 0] *= 1.05 ** sign
+    start[:, 1] /= 1.05 ** sign
+    start[:, 2] += 2.0 * sign
+    if not with_map:
+        start[:, 3] += 0.04 * sign
+    b1map = truth[:, 3] if with_map else None
+    got, m0 = _run_gn_ssfp(snap, start.astype(np.float32), x, h, w, 6, b1map=b1map)
+    err = np.abs(got[:, :4] - truth) / np.array([truth[:, 0], truth[:, 1], np.full(n, 100.0), truth[:, 3]]).T
+    print("max relative errors (T1, T2, B0/100 Hz, B1):", err.max(axis=0))
+    assert err[:, :2].max() < 1e-3 and err[:, 2].max() < 1e-3 and err[:, 3].max() < 1e-3
+    for i in range(n):
+        s, _ = oracle.ssfp_jvp(tuple(truth[i]), (0, 0, 0, 0), h, nstates=w)
+        assert abs(m0[i] - abs(rho[i])) < 2e-3 * abs(rho[i])
+        assert abs(got[i, 4] - abs(rho[i]) * np.linalg.norm(s)) < 2e-3 * abs(rho[i]) * np.linalg.norm(s)

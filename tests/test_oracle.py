@@ -186,3 +186,28 @@ def test_fp64_gauss_newton_converges_to_the_noiseless_truth(oracle):
         g1, g2, pd = oracle.refine_gn_f64((t1 * 1.05, t2 / 1.05, b1), x, h, nstates=w)
         assert abs(g1 - t1) < 1e-6 * t1 and abs(g2 - t2) < 1e-6 * t2
         assert abs(pd - abs(0.7 - 0.4j) * np.linalg.norm(s)) < 1e-9 * pd
+
+
+def test_ssfp_forward_mode_matches_dictionary_and_differences(oracle):
+    """The FP64 forward mode of the bSSFP recursion: its signal equals the
+    oracle's epg_ssfp atoms (one B1 block, before normalisation) and each
+    tangent equals central differences of the signal (T1, T2, B0, B1)."""
+    from cases import c4_ssfp_csv
+    T, w = 80, 20
+    h = c4_ssfp_csv(T, seed=9)
+    th = (900.0, 70.0, 13.0, 1.1)
+    s, _ = oracle.ssfp_jvp(th, (0, 0, 0, 0), h, nstates=w)
+    params = np.array([[th[0], th[1], th[2], th[3]]], np.float32)
+    ref, norms = oracle.dict_atoms("epg_ssfp", params, h, T, nstates=w, return_norms=True)
+    np.testing.assert_allclose(s / np.linalg.norm(s), ref[0], atol=2e-6)
+    for j, step in enumerate((1e-3 * th[0], 1e-3 * th[1], 1e-2, 1e-4)):
+        tg = [0.0] * 4
+        tg[j] = 1.0
+        _, ds = oracle.ssfp_jvp(th, tg, h, nstates=w)
+        tp, tm = list(th), list(th)
+        tp[j] += step
+        tm[j] -= step
+        fd = (oracle.ssfp_jvp(tp, (0, 0, 0, 0), h, nstates=w)[0] -
+              oracle.ssfp_jvp(tm, (0, 0, 0, 0), h, nstates=w)[0]) / (2 * step)
+        err = np.abs(ds - fd).max() / np.abs(fd).max()
+        assert err < 1e-5, (j, err)
