@@ -416,10 +416,17 @@ int snapmrf_mrf_match_noalloc(float *d_maps, const float *d_img, size_t img_stri
 
 /* ------------------------------------------------------------------------
  * Derivatives of the EPG signal.  No counterpart in the reference, which
- * only evaluates the forward recursion; both entry points differentiate its
- * real-valued FISP / SR recursion (epg_fisp, epg_sr: src/functions.cu:687-739,
- * 878-933, every RF phase 0) with the B1 extension of snapmrf_mrf_dict
- * (flip angle alpha_t * B1, no initial pulse).
+ * only evaluates the forward recursion.  Two recursions are differentiated:
+ *   - the real-valued FISP / SR recursion (epg_fisp, epg_sr:
+ *     src/functions.cu:687-739, 878-933, every RF phase 0) with the B1
+ *     extension of snapmrf_mrf_dict (flip angle alpha_t * B1, no initial
+ *     pulse); parameters T1, T2, B1;
+ *   - the complex bSSFP recursion (epg_ssfp, src/functions.cu:935-1019: RF
+ *     with any phase, B0 precession, the 180-degree inversion with TI = 40
+ *     ms), h_mrf in the CSV convention it converts (flip fraction of 60
+ *     degrees, phase in degrees, TR - 16 ms, TE - 3.5 ms), flip angle alpha_t
+ *     * B1 (the continuous form of epg_ssfp's FA x b1); parameters T1, T2, B0,
+ *     B1.  nstates <= 128.
  * ------------------------------------------------------------------------ */
 
 /* Reverse mode (adjoint) with checkpointing.
@@ -429,8 +436,10 @@ int snapmrf_mrf_match_noalloc(float *d_maps, const float *d_img, size_t img_stri
  * d_grad_signal: device complex [natoms][nreps], dL/d(Re s_t, Im s_t) of a
  * real loss L of the (unnormalised) atoms s;
  * d_signal: optional out, the atoms (complex [natoms][nreps]);
- * d_grad_params: out [natoms][3]: dL/dT1, dL/dT2, dL/dB1;
- * d_grad_alpha: optional out [nreps]: dL/dalpha_t summed over atoms;
+ * d_grad_params: out [natoms][3]: dL/dT1, dL/dT2, dL/dB1 (epg_fisp /
+ * epg_sr); [natoms][4]: dL/dT1, dL/dT2, dL/dB0, dL/dB1 (epg_ssfp);
+ * d_grad_alpha: optional out [nreps]: dL/dh_mrf[0][t] (the schedule's flip
+ * entries) summed over atoms;
  * d_grad_alpha_atoms: optional out [natoms][nreps]: the per-atom terms;
  * checkpoint_every: states kept every C steps (0: C = ceil(sqrt(nreps))),
  * so device scratch is natoms * (nreps/C + C) * 3 * nstates floats (rounded
@@ -441,7 +450,10 @@ int snapmrf_epg_adjoint(const float *d_params, int nparams, const float *h_mrf, 
                         float *d_grad_alpha, float *d_grad_alpha_atoms, int checkpoint_every,
                         void *stream);
 
-/* Per-voxel Gauss-Newton refinement of matched (T1, T2), in place.
+/* Per-voxel Gauss-Newton refinement of matched (T1, T2), in place (epg_fisp /
+ * epg_sr); of (T1, T2, B0) and, without d_b1map, B1 too for epg_ssfp (B0
+ * steps limited to max_rel_step x 50 Hz, a voxel stops once its B0 step is
+ * within tol x 100 Hz and its B1 step within tol of B1 as well).
  *
  * Model: voxel x = rho * s(T1, T2, B1) with rho complex, eliminated by
  * variable projection (rho = <s, x> / <s, s>); each iteration runs the

@@ -1048,6 +1048,9 @@ static int echo_shift(const char *echo_type) {
 
 namespace snapmrf {
 // epg_ssfp_grad.cu
+int epg_adjoint_ssfp(const float *d_params, int nparams, const float *h_mrf, size_t nreps, size_t NREPS,
+                     size_t natoms, int nstates, const float *d_grad_signal, float *d_signal, float *d_grad_params,
+                     float *galpha_atoms, int checkpoint_every, cudaStream_t st);
 int refine_gn_ssfp(float *d_maps, int nmaps, const float *img, size_t img_stride, const float *d_b1map,
                    const float *h_mrf, size_t nreps, size_t NREPS, size_t nvoxels, int nstates, int iterations,
                    float max_rel_step, float tol, float *d_m0, cudaStream_t st);
@@ -1067,8 +1070,41 @@ extern "C" int snapmrf_epg_adjoint(const float *d_params, int nparams, const flo
     if (nparams < 4 || nreps == 0 || nreps > NREPS || natoms == 0 || nstates < 1 || nstates > 32 * kMaxS)
         SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "epg_adjoint: bad sizes");
     if (nreps > 0x7fffffff) SNAPMRF_FAIL(SNAPMRF_ERR_UNSUPPORTED, "epg_adjoint: too many time points");
+    if (echo_type && !strcmp(echo_type, "epg_ssfp")) {
+        // the complex bSSFP recursion (epg_ssfp_grad.cu); the per-atom
+        // schedule gradient goes to the caller's buffer or scratch, then the
+        // same deterministic column sum
+        DeviceScratch gbuf;
+        float *gat = d_grad_alpha_atoms;
+        if (!gat) {
+            SNAPMRF_CUDA(gbuf.alloc((size_t)natoms * nreps * sizeof(float) +
+                                    (d_grad_alpha ? (size_t)kSplits * nreps * sizeof(float) : 0), st));
+            gat = gbuf.as<float>();
+        }
+        int rc = epg_adjoint_ssfp(d_params, nparams, h_mrf, nreps, NREPS, natoms, nstates, d_grad_signal, d_signal,
+                                  d_grad_params, gat, checkpoint_every, st);
+        if (rc) return rc;
+        if (d_grad_alpha) {
+            DeviceScratch pbuf;
+            float *partial = nullptr;
+            if (d_grad_alpha_atoms) {
+                SNAPMRF_CUDA(pbuf.alloc((size_t)kSplits * nreps * sizeof(float), st));
+                partial = pbuf.as<float>();
+            } else {
+                partial = gat + (size_t)natoms * nreps;
+            }
+            dim3 pg((unsigned)((nreps + 127) / 128), kSplits);
+            sum_columns_partial_kernel<<<pg, 128, 0, st>>>(partial, gat, (long long)natoms, (int)nreps);
+            SNAPMRF_LAUNCH_CHECK();
+            sum_columns_final_kernel<<<(unsigned)((nreps + 127) / 128), 128, 0, st>>>(d_grad_alpha, partial,
+                                                                                    (int)nreps);
+            SNAPMRF_LAUNCH_CHECK();
+        }
+        return SNAPMRF_OK;
+    }
     const int shift = echo_shift(echo_type);
-    if (shift < 0) SNAPMRF_FAIL(SNAPMRF_ERR_ECHO_TYPE, "epg_adjoint: echo type must be epg_fisp or epg_sr");
+    if (shift < 0)
+        SNAPMRF_FAIL(SNAPMRF_ERR_ECHO_TYPE, "epg_adjoint: echo type must be epg_fisp, epg_sr or epg_ssfp");
     DeviceScratch sbuf;
     Schedule sc;
     int rc = upload_schedule(sbuf, &sc, h_mrf, nreps, NREPS, st, "epg_adjoint");

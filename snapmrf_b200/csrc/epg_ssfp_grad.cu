@@ -573,3 +573,367 @@ int refine_gn_ssfp(float *d_maps, int nmaps, const float *img, size_t img_stride
 }
 
 }  // namespace snapmrf
+
+// --------------------------------------------------------------------------
+// Reverse mode (adjoint) of the complex bSSFP recursion with checkpointing
+// --------------------------------------------------------------------------
+namespace snapmrf {
+namespace ssfpgrad {
+
+struct AdjArgs {
+    const float *alpha, *phi, *TR, *TE;  // converted schedule [nreps]
+    float fa_scale;      // d(converted flip) / d(schedule entry)
+    int nreps;
+    float TI;
+    const float *params; // [n][nparams]: T1, T2, B0, B1
+    int nparams;
+    long long n;
+    int w, L;
+    const float2 *gsig;  // [n][nreps] dL/d(Re s_t, Im s_t)
+    float2 *sig;         // optional out [n][nreps]
+    float *gparams;      // [n][4]: dL/dT1, dL/dT2, dL/dB0, dL/dB1
+    float *galpha_atoms; // [n][nreps]: dL/d(schedule flip entry t) per atom
+    float *ckpt;         // [n][nckpt][6 S L]
+    float *seg;          // [n][C][6 S L]
+    int C, nckpt;
+};
+
+// A saved state is [6][S][L] floats (F+ re, F+ im, F- re, F- im, Z re,
+// Z im): the L lanes of a group touch consecutive words.
+template <int S>
+__device__ __forceinline__ void save(float *dst, int L, int gl, const LaneState<S> &x) {
+#pragma unroll
+    for (int j = 0; j < S; j++) {
+        dst[(0 * S + j) * L + gl] = x.fp[j].x;
+        dst[(1 * S + j) * L + gl] = x.fp[j].y;
+        dst[(2 * S + j) * L + gl] = x.fm[j].x;
+        dst[(3 * S + j) * L + gl] = x.fm[j].y;
+        dst[(4 * S + j) * L + gl] = x.zz[j].x;
+        dst[(5 * S + j) * L + gl] = x.zz[j].y;
+    }
+}
+
+template <int S>
+__device__ __forceinline__ void load(LaneState<S> &x, const float *src, int L, int gl) {
+#pragma unroll
+    for (int j = 0; j < S; j++) {
+        x.fp[j] = make_float2(src[(0 * S + j) * L + gl], src[(1 * S + j) * L + gl]);
+        x.fm[j] = make_float2(src[(2 * S + j) * L + gl], src[(3 * S + j) * L + gl]);
+        x.zz[j] = make_float2(src[(4 * S + j) * L + gl], src[(5 * S + j) * L + gl]);
+    }
+}
+
+// Per-step constants of one atom.
+struct StepC {
+    float2 T[9];
+    float E1a, E2a, E1b, E2b;
+    float2 ea, eb;
+    float ta, tb;
+    float ca, sa;
+    float2 z;
+};
+
+__device__ __forceinline__ StepC step_constants(const AdjArgs &a, int t, float T1, float T2, float B0, float B1) {
+    StepC c;
+    const float tr = a.TR[t], te = a.TE[t];
+    c.ta = te;
+    c.tb = tr - te;
+    __sincosf(a.alpha[t] * B1, &c.sa, &c.ca);
+    float sp, cp;
+    __sincosf(a.phi[t], &sp, &cp);
+    c.z = make_float2(cp, sp);
+    float2 dT[9];
+    rf_and_derivative(c.ca, c.sa, c.z, c.T, dT);
+    c.E1a = expf(-c.ta / T1);
+    c.E2a = expf(-c.ta / T2);
+    c.E1b = expf(-c.tb / T1);
+    c.E2b = expf(-c.tb / T2);
+    c.ea = b0_phasor(B0, c.ta);
+    c.eb = b0_phasor(B0, c.tb);
+    return c;
+}
+
+// One step of the recursion (src/functions.cu:976-1010 order): RF,
+// relax(TE), B0(TE), readout, B0(TR - TE), shift, relax(TR - TE).
+template <int S>
+__device__ __forceinline__ float2 forward_step(LaneState<S> &v, const StepC &c, int gl, int L, int w, bool lane0) {
+    st_rf<S>(v, c.T);
+    st_relax<S>(v, c.E1a, c.E2a, lane0);
+    st_b0<S>(v, c.ea);
+    const float2 s = v.fp[0];
+    st_b0<S>(v, c.eb);
+    st_shift<S>(v, gl, L, w);
+    st_relax<S>(v, c.E1b, c.E2b, lane0);
+    return s;
+}
+
+// Transpose of st_shift on adjoint states: lam_old.F+[k] = lam_new.F+[k+1]
+// (k <= w-2), lam_old.F-[k] = lam_new.F-[k-1] (1 <= k <= w-1), plus
+// conj(lam_new.F+[0]) into lam_old.F-[1] (F-[0] with w = 1), Z unchanged.
+template <int S>
+__device__ __forceinline__ void shift_transpose(LaneState<S> &l, int gl, int L, int w) {
+    const unsigned full = 0xffffffffu;
+    const float2 f0 = l.fp[0];  // lam_new.F+[0] on lane 0
+    // F+ moves down one state: slot j takes j + 1, the top slot the next lane's slot 0
+    float2 dn;
+    dn.x = __shfl_down_sync(full, l.fp[0].x, 1, L);
+    dn.y = __shfl_down_sync(full, l.fp[0].y, 1, L);
+    // F- moves up one state: slot j takes j - 1, slot 0 the previous lane's top slot
+    float2 up;
+    up.x = __shfl_up_sync(full, l.fm[S - 1].x, 1, L);
+    up.y = __shfl_up_sync(full, l.fm[S - 1].y, 1, L);
+#pragma unroll
+    for (int j = 0; j < S - 1; j++) l.fp[j] = l.fp[j + 1];
+    l.fp[S - 1] = (gl == L - 1) ? make_float2(0.f, 0.f) : dn;
+#pragma unroll
+    for (int j = S - 1; j >= 1; j--) l.fm[j] = l.fm[j - 1];
+    l.fm[0] = (gl == 0) ? make_float2(0.f, 0.f) : up;
+    if (gl == 0) {
+        const float2 cf = c_conj(f0);
+        if (w == 1) l.fm[0] = cf;
+        else { l.fm[1].x += cf.x; l.fm[1].y += cf.y; }
+    }
+#pragma unroll
+    for (int j = 0; j < S; j++) {
+        const int k = gl * S + j;
+        if (k >= w - 1) l.fp[j] = make_float2(0.f, 0.f);
+        if (k >= w) l.fm[j] = make_float2(0.f, 0.f);
+    }
+}
+
+// Re sum conj(a) b over this lane's states of the channels in `mask`
+// (1: F+, 2: F-, 4: Z).
+template <int S>
+__device__ __forceinline__ float redot(const LaneState<S> &a, const LaneState<S> &b, int mask) {
+    float r = 0.f;
+#pragma unroll
+    for (int j = 0; j < S; j++) {
+        if (mask & 1) r = fmaf(a.fp[j].x, b.fp[j].x, fmaf(a.fp[j].y, b.fp[j].y, r));
+        if (mask & 2) r = fmaf(a.fm[j].x, b.fm[j].x, fmaf(a.fm[j].y, b.fm[j].y, r));
+        if (mask & 4) r = fmaf(a.zz[j].x, b.zz[j].x, fmaf(a.zz[j].y, b.zz[j].y, r));
+    }
+    return r;
+}
+
+// Re sum [conj(l.F+) i v.F+ - conj(l.F-) i v.F-]: the B0 derivative of a
+// precession that produced v (per unit of phase).
+template <int S>
+__device__ __forceinline__ float b0_term(const LaneState<S> &l, const LaneState<S> &v) {
+    float r = 0.f;
+#pragma unroll
+    for (int j = 0; j < S; j++) {
+        // Re(conj(l) i v) = l.x (-v.y) + l.y v.x
+        r += -l.fp[j].x * v.fp[j].y + l.fp[j].y * v.fp[j].x;
+        r -= -l.fm[j].x * v.fm[j].y + l.fm[j].y * v.fm[j].x;
+    }
+    return r;
+}
+
+template <int S>
+__global__ void __launch_bounds__(kThreads) ssfp_adjoint_kernel(AdjArgs a) {
+    const int L = a.L, apc = kThreads / L;
+    const int tid = threadIdx.x, g = tid / L, gl = tid % L;
+    const bool lane0 = gl == 0;
+    const long long atom = (long long)blockIdx.x * apc + g;
+    const bool active = atom < a.n;
+    const long long at = active ? atom : 0;
+    const float *p = a.params + at * a.nparams;
+    const float T1 = active ? p[0] : 2.f, T2 = active ? p[1] : 1.f, B0 = active ? p[2] : 0.f,
+                B1 = active ? p[3] : 1.f;
+    const int T = a.nreps, w = a.w, C = a.C;
+    const long long LS = (long long)L * S;
+    float *ck = a.ckpt + at * (long long)a.nckpt * 6 * LS;
+    float *sg = a.seg + at * (long long)C * 6 * LS;
+
+    // forward sweep with checkpoints every C steps
+    LaneState<S> v;
+    st_init<S>(v, lane0, T1, T2, 180.f, 0.f, a.TI);
+    for (int t = 0; t < T; t++) {
+        if (t % C == 0 && active) save<S>(ck + (long long)(t / C) * 6 * LS, L, gl, v);
+        const StepC c = step_constants(a, t, T1, T2, B0, B1);
+        const float2 s = forward_step<S>(v, c, gl, L, w, lane0);
+        if (lane0 && active && a.sig) a.sig[at * T + t] = s;
+    }
+    __syncwarp();
+
+    // reverse sweep, one segment at a time
+    LaneState<S> lam;
+    zero<S>(lam);
+    float gE1_T1 = 0.f, gE2_T2 = 0.f, gB0 = 0.f, gB1 = 0.f;  // lane partials, chained per step
+    for (int sgi = a.nckpt - 1; sgi >= 0; sgi--) {
+        const int t0 = sgi * C, t1 = min(T, t0 + C);
+        LaneState<S> u;
+        if (active) load<S>(u, ck + (long long)sgi * 6 * LS, L, gl);
+        else zero<S>(u);
+        for (int t = t0; t < t1; t++) {
+            if (active) save<S>(sg + (long long)(t - t0) * 6 * LS, L, gl, u);
+            const StepC c = step_constants(a, t, T1, T2, B0, B1);
+            forward_step<S>(u, c, gl, L, w, lane0);
+        }
+        __syncwarp();
+        for (int t = t1 - 1; t >= t0; t--) {
+            const StepC c = step_constants(a, t, T1, T2, B0, B1);
+            float2 dT[9], Tm[9];
+            rf_and_derivative(c.ca, c.sa, c.z, Tm, dT);
+            // intermediates of step t from its start state v0
+            LaneState<S> v0, v1, v3, v4, v5;
+            if (active) load<S>(v0, sg + (long long)(t - t0) * 6 * LS, L, gl);
+            else zero<S>(v0);
+            v1 = v0;
+            st_rf<S>(v1, c.T);
+            LaneState<S> v2 = v1;
+            st_relax<S>(v2, c.E1a, c.E2a, lane0);
+            v3 = v2;
+            st_b0<S>(v3, c.ea);
+            v4 = v3;
+            st_b0<S>(v4, c.eb);
+            v5 = v4;
+            st_shift<S>(v5, gl, L, w);
+            // relax(TR - TE): lam5 = E lam6; dL/dE1b = Re<lam6.Z, v5.Z> - Re lam6.Z0
+            const float dE1b = c.E1b * c.tb / (T1 * T1), dE2b = c.E2b * c.tb / (T2 * T2);
+            float gz = redot<S>(lam, v5, 4) - (lane0 ? lam.zz[0].x : 0.f);
+            float gf = redot<S>(lam, v5, 3);
+            gE1_T1 = fmaf(gz, dE1b, gE1_T1);
+            gE2_T2 = fmaf(gf, dE2b, gE2_T2);
+#pragma unroll
+            for (int j = 0; j < S; j++) {
+                lam.fp[j] = c_scale(lam.fp[j], c.E2b);
+                lam.fm[j] = c_scale(lam.fm[j], c.E2b);
+                lam.zz[j] = c_scale(lam.zz[j], c.E1b);
+            }
+            // shift
+            shift_transpose<S>(lam, gl, L, w);
+            // B0 over TR - TE (conjugate phasors), its B0 derivative with v4
+            gB0 = fmaf(b0_term<S>(lam, v4), (float)(2 * M_PI * c.tb / 1000.0), gB0);
+            st_b0<S>(lam, c_conj(c.eb));
+            // readout s_t = v3.F+[0]
+            if (lane0 && active) {
+                const float2 gs = a.gsig[at * T + t];
+                lam.fp[0].x += gs.x;
+                lam.fp[0].y += gs.y;
+            }
+            // B0 over TE
+            gB0 = fmaf(b0_term<S>(lam, v3), (float)(2 * M_PI * c.ta / 1000.0), gB0);
+            st_b0<S>(lam, c_conj(c.ea));
+            // relax(TE)
+            const float dE1a = c.E1a * c.ta / (T1 * T1), dE2a = c.E2a * c.ta / (T2 * T2);
+            gz = redot<S>(lam, v1, 4) - (lane0 ? lam.zz[0].x : 0.f);
+            gf = redot<S>(lam, v1, 3);
+            gE1_T1 = fmaf(gz, dE1a, gE1_T1);
+            gE2_T2 = fmaf(gf, dE2a, gE2_T2);
+#pragma unroll
+            for (int j = 0; j < S; j++) {
+                lam.fp[j] = c_scale(lam.fp[j], c.E2a);
+                lam.fm[j] = c_scale(lam.fm[j], c.E2a);
+                lam.zz[j] = c_scale(lam.zz[j], c.E1a);
+            }
+            // RF: dL/dalpha = Re<lam1, dM v0>; lam0 = M^H lam1
+            float ga = 0.f;
+#pragma unroll
+            for (int j = 0; j < S; j++) {
+                const float2 q0 = rf_row(dT[0], dT[1], dT[2], v0.fp[j], v0.fm[j], v0.zz[j]);
+                const float2 q1 = rf_row(dT[3], dT[4], dT[5], v0.fp[j], v0.fm[j], v0.zz[j]);
+                const float2 q2 = rf_row(dT[6], dT[7], dT[8], v0.fp[j], v0.fm[j], v0.zz[j]);
+                ga = fmaf(lam.fp[j].x, q0.x, fmaf(lam.fp[j].y, q0.y, ga));
+                ga = fmaf(lam.fm[j].x, q1.x, fmaf(lam.fm[j].y, q1.y, ga));
+                ga = fmaf(lam.zz[j].x, q2.x, fmaf(lam.zz[j].y, q2.y, ga));
+                const float2 l0 = lam.fp[j], l1 = lam.fm[j], l2 = lam.zz[j];
+                lam.fp[j] = rf_row(c_conj(c.T[0]), c_conj(c.T[3]), c_conj(c.T[6]), l0, l1, l2);
+                lam.fm[j] = rf_row(c_conj(c.T[1]), c_conj(c.T[4]), c_conj(c.T[7]), l0, l1, l2);
+                lam.zz[j] = rf_row(c_conj(c.T[2]), c_conj(c.T[5]), c_conj(c.T[8]), l0, l1, l2);
+            }
+            // the step's flip-angle gradient over the group's lanes
+            for (int o = 1; o < L; o <<= 1) ga += __shfl_xor_sync(0xffffffffu, ga, o, L);
+            gB1 = fmaf(ga, a.alpha[t], gB1);
+            if (lane0 && active) a.galpha_atoms[at * T + t] = ga * B1 * a.fa_scale;
+        }
+    }
+    // the inversion: Z0 = E1 cos(a0) + 1 - E1, F+0 = conj(q), F-0 = q,
+    // q = E2 sin(a0) (0 + i)
+    if (lane0) {
+        const float alpha0 = (float)(180.f * M_PI / 180.f);
+        float sa0, ca0;
+        __sincosf(alpha0, &sa0, &ca0);
+        const float e1 = expf(-a.TI / T1), e2 = expf(-a.TI / T2);
+        gE1_T1 = fmaf(lam.zz[0].x * (ca0 - 1.f), e1 * a.TI / (T1 * T1), gE1_T1);
+        // d/dT2: F+0 = (0, -e2 sa0), F-0 = (0, e2 sa0)
+        gE2_T2 = fmaf(-lam.fp[0].y * sa0 + lam.fm[0].y * sa0, e2 * a.TI / (T2 * T2), gE2_T2);
+    }
+    for (int o = 1; o < L; o <<= 1) {
+        gE1_T1 += __shfl_xor_sync(0xffffffffu, gE1_T1, o, L);
+        gE2_T2 += __shfl_xor_sync(0xffffffffu, gE2_T2, o, L);
+        gB0 += __shfl_xor_sync(0xffffffffu, gB0, o, L);
+    }
+    if (lane0 && active) {
+        float *gp = a.gparams + at * 4;
+        gp[0] = gE1_T1;
+        gp[1] = gE2_T2;
+        gp[2] = gB0;
+        gp[3] = gB1;
+    }
+}
+
+}  // namespace ssfpgrad
+
+// snapmrf_epg_adjoint for echo_type epg_ssfp: h_mrf in the CSV convention
+// (converted as MRF_dict converts it), TI = 40 ms.  Writes the signal
+// (optional), dL/d(T1, T2, B0, B1) per atom and the per-atom schedule
+// gradient dL/dh_mrf[0][t] into galpha_atoms.
+int epg_adjoint_ssfp(const float *d_params, int nparams, const float *h_mrf, size_t nreps, size_t NREPS,
+                     size_t natoms, int nstates, const float *d_grad_signal, float *d_signal, float *d_grad_params,
+                     float *galpha_atoms, int checkpoint_every, cudaStream_t st) {
+    using namespace ssfpgrad;
+    if (nstates > 32 * 4) SNAPMRF_FAIL(SNAPMRF_ERR_UNSUPPORTED, "epg_adjoint (epg_ssfp): nstates must be <= 128");
+    std::vector<float> h(4 * nreps);
+    const float fa_scale = (float)(60.f * M_PI / 180.f), ph_scale = (float)(M_PI / 180.f);
+    for (size_t t = 0; t < nreps; t++) {
+        h[t] = h_mrf[t] * fa_scale;
+        h[nreps + t] = h_mrf[NREPS + t] * ph_scale;
+        h[2 * nreps + t] = h_mrf[2 * NREPS + t] + 16.f;
+        h[3 * nreps + t] = h_mrf[3 * NREPS + t] + 3.5f;
+    }
+    int L, S;
+    choose_ls(nstates, &L, &S);
+    const int C = checkpoint_every > 0 ? checkpoint_every : (int)std::max(1.0, std::ceil(std::sqrt((double)nreps)));
+    const int nckpt = (int)((nreps + C - 1) / C);
+    const long long LS = (long long)L * S;
+    DeviceScratch sbuf, work;
+    SNAPMRF_CUDA(sbuf.alloc(h.size() * sizeof(float), st));
+    float *hs = static_cast<float *>(stage_acquire(h.size() * sizeof(float)));
+    if (!hs) SNAPMRF_FAIL(SNAPMRF_ERR_ALLOC, "epg_adjoint: cannot allocate a pinned staging buffer");
+    memcpy(hs, h.data(), h.size() * sizeof(float));
+    SNAPMRF_CUDA(stage_upload(sbuf.ptr, hs, h.size() * sizeof(float), st));
+    SNAPMRF_CUDA(stage_release(st));
+    const size_t ck = natoms * (size_t)nckpt * 6 * LS, sgn = natoms * (size_t)C * 6 * LS;
+    SNAPMRF_CUDA(work.alloc((ck + sgn) * sizeof(float), st));
+    AdjArgs a;
+    const float *ds = sbuf.as<float>();
+    a.alpha = ds;
+    a.phi = ds + nreps;
+    a.TR = ds + 2 * nreps;
+    a.TE = ds + 3 * nreps;
+    a.fa_scale = fa_scale;
+    a.nreps = (int)nreps;
+    a.TI = 40.f;
+    a.params = d_params;
+    a.nparams = nparams;
+    a.n = (long long)natoms;
+    a.w = nstates;
+    a.L = L;
+    a.gsig = reinterpret_cast<const float2 *>(d_grad_signal);
+    a.sig = reinterpret_cast<float2 *>(d_signal);
+    a.gparams = d_grad_params;
+    a.galpha_atoms = galpha_atoms;
+    a.ckpt = work.as<float>();
+    a.seg = a.ckpt + ck;
+    a.C = C;
+    a.nckpt = nckpt;
+    const int apc = kThreads / L;
+    dim3 grid((unsigned)((natoms + apc - 1) / apc));
+    if (S == 2) ssfp_adjoint_kernel<2><<<grid, kThreads, 0, st>>>(a);
+    else ssfp_adjoint_kernel<4><<<grid, kThreads, 0, st>>>(a);
+    SNAPMRF_LAUNCH_CHECK();
+    return SNAPMRF_OK;
+}
+
+}  // namespace snapmrf

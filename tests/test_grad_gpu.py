@@ -379,3 +379,68 @@ def test_gn_ssfp_recovers_off_grid_parameters(snap, oracle, with_map):
         s, _ = oracle.ssfp_jvp(tuple(truth[i]), (0, 0, 0, 0), h, nstates=w)
         assert abs(m0[i] - abs(rho[i])) < 2e-3 * abs(rho[i])
         assert abs(got[i, 4] - abs(rho[i]) * np.linalg.norm(s)) < 2e-3 * abs(rho[i]) * np.linalg.norm(s)
+
+
+def test_ssfp_adjoint_matches_fp64_forward_mode_and_differences(snap, oracle):
+    """Reverse mode through the complex bSSFP recursion (B0 precession,
+    alternating RF phase, the inversion) with checkpoints: for a loss linear
+    in the signal, L = sum_t Re(conj(g_t) s_t), the gradients by (T1, T2, B0,
+    B1) equal the FP64 forward mode's, the schedule gradient equals FP64
+    central differences along random directions, the signal equals the FP64
+    recursion's, and the checkpoint interval changes nothing."""
+    import torch
+    from cases import c4_ssfp_csv
+    T, w, n = 150, 30, 8
+    h = c4_ssfp_csv(T, seed=47)
+    rng = np.random.default_rng(48)
+    t1 = np.exp(rng.uniform(np.log(300), np.log(2500), n))
+    t2 = np.minimum(np.exp(rng.uniform(np.log(30), np.log(300), n)), 0.5 * t1)
+    params = np.stack([t1, t2, rng.uniform(-60, 60, n), rng.uniform(0.85, 1.15, n)], 1).astype(np.float32)
+    g = (rng.standard_normal((n, T)) + 1j * rng.standard_normal((n, T))).astype(np.complex64)
+    d_p = torch.from_numpy(params).cuda()
+    d_g = torch.from_numpy(g.view(np.float32).reshape(n, T, 2)).cuda()
+    out = {}
+    for C in (7, 1, T):
+        d_sig = torch.empty((n, T, 2), device="cuda")
+        d_gp = torch.empty((n, 4), device="cuda")
+        d_ga = torch.empty(T, device="cuda")
+        d_gaa = torch.empty((n, T), device="cuda")
+        snap.epg_adjoint(d_p, h, T, T, n, d_g, d_gp, 4, w, "epg_ssfp", d_signal=d_sig, d_grad_alpha=d_ga,
+                         d_grad_alpha_atoms=d_gaa, checkpoint_every=C)
+        torch.cuda.synchronize()
+        out[C] = (d_sig.cpu().numpy(), d_gp.cpu().numpy(), d_ga.cpu().numpy(), d_gaa.cpu().numpy())
+    for C in (1, T):
+        for a, b in zip(out[7], out[C]):
+            np.testing.assert_array_equal(a, b)
+    sig, gp, ga, gaa = out[7]
+    sig = sig[..., 0] + 1j * sig[..., 1]
+    np.testing.assert_allclose(ga, gaa.sum(axis=0), rtol=1e-4, atol=1e-4 * np.abs(gaa).sum(axis=0).max())
+    for i in range(n):
+        th = tuple(params[i].astype(np.float64))
+        s, _ = oracle.ssfp_jvp(th, (0, 0, 0, 0), h, nstates=w)
+        assert np.abs(sig[i] - s).max() <= 1e-5 * np.abs(s).max()
+        for j in range(4):
+            tg = [0.0] * 4
+            tg[j] = 1.0
+            _, ds = oracle.ssfp_jvp(th, tg, h, nstates=w)
+            want = float(np.sum((np.conj(g[i]) * ds).real))
+            scale = float(np.sum(np.abs(g[i]) * np.abs(ds)))
+            assert abs(gp[i, j] - want) <= 1e-3 * abs(want) + 1e-4 * scale, (i, j, gp[i, j], want)
+    # the schedule's flip entries: central differences of the FP64 loss
+    def loss(hh):
+        total = 0.0
+        for i in range(n):
+            s, _ = oracle.ssfp_jvp(tuple(params[i].astype(np.float64)), (0, 0, 0, 0), hh, nstates=w)
+            total += float(np.sum((np.conj(g[i]) * s).real))
+        return total
+    for trial in range(2):
+        v = rng.standard_normal(T)
+        e = 1e-3
+        hp, hm = h.copy(), h.copy()
+        hp[0] = (h[0].astype(np.float64) + e * v).astype(np.float32)
+        hm[0] = (h[0].astype(np.float64) - e * v).astype(np.float32)
+        dv = (hp[0].astype(np.float64) - hm[0]) / (2 * e)
+        fd = (loss(hp) - loss(hm)) / (2 * e)
+        got = float(ga.astype(np.float64) @ dv)
+        print(f"bSSFP schedule gradient along a random direction: adjoint {got:.6e}, FP64 difference {fd:.6e}")
+        assert abs(got - fd) <= 5e-3 * abs(fd) + 1e-3 * float(np.abs(ga) @ np.abs(dv))
