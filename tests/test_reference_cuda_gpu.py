@@ -368,8 +368,8 @@ def test_c1_shape_matching_vs_reference_cuda(snap, c1_blocks):
 
 def test_c4_shape_ssfp_vs_reference_cuda(snap, tmp_path):
     """The large off-resonance configuration's bSSFP dictionary at its shape
-    (T = 500, w = 50, the 6,938 T1/T2 pairs x B0 in [-100, 100] Hz x two B1
-    blocks = 69,380 atoms) against the rebuilt reference's epg_ssfp within
+    (T = 500, w = 50, the 6,938 T1/T2 pairs x 8 B0 values in [-100, 100] Hz
+    x two B1 blocks = 111,008 atoms) against the rebuilt reference's epg_ssfp within
     1e-5; then 4,096 noisy voxels matched without a B1 map (the reference
     merges its blocks by the largest PD: a global first argmax) in FP32 and
     on the tensor cores with complex [Re; Im] operands, equal to the
@@ -378,11 +378,11 @@ def test_c4_shape_ssfp_vs_reference_cuda(snap, tmp_path):
     T, w = 500, 50
     h = c4_ssfp_csv(T)
     t1, t2 = geometric_grid(100.0, 5000.0), geometric_grid(10.0, 2000.0)
-    b0 = np.array([-100.0, -48.0, 0.0, 52.0, 100.0], np.float32)
+    b0 = np.array([-100.0 + 28.0 * k for k in range(8)], np.float32)   # on the -100:4:100 grid
     b1 = np.array([0.9, 1.1], np.float32)
     params = snap.trans_params(t1, t2, b0, b1)
     natoms = params.shape[0] // len(b1)
-    assert params.shape[0] == 69380
+    assert params.shape[0] == 111008
     ref = ref_dict(tmp_path, "epg_ssfp", params, h, T, natoms, w)
     got = run_dict(snap, "epg_ssfp", params, h, T, natoms=natoms, nstates=w)
     rel = rel_err_per_atom(got, ref)
