@@ -161,8 +161,8 @@ def test_adjoint_rejects_unsupported_inputs(snap):
     d_params = torch.from_numpy(atoms_params(2)).cuda()
     g = torch.zeros((2, T, 2), device="cuda")
     gp = torch.zeros((2, 3), device="cuda")
-    with pytest.raises(snap.SnapMRFError):
-        snap.epg_adjoint(d_params, h, T, T, 2, g, gp, 4, 10, "epg_ssfp")
+    with pytest.raises(snap.SnapMRFError, match="epg_fisp, epg_sr or epg_ssfp"):
+        snap.epg_adjoint(d_params, h, T, T, 2, g, gp, 4, 10, "epg_se")
     hp = h.copy()
     hp[1, 3] = 0.5
     with pytest.raises(snap.SnapMRFError):
