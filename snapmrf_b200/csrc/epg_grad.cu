@@ -371,6 +371,12 @@ struct GnArgs {
     int *count_out;
     float tol;
     int finish;               // a voxel that stops in this pass writes PD, M0, B1
+    // part 0: the whole list; 1: the bulk, whole rounds of round_groups groups
+    // of bulk_apc voxels; 2: the tail after the bulk (a finer layout), so that
+    // no round of the bulk kernel runs nearly empty
+    int part;
+    int bulk_apc;
+    long long round_groups;
 };
 
 // A voxel whose map holds no usable start (not finite, T2 <= 0, T1 <= T2)
@@ -458,12 +464,19 @@ __global__ void __launch_bounds__(kGnThreads) gn_kernel(GnArgs a, int chunk) {
     GnStep *sQ = reinterpret_cast<GnStep *>(gn_smem);              // [apc][chunk]
     float *sV = reinterpret_cast<float *>(sQ + apc * chunk);       // [apc][4]: T1, T2, B1, ok
     long long *sI = reinterpret_cast<long long *>(sV + apc * 4);  // [apc]: voxel or -1
-    const long long vox0 = (long long)blockIdx.x * apc;
     const long long nlist = a.list_in ? (long long)*a.count_in : a.nvox;
+    long long first = 0, end = nlist;
+    if (a.part) {
+        const long long groups = (nlist + a.bulk_apc - 1) / a.bulk_apc;
+        const long long bulk = min(nlist, (groups / a.round_groups) * a.round_groups * a.bulk_apc);
+        if (a.part == 1) end = bulk;
+        else first = bulk;
+    }
+    const long long vox0 = first + (long long)blockIdx.x * apc;
     for (int i = tid; i < apc; i += kGnThreads) {
         const long long slot = vox0 + i;
         long long v = -1;
-        if (slot < nlist) v = a.list_in ? (long long)a.list_in[slot] : slot;
+        if (slot < end) v = a.list_in ? (long long)a.list_in[slot] : slot;
         sI[i] = v;
         float T1 = 2.f, T2 = 1.f, B1 = 1.f, ok = 0.f;
         if (v >= 0) {
@@ -1014,6 +1027,19 @@ static void choose(int w, int *L, int *S) {
     default: gn_kernel<7, B><<<GRID, kGnThreads, SMEM, ST>>>(ARGS, CHUNK); break;     \
     }
 
+// Resident CTAs per SM of gn_kernel<P, true> with `smem` bytes.
+static cudaError_t gn_occupancy(int P, size_t smem, int *per_sm) {
+    switch (P) {
+    case 1: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, gn_kernel<1, true>, kGnThreads, smem);
+    case 2: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, gn_kernel<2, true>, kGnThreads, smem);
+    case 3: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, gn_kernel<3, true>, kGnThreads, smem);
+    case 4: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, gn_kernel<4, true>, kGnThreads, smem);
+    case 5: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, gn_kernel<5, true>, kGnThreads, smem);
+    case 6: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, gn_kernel<6, true>, kGnThreads, smem);
+    default: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, gn_kernel<7, true>, kGnThreads, smem);
+    }
+}
+
 // Schedule of the real-valued recursion on the device; fails unless every
 // RF phase is 0.
 static int upload_schedule(DeviceScratch &buf, Schedule *sc, const float *h_mrf, size_t nreps, size_t NREPS,
@@ -1191,6 +1217,9 @@ extern "C" int snapmrf_refine_gn(float *d_maps, int nmaps, const float *img, siz
     a.tol = tol;
     a.list_in = a.count_in = nullptr;
     a.list_out = a.count_out = nullptr;
+    a.part = 0;
+    a.bulk_apc = 1;
+    a.round_groups = 1;
     // voxel lists of the early exit: two lists and two counters
     const bool early = tol > 0.f && iterations > 1;
     DeviceScratch lists;
@@ -1204,10 +1233,47 @@ extern "C" int snapmrf_refine_gn(float *d_maps, int nmaps, const float *img, siz
     }
     const int apc = kGnThreads / L;
     // steps staged per chunk: at most kGnChunk, within 48 KB of shared memory
-    const size_t fixed = (size_t)apc * (4 * sizeof(float) + sizeof(long long));
-    const int chunk = (int)std::min<size_t>(kGnChunk, (48 * 1024 - fixed) / ((size_t)apc * sizeof(GnStep)));
-    const size_t smem = (size_t)apc * chunk * sizeof(GnStep) + fixed;
+    auto smem_for = [&](int apc_, int *chunk_) {
+        const size_t fixed = (size_t)apc_ * (4 * sizeof(float) + sizeof(long long));
+        *chunk_ = (int)std::min<size_t>(kGnChunk, (48 * 1024 - fixed) / ((size_t)apc_ * sizeof(GnStep)));
+        return (size_t)apc_ * *chunk_ * sizeof(GnStep) + fixed;
+    };
+    int chunk = 0;
+    const size_t smem = smem_for(apc, &chunk);
     dim3 grid((unsigned)((nvoxels + apc - 1) / apc));
+    // The tail of the list: the bulk launch takes whole rounds of resident
+    // CTAs, the voxels past the last whole round go to a launch with four
+    // times the lanes per voxel (a quarter of the work per lane), so the last
+    // round does not run nearly empty (C1: 7,200 groups on 1,184 resident
+    // CTAs were 6.08 rounds).  Same operations per state, same results.
+    // SNAPMRF_GN_TAIL=0 turns it off.
+    GnArgs t = a;
+    int P_tail = 0, chunk_tail = 0;
+    size_t smem_tail = 0;
+    dim3 grid_tail(0);
+    {
+        const char *e = getenv("SNAPMRF_GN_TAIL");
+        const int L_tail = std::min(32, 4 * L);
+        P_tail = (nstates + 2 * L_tail - 1) / (2 * L_tail);
+        int dev = 0, sms = 0, per_sm = 0;
+        if (!(e && atoi(e) == 0) && L_tail > L && P_tail >= 1 && P_tail <= kGnMaxPairs &&
+            cudaGetDevice(&dev) == cudaSuccess &&
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess &&
+            gn_occupancy(P, smem, &per_sm) == cudaSuccess && sms > 0 && per_sm > 0) {
+            const int apc_tail = kGnThreads / L_tail;
+            smem_tail = smem_for(apc_tail, &chunk_tail);
+            a.part = 1;
+            a.bulk_apc = apc;
+            a.round_groups = (long long)sms * per_sm;
+            t = a;
+            t.part = 2;
+            t.L = L_tail;
+            const long long tail_max = std::min<long long>((long long)nvoxels, (a.round_groups + 1) * apc);
+            grid_tail = dim3((unsigned)((tail_max + apc_tail - 1) / apc_tail));
+        } else {
+            cudaGetLastError();
+        }
+    }
     // PD, M0 and the B1 column: written by each voxel in the pass where it
     // stops (early exit, or the last iteration); with no iteration at all, by
     // one value-only pass
@@ -1226,11 +1292,21 @@ extern "C" int snapmrf_refine_gn(float *d_maps, int nmaps, const float *img, siz
         a.finish = outputs && (early || last) ? 1 : 0;
         SNAPMRF_GN_DISPATCH(P, true, grid, smem, st, a, chunk);
         SNAPMRF_LAUNCH_CHECK();
+        if (a.part) {
+            t.list_in = a.list_in;
+            t.count_in = a.count_in;
+            t.list_out = a.list_out;
+            t.count_out = a.count_out;
+            t.finish = a.finish;
+            SNAPMRF_GN_DISPATCH(P_tail, true, grid_tail, smem_tail, st, t, chunk_tail);
+            SNAPMRF_LAUNCH_CHECK();
+        }
     }
     if (outputs && iterations == 0) {
         a.list_in = a.count_in = nullptr;
         a.list_out = a.count_out = nullptr;
         a.finish = 1;
+        a.part = 0;
         SNAPMRF_GN_DISPATCH(P, false, grid, smem, st, a, chunk);
         SNAPMRF_LAUNCH_CHECK();
     }
