@@ -15,9 +15,11 @@ B1 map, and its BF16 + refine precision form):
             noise at SNR 40 (sigma = ||s|| / sqrt(T) / 40); each voxel is
             matched within its nearest B1 block
 One step = MRF_dict (all 41 blocks) + MRF_match of every voxel (+ the
-Gauss-Newton refinement in the refined forms).  The headline form is the
-metric's own: BF16 matching with the top-16 rescored in FP32, then at most
-three Gauss-Newton iterations per voxel; `forms` times every other form
+refinement in the refined forms: a sub-grid start interpolated from the
+matched atom's neighbourhood of the dictionary, then Gauss-Newton).  The
+headline form is the metric's own: BF16 matching with the top-16 rescored in
+FP32, then the start and at most three Gauss-Newton iterations per voxel
+(a voxel stops once its step is below 1e-3); `forms` times every other form
 (FP32, FP16, FP8, each tensor-core form with and without refinement) in the
 same run.  `value` is voxels/s with inputs resident in HBM; `e2e` runs the
 same step through the public API from pinned host buffers (parameter table,
@@ -475,7 +477,13 @@ def run_ours(args) -> None:
         if ev is not None:
             ev[2].record(stream)
         if gn:
-            # Gauss-Newton refinement of the matched (T1, T2) at the B1 map
+            # sub-grid start from the matched atom's neighbourhood of the
+            # dictionary, then Gauss-Newton refinement of (T1, T2) at the B1 map
+            if not args.no_gn_start:
+                snap.refine_start(d_maps, d_img, d_atoms, d_params, d_index, T, NATOMS, natoms, nvox,
+                                  d_b1map=d_b1, imag_atoms=True)
+            if ev is not None:
+                ev[4].record(stream)
             snap.refine_gn(d_maps, d_img, h_mrf, T, T, nvox, NSTATES, "epg_fisp", iterations=gn,
                            tol=args.gn_tol, d_b1map=d_b1)
         if ev is not None:
@@ -494,7 +502,7 @@ def run_ours(args) -> None:
         torch.cuda.synchronize()
         barrier()
         torch.cuda.synchronize()
-        evs = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
+        evs = [[torch.cuda.Event(enable_timing=True) for _ in range(5)] for _ in range(args.steps)]
         launches0 = snap.kernel_launches()
         t_start = torch.cuda.Event(enable_timing=True)
         t_end = torch.cuda.Event(enable_timing=True)
@@ -512,6 +520,7 @@ def run_ours(args) -> None:
                 "dict_ms": float(np.mean([e[0].elapsed_time(e[1]) for e in evs])),
                 "match_ms": float(np.mean([e[1].elapsed_time(e[2]) for e in evs])),
                 "gn_ms": float(np.mean([e[2].elapsed_time(e[3]) for e in evs])),
+                "start_ms": float(np.mean([e[2].elapsed_time(e[4]) for e in evs])) if gn else 0.0,
                 "maps": d_maps.cpu().numpy(), "index": d_index.cpu().numpy()}
 
     PRECS = {"fp32": snap.PREC_FP32, "bf16": snap.PREC_BF16, "fp16": snap.PREC_FP16, "fp8": snap.PREC_FP8}
@@ -638,7 +647,10 @@ def run_ours(args) -> None:
         e2e_b1[b].copy_(h_b1, non_blocking=True)
         dict_call(hprec, e2e_par[b])
         snap.MRF_match(d_maps, h_img, d_atoms, e2e_par[b], T, T, NATOMS, natoms, nvox, in_b1map=e2e_b1[b],
-                       img_device_copy=e2e_img[b], upload_early=True, **match_kwargs(hprec))
+                       img_device_copy=e2e_img[b], upload_early=True, d_index=d_index, **match_kwargs(hprec))
+        if not args.no_gn_start:
+            snap.refine_start(d_maps, e2e_img[b], d_atoms, e2e_par[b], d_index, T, NATOMS, natoms, nvox,
+                              d_b1map=e2e_b1[b], imag_atoms=True)
         snap.refine_gn(d_maps, e2e_img[b], h_mrf, T, T, nvox, NSTATES, "epg_fisp", iterations=args.gn_iters,
                        tol=args.gn_tol, d_b1map=e2e_b1[b])
         h_maps.copy_(d_maps, non_blocking=True)
@@ -680,10 +692,12 @@ def run_ours(args) -> None:
     names = list(forms)
     t = reduce_over_ranks([e2e_ms, gn_pass_ms] + [forms[f]["elapsed_ms"] for f in names] +
                           [forms[f]["dict_ms"] for f in names] + [forms[f]["match_ms"] for f in names] +
-                          [forms[f]["gn_ms"] for f in names], "max", dev, world)
+                          [forms[f]["gn_ms"] for f in names] + [forms[f]["start_ms"] for f in names],
+                          "max", dev, world)
     e2e_ms, gn_pass_ms = t[0], t[1]
     n = len(names)
-    fms = {f: {"elapsed": t[2 + i], "dict": t[2 + n + i], "match": t[2 + 2 * n + i], "gn": t[2 + 3 * n + i]}
+    fms = {f: {"elapsed": t[2 + i], "dict": t[2 + n + i], "match": t[2 + 2 * n + i], "gn": t[2 + 3 * n + i],
+               "start": t[2 + 4 * n + i]}
            for i, f in enumerate(names)}
 
     if rank == 0:
@@ -750,12 +764,15 @@ def run_ours(args) -> None:
                        "atoms_per_b1_block": natoms, "b1_blocks": NATOMS // natoms, "voxels": nvox,
                        "echo_type": "epg_fisp",
                        "match": f"bf16 tcgen05, nearest B1 block, top-{topk_of('bf16')} rescored in fp32",
-                       "refine": f"Gauss-Newton, at most {args.gn_iters} iterations, tol {args.gn_tol}",
+                       "refine": ("from the matched grid point" if args.no_gn_start else
+                                  "sub-grid start from the dictionary (refine_start), then") +
+                                 f" Gauss-Newton, at most {args.gn_iters} iterations, tol {args.gn_tol}",
                        "l2": "inputs and outputs larger than L2 (no flush needed)",
                        "parallelism": f"{world} independent slices" if world > 1 else "single GPU"},
             "dict_atoms_per_s": round(world * NATOMS / (dict_ms / 1e3), 1),
             "match_voxels_per_s": round(world * nvox / (match_ms / 1e3), 1),
-            "stage_ms": {"dict": round(dict_ms, 3), "match": round(match_ms, 3), "refine": round(gn_ms, 3)},
+            "stage_ms": {"dict": round(dict_ms, 3), "match": round(match_ms, 3), "refine": round(gn_ms, 3),
+                         "refine_start_part": round(fms[HEAD]["start"], 3)},
             "roofline": rls[0][1],
             "roofline_other": [r for _, r in rls[1:]] + [rl_fp32],
             "peaks": {"fp32_fma_tflops": fp32_peak, "fp32_note": fp32_note, "bf16_tflops": pk["bf16_tflops"],
@@ -764,7 +781,8 @@ def run_ours(args) -> None:
                     "h2d_bytes_per_step": int(params.nbytes + img.nbytes + b1map.nbytes + h_mrf.nbytes),
                     "d2h_bytes_per_step": int(nvox * 5 * 4),
                     "path": "params and B1 map up by the caller, MRF_dict, MRF_match(host image streamed by the "
-                            "library into a caller-owned device buffer, overlapping the dictionary), refine_gn, "
+                            "library into a caller-owned device buffer, overlapping the dictionary), "
+                            "refine_start, refine_gn, "
                             "maps to pinned host memory",
                     "image_upload_ms": round(h2d_ms, 3),
                     "image_upload_gbs": round(img.nbytes / (h2d_ms / 1e3) / 1e9, 1) if h2d_ms == h2d_ms else None,
@@ -773,6 +791,7 @@ def run_ours(args) -> None:
                           "ms_per_step": round(fms[f]["elapsed"] / args.steps, 3),
                           "dict_ms": round(fms[f]["dict"], 3), "match_ms": round(fms[f]["match"], 3),
                           "refine_ms": round(fms[f]["gn"], 3),
+                          **({"refine_start_ms": round(fms[f]["start"], 3)} if f.endswith("+gn") else {}),
                           "t1_median_rel_vs_truth": round(median_rel(forms[f]["maps"][:, 0], vt1), 5),
                           "t2_median_rel_vs_truth": round(median_rel(forms[f]["maps"][:, 1], vt2), 5),
                           **({"speedup_vs_fp32_form": round(fms["fp32"]["elapsed"] / fms[f]["elapsed"], 3)}
@@ -1072,6 +1091,8 @@ def main() -> None:
     ap.add_argument("--nx", type=int, default=NX, help="reduced case for profiling: nx x nx voxels")
     ap.add_argument("--gn-iters", type=int, default=3,
                     help="Gauss-Newton iterations (at most, per voxel) of the refined forms")
+    ap.add_argument("--no-gn-start", action="store_true",
+                    help="refine from the matched grid point instead of the dictionary's sub-grid start")
     ap.add_argument("--gn-tol", type=float, default=1e-3,
                     help="a voxel stops refining once a step moves T1 and T2 by at most this (relative); "
                          "1e-3 lies below the noise-limited error at SNR 40 (~1e-3 median)")

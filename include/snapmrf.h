@@ -469,8 +469,9 @@ int snapmrf_epg_adjoint(const float *d_params, int nparams, const float *h_mrf, 
  * (the matching PD of a unit-norm atom).  Voxels whose maps are not finite
  * or do not hold T1 > T2 > 0 are left as they are.
  * img: device complex [nvoxels][img_stride] (0 = nreps);
- * d_m0: optional out [nvoxels], |rho|.  PD, M0 and the B1 column cost one
- * value-only forward pass at the final parameters.
+ * d_m0: optional out [nvoxels], |rho|.  PD, M0 and the B1 column are
+ * written by the pass in which each voxel stops (with iterations == 0, by
+ * one value-only forward pass).
  * iterations: at most this many Gauss-Newton steps per voxel; with tol > 0 a
  * voxel stops once a step changed both T1 and T2 by at most tol of their
  * values (later iterations run only over the voxels still moving). */
@@ -478,6 +479,42 @@ int snapmrf_refine_gn(float *d_maps, int nmaps, const float *img, size_t img_str
                       const float *d_b1map, const float *h_mrf, size_t nreps, size_t NREPS,
                       size_t nvoxels, int nstates, const char *echo_type, int iterations,
                       float max_rel_step, float tol, float *d_m0, void *stream);
+
+/* Sub-grid start for snapmrf_refine_gn from the dictionary, in place.  No
+ * counterpart in the reference (matching ends on the grid).
+ *
+ * For each voxel, the matched atom d_index[v] (as snapmrf_mrf_match writes
+ * it) and the atoms at the adjacent T1 and T2 values of the parameter table
+ * (trans_params order, src/functions.cu:355-391) form a 3 x 3 stencil; with
+ * d_b1map the stencil is taken from the three B1 blocks around the block of
+ * the match and interpolated quadratically to the voxel's B1.  The stencil
+ * interpolated biquadratically in (log T1, log T2) is a surrogate of the
+ * signal model, accurate to third order in the grid step; the voxel's fit
+ * |<s, x>|^2 / ||s||^2 is maximised over it by Gauss-Newton with variable
+ * projection (on the stencil's Gram matrix and inner products with the voxel,
+ * no recursion), within the stencil, and the result replaces (T1, T2) in
+ * d_maps.  The start is typically within 1e-4 of the least-squares fit
+ * (relative), so one refinement pass meets a stopping tolerance of 1e-3.
+ *
+ * Voxels are left as they are when the index is outside [0, NATOMS), the
+ * maps no longer hold the matched atom's (T1, T2), the atom is on the edge of
+ * the grid (no neighbour on one side in T1 or T2, or the adjacent T2 rows
+ * lack one of the three T1 values), the B1 blocks do not share the stencil's
+ * rows, or the fit leaves T1 > T2 > 0.
+ *
+ * d_maps: device in/out [nvoxels][nmaps] (T1, T2 in columns 0 and 1);
+ * d_atoms: device complex [NATOMS][nreps] (normalised or not);
+ * d_params: device [NATOMS][nparams] (T1, T2, B0, B1), natoms per B1 block;
+ * img: device complex [nvoxels][img_stride] (0 = nreps);
+ * d_b1map: optional device [nvoxels] (needs nparams >= 4);
+ * flags: SNAPMRF_START_IMAG_ATOMS when every atom is purely imaginary (the
+ * zero-phase FISP / SR dictionaries), which reads and multiplies half as much;
+ * d_count: optional device counter, incremented once per voxel moved. */
+#define SNAPMRF_START_IMAG_ATOMS 0x1u
+int snapmrf_refine_start(float *d_maps, int nmaps, const int64_t *d_index, const float *d_atoms,
+                         const float *d_params, int nparams, size_t nreps, size_t NATOMS,
+                         size_t natoms, const float *img, size_t img_stride, size_t nvoxels,
+                         const float *d_b1map, unsigned flags, int *d_count, void *stream);
 
 /* Cramer-Rao bound of (T1, T2) and its gradient with respect to the flip-angle
  * schedule, for designing schedules.  No counterpart in the reference.

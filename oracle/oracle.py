@@ -225,6 +225,161 @@ def refine_gn_f64(theta, x, h_mrf, nstates: int = 101, echo: str = "epg_fisp", i
     return t1, t2, pd
 
 
+def _stencil_f64(params, base: int, n: int, j: int):
+    """3 x 3 stencil st[i][c] (T1 node i, T2 node c) of block-local row j in
+    the block starting at `base`, or None: the matched row's neighbours in
+    its T2 row, and the rows holding the same three T1 values in the adjacent
+    T2 rows of the table (trans_params order, src/functions.cu:355-391)."""
+    P = params[base:base + n]
+    t1, t2, b0 = P[:, 0], P[:, 1], P[:, 2]
+    if j < 1 or j + 1 >= n:
+        return None
+    T1m, T1c, T1p, T2c, B0c = t1[j - 1], t1[j], t1[j + 1], t2[j], b0[j]
+    if t2[j - 1] != T2c or t2[j + 1] != T2c or b0[j - 1] != B0c or b0[j + 1] != B0c:
+        return None
+    if not ((T1m < T1c < T1p) or (T1m > T1c > T1p)):
+        return None
+    st = [[0] * 3 for _ in range(3)]
+    st[0][1], st[1][1], st[2][1] = j - 1, j, j + 1
+    T2n = []
+    for s, d in ((0, -1), (1, 1)):
+        r = j + 2 * d
+        while 0 <= r < n and t2[r] == T2c and b0[r] == B0c:
+            r += d
+        if not 0 <= r < n:
+            return None
+        T2r = t2[r]
+        if b0[r] != B0c or not T2r != T2c or not np.isfinite(T2r):
+            return None
+        while 0 <= r < n and t2[r] == T2r and b0[r] == B0c and t1[r] != T1c:
+            r += d
+        if not 0 <= r < n:
+            return None
+        rc = r
+        if rc < 1 or rc + 1 >= n:
+            return None
+        if not (t1[rc] == T1c and t2[rc] == T2r and b0[rc] == B0c):
+            return None
+        if not (t1[rc - 1] == T1m and t2[rc - 1] == T2r and b0[rc - 1] == B0c):
+            return None
+        if not (t1[rc + 1] == T1p and t2[rc + 1] == T2r and b0[rc + 1] == B0c):
+            return None
+        c = 2 if s else 0
+        st[0][c], st[1][c], st[2][c] = rc - 1, rc, rc + 1
+        T2n.append(T2r)
+    if not (T2n[0] != T2n[1] and (T2n[0] < T2c) == (T2c < T2n[1])):
+        return None
+    return st
+
+
+def refine_start_f64(maps, index, atoms, params, img, natoms: int, b1map=None, iterations: int = 10):
+    """Sub-grid start of the refinement (snapmrf_refine_start) in FP64.  No
+    counterpart in the reference; this is the checker's statement of it.
+
+    Per voxel: the matched atom's 3 x 3 (T1, T2) stencil (_stencil_f64);
+    with a B1 map, the stencil of the three B1 blocks around the match
+    (clamped to the table) interpolated quadratically (Lagrange) to the
+    voxel's B1.  In (U, V) = (log T1 / T1c, log T2 / T2c) the nine signals
+    give the biquadratic surrogate s = sum_pq m_pq U^p V^q; `iterations`
+    Gauss-Newton steps with variable projection on it (each step clipped to
+    half the stencil's width, the point kept within 1.5 times the stencil's
+    extent on each side) from U = V = 0.  Returns
+    (maps with the new T1, T2 as float32, mask of the voxels moved)."""
+    maps = np.array(maps, np.float32, copy=True)
+    atoms = np.asarray(atoms)
+    params = np.asarray(params, np.float32)
+    NATOMS = params.shape[0]
+    nb = NATOMS // natoms
+    moved = np.zeros(maps.shape[0], bool)
+
+    def quad(hm, hp):
+        a1 = 1.0 / (hp * (hp - hm))
+        a2 = -1.0 / (hm * (hp - hm))
+        return a1, a2, 1.0 / hp - a1 * hp, -a2 * hp
+
+    for v in range(maps.shape[0]):
+        k = int(index[v])
+        if k < 0 or k >= NATOMS:
+            continue
+        b, j = divmod(k, natoms)
+        T1c, T2c = params[k, 0], params[k, 1]
+        if maps[v, 0] != T1c or maps[v, 1] != T2c or not (T1c > T2c) or not (T2c > 0):
+            continue
+        st = _stencil_f64(params, b * natoms, natoms, j)
+        if st is None:
+            continue
+        qbase, qw = [b * natoms], [1.0]
+        if b1map is not None and nb >= 3:
+            bs = min(max(b - 1, 0), nb - 3)
+            qbase = [(bs + q) * natoms for q in range(3)]
+            nodes = [float(params[qb + j, 3]) for qb in qbase]
+            ok = all(params[b * natoms + st[i][c], m] == params[qb + st[i][c], m]
+                     for qb in qbase for i in range(3) for c in range(3) for m in range(3))
+            ok = ok and all(params[qb + st[i][c], 3] == nd for qb, nd in zip(qbase, nodes)
+                            for i in range(3) for c in range(3))
+            if not ok or len(set(nodes)) < 3:
+                continue
+            bv = float(b1map[v])
+            if not np.isfinite(bv):
+                continue
+            n0, n1, n2 = nodes
+            qw = [(bv - n1) * (bv - n2) / ((n0 - n1) * (n0 - n2)), (bv - n0) * (bv - n2) / ((n1 - n0) * (n1 - n2)),
+                  (bv - n0) * (bv - n1) / ((n2 - n0) * (n2 - n1))]
+        S = [[sum(w * atoms[qb + st[i][c]].astype(np.complex128) for w, qb in zip(qw, qbase))
+              for c in range(3)] for i in range(3)]
+        bb = b * natoms
+        hum, hup = np.log(params[bb + st[0][1], 0] / np.float64(T1c)), np.log(params[bb + st[2][1], 0] / np.float64(T1c))
+        hvm, hvp = np.log(params[bb + st[1][0], 1] / np.float64(T2c)), np.log(params[bb + st[1][2], 1] / np.float64(T2c))
+        cu, cv = quad(hum, hup), quad(hvm, hvp)
+        m1 = [[None] * 3 for _ in range(3)]
+        for c in range(3):
+            dp, dm = S[2][c] - S[1][c], S[0][c] - S[1][c]
+            m1[0][c], m1[1][c], m1[2][c] = S[1][c], cu[2] * dp + cu[3] * dm, cu[0] * dp + cu[1] * dm
+        M = []
+        for p in range(3):
+            dp, dm = m1[p][2] - m1[p][1], m1[p][0] - m1[p][1]
+            M += [m1[p][1], cv[2] * dp + cv[3] * dm, cv[0] * dp + cv[1] * dm]
+        M = np.array(M)
+        Gh = M.conj() @ M.T
+        pv = M.conj() @ np.asarray(img[v], np.complex128)
+        ulo, uhi = 1.5 * min(hum, hup), 1.5 * max(hum, hup)
+        vlo, vhi = 1.5 * min(hvm, hvp), 1.5 * max(hvm, hvp)
+        U = V = 0.0
+        for _ in range(iterations):
+            Up, Vp, dU, dV = [1, U, U * U], [1, V, V * V], [0, 1, 2 * U], [0, 1, 2 * V]
+            c0 = np.array([Up[p] * Vp[q] for p in range(3) for q in range(3)])
+            c1 = np.array([dU[p] * Vp[q] for p in range(3) for q in range(3)])
+            c2 = np.array([Up[p] * dV[q] for p in range(3) for q in range(3)])
+            Ss = (c0 @ Gh @ c0).real
+            g1, g2 = c0 @ Gh @ c1, c0 @ Gh @ c2
+            H11, H12, H22 = (c1 @ Gh @ c1).real, (c1 @ Gh @ c2).real, (c2 @ Gh @ c2).real
+            P, Q1, Q2 = c0 @ pv, c1 @ pv, c2 @ pv
+            if not Ss > 0:
+                break
+            rho = P / Ss
+            r2 = abs(rho) ** 2
+            A11 = r2 * (H11 - abs(g1) ** 2 / Ss)
+            A12 = r2 * (H12 - (np.conj(g1) * g2).real / Ss)
+            A22 = r2 * (H22 - abs(g2) ** 2 / Ss)
+            b1 = (np.conj(rho) * (Q1 - np.conj(g1) * P / Ss)).real
+            b2 = (np.conj(rho) * (Q2 - np.conj(g2) * P / Ss)).real
+            det = A11 * A22 - A12 * A12
+            if not det > 0 or not A11 > 0 or not np.isfinite(det):
+                break
+            d1, d2 = (A22 * b1 - A12 * b2) / det, (A11 * b2 - A12 * b1) / det
+            if not (np.isfinite(d1) and np.isfinite(d2)):
+                break
+            lu, lv = 0.5 * (max(hum, hup) - min(hum, hup)), 0.5 * (max(hvm, hvp) - min(hvm, hvp))
+            U = min(max(U + min(max(d1, -lu), lu), ulo), uhi)
+            V = min(max(V + min(max(d2, -lv), lv), vlo), vhi)
+        T1, T2 = float(T1c) * np.exp(U), float(T2c) * np.exp(V)
+        if not (np.isfinite(T1) and np.isfinite(T2) and T2 > 0 and T1 > T2 * (1 + 1e-4)):
+            continue
+        maps[v, 0], maps[v, 1] = T1, T2
+        moved[v] = True
+    return maps, moved
+
+
 def svd_compress(atoms, natoms: int, sfrac: float | None = None, rank: int | None = None):
     """Low-rank compression per B1 block, restated from matlab/MRF_dict_B1.m:127-159
     (input.reduce = 1) in FP64 numpy:

@@ -38,6 +38,7 @@ PREC_FP8 = 3
 MATCH_ASSUME_UNIFORM_B1 = 0x1
 MATCH_IMAG_ATOMS = 0x2
 MATCH_UPLOAD_EARLY = 0x4
+START_IMAG_ATOMS = 0x1
 
 ECHO_TYPES = ("epg_ssfp", "roa_ssfp", "epg_sr", "epg_se", "epg_tse1", "epg_tse2", "epg_fisp")
 
@@ -127,6 +128,8 @@ def lib() -> C.CDLL:
                                            C.c_int, vp]
         L.snapmrf_refine_gn.argtypes = [vp, C.c_int, vp, sz, vp, vp, sz, sz, sz, C.c_int, C.c_char_p, C.c_int,
                                         C.c_float, C.c_float, vp, vp]
+        L.snapmrf_refine_start.argtypes = [vp, C.c_int, vp, vp, vp, C.c_int, sz, sz, sz, vp, sz, sz, vp,
+                                           C.c_uint, vp, vp]
         _lib = L
     return _lib
 
@@ -471,6 +474,23 @@ def refine_gn(d_maps, d_img, h_mrf, nreps: int, NREPS: int, nvoxels: int, nstate
                                    h_mrf.ctypes.data, nreps,
                                    NREPS, nvoxels, nstates, echo_type.encode(), iterations, max_rel_step,
                                    tol, _ptr(d_m0), _stream_ptr(stream)))
+
+
+def refine_start(d_maps, d_img, d_atoms, d_params, d_index, nreps: int, NATOMS: int, natoms: int,
+                 nvoxels: int, *, nmaps: int = NMAPS, nparams: int = NPARAMS, img_stride: int = 0,
+                 d_b1map=None, imag_atoms: bool = False, d_count=None, stream=None) -> None:
+    """Sub-grid start for refine_gn, in place: each voxel's matched atom
+    (d_index, int64, as MRF_match writes it) and its 3 x 3 (T1, T2)
+    neighbourhood of the dictionary (d_atoms complex [NATOMS][nreps]; with
+    d_b1map, three B1 blocks interpolated to the voxel's B1) interpolated
+    biquadratically in (log T1, log T2); the fit of the voxel maximised over
+    that surrogate replaces (T1, T2) in d_maps.  Voxels on the grid's edge are
+    left as they are.  imag_atoms: every atom is purely imaginary (zero-phase
+    FISP / SR).  d_count: optional device int32 counter of voxels moved."""
+    _check(lib().snapmrf_refine_start(_ptr(d_maps), nmaps, _ptr(d_index), _ptr(d_atoms), _ptr(d_params),
+                                      nparams, nreps, NATOMS, natoms, _ptr(d_img), img_stride, nvoxels,
+                                      _ptr(d_b1map), START_IMAG_ATOMS if imag_atoms else 0, _ptr(d_count),
+                                      _stream_ptr(stream)))
 
 
 def packed_pitch(nreps: int) -> int:

@@ -23,7 +23,7 @@ NVCC_FLAGS = ARCH + [
     "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O3", "-Xptxas", "-O3",
     f"-I{ROOT / 'include'}", f"-I{CSRC}",
 ]
-SOURCES = ["host.cpp", "ra.cpp", "epg.cu", "match.cu", "match_noalloc.cu", "match_tc.cu", "epg_grad.cu", "epg_ssfp_grad.cu", "svd.cu"]
+SOURCES = ["host.cpp", "ra.cpp", "epg.cu", "match.cu", "match_noalloc.cu", "match_tc.cu", "epg_grad.cu", "epg_ssfp_grad.cu", "refine_start.cu", "svd.cu"]
 
 
 def nvcc() -> str:

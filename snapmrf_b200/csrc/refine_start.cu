@@ -1,0 +1,450 @@
+// Sub-grid start of the Gauss-Newton refinement, from the dictionary.
+//
+// Matching leaves each voxel on a grid point of the dictionary (the atom of
+// the largest |<d, x>| in the reference's MRF_match, src/functions.cu).  The
+// matched atom and its neighbours at the adjacent T1 and T2 values of the
+// parameter table (trans_params order, src/functions.cu:355-391: B1
+// outermost, then B0, T2, T1 innermost, T1 > T2 kept) form a 3 x 3 stencil;
+// with a B1 map the stencil is read from the three B1 blocks around the
+// voxel's B1 and interpolated quadratically to that value.  Interpolated
+// biquadratically in (u, v) = (log T1, log T2), the nine signals give a
+// surrogate s(u, v) of the signal model, accurate to third order in the grid
+// step.  The voxel's fit |<s, x>|^2 / ||s||^2 is maximised over the surrogate
+// by Gauss-Newton with variable projection, using only the 9 x 9 Gram matrix
+// of the stencil and the stencil's nine inner products with the voxel, so no
+// recursion is run.  The result replaces the voxel's (T1, T2): a start close
+// enough to the least-squares fit that one pass of the refinement usually
+// meets its stopping tolerance.  No counterpart in the reference.
+//
+// Layout: one warp per voxel.  Lanes stride over the time points, each
+// accumulating the Gram matrix and the inner products of its samples in the
+// stencil's Taylor basis (s = sum_pq m_pq U^p V^q, U = u - u_0, V = v - v_0),
+// where the nine basis signals are formed from differences of the atoms
+// sample by sample, so the small derivative terms never come out of a
+// difference of large accumulated sums.  The stencil search runs 32 table
+// rows at a time with warp ballots.
+
+#include "common.h"
+
+#include <cmath>
+#include <cstdint>
+
+namespace snapmrf {
+namespace rstart {
+
+constexpr int kWarps = 4;       // voxels per block
+constexpr int kSolveIters = 10;  // Gauss-Newton iterations on the surrogate
+
+struct Args {
+    float *maps;
+    int nmaps;
+    const int64_t *index;
+    const float2 *atoms;
+    long long atom_stride;  // complex samples per atom row
+    const float *params;
+    int nparams;
+    long long NATOMS, natoms;
+    const float2 *img;
+    long long img_stride;
+    int T;
+    long long nvox;
+    const float *b1map;
+    int *count;
+};
+
+__device__ __forceinline__ float prm(const Args &a, long long r, int c) { return __ldg(a.params + r * a.nparams + c); }
+
+// First k in [0, n) for which pred(start + dir * k) holds, 32 rows at a time
+// across the warp; -1 when there is none.
+template <class F>
+__device__ long long warp_find(long long start, int dir, long long n, F pred) {
+    const int lane = threadIdx.x & 31;
+    for (long long k0 = 0; k0 < n; k0 += 32) {
+        const long long k = k0 + lane;
+        const bool hit = k < n && pred(start + dir * k);
+        const unsigned m = __ballot_sync(0xffffffffu, hit);
+        if (m) return k0 + (__ffs(m) - 1);
+    }
+    return -1;
+}
+
+// The 3 x 3 stencil st[i][c] (T1 node i, T2 node c; node 1 the matched atom
+// j) as row numbers within the block starting at `base`.  False unless the
+// matched atom has a neighbour on both sides in T1 and in T2, and the two
+// adjacent T2 rows hold the same three T1 values in the same order.
+__device__ bool find_stencil(const Args &a, long long base, long long j, long long st[3][3]) {
+    const long long n = a.natoms;
+    auto t1 = [&](long long r) { return prm(a, base + r, 0); };
+    auto t2 = [&](long long r) { return prm(a, base + r, 1); };
+    auto b0 = [&](long long r) { return prm(a, base + r, 2); };
+    if (j < 1 || j + 1 >= n) return false;
+    const float T1m = t1(j - 1), T1c = t1(j), T1p = t1(j + 1), T2c = t2(j), B0c = b0(j);
+    if (t2(j - 1) != T2c || t2(j + 1) != T2c || b0(j - 1) != B0c || b0(j + 1) != B0c) return false;
+    if (!((T1m < T1c && T1c < T1p) || (T1m > T1c && T1c > T1p))) return false;
+    st[0][1] = j - 1;
+    st[1][1] = j;
+    st[2][1] = j + 1;
+    float T2n[2];
+#pragma unroll
+    for (int s = 0; s < 2; s++) {
+        const int dir = s ? 1 : -1;
+        // the first row past the T2 row of j (j - 1 and j + 1 belong to it)
+        const long long from = j + 2 * dir;
+        const long long lim = dir < 0 ? from + 1 : n - from;
+        if (lim <= 0) return false;
+        const long long k = warp_find(from, dir, lim, [&](long long r) { return t2(r) != T2c || b0(r) != B0c; });
+        if (k < 0) return false;
+        const long long r0 = from + dir * k;
+        const float T2r = t2(r0);
+        if (b0(r0) != B0c || !(T2r != T2c) || !isfinite(T2r)) return false;
+        // in that row, the atom at the matched T1
+        const long long lim2 = dir < 0 ? r0 + 1 : n - r0;
+        const long long k2 = warp_find(r0, dir, lim2, [&](long long r) {
+            return t2(r) != T2r || b0(r) != B0c || t1(r) == T1c;
+        });
+        if (k2 < 0) return false;
+        const long long rc = r0 + dir * k2;
+        if (rc < 1 || rc + 1 >= n) return false;
+        if (t1(rc) != T1c || t2(rc) != T2r || b0(rc) != B0c) return false;
+        if (t1(rc - 1) != T1m || t2(rc - 1) != T2r || b0(rc - 1) != B0c) return false;
+        if (t1(rc + 1) != T1p || t2(rc + 1) != T2r || b0(rc + 1) != B0c) return false;
+        const int c = s ? 2 : 0;
+        st[0][c] = rc - 1;
+        st[1][c] = rc;
+        st[2][c] = rc + 1;
+        T2n[s] = T2r;
+    }
+    return T2n[0] != T2n[1] && (T2n[0] < T2c) == (T2c < T2n[1]);
+}
+
+// Coefficients of the quadratic through (h_m, y_m), (0, y_0), (h_p, y_p) in
+// the form y_0 + l x + q x^2: l = b1 dp + b2 dm, q = a1 dp + a2 dm with
+// dp = y_p - y_0, dm = y_m - y_0.
+struct Quad {
+    float a1, a2, b1, b2;
+};
+
+__device__ Quad quad_coeffs(float hm, float hp) {
+    Quad c;
+    c.a1 = 1.f / (hp * (hp - hm));
+    c.a2 = -1.f / (hm * (hp - hm));
+    c.b1 = 1.f / hp - c.a1 * hp;
+    c.b2 = -c.a2 * hp;
+    return c;
+}
+
+// Lagrange weights of the three nodes at x.
+__device__ void lagrange3(const float n[3], float x, float w[3]) {
+    w[0] = (x - n[1]) * (x - n[2]) / ((n[0] - n[1]) * (n[0] - n[2]));
+    w[1] = (x - n[0]) * (x - n[2]) / ((n[1] - n[0]) * (n[1] - n[2]));
+    w[2] = (x - n[0]) * (x - n[1]) / ((n[2] - n[0]) * (n[2] - n[1]));
+}
+
+// index of the packed upper triangle of the 9 x 9 Gram matrix
+__device__ __host__ __forceinline__ constexpr int tri(int i, int j) {
+    return i <= j ? i * 9 - i * (i - 1) / 2 + (j - i) : j * 9 - j * (j - 1) / 2 + (i - j);
+}
+
+template <bool IMAG>
+__global__ void __launch_bounds__(kWarps * 32) start_kernel(const __grid_constant__ Args a) {
+    const int lane = threadIdx.x & 31;
+    const long long v = (long long)blockIdx.x * kWarps + (threadIdx.x >> 5);
+    if (v >= a.nvox) return;  // whole warps leave together
+    const long long k = a.index[v];
+    if (k < 0 || k >= a.NATOMS) return;
+    float *mp = a.maps + v * a.nmaps;
+    const long long b = k / a.natoms, j = k - b * a.natoms;
+    const float T1c = prm(a, k, 0), T2c = prm(a, k, 1);
+    // the maps must still hold the matched grid point
+    if (mp[0] != T1c || mp[1] != T2c || !(T1c > T2c) || !(T2c > 0.f)) return;
+    long long st[3][3];
+    if (!find_stencil(a, b * a.natoms, j, st)) return;
+    // B1 blocks and their weights at the voxel's B1
+    const long long nb = a.NATOMS / a.natoms;
+    int nq = 1;
+    long long qbase[3] = {b * a.natoms, b * a.natoms, b * a.natoms};
+    float qw[3] = {1.f, 0.f, 0.f};
+    if (a.b1map && nb >= 3) {
+        const long long bs = min(max(b - 1, 0ll), nb - 3);
+        float nodes[3];
+        bool ok = true;
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+            qbase[q] = (bs + q) * a.natoms;
+            nodes[q] = prm(a, qbase[q] + j, 3);
+        }
+        // the same (T1, T2, B0) rows in every block of the stencil
+        // (one check per lane, selected without indexing the arrays by lane)
+        if (lane < 27) {
+            const int q = lane / 9, i = (lane / 3) % 3, c = lane % 3;
+            long long row = 0, qb = 0;
+            float node = 0.f;
+#pragma unroll
+            for (int ii = 0; ii < 3; ii++)
+#pragma unroll
+                for (int cc = 0; cc < 3; cc++)
+                    if (ii == i && cc == c) row = st[ii][cc];
+#pragma unroll
+            for (int qq = 0; qq < 3; qq++)
+                if (qq == q) {
+                    qb = qbase[qq];
+                    node = nodes[qq];
+                }
+            const long long r0 = b * a.natoms + row, r1 = qb + row;
+            ok = prm(a, r0, 0) == prm(a, r1, 0) && prm(a, r0, 1) == prm(a, r1, 1) &&
+                 prm(a, r0, 2) == prm(a, r1, 2) && prm(a, r1, 3) == node;
+        }
+        if (!__all_sync(0xffffffffu, ok)) return;
+        if (!(nodes[0] != nodes[1] && nodes[1] != nodes[2] && nodes[0] != nodes[2])) return;
+        const float bv = a.b1map[v];
+        if (!isfinite(bv)) return;
+        lagrange3(nodes, bv, qw);
+        nq = 3;
+    }
+    // Taylor coefficients along log T1 (rows) and log T2 (columns); the
+    // node offsets as logs of ratios, exact to rounding
+    const long long bb = b * a.natoms;
+    const float hum = logf(prm(a, bb + st[0][1], 0) / T1c), hup = logf(prm(a, bb + st[2][1], 0) / T1c);
+    const float hvm = logf(prm(a, bb + st[1][0], 1) / T2c), hvp = logf(prm(a, bb + st[1][2], 1) / T2c);
+    const Quad cu = quad_coeffs(hum, hup), cv = quad_coeffs(hvm, hvp);
+    // the stencil rows of T1 node 1 per block and T2 node; T1 nodes 0 and 2
+    // are the rows before and after
+    const float2 *rows[3][3];
+#pragma unroll
+    for (int q = 0; q < 3; q++)
+#pragma unroll
+        for (int c = 0; c < 3; c++) rows[q][c] = a.atoms + (qbase[q] + st[1][c]) * a.atom_stride;
+    const long long rs = a.atom_stride;
+    const float2 *xv = a.img + v * a.img_stride;
+
+    // Hermitian Gram matrix of the Taylor basis, sum_t conj(m_r) m_c: real
+    // part G (upper triangle), imaginary part Gi (strict upper triangle, zero
+    // for purely imaginary atoms); inner products with the voxel,
+    // sum_t conj(m_r) x = (pr, pi)
+    float G[45], Gi[IMAG ? 1 : 45], pr[9], pi[9];
+#pragma unroll
+    for (int i = 0; i < 45; i++) G[i] = 0.f;
+#pragma unroll
+    for (int i = 0; i < (IMAG ? 1 : 45); i++) Gi[i] = 0.f;
+#pragma unroll
+    for (int i = 0; i < 9; i++) pr[i] = pi[i] = 0.f;
+
+    // the stencil of one part (real or imaginary) at one sample in the
+    // Taylor basis: m[p * 3 + q] multiplies U^p V^q
+    auto taylor = [&](const float s[3][3], float m[9]) {
+        float m1[3][3];  // [T1 power][T2 node]
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            const float dp = s[2][c] - s[1][c], dm = s[0][c] - s[1][c];
+            m1[0][c] = s[1][c];
+            m1[1][c] = fmaf(cu.b1, dp, cu.b2 * dm);
+            m1[2][c] = fmaf(cu.a1, dp, cu.a2 * dm);
+        }
+#pragma unroll
+        for (int p = 0; p < 3; p++) {
+            const float dp = m1[p][2] - m1[p][1], dm = m1[p][0] - m1[p][1];
+            m[p * 3] = m1[p][1];
+            m[p * 3 + 1] = fmaf(cv.b1, dp, cv.b2 * dm);
+            m[p * 3 + 2] = fmaf(cv.a1, dp, cv.a2 * dm);
+        }
+    };
+
+    for (int t = lane; t < a.T; t += 32) {
+        const float2 x = xv[t];
+        float sr[3][3], si[3][3];
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                float accr = 0.f, acci = 0.f;
+#pragma unroll
+                for (int q = 0; q < 3; q++) {
+                    if (q < nq) {
+                        const float2 d = __ldg(rows[q][c] + (i - 1) * rs + t);
+                        if (!IMAG) accr = fmaf(qw[q], d.x, accr);
+                        acci = fmaf(qw[q], d.y, acci);
+                    }
+                }
+                sr[i][c] = accr;
+                si[i][c] = acci;
+            }
+        float mi[9];
+        taylor(si, mi);
+        if (IMAG) {
+#pragma unroll
+            for (int r = 0; r < 9; r++) {
+#pragma unroll
+                for (int c = 0; c < 9; c++)
+                    if (c >= r) G[tri(r, c)] = fmaf(mi[r], mi[c], G[tri(r, c)]);
+                // conj(i m) x = (m xi, -m xr)
+                pr[r] = fmaf(mi[r], x.y, pr[r]);
+                pi[r] = fmaf(-mi[r], x.x, pi[r]);
+            }
+        } else {
+            float mr[9];
+            taylor(sr, mr);
+#pragma unroll
+            for (int r = 0; r < 9; r++) {
+#pragma unroll
+                for (int c = 0; c < 9; c++) {
+                    if (c >= r) G[tri(r, c)] = fmaf(mr[r], mr[c], fmaf(mi[r], mi[c], G[tri(r, c)]));
+                    if (c > r) Gi[tri(r, c)] = fmaf(mr[r], mi[c], fmaf(-mi[r], mr[c], Gi[tri(r, c)]));
+                }
+                pr[r] = fmaf(mr[r], x.x, fmaf(mi[r], x.y, pr[r]));
+                pi[r] = fmaf(mr[r], x.y, fmaf(-mi[r], x.x, pi[r]));
+            }
+        }
+    }
+    // warp sums (every lane ends with the totals)
+#pragma unroll
+    for (int i = 0; i < 45; i++)
+#pragma unroll
+        for (int o = 16; o; o >>= 1) G[i] += __shfl_xor_sync(0xffffffffu, G[i], o);
+    if (!IMAG) {
+#pragma unroll
+        for (int i = 0; i < (IMAG ? 1 : 45); i++)
+#pragma unroll
+            for (int o = 16; o; o >>= 1) Gi[i] += __shfl_xor_sync(0xffffffffu, Gi[i], o);
+    }
+#pragma unroll
+    for (int i = 0; i < 9; i++)
+#pragma unroll
+        for (int o = 16; o; o >>= 1) {
+            pr[i] += __shfl_xor_sync(0xffffffffu, pr[i], o);
+            pi[i] += __shfl_xor_sync(0xffffffffu, pi[i], o);
+        }
+    if (lane) return;
+
+    // Gauss-Newton with variable projection on the surrogate s(U, V) =
+    // sum m_pq U^p V^q, ds/dU, ds/dV; the point may leave the stencil by
+    // half its extent on each side (a match more than a grid step from the
+    // fit: the quadratic extrapolates, still nearer than the grid point)
+    const float lu = 0.5f * (fmaxf(hum, hup) - fminf(hum, hup)), lv = 0.5f * (fmaxf(hvm, hvp) - fminf(hvm, hvp));
+    const float ulo = 1.5f * fminf(hum, hup), uhi = 1.5f * fmaxf(hum, hup);
+    const float vlo = 1.5f * fminf(hvm, hvp), vhi = 1.5f * fmaxf(hvm, hvp);
+    float U = 0.f, V = 0.f;
+    for (int it = 0; it < kSolveIters; it++) {
+        const float Up[3] = {1.f, U, U * U}, Vp[3] = {1.f, V, V * V};
+        const float dU[3] = {0.f, 1.f, 2.f * U}, dV[3] = {0.f, 1.f, 2.f * V};
+        float c0[9], c1[9], c2[9];
+#pragma unroll
+        for (int p = 0; p < 3; p++)
+#pragma unroll
+            for (int q = 0; q < 3; q++) {
+                c0[p * 3 + q] = Up[p] * Vp[q];
+                c1[p * 3 + q] = dU[p] * Vp[q];
+                c2[p * 3 + q] = Up[p] * dV[q];
+            }
+        // G c for the three coefficient vectors, and Gi c0 (the imaginary
+        // parts of s^H dS/dU, s^H dS/dV; Gi is antisymmetric)
+        float g0[9], g1[9], g2[9], h0[9];
+#pragma unroll
+        for (int r = 0; r < 9; r++) {
+            float s0 = 0.f, s1 = 0.f, s2 = 0.f, z0 = 0.f;
+#pragma unroll
+            for (int c = 0; c < 9; c++) {
+                const float g = G[tri(r, c)];
+                s0 = fmaf(g, c0[c], s0);
+                s1 = fmaf(g, c1[c], s1);
+                s2 = fmaf(g, c2[c], s2);
+                if (!IMAG && c != r) z0 = fmaf(c < r ? -Gi[tri(r, c)] : Gi[tri(r, c)], c0[c], z0);
+            }
+            g0[r] = s0;
+            g1[r] = s1;
+            g2[r] = s2;
+            h0[r] = z0;
+        }
+        // s^H s, g_j = s^H J_j (complex), H_jk = Re J_j^H J_k, P = s^H x,
+        // Q_j = J_j^H x
+        float Ss = 0.f, G1 = 0.f, G2 = 0.f, G1i = 0.f, G2i = 0.f, H11 = 0.f, H12 = 0.f, H22 = 0.f;
+        float Pr = 0.f, Pi = 0.f, Q1r = 0.f, Q1i = 0.f, Q2r = 0.f, Q2i = 0.f;
+#pragma unroll
+        for (int r = 0; r < 9; r++) {
+            Ss = fmaf(c0[r], g0[r], Ss);
+            G1 = fmaf(c1[r], g0[r], G1);
+            G2 = fmaf(c2[r], g0[r], G2);
+            // c0^T Gi c_j = -(c_j^T Gi c0)
+            G1i = fmaf(-c1[r], h0[r], G1i);
+            G2i = fmaf(-c2[r], h0[r], G2i);
+            H11 = fmaf(c1[r], g1[r], H11);
+            H12 = fmaf(c1[r], g2[r], H12);
+            H22 = fmaf(c2[r], g2[r], H22);
+            Pr = fmaf(c0[r], pr[r], Pr);
+            Pi = fmaf(c0[r], pi[r], Pi);
+            Q1r = fmaf(c1[r], pr[r], Q1r);
+            Q1i = fmaf(c1[r], pi[r], Q1i);
+            Q2r = fmaf(c2[r], pr[r], Q2r);
+            Q2i = fmaf(c2[r], pi[r], Q2i);
+        }
+        if (!(Ss > 0.f)) break;
+        // rho = P / Ss; A_jk = |rho|^2 (H_jk - Re(conj(g_j) g_k) / Ss);
+        // b_j = Re(conj(rho) (Q_j - conj(g_j) P / Ss)); delta = A^-1 b
+        const float rr = Pr / Ss, ri = Pi / Ss, rho2 = rr * rr + ri * ri;
+        const float A11 = rho2 * (H11 - (G1 * G1 + G1i * G1i) / Ss);
+        const float A12 = rho2 * (H12 - (G1 * G2 + G1i * G2i) / Ss);
+        const float A22 = rho2 * (H22 - (G2 * G2 + G2i * G2i) / Ss);
+        // conj(g) P = (gr Pr + gi Pi, gr Pi - gi Pr)
+        const float e1r = Q1r - (G1 * Pr + G1i * Pi) / Ss, e1i = Q1i - (G1 * Pi - G1i * Pr) / Ss;
+        const float e2r = Q2r - (G2 * Pr + G2i * Pi) / Ss, e2i = Q2i - (G2 * Pi - G2i * Pr) / Ss;
+        const float b1 = rr * e1r + ri * e1i, b2 = rr * e2r + ri * e2i;
+        const float det = A11 * A22 - A12 * A12;
+        if (!(det > 0.f) || !(A11 > 0.f) || !isfinite(det)) break;
+        float d1 = (A22 * b1 - A12 * b2) / det, d2 = (A11 * b2 - A12 * b1) / det;
+        if (!isfinite(d1) || !isfinite(d2)) break;
+        // at most half the stencil's width per iteration
+        d1 = fminf(fmaxf(d1, -lu), lu);
+        d2 = fminf(fmaxf(d2, -lv), lv);
+        U = fminf(fmaxf(U + d1, ulo), uhi);
+        V = fminf(fmaxf(V + d2, vlo), vhi);
+    }
+    const float T1 = T1c * expf(U), T2 = T2c * expf(V);
+    if (!isfinite(T1) || !isfinite(T2) || !(T2 > 0.f) || !(T1 > T2 * (1.f + 1e-4f))) return;
+    mp[0] = T1;
+    mp[1] = T2;
+    if (a.count) atomicAdd(a.count, 1);
+}
+
+}  // namespace rstart
+}  // namespace snapmrf
+
+using namespace snapmrf;
+
+extern "C" int snapmrf_refine_start(float *d_maps, int nmaps, const int64_t *d_index, const float *d_atoms,
+                                    const float *d_params, int nparams, size_t nreps, size_t NATOMS,
+                                    size_t natoms, const float *img, size_t img_stride, size_t nvoxels,
+                                    const float *d_b1map, unsigned flags, int *d_count, void *stream) {
+    cudaStream_t st = (cudaStream_t)stream;
+    if (!d_maps || !d_index || !d_atoms || !d_params || !img)
+        SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "refine_start: null pointer");
+    if (nmaps < 2 || nparams < 3 || (d_b1map && nparams < 4) || nreps == 0 || natoms == 0 || NATOMS % natoms)
+        SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "refine_start: bad sizes");
+    if (flags & ~SNAPMRF_START_IMAG_ATOMS) SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "refine_start: unknown flags");
+    if (img_stride == 0) img_stride = nreps;
+    if (img_stride < nreps) SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "refine_start: img_stride < nreps");
+    if (nreps > 0x7fffffff || NATOMS > (size_t)1 << 40 || nvoxels > ((size_t)1 << 31) * rstart::kWarps)
+        SNAPMRF_FAIL(SNAPMRF_ERR_UNSUPPORTED, "refine_start: sizes beyond the supported range");
+    if (nvoxels == 0) return SNAPMRF_OK;
+    rstart::Args a;
+    a.maps = d_maps;
+    a.nmaps = nmaps;
+    a.index = d_index;
+    a.atoms = reinterpret_cast<const float2 *>(d_atoms);
+    a.atom_stride = (long long)nreps;
+    a.params = d_params;
+    a.nparams = nparams;
+    a.NATOMS = (long long)NATOMS;
+    a.natoms = (long long)natoms;
+    a.img = reinterpret_cast<const float2 *>(img);
+    a.img_stride = (long long)img_stride;
+    a.T = (int)nreps;
+    a.nvox = (long long)nvoxels;
+    a.b1map = d_b1map;
+    a.count = d_count;
+    const unsigned grid = (unsigned)((nvoxels + rstart::kWarps - 1) / rstart::kWarps);
+    if (flags & SNAPMRF_START_IMAG_ATOMS)
+        rstart::start_kernel<true><<<grid, rstart::kWarps * 32, 0, st>>>(a);
+    else
+        rstart::start_kernel<false><<<grid, rstart::kWarps * 32, 0, st>>>(a);
+    SNAPMRF_LAUNCH_CHECK();
+    return SNAPMRF_OK;
+}
