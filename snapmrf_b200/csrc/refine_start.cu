@@ -50,7 +50,16 @@ struct Args {
     long long nvox;
     const float *b1map;
     int *count;
+    float *sys;  // [kSysRows (+45 complex)][nvox]: the accumulated system per voxel
 };
+
+// Rows of the per-voxel system handed from the accumulation to the solve:
+// the matched (T1, T2) (T1 NaN: leave the voxel), the stencil's node offsets
+// in log T1 and log T2, the inner products with the voxel (real and
+// imaginary parts), the real part of the Gram matrix (packed upper triangle)
+// and, for complex atoms, its imaginary part.
+constexpr int kRowT1 = 0, kRowT2 = 1, kRowH = 2, kRowPr = 6, kRowPi = 15, kRowG = 24, kRowGi = 69;
+constexpr int kSysRows = 69, kSysRowsComplex = 114;
 
 __device__ __forceinline__ float prm(const Args &a, long long r, int c) { return __ldg(a.params + r * a.nparams + c); }
 
@@ -145,20 +154,25 @@ __device__ __host__ __forceinline__ constexpr int tri(int i, int j) {
     return i <= j ? i * 9 - i * (i - 1) / 2 + (j - i) : j * 9 - j * (j - 1) / 2 + (i - j);
 }
 
+// One warp per voxel: the stencil, then the system of its surrogate
+// accumulated over the time points and written to a.sys.
 template <bool IMAG>
-__global__ void __launch_bounds__(kWarps * 32) start_kernel(const __grid_constant__ Args a) {
+__global__ void __launch_bounds__(kWarps * 32) accumulate_kernel(const __grid_constant__ Args a) {
     const int lane = threadIdx.x & 31;
     const long long v = (long long)blockIdx.x * kWarps + (threadIdx.x >> 5);
     if (v >= a.nvox) return;  // whole warps leave together
+    auto leave = [&]() {
+        if (lane == 0) a.sys[kRowT1 * a.nvox + v] = __int_as_float(0x7fc00000);
+    };
     const long long k = a.index[v];
-    if (k < 0 || k >= a.NATOMS) return;
-    float *mp = a.maps + v * a.nmaps;
+    if (k < 0 || k >= a.NATOMS) return leave();
+    const float *mp = a.maps + v * a.nmaps;
     const long long b = k / a.natoms, j = k - b * a.natoms;
     const float T1c = prm(a, k, 0), T2c = prm(a, k, 1);
     // the maps must still hold the matched grid point
-    if (mp[0] != T1c || mp[1] != T2c || !(T1c > T2c) || !(T2c > 0.f)) return;
+    if (mp[0] != T1c || mp[1] != T2c || !(T1c > T2c) || !(T2c > 0.f)) return leave();
     long long st[3][3];
-    if (!find_stencil(a, b * a.natoms, j, st)) return;
+    if (!find_stencil(a, b * a.natoms, j, st)) return leave();
     // B1 blocks and their weights at the voxel's B1
     const long long nb = a.NATOMS / a.natoms;
     int nq = 1;
@@ -194,10 +208,10 @@ __global__ void __launch_bounds__(kWarps * 32) start_kernel(const __grid_constan
             ok = prm(a, r0, 0) == prm(a, r1, 0) && prm(a, r0, 1) == prm(a, r1, 1) &&
                  prm(a, r0, 2) == prm(a, r1, 2) && prm(a, r1, 3) == node;
         }
-        if (!__all_sync(0xffffffffu, ok)) return;
-        if (!(nodes[0] != nodes[1] && nodes[1] != nodes[2] && nodes[0] != nodes[2])) return;
+        if (!__all_sync(0xffffffffu, ok)) return leave();
+        if (!(nodes[0] != nodes[1] && nodes[1] != nodes[2] && nodes[0] != nodes[2])) return leave();
         const float bv = a.b1map[v];
-        if (!isfinite(bv)) return;
+        if (!isfinite(bv)) return leave();
         lagrange3(nodes, bv, qw);
         nq = 3;
     }
@@ -260,9 +274,14 @@ __global__ void __launch_bounds__(kWarps * 32) start_kernel(const __grid_constan
 #pragma unroll
                 for (int q = 0; q < 3; q++) {
                     if (q < nq) {
-                        const float2 d = __ldg(rows[q][c] + (i - 1) * rs + t);
-                        if (!IMAG) accr = fmaf(qw[q], d.x, accr);
-                        acci = fmaf(qw[q], d.y, acci);
+                        const float2 *pd = rows[q][c] + (i - 1) * rs + t;
+                        if (IMAG) {
+                            acci = fmaf(qw[q], __ldg(reinterpret_cast<const float *>(pd) + 1), acci);
+                        } else {
+                            const float2 d = __ldg(pd);
+                            accr = fmaf(qw[q], d.x, accr);
+                            acci = fmaf(qw[q], d.y, acci);
+                        }
                     }
                 }
                 sr[i][c] = accr;
@@ -313,12 +332,52 @@ __global__ void __launch_bounds__(kWarps * 32) start_kernel(const __grid_constan
             pr[i] += __shfl_xor_sync(0xffffffffu, pr[i], o);
             pi[i] += __shfl_xor_sync(0xffffffffu, pi[i], o);
         }
-    if (lane) return;
+    // the system to the scratch rows, each value by one lane
+    float *sys = a.sys + v;
+    const long long n = a.nvox;
+    const float hv[6] = {T1c, T2c, hum, hup, hvm, hvp};
+#pragma unroll
+    for (int r = 0; r < 6; r++)
+        if ((r & 31) == lane) sys[r * n] = hv[r];
+#pragma unroll
+    for (int r = 0; r < 9; r++) {
+        if (((kRowPr + r) & 31) == lane) sys[(kRowPr + r) * n] = pr[r];
+        if (((kRowPi + r) & 31) == lane) sys[(kRowPi + r) * n] = pi[r];
+    }
+#pragma unroll
+    for (int r = 0; r < 45; r++) {
+        if (((kRowG + r) & 31) == lane) sys[(kRowG + r) * n] = G[r];
+        if (!IMAG && ((kRowGi + r) & 31) == lane) sys[(kRowGi + r) * n] = Gi[r];
+    }
+}
 
-    // Gauss-Newton with variable projection on the surrogate s(U, V) =
-    // sum m_pq U^p V^q, ds/dU, ds/dV; the point may leave the stencil by
-    // half its extent on each side (a match more than a grid step from the
-    // fit: the quadratic extrapolates, still nearer than the grid point)
+// One thread per voxel: Gauss-Newton with variable projection on the
+// surrogate s(U, V) = sum m_pq U^p V^q, ds/dU, ds/dV, from the matched grid
+// point; the point may leave the stencil by half its extent on each side (a
+// match more than a grid step from the fit: the quadratic extrapolates,
+// still nearer than the grid point).
+template <bool IMAG>
+__global__ void __launch_bounds__(128) solve_kernel(const __grid_constant__ Args a) {
+    const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= a.nvox) return;
+    const float *sys = a.sys + v;
+    const long long n = a.nvox;
+    const float T1c = sys[kRowT1 * n];
+    if (isnan(T1c)) return;
+    const float T2c = sys[kRowT2 * n];
+    const float hum = sys[(kRowH + 0) * n], hup = sys[(kRowH + 1) * n];
+    const float hvm = sys[(kRowH + 2) * n], hvp = sys[(kRowH + 3) * n];
+    float G[45], Gi[IMAG ? 1 : 45], pr[9], pi[9];
+#pragma unroll
+    for (int r = 0; r < 45; r++) {
+        G[r] = sys[(kRowG + r) * n];
+        if (!IMAG) Gi[r] = sys[(kRowGi + r) * n];
+    }
+#pragma unroll
+    for (int r = 0; r < 9; r++) {
+        pr[r] = sys[(kRowPr + r) * n];
+        pi[r] = sys[(kRowPi + r) * n];
+    }
     const float lu = 0.5f * (fmaxf(hum, hup) - fminf(hum, hup)), lv = 0.5f * (fmaxf(hvm, hvp) - fminf(hvm, hvp));
     const float ulo = 1.5f * fminf(hum, hup), uhi = 1.5f * fmaxf(hum, hup);
     const float vlo = 1.5f * fminf(hvm, hvp), vhi = 1.5f * fmaxf(hvm, hvp);
@@ -399,6 +458,7 @@ __global__ void __launch_bounds__(kWarps * 32) start_kernel(const __grid_constan
     }
     const float T1 = T1c * expf(U), T2 = T2c * expf(V);
     if (!isfinite(T1) || !isfinite(T2) || !(T2 > 0.f) || !(T1 > T2 * (1.f + 1e-4f))) return;
+    float *mp = a.maps + v * a.nmaps;
     mp[0] = T1;
     mp[1] = T2;
     if (a.count) atomicAdd(a.count, 1);
@@ -421,7 +481,7 @@ extern "C" int snapmrf_refine_start(float *d_maps, int nmaps, const int64_t *d_i
     if (flags & ~SNAPMRF_START_IMAG_ATOMS) SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "refine_start: unknown flags");
     if (img_stride == 0) img_stride = nreps;
     if (img_stride < nreps) SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "refine_start: img_stride < nreps");
-    if (nreps > 0x7fffffff || NATOMS > (size_t)1 << 40 || nvoxels > ((size_t)1 << 31) * rstart::kWarps)
+    if (nreps > 0x7fffffff || NATOMS > (size_t)1 << 40 || nvoxels > ((size_t)1 << 31) - 1)
         SNAPMRF_FAIL(SNAPMRF_ERR_UNSUPPORTED, "refine_start: sizes beyond the supported range");
     if (nvoxels == 0) return SNAPMRF_OK;
     rstart::Args a;
@@ -440,11 +500,21 @@ extern "C" int snapmrf_refine_start(float *d_maps, int nmaps, const int64_t *d_i
     a.nvox = (long long)nvoxels;
     a.b1map = d_b1map;
     a.count = d_count;
+    const bool imag = flags & SNAPMRF_START_IMAG_ATOMS;
+    DeviceScratch sys;
+    SNAPMRF_CUDA(sys.alloc(nvoxels * (imag ? rstart::kSysRows : rstart::kSysRowsComplex) * sizeof(float), st));
+    a.sys = sys.as<float>();
     const unsigned grid = (unsigned)((nvoxels + rstart::kWarps - 1) / rstart::kWarps);
-    if (flags & SNAPMRF_START_IMAG_ATOMS)
-        rstart::start_kernel<true><<<grid, rstart::kWarps * 32, 0, st>>>(a);
-    else
-        rstart::start_kernel<false><<<grid, rstart::kWarps * 32, 0, st>>>(a);
+    const unsigned grid2 = (unsigned)((nvoxels + 127) / 128);
+    if (imag) {
+        rstart::accumulate_kernel<true><<<grid, rstart::kWarps * 32, 0, st>>>(a);
+        SNAPMRF_LAUNCH_CHECK();
+        rstart::solve_kernel<true><<<grid2, 128, 0, st>>>(a);
+    } else {
+        rstart::accumulate_kernel<false><<<grid, rstart::kWarps * 32, 0, st>>>(a);
+        SNAPMRF_LAUNCH_CHECK();
+        rstart::solve_kernel<false><<<grid2, 128, 0, st>>>(a);
+    }
     SNAPMRF_LAUNCH_CHECK();
     return SNAPMRF_OK;
 }
