@@ -28,12 +28,16 @@
 
 #include <cmath>
 #include <cstdint>
+#include <type_traits>
 
 namespace snapmrf {
 namespace rstart {
 
 constexpr int kWarps = 4;       // voxels per block
 constexpr int kSolveIters = 10;  // Gauss-Newton iterations on the surrogate
+// shared-memory slots of staged samples per warp (imaginary atoms, complex)
+template <bool IMAG>
+__host__ __device__ constexpr int stages() { return IMAG ? 5 : 3; }
 
 struct Args {
     float *maps;
@@ -154,6 +158,24 @@ __device__ __host__ __forceinline__ constexpr int tri(int i, int j) {
     return i <= j ? i * 9 - i * (i - 1) / 2 + (j - i) : j * 9 - j * (j - 1) / 2 + (i - j);
 }
 
+// cp.async (Ampere-style asynchronous global -> shared copies, cached in
+// L1 for the 4- and 8-byte forms) and its commit / wait groups.
+__device__ __forceinline__ void cp_async4(void *smem, const void *g) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"((unsigned)__cvta_generic_to_shared(smem)),
+                 "l"(g)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async8(void *smem, const void *g) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"((unsigned)__cvta_generic_to_shared(smem)),
+                 "l"(g)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
 // One warp per voxel: the stencil, then the system of its surrogate
 // accumulated over the time points and written to a.sys.
 template <bool IMAG>
@@ -263,8 +285,49 @@ __global__ void __launch_bounds__(kWarps * 32) accumulate_kernel(const __grid_co
         }
     };
 
-    for (int t = lane; t < a.T; t += 32) {
-        const float2 x = xv[t];
+    // Staging: each lane copies its own samples of the stencil rows and of
+    // the voxel into this warp's ring of kStages shared-memory slots with
+    // cp.async, kStages - 1 chunks of 32 samples ahead of the arithmetic, and
+    // reads back only what it copied itself.  The loads in flight hold no
+    // registers, so many more of them are outstanding per SM than register
+    // prefetching would allow.
+    using V = typename std::conditional<IMAG, float, float2>::type;
+    constexpr int kStages = stages<IMAG>();
+    extern __shared__ __align__(16) unsigned char rs_smem[];
+    V *sa = reinterpret_cast<V *>(rs_smem) + (size_t)(threadIdx.x >> 5) * kStages * 27 * 32;
+    float2 *sx = reinterpret_cast<float2 *>(reinterpret_cast<V *>(rs_smem) + (size_t)kWarps * kStages * 27 * 32) +
+                 (threadIdx.x >> 5) * kStages * 32;
+    const int nch = (a.T + 31) / 32;
+    auto issue = [&](int kc) {
+        const int t = kc * 32 + lane, slot = kc % kStages;
+        if (t < a.T) {
+#pragma unroll
+            for (int q = 0; q < 3; q++)
+                if (q < nq)
+#pragma unroll
+                    for (int i = 0; i < 3; i++)
+#pragma unroll
+                        for (int c = 0; c < 3; c++) {
+                            const float2 *g = rows[q][c] + (i - 1) * rs + t;
+                            V *d = sa + (slot * 27 + q * 9 + i * 3 + c) * 32 + lane;
+                            if (IMAG)
+                                cp_async4(d, reinterpret_cast<const float *>(g) + 1);
+                            else
+                                cp_async8(d, g);
+                        }
+            cp_async8(sx + slot * 32 + lane, xv + t);
+        }
+        cp_async_commit();
+    };
+#pragma unroll
+    for (int kc = 0; kc < kStages - 1; kc++) issue(kc);
+
+    for (int kc = 0; kc < nch; kc++) {
+        issue(kc + kStages - 1);  // (an empty group past the end)
+        cp_async_wait<kStages - 1>();
+        const int t = kc * 32 + lane, slot = kc % kStages;
+        if (t >= a.T) continue;
+        const float2 x = sx[slot * 32 + lane];
         float sr[3][3], si[3][3];
 #pragma unroll
         for (int i = 0; i < 3; i++)
@@ -274,11 +337,10 @@ __global__ void __launch_bounds__(kWarps * 32) accumulate_kernel(const __grid_co
 #pragma unroll
                 for (int q = 0; q < 3; q++) {
                     if (q < nq) {
-                        const float2 *pd = rows[q][c] + (i - 1) * rs + t;
-                        if (IMAG) {
-                            acci = fmaf(qw[q], __ldg(reinterpret_cast<const float *>(pd) + 1), acci);
+                        const V d = sa[(slot * 27 + q * 9 + i * 3 + c) * 32 + lane];
+                        if constexpr (IMAG) {
+                            acci = fmaf(qw[q], d, acci);
                         } else {
-                            const float2 d = __ldg(pd);
                             accr = fmaf(qw[q], d.x, accr);
                             acci = fmaf(qw[q], d.y, acci);
                         }
@@ -479,6 +541,8 @@ extern "C" int snapmrf_refine_start(float *d_maps, int nmaps, const int64_t *d_i
     if (nmaps < 2 || nparams < 3 || (d_b1map && nparams < 4) || nreps == 0 || natoms == 0 || NATOMS % natoms)
         SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "refine_start: bad sizes");
     if (flags & ~SNAPMRF_START_IMAG_ATOMS) SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "refine_start: unknown flags");
+    if ((reinterpret_cast<uintptr_t>(d_atoms) | reinterpret_cast<uintptr_t>(img)) % sizeof(float2))
+        SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "refine_start: atoms and image must be 8-byte aligned (complex)");
     if (img_stride == 0) img_stride = nreps;
     if (img_stride < nreps) SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "refine_start: img_stride < nreps");
     if (nreps > 0x7fffffff || NATOMS > (size_t)1 << 40 || nvoxels > ((size_t)1 << 31) - 1)
@@ -506,12 +570,19 @@ extern "C" int snapmrf_refine_start(float *d_maps, int nmaps, const int64_t *d_i
     a.sys = sys.as<float>();
     const unsigned grid = (unsigned)((nvoxels + rstart::kWarps - 1) / rstart::kWarps);
     const unsigned grid2 = (unsigned)((nvoxels + 127) / 128);
+    // staged samples: per warp kStages x 32 lanes x (27 atom values + the voxel)
+    const size_t smem = (size_t)rstart::kWarps * (imag ? rstart::stages<true>() : rstart::stages<false>()) * 32 *
+                        (27 * (imag ? sizeof(float) : sizeof(float2)) + sizeof(float2));
     if (imag) {
-        rstart::accumulate_kernel<true><<<grid, rstart::kWarps * 32, 0, st>>>(a);
+        SNAPMRF_CUDA(cudaFuncSetAttribute(rstart::accumulate_kernel<true>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        rstart::accumulate_kernel<true><<<grid, rstart::kWarps * 32, smem, st>>>(a);
         SNAPMRF_LAUNCH_CHECK();
         rstart::solve_kernel<true><<<grid2, 128, 0, st>>>(a);
     } else {
-        rstart::accumulate_kernel<false><<<grid, rstart::kWarps * 32, 0, st>>>(a);
+        SNAPMRF_CUDA(cudaFuncSetAttribute(rstart::accumulate_kernel<false>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        rstart::accumulate_kernel<false><<<grid, rstart::kWarps * 32, smem, st>>>(a);
         SNAPMRF_LAUNCH_CHECK();
         rstart::solve_kernel<false><<<grid2, 128, 0, st>>>(a);
     }
