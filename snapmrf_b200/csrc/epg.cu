@@ -54,6 +54,28 @@ __global__ void prepare_alpha_kernel(float *alpha, const float *fa, const float 
     }
 }
 
+// The 16-bit matching operand of the unit-norm atoms
+// (SNAPMRF_DICT_NORMALIZE_OPERAND), after the recursion: row a is
+// Im(atom a) * (1 / norm a), the product the recursion's kernel forms when
+// it normalises, rounded once to the operand's type, and zeros up to the
+// row pitch.  A pass of its own reads every finished atom at the full
+// bandwidth, where reading each atom back at the end of its own recursion
+// waited on one row at a time.  One warp per row (grid-stride over rows),
+// lanes over samples; norms as the recursion wrote them (sqrt of the sum of
+// squares).
+__global__ void pack_operand_kernel(EpgArgs a, long long natoms_total) {
+    const int lane = threadIdx.x & 31;
+    const long long warps = (long long)gridDim.x * (blockDim.x / 32);
+    for (long long at = blockIdx.x * (long long)(blockDim.x / 32) + (threadIdx.x >> 5); at < natoms_total;
+         at += warps) {
+        float inv = a.norms[at];
+        if (inv > 0.f) inv = 1.f / inv;
+        const float2 *row = a.atoms + at * a.nreps;
+        for (long long q = lane; q < a.packed_pitch; q += 32)
+            store_packed(a, at, q, q < a.nreps ? c_scale(row[q], inv).y : 0.f);
+    }
+}
+
 static int parse_echo(const char *s) {
     if (!s) return -1;
     if (!strcmp(s, "epg_ssfp")) return ECHO_SSFP;
@@ -362,6 +384,7 @@ static int dict_impl(float *d_atoms, const float *d_params, const float *h_mrf, 
     a.packed_pitch = 0;
     a.fine_first = 0;
     a.pack_normalized = pack_normalized ? 1 : 0;
+    a.operand_pass = 0;
     void *d_packed = opts ? opts->d_packed : nullptr;
 
     if (echo == ECHO_ROA) {
@@ -404,8 +427,27 @@ static int dict_impl(float *d_atoms, const float *d_params, const float *h_mrf, 
     if (grid.x > 0x7fffffffu) SNAPMRF_FAIL(SNAPMRF_ERR_UNSUPPORTED, "MRF_dict: grid too large");
     if (real_path) {
         const bool fold = !(flags & SNAPMRF_DICT_SEPARATE_RELAX);
+        // the unit-norm operand by a pass of its own over the finished atoms
+        // (norms in scratch when the caller wants none)
+        DeviceScratch norm_scratch;
+        if (pack_normalized) {
+            a.operand_pass = 1;
+            if (!a.norms) {
+                SNAPMRF_CUDA(norm_scratch.alloc((size_t)gen_blocks * natoms * sizeof(float), st));
+                a.norms = norm_scratch.as<float>();
+            }
+        }
         SNAPMRF_CUDA(echo == ECHO_FISP ? dispatch_real<ECHO_FISP>(a, S / 2, fold, grid, st)
                                        : dispatch_real<ECHO_SR>(a, S / 2, fold, grid, st));
+        if (pack_normalized) {
+            int dev = 0, sms = 0;
+            SNAPMRF_CUDA(cudaGetDevice(&dev));
+            SNAPMRF_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+            const long long total = (long long)gen_blocks * (long long)natoms;
+            const long long blocks = std::min<long long>((total + 7) / 8, (long long)sms * 16);
+            pack_operand_kernel<<<(unsigned)blocks, 256, 0, st>>>(a, total);
+            SNAPMRF_LAUNCH_CHECK();
+        }
     } else {
         SNAPMRF_CUDA(launch_epg(echo, a, S, grid, st));
     }

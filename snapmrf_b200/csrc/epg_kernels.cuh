@@ -42,6 +42,9 @@ struct EpgArgs {
     long long fine_first;
     // 16-bit operand of the unit-norm atoms while the atoms stay as generated
     int pack_normalized;
+    // 1: that operand is written by a separate pass over the finished atoms
+    // and their norms (pack_operand_kernel), not by the recursion's kernel
+    int operand_pass;
 };
 
 // Number of per-(atom, step) factors staged: E1/E2 at TE and at TR-TE, plus
@@ -651,18 +654,23 @@ __device__ __forceinline__ void epg_real_cta(const EpgArgs &a, const int L, cons
                 rl2_relax<P>(s, f.z, f.w, lane0);
             }
         }
-        __syncwarp();
-        if (active)
-            for (int q = gl; q < nch; q += L) {
-                const float2 o = sR[g * kRealReadoutStride + q];
-                out[t0 + q] = o;
-                if (a.packed && !a.normalize && !a.pack_normalized) store_packed(a, gatom, t0 + q, o.y);
+        // the chunk's samples, one atom per 32 threads: each store covers 32
+        // consecutive samples of one atom row (256 contiguous bytes)
+        __syncthreads();
+        for (int ga = tid / kRealChunk; ga < apc; ga += kRealThreads / kRealChunk) {
+            const int q = tid % kRealChunk;
+            if (q < nch && atom0 + ga < a.natoms) {
+                const float2 o = sR[ga * kRealReadoutStride + q];
+                const long long at = blk * a.natoms + atom0 + ga;
+                a.atoms[at * nreps + t0 + q] = o;
+                if (a.packed && !a.normalize && !a.pack_normalized) store_packed(a, at, t0 + q, o.y);
             }
+        }
     }
     if (a.normalize || a.norms || a.pack_normalized) {
         nrm = __shfl_sync(0xffffffffu, nrm, 0, L);
         if (a.norms && lane0 && active) a.norms[gatom] = sqrtf(nrm);
-        if (a.normalize || a.pack_normalized) {
+        if (a.normalize || (a.pack_normalized && !a.operand_pass)) {
             __syncwarp();
             float inv = nrm;
             if (inv > 0.f) inv = 1.f / sqrtf(inv);
@@ -681,7 +689,7 @@ __device__ __forceinline__ void epg_real_cta(const EpgArgs &a, const int L, cons
             }
         }
     }
-    if (a.packed && active)
+    if (a.packed && active && !a.operand_pass)
         for (long long q = nreps + gl; q < a.packed_pitch; q += L) store_packed(a, gatom, q, 0.f);
 }
 
