@@ -66,13 +66,52 @@ __global__ void prepare_alpha_kernel(float *alpha, const float *fa, const float 
 __global__ void pack_operand_kernel(EpgArgs a, long long natoms_total) {
     const int lane = threadIdx.x & 31;
     const long long warps = (long long)gridDim.x * (blockDim.x / 32);
+    // eight samples per lane and step: four 16-byte loads of the atom row and
+    // one 16-byte store of the operand where the row allows it
+    const bool vec = a.nreps % 2 == 0 && reinterpret_cast<uintptr_t>(a.atoms) % 16 == 0 &&
+                     reinterpret_cast<uintptr_t>(a.packed) % 16 == 0 && a.packed_pitch % 8 == 0;
+    const long long groups = (a.packed_pitch + 7) / 8;
     for (long long at = blockIdx.x * (long long)(blockDim.x / 32) + (threadIdx.x >> 5); at < natoms_total;
          at += warps) {
         float inv = a.norms[at];
         if (inv > 0.f) inv = 1.f / inv;
         const float2 *row = a.atoms + at * a.nreps;
-        for (long long q = lane; q < a.packed_pitch; q += 32)
-            store_packed(a, at, q, q < a.nreps ? c_scale(row[q], inv).y : 0.f);
+        for (long long gq = lane; gq < groups; gq += 32) {
+            const long long q0 = gq * 8;
+            float v[8];
+            if (vec && q0 + 8 <= a.nreps) {
+                const float4 *r4 = reinterpret_cast<const float4 *>(row + q0);
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    const float4 x = __ldg(r4 + k);
+                    v[2 * k] = c_scale(make_float2(x.x, x.y), inv).y;
+                    v[2 * k + 1] = c_scale(make_float2(x.z, x.w), inv).y;
+                }
+            } else {
+#pragma unroll
+                for (int k = 0; k < 8; k++) v[k] = q0 + k < a.nreps ? c_scale(row[q0 + k], inv).y : 0.f;
+            }
+            if (vec) {
+                uint4 w;
+                uint32_t *wp = reinterpret_cast<uint32_t *>(&w);
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    if (a.packed_half) {
+                        const __half2 h = __floats2half2_rn(v[2 * k], v[2 * k + 1]);
+                        wp[k] = *reinterpret_cast<const uint32_t *>(&h);
+                    } else {
+                        const __nv_bfloat162 h = __floats2bfloat162_rn(v[2 * k], v[2 * k + 1]);
+                        wp[k] = *reinterpret_cast<const uint32_t *>(&h);
+                    }
+                }
+                reinterpret_cast<uint4 *>(static_cast<unsigned char *>(a.packed) +
+                                          (at * a.packed_pitch + q0) * 2)[0] = w;
+            } else {
+#pragma unroll
+                for (int k = 0; k < 8; k++)
+                    if (q0 + k < a.packed_pitch) store_packed(a, at, q0 + k, v[k]);
+            }
+        }
     }
 }
 

@@ -654,18 +654,13 @@ __device__ __forceinline__ void epg_real_cta(const EpgArgs &a, const int L, cons
                 rl2_relax<P>(s, f.z, f.w, lane0);
             }
         }
-        // the chunk's samples, one atom per 32 threads: each store covers 32
-        // consecutive samples of one atom row (256 contiguous bytes)
-        __syncthreads();
-        for (int ga = tid / kRealChunk; ga < apc; ga += kRealThreads / kRealChunk) {
-            const int q = tid % kRealChunk;
-            if (q < nch && atom0 + ga < a.natoms) {
-                const float2 o = sR[ga * kRealReadoutStride + q];
-                const long long at = blk * a.natoms + atom0 + ga;
-                a.atoms[at * nreps + t0 + q] = o;
-                if (a.packed && !a.normalize && !a.pack_normalized) store_packed(a, at, t0 + q, o.y);
+        __syncwarp();
+        if (active)
+            for (int q = gl; q < nch; q += L) {
+                const float2 o = sR[g * kRealReadoutStride + q];
+                out[t0 + q] = o;
+                if (a.packed && !a.normalize && !a.pack_normalized) store_packed(a, gatom, t0 + q, o.y);
             }
-        }
     }
     if (a.normalize || a.norms || a.pack_normalized) {
         nrm = __shfl_sync(0xffffffffu, nrm, 0, L);
