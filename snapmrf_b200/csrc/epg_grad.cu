@@ -42,6 +42,11 @@ constexpr int kThreads = 128;
 #endif
 constexpr int kGnThreads = SNAPMRF_GN_THREADS;
 static_assert(kGnThreads % 32 == 0, "whole warps");
+
+// Voxels per CTA of gn_kernel with L lanes per voxel: 32 / L groups per warp
+// (a group never straddles two warps; with L not a power of two the last
+// 32 mod L lanes of each warp idle).
+__host__ __device__ constexpr int gn_voxels_per_cta(int L) { return (kGnThreads / 32) * (32 / L); }
 constexpr int kMaxS = 8;
 
 struct Schedule {
@@ -419,11 +424,15 @@ __device__ __forceinline__ void p_rf(Pair3<P> &x, float2 c, float2 s, float2 nS,
 // Shift of one packed stream.  States k >= w hold zeros: F- needs no mask
 // (F-[w-1] takes the zero of F-[w]), F+ takes F+[w-1] into slot w, which
 // keep[] (0 at slot w, 1 elsewhere) clears.
+// The neighbours' values come by shuffles from explicit lanes (src_up: the
+// lane below in the group, src_dn: the lane above), so a group may have any
+// width; a group's ends replace what they receive.
 template <int P>
-__device__ __forceinline__ void p_shift(Pair3<P> &x, int gl, int L, int w, const float2 *keep) {
+__device__ __forceinline__ void p_shift(Pair3<P> &x, int gl, int L, int w, const float2 *keep, int src_up,
+                                        int src_dn) {
     const unsigned full = 0xffffffffu;
-    const float up = __shfl_up_sync(full, x.p[P - 1].y, 1, L);
-    const float dn = __shfl_down_sync(full, x.m[0].x, 1, L);
+    const float up = __shfl_sync(full, x.p[P - 1].y, src_up);
+    const float dn = __shfl_sync(full, x.m[0].x, src_dn);
     const float old_m0 = x.m[0].x;
 #pragma unroll
     for (int i = P - 1; i >= 1; i--) x.p[i] = make_float2(x.p[i - 1].y, x.p[i].x);
@@ -455,12 +464,19 @@ constexpr int kGnChunk = 16;
 // final evaluation of PD and M0 at the current parameters.  L lanes per
 // voxel; a block of kGnThreads handles kGnThreads / L voxels in lockstep over
 // chunks of `chunk` steps.
+// (five pairs: at most 170 registers, so that three warps fit on an SM
+// sub-partition)
 template <int P, bool TANGENTS>
-__global__ void __launch_bounds__(kGnThreads) gn_kernel(GnArgs a, int chunk) {
+__global__ void __launch_bounds__(kGnThreads, P == 5 ? 12 * 32 / kGnThreads : 1) gn_kernel(GnArgs a, int chunk) {
     extern __shared__ __align__(16) unsigned char gn_smem[];
-    const int L = a.L, apc = kGnThreads / L;
-    const int tid = threadIdx.x, g = tid / L, gl = tid % L;
+    const int L = a.L, gpw = 32 / L, apc = gn_voxels_per_cta(L);
+    const int tid = threadIdx.x, lane = tid & 31, gl = lane % L;
+    // lanes past the warp's last whole group idle (their group index is
+    // clamped for the shared-memory reads; they write nothing)
+    const bool idle = lane >= gpw * L;
+    const int g = (tid >> 5) * gpw + min(lane / L, gpw - 1);
     const bool lane0 = gl == 0;
+    const int src_up = gl == 0 ? lane : lane - 1, src_dn = lane + 1 < 32 ? lane + 1 : lane;
     GnStep *sQ = reinterpret_cast<GnStep *>(gn_smem);              // [apc][chunk]
     float *sV = reinterpret_cast<float *>(sQ + apc * chunk);       // [apc][4]: T1, T2, B1, ok
     long long *sI = reinterpret_cast<long long *>(sV + apc * 4);  // [apc]: voxel or -1
@@ -498,7 +514,7 @@ __global__ void __launch_bounds__(kGnThreads) gn_kernel(GnArgs a, int chunk) {
     // a block without a usable voxel leaves at once (uniformly)
     if (!__syncthreads_or(tid < apc && sV[4 * tid + 3] != 0.f)) return;
     const long long v = sI[g];
-    const bool active = sV[4 * g + 3] != 0.f;
+    const bool active = !idle && sV[4 * g + 3] != 0.f;
     const int T = a.sch.nreps, w = a.w;
     const int k0 = gl * 2 * P;
     float2 keep[P];
@@ -574,10 +590,10 @@ __global__ void __launch_bounds__(kGnThreads) gn_kernel(GnArgs a, int chunk) {
                 }
             }
             if (a.shift) {
-                p_shift<P>(sv, gl, L, w, keep);
+                p_shift<P>(sv, gl, L, w, keep, src_up, src_dn);
                 if (TANGENTS) {
-                    p_shift<P>(s1, gl, L, w, keep);
-                    p_shift<P>(s2, gl, L, w, keep);
+                    p_shift<P>(s1, gl, L, w, keep, src_up, src_dn);
+                    p_shift<P>(s2, gl, L, w, keep, src_up, src_dn);
                 }
             }
             // relaxation over TR
@@ -669,8 +685,7 @@ constexpr int kGnMaxPairs = 7;  // 8 pairs with both tangents exceed 255 registe
 static void choose_pairs(int w, int *L, int *P) {
     if (const char *e = getenv("SNAPMRF_GN_LAYOUT")) {
         int l = 0, p = 0;
-        if (sscanf(e, "%d,%d", &l, &p) == 2 && l >= 1 && l <= 32 && (l & (l - 1)) == 0 && p >= 1 &&
-            p <= kGnMaxPairs && l * 2 * p >= w) {
+        if (sscanf(e, "%d,%d", &l, &p) == 2 && l >= 1 && l <= 32 && p >= 1 && p <= kGnMaxPairs && l * 2 * p >= w) {
             *L = l;
             *P = p;
             return;
@@ -1231,7 +1246,7 @@ extern "C" int snapmrf_refine_gn(float *d_maps, int nmaps, const float *img, siz
         cnt[0] = lst[1] + nvoxels;
         cnt[1] = cnt[0] + 1;
     }
-    const int apc = kGnThreads / L;
+    const int apc = gn_voxels_per_cta(L);
     // steps staged per chunk: at most kGnChunk, within 48 KB of shared memory
     auto smem_for = [&](int apc_, int *chunk_) {
         const size_t fixed = (size_t)apc_ * (4 * sizeof(float) + sizeof(long long));
@@ -1242,8 +1257,8 @@ extern "C" int snapmrf_refine_gn(float *d_maps, int nmaps, const float *img, siz
     const size_t smem = smem_for(apc, &chunk);
     dim3 grid((unsigned)((nvoxels + apc - 1) / apc));
     // The tail of the list: the bulk launch takes whole rounds of resident
-    // CTAs, the voxels past the last whole round go to a launch with four
-    // times the lanes per voxel (a quarter of the work per lane), so the last
+    // CTAs, the voxels past the last whole round go to a launch with 16 lanes
+    // per voxel (32 from 8 up; a quarter of the work per lane at L = 4), so the last
     // round does not run nearly empty (C1: 7,200 groups on 1,184 resident
     // CTAs were 6.08 rounds).  Same operations per state, same results.
     // SNAPMRF_GN_TAIL=0 turns it off.
@@ -1253,14 +1268,14 @@ extern "C" int snapmrf_refine_gn(float *d_maps, int nmaps, const float *img, siz
     dim3 grid_tail(0);
     {
         const char *e = getenv("SNAPMRF_GN_TAIL");
-        const int L_tail = std::min(32, 4 * L);
+        const int L_tail = L < 8 ? 16 : 32;
         P_tail = (nstates + 2 * L_tail - 1) / (2 * L_tail);
         int dev = 0, sms = 0, per_sm = 0;
         if (!(e && atoi(e) == 0) && L_tail > L && P_tail >= 1 && P_tail <= kGnMaxPairs &&
             cudaGetDevice(&dev) == cudaSuccess &&
             cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess &&
             gn_occupancy(P, smem, &per_sm) == cudaSuccess && sms > 0 && per_sm > 0) {
-            const int apc_tail = kGnThreads / L_tail;
+            const int apc_tail = gn_voxels_per_cta(L_tail);
             smem_tail = smem_for(apc_tail, &chunk_tail);
             a.part = 1;
             a.bulk_apc = apc;
