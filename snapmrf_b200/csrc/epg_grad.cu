@@ -680,7 +680,8 @@ __global__ void __launch_bounds__(kGnThreads, P == 5 ? 12 * 32 / kGnThreads : 1)
 constexpr int kGnMaxPairs = 7;  // 8 pairs with both tangents exceed 255 registers
 
 // Lanes per voxel and state pairs per lane for the refinement: the fewest
-// padded states, then the most pairs per lane (fewer shuffles per state).
+// padded states over power-of-two widths, then the most pairs per lane
+// (fewer shuffles per state), unless another width uses more of the lanes.
 // SNAPMRF_GN_LAYOUT="L,P" overrides the choice when it covers w states.
 static void choose_pairs(int w, int *L, int *P) {
     if (const char *e = getenv("SNAPMRF_GN_LAYOUT")) {
@@ -702,6 +703,19 @@ static void choose_pairs(int w, int *L, int *P) {
             bP = p;
         }
     }
+    // A group width that is not a power of two when it fills the warp's
+    // lanes with more useful states: useful fraction (32 / L) w / (32 * 2P).
+    // C1 (w = 50): 5 lanes x 5 pairs (6 voxels per warp, 94 %) against 4 x 7
+    // (8 voxels, 89 %): one pass 5.97 against 6.11 ms, the same maps.
+    auto useful = [&](int l, int p) { return (double)(32 / l) * w / (32.0 * 2 * p); };
+    double bu = useful(bL, bP);
+    for (int l = 1; l <= 32; l++)
+        for (int p = 1; p <= kGnMaxPairs; p++)
+            if (l * 2 * p >= w && useful(l, p) > bu + 1e-9) {
+                bu = useful(l, p);
+                bL = l;
+                bP = p;
+            }
     *L = bL;
     *P = bP;
 }
