@@ -225,11 +225,17 @@ def refine_gn_f64(theta, x, h_mrf, nstates: int = 101, echo: str = "epg_fisp", i
     return t1, t2, pd
 
 
+START_C, START_UM, START_UP, START_VM, START_VP, START_D = range(6)
+
+
 def _stencil_f64(params, base: int, n: int, j: int):
-    """3 x 3 stencil st[i][c] (T1 node i, T2 node c) of block-local row j in
-    the block starting at `base`, or None: the matched row's neighbours in
-    its T2 row, and the rows holding the same three T1 values in the adjacent
-    T2 rows of the table (trans_params order, src/functions.cu:355-391)."""
+    """Six-point stencil of block-local row j in the block starting at
+    `base`, or None: [matched, T1 below, T1 above, T2 below, T2 above,
+    diagonal] as block-local rows, and whether the diagonal is (T1 above, T2
+    above) (else T1 below, T2 below).  T1 neighbours are the adjacent table
+    rows in the matched T2 row; the T2 neighbours are the rows holding the
+    matched T1 in the adjacent T2 rows of the table (trans_params order,
+    src/functions.cu:355-391)."""
     P = params[base:base + n]
     t1, t2, b0 = P[:, 0], P[:, 1], P[:, 2]
     if j < 1 or j + 1 >= n:
@@ -239,10 +245,8 @@ def _stencil_f64(params, base: int, n: int, j: int):
         return None
     if not ((T1m < T1c < T1p) or (T1m > T1c > T1p)):
         return None
-    st = [[0] * 3 for _ in range(3)]
-    st[0][1], st[1][1], st[2][1] = j - 1, j, j + 1
-    T2n = []
-    for s, d in ((0, -1), (1, 1)):
+    T2n, rcs = [], []
+    for d in (-1, 1):
         r = j + 2 * d
         while 0 <= r < n and t2[r] == T2c and b0[r] == B0c:
             r += d
@@ -255,36 +259,37 @@ def _stencil_f64(params, base: int, n: int, j: int):
             r += d
         if not 0 <= r < n:
             return None
-        rc = r
-        if rc < 1 or rc + 1 >= n:
+        if not (t1[r] == T1c and t2[r] == T2r and b0[r] == B0c):
             return None
-        if not (t1[rc] == T1c and t2[rc] == T2r and b0[rc] == B0c):
-            return None
-        if not (t1[rc - 1] == T1m and t2[rc - 1] == T2r and b0[rc - 1] == B0c):
-            return None
-        if not (t1[rc + 1] == T1p and t2[rc + 1] == T2r and b0[rc + 1] == B0c):
-            return None
-        c = 2 if s else 0
-        st[0][c], st[1][c], st[2][c] = rc - 1, rc, rc + 1
         T2n.append(T2r)
+        rcs.append(r)
     if not (T2n[0] != T2n[1] and (T2n[0] < T2c) == (T2c < T2n[1])):
         return None
-    return st
+    st = [j, j - 1, j + 1, rcs[0], rcs[1], None]
+    du, dm = rcs[1] + 1, rcs[0] - 1
+    if du < n and t1[du] == T1p and t2[du] == T2n[1] and b0[du] == B0c:
+        st[START_D] = du
+        return st, True
+    if dm >= 0 and t1[dm] == T1m and t2[dm] == T2n[0] and b0[dm] == B0c:
+        st[START_D] = dm
+        return st, False
+    return None
 
 
 def refine_start_f64(maps, index, atoms, params, img, natoms: int, b1map=None, iterations: int = 10):
     """Sub-grid start of the refinement (snapmrf_refine_start) in FP64.  No
     counterpart in the reference; this is the checker's statement of it.
 
-    Per voxel: the matched atom's 3 x 3 (T1, T2) stencil (_stencil_f64);
-    with a B1 map, the stencil of the three B1 blocks around the match
-    (clamped to the table) interpolated quadratically (Lagrange) to the
-    voxel's B1.  In (U, V) = (log T1 / T1c, log T2 / T2c) the nine signals
-    give the biquadratic surrogate s = sum_pq m_pq U^p V^q; `iterations`
-    Gauss-Newton steps with variable projection on it (each step clipped to
-    half the stencil's width, the point kept within 1.5 times the stencil's
-    extent on each side) from U = V = 0.  Returns
-    (maps with the new T1, T2 as float32, mask of the voxels moved)."""
+    Per voxel: the matched atom's six-point stencil (_stencil_f64); with a B1
+    map, the stencil of the three B1 blocks around the match (clamped to the
+    table) interpolated quadratically (Lagrange) to the voxel's B1.  In
+    (U, V) = (log T1 / T1c, log T2 / T2c) the six signals give the quadratic
+    surrogate s = c + a U + b V + d U^2 + e V^2 + f U V (a, d through the
+    three nodes along T1; b, e along T2; f from the diagonal node's residual).
+    `iterations` Gauss-Newton steps with variable projection on it (each step
+    clipped to half the stencil's width, the point kept within 1.5 times the
+    stencil's extent on each side) from U = V = 0.  Returns (maps with the
+    new T1, T2 as float32, mask of the voxels moved)."""
     maps = np.array(maps, np.float32, copy=True)
     atoms = np.asarray(atoms)
     params = np.asarray(params, np.float32)
@@ -292,10 +297,9 @@ def refine_start_f64(maps, index, atoms, params, img, natoms: int, b1map=None, i
     nb = NATOMS // natoms
     moved = np.zeros(maps.shape[0], bool)
 
-    def quad(hm, hp):
-        a1 = 1.0 / (hp * (hp - hm))
-        a2 = -1.0 / (hm * (hp - hm))
-        return a1, a2, 1.0 / hp - a1 * hp, -a2 * hp
+    def quad(sm, s0, sp, hm, hp):
+        q = ((sp - s0) / hp - (sm - s0) / hm) / (hp - hm)
+        return (sp - s0) / hp - q * hp, q
 
     for v in range(maps.shape[0]):
         k = int(index[v])
@@ -305,18 +309,18 @@ def refine_start_f64(maps, index, atoms, params, img, natoms: int, b1map=None, i
         T1c, T2c = params[k, 0], params[k, 1]
         if maps[v, 0] != T1c or maps[v, 1] != T2c or not (T1c > T2c) or not (T2c > 0):
             continue
-        st = _stencil_f64(params, b * natoms, natoms, j)
-        if st is None:
+        found = _stencil_f64(params, b * natoms, natoms, j)
+        if found is None:
             continue
-        qbase, qw = [b * natoms], [1.0]
+        st, diag_up = found
+        bb = b * natoms
+        qbase, qw = [bb], [1.0]
         if b1map is not None and nb >= 3:
             bs = min(max(b - 1, 0), nb - 3)
             qbase = [(bs + q) * natoms for q in range(3)]
             nodes = [float(params[qb + j, 3]) for qb in qbase]
-            ok = all(params[b * natoms + st[i][c], m] == params[qb + st[i][c], m]
-                     for qb in qbase for i in range(3) for c in range(3) for m in range(3))
-            ok = ok and all(params[qb + st[i][c], 3] == nd for qb, nd in zip(qbase, nodes)
-                            for i in range(3) for c in range(3))
+            ok = all(params[bb + r, m] == params[qb + r, m] for qb in qbase for r in st for m in range(3))
+            ok = ok and all(params[qb + r, 3] == nd for qb, nd in zip(qbase, nodes) for r in st)
             if not ok or len(set(nodes)) < 3:
                 continue
             bv = float(b1map[v])
@@ -325,31 +329,27 @@ def refine_start_f64(maps, index, atoms, params, img, natoms: int, b1map=None, i
             n0, n1, n2 = nodes
             qw = [(bv - n1) * (bv - n2) / ((n0 - n1) * (n0 - n2)), (bv - n0) * (bv - n2) / ((n1 - n0) * (n1 - n2)),
                   (bv - n0) * (bv - n1) / ((n2 - n0) * (n2 - n1))]
-        S = [[sum(w * atoms[qb + st[i][c]].astype(np.complex128) for w, qb in zip(qw, qbase))
-              for c in range(3)] for i in range(3)]
-        bb = b * natoms
-        hum, hup = np.log(params[bb + st[0][1], 0] / np.float64(T1c)), np.log(params[bb + st[2][1], 0] / np.float64(T1c))
-        hvm, hvp = np.log(params[bb + st[1][0], 1] / np.float64(T2c)), np.log(params[bb + st[1][2], 1] / np.float64(T2c))
-        cu, cv = quad(hum, hup), quad(hvm, hvp)
-        m1 = [[None] * 3 for _ in range(3)]
-        for c in range(3):
-            dp, dm = S[2][c] - S[1][c], S[0][c] - S[1][c]
-            m1[0][c], m1[1][c], m1[2][c] = S[1][c], cu[2] * dp + cu[3] * dm, cu[0] * dp + cu[1] * dm
-        M = []
-        for p in range(3):
-            dp, dm = m1[p][2] - m1[p][1], m1[p][0] - m1[p][1]
-            M += [m1[p][1], cv[2] * dp + cv[3] * dm, cv[0] * dp + cv[1] * dm]
-        M = np.array(M)
+        S = [sum(w * atoms[qb + r].astype(np.complex128) for w, qb in zip(qw, qbase)) for r in st]
+        hum = np.log(params[bb + st[START_UM], 0] / np.float64(T1c))
+        hup = np.log(params[bb + st[START_UP], 0] / np.float64(T1c))
+        hvm = np.log(params[bb + st[START_VM], 1] / np.float64(T2c))
+        hvp = np.log(params[bb + st[START_VP], 1] / np.float64(T2c))
+        hud, hvd = (hup, hvp) if diag_up else (hum, hvm)
+        c = S[START_C]
+        a_, d_ = quad(S[START_UM], c, S[START_UP], hum, hup)
+        b_, e_ = quad(S[START_VM], c, S[START_VP], hvm, hvp)
+        f_ = (S[START_D] - c - a_ * hud - b_ * hvd - d_ * hud ** 2 - e_ * hvd ** 2) / (hud * hvd)
+        M = np.array([c, a_, b_, d_, e_, f_])
         Gh = M.conj() @ M.T
         pv = M.conj() @ np.asarray(img[v], np.complex128)
         ulo, uhi = 1.5 * min(hum, hup), 1.5 * max(hum, hup)
         vlo, vhi = 1.5 * min(hvm, hvp), 1.5 * max(hvm, hvp)
+        lu, lv = 0.5 * (max(hum, hup) - min(hum, hup)), 0.5 * (max(hvm, hvp) - min(hvm, hvp))
         U = V = 0.0
         for _ in range(iterations):
-            Up, Vp, dU, dV = [1, U, U * U], [1, V, V * V], [0, 1, 2 * U], [0, 1, 2 * V]
-            c0 = np.array([Up[p] * Vp[q] for p in range(3) for q in range(3)])
-            c1 = np.array([dU[p] * Vp[q] for p in range(3) for q in range(3)])
-            c2 = np.array([Up[p] * dV[q] for p in range(3) for q in range(3)])
+            c0 = np.array([1.0, U, V, U * U, V * V, U * V])
+            c1 = np.array([0.0, 1.0, 0.0, 2 * U, 0.0, V])
+            c2 = np.array([0.0, 0.0, 1.0, 0.0, 2 * V, U])
             Ss = (c0 @ Gh @ c0).real
             g1, g2 = c0 @ Gh @ c1, c0 @ Gh @ c2
             H11, H12, H22 = (c1 @ Gh @ c1).real, (c1 @ Gh @ c2).real, (c2 @ Gh @ c2).real
@@ -369,7 +369,6 @@ def refine_start_f64(maps, index, atoms, params, img, natoms: int, b1map=None, i
             d1, d2 = (A22 * b1 - A12 * b2) / det, (A11 * b2 - A12 * b1) / det
             if not (np.isfinite(d1) and np.isfinite(d2)):
                 break
-            lu, lv = 0.5 * (max(hum, hup) - min(hum, hup)), 0.5 * (max(hvm, hvp) - min(hvm, hvp))
             U = min(max(U + min(max(d1, -lu), lu), ulo), uhi)
             V = min(max(V + min(max(d2, -lv), lv), vlo), vhi)
         T1, T2 = float(T1c) * np.exp(U), float(T2c) * np.exp(V)

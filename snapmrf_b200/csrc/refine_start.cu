@@ -2,27 +2,30 @@
 //
 // Matching leaves each voxel on a grid point of the dictionary (the atom of
 // the largest |<d, x>| in the reference's MRF_match, src/functions.cu).  The
-// matched atom and its neighbours at the adjacent T1 and T2 values of the
+// matched atom, its neighbours at the adjacent T1 and T2 values of the
 // parameter table (trans_params order, src/functions.cu:355-391: B1
-// outermost, then B0, T2, T1 innermost, T1 > T2 kept) form a 3 x 3 stencil;
-// with a B1 map the stencil is read from the three B1 blocks around the
-// voxel's B1 and interpolated quadratically to that value.  Interpolated
-// biquadratically in (u, v) = (log T1, log T2), the nine signals give a
-// surrogate s(u, v) of the signal model, accurate to third order in the grid
-// step.  The voxel's fit |<s, x>|^2 / ||s||^2 is maximised over the surrogate
-// by Gauss-Newton with variable projection, using only the 9 x 9 Gram matrix
-// of the stencil and the stencil's nine inner products with the voxel, so no
-// recursion is run.  The result replaces the voxel's (T1, T2): a start close
-// enough to the least-squares fit that one pass of the refinement usually
-// meets its stopping tolerance.  No counterpart in the reference.
+// outermost, then B0, T2, T1 innermost, T1 > T2 kept) and one diagonal
+// neighbour form a six-point stencil; with a B1 map the stencil is read from
+// the three B1 blocks around the voxel's B1 and interpolated quadratically to
+// that value.  In (U, V) = (log T1 / T1_0, log T2 / T2_0) the six signals give
+// the quadratic surrogate
+//     s(U, V) = c + a U + b V + d U^2 + e V^2 + f U V
+// of the signal model (exact for quadratics, so accurate to third order in
+// the grid step): a, d from the three nodes along T1, b, e along T2, f from
+// the diagonal node.  The voxel's fit |<s, x>|^2 / ||s||^2 is maximised over
+// the surrogate by Gauss-Newton with variable projection, using only the 6 x 6
+// Gram matrix of (c, a, b, d, e, f) and their inner products with the voxel,
+// so no recursion is run.  The result replaces the voxel's (T1, T2): a start
+// close enough to the least-squares fit that one pass of the refinement
+// usually meets its stopping tolerance.  No counterpart in the reference.
 //
-// Layout: one warp per voxel.  Lanes stride over the time points, each
-// accumulating the Gram matrix and the inner products of its samples in the
-// stencil's Taylor basis (s = sum_pq m_pq U^p V^q, U = u - u_0, V = v - v_0),
-// where the nine basis signals are formed from differences of the atoms
-// sample by sample, so the small derivative terms never come out of a
-// difference of large accumulated sums.  The stencil search runs 32 table
-// rows at a time with warp ballots.
+// Two kernels.  accumulate_kernel: one warp per voxel finds the stencil
+// (32 table rows at a time with warp ballots), then its lanes stride over the
+// time points, each accumulating the Gram matrix and the inner products of
+// its samples in the basis (c, a, b, d, e, f), formed from differences of the
+// atoms sample by sample so that the small derivative terms never come out of
+// a difference of large accumulated sums; the warp's sums go to a scratch
+// system per voxel.  solve_kernel: one thread per voxel solves the surrogate.
 
 #include "common.h"
 
@@ -33,11 +36,19 @@
 namespace snapmrf {
 namespace rstart {
 
-constexpr int kWarps = 4;       // voxels per block
+constexpr int kWarps = 4;        // voxels per block of the accumulation
 constexpr int kSolveIters = 10;  // Gauss-Newton iterations on the surrogate
+constexpr int kPts = 6;          // stencil points (and basis signals)
+constexpr int kTri = kPts * (kPts + 1) / 2;
 // shared-memory slots of staged samples per warp (imaginary atoms, complex)
 template <bool IMAG>
-__host__ __device__ constexpr int stages() { return IMAG ? 5 : 3; }
+__host__ __device__ constexpr int stages() {
+    return IMAG ? 5 : 3;
+}
+
+// Stencil points: the matched atom, T1 below / above, T2 below / above, and
+// the diagonal (T1 above and T2 above, else T1 below and T2 below).
+enum { kC = 0, kUm = 1, kUp = 2, kVm = 3, kVp = 4, kD = 5 };
 
 struct Args {
     float *maps;
@@ -54,16 +65,18 @@ struct Args {
     long long nvox;
     const float *b1map;
     int *count;
-    float *sys;  // [kSysRows (+45 complex)][nvox]: the accumulated system per voxel
+    float *sys;  // [kSysRows (kSysRowsComplex)][nvox]: the accumulated system per voxel
 };
 
 // Rows of the per-voxel system handed from the accumulation to the solve:
-// the matched (T1, T2) (T1 NaN: leave the voxel), the stencil's node offsets
-// in log T1 and log T2, the inner products with the voxel (real and
-// imaginary parts), the real part of the Gram matrix (packed upper triangle)
-// and, for complex atoms, its imaginary part.
-constexpr int kRowT1 = 0, kRowT2 = 1, kRowH = 2, kRowPr = 6, kRowPi = 15, kRowG = 24, kRowGi = 69;
-constexpr int kSysRows = 69, kSysRowsComplex = 114;
+// the matched (T1, T2) (T1 NaN: leave the voxel), the node offsets (log
+// ratios) of T1 below / above, T2 below / above and of the diagonal node, the
+// inner products with the voxel (real and imaginary parts), the real part of
+// the Gram matrix (packed upper triangle) and, for complex atoms, its
+// imaginary part.
+constexpr int kRowT1 = 0, kRowT2 = 1, kRowH = 2, kRowPr = 8, kRowPi = kRowPr + kPts, kRowG = kRowPi + kPts,
+              kRowGi = kRowG + kTri;
+constexpr int kSysRows = kRowGi, kSysRowsComplex = kRowGi + kTri;
 
 __device__ __forceinline__ float prm(const Args &a, long long r, int c) { return __ldg(a.params + r * a.nparams + c); }
 
@@ -81,11 +94,13 @@ __device__ long long warp_find(long long start, int dir, long long n, F pred) {
     return -1;
 }
 
-// The 3 x 3 stencil st[i][c] (T1 node i, T2 node c; node 1 the matched atom
-// j) as row numbers within the block starting at `base`.  False unless the
-// matched atom has a neighbour on both sides in T1 and in T2, and the two
-// adjacent T2 rows hold the same three T1 values in the same order.
-__device__ bool find_stencil(const Args &a, long long base, long long j, long long st[3][3]) {
+// The stencil st[kPts] as row numbers within the block starting at `base`
+// (j: the matched atom); diag_up: the diagonal node is (T1 above, T2 above)
+// rather than (T1 below, T2 below).  False unless the matched atom has a
+// neighbour on both sides in T1 within its T2 row, the adjacent T2 rows on
+// both sides hold the matched T1, and one of them holds the diagonal node,
+// with the same B0 throughout.
+__device__ bool find_stencil(const Args &a, long long base, long long j, long long st[kPts], bool *diag_up) {
     const long long n = a.natoms;
     auto t1 = [&](long long r) { return prm(a, base + r, 0); };
     auto t2 = [&](long long r) { return prm(a, base + r, 1); };
@@ -94,10 +109,11 @@ __device__ bool find_stencil(const Args &a, long long base, long long j, long lo
     const float T1m = t1(j - 1), T1c = t1(j), T1p = t1(j + 1), T2c = t2(j), B0c = b0(j);
     if (t2(j - 1) != T2c || t2(j + 1) != T2c || b0(j - 1) != B0c || b0(j + 1) != B0c) return false;
     if (!((T1m < T1c && T1c < T1p) || (T1m > T1c && T1c > T1p))) return false;
-    st[0][1] = j - 1;
-    st[1][1] = j;
-    st[2][1] = j + 1;
+    st[kC] = j;
+    st[kUm] = j - 1;
+    st[kUp] = j + 1;
     float T2n[2];
+    long long rcs[2];
 #pragma unroll
     for (int s = 0; s < 2; s++) {
         const int dir = s ? 1 : -1;
@@ -117,17 +133,27 @@ __device__ bool find_stencil(const Args &a, long long base, long long j, long lo
         });
         if (k2 < 0) return false;
         const long long rc = r0 + dir * k2;
-        if (rc < 1 || rc + 1 >= n) return false;
         if (t1(rc) != T1c || t2(rc) != T2r || b0(rc) != B0c) return false;
-        if (t1(rc - 1) != T1m || t2(rc - 1) != T2r || b0(rc - 1) != B0c) return false;
-        if (t1(rc + 1) != T1p || t2(rc + 1) != T2r || b0(rc + 1) != B0c) return false;
-        const int c = s ? 2 : 0;
-        st[0][c] = rc - 1;
-        st[1][c] = rc;
-        st[2][c] = rc + 1;
         T2n[s] = T2r;
+        rcs[s] = rc;
     }
-    return T2n[0] != T2n[1] && (T2n[0] < T2c) == (T2c < T2n[1]);
+    if (!(T2n[0] != T2n[1] && (T2n[0] < T2c) == (T2c < T2n[1]))) return false;
+    st[kVm] = rcs[0];
+    st[kVp] = rcs[1];
+    // the diagonal: T1 above in the upper T2 row (the rows list T1 in the
+    // same order), else T1 below in the lower one
+    const long long du = rcs[1] + 1, dm = rcs[0] - 1;
+    if (du < n && t1(du) == T1p && t2(du) == T2n[1] && b0(du) == B0c) {
+        st[kD] = du;
+        *diag_up = true;
+        return true;
+    }
+    if (dm >= 0 && t1(dm) == T1m && t2(dm) == T2n[0] && b0(dm) == B0c) {
+        st[kD] = dm;
+        *diag_up = false;
+        return true;
+    }
+    return false;
 }
 
 // Coefficients of the quadratic through (h_m, y_m), (0, y_0), (h_p, y_p) in
@@ -153,9 +179,9 @@ __device__ void lagrange3(const float n[3], float x, float w[3]) {
     w[2] = (x - n[0]) * (x - n[1]) / ((n[2] - n[0]) * (n[2] - n[1]));
 }
 
-// index of the packed upper triangle of the 9 x 9 Gram matrix
+// index of the packed upper triangle of the kPts x kPts Gram matrix
 __device__ __host__ __forceinline__ constexpr int tri(int i, int j) {
-    return i <= j ? i * 9 - i * (i - 1) / 2 + (j - i) : j * 9 - j * (j - 1) / 2 + (i - j);
+    return i <= j ? i * kPts - i * (i - 1) / 2 + (j - i) : j * kPts - j * (j - 1) / 2 + (i - j);
 }
 
 // cp.async (Ampere-style asynchronous global -> shared copies, cached in
@@ -189,44 +215,43 @@ __global__ void __launch_bounds__(kWarps * 32) accumulate_kernel(const __grid_co
     const long long k = a.index[v];
     if (k < 0 || k >= a.NATOMS) return leave();
     const float *mp = a.maps + v * a.nmaps;
-    const long long b = k / a.natoms, j = k - b * a.natoms;
+    const long long b = k / a.natoms, j = k - b * a.natoms, bb = b * a.natoms;
     const float T1c = prm(a, k, 0), T2c = prm(a, k, 1);
     // the maps must still hold the matched grid point
     if (mp[0] != T1c || mp[1] != T2c || !(T1c > T2c) || !(T2c > 0.f)) return leave();
-    long long st[3][3];
-    if (!find_stencil(a, b * a.natoms, j, st)) return leave();
+    long long st[kPts];
+    bool diag_up = true;
+    if (!find_stencil(a, bb, j, st, &diag_up)) return leave();
     // B1 blocks and their weights at the voxel's B1
     const long long nb = a.NATOMS / a.natoms;
     int nq = 1;
-    long long qbase[3] = {b * a.natoms, b * a.natoms, b * a.natoms};
+    long long qbase[3] = {bb, bb, bb};
     float qw[3] = {1.f, 0.f, 0.f};
     if (a.b1map && nb >= 3) {
         const long long bs = min(max(b - 1, 0ll), nb - 3);
         float nodes[3];
-        bool ok = true;
 #pragma unroll
         for (int q = 0; q < 3; q++) {
             qbase[q] = (bs + q) * a.natoms;
             nodes[q] = prm(a, qbase[q] + j, 3);
         }
-        // the same (T1, T2, B0) rows in every block of the stencil
-        // (one check per lane, selected without indexing the arrays by lane)
-        if (lane < 27) {
-            const int q = lane / 9, i = (lane / 3) % 3, c = lane % 3;
+        // the same (T1, T2, B0) rows in every block of the stencil (one
+        // check per lane, selected without indexing the arrays by lane)
+        bool ok = true;
+        if (lane < 3 * kPts) {
+            const int q = lane / kPts, i = lane % kPts;
             long long row = 0, qb = 0;
             float node = 0.f;
 #pragma unroll
-            for (int ii = 0; ii < 3; ii++)
-#pragma unroll
-                for (int cc = 0; cc < 3; cc++)
-                    if (ii == i && cc == c) row = st[ii][cc];
+            for (int ii = 0; ii < kPts; ii++)
+                if (ii == i) row = st[ii];
 #pragma unroll
             for (int qq = 0; qq < 3; qq++)
                 if (qq == q) {
                     qb = qbase[qq];
                     node = nodes[qq];
                 }
-            const long long r0 = b * a.natoms + row, r1 = qb + row;
+            const long long r0 = bb + row, r1 = qb + row;
             ok = prm(a, r0, 0) == prm(a, r1, 0) && prm(a, r0, 1) == prm(a, r1, 1) &&
                  prm(a, r0, 2) == prm(a, r1, 2) && prm(a, r1, 3) == node;
         }
@@ -237,52 +262,51 @@ __global__ void __launch_bounds__(kWarps * 32) accumulate_kernel(const __grid_co
         lagrange3(nodes, bv, qw);
         nq = 3;
     }
-    // Taylor coefficients along log T1 (rows) and log T2 (columns); the
-    // node offsets as logs of ratios, exact to rounding
-    const long long bb = b * a.natoms;
-    const float hum = logf(prm(a, bb + st[0][1], 0) / T1c), hup = logf(prm(a, bb + st[2][1], 0) / T1c);
-    const float hvm = logf(prm(a, bb + st[1][0], 1) / T2c), hvp = logf(prm(a, bb + st[1][2], 1) / T2c);
+    // node offsets as logs of ratios (exact to rounding) and the basis
+    // coefficients along T1, along T2 and of the diagonal
+    const float hum = logf(prm(a, bb + st[kUm], 0) / T1c), hup = logf(prm(a, bb + st[kUp], 0) / T1c);
+    const float hvm = logf(prm(a, bb + st[kVm], 1) / T2c), hvp = logf(prm(a, bb + st[kVp], 1) / T2c);
+    const float hud = diag_up ? hup : hum, hvd = diag_up ? hvp : hvm;
+    const float hud2 = hud * hud, hvd2 = hvd * hvd, inv_uv = 1.f / (hud * hvd);
     const Quad cu = quad_coeffs(hum, hup), cv = quad_coeffs(hvm, hvp);
-    // the stencil rows of T1 node 1 per block and T2 node; T1 nodes 0 and 2
-    // are the rows before and after
-    const float2 *rows[3][3];
+    const float2 *rows[3][kPts];
 #pragma unroll
     for (int q = 0; q < 3; q++)
 #pragma unroll
-        for (int c = 0; c < 3; c++) rows[q][c] = a.atoms + (qbase[q] + st[1][c]) * a.atom_stride;
-    const long long rs = a.atom_stride;
+        for (int i = 0; i < kPts; i++) rows[q][i] = a.atoms + (qbase[q] + st[i]) * a.atom_stride;
     const float2 *xv = a.img + v * a.img_stride;
 
-    // Hermitian Gram matrix of the Taylor basis, sum_t conj(m_r) m_c: real
-    // part G (upper triangle), imaginary part Gi (strict upper triangle, zero
-    // for purely imaginary atoms); inner products with the voxel,
+    // Hermitian Gram matrix of the basis, sum_t conj(m_r) m_c: real part G
+    // (upper triangle), imaginary part Gi (strict upper triangle, zero for
+    // purely imaginary atoms); inner products with the voxel,
     // sum_t conj(m_r) x = (pr, pi)
-    float G[45], Gi[IMAG ? 1 : 45], pr[9], pi[9];
+    float G[kTri], Gi[IMAG ? 1 : kTri], pr[kPts], pi[kPts];
 #pragma unroll
-    for (int i = 0; i < 45; i++) G[i] = 0.f;
+    for (int i = 0; i < kTri; i++) G[i] = 0.f;
 #pragma unroll
-    for (int i = 0; i < (IMAG ? 1 : 45); i++) Gi[i] = 0.f;
+    for (int i = 0; i < (IMAG ? 1 : kTri); i++) Gi[i] = 0.f;
 #pragma unroll
-    for (int i = 0; i < 9; i++) pr[i] = pi[i] = 0.f;
+    for (int i = 0; i < kPts; i++) pr[i] = pi[i] = 0.f;
 
-    // the stencil of one part (real or imaginary) at one sample in the
-    // Taylor basis: m[p * 3 + q] multiplies U^p V^q
-    auto taylor = [&](const float s[3][3], float m[9]) {
-        float m1[3][3];  // [T1 power][T2 node]
-#pragma unroll
-        for (int c = 0; c < 3; c++) {
-            const float dp = s[2][c] - s[1][c], dm = s[0][c] - s[1][c];
-            m1[0][c] = s[1][c];
-            m1[1][c] = fmaf(cu.b1, dp, cu.b2 * dm);
-            m1[2][c] = fmaf(cu.a1, dp, cu.a2 * dm);
-        }
-#pragma unroll
-        for (int p = 0; p < 3; p++) {
-            const float dp = m1[p][2] - m1[p][1], dm = m1[p][0] - m1[p][1];
-            m[p * 3] = m1[p][1];
-            m[p * 3 + 1] = fmaf(cv.b1, dp, cv.b2 * dm);
-            m[p * 3 + 2] = fmaf(cv.a1, dp, cv.a2 * dm);
-        }
+    // one part (real or imaginary) of the stencil at one sample -> the basis
+    // (c, a, b, d, e, f)
+    auto basis = [&](const float s[kPts], float m[kPts]) {
+        const float c = s[kC];
+        const float dpu = s[kUp] - c, dmu = s[kUm] - c, dpv = s[kVp] - c, dmv = s[kVm] - c;
+        const float au = fmaf(cu.b1, dpu, cu.b2 * dmu), du = fmaf(cu.a1, dpu, cu.a2 * dmu);
+        const float bv = fmaf(cv.b1, dpv, cv.b2 * dmv), ev = fmaf(cv.a1, dpv, cv.a2 * dmv);
+        // the cross term: what the diagonal node leaves after the others
+        float r = s[kD] - c;
+        r = fmaf(-au, hud, r);
+        r = fmaf(-bv, hvd, r);
+        r = fmaf(-du, hud2, r);
+        r = fmaf(-ev, hvd2, r);
+        m[0] = c;
+        m[1] = au;
+        m[2] = bv;
+        m[3] = du;
+        m[4] = ev;
+        m[5] = r * inv_uv;
     };
 
     // Staging: each lane copies its own samples of the stencil rows and of
@@ -291,11 +315,12 @@ __global__ void __launch_bounds__(kWarps * 32) accumulate_kernel(const __grid_co
     // reads back only what it copied itself.  The loads in flight hold no
     // registers, so many more of them are outstanding per SM than register
     // prefetching would allow.
-    using V = typename std::conditional<IMAG, float, float2>::type;
+    using Vt = typename std::conditional<IMAG, float, float2>::type;
     constexpr int kStages = stages<IMAG>();
+    constexpr int kRows = 3 * kPts;
     extern __shared__ __align__(16) unsigned char rs_smem[];
-    V *sa = reinterpret_cast<V *>(rs_smem) + (size_t)(threadIdx.x >> 5) * kStages * 27 * 32;
-    float2 *sx = reinterpret_cast<float2 *>(reinterpret_cast<V *>(rs_smem) + (size_t)kWarps * kStages * 27 * 32) +
+    Vt *sa = reinterpret_cast<Vt *>(rs_smem) + (size_t)(threadIdx.x >> 5) * kStages * kRows * 32;
+    float2 *sx = reinterpret_cast<float2 *>(reinterpret_cast<Vt *>(rs_smem) + (size_t)kWarps * kStages * kRows * 32) +
                  (threadIdx.x >> 5) * kStages * 32;
     const int nch = (a.T + 31) / 32;
     auto issue = [&](int kc) {
@@ -305,16 +330,14 @@ __global__ void __launch_bounds__(kWarps * 32) accumulate_kernel(const __grid_co
             for (int q = 0; q < 3; q++)
                 if (q < nq)
 #pragma unroll
-                    for (int i = 0; i < 3; i++)
-#pragma unroll
-                        for (int c = 0; c < 3; c++) {
-                            const float2 *g = rows[q][c] + (i - 1) * rs + t;
-                            V *d = sa + (slot * 27 + q * 9 + i * 3 + c) * 32 + lane;
-                            if (IMAG)
-                                cp_async4(d, reinterpret_cast<const float *>(g) + 1);
-                            else
-                                cp_async8(d, g);
-                        }
+                    for (int i = 0; i < kPts; i++) {
+                        const float2 *g = rows[q][i] + t;
+                        Vt *d = sa + (slot * kRows + q * kPts + i) * 32 + lane;
+                        if (IMAG)
+                            cp_async4(d, reinterpret_cast<const float *>(g) + 1);
+                        else
+                            cp_async8(d, g);
+                    }
             cp_async8(sx + slot * 32 + lane, xv + t);
         }
         cp_async_commit();
@@ -328,46 +351,44 @@ __global__ void __launch_bounds__(kWarps * 32) accumulate_kernel(const __grid_co
         const int t = kc * 32 + lane, slot = kc % kStages;
         if (t >= a.T) continue;
         const float2 x = sx[slot * 32 + lane];
-        float sr[3][3], si[3][3];
+        float sr[kPts], si[kPts];
 #pragma unroll
-        for (int i = 0; i < 3; i++)
+        for (int i = 0; i < kPts; i++) {
+            float accr = 0.f, acci = 0.f;
 #pragma unroll
-            for (int c = 0; c < 3; c++) {
-                float accr = 0.f, acci = 0.f;
-#pragma unroll
-                for (int q = 0; q < 3; q++) {
-                    if (q < nq) {
-                        const V d = sa[(slot * 27 + q * 9 + i * 3 + c) * 32 + lane];
-                        if constexpr (IMAG) {
-                            acci = fmaf(qw[q], d, acci);
-                        } else {
-                            accr = fmaf(qw[q], d.x, accr);
-                            acci = fmaf(qw[q], d.y, acci);
-                        }
+            for (int q = 0; q < 3; q++) {
+                if (q < nq) {
+                    const Vt d = sa[(slot * kRows + q * kPts + i) * 32 + lane];
+                    if constexpr (IMAG) {
+                        acci = fmaf(qw[q], d, acci);
+                    } else {
+                        accr = fmaf(qw[q], d.x, accr);
+                        acci = fmaf(qw[q], d.y, acci);
                     }
                 }
-                sr[i][c] = accr;
-                si[i][c] = acci;
             }
-        float mi[9];
-        taylor(si, mi);
+            sr[i] = accr;
+            si[i] = acci;
+        }
+        float mi[kPts];
+        basis(si, mi);
         if (IMAG) {
 #pragma unroll
-            for (int r = 0; r < 9; r++) {
+            for (int r = 0; r < kPts; r++) {
 #pragma unroll
-                for (int c = 0; c < 9; c++)
+                for (int c = 0; c < kPts; c++)
                     if (c >= r) G[tri(r, c)] = fmaf(mi[r], mi[c], G[tri(r, c)]);
                 // conj(i m) x = (m xi, -m xr)
                 pr[r] = fmaf(mi[r], x.y, pr[r]);
                 pi[r] = fmaf(-mi[r], x.x, pi[r]);
             }
         } else {
-            float mr[9];
-            taylor(sr, mr);
+            float mr[kPts];
+            basis(sr, mr);
 #pragma unroll
-            for (int r = 0; r < 9; r++) {
+            for (int r = 0; r < kPts; r++) {
 #pragma unroll
-                for (int c = 0; c < 9; c++) {
+                for (int c = 0; c < kPts; c++) {
                     if (c >= r) G[tri(r, c)] = fmaf(mr[r], mr[c], fmaf(mi[r], mi[c], G[tri(r, c)]));
                     if (c > r) Gi[tri(r, c)] = fmaf(mr[r], mi[c], fmaf(-mi[r], mr[c], Gi[tri(r, c)]));
                 }
@@ -378,17 +399,17 @@ __global__ void __launch_bounds__(kWarps * 32) accumulate_kernel(const __grid_co
     }
     // warp sums (every lane ends with the totals)
 #pragma unroll
-    for (int i = 0; i < 45; i++)
+    for (int i = 0; i < kTri; i++)
 #pragma unroll
         for (int o = 16; o; o >>= 1) G[i] += __shfl_xor_sync(0xffffffffu, G[i], o);
     if (!IMAG) {
 #pragma unroll
-        for (int i = 0; i < (IMAG ? 1 : 45); i++)
+        for (int i = 0; i < (IMAG ? 1 : kTri); i++)
 #pragma unroll
             for (int o = 16; o; o >>= 1) Gi[i] += __shfl_xor_sync(0xffffffffu, Gi[i], o);
     }
 #pragma unroll
-    for (int i = 0; i < 9; i++)
+    for (int i = 0; i < kPts; i++)
 #pragma unroll
         for (int o = 16; o; o >>= 1) {
             pr[i] += __shfl_xor_sync(0xffffffffu, pr[i], o);
@@ -397,27 +418,28 @@ __global__ void __launch_bounds__(kWarps * 32) accumulate_kernel(const __grid_co
     // the system to the scratch rows, each value by one lane
     float *sys = a.sys + v;
     const long long n = a.nvox;
-    const float hv[6] = {T1c, T2c, hum, hup, hvm, hvp};
+    const float hv[8] = {T1c, T2c, hum, hup, hvm, hvp, hud, hvd};
 #pragma unroll
-    for (int r = 0; r < 6; r++)
+    for (int r = 0; r < 8; r++)
         if ((r & 31) == lane) sys[r * n] = hv[r];
 #pragma unroll
-    for (int r = 0; r < 9; r++) {
+    for (int r = 0; r < kPts; r++) {
         if (((kRowPr + r) & 31) == lane) sys[(kRowPr + r) * n] = pr[r];
         if (((kRowPi + r) & 31) == lane) sys[(kRowPi + r) * n] = pi[r];
     }
 #pragma unroll
-    for (int r = 0; r < 45; r++) {
+    for (int r = 0; r < kTri; r++) {
         if (((kRowG + r) & 31) == lane) sys[(kRowG + r) * n] = G[r];
         if (!IMAG && ((kRowGi + r) & 31) == lane) sys[(kRowGi + r) * n] = Gi[r];
     }
 }
 
 // One thread per voxel: Gauss-Newton with variable projection on the
-// surrogate s(U, V) = sum m_pq U^p V^q, ds/dU, ds/dV, from the matched grid
-// point; the point may leave the stencil by half its extent on each side (a
-// match more than a grid step from the fit: the quadratic extrapolates,
-// still nearer than the grid point).
+// surrogate s(U, V) = c + a U + b V + d U^2 + e V^2 + f U V and its
+// derivatives, from the matched grid point (U = V = 0).  Each step is
+// clipped to half the stencil's width, and the point may leave the stencil by
+// half its extent on each side (a match more than a grid step from the fit:
+// the quadratic extrapolates, still nearer than the grid point).
 template <bool IMAG>
 __global__ void __launch_bounds__(128) solve_kernel(const __grid_constant__ Args a) {
     const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -429,14 +451,14 @@ __global__ void __launch_bounds__(128) solve_kernel(const __grid_constant__ Args
     const float T2c = sys[kRowT2 * n];
     const float hum = sys[(kRowH + 0) * n], hup = sys[(kRowH + 1) * n];
     const float hvm = sys[(kRowH + 2) * n], hvp = sys[(kRowH + 3) * n];
-    float G[45], Gi[IMAG ? 1 : 45], pr[9], pi[9];
+    float G[kTri], Gi[IMAG ? 1 : kTri], pr[kPts], pi[kPts];
 #pragma unroll
-    for (int r = 0; r < 45; r++) {
+    for (int r = 0; r < kTri; r++) {
         G[r] = sys[(kRowG + r) * n];
         if (!IMAG) Gi[r] = sys[(kRowGi + r) * n];
     }
 #pragma unroll
-    for (int r = 0; r < 9; r++) {
+    for (int r = 0; r < kPts; r++) {
         pr[r] = sys[(kRowPr + r) * n];
         pi[r] = sys[(kRowPi + r) * n];
     }
@@ -445,25 +467,18 @@ __global__ void __launch_bounds__(128) solve_kernel(const __grid_constant__ Args
     const float vlo = 1.5f * fminf(hvm, hvp), vhi = 1.5f * fmaxf(hvm, hvp);
     float U = 0.f, V = 0.f;
     for (int it = 0; it < kSolveIters; it++) {
-        const float Up[3] = {1.f, U, U * U}, Vp[3] = {1.f, V, V * V};
-        const float dU[3] = {0.f, 1.f, 2.f * U}, dV[3] = {0.f, 1.f, 2.f * V};
-        float c0[9], c1[9], c2[9];
+        // coefficient vectors of s, ds/dU and ds/dV in the basis
+        const float c0[kPts] = {1.f, U, V, U * U, V * V, U * V};
+        const float c1[kPts] = {0.f, 1.f, 0.f, 2.f * U, 0.f, V};
+        const float c2[kPts] = {0.f, 0.f, 1.f, 0.f, 2.f * V, U};
+        // G c for the three vectors, and Gi c0 (the imaginary parts of
+        // s^H ds/dU, s^H ds/dV; Gi is antisymmetric)
+        float g0[kPts], g1[kPts], g2[kPts], h0[kPts];
 #pragma unroll
-        for (int p = 0; p < 3; p++)
-#pragma unroll
-            for (int q = 0; q < 3; q++) {
-                c0[p * 3 + q] = Up[p] * Vp[q];
-                c1[p * 3 + q] = dU[p] * Vp[q];
-                c2[p * 3 + q] = Up[p] * dV[q];
-            }
-        // G c for the three coefficient vectors, and Gi c0 (the imaginary
-        // parts of s^H dS/dU, s^H dS/dV; Gi is antisymmetric)
-        float g0[9], g1[9], g2[9], h0[9];
-#pragma unroll
-        for (int r = 0; r < 9; r++) {
+        for (int r = 0; r < kPts; r++) {
             float s0 = 0.f, s1 = 0.f, s2 = 0.f, z0 = 0.f;
 #pragma unroll
-            for (int c = 0; c < 9; c++) {
+            for (int c = 0; c < kPts; c++) {
                 const float g = G[tri(r, c)];
                 s0 = fmaf(g, c0[c], s0);
                 s1 = fmaf(g, c1[c], s1);
@@ -480,7 +495,7 @@ __global__ void __launch_bounds__(128) solve_kernel(const __grid_constant__ Args
         float Ss = 0.f, G1 = 0.f, G2 = 0.f, G1i = 0.f, G2i = 0.f, H11 = 0.f, H12 = 0.f, H22 = 0.f;
         float Pr = 0.f, Pi = 0.f, Q1r = 0.f, Q1i = 0.f, Q2r = 0.f, Q2i = 0.f;
 #pragma unroll
-        for (int r = 0; r < 9; r++) {
+        for (int r = 0; r < kPts; r++) {
             Ss = fmaf(c0[r], g0[r], Ss);
             G1 = fmaf(c1[r], g0[r], G1);
             G2 = fmaf(c2[r], g0[r], G2);
@@ -512,7 +527,6 @@ __global__ void __launch_bounds__(128) solve_kernel(const __grid_constant__ Args
         if (!(det > 0.f) || !(A11 > 0.f) || !isfinite(det)) break;
         float d1 = (A22 * b1 - A12 * b2) / det, d2 = (A11 * b2 - A12 * b1) / det;
         if (!isfinite(d1) || !isfinite(d2)) break;
-        // at most half the stencil's width per iteration
         d1 = fminf(fmaxf(d1, -lu), lu);
         d2 = fminf(fmaxf(d2, -lv), lv);
         U = fminf(fmaxf(U + d1, ulo), uhi);
@@ -570,9 +584,9 @@ extern "C" int snapmrf_refine_start(float *d_maps, int nmaps, const int64_t *d_i
     a.sys = sys.as<float>();
     const unsigned grid = (unsigned)((nvoxels + rstart::kWarps - 1) / rstart::kWarps);
     const unsigned grid2 = (unsigned)((nvoxels + 127) / 128);
-    // staged samples: per warp kStages x 32 lanes x (27 atom values + the voxel)
+    // staged samples: per warp kStages x 32 lanes x (3 kPts atom values + the voxel)
     const size_t smem = (size_t)rstart::kWarps * (imag ? rstart::stages<true>() : rstart::stages<false>()) * 32 *
-                        (27 * (imag ? sizeof(float) : sizeof(float2)) + sizeof(float2));
+                        (3 * rstart::kPts * (imag ? sizeof(float) : sizeof(float2)) + sizeof(float2));
     if (imag) {
         SNAPMRF_CUDA(cudaFuncSetAttribute(rstart::accumulate_kernel<true>,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -589,3 +603,4 @@ extern "C" int snapmrf_refine_start(float *d_maps, int nmaps, const int64_t *d_i
     SNAPMRF_LAUNCH_CHECK();
     return SNAPMRF_OK;
 }
+
