@@ -15,8 +15,8 @@ B1 map, and its BF16 + refine precision form):
             noise at SNR 40 (sigma = ||s|| / sqrt(T) / 40); each voxel is
             matched within its nearest B1 block
 One step = MRF_dict (all 41 blocks) + MRF_match of every voxel (+ the
-refinement in the refined forms: a sub-grid start interpolated from the
-matched atom's neighbourhood of the dictionary, then Gauss-Newton).  The
+refinement in the refined forms: a sub-grid start from a quadratic surrogate
+of the matched atom's neighbourhood of the dictionary, then Gauss-Newton).  The
 headline form is the metric's own: BF16 matching with the top-16 rescored in
 FP32, then the start and at most three Gauss-Newton iterations per voxel
 (a voxel stops once its step is below 1e-3); `forms` times every other form

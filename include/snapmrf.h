@@ -484,23 +484,25 @@ int snapmrf_refine_gn(float *d_maps, int nmaps, const float *img, size_t img_str
  * counterpart in the reference (matching ends on the grid).
  *
  * For each voxel, the matched atom d_index[v] (as snapmrf_mrf_match writes
- * it) and the atoms at the adjacent T1 and T2 values of the parameter table
- * (trans_params order, src/functions.cu:355-391) form a 3 x 3 stencil; with
+ * it), the atoms at the adjacent T1 and T2 values of the parameter table
+ * (trans_params order, src/functions.cu:355-391) and one diagonal neighbour
+ * (T1 and T2 both above, else both below) form a six-point stencil; with
  * d_b1map the stencil is taken from the three B1 blocks around the block of
- * the match and interpolated quadratically to the voxel's B1.  The stencil
- * interpolated biquadratically in (log T1, log T2) is a surrogate of the
- * signal model, accurate to third order in the grid step; the voxel's fit
- * |<s, x>|^2 / ||s||^2 is maximised over it by Gauss-Newton with variable
- * projection (on the stencil's Gram matrix and inner products with the voxel,
- * no recursion), within the stencil, and the result replaces (T1, T2) in
+ * the match and interpolated quadratically to the voxel's B1.  In (log T1,
+ * log T2) the stencil gives the quadratic surrogate c + a U + b V + d U^2 +
+ * e V^2 + f U V of the signal model, accurate to third order in the grid
+ * step; the voxel's fit |<s, x>|^2 / ||s||^2 is maximised over it by
+ * Gauss-Newton with variable projection (on the 6 x 6 Gram matrix of the
+ * surrogate's terms and their inner products with the voxel, no recursion),
+ * within 1.5 times the stencil's extent, and the result replaces (T1, T2) in
  * d_maps.  The start is typically within 1e-4 of the least-squares fit
  * (relative), so one refinement pass meets a stopping tolerance of 1e-3.
  *
  * Voxels are left as they are when the index is outside [0, NATOMS), the
  * maps no longer hold the matched atom's (T1, T2), the atom is on the edge of
- * the grid (no neighbour on one side in T1 or T2, or the adjacent T2 rows
- * lack one of the three T1 values), the B1 blocks do not share the stencil's
- * rows, or the fit leaves T1 > T2 > 0.
+ * the grid (no neighbour on one side in T1 or T2, an adjacent T2 row lacks
+ * the matched T1, or neither diagonal node exists), the B1 blocks do not
+ * share the stencil's rows, or the fit leaves T1 > T2 > 0.
  *
  * d_maps: device in/out [nvoxels][nmaps] (T1, T2 in columns 0 and 1);
  * d_atoms: device complex [NATOMS][nreps] (normalised or not);

@@ -480,11 +480,11 @@ def refine_start(d_maps, d_img, d_atoms, d_params, d_index, nreps: int, NATOMS: 
                  nvoxels: int, *, nmaps: int = NMAPS, nparams: int = NPARAMS, img_stride: int = 0,
                  d_b1map=None, imag_atoms: bool = False, d_count=None, stream=None) -> None:
     """Sub-grid start for refine_gn, in place: each voxel's matched atom
-    (d_index, int64, as MRF_match writes it) and its 3 x 3 (T1, T2)
+    (d_index, int64, as MRF_match writes it) and its six-point (T1, T2)
     neighbourhood of the dictionary (d_atoms complex [NATOMS][nreps]; with
-    d_b1map, three B1 blocks interpolated to the voxel's B1) interpolated
-    biquadratically in (log T1, log T2); the fit of the voxel maximised over
-    that surrogate replaces (T1, T2) in d_maps.  Voxels on the grid's edge are
+    d_b1map, three B1 blocks interpolated to the voxel's B1) give a quadratic
+    surrogate in (log T1, log T2); the fit of the voxel maximised over that
+    surrogate replaces (T1, T2) in d_maps.  Voxels on the grid's edge are
     left as they are.  imag_atoms: every atom is purely imaginary (zero-phase
     FISP / SR).  d_count: optional device int32 counter of voxels moved."""
     _check(lib().snapmrf_refine_start(_ptr(d_maps), nmaps, _ptr(d_index), _ptr(d_atoms), _ptr(d_params),

@@ -58,8 +58,8 @@ def match_f64(orc, img, atoms, params, natoms, b1map):
 
 @pytest.mark.parametrize("with_map", [False, True])
 def test_start_oracle_lands_near_the_truth(oracle, with_map):
-    """Noise-free voxels: where the true (T1, T2) lies inside the matched
-    atom's stencil, the surrogate's optimum is within 1e-4 of it (5e-4 with
+    """Noise-free voxels: where the true (T1, T2) lies within a grid step of
+    the matched atom, the surrogate's optimum is within 1e-4 of it (5e-4 with
     the quadratic in B1 across blocks 0.02 apart; the grid point is up to
     2.5 % away); where the match landed more than a grid step
     from the truth (a correlated T1-T2 valley, or the B1 of the block away
