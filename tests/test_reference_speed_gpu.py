@@ -4,8 +4,8 @@ on the same GPU: 6,659 atoms (-t 100:55:5000 -s 10:22:2000, epg_fisp, w = 50,
 T = 1000) and 240 x 240 noisy voxels, no B1 map.  Criteria: the same
 (T1, T2, B0, B1) on >= 99.9 % of the voxels, and this package's dictionary
 and matching (FP32, CUDA events, first-call costs and the image upload
-included) each faster than the reference's (its clock() times).  The
-timings are printed.  Skipped where oracle/_ref was not built."""
+included) each faster than the reference's (its clock() times), the faster
+of two runs of each program.  The timings are printed.  Skipped where oracle/_ref was not built."""
 import re
 import subprocess
 from pathlib import Path
@@ -47,8 +47,13 @@ def test_mrf_faster_than_rebuilt_reference_same_maps(snap, tmp_path):
     noise = 0.002 * np.abs(img).mean() * (rng.standard_normal(img.shape) + 1j * rng.standard_normal(img.shape))
     snap.ra_write(str(tmp_path / "img.ra"), (img + noise).astype(np.complex64).reshape(240, 240, T))
     del img, noise
-    ref = _run(REF, grid + ["sched.csv", "img.ra", "-m", "maps_ref.ra"], tmp_path)
-    ours = _run(CLI, grid + ["sched.csv", "img.ra", "-m", "maps_ours.ra"], tmp_path)
+    # each program twice, its faster run kept (the times include reading and
+    # uploading a 461 MB image, where one slow run of the host can cost
+    # either side a few hundred ms)
+    runs_ref = [_run(REF, grid + ["sched.csv", "img.ra", "-m", "maps_ref.ra"], tmp_path) for _ in range(2)]
+    runs_ours = [_run(CLI, grid + ["sched.csv", "img.ra", "-m", "maps_ours.ra"], tmp_path) for _ in range(2)]
+    ref = {k: min(r[k] for r in runs_ref) for k in runs_ref[0]}
+    ours = {k: min(r[k] for r in runs_ours) for k in runs_ours[0]}
     print(f"reference (rebuilt, clock()): {ref}; this package (CUDA events): {ours}")
     mr = snap.ra_read(str(tmp_path / "maps_ref.ra")).reshape(-1, 5)
     mo = snap.ra_read(str(tmp_path / "maps_ours.ra")).reshape(-1, 5)
