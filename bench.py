@@ -730,11 +730,13 @@ def run_ours(args) -> None:
                             achieved_convention=round(nvox * 8.0 * T * natoms / (match_ms / 1e3) / 1e12, 2),
                             convention_note="8 T flop per voxel-atom pair (complex scores); purely imaginary "
                                             "atoms execute 4 T")
-        rl_gn = roofline("gn_kernel<7, tangents>: one Gauss-Newton pass over every voxel", "fp32",
+        rl_gn = roofline("gn_kernel<5, tangents> (5 lanes x 5 state pairs per voxel) and its tail launch: "
+                         "one Gauss-Newton pass over every voxel", "fp32",
                          nvox * T * NSTATES * GN_FLOP_PER_STATE_STEP, gn_pass_ms, fp32_peak, fp32_note,
                          note="78 flop per state-step at the pipe's rate (signal and two tangents); the "
-                              f"refinement runs up to {args.gn_iters} such passes over the voxels still moving "
-                              f"({gn_ms:.2f} ms in the step)")
+                              "refinement stage is the sub-grid start "
+                              f"({fms[HEAD]['start']:.2f} ms) and up to {args.gn_iters} such passes over the "
+                              f"voxels still moving ({gn_ms:.2f} ms in the step)")
         rls = sorted([(gn_ms, rl_gn), (dict_ms, rl_dict), (match_ms, rl_match)], key=lambda x: -x[0])
         rl_fp32 = roofline("match_fp32_kernel<imag>: FP32 B1-bin match (fp32 form), whole call", "fp32",
                            nvox * 4.0 * T * natoms, fms["fp32"]["match"], fp32_peak, fp32_note)
