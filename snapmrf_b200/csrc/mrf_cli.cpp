@@ -64,9 +64,11 @@ static void usage() {
             "\t    --max-rank r\t\t largest rank --compress may keep (default 64)\n"
             "\t    --out-basis <rafile>\t the bases U_r, complex (nreps, r x B1 blocks)\n"
             "\t    --out-compressed <rafile>\t the compressed atoms, complex (r, NATOMS)\n"
-            "\t    --refine n\t\t\t Gauss-Newton refinement of T1/T2 after matching, at\n"
-            "\t\t\t\t\t most n iterations per voxel (epg_fisp / epg_sr with\n"
-            "\t\t\t\t\t every RF phase 0; flip angle x B1 as --all-b1-blocks)\n"
+            "\t    --refine n\t\t\t Gauss-Newton refinement after matching, at most n\n"
+            "\t\t\t\t\t iterations per voxel, from a sub-grid start taken\n"
+            "\t\t\t\t\t from the dictionary (epg_fisp / epg_sr with every\n"
+            "\t\t\t\t\t RF phase 0, flip angle x B1 as --all-b1-blocks:\n"
+            "\t\t\t\t\t T1, T2; epg_ssfp: also B0 and B1)\n"
             "\t-h, --help\t\t\t show this help\n");
 }
 
@@ -340,6 +342,13 @@ int main(int argc, char **argv) {
         }
         float *d_maps;
         cuda_check(cudaMalloc((void **)&d_maps, nmaps * nvoxels * sizeof(float)), "cudaMalloc");
+        // the refinement starts from the matched atom's neighbourhood of the
+        // dictionary, which needs the match's atom index
+        int64_t *d_index = NULL;
+        if (refine > 0) {
+            cuda_check(cudaMalloc((void **)&d_index, nvoxels * sizeof(int64_t)), "cudaMalloc");
+            mopt.d_index = d_index;
+        }
         printf("Matching...\n");
         cudaEventRecord(e0, st);
         check(snapmrf_mrf_match(d_maps, reinterpret_cast<const float *>(img.data), 1, d_atoms, d_params,
@@ -361,8 +370,12 @@ int main(int argc, char **argv) {
                 cuda_check(cudaMemcpyAsync(d_b1, b1ra.data, nvoxels * sizeof(float), cudaMemcpyHostToDevice, st),
                            "cudaMemcpy");
             }
-            printf("Refining (Gauss-Newton, at most %d iterations)...\n", refine);
+            printf("Refining (sub-grid start from the dictionary, then Gauss-Newton, at most %d iterations)...\n",
+                   refine);
             cudaEventRecord(e0, st);
+            check(snapmrf_refine_start(d_maps, nmaps, d_index, d_atoms, d_params, nparams, nreps, NATOMS, natoms,
+                                       d_img, nt, nvoxels, d_b1, 0, NULL, st),
+                  "refine_start");
             check(snapmrf_refine_gn(d_maps, nmaps, d_img, nt, d_b1, h_mrf.data(), m, NREPS, nvoxels, nstates,
                                     echo_type, refine, 0.2f, 1e-4f, NULL, st),
                   "refine_gn");
@@ -372,6 +385,7 @@ int main(int argc, char **argv) {
             printf("Elapsed refinement time: %.4f s\n\n", ms / 1e3);
             cudaFree(d_img);
             if (d_b1) cudaFree(d_b1);
+            cudaFree(d_index);
         }
         if (!out_maps) out_maps = "../result/maps.ra";
         printf("Output maps: %s\n", out_maps);
