@@ -429,7 +429,7 @@ __device__ __forceinline__ void p_rf(Pair3<P> &x, float2 c, float2 s, float2 nS,
 // width; a group's ends replace what they receive.
 template <int P>
 __device__ __forceinline__ void p_shift(Pair3<P> &x, int gl, int L, int w, const float2 *keep, int src_up,
-                                        int src_dn) {
+                                        int src_dn, bool padded) {
     const unsigned full = 0xffffffffu;
     const float up = __shfl_sync(full, x.p[P - 1].y, src_up);
     const float dn = __shfl_sync(full, x.m[0].x, src_dn);
@@ -441,8 +441,11 @@ __device__ __forceinline__ void p_shift(Pair3<P> &x, int gl, int L, int w, const
     for (int i = 0; i < P - 1; i++) x.m[i] = make_float2(x.m[i].y, x.m[i + 1].x);
     x.m[P - 1] = make_float2(x.m[P - 1].y, (gl == L - 1) ? 0.f : dn);
     if (gl == 0) x.p[0].x = -((w == 1) ? old_m0 : x.m[0].x);
+    // (no slot w without padding: the last lane's F- takes a zero instead)
+    if (padded) {
 #pragma unroll
-    for (int i = 0; i < P; i++) x.p[i] = __fmul2_rn(x.p[i], keep[i]);
+        for (int i = 0; i < P; i++) x.p[i] = __fmul2_rn(x.p[i], keep[i]);
+    }
 }
 
 // Per-step constants of one voxel, staged in shared memory per chunk.
@@ -466,7 +469,9 @@ constexpr int kGnChunk = 16;
 // chunks of `chunk` steps.
 // (five pairs: at most 170 registers, so that three warps fit on an SM
 // sub-partition)
-template <int P, bool TANGENTS>
+// PAD: the layout has slots past the last state (L * 2P > w), whose F+ slot
+// w the shift must clear.
+template <int P, bool TANGENTS, bool PAD = true>
 __global__ void __launch_bounds__(kGnThreads, P == 5 ? 12 * 32 / kGnThreads : 1) gn_kernel(GnArgs a, int chunk) {
     extern __shared__ __align__(16) unsigned char gn_smem[];
     const int L = a.L, gpw = 32 / L, apc = gn_voxels_per_cta(L);
@@ -517,6 +522,7 @@ __global__ void __launch_bounds__(kGnThreads, P == 5 ? 12 * 32 / kGnThreads : 1)
     const bool active = !idle && sV[4 * g + 3] != 0.f;
     const int T = a.sch.nreps, w = a.w;
     const int k0 = gl * 2 * P;
+    constexpr bool padded = PAD;
     float2 keep[P];
 #pragma unroll
     for (int i = 0; i < P; i++)
@@ -590,10 +596,10 @@ __global__ void __launch_bounds__(kGnThreads, P == 5 ? 12 * 32 / kGnThreads : 1)
                 }
             }
             if (a.shift) {
-                p_shift<P>(sv, gl, L, w, keep, src_up, src_dn);
+                p_shift<P>(sv, gl, L, w, keep, src_up, src_dn, padded);
                 if (TANGENTS) {
-                    p_shift<P>(s1, gl, L, w, keep, src_up, src_dn);
-                    p_shift<P>(s2, gl, L, w, keep, src_up, src_dn);
+                    p_shift<P>(s1, gl, L, w, keep, src_up, src_dn, padded);
+                    p_shift<P>(s2, gl, L, w, keep, src_up, src_dn, padded);
                 }
             }
             // relaxation over TR
@@ -1045,16 +1051,25 @@ static void choose(int w, int *L, int *S) {
     default: KERNEL<8><<<GRID, kThreads, 0, ST>>>(ARGS); break;           \
     }
 
-#define SNAPMRF_GN_DISPATCH(P, B, GRID, SMEM, ST, ARGS, CHUNK)                      \
-    switch (P) {                                                                    \
-    case 1: gn_kernel<1, B><<<GRID, kGnThreads, SMEM, ST>>>(ARGS, CHUNK); break;      \
-    case 2: gn_kernel<2, B><<<GRID, kGnThreads, SMEM, ST>>>(ARGS, CHUNK); break;      \
-    case 3: gn_kernel<3, B><<<GRID, kGnThreads, SMEM, ST>>>(ARGS, CHUNK); break;      \
-    case 4: gn_kernel<4, B><<<GRID, kGnThreads, SMEM, ST>>>(ARGS, CHUNK); break;      \
-    case 5: gn_kernel<5, B><<<GRID, kGnThreads, SMEM, ST>>>(ARGS, CHUNK); break;      \
-    case 6: gn_kernel<6, B><<<GRID, kGnThreads, SMEM, ST>>>(ARGS, CHUNK); break;      \
-    default: gn_kernel<7, B><<<GRID, kGnThreads, SMEM, ST>>>(ARGS, CHUNK); break;     \
+#define SNAPMRF_GN_DISPATCH_PAD(P, B, PAD, GRID, SMEM, ST, ARGS, CHUNK)                   \
+    switch (P) {                                                                         \
+    case 1: gn_kernel<1, B, PAD><<<GRID, kGnThreads, SMEM, ST>>>(ARGS, CHUNK); break;      \
+    case 2: gn_kernel<2, B, PAD><<<GRID, kGnThreads, SMEM, ST>>>(ARGS, CHUNK); break;      \
+    case 3: gn_kernel<3, B, PAD><<<GRID, kGnThreads, SMEM, ST>>>(ARGS, CHUNK); break;      \
+    case 4: gn_kernel<4, B, PAD><<<GRID, kGnThreads, SMEM, ST>>>(ARGS, CHUNK); break;      \
+    case 5: gn_kernel<5, B, PAD><<<GRID, kGnThreads, SMEM, ST>>>(ARGS, CHUNK); break;      \
+    case 6: gn_kernel<6, B, PAD><<<GRID, kGnThreads, SMEM, ST>>>(ARGS, CHUNK); break;      \
+    default: gn_kernel<7, B, PAD><<<GRID, kGnThreads, SMEM, ST>>>(ARGS, CHUNK); break;     \
     }
+// (the layout's padding, L * 2P > w, picks the kernel that clears slot w)
+#define SNAPMRF_GN_DISPATCH(P, B, GRID, SMEM, ST, ARGS, CHUNK)                              \
+    do {                                                                                 \
+        if ((ARGS).L * 2 * (P) > (ARGS).w) {                                             \
+            SNAPMRF_GN_DISPATCH_PAD(P, B, true, GRID, SMEM, ST, ARGS, CHUNK);             \
+        } else {                                                                         \
+            SNAPMRF_GN_DISPATCH_PAD(P, B, false, GRID, SMEM, ST, ARGS, CHUNK);            \
+        }                                                                                \
+    } while (0)
 
 // Resident CTAs per SM of gn_kernel<P, true> with `smem` bytes.
 static cudaError_t gn_occupancy(int P, size_t smem, int *per_sm) {
