@@ -528,8 +528,11 @@ __global__ void __launch_bounds__(kGnThreads, P == 5 ? 12 * 32 / kGnThreads : 1)
     const int g = (tid >> 5) * gpw + min(lane / L, gpw - 1);
     const bool lane0 = gl == 0;
     const int src_up = gl == 0 ? lane : lane - 1, src_dn = lane + 1 < 32 ? lane + 1 : lane;
-    GnStep *sQ = reinterpret_cast<GnStep *>(gn_smem);              // [apc][chunk]
-    float *sV = reinterpret_cast<float *>(sQ + apc * chunk);       // [apc][4]: T1, T2, B1, ok
+    // [apc][chunk] steps, each voxel's row padded by 16 bytes so that the
+    // voxels of a warp read different banks
+    const int qrow = chunk * (int)sizeof(GnStep) + 16;
+    auto step_row = [&](int ga) { return reinterpret_cast<GnStep *>(gn_smem + (size_t)ga * qrow); };
+    float *sV = reinterpret_cast<float *>(gn_smem + (size_t)apc * qrow);  // [apc][4]: T1, T2, B1, ok
     long long *sI = reinterpret_cast<long long *>(sV + apc * 4);  // [apc]: voxel or -1
     const long long nlist = a.list_in ? (long long)*a.count_in : a.nvox;
     long long first = 0, end = nlist;
@@ -626,10 +629,10 @@ __global__ void __launch_bounds__(kGnThreads, P == 5 ? 12 * 32 / kGnThreads : 1)
             if (vv >= 0) xv = a.img[vv * a.img_stride + t];
             q.xr = xv.x;
             q.xi = xv.y;
-            sQ[ga * chunk + i] = q;
+            step_row(ga)[i] = q;
         }
         __syncthreads();
-        const GnStep *qs = sQ + g * chunk;
+        const GnStep *qs = step_row(g);
         for (int i = 0; i < nch; i++) {
             const GnStep &q = qs[i];
             FoldedRF k;
@@ -1351,7 +1354,7 @@ extern "C" int snapmrf_refine_gn(float *d_maps, int nmaps, const float *img, siz
     const int apc = gn_voxels_per_cta(L);
     // steps staged per chunk: at most kGnChunk, within 48 KB of shared memory
     auto smem_for = [&](int apc_, int *chunk_) {
-        const size_t fixed = (size_t)apc_ * (4 * sizeof(float) + sizeof(long long));
+        const size_t fixed = (size_t)apc_ * (4 * sizeof(float) + sizeof(long long) + 16);
         *chunk_ = (int)std::min<size_t>(kGnChunk, (48 * 1024 - fixed) / ((size_t)apc_ * sizeof(GnStep)));
         return (size_t)apc_ * *chunk_ * sizeof(GnStep) + fixed;
     };
