@@ -495,16 +495,12 @@ __device__ __forceinline__ void p_shift(Pair3<P> &x, int gl, int L, int w, const
 // so it commutes with the dephasing shift: relax(TE), shift, relax(TR-TE)
 // equals shift, relax(TR), and the readout after relax(TE) is E2(TE) f+[0]
 // taken right after the RF pulse.
-// The relaxation over the previous interval (TR_{t-1}; none before the
-// first pulse) is folded into step t's RF coefficients, which are formed
-// once per voxel and step when the chunk is staged, as packed pairs for the
-// two-wide instructions of every lane of the voxel.
-struct __align__(16) GnStep {
-    float2 c, s, nS, hS, C, e2;  // folded RF: c E2, s E2, -S E1, hS E2, C E1, E2
-    float2 cu, su, hSu;          // the unscaled c, s, hS (T2 tangent, relaxed before its RF)
-    float2 nSd, Cd, dE2;         // T1 tangent's source: -S dE1, C dE1; T2 tangent's dE2
-    float S, Cc, rec, dE1;       // sin, cos of alpha_t B1; recovery 1 - E1; dE1
-    float Ea, dEa, xr, xi;       // E2 over TE (readout) and dEa/dT2; voxel sample
+struct GnStep {
+    float C, S;            // cos, sin of alpha_t * B1
+    float E1, E2;          // relaxation over TR
+    float dE1, dE2;        // dE1/dT1, dE2/dT2
+    float Ea, dEa;         // E2 over TE (readout) and dEa/dT2
+    float xr, xi;          // voxel sample
 };
 
 constexpr int kGnChunk = 16;
@@ -596,32 +592,15 @@ __global__ void __launch_bounds__(kGnThreads, P == 5 ? 12 * 32 / kGnThreads : 1)
             const float T1 = sV[4 * ga], T2 = sV[4 * ga + 1], B1 = sV[4 * ga + 2];
             const int t = t0 + i;
             GnStep q;
-            float Sn, Cs;
-            __sincosf(a.sch.alpha[t] * B1, &Sn, &Cs);
+            __sincosf(a.sch.alpha[t] * B1, &q.S, &q.C);
             // the relaxation folded into this step's RF is the previous
             // interval's (none before the first pulse: E = 1, dE = 0)
             const float ta = a.sch.TE[t], tr = t > 0 ? a.sch.TR[t - 1] : 0.f;
             const float r1 = 1.f / T1, r2 = 1.f / T2;
-            const float E1 = __expf(-tr * r1), E2 = __expf(-tr * r2);
-            const float dE1 = E1 * tr * r1 * r1, dE2 = E2 * tr * r2 * r2;
-            const float cc = (1 + Cs) / 2, ss = (1 - Cs) / 2, hS = 0.5f * Sn;
-            auto two = [](float x) { return make_float2(x, x); };
-            q.c = two(cc * E2);
-            q.s = two(ss * E2);
-            q.nS = two(-Sn * E1);
-            q.hS = two(hS * E2);
-            q.C = two(Cs * E1);
-            q.e2 = two(E2);
-            q.cu = two(cc);
-            q.su = two(ss);
-            q.hSu = two(hS);
-            q.nSd = two(-Sn * dE1);
-            q.Cd = two(Cs * dE1);
-            q.dE2 = two(dE2);
-            q.S = Sn;
-            q.Cc = Cs;
-            q.rec = 1.f - E1;
-            q.dE1 = dE1;
+            q.E1 = __expf(-tr * r1);
+            q.E2 = __expf(-tr * r2);
+            q.dE1 = q.E1 * tr * r1 * r1;
+            q.dE2 = q.E2 * tr * r2 * r2;
             q.Ea = __expf(-ta * r2);
             q.dEa = q.Ea * ta * r2 * r2;
             const long long vv = sI[ga];
@@ -634,46 +613,52 @@ __global__ void __launch_bounds__(kGnThreads, P == 5 ? 12 * 32 / kGnThreads : 1)
         __syncthreads();
         const GnStep *qs = step_row(g);
         for (int i = 0; i < nch; i++) {
-            const GnStep &q = qs[i];
+            const GnStep q = qs[i];
+            const float cc = (1 + q.C) / 2, ss = (1 - q.C) / 2, hS = 0.5f * q.S;
+            // RF coefficients with the previous interval's relaxation folded in
             FoldedRF k;
-            k.c = q.c;
-            k.s = q.s;
-            k.nS = q.nS;
-            k.hS = q.hS;
-            k.C = q.C;
-            k.e2 = q.e2;
-            const float rec = q.rec;
+            k.c = make_float2(cc * q.E2, cc * q.E2);
+            k.s = make_float2(ss * q.E2, ss * q.E2);
+            k.nS = make_float2(-q.S * q.E1, -q.S * q.E1);
+            k.hS = make_float2(hS * q.E2, hS * q.E2);
+            k.C = make_float2(q.C * q.E1, q.C * q.E1);
+            k.e2 = make_float2(q.E2, q.E2);
+            // the signal's recovery 1 - E1 on state 0's Z, through the RF's Z column
+            const float rec = 1.f - q.E1;
             if (TANGENTS) {
                 // T2 tangent, relaxed first (product rule on the pre-relaxation
-                // signal: F+- += dE2 f+-), then the folded RF with E2 = 1 on
-                // F+- (already relaxed) and E1 on Z
+                // signal: F+- += dE2 f+-), then the same folded RF
+                const float2 de2 = make_float2(q.dE2, q.dE2), e2 = make_float2(q.E2, q.E2);
 #pragma unroll
                 for (int j = 0; j < P; j++) {
-                    s2.p[j] = __ffma2_rn(q.dE2, sv.p[j], __fmul2_rn(q.e2, s2.p[j]));
-                    s2.m[j] = __ffma2_rn(q.dE2, sv.m[j], __fmul2_rn(q.e2, s2.m[j]));
+                    s2.p[j] = __ffma2_rn(de2, sv.p[j], __fmul2_rn(e2, s2.p[j]));
+                    s2.m[j] = __ffma2_rn(de2, sv.m[j], __fmul2_rn(e2, s2.m[j]));
                 }
+                // (its Z relaxes by E1 only, and F+- were relaxed above: the
+                // folded RF with E2 = 1 on F+- and E1 on Z)
                 FoldedRF k2;
-                k2.c = q.cu;
-                k2.s = q.su;
-                k2.nS = q.nS;
-                k2.hS = q.hSu;
-                k2.C = q.C;
+                k2.c = make_float2(cc, cc);
+                k2.s = make_float2(ss, ss);
+                k2.nS = k.nS;
+                k2.hS = make_float2(hS, hS);
+                k2.C = k.C;
                 k2.e2 = make_float2(1.f, 1.f);
                 p_rf_folded<P>(s2, k2);
                 // T1 tangent: the source dE1 z_signal and the recovery's
                 // derivative -dE1 on state 0
-                p_rf_folded_t1<P>(s1, k, sv.z, q.nSd, q.Cd);
+                p_rf_folded_t1<P>(s1, k, sv.z, make_float2(-q.S * q.dE1, -q.S * q.dE1),
+                                  make_float2(q.C * q.dE1, q.C * q.dE1));
                 if (lane0) {
                     s1.p[0].x = fmaf(q.S, q.dE1, s1.p[0].x);
                     s1.m[0].x = fmaf(-q.S, q.dE1, s1.m[0].x);
-                    s1.z[0].x = fmaf(-q.Cc, q.dE1, s1.z[0].x);
+                    s1.z[0].x = fmaf(-q.C, q.dE1, s1.z[0].x);
                 }
             }
             p_rf_folded<P>(sv, k);
             if (lane0) {
                 sv.p[0].x = fmaf(-q.S, rec, sv.p[0].x);
                 sv.m[0].x = fmaf(q.S, rec, sv.m[0].x);
-                sv.z[0].x = fmaf(q.Cc, rec, sv.z[0].x);
+                sv.z[0].x = fmaf(q.C, rec, sv.z[0].x);
                 // readout s_t = i Ea f+[0] (relaxation over TE)
                 const float f = q.Ea * sv.p[0].x;
                 Ss = fmaf(f, f, Ss);
