@@ -202,31 +202,36 @@ __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
-// One warp per voxel: the stencil, then the system of its surrogate
-// accumulated over the time points and written to a.sys.
-template <bool IMAG>
-__global__ void __launch_bounds__(kWarps * 32) accumulate_kernel(const __grid_constant__ Args a) {
-    const int lane = threadIdx.x & 31;
-    const long long v = (long long)blockIdx.x * kWarps + (threadIdx.x >> 5);
-    if (v >= a.nvox) return;  // whole warps leave together
-    auto leave = [&]() {
-        if (lane == 0) a.sys[kRowT1 * a.nvox + v] = __int_as_float(0x7fc00000);
-    };
+// What the accumulation of one voxel needs: its stencil's rows (per B1
+// block of the stencil) and their weights, the node offsets and the basis
+// coefficients.
+struct Prep {
+    const float2 *rows[3][kPts];
+    float qw[3];
+    int nq;
+    float T1c, T2c, hum, hup, hvm, hvp, hud, hvd, hud2, hvd2, inv_uv;
+    Quad cu, cv;
+};
+
+// The stencil of voxel v and its B1 weights (the whole warp takes part);
+// false: the voxel keeps its grid point.
+__device__ __forceinline__ bool prepare(const Args &a, long long v, int lane, Prep &P) {
     const long long k = a.index[v];
-    if (k < 0 || k >= a.NATOMS) return leave();
+    if (k < 0 || k >= a.NATOMS) return false;
     const float *mp = a.maps + v * a.nmaps;
     const long long b = k / a.natoms, j = k - b * a.natoms, bb = b * a.natoms;
     const float T1c = prm(a, k, 0), T2c = prm(a, k, 1);
     // the maps must still hold the matched grid point
-    if (mp[0] != T1c || mp[1] != T2c || !(T1c > T2c) || !(T2c > 0.f)) return leave();
+    if (mp[0] != T1c || mp[1] != T2c || !(T1c > T2c) || !(T2c > 0.f)) return false;
     long long st[kPts];
     bool diag_up = true;
-    if (!find_stencil(a, bb, j, st, &diag_up)) return leave();
+    if (!find_stencil(a, bb, j, st, &diag_up)) return false;
     // B1 blocks and their weights at the voxel's B1
     const long long nb = a.NATOMS / a.natoms;
-    int nq = 1;
+    P.nq = 1;
     long long qbase[3] = {bb, bb, bb};
-    float qw[3] = {1.f, 0.f, 0.f};
+    P.qw[0] = 1.f;
+    P.qw[1] = P.qw[2] = 0.f;
     if (a.b1map && nb >= 3) {
         const long long bs = min(max(b - 1, 0ll), nb - 3);
         float nodes[3];
@@ -255,25 +260,74 @@ __global__ void __launch_bounds__(kWarps * 32) accumulate_kernel(const __grid_co
             ok = prm(a, r0, 0) == prm(a, r1, 0) && prm(a, r0, 1) == prm(a, r1, 1) &&
                  prm(a, r0, 2) == prm(a, r1, 2) && prm(a, r1, 3) == node;
         }
-        if (!__all_sync(0xffffffffu, ok)) return leave();
-        if (!(nodes[0] != nodes[1] && nodes[1] != nodes[2] && nodes[0] != nodes[2])) return leave();
+        if (!__all_sync(0xffffffffu, ok)) return false;
+        if (!(nodes[0] != nodes[1] && nodes[1] != nodes[2] && nodes[0] != nodes[2])) return false;
         const float bv = a.b1map[v];
-        if (!isfinite(bv)) return leave();
-        lagrange3(nodes, bv, qw);
-        nq = 3;
+        if (!isfinite(bv)) return false;
+        lagrange3(nodes, bv, P.qw);
+        P.nq = 3;
     }
     // node offsets as logs of ratios (exact to rounding) and the basis
     // coefficients along T1, along T2 and of the diagonal
-    const float hum = logf(prm(a, bb + st[kUm], 0) / T1c), hup = logf(prm(a, bb + st[kUp], 0) / T1c);
-    const float hvm = logf(prm(a, bb + st[kVm], 1) / T2c), hvp = logf(prm(a, bb + st[kVp], 1) / T2c);
-    const float hud = diag_up ? hup : hum, hvd = diag_up ? hvp : hvm;
-    const float hud2 = hud * hud, hvd2 = hvd * hvd, inv_uv = 1.f / (hud * hvd);
-    const Quad cu = quad_coeffs(hum, hup), cv = quad_coeffs(hvm, hvp);
-    const float2 *rows[3][kPts];
+    P.T1c = T1c;
+    P.T2c = T2c;
+    P.hum = logf(prm(a, bb + st[kUm], 0) / T1c);
+    P.hup = logf(prm(a, bb + st[kUp], 0) / T1c);
+    P.hvm = logf(prm(a, bb + st[kVm], 1) / T2c);
+    P.hvp = logf(prm(a, bb + st[kVp], 1) / T2c);
+    P.hud = diag_up ? P.hup : P.hum;
+    P.hvd = diag_up ? P.hvp : P.hvm;
+    P.hud2 = P.hud * P.hud;
+    P.hvd2 = P.hvd * P.hvd;
+    P.inv_uv = 1.f / (P.hud * P.hvd);
+    P.cu = quad_coeffs(P.hum, P.hup);
+    P.cv = quad_coeffs(P.hvm, P.hvp);
 #pragma unroll
     for (int q = 0; q < 3; q++)
 #pragma unroll
-        for (int i = 0; i < kPts; i++) rows[q][i] = a.atoms + (qbase[q] + st[i]) * a.atom_stride;
+        for (int i = 0; i < kPts; i++) P.rows[q][i] = a.atoms + (qbase[q] + st[i]) * a.atom_stride;
+    return true;
+}
+
+// The warp's sums of the system to the scratch rows, each value by one lane.
+template <bool IMAG>
+__device__ __forceinline__ void write_system(const Args &a, long long v, int lane, const Prep &P,
+                                             const float *G, const float *Gi, const float *pr, const float *pi) {
+    float *sys = a.sys + v;
+    const long long n = a.nvox;
+    const float hv[8] = {P.T1c, P.T2c, P.hum, P.hup, P.hvm, P.hvp, P.hud, P.hvd};
+#pragma unroll
+    for (int r = 0; r < 8; r++)
+        if ((r & 31) == lane) sys[r * n] = hv[r];
+#pragma unroll
+    for (int r = 0; r < kPts; r++) {
+        if (((kRowPr + r) & 31) == lane) sys[(kRowPr + r) * n] = pr[r];
+        if (((kRowPi + r) & 31) == lane) sys[(kRowPi + r) * n] = pi[r];
+    }
+#pragma unroll
+    for (int r = 0; r < kTri; r++) {
+        if (((kRowG + r) & 31) == lane) sys[(kRowG + r) * n] = G[r];
+        if (!IMAG && ((kRowGi + r) & 31) == lane) sys[(kRowGi + r) * n] = Gi[r];
+    }
+}
+
+// One warp per voxel (complex atoms): the stencil, then the system of its
+// surrogate accumulated over the time points and written to a.sys.
+template <bool IMAG>
+__global__ void __launch_bounds__(kWarps * 32) accumulate_kernel(const __grid_constant__ Args a) {
+    const int lane = threadIdx.x & 31;
+    const long long v = (long long)blockIdx.x * kWarps + (threadIdx.x >> 5);
+    if (v >= a.nvox) return;  // whole warps leave together
+    Prep P;
+    if (!prepare(a, v, lane, P)) {
+        if (lane == 0) a.sys[kRowT1 * a.nvox + v] = __int_as_float(0x7fc00000);
+        return;
+    }
+    const int nq = P.nq;
+    const float *qw = P.qw;
+    const Quad cu = P.cu, cv = P.cv;
+    const float hud = P.hud, hvd = P.hvd, hud2 = P.hud2, hvd2 = P.hvd2, inv_uv = P.inv_uv;
+    const float2 *const(*rows)[kPts] = P.rows;
     const float2 *xv = a.img + v * a.img_stride;
 
     // Hermitian Gram matrix of the basis, sum_t conj(m_r) m_c: real part G
@@ -415,23 +469,152 @@ __global__ void __launch_bounds__(kWarps * 32) accumulate_kernel(const __grid_co
             pr[i] += __shfl_xor_sync(0xffffffffu, pr[i], o);
             pi[i] += __shfl_xor_sync(0xffffffffu, pi[i], o);
         }
-    // the system to the scratch rows, each value by one lane
-    float *sys = a.sys + v;
-    const long long n = a.nvox;
-    const float hv[8] = {T1c, T2c, hum, hup, hvm, hvp, hud, hvd};
-#pragma unroll
-    for (int r = 0; r < 8; r++)
-        if ((r & 31) == lane) sys[r * n] = hv[r];
-#pragma unroll
-    for (int r = 0; r < kPts; r++) {
-        if (((kRowPr + r) & 31) == lane) sys[(kRowPr + r) * n] = pr[r];
-        if (((kRowPi + r) & 31) == lane) sys[(kRowPi + r) * n] = pi[r];
+    write_system<IMAG>(a, v, lane, P, G, Gi, pr, pi);
+}
+
+// cp.async of `size` bytes of which the first `src_bytes` are read and the
+// rest zero-filled (src_bytes 0: zeros, nothing read).
+__device__ __forceinline__ void cp_async4_zfill(void *smem, const void *g, int src_bytes) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"((unsigned)__cvta_generic_to_shared(smem)),
+                 "l"(g), "r"(src_bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async8_zfill(void *smem, const void *g, int src_bytes) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"((unsigned)__cvta_generic_to_shared(smem)),
+                 "l"(g), "r"(src_bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ float2 two(float x) { return make_float2(x, x); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
+
+constexpr int kStagesImag2 = 3;  // slots of 64 staged samples per warp
+
+// One warp per voxel, purely imaginary atoms (zero-phase FISP / SR): each
+// lane takes two adjacent samples of every chunk of 64 as a packed pair, so
+// that the stencil's weights, the basis and the sums run on two-wide FP32
+// instructions, with two partial sums per entry (the even and the odd
+// samples) added at the end.  The imaginary parts of the stencil rows and
+// the voxel samples are staged with cp.async as above; the samples past the
+// last one are zero-filled by the copies, so they add nothing.
+__global__ void __launch_bounds__(kWarps * 32) accumulate_imag_kernel(const __grid_constant__ Args a) {
+    const int lane = threadIdx.x & 31;
+    const long long v = (long long)blockIdx.x * kWarps + (threadIdx.x >> 5);
+    if (v >= a.nvox) return;  // whole warps leave together
+    Prep P;
+    if (!prepare(a, v, lane, P)) {
+        if (lane == 0) a.sys[kRowT1 * a.nvox + v] = __int_as_float(0x7fc00000);
+        return;
     }
+    const int nq = P.nq;
+    const float2 qw0 = two(P.qw[0]), qw1 = two(P.qw[1]), qw2 = two(P.qw[2]);
+    const float2 a1u = two(P.cu.a1), a2u = two(P.cu.a2), b1u = two(P.cu.b1), b2u = two(P.cu.b2);
+    const float2 a1v = two(P.cv.a1), a2v = two(P.cv.a2), b1v = two(P.cv.b1), b2v = two(P.cv.b2);
+    const float2 nhud = two(-P.hud), nhvd = two(-P.hvd), nhud2 = two(-P.hud2), nhvd2 = two(-P.hvd2);
+    const float2 inv_uv = two(P.inv_uv);
+    const float2 *xv = a.img + v * a.img_stride;
+
+    constexpr int kRows = 3 * kPts;
+    constexpr int S = kStagesImag2;
+    extern __shared__ __align__(16) unsigned char rs_smem[];
+    float2 *sa = reinterpret_cast<float2 *>(rs_smem) + (size_t)(threadIdx.x >> 5) * S * kRows * 32;
+    float4 *sx = reinterpret_cast<float4 *>(reinterpret_cast<float2 *>(rs_smem) + (size_t)kWarps * S * kRows * 32) +
+                 (threadIdx.x >> 5) * S * 32;
+    const int nch = (a.T + 63) / 64;
+    auto issue = [&](int kc) {
+        const int t0 = kc * 64 + 2 * lane, slot = kc % S;
+        if (kc < nch) {
+            const int b0 = t0 < a.T ? 4 : 0, b1 = t0 + 1 < a.T ? 4 : 0;
 #pragma unroll
-    for (int r = 0; r < kTri; r++) {
-        if (((kRowG + r) & 31) == lane) sys[(kRowG + r) * n] = G[r];
-        if (!IMAG && ((kRowGi + r) & 31) == lane) sys[(kRowGi + r) * n] = Gi[r];
+            for (int q = 0; q < 3; q++)
+                if (q < nq)
+#pragma unroll
+                    for (int i = 0; i < kPts; i++) {
+                        // (a sample past the end reads nothing: its address is the row's)
+                        const float *g = reinterpret_cast<const float *>(P.rows[q][i]);
+                        float *d = reinterpret_cast<float *>(sa + (slot * kRows + q * kPts + i) * 32 + lane);
+                        cp_async4_zfill(d, g + (b0 ? 2 * t0 + 1 : 1), b0);
+                        cp_async4_zfill(d + 1, g + (b1 ? 2 * t0 + 3 : 1), b1);
+                    }
+            float *dx = reinterpret_cast<float *>(sx + slot * 32 + lane);
+            cp_async8_zfill(dx, xv + (b0 ? t0 : 0), 2 * b0);
+            cp_async8_zfill(dx + 2, xv + (b1 ? t0 + 1 : 0), 2 * b1);
+        }
+        cp_async_commit();
+    };
+#pragma unroll
+    for (int kc = 0; kc < S - 1; kc++) issue(kc);
+
+    float2 G2[kTri], pr2[kPts], pi2[kPts];
+#pragma unroll
+    for (int i = 0; i < kTri; i++) G2[i] = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int i = 0; i < kPts; i++) pr2[i] = pi2[i] = make_float2(0.f, 0.f);
+
+    for (int kc = 0; kc < nch; kc++) {
+        issue(kc + S - 1);  // (an empty group past the end)
+        cp_async_wait<S - 1>();
+        if (kc * 64 + 2 * lane >= a.T) continue;
+        const int slot = kc % S;
+        const float4 x4 = sx[slot * 32 + lane];
+        const float2 xr = make_float2(x4.x, x4.z), nxr = make_float2(-x4.x, -x4.z), xi = make_float2(x4.y, x4.w);
+        float2 sv[kPts];
+#pragma unroll
+        for (int i = 0; i < kPts; i++) {
+            const float2 *d = sa + (slot * kRows + i) * 32 + lane;
+            float2 acc = __fmul2_rn(qw0, d[0]);
+            if (nq > 1) {
+                acc = __ffma2_rn(qw1, d[kPts * 32], acc);
+                acc = __ffma2_rn(qw2, d[2 * kPts * 32], acc);
+            }
+            sv[i] = acc;
+        }
+        // the basis (c, a, b, d, e, f) of both samples
+        float2 m[kPts];
+        const float2 c = sv[kC];
+        const float2 dpu = sub2(sv[kUp], c), dmu = sub2(sv[kUm], c), dpv = sub2(sv[kVp], c), dmv = sub2(sv[kVm], c);
+        m[0] = c;
+        m[1] = __ffma2_rn(b1u, dpu, __fmul2_rn(b2u, dmu));
+        m[3] = __ffma2_rn(a1u, dpu, __fmul2_rn(a2u, dmu));
+        m[2] = __ffma2_rn(b1v, dpv, __fmul2_rn(b2v, dmv));
+        m[4] = __ffma2_rn(a1v, dpv, __fmul2_rn(a2v, dmv));
+        float2 r = sub2(sv[kD], c);
+        r = __ffma2_rn(m[1], nhud, r);
+        r = __ffma2_rn(m[2], nhvd, r);
+        r = __ffma2_rn(m[3], nhud2, r);
+        r = __ffma2_rn(m[4], nhvd2, r);
+        m[5] = __fmul2_rn(r, inv_uv);
+#pragma unroll
+        for (int rr = 0; rr < kPts; rr++) {
+#pragma unroll
+            for (int cc = 0; cc < kPts; cc++)
+                if (cc >= rr) G2[tri(rr, cc)] = __ffma2_rn(m[rr], m[cc], G2[tri(rr, cc)]);
+            // conj(i m) x = (m xi, -m xr)
+            pr2[rr] = __ffma2_rn(m[rr], xi, pr2[rr]);
+            pi2[rr] = __ffma2_rn(m[rr], nxr, pi2[rr]);
+        }
     }
+    float G[kTri], pr[kPts], pi[kPts];
+#pragma unroll
+    for (int i = 0; i < kTri; i++) G[i] = G2[i].x + G2[i].y;
+#pragma unroll
+    for (int i = 0; i < kPts; i++) {
+        pr[i] = pr2[i].x + pr2[i].y;
+        pi[i] = pi2[i].x + pi2[i].y;
+    }
+    // warp sums (every lane ends with the totals)
+#pragma unroll
+    for (int i = 0; i < kTri; i++)
+#pragma unroll
+        for (int o = 16; o; o >>= 1) G[i] += __shfl_xor_sync(0xffffffffu, G[i], o);
+#pragma unroll
+    for (int i = 0; i < kPts; i++)
+#pragma unroll
+        for (int o = 16; o; o >>= 1) {
+            pr[i] += __shfl_xor_sync(0xffffffffu, pr[i], o);
+            pi[i] += __shfl_xor_sync(0xffffffffu, pi[i], o);
+        }
+    write_system<true>(a, v, lane, P, G, nullptr, pr, pi);
 }
 
 // One thread per voxel: Gauss-Newton with variable projection on the
@@ -588,9 +771,13 @@ extern "C" int snapmrf_refine_start(float *d_maps, int nmaps, const int64_t *d_i
     const size_t smem = (size_t)rstart::kWarps * (imag ? rstart::stages<true>() : rstart::stages<false>()) * 32 *
                         (3 * rstart::kPts * (imag ? sizeof(float) : sizeof(float2)) + sizeof(float2));
     if (imag) {
-        SNAPMRF_CUDA(cudaFuncSetAttribute(rstart::accumulate_kernel<true>,
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        rstart::accumulate_kernel<true><<<grid, rstart::kWarps * 32, smem, st>>>(a);
+        // staged pairs of samples: per warp kStagesImag2 x 32 lanes x (3 kPts
+        // pairs of imaginary parts + two complex voxel samples)
+        const size_t smem2 = (size_t)rstart::kWarps * rstart::kStagesImag2 * 32 *
+                             (3 * rstart::kPts * sizeof(float2) + sizeof(float4));
+        SNAPMRF_CUDA(cudaFuncSetAttribute(rstart::accumulate_imag_kernel,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2));
+        rstart::accumulate_imag_kernel<<<grid, rstart::kWarps * 32, smem2, st>>>(a);
         SNAPMRF_LAUNCH_CHECK();
         rstart::solve_kernel<true><<<grid2, 128, 0, st>>>(a);
     } else {
