@@ -448,9 +448,12 @@ def run_ours(args) -> None:
     # per atom) from the dictionary kernel instead of packing the atoms again,
     # and the dictionary normalises only that operand: the FP32 atoms stay as
     # generated, with their norms, which the exact rescoring divides by
+    # (and, zero-phase FISP atoms being purely imaginary, it writes their
+    # imaginary parts as FP32 rows, which the rescoring and the sub-grid start
+    # read at half the bytes of complex rows)
     d_packed = torch.empty((NATOMS, snap.packed_pitch(T)), dtype=torch.int16, device=dev)
     d_norms = torch.empty(NATOMS, dtype=torch.float32, device=dev)
-    flags_packed = snap.DICT_ALL_B1_BLOCKS | snap.DICT_NORMALIZE_OPERAND
+    flags_packed = snap.DICT_ALL_B1_BLOCKS | snap.DICT_NORMALIZE_OPERAND | snap.DICT_IMAG_ROWS
 
     def packs(precision):
         return precision in (snap.PREC_BF16, snap.PREC_FP16)
@@ -463,7 +466,7 @@ def run_ours(args) -> None:
 
     def match_kwargs(precision):
         pk = packs(precision)
-        return dict(flags=MATCH_FLAGS, precision=precision, topk=args.topk,
+        return dict(flags=MATCH_FLAGS | (snap.MATCH_IMAG_ROWS if pk else 0), precision=precision, topk=args.topk,
                     packed_atoms=d_packed if pk else None, atom_norms=d_norms if pk else None)
 
     def step(precision, ev=None, gn=0):
@@ -481,7 +484,7 @@ def run_ours(args) -> None:
             # dictionary, then Gauss-Newton refinement of (T1, T2) at the B1 map
             if not args.no_gn_start:
                 snap.refine_start(d_maps, d_img, d_atoms, d_params, d_index, T, NATOMS, natoms, nvox,
-                                  d_b1map=d_b1, imag_atoms=True)
+                                  d_b1map=d_b1, imag_atoms=True, imag_rows=packs(precision))
             if ev is not None:
                 ev[4].record(stream)
             snap.refine_gn(d_maps, d_img, h_mrf, T, T, nvox, NSTATES, "epg_fisp", iterations=gn,
@@ -650,7 +653,7 @@ def run_ours(args) -> None:
                        img_device_copy=e2e_img[b], upload_early=True, d_index=d_index, **match_kwargs(hprec))
         if not args.no_gn_start:
             snap.refine_start(d_maps, e2e_img[b], d_atoms, e2e_par[b], d_index, T, NATOMS, natoms, nvox,
-                              d_b1map=e2e_b1[b], imag_atoms=True)
+                              d_b1map=e2e_b1[b], imag_atoms=True, imag_rows=packs(hprec))
         snap.refine_gn(d_maps, e2e_img[b], h_mrf, T, T, nvox, NSTATES, "epg_fisp", iterations=args.gn_iters,
                        tol=args.gn_tol, d_b1map=e2e_b1[b])
         h_maps.copy_(d_maps, non_blocking=True)

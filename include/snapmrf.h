@@ -151,6 +151,14 @@ void snapmrf_ra_free(snapmrf_ra *a);
  * d_norms, their norms.  snapmrf_mrf_match takes such a dictionary with
  * snapmrf_match_opts.atom_norms.  Saves rewriting the FP32 atoms. */
 #define SNAPMRF_DICT_NORMALIZE_OPERAND 0x10u
+/* epg_fisp / epg_sr with every RF phase 0 only (their atoms are purely
+ * imaginary): d_atoms receives Im(atom) as FP32 rows, [NATOMS][nreps] float
+ * (half the bytes of the complex rows, whose real parts are zeros), with the
+ * same values bit for bit.  snapmrf_mrf_match reads such rows with
+ * SNAPMRF_MATCH_IMAG_ROWS and snapmrf_refine_start with
+ * SNAPMRF_START_IMAG_ROWS.  Other echo types and schedules fail with
+ * SNAPMRF_ERR_UNSUPPORTED. */
+#define SNAPMRF_DICT_IMAG_ROWS 0x20u
 
 typedef struct snapmrf_dict_opts {
     unsigned flags;  /* SNAPMRF_DICT_* */
@@ -238,6 +246,12 @@ int snapmrf_normalize(float *d_atoms, size_t nreps, size_t NATOMS, float *d_norm
  * that no work queued before this call still uses img_device_copy (for
  * instance by alternating two buffers between calls). */
 #define SNAPMRF_MATCH_UPLOAD_EARLY 0x4u
+/* d_atoms holds Im(atom) rows as SNAPMRF_DICT_IMAG_ROWS writes them
+ * ([NATOMS][atom_stride] float).  Needs SNAPMRF_MATCH_IMAG_ATOMS, BF16 or
+ * FP16 matching and packed_atoms (the atoms are read only by the FP32
+ * rescoring of the candidates); other forms fail with
+ * SNAPMRF_ERR_UNSUPPORTED. */
+#define SNAPMRF_MATCH_IMAG_ROWS 0x8u
 
 typedef struct snapmrf_match_opts {
     int precision;          /* SNAPMRF_PREC_* */
@@ -510,9 +524,13 @@ int snapmrf_refine_gn(float *d_maps, int nmaps, const float *img, size_t img_str
  * img: device complex [nvoxels][img_stride] (0 = nreps);
  * d_b1map: optional device [nvoxels] (needs nparams >= 4);
  * flags: SNAPMRF_START_IMAG_ATOMS when every atom is purely imaginary (the
- * zero-phase FISP / SR dictionaries), which reads and multiplies half as much;
+ * zero-phase FISP / SR dictionaries), which multiplies half as much;
+ * SNAPMRF_START_IMAG_ROWS (with SNAPMRF_START_IMAG_ATOMS) when d_atoms holds
+ * Im(atom) rows as SNAPMRF_DICT_IMAG_ROWS writes them ([NATOMS][nreps]
+ * float), which also reads half as much;
  * d_count: optional device counter, incremented once per voxel moved. */
 #define SNAPMRF_START_IMAG_ATOMS 0x1u
+#define SNAPMRF_START_IMAG_ROWS 0x2u
 int snapmrf_refine_start(float *d_maps, int nmaps, const int64_t *d_index, const float *d_atoms,
                          const float *d_params, int nparams, size_t nreps, size_t NATOMS,
                          size_t natoms, const float *img, size_t img_stride, size_t nvoxels,

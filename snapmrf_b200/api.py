@@ -30,6 +30,7 @@ DICT_NORMALIZE = 0x2
 DICT_REFERENCE_ORDER = 0x4
 DICT_SEPARATE_RELAX = 0x8
 DICT_NORMALIZE_OPERAND = 0x10
+DICT_IMAG_ROWS = 0x20
 # matching
 PREC_FP32 = 0
 PREC_BF16 = 1
@@ -38,7 +39,9 @@ PREC_FP8 = 3
 MATCH_ASSUME_UNIFORM_B1 = 0x1
 MATCH_IMAG_ATOMS = 0x2
 MATCH_UPLOAD_EARLY = 0x4
+MATCH_IMAG_ROWS = 0x8
 START_IMAG_ATOMS = 0x1
+START_IMAG_ROWS = 0x2
 
 ECHO_TYPES = ("epg_ssfp", "roa_ssfp", "epg_sr", "epg_se", "epg_tse1", "epg_tse2", "epg_fisp")
 
@@ -478,7 +481,8 @@ def refine_gn(d_maps, d_img, h_mrf, nreps: int, NREPS: int, nvoxels: int, nstate
 
 def refine_start(d_maps, d_img, d_atoms, d_params, d_index, nreps: int, NATOMS: int, natoms: int,
                  nvoxels: int, *, nmaps: int = NMAPS, nparams: int = NPARAMS, img_stride: int = 0,
-                 d_b1map=None, imag_atoms: bool = False, d_count=None, stream=None) -> None:
+                 d_b1map=None, imag_atoms: bool = False, imag_rows: bool = False, d_count=None,
+                 stream=None) -> None:
     """Sub-grid start for refine_gn, in place: each voxel's matched atom
     (d_index, int64, as MRF_match writes it) and its six-point (T1, T2)
     neighbourhood of the dictionary (d_atoms complex [NATOMS][nreps]; with
@@ -486,10 +490,14 @@ def refine_start(d_maps, d_img, d_atoms, d_params, d_index, nreps: int, NATOMS: 
     surrogate in (log T1, log T2); the fit of the voxel maximised over that
     surrogate replaces (T1, T2) in d_maps.  Voxels on the grid's edge are
     left as they are.  imag_atoms: every atom is purely imaginary (zero-phase
-    FISP / SR).  d_count: optional device int32 counter of voxels moved."""
+    FISP / SR); imag_rows (with imag_atoms): d_atoms holds their Im rows as
+    MRF_dict(flags=DICT_IMAG_ROWS) writes them.  d_count: optional device
+    int32 counter of voxels moved."""
     _check(lib().snapmrf_refine_start(_ptr(d_maps), nmaps, _ptr(d_index), _ptr(d_atoms), _ptr(d_params),
                                       nparams, nreps, NATOMS, natoms, _ptr(d_img), img_stride, nvoxels,
-                                      _ptr(d_b1map), START_IMAG_ATOMS if imag_atoms else 0, _ptr(d_count),
+                                      _ptr(d_b1map),
+                                      (START_IMAG_ATOMS if imag_atoms else 0) | (START_IMAG_ROWS if imag_rows else 0),
+                                      _ptr(d_count),
                                       _stream_ptr(stream)))
 
 

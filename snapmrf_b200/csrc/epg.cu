@@ -68,7 +68,7 @@ __global__ void pack_operand_kernel(EpgArgs a, long long natoms_total) {
     const long long warps = (long long)gridDim.x * (blockDim.x / 32);
     // eight samples per lane and step: four 16-byte loads of the atom row and
     // one 16-byte store of the operand where the row allows it
-    const bool vec = a.nreps % 2 == 0 && reinterpret_cast<uintptr_t>(a.atoms) % 16 == 0 &&
+    const bool vec = a.nreps % (a.imag_rows ? 4 : 2) == 0 && reinterpret_cast<uintptr_t>(a.atoms) % 16 == 0 &&
                      reinterpret_cast<uintptr_t>(a.packed) % 16 == 0 && a.packed_pitch % 8 == 0;
     const long long groups = (a.packed_pitch + 7) / 8;
     for (long long at = blockIdx.x * (long long)(blockDim.x / 32) + (threadIdx.x >> 5); at < natoms_total;
@@ -76,20 +76,34 @@ __global__ void pack_operand_kernel(EpgArgs a, long long natoms_total) {
         float inv = a.norms[at];
         if (inv > 0.f) inv = 1.f / inv;
         const float2 *row = a.atoms + at * a.nreps;
+        const float *irow = reinterpret_cast<const float *>(a.atoms) + at * a.nreps;  // (imaginary rows)
         for (long long gq = lane; gq < groups; gq += 32) {
             const long long q0 = gq * 8;
             float v[8];
             if (vec && q0 + 8 <= a.nreps) {
-                const float4 *r4 = reinterpret_cast<const float4 *>(row + q0);
+                if (a.imag_rows) {
+                    const float4 *r4 = reinterpret_cast<const float4 *>(irow + q0);
 #pragma unroll
-                for (int k = 0; k < 4; k++) {
-                    const float4 x = __ldg(r4 + k);
-                    v[2 * k] = c_scale(make_float2(x.x, x.y), inv).y;
-                    v[2 * k + 1] = c_scale(make_float2(x.z, x.w), inv).y;
+                    for (int k = 0; k < 2; k++) {
+                        const float4 x = __ldg(r4 + k);
+                        v[4 * k] = x.x * inv;
+                        v[4 * k + 1] = x.y * inv;
+                        v[4 * k + 2] = x.z * inv;
+                        v[4 * k + 3] = x.w * inv;
+                    }
+                } else {
+                    const float4 *r4 = reinterpret_cast<const float4 *>(row + q0);
+#pragma unroll
+                    for (int k = 0; k < 4; k++) {
+                        const float4 x = __ldg(r4 + k);
+                        v[2 * k] = c_scale(make_float2(x.x, x.y), inv).y;
+                        v[2 * k + 1] = c_scale(make_float2(x.z, x.w), inv).y;
+                    }
                 }
             } else {
 #pragma unroll
-                for (int k = 0; k < 8; k++) v[k] = q0 + k < a.nreps ? c_scale(row[q0 + k], inv).y : 0.f;
+                for (int k = 0; k < 8; k++)
+                    v[k] = q0 + k >= a.nreps ? 0.f : a.imag_rows ? irow[q0 + k] * inv : c_scale(row[q0 + k], inv).y;
             }
             if (vec) {
                 uint4 w;
@@ -424,9 +438,13 @@ static int dict_impl(float *d_atoms, const float *d_params, const float *h_mrf, 
     a.fine_first = 0;
     a.pack_normalized = pack_normalized ? 1 : 0;
     a.operand_pass = 0;
+    a.imag_rows = (flags & SNAPMRF_DICT_IMAG_ROWS) ? 1 : 0;
     void *d_packed = opts ? opts->d_packed : nullptr;
 
     if (echo == ECHO_ROA) {
+        if (a.imag_rows)
+            SNAPMRF_FAIL(SNAPMRF_ERR_UNSUPPORTED,
+                         "MRF_dict: SNAPMRF_DICT_IMAG_ROWS needs epg_fisp / epg_sr with every RF phase 0");
         if (d_packed)
             SNAPMRF_FAIL(SNAPMRF_ERR_UNSUPPORTED, "MRF_dict: d_packed needs epg_fisp / epg_sr with every RF phase 0");
         if (n_iso > 32 * 8) SNAPMRF_FAIL(SNAPMRF_ERR_UNSUPPORTED, "MRF_dict: n_iso must be <= 256");
@@ -445,6 +463,10 @@ static int dict_impl(float *d_atoms, const float *d_params, const float *h_mrf, 
                      "MRF_dict: nstates must be in [1, %d] for this echo type and schedule "
                      "(up to %d for epg_fisp / epg_sr with all RF phases 0)",
                      32 * kMaxStatesPerLane, 32 * kMaxRealStatesPerLane);
+    if (a.imag_rows && !real_path)
+        SNAPMRF_FAIL(SNAPMRF_ERR_UNSUPPORTED,
+                     "MRF_dict: SNAPMRF_DICT_IMAG_ROWS needs epg_fisp / epg_sr with every RF phase 0 "
+                     "(purely imaginary atoms)");
     if (d_packed) {
         if (!real_path)
             SNAPMRF_FAIL(SNAPMRF_ERR_UNSUPPORTED,

@@ -45,6 +45,9 @@ struct EpgArgs {
     // 1: that operand is written by a separate pass over the finished atoms
     // and their norms (pack_operand_kernel), not by the recursion's kernel
     int operand_pass;
+    // 1: atoms written as Im rows, [blocks][natoms][nreps] float (the
+    // real-valued recursion only; its atoms are purely imaginary)
+    int imag_rows;
 };
 
 // Number of per-(atom, step) factors staged: E1/E2 at TE and at TR-TE, plus
@@ -598,6 +601,7 @@ __device__ __forceinline__ void epg_real_cta(const EpgArgs &a, const int L, cons
 
     float nrm = 0.f;
     float2 *out = a.atoms + gatom * nreps;
+    float *outi = reinterpret_cast<float *>(a.atoms) + gatom * nreps;  // (imaginary rows)
     for (long long t0 = 0; t0 < nreps; t0 += kRealChunk) {
         const int nch = (int)min((long long)kRealChunk, nreps - t0);
         __syncthreads();
@@ -658,7 +662,10 @@ __device__ __forceinline__ void epg_real_cta(const EpgArgs &a, const int L, cons
         if (active)
             for (int q = gl; q < nch; q += L) {
                 const float2 o = sR[g * kRealReadoutStride + q];
-                out[t0 + q] = o;
+                if (a.imag_rows)
+                    outi[t0 + q] = o.y;
+                else
+                    out[t0 + q] = o;
                 if (a.packed && !a.normalize && !a.pack_normalized) store_packed(a, gatom, t0 + q, o.y);
             }
     }
@@ -670,7 +677,14 @@ __device__ __forceinline__ void epg_real_cta(const EpgArgs &a, const int L, cons
             float inv = nrm;
             if (inv > 0.f) inv = 1.f / sqrtf(inv);
             if (active) {
-                if (a.normalize) {
+                if (a.normalize && a.imag_rows) {
+                    // (the same product as the complex row's imaginary part)
+                    for (long long q = gl; q < nreps; q += L) {
+                        const float o = outi[q] * inv;
+                        outi[q] = o;
+                        if (a.packed) store_packed(a, gatom, q, o);
+                    }
+                } else if (a.normalize) {
                     for (long long q = gl; q < nreps; q += L) {
                         const float2 o = c_scale(out[q], inv);
                         out[q] = o;
@@ -679,7 +693,8 @@ __device__ __forceinline__ void epg_real_cta(const EpgArgs &a, const int L, cons
                 } else {
                     // the operand of the unit-norm atom (the same product
                     // as above); the atom itself is not rewritten
-                    for (long long q = gl; q < nreps; q += L) store_packed(a, gatom, q, c_scale(out[q], inv).y);
+                    for (long long q = gl; q < nreps; q += L)
+                        store_packed(a, gatom, q, a.imag_rows ? outi[q] * inv : c_scale(out[q], inv).y);
                 }
             }
         }

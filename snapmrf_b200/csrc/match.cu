@@ -271,6 +271,12 @@ extern "C" int snapmrf_mrf_match(float *d_maps, const float *img, int img_on_hos
     if (atom_norms && (comp || !opts->packed_atoms ||
                        (precision != SNAPMRF_PREC_BF16 && precision != SNAPMRF_PREC_FP16)))
         SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "MRF_match: atom_norms needs BF16 / FP16 matching with packed_atoms");
+    const bool imag_rows = (flags & SNAPMRF_MATCH_IMAG_ROWS) != 0;
+    if (imag_rows && (comp || !opts->packed_atoms || !(flags & SNAPMRF_MATCH_IMAG_ATOMS) ||
+                      (precision != SNAPMRF_PREC_BF16 && precision != SNAPMRF_PREC_FP16)))
+        SNAPMRF_FAIL(SNAPMRF_ERR_UNSUPPORTED,
+                     "MRF_match: SNAPMRF_MATCH_IMAG_ROWS needs BF16 / FP16 matching with packed_atoms and "
+                     "SNAPMRF_MATCH_IMAG_ATOMS");
     if (comp) {
         if (!opts->coeffs || opts->rank < 1 || opts->basis_rows < (size_t)opts->rank ||
             opts->basis_stride < nreps || opts->coeff_stride < (size_t)opts->rank)
@@ -361,6 +367,7 @@ extern "C" int snapmrf_mrf_match(float *d_maps, const float *img, int img_on_hos
         q.imag = (flags & SNAPMRF_MATCH_IMAG_ATOMS) != 0;
         q.packed = opts ? opts->packed_atoms : nullptr;
         q.atom_norms = atom_norms;
+        q.imag_rows = imag_rows;
         if (q.packed && (!q.imag || q.fmt == 2 || opts->packed_nreps != nreps))
             SNAPMRF_FAIL(SNAPMRF_ERR_INVALID,
                          "MRF_match: packed_atoms need SNAPMRF_MATCH_IMAG_ATOMS, BF16 / FP16 and packed_nreps == nreps");

@@ -684,7 +684,9 @@ __global__ void pack_atoms_e4m3_kernel(unsigned char *B, float *ascale2, const f
 // atom index) are rescored.  The map gets the candidate with the largest |s| (lowest
 // atom index on ties, nothing unless |s| > 0, like generate_maps' strict '>'
 // from 0).  VEC: two samples per 16-byte load (strides even, rows aligned).
-template <int TOPK, bool VEC>
+// ROWS: the atoms are Im rows of purely imaginary atoms, [NATOMS][atom_stride]
+// float (SNAPMRF_DICT_IMAG_ROWS); VEC then reads four samples per 16 bytes.
+template <int TOPK, bool VEC, bool ROWS = false>
 __global__ void rescore_kernel(float *maps, long long *index_out, const float *top_s, const int *top_i,
                                const long long *perm, const long long *tile_start, int nbins, const int *vox_bin,
                                const float2 *atoms, long long atom_stride, const float2 *img, long long img_stride,
@@ -747,7 +749,40 @@ __global__ void rescore_kernel(float *maps, long long *index_out, const float *t
     const bool scaled = TOPK != 16 && atom_norms && lane < TOPK && cand >= 0;
     const float my_norm = scaled ? atom_norms[bin * bin_natoms + cand] : 1.f;
     const float2 *x = img + v * img_stride;
-    if (VEC) {
+    if (ROWS) {
+        // s = i d: conj(s) x = (d xi, -d xr)
+        const float *rowf[TOPK];
+#pragma unroll
+        for (int k = 0; k < TOPK; k++)
+            rowf[k] = reinterpret_cast<const float *>(atoms) + (bin * bin_natoms + (ci[k] >= 0 ? ci[k] : 0)) * atom_stride;
+        if (VEC) {
+            const long long n4 = nreps / 4;
+            for (long long t = lane; t < n4; t += 32) {
+                const float4 x0 = reinterpret_cast<const float4 *>(x)[2 * t];
+                const float4 x1 = reinterpret_cast<const float4 *>(x)[2 * t + 1];
+#pragma unroll
+                for (int k = 0; k < TOPK; k++) {
+                    if (ci[k] < 0) continue;
+                    const float4 d = reinterpret_cast<const float4 *>(rowf[k])[t];
+                    re[k] += d.x * x0.y + d.y * x0.w;
+                    im[k] -= d.x * x0.x + d.y * x0.z;
+                    re[k] += d.z * x1.y + d.w * x1.w;
+                    im[k] -= d.z * x1.x + d.w * x1.z;
+                }
+            }
+        } else {
+            for (long long t = lane; t < nreps; t += 32) {
+                const float2 xv = x[t];
+#pragma unroll
+                for (int k = 0; k < TOPK; k++) {
+                    if (ci[k] < 0) continue;
+                    const float d = rowf[k][t];
+                    re[k] += d * xv.y;
+                    im[k] -= d * xv.x;
+                }
+            }
+        }
+    } else if (VEC) {
         const long long n2 = nreps / 2;
         for (long long t = lane; t < n2; t += 32) {
             const float4 xv = reinterpret_cast<const float4 *>(x)[t];
@@ -1071,10 +1106,15 @@ int match_bf16(const TcMatchRequest &q, cudaStream_t st) {
     const float2 *ratoms = rfull ? q.atoms : q.coeffs, *rimg = rfull ? q.img : cimg;
     const long long ras = rfull ? q.atom_stride : q.coeff_stride, ris = rfull ? q.img_stride : rs;
     const long long rn = rfull ? q.nreps : q.rank;
-    const bool vec = rn % 2 == 0 && ras % 2 == 0 && ris % 2 == 0 && reinterpret_cast<uintptr_t>(ratoms) % 16 == 0 &&
-                     reinterpret_cast<uintptr_t>(rimg) % 16 == 0;
-    auto rk = vec ? pick(rescore_kernel<16, true>, rescore_kernel<8, true>, rescore_kernel<4, true>)
-                  : pick(rescore_kernel<16, false>, rescore_kernel<8, false>, rescore_kernel<4, false>);
+    const bool rows = rfull && q.imag_rows;
+    const bool vec = rn % (rows ? 4 : 2) == 0 && ras % (rows ? 4 : 2) == 0 && ris % 2 == 0 &&
+                     reinterpret_cast<uintptr_t>(ratoms) % 16 == 0 && reinterpret_cast<uintptr_t>(rimg) % 16 == 0;
+    auto rk = rows ? (vec ? pick(rescore_kernel<16, true, true>, rescore_kernel<8, true, true>,
+                                 rescore_kernel<4, true, true>)
+                          : pick(rescore_kernel<16, false, true>, rescore_kernel<8, false, true>,
+                                 rescore_kernel<4, false, true>))
+                   : vec ? pick(rescore_kernel<16, true>, rescore_kernel<8, true>, rescore_kernel<4, true>)
+                         : pick(rescore_kernel<16, false>, rescore_kernel<8, false>, rescore_kernel<4, false>);
     rk<<<nblk(cap * 32, 256), 256, 0, st>>>(q.maps, q.index_out, top_s, top_i, perm, tile_start, nbins,
                                             q.b1map ? vox_bin : nullptr, ratoms, ras, rimg, ris, rn, q.params,
                                             q.nparams, bin_natoms, err, rfull ? q.atom_norms : nullptr);

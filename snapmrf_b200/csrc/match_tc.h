@@ -32,6 +32,9 @@ struct TcMatchRequest {
     // optional device [NATOMS]: norms of `atoms`, which are not normalised;
     // the rescoring divides each candidate's inner product by its norm
     const float *atom_norms = nullptr;
+    // `atoms` holds Im rows ([NATOMS][atom_stride] float) of purely
+    // imaginary atoms; only the rescoring reads them (packed operand given)
+    bool imag_rows = false;
 };
 
 // BF16 / FP16 / E4M3 tcgen05 scores + top-k + FP32 rescoring; enqueued on st.

@@ -66,6 +66,7 @@ struct Args {
     const float *b1map;
     int *count;
     float *sys;  // [kSysRows (kSysRowsComplex)][nvox]: the accumulated system per voxel
+    int imag_rows;  // atoms as Im rows, [NATOMS][atom_stride] float
 };
 
 // Rows of the per-voxel system handed from the accumulation to the solve:
@@ -282,10 +283,14 @@ __device__ __forceinline__ bool prepare(const Args &a, long long v, int lane, Pr
     P.inv_uv = 1.f / (P.hud * P.hvd);
     P.cu = quad_coeffs(P.hum, P.hup);
     P.cv = quad_coeffs(P.hvm, P.hvp);
+    // (with Im rows, the float row's start in the same pointer)
 #pragma unroll
     for (int q = 0; q < 3; q++)
 #pragma unroll
-        for (int i = 0; i < kPts; i++) P.rows[q][i] = a.atoms + (qbase[q] + st[i]) * a.atom_stride;
+        for (int i = 0; i < kPts; i++)
+            P.rows[q][i] = a.imag_rows ? reinterpret_cast<const float2 *>(reinterpret_cast<const float *>(a.atoms) +
+                                                                          (qbase[q] + st[i]) * a.atom_stride)
+                                       : a.atoms + (qbase[q] + st[i]) * a.atom_stride;
     return true;
 }
 
@@ -530,11 +535,17 @@ __global__ void __launch_bounds__(kWarps * 32) accumulate_imag_kernel(const __gr
                 if (q < nq)
 #pragma unroll
                     for (int i = 0; i < kPts; i++) {
-                        // (a sample past the end reads nothing: its address is the row's)
+                        // (a sample past the end reads nothing: its address is the row's;
+                        // Im of sample t: g[t] in Im rows, g[2t + 1] in complex rows)
                         const float *g = reinterpret_cast<const float *>(P.rows[q][i]);
                         float *d = reinterpret_cast<float *>(sa + (slot * kRows + q * kPts + i) * 32 + lane);
-                        cp_async4_zfill(d, g + (b0 ? 2 * t0 + 1 : 1), b0);
-                        cp_async4_zfill(d + 1, g + (b1 ? 2 * t0 + 3 : 1), b1);
+                        if (a.imag_rows) {
+                            cp_async4_zfill(d, g + (b0 ? t0 : 0), b0);
+                            cp_async4_zfill(d + 1, g + (b1 ? t0 + 1 : 0), b1);
+                        } else {
+                            cp_async4_zfill(d, g + (b0 ? 2 * t0 + 1 : 1), b0);
+                            cp_async4_zfill(d + 1, g + (b1 ? 2 * t0 + 3 : 1), b1);
+                        }
                     }
             float *dx = reinterpret_cast<float *>(sx + slot * 32 + lane);
             cp_async8_zfill(dx, xv + (b0 ? t0 : 0), 2 * b0);
@@ -737,9 +748,15 @@ extern "C" int snapmrf_refine_start(float *d_maps, int nmaps, const int64_t *d_i
         SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "refine_start: null pointer");
     if (nmaps < 2 || nparams < 3 || (d_b1map && nparams < 4) || nreps == 0 || natoms == 0 || NATOMS % natoms)
         SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "refine_start: bad sizes");
-    if (flags & ~SNAPMRF_START_IMAG_ATOMS) SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "refine_start: unknown flags");
-    if ((reinterpret_cast<uintptr_t>(d_atoms) | reinterpret_cast<uintptr_t>(img)) % sizeof(float2))
-        SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "refine_start: atoms and image must be 8-byte aligned (complex)");
+    if (flags & ~(SNAPMRF_START_IMAG_ATOMS | SNAPMRF_START_IMAG_ROWS))
+        SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "refine_start: unknown flags");
+    if ((flags & SNAPMRF_START_IMAG_ROWS) && !(flags & SNAPMRF_START_IMAG_ATOMS))
+        SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "refine_start: SNAPMRF_START_IMAG_ROWS needs SNAPMRF_START_IMAG_ATOMS");
+    if ((reinterpret_cast<uintptr_t>(d_atoms) | reinterpret_cast<uintptr_t>(img)) %
+        ((flags & SNAPMRF_START_IMAG_ROWS) ? sizeof(float) : sizeof(float2)))
+        SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "refine_start: atoms and image must be aligned to their elements");
+    if (reinterpret_cast<uintptr_t>(img) % sizeof(float2))
+        SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "refine_start: the image must be 8-byte aligned (complex)");
     if (img_stride == 0) img_stride = nreps;
     if (img_stride < nreps) SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "refine_start: img_stride < nreps");
     if (nreps > 0x7fffffff || NATOMS > (size_t)1 << 40 || nvoxels > ((size_t)1 << 31) - 1)
@@ -761,6 +778,7 @@ extern "C" int snapmrf_refine_start(float *d_maps, int nmaps, const int64_t *d_i
     a.nvox = (long long)nvoxels;
     a.b1map = d_b1map;
     a.count = d_count;
+    a.imag_rows = (flags & SNAPMRF_START_IMAG_ROWS) ? 1 : 0;
     const bool imag = flags & SNAPMRF_START_IMAG_ATOMS;
     DeviceScratch sys;
     SNAPMRF_CUDA(sys.alloc(nvoxels * (imag ? rstart::kSysRows : rstart::kSysRowsComplex) * sizeof(float), st));
