@@ -120,4 +120,4 @@ def test_imag_rows_match_and_start_like_complex_rows(snap, prec_name):
     # the rows (two from complex rows), so rounding only
     np.testing.assert_allclose(m_r[:, 4], m_c[:, 4], rtol=1e-6)
     np.testing.assert_array_equal(s_r[:, :4], s_c[:, :4])
-    assert c_r == c_c and c_c > 0.9 * nvox
+    assert c_r == c_c and c_c > 0.7 * nvox  # (voxels next to the small grid's edges keep their grid point)
