@@ -1358,7 +1358,10 @@ extern "C" int snapmrf_refine_gn(float *d_maps, int nmaps, const float *img, siz
     dim3 grid_tail(0);
     {
         const char *e = getenv("SNAPMRF_GN_TAIL");
-        const int L_tail = L < 8 ? 16 : 32;
+        // SNAPMRF_GN_TAIL_LANES overrides the tail's lanes per voxel (tuning)
+        const char *el = getenv("SNAPMRF_GN_TAIL_LANES");
+        int L_tail = L < 8 ? 16 : 32;
+        if (el && atoi(el) > L && atoi(el) <= 32) L_tail = atoi(el);
         P_tail = (nstates + 2 * L_tail - 1) / (2 * L_tail);
         int dev = 0, sms = 0, per_sm = 0;
         if (!(e && atoi(e) == 0) && L_tail > L && P_tail >= 1 && P_tail <= kGnMaxPairs &&
