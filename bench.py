@@ -87,11 +87,13 @@ GN_FLOP_PER_STATE_STEP = 78
 SSFP_FLOP_PER_STATE_STEP = 90
 ROA_FLOP_PER_ISO_STEP = 31
 # DRAM bytes per dictionary atom of the headline dictionary form (T = 1000,
-# w = 50, the 16-bit matching operand of the unit-norm atoms, FP32 atoms as
-# generated) measured by ncu on the reduced workload (5 B1 blocks, 34,690
-# atoms: 241.1 MB read + 306.0 MB written in one launch); traffic grows with
-# the atom count, so a full launch moves this times NATOMS.
-DICT_DRAM_BYTES_PER_ATOM = (241.051904e6 + 305.966080e6) / 34690
+# w = 50: the imaginary parts of the atoms as FP32 rows with their norms, then
+# the 16-bit matching operand of the unit-norm atoms by its own pass) measured
+# by ncu on the reduced workload (5 B1 blocks, 34,690 atoms: the recursion
+# 0.9 MB read + 82.2 MB written, the operand pass 138.9 MB read + 38.3 MB
+# written); traffic grows with the atom count, so a full call moves this times
+# NATOMS.
+DICT_DRAM_BYTES_PER_ATOM = (0.890368e6 + 82.166016e6 + 138.915328e6 + 38.296320e6) / 34690
 PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
 
 
@@ -724,8 +726,9 @@ def run_ours(args) -> None:
                            convention_note="66 flop per state-step (complex recursion); the real recursion "
                                            "executes 16 (8 FP32-pipe operations)",
                            traffic=round(DICT_DRAM_BYTES_PER_ATOM * NATOMS),
-                           traffic_note="ncu DRAM bytes of the reduced case scaled by atoms; algorithmic "
-                                        f"output {NATOMS * T * 8} B")
+                           traffic_note="ncu DRAM bytes of the reduced case (recursion and operand pass) "
+                                        "scaled by atoms; algorithmic output (imaginary rows and 16-bit "
+                                        f"operand) {NATOMS * (T * 4 + snap.packed_pitch(T) * 2)} B")
         mm_flop = nvox * 4.0 * T * natoms   # purely imaginary atoms: 2 A rows x 1 B row x K = T
         rl_match = roofline(f"bf16 tcgen05 B1-bin match (+ packing, fp32 top-{topk_of('bf16')} rescoring), "
                             "whole call", "tensor", mm_flop, match_ms, pk["bf16_tflops"],
