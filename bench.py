@@ -76,11 +76,12 @@ SNR = 40.0
 # rate of 2 flop per operation.
 FLOP_PER_STATE_STEP = 66
 FLOP_PER_STATE_STEP_EXECUTED = 16
-# Gauss-Newton pass (signal + dT1 + dT2 tangents, packed two-wide): per state
-# and step 3 x 8 RF operations, 3 shift masks and 12 relaxation operations
-# with the tangents' product-rule terms = 39 FP32-pipe operations, 78 flop
-# at the pipe's rate.
-GN_FLOP_PER_STATE_STEP = 78
+# Gauss-Newton pass (signal + dT1 + dT2 tangents, packed two-wide, the
+# relaxation folded into the RF): per state and step the signal's RF 8, the
+# T1 tangent's RF with its product-rule source 10, the T2 tangent's
+# relaxation 4 and RF 8 = 30 FP32-pipe operations, 60 flop at the pipe's rate
+# (the unfolded form with the shift mask executed 39).
+GN_FLOP_PER_STATE_STEP = 60
 # bSSFP (complex recursion with B0 precession), convention: RF 54 + two
 # relaxations 12 + two B0 precessions 24 flop; ROA: 31 flop per isochromat
 # and step.
@@ -739,7 +740,7 @@ def run_ours(args) -> None:
         rl_gn = roofline("gn_kernel<5, tangents> (5 lanes x 5 state pairs per voxel) and its tail launch: "
                          "one Gauss-Newton pass over every voxel", "fp32",
                          nvox * T * NSTATES * GN_FLOP_PER_STATE_STEP, gn_pass_ms, fp32_peak, fp32_note,
-                         note="78 flop per state-step at the pipe's rate (signal and two tangents); the "
+                         note="60 flop per state-step at the pipe's rate (signal and two tangents); the "
                               "refinement stage is the sub-grid start "
                               f"({fms[HEAD]['start']:.2f} ms) and up to {args.gn_iters} such passes over the "
                               f"voxels still moving ({gn_ms:.2f} ms in the step)")
