@@ -503,8 +503,7 @@ constexpr int kRealReadoutStride = kRealChunk + 1;  // float2 per group
 inline size_t epg_real_smem_bytes(int L) {
     int apc = kRealThreads / L;
     return (size_t)kRealChunk * 10 * sizeof(float2) + (size_t)apc * kRealFS * sizeof(float) +
-           (size_t)apc * kRealReadoutStride * sizeof(float2) + (size_t)apc * 4 * sizeof(float) +
-           (size_t)apc * (sizeof(int) + sizeof(float)) + sizeof(int);
+           (size_t)apc * kRealReadoutStride * sizeof(float2) + (size_t)apc * 4 * sizeof(float);
 }
 
 // (An explicit minimum of 1 block per SM lets ptxas use more registers and
@@ -557,14 +556,6 @@ __device__ __forceinline__ void epg_real_cta(const EpgArgs &a, const int L, cons
     float *sF = reinterpret_cast<float *>(sC + kRealChunk * 10);   // [apc][FS]
     float2 *sR = reinterpret_cast<float2 *>(sF + apc * FS);    // [apc][kRealReadoutStride]
     float *sP = reinterpret_cast<float *>(sR + apc * kRealReadoutStride);
-    // FOLD: E2 over TR and TE depends on T2 alone, which consecutive atoms of
-    // the table share (T1 is innermost): the factors are formed once per
-    // distinct T2 of the CTA, in slot sL[atom] of the rates sK[slot]
-    int *sL = reinterpret_cast<int *>(sP + apc * 4);
-    float *sK = reinterpret_cast<float *>(sL + apc);
-    int *sNs = reinterpret_cast<int *>(sK + apc);
-    float2 *sFa = reinterpret_cast<float2 *>(sF);                 // [apc][FS / 4]: E1, 1 - E1
-    float2 *sFb = sFa + apc * (FS / 4);                            // [slots][FS / 4]: E2 (TR), E2 (TE)
 
     for (int i = tid; i < apc; i += kRealThreads) {
         long long at = atom0 + i;
@@ -585,17 +576,6 @@ __device__ __forceinline__ void epg_real_cta(const EpgArgs &a, const int L, cons
     const float *TR = a.sched + 2 * nreps;
     const float *TE = a.sched + 3 * nreps;
     __syncthreads();
-    if (FOLD && tid == 0) {
-        int ns = 0;
-        for (int i = 0; i < apc; i++) {
-            if (i == 0 || sP[4 * i + 3] != sP[4 * (i - 1) + 3]) sK[ns++] = sP[4 * i + 3];
-            sL[i] = ns - 1;
-        }
-        *sNs = ns;
-    }
-    __syncthreads();
-    const int nslots = FOLD ? *sNs : 0;
-    const int myslot = FOLD ? sL[g] : 0;
     const int w = a.nstates;
     // TAIL layouts: 0 at slot w (cleared after each shift), 1 elsewhere
     float2 tail_keep = make_float2(1.f, 1.f);
@@ -626,45 +606,30 @@ __device__ __forceinline__ void epg_real_cta(const EpgArgs &a, const int L, cons
         const int nch = (int)min((long long)kRealChunk, nreps - t0);
         __syncthreads();
         for (int i = tid; i < nch; i += kRealThreads) rf_real_coeffs2(alpha[t0 + i], phi[t0 + i], sC + 10 * i);
-        if (FOLD) {
-            // E1 over the previous step's TR (1 before the first step) and
-            // Z0's recovery 1 - E1 per atom; E2 over the previous TR and over
-            // this step's TE per distinct T2; rates as reciprocals (|t / T| <
-            // 1, so the argument's rounding moves exp by far less than an ulp)
-            for (int idx = tid; idx < apc * nch; idx += kRealThreads) {
-                const int ga = idx / nch, i = idx - ga * nch;
+        for (int idx = tid; idx < apc * nch; idx += kRealThreads) {
+            int ga = idx / nch, i = idx - ga * nch;
+            float t1 = sP[4 * ga], t2 = sP[4 * ga + 1];
+            float4 f;
+            if (FOLD) {
+                // (E1, E2) over the previous step's TR (1 before the first
+                // step), E2 over this step's TE, and Z0's recovery 1 - E1;
+                // rates as reciprocals (|t / T| < 1, so the argument's
+                // rounding moves exp by far less than an ulp)
                 const long long t = t0 + i;
                 const float trp = t > 0 ? TR[t - 1] : 0.f;
-                const float e1 = t > 0 ? expf(-trp * sP[4 * ga + 2]) : 1.f;
-                sFa[ga * (FS / 4) + i] = make_float2(e1, 1.f - e1);
+                const float r1 = sP[4 * ga + 2], r2 = sP[4 * ga + 3];
+                const float e1 = t > 0 ? expf(-trp * r1) : 1.f, e2 = t > 0 ? expf(-trp * r2) : 1.f;
+                f = make_float4(e1, e2, expf(-TE[t] * r2), 1.f - e1);
+            } else {
+                float tr = TR[t0 + i], te = TE[t0 + i];
+                float ta = te, tb = tr - te;
+                f = make_float4(expf(-ta / t1), expf(-ta / t2), expf(-tb / t1), expf(-tb / t2));
             }
-            for (int idx = tid; idx < nslots * nch; idx += kRealThreads) {
-                const int k = idx / nch, i = idx - k * nch;
-                const long long t = t0 + i;
-                const float trp = t > 0 ? TR[t - 1] : 0.f;
-                const float r2 = sK[k];
-                sFb[k * (FS / 4) + i] = make_float2(t > 0 ? expf(-trp * r2) : 1.f, expf(-TE[t] * r2));
-            }
-        } else {
-            for (int idx = tid; idx < apc * nch; idx += kRealThreads) {
-                const int ga = idx / nch, i = idx - ga * nch;
-                const float t1 = sP[4 * ga], t2 = sP[4 * ga + 1];
-                const float tr = TR[t0 + i], te = TE[t0 + i];
-                const float ta = te, tb = tr - te;
-                *reinterpret_cast<float4 *>(sF + ga * FS + i * NF) =
-                    make_float4(expf(-ta / t1), expf(-ta / t2), expf(-tb / t1), expf(-tb / t2));
-            }
+            *reinterpret_cast<float4 *>(sF + ga * FS + i * NF) = f;
         }
         __syncthreads();
         for (int i = 0; i < nch; i++) {
-            float4 f;
-            if (FOLD) {
-                // (E1, E2 over TR, E2 over TE, 1 - E1)
-                const float2 fa = sFa[g * (FS / 4) + i], fb = sFb[myslot * (FS / 4) + i];
-                f = make_float4(fa.x, fb.x, fb.y, fa.y);
-            } else {
-                f = *reinterpret_cast<const float4 *>(sF + g * FS + i * NF);
-            }
+            const float4 f = *reinterpret_cast<const float4 *>(sF + g * FS + i * NF);
             if (FOLD) {
                 const float2 *c = sC + 10 * i;
                 const float2 e1 = make_float2(f.x, f.x), e2 = make_float2(f.y, f.y);
