@@ -471,20 +471,46 @@ __global__ void pack_voxels_split_kernel(void *A, const float2 *img, long long i
     if (slot >= nslots) return;
     const long long v = perm[slot];
     const float2 *x = img + (v >= 0 ? v : 0) * img_stride;
+    // two samples per 16-byte load where every row starts 16-byte aligned
+    const bool vec = img_stride % 2 == 0 && reinterpret_cast<uintptr_t>(img) % 16 == 0;
+    const float4 *x4 = reinterpret_cast<const float4 *>(x);
     float n = 0.f;
-    if (v >= 0)
-        for (long long t = lane; t < nreps; t += 32) n += x[t].x * x[t].x + x[t].y * x[t].y;
+    if (v >= 0) {
+        if (vec) {
+            for (long long t = lane; t < nreps / 2; t += 32) {
+                const float4 q = x4[t];
+                n += q.x * q.x + q.y * q.y + q.z * q.z + q.w * q.w;
+            }
+            if ((nreps & 1) && lane == 0) n += x[nreps - 1].x * x[nreps - 1].x + x[nreps - 1].y * x[nreps - 1].y;
+        } else {
+            for (long long t = lane; t < nreps; t += 32) n += x[t].x * x[t].x + x[t].y * x[t].y;
+        }
+    }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) n += __shfl_xor_sync(0xffffffffu, n, o);
     const float inv = n > 0.f ? rsqrtf(n) : 0.f;
     typename P::T *rr = reinterpret_cast<typename P::T *>(A) + (2 * slot) * (Kp / 2);
     typename P::T *ri = rr + Kp / 2;
-    for (long long t = lane; t < Kp / 2; t += 32) {
-        float2 a = make_float2(0.f, 0.f), b = make_float2(0.f, 0.f);
-        if (v >= 0 && 2 * t < nreps) a = x[2 * t];
-        if (v >= 0 && 2 * t + 1 < nreps) b = x[2 * t + 1];
-        rr[t] = P::make(a.x * inv, b.x * inv);
-        ri[t] = P::make(a.y * inv, b.y * inv);
+    // four samples per lane and step: two pairs of each row in one 8-byte store
+    for (long long g = lane; g < Kp / 4; g += 32) {
+        const long long t = 4 * g;
+        float2 s[4];
+        if (vec && v >= 0 && t + 4 <= nreps) {
+            const float4 q0 = x4[2 * g], q1 = x4[2 * g + 1];
+            s[0] = make_float2(q0.x, q0.y);
+            s[1] = make_float2(q0.z, q0.w);
+            s[2] = make_float2(q1.x, q1.y);
+            s[3] = make_float2(q1.z, q1.w);
+        } else {
+#pragma unroll
+            for (int u = 0; u < 4; u++) s[u] = v >= 0 && t + u < nreps ? x[t + u] : make_float2(0.f, 0.f);
+        }
+        const typename P::T r0 = P::make(s[0].x * inv, s[1].x * inv), r1 = P::make(s[2].x * inv, s[3].x * inv);
+        const typename P::T i0 = P::make(s[0].y * inv, s[1].y * inv), i1 = P::make(s[2].y * inv, s[3].y * inv);
+        reinterpret_cast<uint2 *>(rr)[g] =
+            make_uint2(*reinterpret_cast<const uint32_t *>(&r0), *reinterpret_cast<const uint32_t *>(&r1));
+        reinterpret_cast<uint2 *>(ri)[g] =
+            make_uint2(*reinterpret_cast<const uint32_t *>(&i0), *reinterpret_cast<const uint32_t *>(&i1));
     }
 }
 
