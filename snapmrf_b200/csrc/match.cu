@@ -380,6 +380,28 @@ extern "C" int snapmrf_mrf_match(float *d_maps, const float *img, int img_on_hos
         q.topk = (opts && opts->topk) ? opts->topk : (q.fmt == 1 ? 4 : 16);
         if (q.topk != 4 && q.topk != 8 && q.topk != 16)
             SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "MRF_match: topk must be 4, 8 or 16 (got %d)", q.topk);
+        if (img_on_host && up.nchunks >= 4) {
+            // A streamed image: the voxels of all but the last two chunks are
+            // matched as soon as they have arrived (and the work queued
+            // before, such as the dictionary, is done), the rest when the
+            // upload ends, so that only about a quarter of the matching waits
+            // for the last copies.  Each voxel's scores, candidates and
+            // rescoring do not depend on the other voxels of its call.
+            const long long vA = up.first(up.nchunks - 2);
+            SNAPMRF_CUDA(cudaStreamWaitEvent(st, up.ev[up.nchunks - 3], 0));
+            TcMatchRequest qa = q;
+            qa.nvox = vA;
+            int rc = match_bf16(qa, st);
+            if (rc) return rc;
+            SNAPMRF_CUDA(cudaStreamWaitEvent(st, up.done(), 0));
+            TcMatchRequest qb = q;
+            qb.maps = q.maps + vA * 5;
+            qb.index_out = q.index_out ? q.index_out + vA : nullptr;
+            qb.img = q.img + vA * q.img_stride;
+            qb.b1map = q.b1map ? q.b1map + vA : nullptr;
+            qb.nvox = nvox - vA;
+            return match_bf16(qb, st);
+        }
         if (img_on_host) SNAPMRF_CUDA(cudaStreamWaitEvent(st, up.done(), 0));
         return match_bf16(q, st);
     }
