@@ -202,18 +202,19 @@ def test_fp32_imaginary_atom_form_rejects_complex_atoms(snap, oracle):
 
 @pytest.mark.parametrize("prec", [0, 2])
 def test_host_image_streamed_in_chunks(snap, oracle, prec):
-    """A host image of 43 MB (three 16 MB chunks) with padded rows: the
+    """A host image of 72 MB (four chunks of 18 MB) with padded rows: the
     library streams it to the device chunk by chunk on its copy stream and
-    (FP32) matches each chunk as it arrives; maps and indices equal the
-    device-image call's bit for bit, with and without a B1 map, pageable and
-    page-locked, and img_device_copy keeps the uploaded rows.  The
-    tensor-core form with SNAPMRF_MATCH_UPLOAD_EARLY (the upload overlapping
-    the work already queued) gives the same maps too."""
+    (FP32) matches each chunk as it arrives, (tensor cores) the first two
+    chunks' voxels once they have arrived and the rest at the end; maps and
+    indices equal the device-image call's bit for bit, with and without a B1
+    map, pageable and page-locked, and img_device_copy keeps the uploaded
+    rows.  The tensor-core form with SNAPMRF_MATCH_UPLOAD_EARLY (the upload
+    overlapping the work already queued) gives the same maps too."""
     import torch
     T = 600
     b1s = np.float32([0.8, 1.0, 1.2])
     atoms, params, natoms = _dictionary(snap, oracle, b1s=b1s, T=T)
-    nvox = 9000
+    nvox = 15000
     img = np.zeros((nvox, T + 3), np.complex64)
     img[:, :T] = _voxels(atoms, nvox, 21)
     b1map = np.random.default_rng(22).uniform(0.7, 1.3, nvox).astype(np.float32)
