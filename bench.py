@@ -646,11 +646,29 @@ def run_ours(args) -> None:
     k_step = [0]
     hprec = PRECS[HEAD.split("+")[0]]
 
+    # The caller's small uploads (parameter table, B1 map) go on a stream of
+    # their own, so that they do not queue behind the work of the previous
+    # step on the compute stream and then behind the image copies already
+    # started for the next steps; the compute stream waits for them.  Before
+    # a step reuses a pair of buffers, the host waits for the step that last
+    # used them (two steps back), so no early upload overwrites rows that are
+    # still being read.
+    side = torch.cuda.Stream()
+    buf_free = [torch.cuda.Event(), torch.cuda.Event()]
+    buf_used = [False, False]
+
     def e2e_step():
         b = k_step[0] % 2
         k_step[0] += 1
-        e2e_par[b].copy_(h_params, non_blocking=True)
-        e2e_b1[b].copy_(h_b1, non_blocking=True)
+        if buf_used[b]:
+            buf_free[b].synchronize()
+        buf_used[b] = True
+        with torch.cuda.stream(side):
+            e2e_par[b].copy_(h_params, non_blocking=True)
+            e2e_b1[b].copy_(h_b1, non_blocking=True)
+        up = torch.cuda.Event()
+        up.record(side)
+        stream.wait_event(up)
         dict_call(hprec, e2e_par[b])
         snap.MRF_match(d_maps, h_img, d_atoms, e2e_par[b], T, T, NATOMS, natoms, nvox, in_b1map=e2e_b1[b],
                        img_device_copy=e2e_img[b], upload_early=True, d_index=d_index, **match_kwargs(hprec))
@@ -659,6 +677,7 @@ def run_ours(args) -> None:
                               d_b1map=e2e_b1[b], imag_atoms=True, imag_rows=packs(hprec))
         snap.refine_gn(d_maps, e2e_img[b], h_mrf, T, T, nvox, NSTATES, "epg_fisp", iterations=args.gn_iters,
                        tol=args.gn_tol, d_b1map=e2e_b1[b])
+        buf_free[b].record(stream)
         h_maps.copy_(d_maps, non_blocking=True)
 
     e2e_ms = float("nan")
