@@ -489,6 +489,12 @@ __device__ __forceinline__ void cp_async8_zfill(void *smem, const void *g, int s
                  "l"(g), "r"(src_bytes)
                  : "memory");
 }
+// (16 bytes, not kept in L1: the voxel's own samples are read once)
+__device__ __forceinline__ void cp_async16_zfill(void *smem, const void *g, int src_bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"((unsigned)__cvta_generic_to_shared(smem)),
+                 "l"(g), "r"(src_bytes)
+                 : "memory");
+}
 
 __device__ __forceinline__ float2 two(float x) { return make_float2(x, x); }
 __device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
@@ -502,6 +508,11 @@ constexpr int kStagesImag2 = 3;  // slots of 64 staged samples per warp
 // samples) added at the end.  The imaginary parts of the stencil rows and
 // the voxel samples are staged with cp.async as above; the samples past the
 // last one are zero-filled by the copies, so they add nothing.
+//
+// PAIRS: Im rows whose sample pairs are 8-byte aligned (even row stride) and
+// an image whose pairs of complex samples are 16-byte aligned: one copy of a
+// pair per row and one of the voxel's two samples, instead of one per sample.
+template <bool PAIRS>
 __global__ void __launch_bounds__(kWarps * 32) accumulate_imag_kernel(const __grid_constant__ Args a) {
     const int lane = threadIdx.x & 31;
     const long long v = (long long)blockIdx.x * kWarps + (threadIdx.x >> 5);
@@ -539,7 +550,9 @@ __global__ void __launch_bounds__(kWarps * 32) accumulate_imag_kernel(const __gr
                         // Im of sample t: g[t] in Im rows, g[2t + 1] in complex rows)
                         const float *g = reinterpret_cast<const float *>(P.rows[q][i]);
                         float *d = reinterpret_cast<float *>(sa + (slot * kRows + q * kPts + i) * 32 + lane);
-                        if (a.imag_rows) {
+                        if (PAIRS) {
+                            cp_async8_zfill(d, g + (b0 ? t0 : 0), b0 + b1);
+                        } else if (a.imag_rows) {
                             cp_async4_zfill(d, g + (b0 ? t0 : 0), b0);
                             cp_async4_zfill(d + 1, g + (b1 ? t0 + 1 : 0), b1);
                         } else {
@@ -548,8 +561,12 @@ __global__ void __launch_bounds__(kWarps * 32) accumulate_imag_kernel(const __gr
                         }
                     }
             float *dx = reinterpret_cast<float *>(sx + slot * 32 + lane);
-            cp_async8_zfill(dx, xv + (b0 ? t0 : 0), 2 * b0);
-            cp_async8_zfill(dx + 2, xv + (b1 ? t0 + 1 : 0), 2 * b1);
+            if (PAIRS) {
+                cp_async16_zfill(dx, xv + (b0 ? t0 : 0), 2 * (b0 + b1));
+            } else {
+                cp_async8_zfill(dx, xv + (b0 ? t0 : 0), 2 * b0);
+                cp_async8_zfill(dx + 2, xv + (b1 ? t0 + 1 : 0), 2 * b1);
+            }
         }
         cp_async_commit();
     };
@@ -793,9 +810,11 @@ extern "C" int snapmrf_refine_start(float *d_maps, int nmaps, const int64_t *d_i
         // pairs of imaginary parts + two complex voxel samples)
         const size_t smem2 = (size_t)rstart::kWarps * rstart::kStagesImag2 * 32 *
                              (3 * rstart::kPts * sizeof(float2) + sizeof(float4));
-        SNAPMRF_CUDA(cudaFuncSetAttribute(rstart::accumulate_imag_kernel,
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2));
-        rstart::accumulate_imag_kernel<<<grid, rstart::kWarps * 32, smem2, st>>>(a);
+        const bool pairs = a.imag_rows && nreps % 2 == 0 && img_stride % 2 == 0 &&
+                           reinterpret_cast<uintptr_t>(d_atoms) % 8 == 0 && reinterpret_cast<uintptr_t>(img) % 16 == 0;
+        auto kern = pairs ? rstart::accumulate_imag_kernel<true> : rstart::accumulate_imag_kernel<false>;
+        SNAPMRF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2));
+        kern<<<grid, rstart::kWarps * 32, smem2, st>>>(a);
         SNAPMRF_LAUNCH_CHECK();
         rstart::solve_kernel<true><<<grid2, 128, 0, st>>>(a);
     } else {

@@ -168,6 +168,31 @@ def test_start_kernel_matches_fp64_restatement(snap, oracle, with_map, imag):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("T", [400, 401])
+def test_start_from_imaginary_rows_equals_complex_rows(snap, oracle, T):
+    """The start read from the FP32 Im rows (SNAPMRF_START_IMAG_ROWS: with an
+    even T and row stride each lane copies its two samples of a row at once,
+    with an odd T one at a time) equals the start read from the complex
+    rows, bit for bit, and moves the voxels."""
+    import torch
+    w, n = 30, 300
+    c = _device_case(snap, oracle, T, w, n, seed=5, with_map=True, noise=0.02)
+    d_rows = torch.empty((c["NATOMS"], T), dtype=torch.float32, device="cuda")
+    snap.MRF_dict(d_rows, c["d_params"], c["h"], T, T, c["NATOMS"], c["natoms"], 4, w, "epg_fisp",
+                  flags=snap.DICT_ALL_B1_BLOCKS | snap.DICT_NORMALIZE | snap.DICT_IMAG_ROWS)
+    maps0 = c["d_maps"].clone()
+    out = []
+    for atoms, rows in ((c["d_atoms"], False), (d_rows, True)):
+        c["d_maps"].copy_(maps0)
+        snap.refine_start(c["d_maps"], c["d_img"], atoms, c["d_params"], c["d_index"], T, c["NATOMS"],
+                          c["natoms"], n, d_b1map=c["d_b1"], imag_atoms=True, imag_rows=rows)
+        out.append(c["d_maps"].cpu().numpy())
+    m0 = maps0.cpu().numpy()
+    assert np.any(out[0][:, :2] != m0[:, :2], axis=1).mean() > 0.9
+    np.testing.assert_array_equal(out[1], out[0])
+
+
+@pytest.mark.gpu
 def test_start_then_one_pass_reaches_the_converged_fit(snap, oracle):
     """Matched grid point -> start -> one refinement pass lands where FP64
     Gauss-Newton run to convergence from the grid point lands (median 2e-5,
