@@ -859,19 +859,30 @@ __global__ void __launch_bounds__(kEpgThreads) roa_kernel(EpgArgs a) {
     }
 }
 
-// Multi-isochromat ROA: one warp per atom, lanes hold IPL isochromats each.
-// Isochromat j precesses by an extra pi*j/n_iso per half TR (2*pi*j/n_iso
-// per TR, so the n_iso isochromats dephase uniformly across 2*pi); the
-// readout is the mean of Mx + iMy over isochromats.
+// Multi-isochromat ROA: a group of G lanes per atom (G = 8, 16 or 32, a
+// divisor of the warp), IPL isochromats per lane; lane r of a group holds
+// isochromats r*IPL .. r*IPL + IPL - 1 (those past n_iso idle), so that G*IPL
+// close above n_iso wastes few slots (n_iso = 100: 8 x 13 = 104, where 32
+// lanes x 4 carried 128).  Isochromat j precesses by an extra pi*j/n_iso per
+// half TR (2*pi*j/n_iso per TR, so the n_iso isochromats dephase uniformly
+// across 2*pi); the readout is the mean of Mx + iMy over isochromats.  The
+// relaxation over TR is folded into the rotation's rows (E2 into the rows of
+// Mx and My, E1 into Mz's, whose recovery 1 - E1 starts the sum; the row's
+// Mx entry is zero), and the step's relaxation factors and B0 phasor are
+// computed once per atom and step by the group's lanes and staged.
 template <int IPL>
-__global__ void __launch_bounds__(kEpgThreads) roa_iso_kernel(EpgArgs a) {
-    constexpr int WPC = kEpgThreads / 32;
+__global__ void __launch_bounds__(kEpgThreads) roa_iso_kernel(EpgArgs a, int G) {
+    constexpr int MAXA = kEpgThreads / 8;  // atoms per CTA at G = 8
     __shared__ RoaStep sT[kChunk];
-    __shared__ float2 sPart[WPC][kChunk][33];
-    const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
+    // (rows padded by one entry: the groups of a warp read and write
+    // different banks)
+    __shared__ float4 sF[MAXA][kChunk + 1];   // per atom and step: E1, E2, sin, cos of beta
+    __shared__ float2 sOut[MAXA][kChunk + 1];  // the readout
+    const int tid = threadIdx.x;
+    const int apc = kEpgThreads / G, ga = tid / G, r = tid % G;
     const long long blk = blockIdx.y;
     const long long nreps = a.nreps;
-    const long long ab = (long long)blockIdx.x * WPC + warp;
+    const long long ab = (long long)blockIdx.x * apc + ga;
     const bool active = ab < a.natoms;
     const long long gatom = blk * a.natoms + ab;
     float t1 = 1.f, t2 = 1.f, b0 = 0.f;
@@ -885,16 +896,20 @@ __global__ void __launch_bounds__(kEpgThreads) roa_iso_kernel(EpgArgs a) {
     const float *phi = a.sched + nreps;
     const float *TR = a.sched + 2 * nreps;
     const int n_iso = a.n_iso;
+    float i0, i1, i2;
+    roa_init(t1, t2, i0, i1, i2, a.init_alpha_deg, a.init_phi_deg, a.init_ti);
+    // (a slot past n_iso gets a zero rotation: its Mx, My stay 0 after the
+    // first step and its readout adds exactly 0)
     float m0[IPL], m1[IPL], m2[IPL], cd[IPL], sd[IPL];
-    bool valid[IPL];
 #pragma unroll
     for (int q = 0; q < IPL; q++) {
-        int j = lane * IPL + q;
-        valid[q] = j < n_iso;
-        roa_init(t1, t2, m0[q], m1[q], m2[q], a.init_alpha_deg, a.init_phi_deg, a.init_ti);
+        const int j = r * IPL + q;
+        m0[q] = i0;
+        m1[q] = i1;
+        m2[q] = i2;
         double d = M_PI * (double)j / (double)n_iso;
-        cd[q] = (float)cos(d);
-        sd[q] = (float)sin(d);
+        cd[q] = j < n_iso ? (float)cos(d) : 0.f;
+        sd[q] = j < n_iso ? (float)sin(d) : 0.f;
     }
     const float inv_n = 1.f / (float)n_iso;
     float nrm = 0.f;
@@ -903,65 +918,72 @@ __global__ void __launch_bounds__(kEpgThreads) roa_iso_kernel(EpgArgs a) {
         const int nch = (int)min((long long)kChunk, nreps - t0);
         __syncthreads();
         for (int i = tid; i < nch; i += kEpgThreads) roa_matrix(alpha[t0 + i], phi[t0 + i], sT[i].T);
-        // the atom's relaxation and off-resonance factors of step t0 + l are
-        // computed once, by lane l (kChunk <= 32), and broadcast to the warp
-        float e1_l = 1.f, e2_l = 1.f, sb_l = 0.f, cb_l = 1.f;
-        if (lane < nch) {
-            const float tr = TR[t0 + lane];
-            e1_l = expf(-tr / t1);
-            e2_l = expf(-tr / t2);
+        for (int i = r; i < nch; i += G) {
+            const float tr = TR[t0 + i];
+            float sb, cb;
             const float beta = (float)(M_PI * b0 * tr / 1000.f);
-            __sincosf(beta, &sb_l, &cb_l);
+            __sincosf(beta, &sb, &cb);
+            sF[ga][i] = make_float4(expf(-tr / t1), expf(-tr / t2), sb, cb);
         }
         __syncthreads();
         for (int i = 0; i < nch; i++) {
             const float *T = sT[i].T;
-            const float E1 = __shfl_sync(0xffffffffu, e1_l, i), E2 = __shfl_sync(0xffffffffu, e2_l, i);
-            const float sb = __shfl_sync(0xffffffffu, sb_l, i), cb = __shfl_sync(0xffffffffu, cb_l, i);
+            const float4 f = sF[ga][i];
+            const float E1 = f.x, E2 = f.y, sb = f.z, cb = f.w;
+            const float a0 = E2 * T[0], a3 = E2 * T[3], a6 = E2 * T[6];
+            const float a1 = E2 * T[1], a4 = E2 * T[4], a7 = E2 * T[7];
+            const float c5 = E1 * T[5], c8 = E1 * T[8], rec = 1.f - E1;
             float px = 0.f, py = 0.f;
 #pragma unroll
             for (int q = 0; q < IPL; q++) {
-                float n0 = fmaf(T[6], m2[q], fmaf(T[3], m1[q], T[0] * m0[q]));
-                float n1 = fmaf(T[7], m2[q], fmaf(T[4], m1[q], T[1] * m0[q]));
-                float n2 = fmaf(T[8], m2[q], fmaf(T[5], m1[q], T[2] * m0[q]));
-                float x = E2 * n0, y = E2 * n1;
-                m2[q] = E1 * n2 + (1 - E1);
+                const float x = fmaf(a6, m2[q], fmaf(a3, m1[q], a0 * m0[q]));
+                const float y = fmaf(a7, m2[q], fmaf(a4, m1[q], a1 * m0[q]));
+                m2[q] = fmaf(c8, m2[q], fmaf(c5, m1[q], rec));
                 // rotation by beta then by the isochromat's delta
-                float cx = cb * cd[q] - sb * sd[q], sx = sb * cd[q] + cb * sd[q];
-                float w1 = cx * x + sx * y, w2 = cx * y - sx * x;
-                if (valid[q]) {
-                    px += w1;
-                    py += w2;
-                }
+                const float cx = cb * cd[q] - sb * sd[q], sx = sb * cd[q] + cb * sd[q];
+                const float w1 = cx * x + sx * y, w2 = cx * y - sx * x;
+                px += w1;
+                py += w2;
                 m0[q] = cx * w1 + sx * w2;
                 m1[q] = cx * w2 - sx * w1;
             }
-            sPart[warp][i][lane] = make_float2(px, py);
-        }
-        __syncwarp();
-        if (lane < nch) {
-            float sx = 0.f, sy = 0.f;
-            for (int l = 0; l < 32; l++) {
-                float2 v = sPart[warp][lane][l];
-                sx += v.x;
-                sy += v.y;
+            // the group's sum (a group never straddles a warp)
+            for (int o = G / 2; o; o >>= 1) {
+                px += __shfl_xor_sync(0xffffffffu, px, o);
+                py += __shfl_xor_sync(0xffffffffu, py, o);
             }
-            sPart[warp][lane][32] = make_float2(sx * inv_n, sy * inv_n);
+            if (r == 0) sOut[ga][i] = make_float2(px * inv_n, py * inv_n);
         }
         __syncwarp();
-        for (int i = 0; i < nch; i++) {
-            float2 v = sPart[warp][i][32];
-            nrm += v.x * v.x + v.y * v.y;
+        for (int i = r; i < nch; i += G) {
+            const float2 v = sOut[ga][i];
+            nrm = fmaf(v.x, v.x, fmaf(v.y, v.y, nrm));
+            if (active) out[t0 + i] = v;
         }
-        if (active && lane < nch) out[t0 + lane] = sPart[warp][lane][32];
     }
+    for (int o = G / 2; o; o >>= 1) nrm += __shfl_xor_sync(0xffffffffu, nrm, o);
+    if (a.norms && active && r == 0) a.norms[gatom] = sqrtf(nrm);
+    // (with G = 32 a lane rescales samples another lane of the group wrote)
     __syncwarp();
-    if (a.norms && active && lane == 0) a.norms[gatom] = sqrtf(nrm);
     if (a.normalize && active) {
         float inv = nrm;
         if (inv > 0.f) inv = 1.f / sqrtf(inv);
-        for (long long q = lane; q < nreps; q += 32) out[q] = c_scale(out[q], inv);
+        for (long long q = r; q < nreps; q += G) out[q] = c_scale(out[q], inv);
     }
+}
+
+// Isochromats per lane and lanes per atom of roa_iso_kernel: the fewest
+// slots G * IPL >= n_iso (n_iso <= 256), then the most isochromats per lane.
+inline void roa_iso_layout(int n_iso, int *G, int *ipl) {
+    static const int ipls[] = {13, 8, 7, 4, 2, 1};
+    int best = 1 << 30;
+    for (int g : {8, 16, 32})
+        for (int i : ipls)
+            if (g * i >= n_iso && (g * i < best || (g * i == best && i > *ipl))) {
+                best = g * i;
+                *G = g;
+                *ipl = i;
+            }
 }
 
 inline cudaError_t launch_roa(const EpgArgs &a, long long natoms, unsigned gen_blocks,
@@ -970,13 +992,18 @@ inline cudaError_t launch_roa(const EpgArgs &a, long long natoms, unsigned gen_b
         dim3 grid((unsigned)((natoms + kEpgThreads - 1) / kEpgThreads), gen_blocks);
         roa_kernel<<<grid, kEpgThreads, 0, st>>>(a);
     } else {
-        const long long wpc = kEpgThreads / 32;
-        dim3 grid((unsigned)((natoms + wpc - 1) / wpc), gen_blocks);
-        int ipl = (a.n_iso + 31) / 32;
-        if (ipl <= 1) roa_iso_kernel<1><<<grid, kEpgThreads, 0, st>>>(a);
-        else if (ipl <= 2) roa_iso_kernel<2><<<grid, kEpgThreads, 0, st>>>(a);
-        else if (ipl <= 4) roa_iso_kernel<4><<<grid, kEpgThreads, 0, st>>>(a);
-        else roa_iso_kernel<8><<<grid, kEpgThreads, 0, st>>>(a);
+        int G = 32, ipl = 0;
+        roa_iso_layout(a.n_iso, &G, &ipl);
+        const long long apc = kEpgThreads / G;
+        dim3 grid((unsigned)((natoms + apc - 1) / apc), gen_blocks);
+        switch (ipl) {
+        case 1: roa_iso_kernel<1><<<grid, kEpgThreads, 0, st>>>(a, G); break;
+        case 2: roa_iso_kernel<2><<<grid, kEpgThreads, 0, st>>>(a, G); break;
+        case 4: roa_iso_kernel<4><<<grid, kEpgThreads, 0, st>>>(a, G); break;
+        case 7: roa_iso_kernel<7><<<grid, kEpgThreads, 0, st>>>(a, G); break;
+        case 8: roa_iso_kernel<8><<<grid, kEpgThreads, 0, st>>>(a, G); break;
+        default: roa_iso_kernel<13><<<grid, kEpgThreads, 0, st>>>(a, G); break;
+        }
     }
     note_launches(1);
     return cudaGetLastError();
