@@ -98,9 +98,9 @@ def test_ssfp_b0_b1_blocks_vs_oracle(snap, oracle):
     np.testing.assert_allclose(np.linalg.norm(got, axis=1), 1.0, rtol=1e-5)
 
 
-# (1, 2, 4 and 8 isochromats per lane: the one-at-a-time form and the packed
-# pairs of 50, 100 and 200)
-@pytest.mark.parametrize("n_iso", [1, 7, 50, 100, 200])
+# (the single-isochromat kernel, then groups of 8 lanes x 1, 8 x 7, 8 x 13,
+# 16 x 13 and 32 x 8 isochromats per atom)
+@pytest.mark.parametrize("n_iso", [1, 7, 50, 100, 200, 256])
 def test_roa_vs_oracle(snap, oracle, n_iso):
     T = 200
     h = _ssfp_csv(T, 4)
