@@ -536,6 +536,20 @@ int snapmrf_refine_start(float *d_maps, int nmaps, const int64_t *d_index, const
                          size_t natoms, const float *img, size_t img_stride, size_t nvoxels,
                          const float *d_b1map, unsigned flags, int *d_count, void *stream);
 
+/* Forward mode (Jacobian-vector products) of the real FISP / SR recursion.
+ * No counterpart in the reference; the forward model is its epg_fisp / epg_sr
+ * (src/functions.cu:687-933) with flip angle alpha_t * B1 and every RF phase 0.
+ *
+ * d_params: device [natoms][nparams] (T1, T2, B0, B1; nparams >= 4);
+ * h_mrf: host [4][NREPS] schedule as for snapmrf_mrf_dict (row 1 must be 0);
+ * d_out: device out [natoms][3][nreps] = f, df/dT1, df/dT2, where s = i f is
+ * the atom as generated (unnormalised).  The product of the Jacobian with a
+ * direction (dT1, dT2) is dT1 * df/dT1 + dT2 * df/dT2.  echo_type: "epg_fisp"
+ * or "epg_sr"; nstates <= 256. */
+int snapmrf_epg_jvp(const float *d_params, int nparams, const float *h_mrf, size_t nreps,
+                    size_t NREPS, size_t natoms, int nstates, const char *echo_type, float *d_out,
+                    void *stream);
+
 /* Cramer-Rao bound of (T1, T2) and its gradient with respect to the flip-angle
  * schedule, for designing schedules.  No counterpart in the reference.
  *

@@ -5,6 +5,6 @@ from .api import (  # noqa: F401
     MATCH_IMAG_ROWS, MATCH_UPLOAD_EARLY, START_IMAG_ATOMS, START_IMAG_ROWS, refine_start, scratch_allocations, selftest_bounded_wait,
     NMAPS, NOALLOC_MAX_B1_BLOCKS, NOALLOC_MAX_VOXELS, NPARAMS, PREC_BF16, PREC_FP16, PREC_FP32, PREC_FP8, SnapMRFError, MRF_dict,
     MRF_match, MRF_match_noalloc, compute_natoms, csv_dim,
-    csv_read, crb_gradient, device_error, epg_adjoint, grid_params, refine_gn, kernel_launches, lib, packed_pitch, linspace, logspace, normalize, parse_length, parse_params,
+    csv_read, crb_gradient, device_error, epg_adjoint, epg_jvp, grid_params, refine_gn, kernel_launches, lib, packed_pitch, linspace, logspace, normalize, parse_length, parse_params,
     parse_range, ra_read, ra_write, trans_params, Compressed, SVD_IMAG_ATOMS, SVD_MAX_SUBSPACE, svd_compress,
 )

@@ -127,6 +127,7 @@ def lib() -> C.CDLL:
                                                 vp, vp, vp]
         L.snapmrf_epg_adjoint.argtypes = [vp, C.c_int, vp, sz, sz, sz, C.c_int, C.c_char_p, vp, vp, vp,
                                           vp, vp, C.c_int, vp]
+        L.snapmrf_epg_jvp.argtypes = [vp, C.c_int, vp, sz, sz, sz, C.c_int, C.c_char_p, vp, vp]
         L.snapmrf_crb_gradient.argtypes = [vp, C.c_int, vp, sz, sz, sz, C.c_int, C.c_char_p, vp, vp, vp,
                                            C.c_int, vp]
         L.snapmrf_refine_gn.argtypes = [vp, C.c_int, vp, sz, vp, vp, sz, sz, sz, C.c_int, C.c_char_p, C.c_int,
@@ -504,6 +505,17 @@ def refine_start(d_maps, d_img, d_atoms, d_params, d_index, nreps: int, NATOMS: 
 def packed_pitch(nreps: int) -> int:
     """Row pitch (elements) of atoms packed by MRF_dict(d_packed=...)."""
     return int(lib().snapmrf_packed_pitch(nreps))
+
+
+def epg_jvp(d_params, h_mrf, nreps: int, NREPS: int, natoms: int, d_out, nparams: int = NPARAMS,
+            nstates: int = 101, echo_type: str = "epg_fisp", stream=None) -> None:
+    """Forward mode of the real FISP / SR recursion: d_out [natoms][3][nreps]
+    = f, df/dT1, df/dT2 of each atom s = i f as generated (d_params rows T1,
+    T2, B0, B1; flip angle alpha_t * B1).  A Jacobian-vector product along
+    (dT1, dT2) is dT1 * d_out[:, 1] + dT2 * d_out[:, 2]."""
+    h_mrf = _schedule(h_mrf, NREPS)
+    _check(lib().snapmrf_epg_jvp(_ptr(d_params), nparams, h_mrf.ctypes.data, nreps, NREPS, natoms, nstates,
+                                 echo_type.encode(), _ptr(d_out), _stream_ptr(stream)))
 
 
 def crb_gradient(d_params, h_mrf, nreps: int, NREPS: int, ntissues: int, d_loss, d_grad_alpha,

@@ -1421,6 +1421,51 @@ extern "C" int snapmrf_refine_gn(float *d_maps, int nmaps, const float *img, siz
     return SNAPMRF_OK;
 }
 
+// Forward mode: the signal and its T1 / T2 tangents, by the CRB's forward
+// pass (the augmented recursion of aug_step) with one stored state per atom
+// (the state at t = 0; nothing reads it back).
+extern "C" int snapmrf_epg_jvp(const float *d_params, int nparams, const float *h_mrf, size_t nreps,
+                               size_t NREPS, size_t natoms, int nstates, const char *echo_type, float *d_out,
+                               void *stream) {
+    cudaStream_t st = (cudaStream_t)stream;
+    if (!d_params || !h_mrf || !d_out) SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "epg_jvp: null pointer");
+    if (nparams < 4 || nreps == 0 || nreps > NREPS || natoms == 0 || nstates < 1 || nstates > 32 * kMaxS)
+        SNAPMRF_FAIL(SNAPMRF_ERR_INVALID, "epg_jvp: bad sizes");
+    if (nreps > 0x7fffffff || natoms > 0x7fffffff)
+        SNAPMRF_FAIL(SNAPMRF_ERR_UNSUPPORTED, "epg_jvp: too many time points or atoms");
+    const int shift = echo_shift(echo_type);
+    if (shift < 0) SNAPMRF_FAIL(SNAPMRF_ERR_ECHO_TYPE, "epg_jvp: echo type must be epg_fisp or epg_sr");
+    DeviceScratch sbuf;
+    Schedule sc;
+    int rc = upload_schedule(sbuf, &sc, h_mrf, nreps, NREPS, st, "epg_jvp");
+    if (rc) return rc;
+    int L, S;
+    choose(nstates, &L, &S);
+    const size_t LS = (size_t)L * S;
+    DeviceScratch work;
+    SNAPMRF_CUDA(work.alloc(natoms * 9 * LS * sizeof(float), st));
+    CrbArgs a;
+    a.sch = sc;
+    a.params = d_params;
+    a.nparams = nparams;
+    a.n = (long long)natoms;
+    a.w = nstates;
+    a.L = L;
+    a.shift = shift;
+    a.fvec = d_out;
+    a.gvec = nullptr;
+    a.ckpt = work.as<float>();
+    a.seg = nullptr;
+    a.galpha = nullptr;
+    a.C = (int)nreps;  // one checkpoint, at t = 0
+    a.nckpt = 1;
+    const int apc = kThreads / L;
+    dim3 grid((unsigned)((natoms + apc - 1) / apc));
+    SNAPMRF_GRAD_DISPATCH(crb_forward_kernel, S, grid, st, a);
+    SNAPMRF_LAUNCH_CHECK();
+    return SNAPMRF_OK;
+}
+
 extern "C" int snapmrf_crb_gradient(const float *d_params, int nparams, const float *h_mrf, size_t nreps,
                                     size_t NREPS, size_t ntissues, int nstates, const char *echo_type, float *d_loss,
                                     float *d_grad_alpha, float *d_signals, int checkpoint_every, void *stream) {

@@ -175,3 +175,15 @@ def test_normalize_operand_argument_errors_without_gpu(snap):
                dict(precision=snap.PREC_FP16)):
         with pytest.raises(snap.SnapMRFError, match="atom_norms"):
             snap.MRF_match(1, img, 1, 1, 10, 10, 4, 4, 4, atom_norms=1, stream=0, **kw)
+
+
+def test_epg_jvp_refuses_bad_arguments_before_any_device_work(snap):
+    """The forward-mode entry point checks its pointers, sizes and echo type
+    before it touches the device (no GPU needed)."""
+    h = np.zeros((4, 8), np.float32)
+    with pytest.raises(snap.SnapMRFError, match="null pointer"):
+        snap.epg_jvp(None, h, 8, 8, 1, None)
+    with pytest.raises(snap.SnapMRFError, match="bad sizes"):
+        snap.epg_jvp(1, h, 8, 8, 0, 1)
+    with pytest.raises(snap.SnapMRFError, match="echo type"):
+        snap.epg_jvp(1, h, 8, 8, 1, 1, echo_type="epg_ssfp")
